@@ -1,0 +1,252 @@
+"""CPU oracles for the ALPACA block right-hand side (TEST INFRASTRUCTURE ONLY).
+
+Two independent implementations of the same path, used only by ``tests/``,
+``__graft_entry__.smoke()`` and ``bench.py``'s CPU arm, always as the checker of
+the CUDA path and never as the thing measured or shipped:
+
+* :class:`Restatement` - ``oracle/alpaca_oracle.c``, a plain-C restatement of
+  the reference (tumaer/ALPACA) hot path, built to ``oracle/_build/liboracle.so``.
+* :class:`Reference` - ALPACA's own sources compiled in place by
+  ``oracle/Makefile`` into ``oracle/_ref/libalpref_d<D>_<variant>.so`` (absent
+  when the reference sources were not available at build time).
+
+Both expose the same methods on numpy arrays in the reference's block layout:
+``u[nb, ne, TCX, TCY, TCZ]`` (TC = 24 in active, 1 in inactive dimensions).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+FLUX_SPLITTING, FINITE_VOLUME = 0, 1
+RECON_CONSERVATIVE, RECON_PRIMITIVE, RECON_CHARACTERISTIC = 0, 1, 2
+
+# variant name -> (solver, reconstruction), as selected in the reference's
+# user_specifications/riemann_solver_settings.h and state_reconstruction_settings.h
+VARIANTS = {
+    "fvchar": (FINITE_VOLUME, RECON_CHARACTERISTIC),
+    "fvprim": (FINITE_VOLUME, RECON_PRIMITIVE),
+    "fsroe": (FLUX_SPLITTING, RECON_CHARACTERISTIC),
+}
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_D)
+
+
+def _ip(a: np.ndarray):
+    assert a.dtype == np.int32 and a.flags.c_contiguous
+    return a.ctypes.data_as(_I)
+
+
+def build(quiet: bool = True) -> None:
+    """Build both oracles (make -C oracle); the reference part needs its sources."""
+    out = subprocess.run(["make", "-C", HERE, "-j", str(os.cpu_count() or 4), "all"],
+                         capture_output=True, text=True)
+    if out.returncode != 0:
+        raise RuntimeError("oracle build failed:\n" + out.stdout[-4000:] + out.stderr[-4000:])
+    if not quiet:
+        print(out.stdout[-2000:])
+
+
+def geometry(dim: int):
+    tc = tuple(24 if d < dim else 1 for d in range(3))
+    ic = tuple(16 if d < dim else 1 for d in range(3))
+    return tc, ic
+
+
+class _Common:
+    dim: int
+    ne: int
+
+    def _shapes(self, nb):
+        tc, ic = geometry(self.dim)
+        return (nb, self.ne) + tc, (nb, self.ne) + tuple(n + 1 for n in ic)
+
+
+class Restatement(_Common):
+    """The plain-C restatement, for one dimension and scheme variant."""
+
+    _lib = None
+
+    def __init__(self, dim: int, variant: str = "fvchar"):
+        if Restatement._lib is None:
+            if not os.path.exists(RESTATEMENT_SO):
+                build()
+            lib = C.CDLL(RESTATEMENT_SO)
+            lib.oracle_weno5.argtypes = [_D, _D, _D]
+            lib.oracle_eos.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, _D, _D, _D]
+            lib.oracle_prime_states.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int, _D]
+            lib.oracle_space_rhs.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, C.c_double,
+                                             C.c_double, C.c_int, C.c_double, _D, _D, _D, _D, C.c_int]
+            lib.oracle_timestep.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int,
+                                            C.c_double, C.c_double, C.c_double, C.c_double, _D]
+            lib.oracle_halo_fill.argtypes = [C.c_int, _D, C.c_int, C.c_int, _I, C.c_int]
+            lib.oracle_halo_update.argtypes = [C.c_int, _D, C.c_int, _I]
+            lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
+                                       C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.c_int, C.c_int, _D, _I, _D]
+            Restatement._lib = lib
+        self.lib = Restatement._lib
+        self.dim = dim
+        self.ne = dim + 2
+        self.variant = variant
+        self.solver, self.recon = VARIANTS[variant]
+
+    # -- scalar kernels --
+    def weno5(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        l, r = C.c_double(), C.c_double()
+        self.lib.oracle_weno5(_dp(v), C.byref(l), C.byref(r))
+        return l.value, r.value
+
+    def eos(self, gamma, B, safe, cons, prim):
+        cons = np.ascontiguousarray(cons, dtype=np.float64)
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        out = np.zeros(6)
+        self.lib.oracle_eos(self.dim, gamma, B, int(safe), _dp(cons), _dp(prim), _dp(out))
+        return out
+
+    # -- block kernels --
+    def prime_states(self, u, gamma, B=0.0, safe=False):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p = np.empty_like(u)
+        self.lib.oracle_prime_states(self.dim, _dp(u), u.shape[0], gamma, B, int(safe), _dp(p))
+        return p
+
+    def space_rhs(self, u, gamma, B, safe, cell_size, nthreads=1):
+        """Returns (fx, fy, fz, rhs) for blocks whose halos are filled."""
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        nb = u.shape[0]
+        _, fshape = self._shapes(nb)
+        fx, fy, fz = (np.zeros(fshape) for _ in range(3))
+        rhs = np.zeros_like(u)
+        rc = self.lib.oracle_space_rhs(self.dim, self.solver, self.recon, _dp(u), nb, gamma, B,
+                                       int(safe), cell_size, _dp(fx), _dp(fy), _dp(fz), _dp(rhs),
+                                       nthreads)
+        if rc:
+            raise RuntimeError(f"oracle_space_rhs rc={rc}")
+        return fx, fy, fz, rhs
+
+    def timestep(self, u, gamma, B, safe, cell_size, cfl, t=0.0, t_end=1e300):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        dt = C.c_double()
+        self.lib.oracle_timestep(self.dim, _dp(u), u.shape[0], gamma, B, int(safe), cell_size, cfl,
+                                 t, t_end, C.byref(dt))
+        return dt.value
+
+    def halo_fill(self, u, nbr26, faces_only=False):
+        """In-place same-level halo copy over 26 (or 2*dim face) regions."""
+        assert u.dtype == np.float64 and u.flags.c_contiguous
+        nbr26 = np.ascontiguousarray(nbr26, dtype=np.int32)
+        self.lib.oracle_halo_fill(self.dim, _dp(u), u.shape[0], u.shape[1], _ip(nbr26),
+                                  int(faces_only))
+        return u
+
+    def halo_update(self, u, nbr):
+        """In-place six-face halo copy plus zero-gradient slabs on domain faces."""
+        assert u.dtype == np.float64 and u.flags.c_contiguous
+        nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+        self.lib.oracle_halo_update(self.dim, _dp(u), u.shape[0], _ip(nbr))
+        return u
+
+    def run(self, u, nbr, gamma, B, safe, cell_size, cfl, t_end, max_steps=0, t0=0.0,
+            nthreads=1):
+        """Single-level time loop. Returns (u_final, t, steps, dt_log)."""
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+        cap = max_steps if max_steps > 0 else 1000000
+        dts = np.zeros(cap)
+        t = C.c_double(t0)
+        steps = C.c_int()
+        rc = self.lib.oracle_run(self.dim, self.solver, self.recon, _dp(u), u.shape[0], _ip(nbr),
+                                 gamma, B, int(safe), cell_size, cfl, t_end, max_steps, nthreads,
+                                 C.byref(t), C.byref(steps), _dp(dts))
+        if rc:
+            raise RuntimeError(f"oracle_run rc={rc}")
+        return u, t.value, steps.value, dts[: steps.value].copy()
+
+
+class Reference(_Common):
+    """ALPACA's own hot-path code (oracle/_ref), one library per dimension and variant."""
+
+    _libs: dict = {}
+
+    @staticmethod
+    def available(dim: int = 3, variant: str = "fvchar") -> bool:
+        return os.path.exists(os.path.join(REF_DIR, f"libalpref_d{dim}_{variant}.so"))
+
+    def __init__(self, dim: int, variant: str = "fvchar"):
+        key = (dim, variant)
+        path = os.path.join(REF_DIR, f"libalpref_d{dim}_{variant}.so")
+        if key not in Reference._libs:
+            if not os.path.exists(path):
+                raise FileNotFoundError(path)
+            lib = C.CDLL(path)
+            lib.ref_config.argtypes = [_I] * 5
+            lib.ref_weno5.argtypes = [_D, _D, _D]
+            lib.ref_eos.argtypes = [C.c_double, C.c_double, C.c_int, _D, _D, _D]
+            lib.ref_prime_states.argtypes = [_D, C.c_int, C.c_double, C.c_double, C.c_int, _D]
+            lib.ref_space_rhs.argtypes = [_D, C.c_int, C.c_double, C.c_double, C.c_int, C.c_double,
+                                          _D, _D, _D, _D, C.c_int]
+            lib.ref_run.argtypes = [_D, C.c_int, _I, C.c_double, C.c_double, C.c_int, C.c_double,
+                                    C.c_double, C.c_double, C.c_int, C.c_int, _D, _I, _D]
+            Reference._libs[key] = lib
+        self.lib = Reference._libs[key]
+        vals = [C.c_int() for _ in range(5)]
+        self.lib.ref_config(*[C.byref(v) for v in vals])
+        self.dim, self.ne = vals[0].value, vals[1].value
+        assert self.dim == dim
+        self.variant = variant
+
+    def weno5(self, v):
+        v = np.ascontiguousarray(v, dtype=np.float64)
+        l, r = C.c_double(), C.c_double()
+        self.lib.ref_weno5(_dp(v), C.byref(l), C.byref(r))
+        return l.value, r.value
+
+    def eos(self, gamma, B, safe, cons, prim):
+        cons = np.ascontiguousarray(cons, dtype=np.float64)
+        prim = np.ascontiguousarray(prim, dtype=np.float64)
+        out = np.zeros(6)
+        self.lib.ref_eos(gamma, B, int(safe), _dp(cons), _dp(prim), _dp(out))
+        return out
+
+    def prime_states(self, u, gamma, B=0.0, safe=False):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        p = np.empty_like(u)
+        self.lib.ref_prime_states(_dp(u), u.shape[0], gamma, B, int(safe), _dp(p))
+        return p
+
+    def space_rhs(self, u, gamma, B, safe, cell_size, nthreads=1):
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        nb = u.shape[0]
+        _, fshape = self._shapes(nb)
+        fx, fy, fz = (np.zeros(fshape) for _ in range(3))
+        rhs = np.zeros_like(u)
+        self.lib.ref_space_rhs(_dp(u), nb, gamma, B, int(safe), cell_size, _dp(fx), _dp(fy),
+                               _dp(fz), _dp(rhs), nthreads)
+        return fx, fy, fz, rhs
+
+    def run(self, u, nbr, gamma, B, safe, cell_size, cfl, t_end, max_steps=0, t0=0.0,
+            nthreads=1):
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        nbr = np.ascontiguousarray(nbr, dtype=np.int32)
+        cap = max_steps if max_steps > 0 else 1000000
+        dts = np.zeros(cap)
+        t = C.c_double(t0)
+        steps = C.c_int()
+        self.lib.ref_run(_dp(u), u.shape[0], _ip(nbr), gamma, B, int(safe), cell_size, cfl, t_end,
+                         max_steps, nthreads, C.byref(t), C.byref(steps), _dp(dts))
+        return u, t.value, steps.value, dts[: steps.value].copy()

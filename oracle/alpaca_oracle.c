@@ -1,0 +1,994 @@
+/* TEST INFRASTRUCTURE ONLY — the CPU oracle, never part of the product path.
+ *
+ * Plain-C restatement of tumaer/ALPACA's per-block finite-volume right-hand
+ * side, halo fill, CFL time step and SSP-RK3 stage update. Each function cites
+ * the reference lines it restates (paths relative to ALPACA's src/). Every
+ * multiply and add is written in the reference's association order, and the
+ * file is compiled with -ffp-contract=off, so on the same inputs it reproduces
+ * the reference compiled with the same flags bit for bit (checked by
+ * tests/test_oracle.py against oracle/_ref, the reference's own sources built
+ * by oracle/Makefile).
+ *
+ * Supported selections (user_specifications): EquationSet::Euler;
+ * ConvectiveTermSolvers::FiniteVolume with StateReconstructionType::
+ * Characteristic or Primitive, ReconstructionStencils::WENO5,
+ * RiemannSolvers::Hllc and SignalSpeed::Einfeldt; ConvectiveTermSolvers::
+ * FluxSplitting with FluxSplitting::Roe; TimeIntegrators::RK3; FUSY on;
+ * StiffenedGas and StiffenedGasSafe.
+ */
+#include "alpaca_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define IC 16
+#define HS 4
+#define TC (IC + 2 * HS)
+#define MAXNE 5
+
+enum { MASS = 0, ENERGY = 1, MOMX = 2 };     /* field_setup.h:101-112 */
+enum { RHO = 0, PRES = 1, VELX = 2 };        /* field_setup.h:114-130 */
+
+typedef struct {
+  int dim, ne, np;
+  int tc[3], ic[3];
+  long cells, faces;
+} Geom;
+
+static Geom make_geom(int dim) {
+  Geom g;
+  g.dim = dim;
+  g.ne = dim + 2;
+  g.np = dim + 2;
+  for (int d = 0; d < 3; ++d) {
+    g.tc[d] = d < dim ? TC : 1;
+    g.ic[d] = d < dim ? IC : 1;
+  }
+  g.cells = (long)g.tc[0] * g.tc[1] * g.tc[2];
+  g.faces = (long)(g.ic[0] + 1) * (g.ic[1] + 1) * (g.ic[2] + 1);
+  return g;
+}
+
+static inline long cidx(const Geom *g, int i, int j, int k) {
+  return ((long)i * g->tc[1] + j) * g->tc[2] + k;
+}
+static inline long fidx(const Geom *g, int i, int j, int k) {
+  return ((long)i * (g->ic[1] + 1) + j) * (g->ic[2] + 1) + k;
+}
+/* first / last interior index per dimension (compile_time_constants.h:314-347) */
+static inline int fic(const Geom *g, int d) { return d < g->dim ? HS : 0; }
+static inline int lic(const Geom *g, int d) { return d < g->dim ? HS + IC - 1 : 0; }
+
+typedef struct {
+  int dim;
+  double gamma, B;
+  int safe;
+} Eos;
+
+/* std::min / std::max with the reference's tie behaviour */
+static inline double dmin(double a, double b) { return (b < a) ? b : a; }
+static inline double dmax(double a, double b) { return (a < b) ? b : a; }
+
+/* ConsistencyManagedSum with FUSY on (utilities/mathematical_functions.h:79-89) */
+static double cms3(double a, double b, double c) {
+  double const s1 = (a + b) + c;
+  double const s2 = (a + c) + b;
+  double const s3 = (b + c) + a;
+  double mn = s1, mx = s1;
+  if (s2 < mn) mn = s2;
+  if (s3 < mn) mn = s3;
+  if (mx < s2) mx = s2;
+  if (mx < s3) mx = s3;
+  return 0.5 * (mn + mx);
+}
+
+/* DimensionAwareConsistencyManagedSum (mathematical_functions.h:98-108) */
+static inline double dacms(int dim, double a, double b, double c) {
+  if (dim == 1) return a;
+  if (dim == 2) return a + b;
+  return cms3(a, b, c);
+}
+
+/* ConsistencyManagedSum(std::array<double, DIM>) (mathematical_functions.h:130-150) */
+static inline double cms_array(int dim, const double *v) {
+  if (dim == 1) return v[0];
+  if (dim == 2) return v[0] + v[1];
+  return cms3(v[0], v[1], v[2]);
+}
+
+/* ---- equation of state ------------------------------------------------- */
+
+/* GenericStiffenedGas::CalculatePressure<false> (generic_stiffened_gas.h:40-57),
+ * StiffenedGasSafe::ComputePressure (stiffened_gas_safe.cpp:61-75) */
+static double eos_pressure(const Eos *e, double mass, double mx, double my,
+                           double mz, double energy) {
+  if (e->safe) {
+    double const p = -e->gamma * e->B +
+                     (e->gamma - 1.0) *
+                         (energy - 0.5 * dacms(e->dim, mx * mx, my * my, mz * mz) /
+                                       dmax(mass, DBL_EPSILON));
+    return dmax(p, -e->B + DBL_EPSILON);
+  }
+  double const q = 0.5 * dacms(e->dim, mx * mx, my * my, mz * mz);
+  return -e->gamma * e->B + (e->gamma - 1.0) * (energy - q / mass);
+}
+
+/* StiffenedGas::ComputeEnthalpy (stiffened_gas.cpp:88-96), safe: stiffened_gas_safe.cpp:77-84 */
+static double eos_enthalpy(const Eos *e, double mass, double mx, double my,
+                           double mz, double energy) {
+  double const p = eos_pressure(e, mass, mx, my, mz, energy);
+  if (e->safe) return (energy + p) / dmax(mass, DBL_EPSILON);
+  return (energy + p) / mass;
+}
+
+/* GenericStiffenedGas::CalculateEnergy (generic_stiffened_gas.h:70-79) */
+static double eos_energy(const Eos *e, double rho, double u, double v, double w,
+                         double p) {
+  return (p + e->gamma * e->B) / (e->gamma - 1.0) +
+         (0.5 * dacms(e->dim, u * u, v * v, w * w) * rho);
+}
+
+/* GenericStiffenedGas::CalculateSpeedOfSound (generic_stiffened_gas.h:90-102),
+ * StiffenedGasSafe::ComputeSpeedOfSound (stiffened_gas_safe.cpp:140-146) */
+static double eos_speed_of_sound(const Eos *e, double rho, double p) {
+  if (e->safe) {
+    double const c2 = e->gamma * (p + e->B) / dmax(rho, DBL_EPSILON);
+    return sqrt(dmax(c2, DBL_EPSILON));
+  }
+  return sqrt(e->gamma * (p + e->B) / rho);
+}
+
+/* StiffenedGas::ComputePsi (stiffened_gas.cpp:133-136) */
+static inline double eos_psi(const Eos *e, double p, double one_rho) {
+  return (p + e->gamma * e->B) * one_rho;
+}
+
+/* StiffenedGas::GetGruneisen (stiffened_gas.cpp:113) */
+static inline double eos_gruneisen(const Eos *e) { return e->gamma - 1.0; }
+
+/* ConservativesToPrimeStates (prime_state_handler.h:277-371), Euler set */
+static void cons_to_prim(const Eos *e, const double *c, double *p) {
+  int const dim = e->dim;
+  p[RHO] = c[MASS];
+  double const one_density = 1.0 / c[MASS];
+  for (int d = 0; d < dim; ++d) p[VELX + d] = c[MOMX + d] * one_density;
+  p[PRES] = eos_pressure(e, c[MASS], c[MOMX], dim > 1 ? c[MOMX + 1] : 0.0,
+                         dim > 2 ? c[MOMX + 2] : 0.0, c[ENERGY]);
+}
+
+/* PrimeStatesToConservatives (prime_state_handler.h:195-275), Euler set */
+static void prim_to_cons(const Eos *e, const double *p, double *c) {
+  int const dim = e->dim;
+  c[MASS] = p[RHO];
+  for (int d = 0; d < dim; ++d) c[MOMX + d] = p[VELX + d] * p[RHO];
+  c[ENERGY] = eos_energy(e, p[RHO], p[VELX], dim > 1 ? p[VELX + 1] : 0.0,
+                         dim > 2 ? p[VELX + 2] : 0.0, p[PRES]);
+}
+
+/* ---- WENO5-JS (stencils/spatial_reconstruction_stencils/weno5.h:88-158) -- */
+
+/* evaluation properties {offset, sign}: UpwindLeft {0,1}, UpwindRight {1,-1}
+ * (stencils/apply_wrapper.h:47-57); downstream stencil size 2. */
+static double weno5(const double *a, int offset, int sign) {
+  double const v1 = a[2 + offset - 2 * sign];
+  double const v2 = a[2 + offset - 1 * sign];
+  double const v3 = a[2 + offset];
+  double const v4 = a[2 + offset + 1 * sign];
+  double const v5 = a[2 + offset + 2 * sign];
+  double const c1 = 13.0 / 12.0, c2 = 0.25;
+
+  double const s11 = 1.0 * v1 + -2.0 * v2 + 1.0 * v3;
+  double const s12 = 1.0 * v1 + -4.0 * v2 + 3.0 * v3;
+  double const s1 = c1 * s11 * s11 + c2 * s12 * s12;
+  double const s21 = 1.0 * v2 + -2.0 * v3 + 1.0 * v4;
+  double const s22 = 1.0 * v2 + -1.0 * v4;
+  double const s2 = c1 * s21 * s21 + c2 * s22 * s22;
+  double const s31 = 1.0 * v3 + -2.0 * v4 + 1.0 * v5;
+  double const s32 = 3.0 * v3 + -4.0 * v4 + 1.0 * v5;
+  double const s3 = c1 * s31 * s31 + c2 * s32 * s32;
+
+  double const eps = 1.0e-6;
+  double const a1 = 0.1 / ((s1 + eps) * (s1 + eps));
+  double const a2 = 0.6 / ((s2 + eps) * (s2 + eps));
+  double const a3 = 0.3 / ((s3 + eps) * (s3 + eps));
+  double const one_a_sum = 1.0 / (a1 + a2 + a3);
+  double const w1 = a1 * one_a_sum;
+  double const w2 = a2 * one_a_sum;
+  double const w3 = a3 * one_a_sum;
+
+  return w1 * (2.0 / 6.0 * v1 + -7.0 / 6.0 * v2 + 11.0 / 6.0 * v3) +
+         w2 * (-1.0 / 6.0 * v2 + 5.0 / 6.0 * v3 + 2.0 / 6.0 * v4) +
+         w3 * (2.0 / 6.0 * v3 + 5.0 / 6.0 * v4 + -1.0 / 6.0 * v5);
+}
+static inline double weno5_left(const double *a) { return weno5(a, 0, 1); }
+static inline double weno5_right(const double *a) { return weno5(a, 1, -1); }
+
+/* ---- Roe eigensystem (solvers/eigendecomposition.h:181-467) ------------ */
+
+/* minor directions (eigendecomposition.h:84-125) */
+static inline int minor_dir(int dir, int m) {
+  static const int tab[3][2] = {{1, 2}, {0, 2}, {0, 1}};
+  return tab[dir][m];
+}
+
+/* symmetry-preserving summation sequences
+ * (solvers/state_reconstruction/state_reconstruction.h:35-58) */
+static const int *summation_sequence(int dim, int dir) {
+  static const int s1[3] = {MOMX, MASS, ENERGY};
+  static const int s2[4] = {MOMX, MOMX + 1, MASS, ENERGY};
+  static const int s3[3][5] = {{MOMX + 1, MOMX + 2, MOMX, MASS, ENERGY},
+                               {MOMX + 2, MOMX, MOMX + 1, MASS, ENERGY},
+                               {MOMX, MOMX + 1, MOMX + 2, MASS, ENERGY}};
+  if (dim == 1) return s1;
+  if (dim == 2) return s2;
+  return s3[dir];
+}
+
+typedef struct {
+  double L[MAXNE][MAXNE];
+  double R[MAXNE][MAXNE];
+  double ev[MAXNE];
+} Eigen;
+
+/* One face of ComputeRoeEigendecomposition<DIR> between cell t and neighbour n.
+ * u: conservatives of the block, p: prime states of the block. Leaves the
+ * output untouched when a density is non-positive (eigendecomposition.h:244). */
+static void roe_eigen(const Geom *g, const Eos *e, int dir, const double *u,
+                      const double *p, long t, long n, Eigen *out) {
+  int const dim = g->dim, ne = g->ne;
+  long const C = g->cells;
+  double const rho_t = u[MASS * C + t], rho_n = u[MASS * C + n];
+  if (rho_t <= 0.0 || rho_n <= 0.0) return;
+  int const principal = dir;
+  int const minor1 = dim > 1 ? minor_dir(dir, 0) : 0;
+  int const minor2 = dim > 2 ? minor_dir(dir, 1) : 0;
+  int const ev_principal = dim;
+  double const gru = eos_gruneisen(e);
+
+  double const one_rho_t = 1.0 / rho_t;
+  double const energy_t = u[ENERGY * C + t];
+  double const mx_t = u[MOMX * C + t];
+  double const my_t = dim > 1 ? u[(MOMX + 1) * C + t] : 0.0;
+  double const mz_t = dim > 2 ? u[(MOMX + 2) * C + t] : 0.0;
+  double const up_t = p[(VELX + principal) * C + t];
+  double const u1_t = dim > 1 ? p[(VELX + minor1) * C + t] : 0.0;
+  double const u2_t = dim > 2 ? p[(VELX + minor2) * C + t] : 0.0;
+  double const p_t = p[PRES * C + t];
+  double const psi_t = eos_psi(e, p_t, one_rho_t);
+
+  double const one_rho_n = 1.0 / rho_n;
+  double const energy_n = u[ENERGY * C + n];
+  double const mx_n = u[MOMX * C + n];
+  double const my_n = dim > 1 ? u[(MOMX + 1) * C + n] : 0.0;
+  double const mz_n = dim > 2 ? u[(MOMX + 2) * C + n] : 0.0;
+  double const up_n = p[(VELX + principal) * C + n];
+  double const u1_n = dim > 1 ? p[(VELX + minor1) * C + n] : 0.0;
+  double const u2_n = dim > 2 ? p[(VELX + minor2) * C + n] : 0.0;
+  double const p_n = p[PRES * C + n];
+  double const psi_n = eos_psi(e, p_n, one_rho_n);
+
+  double const sr_t = sqrt(rho_t);
+  double const sr_n = sqrt(rho_n);
+  double const rho_div = 1.0 / (sr_t + sr_n);
+  double const rho_roe = sr_t * sr_n;
+  double const one_rho_roe = 1.0 / rho_roe;
+
+  double const up = ((up_t * sr_t) + (up_n * sr_n)) * rho_div;
+  double const u1 = ((u1_t * sr_t) + (u1_n * sr_n)) * rho_div;
+  double const u2 = ((u2_t * sr_t) + (u2_n * sr_n)) * rho_div;
+  double const psi = ((psi_t * sr_t) + (psi_n * sr_n)) * rho_div;
+  double const H = (eos_enthalpy(e, rho_t, mx_t, my_t, mz_t, energy_t) * sr_t +
+                    eos_enthalpy(e, rho_n, mx_n, my_n, mz_n, energy_n) * sr_n) *
+                   rho_div;
+
+  double const q2 = dacms(dim, up * up, u1 * u1, u2 * u2);
+  double const tmp = dacms(dim, (up_t - up_n) * (up_t - up_n),
+                           (u1_t - u1_n) * (u1_t - u1_n),
+                           (u2_t - u2_n) * (u2_t - u2_n));
+  double const p_over_rho =
+      ((p_t * one_rho_t) * sr_t + (p_n * one_rho_n) * sr_n) * rho_div +
+      0.5 * rho_roe * (rho_div * rho_div) * tmp;
+  double const cc = psi + gru * p_over_rho;
+  double const one_cc = 1.0 / cc;
+  double const c = sqrt(cc);
+
+  int const mP = MOMX + principal, m1 = MOMX + minor1, m2 = MOMX + minor2;
+  double(*L)[MAXNE] = out->L;
+  double(*R)[MAXNE] = out->R;
+
+  /* left eigenvectors (eigendecomposition.h:316-359) */
+  L[0][MASS] = 0.5 * one_cc * (gru * q2 - gru * H + (up + c) * c);
+  L[0][mP] = 0.5 * one_cc * (-up * gru - c);
+  if (dim > 1) L[0][m1] = 0.5 * one_cc * (-u1 * gru);
+  if (dim > 2) L[0][m2] = 0.5 * one_cc * (-u2 * gru);
+  L[0][ENERGY] = 0.5 * one_cc * gru;
+  if (dim > 1) {
+    L[1][MASS] = u1 * one_rho_roe;
+    L[1][mP] = 0.0;
+    L[1][m1] = -one_rho_roe;
+    if (dim > 2) L[1][m2] = 0.0;
+    L[1][ENERGY] = 0.0;
+  }
+  if (dim > 2) {
+    L[2][MASS] = -u2 * one_rho_roe;
+    L[2][mP] = 0.0;
+    L[2][m1] = 0.0;
+    L[2][m2] = one_rho_roe;
+    L[2][ENERGY] = 0.0;
+  }
+  L[ev_principal][MASS] = one_cc * (H - q2);
+  L[ev_principal][mP] = one_cc * up;
+  if (dim > 1) L[ev_principal][m1] = one_cc * u1;
+  if (dim > 2) L[ev_principal][m2] = one_cc * u2;
+  L[ev_principal][ENERGY] = -one_cc;
+  L[ne - 1][MASS] = 0.5 * one_cc * (gru * q2 - gru * H - (up - c) * c);
+  L[ne - 1][mP] = 0.5 * one_cc * (-up * gru + c);
+  if (dim > 1) L[ne - 1][m1] = 0.5 * one_cc * (-u1 * gru);
+  if (dim > 2) L[ne - 1][m2] = 0.5 * one_cc * (-u2 * gru);
+  L[ne - 1][ENERGY] = 0.5 * one_cc * gru;
+
+  /* right eigenvectors (eigendecomposition.h:366-409) */
+  R[MASS][0] = 1.0;
+  if (dim > 1) R[MASS][1] = 0.0;
+  if (dim > 2) R[MASS][2] = 0.0;
+  R[MASS][ev_principal] = gru;
+  R[MASS][ne - 1] = 1.0;
+  R[mP][0] = up - c;
+  if (dim > 1) R[mP][1] = 0.0;
+  if (dim > 2) R[mP][2] = 0.0;
+  R[mP][ev_principal] = gru * up;
+  R[mP][ne - 1] = up + c;
+  if (dim > 1) {
+    R[m1][0] = u1;
+    R[m1][1] = -rho_roe;
+    if (dim > 2) R[m1][2] = 0.0;
+    R[m1][ev_principal] = gru * u1;
+    R[m1][ne - 1] = u1;
+  }
+  if (dim > 2) {
+    R[m2][0] = u2;
+    R[m2][1] = 0.0;
+    R[m2][2] = rho_roe;
+    R[m2][ev_principal] = gru * u2;
+    R[m2][ne - 1] = u2;
+  }
+  R[ENERGY][0] = H - up * c;
+  if (dim > 1) R[ENERGY][1] = -u1 * rho_roe;
+  if (dim > 2) R[ENERGY][2] = rho_roe * u2;
+  R[ENERGY][ev_principal] = gru * H - c * c;
+  R[ENERGY][ne - 1] = H + up * c;
+
+  /* Roe flux-splitting wave speeds (eigendecomposition.h:416-421, 64-72) */
+  out->ev[0] = fabs(up - c);
+  out->ev[ne - 1] = fabs(up + c);
+  for (int l = 1; l < ne - 1; ++l) out->ev[l] = fabs(up);
+}
+
+/* TransformToPhysicalSpace (eigendecomposition.h:144-165) */
+static void to_physical(int ne, const double *ch, double R[MAXNE][MAXNE],
+                        double *out) {
+  for (int l = 0; l < ne; ++l) {
+    out[l] = 0.0;
+    for (int n = 1; n < ne - 1; ++n) out[l] += ch[n] * R[l][n];
+    out[l] += (ch[0] * R[l][0] + ch[ne - 1] * R[l][ne - 1]);
+  }
+}
+
+/* ---- HLLC with Einfeldt signal speeds ---------------------------------- */
+
+/* CalculateSignalSpeed, Einfeldt branch (hll_signal_speed_calculator.h:77-101) */
+static void einfeldt(double rl, double rr, double ul, double ur, double cl,
+                     double cr, double *sl, double *sr) {
+  double const srl = sqrt(rl);
+  double const srr = sqrt(rr);
+  double const rho_div = 1.0 / (srl + srr);
+  double const u_roe = ((ul * srl) + (ur * srr)) * rho_div;
+  double const c_e = sqrt(((cl * cl * srl) + (cr * cr * srr)) * rho_div +
+                          (0.5 * srl * srr * rho_div * rho_div) * (ur - ul) *
+                              (ur - ul));
+  *sl = dmin(u_roe - c_e, ul - cl);
+  *sr = dmax(u_roe + c_e, ur + cr);
+}
+
+static inline int signum(double x) { return (0.0 < x) - (x < 0.0); }
+
+/* HllcRiemannSolver::SolveRiemannProblemImplementation
+ * (riemann_solvers/hllc_riemann_solver.h:52-198) */
+static void hllc(const Eos *e, int dir, const double *cl, const double *cr,
+                 const double *pl, const double *pr, double *flux) {
+  int const dim = e->dim, ne = dim + 2;
+  int const mP = MOMX + dir, vP = VELX + dir;
+  double qsl[MAXNE], qsr[MAXNE], fl[MAXNE], fr[MAXNE];
+
+  double const pres_l = pl[PRES], pres_r = pr[PRES];
+  double const one_rl = 1.0 / cl[MASS], one_rr = 1.0 / cr[MASS];
+  double const vel_l = pl[vP], vel_r = pr[vP];
+  double const c_l = eos_speed_of_sound(e, cl[MASS], pres_l);
+  double const c_r = eos_speed_of_sound(e, cr[MASS], pres_r);
+  double sls, srs;
+  einfeldt(cl[MASS], cr[MASS], vel_l, vel_r, c_l, c_r, &sls, &srs);
+  double const s_star =
+      ((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r))) /
+      (cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
+  double const sl = dmin(sls, 0.0);
+  double const sr = dmax(srs, 0.0);
+  double const chi_l = (sls - vel_l) / (sls - s_star);
+  double const chi_r = (srs - vel_r) / (srs - s_star);
+
+  qsl[MASS] = cl[MASS] * chi_l;
+  qsl[mP] = cl[MASS] * chi_l * s_star;
+  qsl[ENERGY] = cl[MASS] * chi_l *
+                (cl[ENERGY] * one_rl +
+                 (s_star - vel_l) * (s_star + pres_l / (cl[MASS] * (sl - vel_l))));
+  qsr[MASS] = cr[MASS] * chi_r;
+  qsr[mP] = cr[MASS] * chi_r * s_star;
+  qsr[ENERGY] = cr[MASS] * chi_r *
+                (cr[ENERGY] * one_rr +
+                 (s_star - vel_r) * (s_star + pres_r / (cr[MASS] * (sr - vel_r))));
+
+  fl[MASS] = cl[mP];
+  fl[mP] = ((cl[mP] * cl[mP]) * one_rl) + pres_l;
+  fl[ENERGY] = vel_l * (cl[ENERGY] + pres_l);
+  fr[MASS] = cr[mP];
+  fr[mP] = ((cr[mP] * cr[mP]) * one_rr) + pres_r;
+  fr[ENERGY] = vel_r * (cr[ENERGY] + pres_r);
+
+  for (int d = 0; d < dim - 1; ++d) {
+    int const mm = MOMX + minor_dir(dir, d);
+    qsl[mm] = chi_l * cl[mm];
+    qsr[mm] = chi_r * cr[mm];
+    fl[mm] = vel_l * cl[mm];
+    fr[mm] = vel_r * cr[mm];
+  }
+  int const sg = signum(s_star);
+  for (int n = 0; n < ne; ++n) {
+    double const fsl = fl[n] + (sl * (qsl[n] - cl[n]));
+    double const fsr = fr[n] + (sr * (qsr[n] - cr[n]));
+    flux[n] = (0.5 * (1.0 + sg) * fsl + 0.5 * (1.0 - sg) * fsr);
+  }
+}
+
+/* ---- per-block right-hand side ----------------------------------------- */
+
+typedef struct {
+  double *prim;   /* [np][cells] */
+  Eigen *eig;     /* [faces] */
+  double *adv;    /* [ne][cells] (flux splitting) */
+} Work;
+
+static void work_alloc(const Geom *g, Work *w) {
+  w->prim = (double *)malloc(sizeof(double) * g->np * g->cells);
+  w->eig = (Eigen *)malloc(sizeof(Eigen) * g->faces);
+  w->adv = (double *)malloc(sizeof(double) * g->ne * g->cells);
+}
+static void work_free(Work *w) {
+  free(w->prim);
+  free(w->eig);
+  free(w->adv);
+}
+
+/* block-wide prime states (prime_state_handler.h:141-152) */
+static void block_primes(const Geom *g, const Eos *e, const double *u, double *p) {
+  double c[MAXNE], q[MAXNE];
+  for (long x = 0; x < g->cells; ++x) {
+    for (int f = 0; f < g->ne; ++f) c[f] = u[f * g->cells + x];
+    cons_to_prim(e, c, q);
+    for (int f = 0; f < g->np; ++f) p[f * g->cells + x] = q[f];
+  }
+}
+
+/* face-index ranges of ComputeFluxes<DIR> (finite_volume_scheme.cpp:165-188) */
+static void face_range(const Geom *g, int dir, int lo[3], int hi[3], int off[3]) {
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = d == dir ? fic(g, d) - 1 : fic(g, d);
+    hi[d] = lic(g, d);
+    off[d] = d < g->dim ? fic(g, d) - 1 : -1;
+  }
+}
+
+static void eigen_direction(const Geom *g, const Eos *e, int dir, const double *u,
+                            const double *p, Eigen *eig) {
+  int lo[3], hi[3], off[3];
+  face_range(g, dir, lo, hi, off);
+  for (int i = lo[0]; i <= hi[0]; ++i)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int k = lo[2]; k <= hi[2]; ++k) {
+        long const t = cidx(g, i, j, k);
+        long const n = cidx(g, i + (dir == 0), j + (dir == 1), k + (dir == 2));
+        roe_eigen(g, e, dir, u, p, t, n, &eig[fidx(g, i - off[0], j - off[1], k - off[2])]);
+      }
+}
+
+/* FiniteVolumeScheme::ComputeFluxes<DIR> (finite_volume_scheme.cpp:160-251) with
+ * CharacteristicStateReconstruction (characteristic_state_reconstruction.h:57-136)
+ * or PrimitiveStateReconstruction (primitive_state_reconstruction.h:56-107). */
+static void fv_fluxes(const Geom *g, const Eos *e, int recon, int dir,
+                      const double *u, const double *p, Eigen *eig, double *flux) {
+  int const ne = g->ne, np = g->np;
+  long const C = g->cells;
+  int lo[3], hi[3], off[3];
+  face_range(g, dir, lo, hi, off);
+  int const *seq = summation_sequence(g->dim, dir);
+  double const B = e->B;
+  for (int i = lo[0]; i <= hi[0]; ++i)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int k = lo[2]; k <= hi[2]; ++k) {
+        long const fi = fidx(g, i - off[0], j - off[1], k - off[2]);
+        long cells6[6];
+        for (int m = 0; m < 6; ++m) {
+          int const s = m - 2;
+          cells6[m] = cidx(g, i + (dir == 0) * s, j + (dir == 1) * s, k + (dir == 2) * s);
+        }
+        double cm[MAXNE], cp[MAXNE], pm[MAXNE], pp[MAXNE];
+        if (recon == ORACLE_RECON_CHARACTERISTIC) {
+          double chm[MAXNE], chp[MAXNE], uc[6];
+          for (int n = 0; n < ne; ++n) {
+            for (int m = 0; m < 6; ++m) {
+              uc[m] = 0.0;
+              for (int s = 0; s < ne; ++s) {
+                int const l = seq[s];
+                uc[m] += eig[fi].L[n][l] * u[l * C + cells6[m]];
+              }
+            }
+            chm[n] = weno5_left(uc);
+            chp[n] = weno5_right(uc);
+          }
+          to_physical(ne, chm, eig[fi].R, cm);
+          to_physical(ne, chp, eig[fi].R, cp);
+          if (cm[MASS] <= DBL_EPSILON || cp[MASS] <= DBL_EPSILON) continue;
+          cons_to_prim(e, cm, pm);
+          cons_to_prim(e, cp, pp);
+        } else {
+          double arr[6];
+          for (int n = 0; n < np; ++n) {
+            for (int m = 0; m < 6; ++m) arr[m] = p[n * C + cells6[m]];
+            pm[n] = weno5_left(arr);
+            pp[n] = weno5_right(arr);
+          }
+          prim_to_cons(e, pm, cm);
+          prim_to_cons(e, pp, cp);
+        }
+        if (cm[MASS] <= DBL_EPSILON || cp[MASS] <= DBL_EPSILON) continue;
+        if (pm[PRES] <= -B || pp[PRES] <= -B) continue;
+        double f[MAXNE];
+        hllc(e, dir, cm, cp, pm, pp, f);
+        for (int n = 0; n < ne; ++n) flux[n * g->faces + fi] += f[n];
+      }
+}
+
+/* ComputeAdvection<DIR> (flux_splitting_scheme.cpp:42-76) */
+static void advection(const Geom *g, int dir, const double *u, const double *p,
+                      double *adv) {
+  long const C = g->cells;
+  for (long x = 0; x < C; ++x) {
+    double const rho = p[RHO * C + x], pres = p[PRES * C + x];
+    double const energy = u[ENERGY * C + x];
+    double const vel = p[(VELX + dir) * C + x];
+    adv[MASS * C + x] = rho * vel;
+    adv[ENERGY * C + x] = (energy + pres) * vel;
+    for (int d = 0; d < g->dim; ++d)
+      adv[(MOMX + d) * C + x] = rho * (vel * p[(VELX + d) * C + x]);
+    adv[(MOMX + dir) * C + x] += pres;
+  }
+}
+
+/* FluxSplittingScheme::ComputeFluxes<DIR> (flux_splitting_scheme.cpp:185-315) */
+static void fs_fluxes(const Geom *g, int dir, const double *u, const double *adv,
+                      Eigen *eig, double *flux) {
+  int const ne = g->ne;
+  long const C = g->cells;
+  int lo[3], hi[3], off[3];
+  face_range(g, dir, lo, hi, off);
+  int const *seq = summation_sequence(g->dim, dir);
+  for (int i = lo[0]; i <= hi[0]; ++i)
+    for (int j = lo[1]; j <= hi[1]; ++j)
+      for (int k = lo[2]; k <= hi[2]; ++k) {
+        long const fi = fidx(g, i - off[0], j - off[1], k - off[2]);
+        long cells6[6];
+        for (int m = 0; m < 6; ++m) {
+          int const s = m - 2;
+          cells6[m] = cidx(g, i + (dir == 0) * s, j + (dir == 1) * s, k + (dir == 2) * s);
+        }
+        double chf[MAXNE], pos[6], neg[6], phys[MAXNE];
+        for (int n = 0; n < ne; ++n) {
+          double const alpha = eig[fi].ev[n];
+          for (int m = 0; m < 6; ++m) {
+            pos[m] = 0.0;
+            neg[m] = 0.0;
+            for (int s = 0; s < ne; ++s) {
+              int const l = seq[s];
+              double const uct = u[l * C + cells6[m]] * eig[fi].L[n][l];
+              double const act = adv[l * C + cells6[m]] * eig[fi].L[n][l];
+              pos[m] += (act + alpha * uct);
+              neg[m] += (act - alpha * uct);
+            }
+          }
+          chf[n] = 0.5 * (weno5_left(pos) + weno5_right(neg));
+        }
+        to_physical(ne, chf, eig[fi].R, phys);
+        for (int l = 0; l < ne; ++l) flux[l * g->faces + fi] += phys[l];
+      }
+}
+
+/* Convective fluxes of one block (FiniteVolumeScheme::UpdateImplementation,
+ * finite_volume_scheme.cpp:45-145; FluxSplittingScheme::UpdateImplementation,
+ * flux_splitting_scheme.cpp:97-168). fx, fy, fz are zeroed first as
+ * SpaceSolver::UpdateFluxes does (space_solver.cpp:89-98). */
+static void block_fluxes(const Geom *g, const Eos *e, int solver, int recon,
+                         const double *u, Work *w, double *f[3]) {
+  long const nf = (long)g->ne * g->faces;
+  for (int d = 0; d < 3; ++d) memset(f[d], 0, sizeof(double) * nf);
+  block_primes(g, e, u, w->prim);
+  memset(w->eig, 0, sizeof(Eigen) * g->faces);
+  int const need_eigen = solver == ORACLE_FLUX_SPLITTING ||
+                         recon == ORACLE_RECON_CHARACTERISTIC;
+  for (int dir = 0; dir < g->dim; ++dir) {
+    if (need_eigen) eigen_direction(g, e, dir, u, w->prim, w->eig);
+    if (solver == ORACLE_FINITE_VOLUME) {
+      fv_fluxes(g, e, recon, dir, u, w->prim, w->eig, f[dir]);
+    } else {
+      advection(g, dir, u, w->prim, w->adv);
+      fs_fluxes(g, dir, u, w->adv, w->eig, f[dir]);
+    }
+  }
+}
+
+/* RHS zeroing and divergence of SpaceSolver::UpdateFluxes
+ * (space_solver.cpp:58-70, 131-153); volume forces are zero. */
+static void block_divergence(const Geom *g, double cell_size, double *f[3],
+                             double *rhs) {
+  memset(rhs, 0, sizeof(double) * g->ne * g->cells);
+  double const one_cell_size = 1.0 / cell_size;
+  for (int e = 0; e < g->ne; ++e) {
+    const double *fx = f[0] + e * g->faces;
+    const double *fy = f[1] + e * g->faces;
+    const double *fz = f[2] + e * g->faces;
+    for (int i = 0; i < g->ic[0]; ++i)
+      for (int j = 0; j < g->ic[1]; ++j)
+        for (int k = 0; k < g->ic[2]; ++k) {
+          double const dx = fx[fidx(g, i, j + 1, k + 1)] - fx[fidx(g, i + 1, j + 1, k + 1)];
+          double const dy = fy[fidx(g, i + 1, j, k + 1)] - fy[fidx(g, i + 1, j + 1, k + 1)];
+          double const dz = fz[fidx(g, i + 1, j + 1, k)] - fz[fidx(g, i + 1, j + 1, k + 1)];
+          long const c = cidx(g, i + fic(g, 0), j + fic(g, 1), k + fic(g, 2));
+          rhs[e * g->cells + c] += 0.0 + dacms(g->dim, dx, dy, dz) * one_cell_size;
+        }
+  }
+}
+
+/* ---- threading ---------------------------------------------------------- */
+
+typedef void (*task_fn)(void *ctx, int block, Work *w, double *f[3]);
+typedef struct {
+  task_fn fn;
+  void *ctx;
+  const Geom *g;
+  int nb, nthreads, tid;
+} ThreadArg;
+
+static void *thread_main(void *p) {
+  ThreadArg *a = (ThreadArg *)p;
+  Work w;
+  work_alloc(a->g, &w);
+  long const nf = (long)a->g->ne * a->g->faces;
+  double *fb = (double *)malloc(sizeof(double) * 3 * nf);
+  double *f[3] = {fb, fb + nf, fb + 2 * nf};
+  for (int b = a->tid; b < a->nb; b += a->nthreads) a->fn(a->ctx, b, &w, f);
+  free(fb);
+  work_free(&w);
+  return NULL;
+}
+
+static void parallel_blocks(const Geom *g, int nb, int nthreads, task_fn fn, void *ctx) {
+  if (nthreads < 1) nthreads = 1;
+  if (nthreads > nb) nthreads = nb > 0 ? nb : 1;
+  pthread_t th[256];
+  ThreadArg args[256];
+  if (nthreads > 256) nthreads = 256;
+  for (int t = 0; t < nthreads; ++t) {
+    args[t].fn = fn;
+    args[t].ctx = ctx;
+    args[t].g = g;
+    args[t].nb = nb;
+    args[t].nthreads = nthreads;
+    args[t].tid = t;
+  }
+  if (nthreads == 1) {
+    thread_main(&args[0]);
+    return;
+  }
+  for (int t = 0; t < nthreads; ++t) pthread_create(&th[t], NULL, thread_main, &args[t]);
+  for (int t = 0; t < nthreads; ++t) pthread_join(th[t], NULL);
+}
+
+/* ---- public entry points ------------------------------------------------ */
+
+int oracle_weno5(const double *v6, double *left, double *right) {
+  *left = weno5_left(v6);
+  *right = weno5_right(v6);
+  return 0;
+}
+
+int oracle_eos(int dim, double gamma, double B, int safe, const double *cons,
+               const double *prim, double *out) {
+  Eos e = {dim, gamma, B, safe};
+  out[0] = eos_pressure(&e, cons[0], cons[2], cons[3], cons[4], cons[1]);
+  out[1] = eos_enthalpy(&e, cons[0], cons[2], cons[3], cons[4], cons[1]);
+  out[2] = eos_energy(&e, prim[0], prim[2], prim[3], prim[4], prim[1]);
+  out[3] = eos_speed_of_sound(&e, prim[0], prim[1]);
+  out[4] = eos_psi(&e, prim[1], 1.0 / prim[0]);
+  out[5] = eos_gruneisen(&e);
+  return 0;
+}
+
+int oracle_prime_states(int dim, const double *u, int nb, double gamma, double B,
+                        int safe, double *p) {
+  if (dim < 1 || dim > 3) return 1;
+  Geom g = make_geom(dim);
+  Eos e = {dim, gamma, B, safe};
+  for (int b = 0; b < nb; ++b)
+    block_primes(&g, &e, u + (long)b * g.ne * g.cells, p + (long)b * g.np * g.cells);
+  return 0;
+}
+
+typedef struct {
+  const Geom *g;
+  const Eos *e;
+  int solver, recon;
+  const double *u;
+  double cell_size;
+  double *fx, *fy, *fz, *rhs;
+} RhsCtx;
+
+static void rhs_task(void *vctx, int b, Work *w, double *f[3]) {
+  RhsCtx *c = (RhsCtx *)vctx;
+  const Geom *g = c->g;
+  long const nf = (long)g->ne * g->faces;
+  block_fluxes(g, c->e, c->solver, c->recon, c->u + (long)b * g->ne * g->cells, w, f);
+  if (c->fx) memcpy(c->fx + b * nf, f[0], sizeof(double) * nf);
+  if (c->fy) memcpy(c->fy + b * nf, f[1], sizeof(double) * nf);
+  if (c->fz) memcpy(c->fz + b * nf, f[2], sizeof(double) * nf);
+  if (c->rhs) block_divergence(g, c->cell_size, f, c->rhs + (long)b * g->ne * g->cells);
+}
+
+int oracle_space_rhs(int dim, int solver, int recon, const double *u, int nb,
+                     double gamma, double B, int safe, double cell_size, double *fx,
+                     double *fy, double *fz, double *rhs, int nthreads) {
+  if (dim < 1 || dim > 3) return 1;
+  if (solver == ORACLE_FINITE_VOLUME && recon == ORACLE_RECON_CONSERVATIVE) return 2;
+  Geom g = make_geom(dim);
+  Eos e = {dim, gamma, B, safe};
+  RhsCtx c = {&g, &e, solver, recon, u, cell_size, fx, fy, fz, rhs};
+  parallel_blocks(&g, nb, nthreads, rhs_task, &c);
+  return 0;
+}
+
+/* ComputeTimestepSize (modular_algorithm_assembler.cpp:1840-1870, 1932,
+ * 1961-1982): max over interior cells of the consistency-managed sum of
+ * |u_d| + c, dt = CFL / (s / dx), clipped to the end time. The zero
+ * viscous / capillary / heat / gravity max() terms leave dt unchanged. */
+int oracle_timestep(int dim, const double *u, int nb, double gamma, double B,
+                    int safe, double cell_size, double cfl, double t, double t_end,
+                    double *dt_out) {
+  Geom g = make_geom(dim);
+  Eos e = {dim, gamma, B, safe};
+  double s = 0.0;
+  double c[MAXNE], p[MAXNE], vps[3];
+  for (int b = 0; b < nb; ++b) {
+    const double *ub = u + (long)b * g.ne * g.cells;
+    for (int i = fic(&g, 0); i <= lic(&g, 0); ++i)
+      for (int j = fic(&g, 1); j <= lic(&g, 1); ++j)
+        for (int k = fic(&g, 2); k <= lic(&g, 2); ++k) {
+          long const x = cidx(&g, i, j, k);
+          for (int f = 0; f < g.ne; ++f) c[f] = ub[f * g.cells + x];
+          cons_to_prim(&e, c, p);
+          double const cs = eos_speed_of_sound(&e, p[RHO], p[PRES]);
+          for (int d = 0; d < dim; ++d) vps[d] = fabs(p[VELX + d]) + cs;
+          s = dmax(s, cms_array(dim, vps));
+        }
+  }
+  double dt = s / cell_size;
+  double local;
+  if (dt == 0.0)
+    local = DBL_MAX;
+  else
+    local = cfl / dt;
+  if (t + local > t_end) local = dmax(t_end - t, 0.0);
+  *dt_out = local;
+  return 0;
+}
+
+/* Same-level halo copy. nbr26 holds 26 neighbour indices per block (-1: none),
+ * ordered by direction offsets (ox, oy, oz) in {-1,0,1}^3 \ {0} with ox slowest:
+ * index = (ox+1)*9 + (oy+1)*3 + (oz+1), minus one past the centre (13). The
+ * region for offset +1 is [HS+IC, TC) filled from the neighbour's [HS, 2HS),
+ * for -1 it is [0, HS) from the neighbour's [IC, IC+HS), for 0 the interior
+ * (communication_types.h:45-132; internal_halo_manager.cpp:439-459).
+ * faces_only copies only the 2*dim planes. */
+int oracle_halo_fill(int dim, double *u, int nb, int nfields, const int *nbr26,
+                     int faces_only) {
+  Geom g = make_geom(dim);
+  for (int b = 0; b < nb; ++b) {
+    for (int o = 0; o < 27; ++o) {
+      if (o == 13) continue;
+      int const oo[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+      int nz = 0, skip = 0;
+      for (int d = 0; d < 3; ++d) {
+        if (oo[d] != 0) ++nz;
+        if (d >= dim && oo[d] != 0) skip = 1;
+      }
+      if (skip || (faces_only && nz != 1)) continue;
+      int const slot = o < 13 ? o : o - 1;
+      int const n = nbr26[26 * b + slot];
+      if (n < 0) continue;
+      int lo[3], ext[3], src[3];
+      for (int d = 0; d < 3; ++d) {
+        if (d >= dim) {
+          lo[d] = 0; ext[d] = 1; src[d] = 0;
+        } else if (oo[d] == 0) {
+          lo[d] = HS; ext[d] = IC; src[d] = HS;
+        } else if (oo[d] > 0) {
+          lo[d] = HS + IC; ext[d] = HS; src[d] = HS;
+        } else {
+          lo[d] = 0; ext[d] = HS; src[d] = IC;
+        }
+      }
+      for (int f = 0; f < nfields; ++f) {
+        double *dst = u + ((long)b * nfields + f) * g.cells;
+        const double *s = u + ((long)n * nfields + f) * g.cells;
+        for (int i = 0; i < ext[0]; ++i)
+          for (int j = 0; j < ext[1]; ++j)
+            for (int k = 0; k < ext[2]; ++k)
+              dst[cidx(&g, lo[0] + i, lo[1] + j, lo[2] + k)] =
+                  s[cidx(&g, src[0] + i, src[1] + j, src[2] + k)];
+      }
+    }
+  }
+  return 0;
+}
+
+/* Face halos from the six-entry neighbour table (W,E,S,N,B,T) followed by the
+ * zero-gradient slabs of domain faces (boundary_constants.h:103-160, 211-252),
+ * external after internal as in halo_manager.cpp:87-124. */
+static void halo_update6(const Geom *g, double *u, int nb, const int *nbr) {
+  int const ne = g->ne;
+  for (int b = 0; b < nb; ++b)
+    for (int face = 0; face < 2 * g->dim; ++face) {
+      int const n = nbr[6 * b + face];
+      if (n < 0) continue;
+      int const dir = face / 2, high = face % 2;
+      int lo[3], ext[3], src[3];
+      for (int d = 0; d < 3; ++d) {
+        lo[d] = fic(g, d);
+        ext[d] = g->ic[d];
+        src[d] = fic(g, d);
+      }
+      ext[dir] = HS;
+      lo[dir] = high ? HS + IC : 0;
+      src[dir] = high ? HS : IC;
+      for (int f = 0; f < ne; ++f) {
+        double *dst = u + ((long)b * ne + f) * g->cells;
+        const double *s = u + ((long)n * ne + f) * g->cells;
+        for (int i = 0; i < ext[0]; ++i)
+          for (int j = 0; j < ext[1]; ++j)
+            for (int k = 0; k < ext[2]; ++k)
+              dst[cidx(g, lo[0] + i, lo[1] + j, lo[2] + k)] =
+                  s[cidx(g, src[0] + i, src[1] + j, src[2] + k)];
+      }
+    }
+  for (int b = 0; b < nb; ++b)
+    for (int face = 0; face < 2 * g->dim; ++face) {
+      if (nbr[6 * b + face] >= 0) continue;
+      int const dir = face / 2, high = face % 2;
+      int const s = high ? HS + IC - 1 : HS;
+      int const h0 = high ? HS + IC : 0, h1 = high ? TC : HS;
+      for (int f = 0; f < ne; ++f) {
+        double *x = u + ((long)b * ne + f) * g->cells;
+        for (int i = 0; i < g->tc[0]; ++i)
+          for (int j = 0; j < g->tc[1]; ++j)
+            for (int k = 0; k < g->tc[2]; ++k) {
+              int const idx[3] = {i, j, k};
+              if (idx[dir] < h0 || idx[dir] >= h1) continue;
+              int si = i, sj = j, sk = k;
+              if (dir == 0) si = s;
+              if (dir == 1) sj = s;
+              if (dir == 2) sk = s;
+              x[cidx(g, i, j, k)] = x[cidx(g, si, sj, sk)];
+            }
+      }
+    }
+}
+
+int oracle_halo_update(int dim, double *u, int nb, const int *nbr) {
+  if (dim < 1 || dim > 3) return 1;
+  Geom g = make_geom(dim);
+  halo_update6(&g, u, nb, nbr);
+  return 0;
+}
+
+/* SSP-RK3 (runge_kutta_3_TVD.h:41-59) */
+static const double rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
+static const double rk_a[3][2] = {{0.0, 0.0}, {0.25, 0.75}, {2.0 / 3.0, 1.0 / 3.0}};
+
+typedef struct {
+  const Geom *g;
+  const Eos *e;
+  int solver, recon, stage;
+  double *u, *u0, *rhs;
+  double cell_size, dt;
+} StageCtx;
+
+/* ComputeRightHandSide per block (modular_algorithm_assembler.cpp:990-1007):
+ * FillInitialBuffer (time_integrator.h:369-406), UpdateFluxes, then
+ * PrepareBufferForIntegration (time_integrator.h:434-457) over all cells, then
+ * IntegrateConservatives (time_integrator.h:98-113) on the interior. */
+static void stage_task(void *vctx, int b, Work *w, double *f[3]) {
+  StageCtx *c = (StageCtx *)vctx;
+  const Geom *g = c->g;
+  long const n = (long)g->ne * g->cells;
+  double *u = c->u + b * n, *u0 = c->u0 + b * n, *r = c->rhs + b * n;
+  if (c->stage == 0) memcpy(u0, u, sizeof(double) * n);
+  block_fluxes(g, c->e, c->solver, c->recon, u, w, f);
+  block_divergence(g, c->cell_size, f, r);
+  if (c->stage != 0) {
+    double const m0 = rk_a[c->stage][0], m1 = rk_a[c->stage][1];
+    for (long x = 0; x < n; ++x) u[x] = m0 * u[x] + m1 * u0[x];
+  }
+  double const step = rk_c[c->stage] * (0.0 + c->dt);
+  for (int e = 0; e < g->ne; ++e)
+    for (int i = fic(g, 0); i <= lic(g, 0); ++i)
+      for (int j = fic(g, 1); j <= lic(g, 1); ++j)
+        for (int k = fic(g, 2); k <= lic(g, 2); ++k) {
+          long const x = e * g->cells + cidx(g, i, j, k);
+          r[x] = u[x] + step * r[x];
+        }
+}
+
+/* Single-level, single-phase Advance (modular_algorithm_assembler.cpp:575-874):
+ * dt, then three stages of RHS / prepare / integrate, halo update of the
+ * integrated buffer (:726) and the buffer swap (:830). */
+int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr,
+               double gamma, double B, int safe, double cell_size, double cfl,
+               double t_end, int max_steps, int nthreads, double *t_io,
+               int *steps_done, double *dt_log) {
+  if (dim < 1 || dim > 3) return 1;
+  Geom g = make_geom(dim);
+  Eos e = {dim, gamma, B, safe};
+  long const n = (long)nb * g.ne * g.cells;
+  double *u0 = (double *)malloc(sizeof(double) * n);
+  double *rhs = (double *)malloc(sizeof(double) * n);
+  if (!u0 || !rhs) {
+    free(u0);
+    free(rhs);
+    return 3;
+  }
+  memcpy(u0, u, sizeof(double) * n);
+  memcpy(rhs, u, sizeof(double) * n);
+  halo_update6(&g, u, nb, nbr);
+  double *cur = u, *other = rhs;
+  double t = *t_io;
+  int steps = 0;
+  while (t < t_end && (max_steps <= 0 || steps < max_steps)) {
+    double dt;
+    oracle_timestep(dim, cur, nb, gamma, B, safe, cell_size, cfl, t, t_end, &dt);
+    if (dt_log) dt_log[steps] = dt;
+    for (int stage = 0; stage < 3; ++stage) {
+      StageCtx c = {&g, &e, solver, recon, stage, cur, u0, other, cell_size, dt};
+      parallel_blocks(&g, nb, nthreads, stage_task, &c);
+      halo_update6(&g, other, nb, nbr);
+      double *tmp = cur;
+      cur = other;
+      other = tmp;
+    }
+    t = t + (0.0 + dt);
+    ++steps;
+  }
+  if (cur != u) memcpy(u, cur, sizeof(double) * n);
+  free(u0);
+  free(rhs);
+  *t_io = t;
+  *steps_done = steps;
+  return 0;
+}

@@ -1,0 +1,167 @@
+"""Python face of the C ABI: stateless drop-in calls on device tensors and the
+device-resident Engine. torch is used only to hold device memory and streams.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import native as N
+from .cases import Case, block_shape
+
+VARIANTS = ("fvchar", "fvprim", "fsroe")
+
+
+def _ptr(t) -> C.c_void_p:
+    return C.c_void_p(t.data_ptr()) if t is not None else C.c_void_p(0)
+
+
+def _stream(stream=None) -> C.c_void_p:
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def flux_shape(dim: int, nb: int):
+    ne = dim + 2
+    return (nb, ne, 17, 17 if dim > 1 else 2, 17 if dim > 2 else 2)
+
+
+def convective_fluxes(u, dim: int, variant: str, material: N.Material, cell_size: float,
+                      precision: int = N.FP64, stream=None):
+    """ConvectiveTermSolver::UpdateConvectiveFluxes on nb blocks (device tensor
+    [nb, ne, TCX, TCY, TCZ] float64). Returns zero-initialised flux arrays with
+    the fluxes added, in the reference layout."""
+    import torch
+    nb = u.shape[0]
+    shp = flux_shape(dim, nb)
+    f = [torch.zeros(shp, dtype=torch.float64, device=u.device) if d < dim else None
+         for d in range(3)]
+    sch = N.Scheme.make(variant, precision)
+    N.check(N.lib().alp_convective_fluxes(dim, C.byref(sch), C.byref(material), _ptr(u), nb,
+                                          cell_size, _ptr(f[0]), _ptr(f[1]), _ptr(f[2]),
+                                          _stream(stream)))
+    return f
+
+
+def space_rhs(u, dim: int, variant: str, material: N.Material, cell_size: float,
+              precision: int = N.FP64, stream=None, workspace=None):
+    """SpaceSolver::UpdateFluxes right-hand side (reference layout)."""
+    import torch
+    nb = u.shape[0]
+    rhs = torch.empty_like(u)
+    nbytes = N.lib().alp_space_rhs_workspace_size(dim, nb)
+    if workspace is None:
+        workspace = torch.empty(max(nbytes // 8, 1), dtype=torch.float64, device=u.device)
+    sch = N.Scheme.make(variant, precision)
+    N.check(N.lib().alp_space_rhs(dim, C.byref(sch), C.byref(material), _ptr(u), nb, cell_size,
+                                  _ptr(rhs), _ptr(workspace), workspace.numel() * 8,
+                                  _stream(stream)))
+    return rhs
+
+
+def prime_states(u, dim: int, material: N.Material, stream=None):
+    import torch
+    p = torch.empty_like(u)
+    N.check(N.lib().alp_prime_states(dim, C.byref(material), _ptr(u), u.shape[0], _ptr(p),
+                                     _stream(stream)))
+    return p
+
+
+def halo_update(u, dim: int, nbr26, mode: int = N.HALO_ALL, stream=None):
+    """In-place halo update; nbr26 is an int32 device tensor [nb, 26]."""
+    N.check(N.lib().alp_halo_update(dim, _ptr(u), u.shape[0], u.shape[1], _ptr(nbr26), mode,
+                                    _stream(stream)))
+    return u
+
+
+def timestep_size(u, dim: int, material: N.Material, cell_size: float, cfl: float,
+                  t: float = 0.0, t_end: float = 1e300, stream=None) -> float:
+    import torch
+    ws = torch.empty(1, dtype=torch.float64, device=u.device)
+    dt = C.c_double()
+    N.check(N.lib().alp_timestep_size(dim, C.byref(material), _ptr(u), u.shape[0], cell_size, cfl,
+                                      t, t_end, C.byref(dt), _ptr(ws), _stream(stream)))
+    return dt.value
+
+
+def rk3_stage(u, u0, rhs, dim: int, stage: int, dt: float, stream=None):
+    N.check(N.lib().alp_rk3_stage(dim, _ptr(u), _ptr(u0), _ptr(rhs), u.shape[0], stage, dt,
+                                  _stream(stream)))
+    return u
+
+
+class Engine:
+    """Device-resident cases advanced by the fused step (alp_engine_*)."""
+
+    def __init__(self, dim: int, variant: str = "fvchar", precision: int = N.FP64,
+                 capacity_blocks: int = 1024, max_cases: int = 64, graph: bool = True):
+        self.dim = dim
+        self.ne = dim + 2
+        self.variant = variant
+        sch = N.Scheme.make(variant, precision)
+        h = C.c_void_p()
+        N.check(N.lib().alp_engine_create(dim, C.byref(sch), capacity_blocks, max_cases,
+                                          C.byref(h)))
+        self.h = h
+        self.nb = {}
+        if not graph:
+            N.check(N.lib().alp_engine_set_graph(self.h, 0))
+
+    def close(self):
+        if self.h:
+            N.lib().alp_engine_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_case(self, case: Case, t0: float = 0.0, max_steps: int | None = None) -> int:
+        g = case.grid
+        u = np.ascontiguousarray(case.u, dtype=np.float64)
+        nbr = np.ascontiguousarray(g.nbr26, dtype=np.int32)
+        mat = N.Material.make(case.gamma, case.B, False)
+        cid = C.c_int()
+        steps = case.steps if max_steps is None else max_steps
+        N.check(N.lib().alp_engine_add_case(
+            self.h, C.byref(mat), g.cell_size, case.cfl, t0, case.t_end, steps, g.nb,
+            nbr.ctypes.data_as(C.POINTER(C.c_int)), u.ctypes.data_as(C.POINTER(C.c_double)),
+            C.byref(cid)))
+        self.nb[cid.value] = (g.nb, u.shape)
+        return cid.value
+
+    def remove_case(self, cid: int):
+        N.check(N.lib().alp_engine_remove_case(self.h, cid))
+        self.nb.pop(cid, None)
+
+    def step(self, n: int = 1):
+        N.check(N.lib().alp_engine_step(self.h, n))
+
+    def get(self, cid: int):
+        nb, shp = self.nb[cid]
+        out = np.empty(shp, dtype=np.float64)
+        t = C.c_double()
+        steps = C.c_int()
+        N.check(N.lib().alp_engine_get_case(self.h, cid, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                            C.byref(t), C.byref(steps)))
+        return out, t.value, steps.value
+
+    def all_done(self) -> bool:
+        d = C.c_int()
+        N.check(N.lib().alp_engine_all_done(self.h, C.byref(d)))
+        return bool(d.value)
+
+    def run_to_end(self, chunk: int = 16, max_chunks: int = 1 << 20):
+        for _ in range(max_chunks):
+            if self.all_done():
+                return
+            self.step(chunk)
+        raise RuntimeError("engine did not finish")
+
+    @property
+    def launches_per_step(self) -> int:
+        return N.lib().alp_engine_launches_per_step(self.h)

@@ -1,0 +1,541 @@
+// C ABI (include/alpaca_b200.h): stateless drop-in calls and the engine that
+// keeps cases device-resident and replays its step as a CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/alpaca_b200.h"
+#include "kernels.cuh"
+
+using namespace alp;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, std::string const &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+int cuda_fail(cudaError_t e, char const *where) {
+  return fail(ALP_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
+}
+
+#define ALP_CUDA(call)                                   \
+  do {                                                   \
+    cudaError_t const e_ = (call);                       \
+    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
+  } while (0)
+
+int faces_of(int dim) {
+  return 17 * (dim > 1 ? 17 : 2) * (dim > 2 ? 17 : 2);
+}
+int cells_of(int dim) { return 24 * (dim > 1 ? 24 : 1) * (dim > 2 ? 24 : 1); }
+
+int scheme_id(alp_scheme const *s, int *id, int *precision) {
+  if (!s) return fail(ALP_ERR_INVALID, "scheme is null");
+  if (s->reconstruction_stencil != ALP_STENCIL_WENO5)
+    return fail(ALP_ERR_INVALID, "only ReconstructionStencils::WENO5 is compiled");
+  if (s->time_integrator != ALP_RK3)
+    return fail(ALP_ERR_INVALID, "only TimeIntegrators::RK3 is compiled");
+  if (s->precision != ALP_FP64 && s->precision != ALP_FP32_FLUX)
+    return fail(ALP_ERR_INVALID, "precision must be ALP_FP64 or ALP_FP32_FLUX");
+  *precision = s->precision;
+  if (s->convective_term_solver == ALP_FINITE_VOLUME) {
+    if (s->riemann_solver != ALP_RIEMANN_HLLC || s->signal_speed != ALP_SIGNAL_SPEED_EINFELDT)
+      return fail(ALP_ERR_INVALID, "FiniteVolume is compiled with Hllc + Einfeldt only");
+    if (s->state_reconstruction == ALP_RECON_CHARACTERISTIC) {
+      *id = FV_CHAR;
+      return ALP_OK;
+    }
+    if (s->state_reconstruction == ALP_RECON_PRIMITIVE) {
+      *id = FV_PRIM;
+      return ALP_OK;
+    }
+    return fail(ALP_ERR_INVALID, "FiniteVolume needs Primitive or Characteristic reconstruction");
+  }
+  if (s->convective_term_solver == ALP_FLUX_SPLITTING) {
+    if (s->flux_splitting != ALP_FLUX_SPLITTING_ROE)
+      return fail(ALP_ERR_INVALID, "FluxSplitting is compiled with FluxSplitting::Roe only");
+    *id = FS_ROE;
+    return ALP_OK;
+  }
+  return fail(ALP_ERR_INVALID, "unknown convective_term_solver");
+}
+
+int check_material(alp_material const *m) {
+  if (!m) return fail(ALP_ERR_INVALID, "material is null");
+  if (!(m->gamma > 1.0)) return fail(ALP_ERR_INVALID, "gamma must exceed 1");
+  if (!(m->background_pressure >= 0.0)) return fail(ALP_ERR_INVALID, "background pressure < 0");
+  return ALP_OK;
+}
+
+BlockMeta meta_of(alp_material const *m, double cell_size, int case_id) {
+  BlockMeta b;
+  b.cell_size = cell_size;
+  b.gamma = m->gamma;
+  b.B = m->background_pressure;
+  b.safe = m->safe ? 1 : 0;
+  b.case_id = case_id;
+  return b;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *alp_version(void) { return "alpaca_b200 0.1 (sm_100a)"; }
+const char *alp_last_error(void) { return g_last_error.c_str(); }
+
+void alp_scheme_default(alp_scheme *s) {
+  s->convective_term_solver = ALP_FINITE_VOLUME;
+  s->state_reconstruction = ALP_RECON_CHARACTERISTIC;
+  s->reconstruction_stencil = ALP_STENCIL_WENO5;
+  s->riemann_solver = ALP_RIEMANN_HLLC;
+  s->signal_speed = ALP_SIGNAL_SPEED_EINFELDT;
+  s->flux_splitting = ALP_FLUX_SPLITTING_ROE;
+  s->time_integrator = ALP_RK3;
+  s->precision = ALP_FP64;
+}
+
+int alp_convective_fluxes(int dim, const alp_scheme *scheme, const alp_material *mat,
+                          const double *d_blocks, int nb, double cell_size, double *d_fx,
+                          double *d_fy, double *d_fz, alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  int sid, prec;
+  if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  if (int rc = check_material(mat)) return rc;
+  if (nb < 0 || (nb > 0 && !d_blocks)) return fail(ALP_ERR_INVALID, "bad block buffer");
+  double *F[3] = {d_fx, d_fy, d_fz};
+  for (int d = 0; d < dim; ++d)
+    if (!F[d] && nb > 0) return fail(ALP_ERR_INVALID, "flux buffer is null");
+  Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
+           meta_of(mat, cell_size, 0), (cudaStream_t)stream};
+  long long const stride = (long long)(dim + 2) * faces_of(dim);
+  for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F[d], stride, true));
+  return ALP_OK;
+}
+
+size_t alp_space_rhs_workspace_size(int dim, int nb) {
+  if (dim < 1 || dim > 3 || nb < 0) return 0;
+  return (size_t)nb * dim * (dim + 2) * faces_of(dim) * sizeof(double);
+}
+
+int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
+                  const double *d_blocks, int nb, double cell_size, double *d_rhs,
+                  void *d_workspace, size_t workspace_bytes, alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  int sid, prec;
+  if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  if (int rc = check_material(mat)) return rc;
+  if (nb <= 0) return ALP_OK;
+  if (!d_blocks || !d_rhs) return fail(ALP_ERR_INVALID, "null buffer");
+  if (!d_workspace || workspace_bytes < alp_space_rhs_workspace_size(dim, nb))
+    return fail(ALP_ERR_INVALID, "workspace too small");
+  double *F = static_cast<double *>(d_workspace);
+  Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
+           meta_of(mat, cell_size, 0), (cudaStream_t)stream};
+  long long const dstride = (long long)(dim + 2) * faces_of(dim);
+  long long const stride = dstride * dim;
+  for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F + d * dstride, stride, false));
+  ALP_CUDA(launch_divergence(L, F, stride, dstride, d_rhs));
+  return ALP_OK;
+}
+
+int alp_prime_states(int dim, const alp_material *mat, const double *d_blocks, int nb,
+                     double *d_primes, alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  if (int rc = check_material(mat)) return rc;
+  if (nb <= 0) return ALP_OK;
+  if (!d_blocks || !d_primes) return fail(ALP_ERR_INVALID, "null buffer");
+  Launch L{dim, 0, 0, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
+           meta_of(mat, 1.0, 0), (cudaStream_t)stream};
+  ALP_CUDA(launch_prime_states(L, d_primes));
+  return ALP_OK;
+}
+
+int alp_halo_update(int dim, double *d_blocks, int nb, int nfields, const int *d_nbr26, int mode,
+                    alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  if (mode != ALP_HALO_ALL && mode != ALP_HALO_FACES) return fail(ALP_ERR_INVALID, "bad mode");
+  if (nfields < 1) return fail(ALP_ERR_INVALID, "nfields < 1");
+  if (nb <= 0) return ALP_OK;
+  if (!d_blocks || !d_nbr26) return fail(ALP_ERR_INVALID, "null buffer");
+  BlockMeta def{};
+  Launch L{dim, 0, 0, d_blocks, nullptr, nb, nullptr, def, (cudaStream_t)stream};
+  ALP_CUDA(launch_halo(L, d_nbr26, mode == ALP_HALO_FACES, nfields, nullptr));
+  return ALP_OK;
+}
+
+int alp_timestep_size(int dim, const alp_material *mat, const double *d_blocks, int nb,
+                      double cell_size, double cfl, double t, double t_end, double *h_dt,
+                      void *d_workspace, alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  if (int rc = check_material(mat)) return rc;
+  if (!h_dt) return fail(ALP_ERR_INVALID, "h_dt is null");
+  unsigned long long bits = 0ull;
+  if (nb > 0) {
+    if (!d_workspace) return fail(ALP_ERR_INVALID, "workspace is null");
+    auto *d_bits = static_cast<unsigned long long *>(d_workspace);
+    ALP_CUDA(cudaMemsetAsync(d_bits, 0, sizeof(unsigned long long), (cudaStream_t)stream));
+    Launch L{dim, 0, 0, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
+             meta_of(mat, cell_size, 0), (cudaStream_t)stream};
+    ALP_CUDA(launch_signal_speed(L, nullptr, d_bits));
+    ALP_CUDA(cudaMemcpyAsync(&bits, d_bits, sizeof(bits), cudaMemcpyDeviceToHost,
+                             (cudaStream_t)stream));
+    ALP_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  }
+  double smax;
+  std::memcpy(&smax, &bits, sizeof(smax));
+  // modular_algorithm_assembler.cpp:1932, 1961-1982
+  double const dt = smax / cell_size;
+  double local = dt == 0.0 ? 1.7976931348623157e308 : cfl / dt;
+  if (t + local > t_end) local = std::max(t_end - t, 0.0);
+  *h_dt = local;
+  return ALP_OK;
+}
+
+int alp_rk3_stage(int dim, double *d_blocks, double *d_initial, const double *d_rhs, int nb,
+                  int stage, double dt, alp_stream_t stream) {
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  if (stage < 0 || stage > 2) return fail(ALP_ERR_INVALID, "stage must be 0, 1 or 2");
+  if (nb <= 0) return ALP_OK;
+  if (!d_blocks || !d_initial || !d_rhs) return fail(ALP_ERR_INVALID, "null buffer");
+  ALP_CUDA(launch_rk_stage_rhs(dim, d_blocks, d_initial, d_rhs, nb, stage, dt,
+                               (cudaStream_t)stream));
+  return ALP_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// engine
+// ---------------------------------------------------------------------------
+
+struct alp_engine {
+  int dim = 3, scheme = FV_CHAR, precision = FP64;
+  int capacity = 0, max_cases = 0;
+  int ne = 5, cells = 0, faces = 0;
+  double *U = nullptr, *U0 = nullptr, *F = nullptr;
+  BlockMeta *meta = nullptr;
+  int *nbr26 = nullptr;
+  int *work = nullptr;
+  CaseState *cases = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool use_graph = true;
+  bool graph_dirty = true;
+
+  // host mirrors
+  std::vector<BlockMeta> h_meta;
+  std::vector<int> h_nbr26;
+  std::map<int, int> free_ranges;  // start -> length
+  struct CaseRec {
+    bool live = false;
+    int first = 0, nb = 0;
+  };
+  std::vector<CaseRec> case_rec;
+  std::vector<int> h_work;
+  int nwork = 0;
+
+  long long dstride() const { return (long long)ne * faces; }
+  long long stride() const { return dstride() * dim; }
+
+  int record_step() {
+    Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
+    ALP_CUDA(launch_signal_speed(L, cases, nullptr));
+    ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
+    for (int s = 0; s < 3; ++s) {
+      for (int d = 0; d < dim; ++d)
+        ALP_CUDA(launch_face_flux(L, d, F + d * dstride(), stride(), false));
+      ALP_CUDA(launch_stage_update(L, U0, F, stride(), dstride(), s, cases, 0.0));
+      ALP_CUDA(launch_halo(L, nbr26, true, ne, cases));
+    }
+    ALP_CUDA(launch_step_commit(cases, max_cases, stream));
+    return ALP_OK;
+  }
+
+  int rebuild_work() {
+    h_work.clear();
+    for (auto const &c : case_rec)
+      if (c.live)
+        for (int b = 0; b < c.nb; ++b) h_work.push_back(c.first + b);
+    nwork = (int)h_work.size();
+    if (nwork)
+      ALP_CUDA(cudaMemcpyAsync(work, h_work.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice,
+                               stream));
+    graph_dirty = true;
+    return ALP_OK;
+  }
+
+  int alloc_range(int n, int *first) {
+    for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
+      if (it->second >= n) {
+        *first = it->first;
+        int const rest = it->second - n, start = it->first + n;
+        free_ranges.erase(it);
+        if (rest > 0) free_ranges[start] = rest;
+        return ALP_OK;
+      }
+    }
+    return fail(ALP_ERR_CAPACITY, "no contiguous free block range of the requested size");
+  }
+
+  void free_range(int first, int n) {
+    auto it = free_ranges.emplace(first, n).first;
+    auto nx = std::next(it);
+    if (nx != free_ranges.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_ranges.erase(nx);
+    }
+    if (it != free_ranges.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_ranges.erase(it);
+      }
+    }
+  }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    cudaFree(U);
+    cudaFree(U0);
+    cudaFree(F);
+    cudaFree(meta);
+    cudaFree(nbr26);
+    cudaFree(work);
+    cudaFree(cases);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+extern "C" {
+
+size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
+  if (dim < 1 || dim > 3) return 0;
+  size_t const ne = dim + 2;
+  size_t const blk = ne * cells_of(dim) * sizeof(double);
+  size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double);
+  return (size_t)capacity_blocks *
+             (2 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
+         (size_t)max_cases * sizeof(CaseState);
+}
+
+int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
+                      alp_engine **out) {
+  if (!out) return fail(ALP_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  if (capacity_blocks <= 0 || max_cases <= 0) return fail(ALP_ERR_INVALID, "empty engine");
+  int sid, prec;
+  if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  alp_engine *e = new (std::nothrow) alp_engine;
+  if (!e) return fail(ALP_ERR_CAPACITY, "host allocation failed");
+  e->dim = dim;
+  e->scheme = sid;
+  e->precision = prec;
+  e->capacity = capacity_blocks;
+  e->max_cases = max_cases;
+  e->ne = dim + 2;
+  e->cells = cells_of(dim);
+  e->faces = faces_of(dim);
+  size_t const blk = (size_t)e->ne * e->cells;
+  cudaError_t err = cudaSuccess;
+  auto grab = [&](void **p, size_t bytes) {
+    if (err == cudaSuccess) err = cudaMalloc(p, bytes);
+  };
+  grab((void **)&e->U, blk * capacity_blocks * sizeof(double));
+  grab((void **)&e->U0, blk * capacity_blocks * sizeof(double));
+  grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
+  grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
+  grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
+  grab((void **)&e->work, sizeof(int) * capacity_blocks);
+  grab((void **)&e->cases, sizeof(CaseState) * max_cases);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (err == cudaSuccess)
+    err = cudaMemsetAsync(e->cases, 0, sizeof(CaseState) * max_cases, e->stream);
+  if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
+  if (err != cudaSuccess) {
+    e->release();
+    delete e;
+    return cuda_fail(err, "alp_engine_create");
+  }
+  e->h_meta.assign(capacity_blocks, BlockMeta{});
+  e->h_nbr26.assign((size_t)capacity_blocks * 26, -1);
+  e->free_ranges[0] = capacity_blocks;
+  e->case_rec.assign(max_cases, {});
+  *out = e;
+  return ALP_OK;
+}
+
+int alp_engine_destroy(alp_engine *e) {
+  if (!e) return ALP_OK;
+  cudaStreamSynchronize(e->stream);
+  e->release();
+  delete e;
+  return ALP_OK;
+}
+
+int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size, double cfl,
+                        double t0, double t_end, int max_steps, int nb, const int *h_nbr26,
+                        const double *h_blocks, int *case_id) {
+  if (!e || !case_id) return fail(ALP_ERR_INVALID, "null argument");
+  if (int rc = check_material(mat)) return rc;
+  if (nb <= 0 || !h_nbr26 || !h_blocks) return fail(ALP_ERR_INVALID, "bad case blocks");
+  if (!(cell_size > 0.0) || !(cfl > 0.0)) return fail(ALP_ERR_INVALID, "bad cell size / cfl");
+  for (size_t i = 0; i < (size_t)nb * 26; ++i)
+    if (h_nbr26[i] < -1 || h_nbr26[i] >= nb) return fail(ALP_ERR_INVALID, "neighbour out of range");
+  int cid = -1;
+  for (int c = 0; c < e->max_cases; ++c)
+    if (!e->case_rec[c].live) {
+      cid = c;
+      break;
+    }
+  if (cid < 0) return fail(ALP_ERR_CAPACITY, "case table full");
+  int first;
+  if (int rc = e->alloc_range(nb, &first)) return rc;
+  e->case_rec[cid] = {true, first, nb};
+  for (int b = 0; b < nb; ++b) {
+    e->h_meta[first + b] = meta_of(mat, cell_size, cid);
+    for (int s = 0; s < 26; ++s) {
+      int const n = h_nbr26[(size_t)b * 26 + s];
+      e->h_nbr26[(size_t)(first + b) * 26 + s] = n < 0 ? -1 : first + n;
+    }
+  }
+  size_t const blk = (size_t)e->ne * e->cells;
+  ALP_CUDA(cudaMemcpyAsync(e->U + blk * first, h_blocks, blk * nb * sizeof(double),
+                           cudaMemcpyHostToDevice, e->stream));
+  ALP_CUDA(cudaMemcpyAsync(e->meta + first, e->h_meta.data() + first, sizeof(BlockMeta) * nb,
+                           cudaMemcpyHostToDevice, e->stream));
+  ALP_CUDA(cudaMemcpyAsync(e->nbr26 + (size_t)first * 26, e->h_nbr26.data() + (size_t)first * 26,
+                           sizeof(int) * 26 * nb, cudaMemcpyHostToDevice, e->stream));
+  CaseState cs{};
+  cs.t = t0;
+  cs.t_end = t_end;
+  cs.cfl = cfl;
+  cs.dt = 0.0;
+  cs.h_min = cell_size;
+  cs.smax_bits = 0ull;
+  cs.steps = 0;
+  cs.max_steps = max_steps;
+  cs.status = 0;
+  ALP_CUDA(cudaMemcpyAsync(e->cases + cid, &cs, sizeof(cs), cudaMemcpyHostToDevice, e->stream));
+  // fill the halos of the new blocks from their interiors
+  BlockMeta def{};
+  Launch L{e->dim, e->scheme, e->precision, e->U, nullptr, nb, nullptr, def, e->stream};
+  if (int rc = e->rebuild_work()) return rc;
+  // the case's blocks are contiguous in h_work order; find its offset
+  int off = 0;
+  for (int c = 0; c < cid; ++c)
+    if (e->case_rec[c].live) off += e->case_rec[c].nb;
+  L.work = e->work + off;
+  ALP_CUDA(launch_halo(L, e->nbr26, true, e->ne, nullptr));
+  // cudaMemcpyAsync from pageable memory returns once the source is consumed
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  *case_id = cid;
+  return ALP_OK;
+}
+
+int alp_engine_remove_case(alp_engine *e, int case_id) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (case_id < 0 || case_id >= e->max_cases || !e->case_rec[case_id].live)
+    return fail(ALP_ERR_NOT_FOUND, "unknown case");
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  auto &c = e->case_rec[case_id];
+  e->free_range(c.first, c.nb);
+  c = {};
+  CaseState cs{};
+  ALP_CUDA(cudaMemcpyAsync(e->cases + case_id, &cs, sizeof(cs), cudaMemcpyHostToDevice, e->stream));
+  return e->rebuild_work();
+}
+
+int alp_engine_step(alp_engine *e, int n) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (n <= 0 || e->nwork == 0) return ALP_OK;
+  if (!e->use_graph) {
+    for (int i = 0; i < n; ++i)
+      if (int rc = e->record_step()) return rc;
+    return ALP_OK;
+  }
+  if (e->graph_dirty || !e->graph) {
+    if (e->graph) {
+      cudaGraphExecDestroy(e->graph);
+      e->graph = nullptr;
+    }
+    cudaGraph_t g;
+    ALP_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
+    int const rc = e->record_step();
+    cudaError_t const ce = cudaStreamEndCapture(e->stream, &g);
+    if (rc) {
+      if (ce == cudaSuccess) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (ce != cudaSuccess) return cuda_fail(ce, "cudaStreamEndCapture");
+    cudaError_t const ie = cudaGraphInstantiate(&e->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return cuda_fail(ie, "cudaGraphInstantiate");
+    e->graph_dirty = false;
+  }
+  for (int i = 0; i < n; ++i) ALP_CUDA(cudaGraphLaunch(e->graph, e->stream));
+  return ALP_OK;
+}
+
+int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t, int *steps) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (case_id < 0 || case_id >= e->max_cases || !e->case_rec[case_id].live)
+    return fail(ALP_ERR_NOT_FOUND, "unknown case");
+  auto const &c = e->case_rec[case_id];
+  size_t const blk = (size_t)e->ne * e->cells;
+  CaseState cs;
+  if (h_blocks)
+    ALP_CUDA(cudaMemcpyAsync(h_blocks, e->U + blk * c.first, blk * c.nb * sizeof(double),
+                             cudaMemcpyDeviceToHost, e->stream));
+  ALP_CUDA(cudaMemcpyAsync(&cs, e->cases + case_id, sizeof(cs), cudaMemcpyDeviceToHost, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  if (t) *t = cs.t;
+  if (steps) *steps = cs.steps;
+  if (cs.status) return fail(ALP_ERR_NUMERIC, "non-finite or non-positive state; case stopped");
+  return ALP_OK;
+}
+
+int alp_engine_all_done(alp_engine *e, int *done) {
+  if (!e || !done) return fail(ALP_ERR_INVALID, "null argument");
+  std::vector<CaseState> cs(e->max_cases);
+  ALP_CUDA(cudaMemcpyAsync(cs.data(), e->cases, sizeof(CaseState) * e->max_cases,
+                           cudaMemcpyDeviceToHost, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  int d = 1;
+  for (int c = 0; c < e->max_cases; ++c) {
+    if (!e->case_rec[c].live) continue;
+    bool const finished = !(cs[c].t < cs[c].t_end) ||
+                          (cs[c].max_steps > 0 && cs[c].steps >= cs[c].max_steps) ||
+                          cs[c].status != 0;
+    if (!finished) d = 0;
+  }
+  *done = d;
+  return ALP_OK;
+}
+
+alp_stream_t alp_engine_stream(alp_engine *e) { return e ? (alp_stream_t)e->stream : nullptr; }
+
+int alp_engine_set_graph(alp_engine *e, int enabled) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  e->use_graph = enabled != 0;
+  return ALP_OK;
+}
+
+int alp_engine_launches_per_step(alp_engine *e) {
+  if (!e) return 0;
+  // signal speed, dt, 3 x (dim face fluxes, stage update, halo copy + zero gradient), commit
+  return 2 + 3 * (e->dim + 1 + 2) + 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,758 @@
+// Block kernels of the ALPACA right-hand side and SSP-RK3 stage update on sm_100a.
+//
+// Data stays in the reference's block layout (layout.cuh). One launch per sweep
+// direction computes the face fluxes of all work items (thread per face, the
+// 6-cell stencil read through L1), one launch applies the flux divergence and
+// the RK3 stage, one launch refreshes the face halos from neighbour interiors.
+#include <cfloat>
+#include <cstdio>
+
+#include "kernels.cuh"
+#include "numerics.cuh"
+
+namespace alp {
+
+namespace {
+
+__device__ __forceinline__ int slot_of(int const *work, int item) {
+  return work ? work[item] : item;
+}
+
+// Structural nonzeros of the left eigenvector matrix row n, column l
+// (eigendecomposition.h:316-359).
+template <int DIM, int DIR>
+__host__ __device__ constexpr bool left_nonzero(int n, int l) {
+  // the rows of the two acoustic waves and of the principal-momentum wave are full
+  if (n == 0 || n == DIM + 1 || n == DIM) return true;
+  // minor-momentum waves: mass and their own momentum only
+  return l == MASS || l == MOMX + (n == 1 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+}
+
+// ---------------------------------------------------------------------------
+// face flux
+// ---------------------------------------------------------------------------
+
+template <int DIM, int DIR> struct FaceMap {
+  static constexpr int O1 = DIR == 0 ? 1 : 0;
+  static constexpr int O2 = DIR == 2 ? 1 : 2;
+  static constexpr int E1 = Geo<DIM>::ic(O1);
+  static constexpr int E2 = Geo<DIM>::ic(O2);
+  static constexpr int COUNT = (IC + 1) * E1 * E2;
+  // Thread t -> face (a along DIR, p1, p2 across). Consecutive threads walk the
+  // fastest-varying stored dimension so that stencil loads coalesce.
+  __device__ static void decode(int t, int &a, int &p1, int &p2) {
+    if constexpr (DIR == DIM - 1) {
+      a = t % (IC + 1);
+      int const r = t / (IC + 1);
+      p1 = r / E2;
+      p2 = r % E2;
+    } else {
+      a = t / (E1 * E2);
+      p1 = (t / E2) % E1;
+      p2 = t % E2;
+    }
+  }
+};
+
+template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM>
+__global__ void __launch_bounds__(128)
+face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                 BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
+                 long long stride) {
+  using G = Geo<DIM>;
+  using M = FaceMap<DIM, DIR>;
+  constexpr int NE = G::NE;
+  int const item = blockIdx.x;
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= M::COUNT) return;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+
+  int a, p1, p2;
+  M::decode(t, a, p1, p2);
+  int c0[3];
+  c0[DIR] = HS + a - 3;
+  c0[M::O1] = G::fic(M::O1) + p1;
+  c0[M::O2] = G::fic(M::O2) + p2;
+  constexpr int step = DIR == 0 ? G::TCY * G::TCZ : (DIR == 1 ? G::TCZ : 1);
+  double const *ub = U + (size_t)slot * G::BLOCK_DOUBLES + G::cell(c0[0], c0[1], c0[2]);
+
+  double cons[6][NE];
+#pragma unroll
+  for (int m = 0; m < 6; ++m)
+#pragma unroll
+    for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(ub + f * G::CELLS + m * step);
+
+  T flux[NE];
+  bool valid = true;
+  constexpr int mP = MOMX + DIR;
+
+  if constexpr (SCHEME == FV_CHAR || SCHEME == FS_ROE) {
+    auto const pt = cell_prims<DIM, DIR>(eos, cons[2]);
+    auto const pn = cell_prims<DIM, DIR>(eos, cons[3]);
+    if (!(pt.rho > 0.0) || !(pn.rho > 0.0)) valid = false;
+    Roe<T> const r = roe_average<DIM, DIR, T>(eos, pt, pn);
+    T ch[2][NE];
+    if constexpr (SCHEME == FV_CHAR) {
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        T L[NE];
+        left_row<DIM, DIR, T>(n, r, L);
+        T uc[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          T s = T(0);
+          bool first = true;
+#pragma unroll
+          for (int q = 0; q < NE; ++q) {
+            int const l = sum_seq<DIM, DIR>(q);
+            if (!left_nonzero<DIM, DIR>(n, l)) continue;
+            T const prod = L[l] * T(cons[m][l]);
+            s = first ? prod : s + prod;
+            first = false;
+          }
+          uc[m] = s;
+        }
+        ch[0][n] = weno5_left(uc);
+        ch[1][n] = weno5_right(uc);
+      }
+      T cm[NE], cp[NE];
+      to_physical<DIM, DIR, T>(r, ch[0], cm);
+      to_physical<DIM, DIR, T>(r, ch[1], cp);
+      if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
+      // prime states of the reconstructed states (prime_state_handler.h:277-371),
+      // pressure recovered in double
+      double const pm = eos_pressure<DIM>(eos, double(cm[MASS]), double(cm[MOMX]),
+                                          DIM > 1 ? double(cm[MOMX + (DIM > 1)]) : 0.0,
+                                          DIM > 2 ? double(cm[MOMX + 2 * (DIM > 2)]) : 0.0,
+                                          double(cm[ENERGY]));
+      double const pp = eos_pressure<DIM>(eos, double(cp[MASS]), double(cp[MOMX]),
+                                          DIM > 1 ? double(cp[MOMX + (DIM > 1)]) : 0.0,
+                                          DIM > 2 ? double(cp[MOMX + 2 * (DIM > 2)]) : 0.0,
+                                          double(cp[ENERGY]));
+      if (!(pm > -bm.B) || !(pp > -bm.B)) valid = false;
+      T const vl = cm[mP] * (T(1) / cm[MASS]);
+      T const vr = cp[mP] * (T(1) / cp[MASS]);
+      hllc<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, flux);
+    } else {
+      // Roe flux-vector splitting (flux_splitting_scheme.cpp:42-76, 185-315)
+      T adv[6][NE];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        double const one_rho = 1.0 / cons[m][MASS];
+        double const p = eos_pressure<DIM>(
+            eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
+            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY]);
+        double const vel = cons[m][mP] * one_rho;
+        double const rho = cons[m][MASS];
+        adv[m][MASS] = T(rho * vel);
+        adv[m][ENERGY] = T((cons[m][ENERGY] + p) * vel);
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) {
+          double const vd = cons[m][MOMX + d] * one_rho;
+          double v = rho * (vel * vd);
+          if (d == DIR) v += p;
+          adv[m][MOMX + d] = T(v);
+        }
+      }
+      T const ev_nl0 = fabs(r.up - r.c), ev_nl1 = fabs(r.up + r.c), ev_lin = fabs(r.up);
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        T L[NE];
+        left_row<DIM, DIR, T>(n, r, L);
+        T const alpha = n == 0 ? ev_nl0 : (n == NE - 1 ? ev_nl1 : ev_lin);
+        T pos[6], neg[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          T sp = T(0), sn = T(0);
+          bool first = true;
+#pragma unroll
+          for (int q = 0; q < NE; ++q) {
+            int const l = sum_seq<DIM, DIR>(q);
+            if (!left_nonzero<DIM, DIR>(n, l)) continue;
+            T const uct = T(cons[m][l]) * L[l];
+            T const act = adv[m][l] * L[l];
+            T const tp = act + alpha * uct;
+            T const tn = act - alpha * uct;
+            sp = first ? tp : sp + tp;
+            sn = first ? tn : sn + tn;
+            first = false;
+          }
+          pos[m] = sp;
+          neg[m] = sn;
+        }
+        ch[0][n] = T(0.5) * (weno5_left(pos) + weno5_right(neg));
+      }
+      to_physical<DIM, DIR, T>(r, ch[0], flux);
+    }
+  } else {
+    // FV primitive reconstruction (primitive_state_reconstruction.h:56-107)
+    T pm[NE], pp[NE];
+    {
+      double prim[6][NE];
+#pragma unroll
+      for (int m = 0; m < 6; ++m) {
+        prim[m][RHO] = cons[m][MASS];
+        double const one_rho = 1.0 / cons[m][MASS];
+#pragma unroll
+        for (int d = 0; d < DIM; ++d) prim[m][VELX + d] = cons[m][MOMX + d] * one_rho;
+        prim[m][PRES] = eos_pressure<DIM>(
+            eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
+            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY]);
+      }
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        T arr[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n]);
+        pm[n] = weno5_left(arr);
+        pp[n] = weno5_right(arr);
+      }
+    }
+    // PrimeStatesToConservatives (prime_state_handler.h:195-275)
+    T cm[NE], cp[NE];
+    cm[MASS] = pm[RHO];
+    cp[MASS] = pp[RHO];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) {
+      cm[MOMX + d] = pm[VELX + d] * pm[RHO];
+      cp[MOMX + d] = pp[VELX + d] * pp[RHO];
+    }
+    cm[ENERGY] = eos_energy<DIM, T>(eos, pm[RHO], pm[VELX], DIM > 1 ? pm[VELX + (DIM > 1)] : T(0),
+                                    DIM > 2 ? pm[VELX + 2 * (DIM > 2)] : T(0), pm[PRES]);
+    cp[ENERGY] = eos_energy<DIM, T>(eos, pp[RHO], pp[VELX], DIM > 1 ? pp[VELX + (DIM > 1)] : T(0),
+                                    DIM > 2 ? pp[VELX + 2 * (DIM > 2)] : T(0), pp[PRES]);
+    if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
+    if (!(double(pm[PRES]) > -bm.B) || !(double(pp[PRES]) > -bm.B)) valid = false;
+    hllc<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR], flux);
+  }
+
+  int fi[3];
+  fi[DIR] = a;
+  fi[M::O1] = p1 + 1;
+  fi[M::O2] = p2 + 1;
+  double *fo = F + (long long)item * stride + G::face(fi[0], fi[1], fi[2]);
+#pragma unroll
+  for (int f = 0; f < NE; ++f) {
+    double const v = valid ? double(flux[f]) : 0.0;
+    if (ACCUM) {
+      if (valid) fo[f * G::FACES] += v;
+    } else {
+      fo[f * G::FACES] = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// divergence, stage update
+// ---------------------------------------------------------------------------
+
+// Flux divergence of interior cell (i, j, k) for field f (space_solver.cpp:131-153):
+// DimensionAwareConsistencyManagedSum(dFx, dFy, dFz) * (1 / cell_size).
+template <int DIM>
+__device__ __forceinline__ double divergence(double const *Fx, double const *Fy,
+                                             double const *Fz, int i, int j, int k,
+                                             double one_cell_size) {
+  using G = Geo<DIM>;
+  double const dx = Fx[G::face(i, j + 1, k + 1)] - Fx[G::face(i + 1, j + 1, k + 1)];
+  double dy = 0.0, dz = 0.0;
+  if constexpr (DIM > 1) dy = Fy[G::face(i + 1, j, k + 1)] - Fy[G::face(i + 1, j + 1, k + 1)];
+  if constexpr (DIM > 2) dz = Fz[G::face(i + 1, j + 1, k)] - Fz[G::face(i + 1, j + 1, k + 1)];
+  return dacms<DIM>(dx, dy, dz) * one_cell_size;
+}
+
+template <int DIM>
+__device__ __forceinline__ void interior_coords(int t, int &i, int &j, int &k) {
+  if constexpr (DIM == 3) {
+    i = t >> 8;
+    j = (t >> 4) & 15;
+    k = t & 15;
+  } else if constexpr (DIM == 2) {
+    i = t >> 4;
+    j = t & 15;
+    k = 0;
+  } else {
+    i = t;
+    j = 0;
+    k = 0;
+  }
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+divergence_kernel(int const *__restrict__ work, BlockMeta const *__restrict__ meta, BlockMeta def,
+                  double const *__restrict__ F, long long stride, long long dstride,
+                  double *__restrict__ rhs) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  double *rb = rhs + (size_t)slot * G::BLOCK_DOUBLES;
+  // zero every cell (space_solver.cpp:58-70), then write the interior
+  for (int x = threadIdx.x; x < G::BLOCK_DOUBLES; x += blockDim.x) rb[x] = 0.0;
+  __syncthreads();
+  BlockMeta const bm = meta ? meta[slot] : def;
+  double const ocs = 1.0 / bm.cell_size;
+  double const *Fb = F + (long long)item * stride;
+  for (int t = threadIdx.x; t < G::INTERIOR; t += blockDim.x) {
+    int i, j, k;
+    interior_coords<DIM>(t, i, j, k);
+    int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+#pragma unroll
+    for (int f = 0; f < G::NE; ++f) {
+      double const *fx = Fb + f * G::FACES;
+      rb[f * G::CELLS + c] =
+          0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
+    }
+  }
+}
+
+// SSP-RK3 stage (runge_kutta_3_TVD.h:41-59; time_integrator.h:98-113, 369-457)
+__constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
+__constant__ double kRkA0[3] = {0.0, 0.25, 2.0 / 3.0};
+__constant__ double kRkA1[3] = {0.0, 0.75, 1.0 / 3.0};
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+stage_update_kernel(double *__restrict__ U, double *__restrict__ U0, int const *__restrict__ work,
+                    BlockMeta const *__restrict__ meta, BlockMeta def,
+                    double const *__restrict__ F, long long stride, long long dstride, int stage,
+                    CaseState const *__restrict__ cases, double dt_all) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  double const dt = cases ? cases[bm.case_id].dt : dt_all;
+  if (!(dt > 0.0)) return;
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= G::INTERIOR) return;
+  int i, j, k;
+  interior_coords<DIM>(t, i, j, k);
+  int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+  double const ocs = 1.0 / bm.cell_size;
+  double const cdt = kRkC[stage] * (0.0 + dt);
+  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+  double const *Fb = F + (long long)item * stride;
+  size_t const base = (size_t)slot * G::BLOCK_DOUBLES + c;
+#pragma unroll
+  for (int f = 0; f < G::NE; ++f) {
+    double const *fx = Fb + f * G::FACES;
+    double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
+    size_t const x = base + (size_t)f * G::CELLS;
+    double u = U[x];
+    if (stage == 0) {
+      U0[x] = u;
+    } else {
+      u = a0 * u + a1 * U0[x];
+    }
+    U[x] = u + cdt * rhs;
+  }
+}
+
+// Stage update from a reference-layout right-hand-side buffer.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+rk_stage_rhs_kernel(double *__restrict__ U, double *__restrict__ U0,
+                    double const *__restrict__ rhs, int stage, double dt) {
+  using G = Geo<DIM>;
+  int const slot = blockIdx.x;
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= G::INTERIOR) return;
+  int i, j, k;
+  interior_coords<DIM>(t, i, j, k);
+  int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+  double const cdt = kRkC[stage] * (0.0 + dt);
+  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+#pragma unroll
+  for (int f = 0; f < G::NE; ++f) {
+    size_t const x = (size_t)slot * G::BLOCK_DOUBLES + (size_t)f * G::CELLS + c;
+    double u = U[x];
+    if (stage == 0) U0[x] = u;
+    else u = a0 * u + a1 * U0[x];
+    U[x] = u + cdt * rhs[x];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// halos
+// ---------------------------------------------------------------------------
+
+// Same-level halo regions (communication_types.h:45-132): for direction offset
+// o = +1 the halo [HS+IC, TC) takes the neighbour's [HS, 2HS); o = -1 the halo
+// [0, HS) takes the neighbour's [IC, IC+HS); o = 0 spans the interior.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+halo_region_kernel(double *__restrict__ U, int const *__restrict__ work,
+                   int const *__restrict__ nbr26, BlockMeta const *__restrict__ meta,
+                   CaseState const *__restrict__ cases, int faces_only, int nfields) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  if (cases && meta && !(cases[meta[slot].case_id].dt > 0.0)) return;
+  // blockIdx.y enumerates the 26 (or 2*DIM) regions
+  int o;
+  if (faces_only) {
+    int const face = blockIdx.y;  // W,E,S,N,B,T
+    int off[3] = {0, 0, 0};
+    off[face / 2] = (face & 1) ? 1 : -1;
+    o = (off[0] + 1) * 9 + (off[1] + 1) * 3 + (off[2] + 1);
+  } else {
+    o = blockIdx.y < 13 ? blockIdx.y : blockIdx.y + 1;
+  }
+  int const off[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+  for (int d = DIM; d < 3; ++d)
+    if (off[d] != 0) return;
+  int const n = nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)];
+  if (n < 0) return;  // domain face: zero gradient below
+  int lo[3], ext[3], src[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    if (d >= DIM) {
+      lo[d] = 0; ext[d] = 1; src[d] = 0;
+    } else if (off[d] == 0) {
+      lo[d] = HS; ext[d] = IC; src[d] = HS;
+    } else if (off[d] > 0) {
+      lo[d] = HS + IC; ext[d] = HS; src[d] = HS;
+    } else {
+      lo[d] = 0; ext[d] = HS; src[d] = IC;
+    }
+  }
+  int const cells = ext[0] * ext[1] * ext[2];
+  double *dst = U + (size_t)slot * nfields * G::CELLS;
+  double const *sb = U + (size_t)n * nfields * G::CELLS;
+  for (int x = threadIdx.x; x < cells * nfields; x += blockDim.x) {
+    int const f = x / cells;
+    int const r = x - f * cells;
+    int const kk = r % ext[2];
+    int const jj = (r / ext[2]) % ext[1];
+    int const ii = r / (ext[2] * ext[1]);
+    dst[f * G::CELLS + G::cell(lo[0] + ii, lo[1] + jj, lo[2] + kk)] =
+        sb[f * G::CELLS + G::cell(src[0] + ii, src[1] + jj, src[2] + kk)];
+  }
+}
+
+// Zero-gradient halos of domain faces (boundary_constants.h:103-160, 211-252):
+// the halo takes the value of the first / last interior plane. With
+// faces_only the copy covers the interior extent of the face, otherwise the
+// reference's full TC x TC slab.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
+                     int const *__restrict__ nbr26, BlockMeta const *__restrict__ meta,
+                     CaseState const *__restrict__ cases, int faces_only, int nfields) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  if (cases && meta && !(cases[meta[slot].case_id].dt > 0.0)) return;
+  int const face = blockIdx.y;
+  int const dir = face / 2, high = face & 1;
+  int off[3] = {0, 0, 0};
+  off[dir] = high ? 1 : -1;
+  int const o = (off[0] + 1) * 9 + (off[1] + 1) * 3 + (off[2] + 1);
+  if (nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)] >= 0) return;
+  int lo[3], ext[3];
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    lo[d] = faces_only ? G::fic(d) : 0;
+    ext[d] = faces_only ? G::ic(d) : G::tc(d);
+  }
+  lo[dir] = high ? HS + IC : 0;
+  ext[dir] = HS;
+  int const plane = high ? HS + IC - 1 : HS;
+  int const cells = ext[0] * ext[1] * ext[2];
+  double *b = U + (size_t)slot * nfields * G::CELLS;
+  for (int x = threadIdx.x; x < cells * nfields; x += blockDim.x) {
+    int const f = x / cells;
+    int const r = x - f * cells;
+    int c[3];
+    c[2] = lo[2] + r % ext[2];
+    c[1] = lo[1] + (r / ext[2]) % ext[1];
+    c[0] = lo[0] + r / (ext[2] * ext[1]);
+    int s[3] = {c[0], c[1], c[2]};
+    s[dir] = plane;
+    b[f * G::CELLS + G::cell(c[0], c[1], c[2])] = b[f * G::CELLS + G::cell(s[0], s[1], s[2])];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// prime states, signal speed, dt
+// ---------------------------------------------------------------------------
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+prime_states_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                    BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ P) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+  double const *ub = U + (size_t)slot * G::BLOCK_DOUBLES;
+  double *pb = P + (size_t)slot * G::BLOCK_DOUBLES;
+  for (int x = blockIdx.y * blockDim.x + threadIdx.x; x < G::CELLS; x += gridDim.y * blockDim.x) {
+    double c[G::NE];
+#pragma unroll
+    for (int f = 0; f < G::NE; ++f) c[f] = ub[f * G::CELLS + x];
+    double const one_density = 1.0 / c[MASS];
+    pb[RHO * G::CELLS + x] = c[MASS];
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) pb[(VELX + d) * G::CELLS + x] = c[MOMX + d] * one_density;
+    pb[PRES * G::CELLS + x] = eos_pressure<DIM>(eos, c[MASS], c[MOMX],
+                                                DIM > 1 ? c[MOMX + (DIM > 1)] : 0.0,
+                                                DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY]);
+  }
+}
+
+// Signal speed of ComputeTimestepSize (modular_algorithm_assembler.cpp:1840-1870):
+// max over interior cells of ConsistencyManagedSum(|u_d| + c).
+template <int DIM>
+__global__ void __launch_bounds__(256)
+signal_speed_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                    BlockMeta const *__restrict__ meta, BlockMeta def, CaseState *cases,
+                    unsigned long long *out) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+  double const *ub = U + (size_t)slot * G::BLOCK_DOUBLES;
+  double smax = 0.0;
+  int bad = 0;
+  for (int t = threadIdx.x; t < G::INTERIOR; t += blockDim.x) {
+    int i, j, k;
+    interior_coords<DIM>(t, i, j, k);
+    int const x = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+    double c[G::NE];
+#pragma unroll
+    for (int f = 0; f < G::NE; ++f) c[f] = ub[f * G::CELLS + x];
+    double const one_density = 1.0 / c[MASS];
+    double const p = eos_pressure<DIM>(eos, c[MASS], c[MOMX], DIM > 1 ? c[MOMX + (DIM > 1)] : 0.0,
+                                       DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY]);
+    double const cs = eos_speed_of_sound<double>(eos, c[MASS], p);
+    double v[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) v[d] = fabs(c[MOMX + d] * one_density) + cs;
+    double s;
+    if constexpr (DIM == 1) s = v[0];
+    else if constexpr (DIM == 2) s = v[0] + v[1];
+    else s = cms3(v[0], v[1], v[2]);
+    if (!(s >= 0.0) || !(c[MASS] > 0.0)) bad = 1;  // NaN, negative density or c^2 < 0
+    smax = dmax(smax, s);
+  }
+  if (__syncthreads_or(bad) && threadIdx.x == 0 && cases) atomicOr(&cases[bm.case_id].status, 1);
+  // warp then CTA max (non-negative doubles order like their bit patterns)
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) smax = dmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+  __shared__ double red[32];
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = smax;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if (threadIdx.x == 0) {
+      unsigned long long *dst = cases ? &cases[bm.case_id].smax_bits : out;
+      atomicMax(dst, (unsigned long long)__double_as_longlong(v));
+    }
+  }
+}
+
+// dt = CFL / (smax / dx_finest), clipped to the end time
+// (modular_algorithm_assembler.cpp:1932, 1961-1982); 0 once t >= t_end or the
+// step budget is spent, which makes every kernel skip the case.
+__global__ void dt_finalize_kernel(CaseState *cases, int n) {
+  int const c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  CaseState &s = cases[c];
+  double const smax = __longlong_as_double((long long)s.smax_bits);
+  s.smax_bits = 0ull;
+  double dt = smax / s.h_min;
+  double local = dt == 0.0 ? DBL_MAX : s.cfl / dt;
+  if (s.t + local > s.t_end) local = dmax(s.t_end - s.t, 0.0);
+  if (!(s.t < s.t_end)) local = 0.0;
+  if (s.max_steps > 0 && s.steps >= s.max_steps) local = 0.0;
+  if (s.status) local = 0.0;
+  s.dt = local;
+}
+
+__global__ void step_commit_kernel(CaseState *cases, int n) {
+  int const c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  CaseState &s = cases[c];
+  if (s.dt > 0.0) {
+    s.t = s.t + (0.0 + s.dt);
+    s.steps += 1;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <int DIM, int DIR, typename T, bool ACC>
+cudaError_t face_flux_dir(Launch const &L, double *F, long long stride, int threads) {
+  using M = FaceMap<DIM, DIR>;
+  dim3 grid(L.nwork, (M::COUNT + threads - 1) / threads);
+  switch (L.scheme) {
+    case FV_CHAR:
+      face_flux_kernel<DIM, DIR, FV_CHAR, T, ACC>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride);
+      break;
+    case FV_PRIM:
+      face_flux_kernel<DIM, DIR, FV_PRIM, T, ACC>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride);
+      break;
+    case FS_ROE:
+      face_flux_kernel<DIM, DIR, FS_ROE, T, ACC>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <int DIM, typename T, bool ACC>
+cudaError_t face_flux_dim(Launch const &L, int dir, double *F, long long stride, int threads) {
+  if (dir == 0) return face_flux_dir<DIM, 0, T, ACC>(L, F, stride, threads);
+  if constexpr (DIM > 1)
+    if (dir == 1) return face_flux_dir<DIM, 1, T, ACC>(L, F, stride, threads);
+  if constexpr (DIM > 2)
+    if (dir == 2) return face_flux_dir<DIM, 2, T, ACC>(L, F, stride, threads);
+  return cudaErrorInvalidValue;
+}
+
+template <typename T, bool ACC>
+cudaError_t face_flux_t(Launch const &L, int dir, double *F, long long stride, int threads) {
+  switch (L.dim) {
+    case 1: return face_flux_dim<1, T, ACC>(L, dir, F, stride, threads);
+    case 2: return face_flux_dim<2, T, ACC>(L, dir, F, stride, threads);
+    case 3: return face_flux_dim<3, T, ACC>(L, dir, F, stride, threads);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int interior_of(int dim) { return dim == 3 ? 4096 : (dim == 2 ? 256 : 16); }
+
+}  // namespace
+
+cudaError_t launch_face_flux(Launch const &L, int dir, double *F, long long stride, bool accumulate,
+                             int block_threads) {
+  if (L.nwork <= 0) return cudaSuccess;
+  int const threads = block_threads > 0 ? block_threads : 128;
+  if (threads > 128 || (threads & 31)) return cudaErrorInvalidValue;
+  if (L.precision == FP32_FLUX)
+    return accumulate ? face_flux_t<float, true>(L, dir, F, stride, threads)
+                      : face_flux_t<float, false>(L, dir, F, stride, threads);
+  return accumulate ? face_flux_t<double, true>(L, dir, F, stride, threads)
+                    : face_flux_t<double, false>(L, dir, F, stride, threads);
+}
+
+cudaError_t launch_divergence(Launch const &L, double const *F, long long stride,
+                              long long dstride, double *rhs) {
+  if (L.nwork <= 0) return cudaSuccess;
+  dim3 grid(L.nwork);
+  switch (L.dim) {
+    case 1: divergence_kernel<1><<<grid, 256, 0, L.stream>>>(L.work, L.meta, L.def, F, stride, dstride, rhs); break;
+    case 2: divergence_kernel<2><<<grid, 256, 0, L.stream>>>(L.work, L.meta, L.def, F, stride, dstride, rhs); break;
+    case 3: divergence_kernel<3><<<grid, 256, 0, L.stream>>>(L.work, L.meta, L.def, F, stride, dstride, rhs); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage_update(Launch const &L, double *U0, double const *F, long long stride,
+                                long long dstride, int stage, CaseState const *cases, double dt) {
+  if (L.nwork <= 0) return cudaSuccess;
+  if (stage < 0 || stage > 2) return cudaErrorInvalidValue;
+  int const threads = 256;
+  dim3 grid(L.nwork, (interior_of(L.dim) + threads - 1) / threads);
+  switch (L.dim) {
+    case 1: stage_update_kernel<1><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    case 2: stage_update_kernel<2><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    case 3: stage_update_kernel<3><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rk_stage_rhs(int dim, double *U, double *U0, double const *rhs, int nb,
+                                int stage, double dt, cudaStream_t stream) {
+  if (nb <= 0) return cudaSuccess;
+  if (stage < 0 || stage > 2) return cudaErrorInvalidValue;
+  dim3 grid(nb, (interior_of(dim) + 255) / 256);
+  switch (dim) {
+    case 1: rk_stage_rhs_kernel<1><<<grid, 256, 0, stream>>>(U, U0, rhs, stage, dt); break;
+    case 2: rk_stage_rhs_kernel<2><<<grid, 256, 0, stream>>>(U, U0, rhs, stage, dt); break;
+    case 3: rk_stage_rhs_kernel<3><<<grid, 256, 0, stream>>>(U, U0, rhs, stage, dt); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_halo(Launch const &L, int const *nbr26, bool faces_only, int nfields,
+                        CaseState const *cases) {
+  if (L.nwork <= 0) return cudaSuccess;
+  int const regions = faces_only ? 2 * L.dim : 26;
+  dim3 g1(L.nwork, regions), g2(L.nwork, 2 * L.dim);
+  int const fo = faces_only ? 1 : 0;
+  switch (L.dim) {
+    case 1:
+      halo_region_kernel<1><<<g1, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      zero_gradient_kernel<1><<<g2, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      break;
+    case 2:
+      halo_region_kernel<2><<<g1, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      zero_gradient_kernel<2><<<g2, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      break;
+    case 3:
+      halo_region_kernel<3><<<g1, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      zero_gradient_kernel<3><<<g2, 256, 0, L.stream>>>(L.U, L.work, nbr26, L.meta, cases, fo, nfields);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_prime_states(Launch const &L, double *P) {
+  if (L.nwork <= 0) return cudaSuccess;
+  dim3 grid(L.nwork, 8);
+  switch (L.dim) {
+    case 1: prime_states_kernel<1><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, P); break;
+    case 2: prime_states_kernel<2><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, P); break;
+    case 3: prime_states_kernel<3><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, P); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_signal_speed(Launch const &L, CaseState *cases, unsigned long long *out) {
+  if (L.nwork <= 0) return cudaSuccess;
+  dim3 grid(L.nwork);
+  switch (L.dim) {
+    case 1: signal_speed_kernel<1><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
+    case 2: signal_speed_kernel<2><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
+    case 3: signal_speed_kernel<3><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_dt_finalize(CaseState *cases, int n, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  dt_finalize_kernel<<<(n + 127) / 128, 128, 0, stream>>>(cases, n);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_step_commit(CaseState *cases, int n, cudaStream_t stream) {
+  if (n <= 0) return cudaSuccess;
+  step_commit_kernel<<<(n + 127) / 128, 128, 0, stream>>>(cases, n);
+  return cudaGetLastError();
+}
+
+}  // namespace alp

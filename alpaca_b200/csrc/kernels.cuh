@@ -1,0 +1,78 @@
+// Launch interface of the block kernels (implemented in kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "layout.cuh"
+
+namespace alp {
+
+// Scheme ids of the compiled instantiations. They correspond to the
+// reference's compile-time selections (user_specifications):
+//   FV_CHAR : ConvectiveTermSolvers::FiniteVolume + StateReconstructionType::Characteristic
+//   FV_PRIM : ConvectiveTermSolvers::FiniteVolume + StateReconstructionType::Primitive
+//   FS_ROE  : ConvectiveTermSolvers::FluxSplitting + FluxSplitting::Roe
+// all with ReconstructionStencils::WENO5, RiemannSolvers::Hllc, SignalSpeed::Einfeldt.
+enum Scheme { FV_CHAR = 0, FV_PRIM = 1, FS_ROE = 2 };
+enum Precision { FP64 = 0, FP32_FLUX = 1 };
+
+// Work description shared by the launchers. A null `work` means the identity
+// worklist (item i is slot i); a null `meta` means every block uses `def`.
+struct Launch {
+  int dim;
+  int scheme;
+  int precision;
+  double *U;               // [slots][NE][cells]
+  int const *work;         // [nwork] slot ids, or null
+  int nwork;
+  BlockMeta const *meta;   // [slots], or null
+  BlockMeta def;
+  cudaStream_t stream;
+};
+
+// Face fluxes of direction `dir` for every work item into
+// F[item * flux_item_stride + field * FACES + face] (reference flux-array
+// layout). accumulate: += (drop-in contract), else = (zero for skipped faces).
+cudaError_t launch_face_flux(Launch const &L, int dir, double *F, long long flux_item_stride,
+                             bool accumulate, int block_threads = 0);
+
+// SpaceSolver right-hand side: rhs (reference layout, all cells) = 0, interior
+// = consistency-managed flux divergence / cell size. F as written by
+// launch_face_flux for each direction at F + dir * dir_stride.
+cudaError_t launch_divergence(Launch const &L, double const *F, long long flux_item_stride,
+                              long long dir_stride, double *rhs);
+
+// RK3 stage: U0 <- U on stage 0; U <- a0*U + a1*U0 + c*dt*div(F) on the
+// interior, dt per case from cases[meta.case_id].dt (skip when dt == 0).
+// When cases is null, `dt` is used for every block.
+cudaError_t launch_stage_update(Launch const &L, double *U0, double const *F,
+                                long long flux_item_stride, long long dir_stride, int stage,
+                                CaseState const *cases, double dt);
+
+// RK3 stage from a reference-layout RHS buffer, blocks 0..nb-1.
+cudaError_t launch_rk_stage_rhs(int dim, double *U, double *U0, double const *rhs, int nb,
+                                int stage, double dt, cudaStream_t stream);
+
+// Halo update of the work items' blocks. nbr26: [slots][26] neighbour slot ids
+// (-1 = domain face with zero gradient). faces_only copies the 2*dim face
+// slabs over the interior extent (all the dimension-split scheme reads);
+// otherwise all 26 regions followed by the reference's full zero-gradient slabs.
+// nfields: number of fields per block (NE for conservative buffers).
+// When cases != null, blocks of cases with dt == 0 are skipped.
+cudaError_t launch_halo(Launch const &L, int const *nbr26, bool faces_only, int nfields,
+                        CaseState const *cases);
+
+// Prime states of every cell (reference layout) into P.
+cudaError_t launch_prime_states(Launch const &L, double *P);
+
+// Max signal speed per case over the work items' interior cells, folded into
+// cases[case_id].smax_bits; with cases == null into *smax_bits_out.
+cudaError_t launch_signal_speed(Launch const &L, CaseState *cases,
+                                unsigned long long *smax_bits_out);
+
+// dt for every case from its smax (ComputeTimestepSize), then resets smax.
+cudaError_t launch_dt_finalize(CaseState *cases, int ncases, cudaStream_t stream);
+// t += dt, steps += (dt > 0) for every case.
+cudaError_t launch_step_commit(CaseState *cases, int ncases, cudaStream_t stream);
+
+}  // namespace alp

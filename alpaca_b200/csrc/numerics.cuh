@@ -1,0 +1,343 @@
+// Device numerics of the ALPACA face flux: stiffened-gas EOS, WENO5-JS, the
+// Roe eigensystem, HLLC with Einfeldt speeds and Roe flux-vector splitting.
+// Each function states the reference lines (ALPACA src/) whose arithmetic it
+// follows; the association order of every sum is kept so that results agree
+// with the CPU reference to rounding (FMA contraction is the only difference).
+// T is the compute type of reconstruction and flux (double, or float in the
+// FP32-flux form); pressure recovery from total energy always runs in double.
+#pragma once
+
+#include <cfloat>
+
+#include "layout.cuh"
+
+namespace alp {
+
+template <typename T> __device__ __forceinline__ T dmin(T a, T b) { return (b < a) ? b : a; }
+template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return (a < b) ? b : a; }
+template <typename T> __device__ __forceinline__ T eps_of();
+template <> __device__ __forceinline__ double eps_of<double>() { return DBL_EPSILON; }
+template <> __device__ __forceinline__ float eps_of<float>() { return FLT_EPSILON; }
+
+// ConsistencyManagedSum with FUSY on (utilities/mathematical_functions.h:79-89)
+template <typename T> __device__ __forceinline__ T cms3(T a, T b, T c) {
+  T const s1 = (a + b) + c;
+  T const s2 = (a + c) + b;
+  T const s3 = (b + c) + a;
+  T mn = s1, mx = s1;
+  if (s2 < mn) mn = s2;
+  if (s3 < mn) mn = s3;
+  if (mx < s2) mx = s2;
+  if (mx < s3) mx = s3;
+  return T(0.5) * (mn + mx);
+}
+
+// DimensionAwareConsistencyManagedSum (mathematical_functions.h:98-108)
+template <int DIM, typename T> __device__ __forceinline__ T dacms(T a, T b, T c) {
+  if constexpr (DIM == 1) return a;
+  else if constexpr (DIM == 2) return a + b;
+  else return cms3(a, b, c);
+}
+
+// ---- stiffened gas (generic_stiffened_gas.h:40-102, stiffened_gas.cpp:62-149,
+//      stiffened_gas_safe.cpp:61-146) --------------------------------------
+
+struct Eos {
+  double gamma, B;
+  int safe;
+};
+
+template <int DIM>
+__device__ __forceinline__ double eos_pressure(Eos const &e, double mass, double mx, double my,
+                                               double mz, double energy) {
+  if (e.safe) {
+    double const p = -e.gamma * e.B + (e.gamma - 1.0) *
+                                          (energy - 0.5 * dacms<DIM>(mx * mx, my * my, mz * mz) /
+                                                        dmax(mass, DBL_EPSILON));
+    return dmax(p, -e.B + DBL_EPSILON);
+  }
+  double const q = 0.5 * dacms<DIM>(mx * mx, my * my, mz * mz);
+  return -e.gamma * e.B + (e.gamma - 1.0) * (energy - q / mass);
+}
+
+template <int DIM, typename T>
+__device__ __forceinline__ T eos_energy(Eos const &e, T rho, T u, T v, T w, T p) {
+  T const g = T(e.gamma), B = T(e.B);
+  return (p + g * B) / (g - T(1)) + (T(0.5) * dacms<DIM>(u * u, v * v, w * w) * rho);
+}
+
+template <typename T> __device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p) {
+  T const g = T(e.gamma), B = T(e.B);
+  if (e.safe) {
+    T const c2 = g * (p + B) / dmax(rho, eps_of<T>());
+    return sqrt(dmax(c2, eps_of<T>()));
+  }
+  return sqrt(g * (p + B) / rho);
+}
+
+// ---- WENO5-JS (stencils/spatial_reconstruction_stencils/weno5.h:88-158) --
+// a[0..5] are cells i-2..i+3 around face i+1/2; UpwindLeft uses {offset 0,
+// sign +1}, UpwindRight {1, -1} (stencils/apply_wrapper.h:47-57).
+template <typename T>
+__device__ __forceinline__ T weno5_core(T v1, T v2, T v3, T v4, T v5) {
+  T const c1 = T(13.0 / 12.0), c2 = T(0.25);
+  T const s11 = v1 + T(-2.0) * v2 + v3;
+  T const s12 = v1 + T(-4.0) * v2 + T(3.0) * v3;
+  T const s1 = c1 * s11 * s11 + c2 * s12 * s12;
+  T const s21 = v2 + T(-2.0) * v3 + v4;
+  T const s22 = v2 + T(-1.0) * v4;
+  T const s2 = c1 * s21 * s21 + c2 * s22 * s22;
+  T const s31 = v3 + T(-2.0) * v4 + v5;
+  T const s32 = T(3.0) * v3 + T(-4.0) * v4 + v5;
+  T const s3 = c1 * s31 * s31 + c2 * s32 * s32;
+  T const eps = T(1.0e-6);
+  T const a1 = T(0.1) / ((s1 + eps) * (s1 + eps));
+  T const a2 = T(0.6) / ((s2 + eps) * (s2 + eps));
+  T const a3 = T(0.3) / ((s3 + eps) * (s3 + eps));
+  T const one_a_sum = T(1.0) / (a1 + a2 + a3);
+  T const w1 = a1 * one_a_sum;
+  T const w2 = a2 * one_a_sum;
+  T const w3 = a3 * one_a_sum;
+  return w1 * (T(2.0 / 6.0) * v1 + T(-7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3) +
+         w2 * (T(-1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(2.0 / 6.0) * v4) +
+         w3 * (T(2.0 / 6.0) * v3 + T(5.0 / 6.0) * v4 + T(-1.0 / 6.0) * v5);
+}
+template <typename T> __device__ __forceinline__ T weno5_left(T const (&a)[6]) {
+  return weno5_core(a[0], a[1], a[2], a[3], a[4]);
+}
+template <typename T> __device__ __forceinline__ T weno5_right(T const (&a)[6]) {
+  return weno5_core(a[5], a[4], a[3], a[2], a[1]);
+}
+
+// ---- Roe eigensystem (solvers/eigendecomposition.h:181-467) --------------
+// The left/right eigenvector matrices are never stored: their entries are
+// generated from the Roe-averaged scalars below when applied.
+template <typename T> struct Roe {
+  T up, u1, u2;     // principal, first and second minor velocity
+  T H;              // enthalpy
+  T c, cc, one_cc;  // speed of sound, c^2, 1/c^2
+  T half_cc;        // 0.5 * one_cc
+  T gru;            // Gruneisen coefficient gamma - 1
+  T rho, one_rho;   // Roe density and its inverse
+  T q2;             // |u|^2 (dimension-aware sum)
+};
+
+// minor directions (eigendecomposition.h:84-125)
+template <int DIR> struct Minor;
+template <> struct Minor<0> { static constexpr int m1 = 1, m2 = 2; };
+template <> struct Minor<1> { static constexpr int m1 = 0, m2 = 2; };
+template <> struct Minor<2> { static constexpr int m1 = 0, m2 = 1; };
+
+// symmetry-preserving summation order of the characteristic projection
+// (solvers/state_reconstruction/state_reconstruction.h:35-58): position q of
+// the sequence for direction DIR.
+template <int DIM, int DIR> __host__ __device__ constexpr int sum_seq(int q) {
+  if (DIM == 1) return q == 0 ? MOMX : (q == 1 ? MASS : ENERGY);
+  if (DIM == 2) return q < 2 ? MOMX + q : (q == 2 ? MASS : ENERGY);
+  if (q >= 3) return q == 3 ? MASS : ENERGY;
+  // 3D: X -> (MomY, MomZ, MomX), Y -> (MomZ, MomX, MomY), Z -> (MomX, MomY, MomZ)
+  return MOMX + (DIR + 1 + q) % 3;
+}
+
+// Cell quantities the Roe average needs; conservatives are double.
+template <int DIM, int DIR> struct CellPrims {
+  double rho, one_rho, p, up, u1, u2, H;
+};
+
+template <int DIM, int DIR>
+__device__ __forceinline__ CellPrims<DIM, DIR> cell_prims(Eos const &e, double const (&c)[DIM + 2]) {
+  CellPrims<DIM, DIR> r;
+  r.rho = c[MASS];
+  r.one_rho = 1.0 / c[MASS];
+  double const mx = c[MOMX];
+  double const my = DIM > 1 ? c[MOMX + (DIM > 1 ? 1 : 0)] : 0.0;
+  double const mz = DIM > 2 ? c[MOMX + (DIM > 2 ? 2 : 0)] : 0.0;
+  // velocities from the prime-state buffer: momentum * (1/rho)
+  // (prime_state_handler.h:293-311)
+  r.up = c[MOMX + DIR] * r.one_rho;
+  r.u1 = DIM > 1 ? c[MOMX + (DIM > 1 ? Minor<DIR>::m1 : 0)] * r.one_rho : 0.0;
+  r.u2 = DIM > 2 ? c[MOMX + (DIM > 2 ? Minor<DIR>::m2 : 0)] * r.one_rho : 0.0;
+  r.p = eos_pressure<DIM>(e, c[MASS], mx, my, mz, c[ENERGY]);
+  // Enthalpy (stiffened_gas.cpp:88-96 / stiffened_gas_safe.cpp:77-84)
+  r.H = e.safe ? (c[ENERGY] + r.p) / dmax(c[MASS], DBL_EPSILON) : (c[ENERGY] + r.p) / c[MASS];
+  return r;
+}
+
+// Roe averages of one face (eigendecomposition.h:252-310)
+template <int DIM, int DIR, typename T>
+__device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> const &t,
+                                              CellPrims<DIM, DIR> const &n) {
+  Roe<T> r;
+  T const gB = T(e.gamma * e.B);
+  T const psi_t = (T(t.p) + gB) * T(t.one_rho);
+  T const psi_n = (T(n.p) + gB) * T(n.one_rho);
+  T const sr_t = sqrt(T(t.rho));
+  T const sr_n = sqrt(T(n.rho));
+  T const rho_div = T(1) / (sr_t + sr_n);
+  r.rho = sr_t * sr_n;
+  r.one_rho = T(1) / r.rho;
+  r.up = ((T(t.up) * sr_t) + (T(n.up) * sr_n)) * rho_div;
+  r.u1 = ((T(t.u1) * sr_t) + (T(n.u1) * sr_n)) * rho_div;
+  r.u2 = ((T(t.u2) * sr_t) + (T(n.u2) * sr_n)) * rho_div;
+  T const psi = ((psi_t * sr_t) + (psi_n * sr_n)) * rho_div;
+  r.H = (T(t.H) * sr_t + T(n.H) * sr_n) * rho_div;
+  r.gru = T(e.gamma - 1.0);
+  r.q2 = dacms<DIM>(r.up * r.up, r.u1 * r.u1, r.u2 * r.u2);
+  T const dup = T(t.up) - T(n.up), du1 = T(t.u1) - T(n.u1), du2 = T(t.u2) - T(n.u2);
+  T const tmp = dacms<DIM>(dup * dup, du1 * du1, du2 * du2);
+  T const p_over_rho = ((T(t.p) * T(t.one_rho)) * sr_t + (T(n.p) * T(n.one_rho)) * sr_n) * rho_div +
+                       T(0.5) * r.rho * (rho_div * rho_div) * tmp;
+  r.cc = psi + r.gru * p_over_rho;
+  r.one_cc = T(1) / r.cc;
+  r.c = sqrt(r.cc);
+  r.half_cc = T(0.5) * r.one_cc;
+  return r;
+}
+
+// Row n of the left eigenvector matrix, indexed by conservative equation
+// (eigendecomposition.h:316-359). Entries that are structurally zero are
+// returned as 0 and skipped by the projection (adding 0*u leaves a sum unchanged).
+template <int DIM, int DIR, typename T>
+__device__ __forceinline__ void left_row(int n, Roe<T> const &r, T (&L)[DIM + 2]) {
+  constexpr int NE = DIM + 2;
+  constexpr int mP = MOMX + DIR;
+  constexpr int m1 = MOMX + (DIM > 1 ? Minor<DIR>::m1 : 0);
+  constexpr int m2 = MOMX + (DIM > 2 ? Minor<DIR>::m2 : 0);
+#pragma unroll
+  for (int l = 0; l < NE; ++l) L[l] = T(0);
+  if (n == 0 || n == NE - 1) {
+    T const sgn = n == 0 ? T(1) : T(-1);
+    // 0.5/cc * (gru q^2 - gru H +/- (u +/- c) c)
+    if (n == 0)
+      L[MASS] = r.half_cc * (r.gru * r.q2 - r.gru * r.H + (r.up + r.c) * r.c);
+    else
+      L[MASS] = r.half_cc * (r.gru * r.q2 - r.gru * r.H - (r.up - r.c) * r.c);
+    L[mP] = r.half_cc * (-r.up * r.gru - sgn * r.c);
+    if (DIM > 1) L[m1] = r.half_cc * (-r.u1 * r.gru);
+    if (DIM > 2) L[m2] = r.half_cc * (-r.u2 * r.gru);
+    L[ENERGY] = r.half_cc * r.gru;
+  } else if (n == DIM) {  // principal-momentum wave
+    L[MASS] = r.one_cc * (r.H - r.q2);
+    L[mP] = r.one_cc * r.up;
+    if (DIM > 1) L[m1] = r.one_cc * r.u1;
+    if (DIM > 2) L[m2] = r.one_cc * r.u2;
+    L[ENERGY] = -r.one_cc;
+  } else if (n == 1) {  // first minor momentum (DIM >= 2)
+    L[MASS] = r.u1 * r.one_rho;
+    L[m1] = -r.one_rho;
+  } else {  // n == 2, second minor momentum (DIM == 3)
+    L[MASS] = -r.u2 * r.one_rho;
+    L[m2] = r.one_rho;
+  }
+}
+
+// TransformToPhysicalSpace with generated right eigenvectors
+// (eigendecomposition.h:144-165 and 366-409): linear waves summed first, then
+// the nonlinear pair (u-c, u+c) added together.
+template <int DIM, int DIR, typename T>
+__device__ __forceinline__ void to_physical(Roe<T> const &r, T const (&ch)[DIM + 2],
+                                            T (&out)[DIM + 2]) {
+  constexpr int NE = DIM + 2;
+  constexpr int EV = DIM;
+  constexpr int mP = MOMX + DIR;
+  constexpr int m1 = MOMX + (DIM > 1 ? Minor<DIR>::m1 : 0);
+  constexpr int m2 = MOMX + (DIM > 2 ? Minor<DIR>::m2 : 0);
+  // R[MASS][*] = (1, 0, 0, gru, 1)
+  {
+    T s = ch[EV] * r.gru;  // minor columns are zero
+    out[MASS] = s + (ch[0] * T(1) + ch[NE - 1] * T(1));
+  }
+  // R[mP][*] = (u-c, 0, 0, gru*u, u+c)
+  {
+    T s = ch[EV] * (r.gru * r.up);
+    out[mP] = s + (ch[0] * (r.up - r.c) + ch[NE - 1] * (r.up + r.c));
+  }
+  if constexpr (DIM > 1) {
+    // R[m1][*] = (u1, -rho, 0, gru*u1, u1)
+    T s = ch[1] * (-r.rho);
+    s = s + ch[EV] * (r.gru * r.u1);
+    out[m1] = s + (ch[0] * r.u1 + ch[NE - 1] * r.u1);
+  }
+  if constexpr (DIM > 2) {
+    // R[m2][*] = (u2, 0, rho, gru*u2, u2)
+    T s = ch[2] * r.rho;
+    s = s + ch[EV] * (r.gru * r.u2);
+    out[m2] = s + (ch[0] * r.u2 + ch[NE - 1] * r.u2);
+  }
+  // R[ENERGY][*] = (H - u c, -u1 rho, rho u2, gru H - c c, H + u c)
+  {
+    T s = T(0);
+    if constexpr (DIM > 1) s = ch[1] * (-r.u1 * r.rho);
+    if constexpr (DIM > 2) s = s + ch[2] * (r.rho * r.u2);
+    s = s + ch[EV] * (r.gru * r.H - r.c * r.c);
+    out[ENERGY] = s + (ch[0] * (r.H - r.up * r.c) + ch[NE - 1] * (r.H + r.up * r.c));
+  }
+}
+
+// ---- HLLC with Einfeldt signal speeds -------------------------------------
+// CalculateSignalSpeed, Einfeldt (hll_signal_speed_calculator.h:77-101) and
+// HllcRiemannSolver::SolveRiemannProblemImplementation (hllc_riemann_solver.h:52-198)
+template <int DIM, int DIR, typename T>
+__device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T const (&cr)[DIM + 2],
+                                     T pres_l, T pres_r, T vel_l, T vel_r,
+                                     T (&flux)[DIM + 2]) {
+  constexpr int NE = DIM + 2;
+  constexpr int mP = MOMX + DIR;
+  T const one_rl = T(1) / cl[MASS], one_rr = T(1) / cr[MASS];
+  T const c_l = eos_speed_of_sound(e, cl[MASS], pres_l);
+  T const c_r = eos_speed_of_sound(e, cr[MASS], pres_r);
+  T const srl = sqrt(cl[MASS]);
+  T const srr = sqrt(cr[MASS]);
+  T const rho_div = T(1) / (srl + srr);
+  T const u_roe = ((vel_l * srl) + (vel_r * srr)) * rho_div;
+  T const c_e = sqrt(((c_l * c_l * srl) + (c_r * c_r * srr)) * rho_div +
+                     (T(0.5) * srl * srr * rho_div * rho_div) * (vel_r - vel_l) * (vel_r - vel_l));
+  T const sls = dmin(u_roe - c_e, vel_l - c_l);
+  T const srs = dmax(u_roe + c_e, vel_r + c_r);
+  T const s_star = ((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r))) /
+                   (cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
+  T const sl = dmin(sls, T(0));
+  T const sr = dmax(srs, T(0));
+  T const chi_l = (sls - vel_l) / (sls - s_star);
+  T const chi_r = (srs - vel_r) / (srs - s_star);
+  T const rchi_l = cl[MASS] * chi_l, rchi_r = cr[MASS] * chi_r;
+  T const sg = T((T(0) < s_star) - (s_star < T(0)));
+  T const wl = T(0.5) * (T(1) + sg), wr = T(0.5) * (T(1) - sg);
+  // mass
+  {
+    T const fsl = cl[mP] + (sl * (rchi_l - cl[MASS]));
+    T const fsr = cr[mP] + (sr * (rchi_r - cr[MASS]));
+    flux[MASS] = wl * fsl + wr * fsr;
+  }
+  // principal momentum
+  {
+    T const fl = ((cl[mP] * cl[mP]) * one_rl) + pres_l;
+    T const fr = ((cr[mP] * cr[mP]) * one_rr) + pres_r;
+    T const fsl = fl + (sl * (rchi_l * s_star - cl[mP]));
+    T const fsr = fr + (sr * (rchi_r * s_star - cr[mP]));
+    flux[mP] = wl * fsl + wr * fsr;
+  }
+  // energy (the star-state pressure term uses the clamped speeds, :131-144)
+  {
+    T const el = rchi_l * (cl[ENERGY] * one_rl +
+                           (s_star - vel_l) * (s_star + pres_l / (cl[MASS] * (sl - vel_l))));
+    T const er = rchi_r * (cr[ENERGY] * one_rr +
+                           (s_star - vel_r) * (s_star + pres_r / (cr[MASS] * (sr - vel_r))));
+    T const fl = vel_l * (cl[ENERGY] + pres_l);
+    T const fr = vel_r * (cr[ENERGY] + pres_r);
+    T const fsl = fl + (sl * (el - cl[ENERGY]));
+    T const fsr = fr + (sr * (er - cr[ENERGY]));
+    flux[ENERGY] = wl * fsl + wr * fsr;
+  }
+  // minor momenta
+#pragma unroll
+  for (int d = 0; d < DIM - 1; ++d) {
+    int const mm = MOMX + (d == 0 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+    T const fsl = vel_l * cl[mm] + (sl * (chi_l * cl[mm] - cl[mm]));
+    T const fsr = vel_r * cr[mm] + (sr * (chi_r * cr[mm] - cr[mm]));
+    flux[mm] = wl * fsl + wr * fsr;
+  }
+  (void)NE;
+}
+
+}  // namespace alp

@@ -1,0 +1,128 @@
+"""ctypes bindings of the C ABI in include/alpaca_b200.h.
+
+The CUDA library is built in-tree (alpaca_b200/libalpaca_b200.so). Loading
+fails loudly when it is missing: there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libalpaca_b200.so")
+HEADER = os.path.join(os.path.dirname(HERE), "include", "alpaca_b200.h")
+
+ALP_OK, ALP_ERR_INVALID, ALP_ERR_CUDA, ALP_ERR_CAPACITY, ALP_ERR_NOT_FOUND, ALP_ERR_NUMERIC = range(6)
+FLUX_SPLITTING, FINITE_VOLUME = 0, 1
+RECON_CONSERVATIVE, RECON_PRIMITIVE, RECON_CHARACTERISTIC = 0, 1, 2
+STENCIL_WENO5 = 4
+RIEMANN_HLLC = 0
+SIGNAL_SPEED_EINFELDT = 0
+FLUX_SPLITTING_ROE = 0
+RK3 = 1
+FP64, FP32_FLUX = 0, 1
+HALO_ALL, HALO_FACES = 0, 1
+
+
+class AlpacaError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"alpaca_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Scheme(C.Structure):
+    """alp_scheme: the reference's user_specifications selections."""
+    _fields_ = [("convective_term_solver", C.c_int), ("state_reconstruction", C.c_int),
+                ("reconstruction_stencil", C.c_int), ("riemann_solver", C.c_int),
+                ("signal_speed", C.c_int), ("flux_splitting", C.c_int),
+                ("time_integrator", C.c_int), ("precision", C.c_int)]
+
+    @classmethod
+    def make(cls, variant: str = "fvchar", precision: int = FP64) -> "Scheme":
+        s = cls()
+        s.convective_term_solver = FINITE_VOLUME
+        s.state_reconstruction = RECON_CHARACTERISTIC
+        s.reconstruction_stencil = STENCIL_WENO5
+        s.riemann_solver = RIEMANN_HLLC
+        s.signal_speed = SIGNAL_SPEED_EINFELDT
+        s.flux_splitting = FLUX_SPLITTING_ROE
+        s.time_integrator = RK3
+        s.precision = precision
+        if variant == "fvprim":
+            s.state_reconstruction = RECON_PRIMITIVE
+        elif variant == "fsroe":
+            s.convective_term_solver = FLUX_SPLITTING
+        elif variant != "fvchar":
+            raise ValueError(variant)
+        return s
+
+
+class Material(C.Structure):
+    """alp_material: stiffened gas (gamma, background pressure B, safe variant)."""
+    _fields_ = [("gamma", C.c_double), ("background_pressure", C.c_double), ("safe", C.c_int)]
+
+    @classmethod
+    def make(cls, gamma: float, B: float = 0.0, safe: bool = False) -> "Material":
+        return cls(gamma, B, int(safe))
+
+
+_D = C.POINTER(C.c_double)
+_I = C.POINTER(C.c_int)
+_V = C.c_void_p
+_S = C.c_void_p  # stream
+_SIGS = {
+    "alp_version": (C.c_char_p, []),
+    "alp_last_error": (C.c_char_p, []),
+    "alp_scheme_default": (None, [C.POINTER(Scheme)]),
+    "alp_convective_fluxes": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _V, C.c_int,
+                                        C.c_double, _V, _V, _V, _S]),
+    "alp_space_rhs_workspace_size": (C.c_size_t, [C.c_int, C.c_int]),
+    "alp_space_rhs": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _V, C.c_int,
+                                C.c_double, _V, _V, C.c_size_t, _S]),
+    "alp_prime_states": (C.c_int, [C.c_int, C.POINTER(Material), _V, C.c_int, _V, _S]),
+    "alp_halo_update": (C.c_int, [C.c_int, _V, C.c_int, C.c_int, _V, C.c_int, _S]),
+    "alp_timestep_size": (C.c_int, [C.c_int, C.POINTER(Material), _V, C.c_int, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, _D, _V, _S]),
+    "alp_rk3_stage": (C.c_int, [C.c_int, _V, _V, _V, C.c_int, C.c_int, C.c_double, _S]),
+    "alp_engine_create": (C.c_int, [C.c_int, C.POINTER(Scheme), C.c_int, C.c_int, C.POINTER(_V)]),
+    "alp_engine_destroy": (C.c_int, [_V]),
+    "alp_engine_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
+    "alp_engine_add_case": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_int, C.c_int, _I, _D, _I]),
+    "alp_engine_remove_case": (C.c_int, [_V, C.c_int]),
+    "alp_engine_step": (C.c_int, [_V, C.c_int]),
+    "alp_engine_get_case": (C.c_int, [_V, C.c_int, _D, _D, _I]),
+    "alp_engine_all_done": (C.c_int, [_V, _I]),
+    "alp_engine_stream": (_S, [_V]),
+    "alp_engine_set_graph": (C.c_int, [_V, C.c_int]),
+    "alp_engine_launches_per_step": (C.c_int, [_V]),
+}
+
+_lib = None
+
+
+def declared_symbols() -> list[str]:
+    """Function names declared in include/alpaca_b200.h."""
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"\b(alp_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with "
+                              "`python -c 'import __graft_entry__ as g; g.build()'`")
+        l = C.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            f = getattr(l, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != ALP_OK:
+        raise AlpacaError(rc, lib().alp_last_error().decode())

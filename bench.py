@@ -1,0 +1,326 @@
+"""Benchmark of the block RHS + SSP-RK3 engine on the 3D periodic 128^3 case.
+
+Workload (the headline configuration): 8 x 8 x 8 = 512 blocks of 16^3 cells
+(128^3 cells, 4-cell halos), ideal gas gamma 1.4, seeded Fourier-mode fields
+with a planar Mach-2 Rankine-Hugoniot shock, WENO5-JS characteristic
+reconstruction + HLLC (Einfeldt) + SSP-RK3 at CFL 0.6, all FP64.
+One step = one full SSP-RK3 step of the whole domain (dt reduction, three
+stages of fluxes / divergence + stage update / halo fill).
+metric: cell-updates/s = interior cells x steps / time.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Under torchrun each rank advances its own copy of the case (replicas: the path
+does not shard across GPUs); value = cells x steps x N / max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+B_ALG_3D = 320.0  # algorithmic HBM bytes per 3D cell-update (64 * N_eq, FP64 state)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--variant", default="fvchar", choices=["fvchar", "fvprim", "fsroe"])
+    p.add_argument("--blocks", type=int, default=8, help="blocks per dimension")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = []
+        mx = None
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in self.rows:
+            try:
+                sm.append(float(r[1]))
+                mx = float(r[2])
+                for n, v in zip(names, r[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+    return ws, rank, local
+
+
+def max_over_ranks(x: float, ws: int, dev=None) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=dev if dev is not None else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws: int, dev=None):
+    if ws > 1:
+        import torch.distributed as dist
+        if dev is not None:
+            dist.barrier(device_ids=[dev.index])
+        else:
+            dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# CPU arm: the reference's own hot path (oracle/_ref) on the host cores
+# ---------------------------------------------------------------------------
+
+def reference_cpu_sample(variant: str, budget_s: float, nthreads: int, steps: int | None = None,
+                         warmup: int = 0):
+    """Times the reference's compiled code (oracle/_ref; the restatement when the
+    reference was not built) on a 4x4x4-block periodic sample of the workload."""
+    import oracle
+    from alpaca_b200 import cases
+    kind = "reference" if oracle.Reference.available(3, variant) else "port"
+    impl = oracle.Reference(3, variant) if kind == "reference" else oracle.Restatement(3, variant)
+    case = cases.fourier_shock(4, dim=3, seed=1)
+    g = case.grid
+    u = case.u
+    if warmup:
+        u = impl.run(u, g.nbr, case.gamma, 0.0, False, g.cell_size, case.cfl, 1e300,
+                     max_steps=warmup, nthreads=nthreads)[0]
+    if steps is None:
+        t0 = time.perf_counter()
+        u = impl.run(u, g.nbr, case.gamma, 0.0, False, g.cell_size, case.cfl, 1e300, max_steps=1,
+                     nthreads=nthreads)[0]
+        one = time.perf_counter() - t0
+        steps = max(1, int(budget_s / max(one, 1e-3)))
+    t0 = time.perf_counter()
+    impl.run(u, g.nbr, case.gamma, 0.0, False, g.cell_size, case.cfl, 1e300, max_steps=steps,
+             nthreads=nthreads)
+    dt = time.perf_counter() - t0
+    cells = g.nb * 4096
+    return {"value": cells * steps / dt, "unit": METRIC, "cores": nthreads, "kind": kind,
+            "sample": f"{steps} SSP-RK3 steps of a 4x4x4-block (64^3-cell) periodic sample of the "
+                      f"same Fourier + Mach-2 workload, {variant}, FP64, {nthreads} threads",
+            "seconds": dt, "steps": steps}
+
+
+def run_reference_arm(args, ws, rank):
+    if rank != 0:
+        return
+    n = os.cpu_count() or 1
+    r = reference_cpu_sample(args.variant, 0.0, n, steps=args.steps, warmup=args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": r["seconds"] * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "impl": "reference",
+            "config": {"workload": "3d_periodic_fourier_mach2_128cubed_sample64cubed",
+                       "variant": args.variant, "blocks": 64, "cells": 64 ** 3},
+            "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def fp64_peak():
+    lib = C.CDLL(os.path.join(ROOT, "alpaca_b200", "libalpaca_b200_probe.so"))
+    lib.alp_probe_fp64_peak.argtypes = [C.c_int, C.c_int, C.POINTER(C.c_double)]
+    v = C.c_double()
+    if lib.alp_probe_fp64_peak(20000, 8, C.byref(v)) != 0:
+        return None
+    return v.value
+
+
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+
+    from alpaca_b200 import api, cases
+    from alpaca_b200 import native as N
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nbd = args.blocks
+    case = cases.fourier_shock(nbd, dim=3, seed=1)
+    cells = case.grid.nb * 4096
+    eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
+    stream = torch.cuda.ExternalStream(N.lib().alp_engine_stream(eng.h))
+    cid = eng.add_case(case, max_steps=0)
+    eng.step(args.warmup)
+    torch.cuda.synchronize()
+    barrier(ws, dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clocks:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        eng.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    torch.cuda.synchronize()
+    barrier(ws, dev)
+    ms = max_over_ranks(e0.elapsed_time(e1), ws, dev)
+    value = cells * args.steps * ws / (ms * 1e-3)
+    _, t_sim, steps_done = eng.get(cid)
+    launches = args.steps * eng.launches_per_step
+    eng.close()
+
+    # end to end through the public C ABI from pinned host buffers: upload the
+    # case, run the steps, read the state back (copies inside the timed region)
+    e2e = None
+    if not args.no_e2e:
+        host = torch.from_numpy(np.ascontiguousarray(case.u)).pin_memory()
+        case_p = cases.Case(case.name, case.grid, host.numpy(), case.gamma, case.B, case.cfl,
+                            case.t_end, 0)
+        out = torch.empty_like(host).pin_memory()
+        eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
+        stream = torch.cuda.ExternalStream(N.lib().alp_engine_stream(eng.h))
+        cid = eng.add_case(case_p, max_steps=0)
+        eng.step(args.warmup)
+        eng.remove_case(cid)
+        torch.cuda.synchronize()
+        barrier(ws, dev)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        cid = eng.add_case(case_p, max_steps=0)
+        eng.step(args.steps)
+        t_ = C.c_double()
+        s_ = C.c_int()
+        N.check(N.lib().alp_engine_get_case(eng.h, cid, C.cast(out.data_ptr(), C.POINTER(C.c_double)),
+                                            C.byref(t_), C.byref(s_)))
+        f1.record(stream)
+        f1.synchronize()
+        barrier(ws, dev)
+        ems = max_over_ranks(f0.elapsed_time(f1), ws, dev)
+        eng.close()
+        nbytes = host.numel() * 8
+        e2e = {"value": cells * args.steps * ws / (ems * 1e-3), "unit": METRIC,
+               "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
+               "ms": ems, "note": "one case per timed region: pinned H2D of the 512 blocks, "
+                                  f"{args.steps} steps, D2H of the final state; bytes amortised per step"}
+
+    if rank != 0:
+        return
+    hbm, src = peaks()
+    achieved = cells * args.steps / (ms * 1e-3) * B_ALG_3D / 1e9
+    fp64 = fp64_peak()
+    cpu = None
+    if not args.no_cpu_baseline:
+        cpu = reference_cpu_sample(args.variant, 15.0, os.cpu_count() or 1)
+        cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    clk = clocks.summary()
+    line = {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "3d_periodic_fourier_mach2_128cubed", "blocks": case.grid.nb,
+                   "cells_per_gpu": cells, "variant": args.variant,
+                   "scheme": "WENO5-JS characteristic + HLLC/Einfeldt + SSP-RK3" if args.variant == "fvchar" else args.variant,
+                   "cfl": 0.6, "l2": "state 283 MB per buffer > 126 MB L2 (no flush needed)",
+                   "parallelism": f"replicas x{ws}", "sim_time_reached": t_sim,
+                   "steps_done": steps_done},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "traffic": None,
+                     "peak_source": src,
+                     "kernel": "whole SSP-RK3 step (one CUDA-graph launch), 320 B/cell-update",
+                     "fp64_pipe_peak_tflops_measured": fp64},
+        "cpu_baseline": cpu,
+        "e2e": e2e,
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    try:
+        if args.impl == "reference":
+            run_reference_arm(args, ws, rank)
+        else:
+            run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

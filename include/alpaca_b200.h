@@ -1,0 +1,199 @@
+/*
+ * alpaca_b200 — C ABI of the B200 block right-hand side / SSP-RK3 engine.
+ *
+ * Drop-in for the hot path of tumaer/ALPACA (paths below are relative to the
+ * reference's src/): the convective term of SpaceSolver::UpdateFluxes, the
+ * prime-state conversion, the same-level halo update, ComputeTimestepSize and
+ * the RungeKutta3TVD stage update. Every buffer uses the reference's block
+ * layout (block_definitions/field_buffer.h:37-40): per block and field a
+ * C-ordered double[TCX][TCY][TCZ], TC = 24 in active dimensions and 1 in
+ * inactive ones, conservatives ordered Mass, Energy, MomentumX[, Y[, Z]]
+ * (block_definitions/field_setup.h:101-112), blocks one after the other.
+ *
+ * Conventions: pointers named d_* are device pointers, h_* host pointers.
+ * Every call is asynchronous on the given stream (0 = legacy default stream)
+ * and returns ALP_OK or an error code; no C++ exception crosses the ABI. The
+ * stateless calls allocate nothing; the engine allocates its device pool when
+ * it is created and never while stepping.
+ */
+#ifndef ALPACA_B200_H
+#define ALPACA_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st *alp_stream_t; /* == cudaStream_t */
+
+/* ---- status codes -------------------------------------------------------- */
+enum {
+  ALP_OK = 0,
+  ALP_ERR_INVALID = 1,       /* bad argument or unsupported selection */
+  ALP_ERR_CUDA = 2,          /* a CUDA call failed (see alp_last_error) */
+  ALP_ERR_CAPACITY = 3,      /* engine pool / case table full */
+  ALP_ERR_NOT_FOUND = 4,     /* unknown case id */
+  ALP_ERR_NUMERIC = 5        /* non-finite or non-positive state detected */
+};
+
+/* ---- scheme selection ---------------------------------------------------
+ * The values mirror the reference's compile-time enums so that a shadow of
+ * user_specifications/ selects the same combination:
+ *   convective_term_solver   riemann_solver_settings.h:28  (FluxSplitting=0, FiniteVolume=1)
+ *   state_reconstruction     state_reconstruction_settings.h:25 (Conservative=0, Primitive=1, Characteristic=2)
+ *   reconstruction_stencil   stencil_setup.h:26-43 (WENO5 = 4)
+ *   riemann_solver           riemann_solver_settings.h:47 (Hllc=0, Hllc_LM=1, Hll=2)
+ *   signal_speed             enums/signal_speed.h:31 (Einfeldt = 0)
+ *   flux_splitting           enums/flux_splitting.h:31 (Roe = 0)
+ *   time_integrator          numerical_setup.h:26 (RK2=0, RK3=1)
+ * Supported: FiniteVolume + {Primitive, Characteristic} + WENO5 + Hllc +
+ * Einfeldt, and FluxSplitting + Roe + WENO5; RK3.
+ * precision: ALP_FP64 (all arithmetic in double) or ALP_FP32_FLUX
+ * (reconstruction, smoothness indicators and Riemann fluxes in float; state,
+ * RK accumulation, pressure recovery and dt in double). */
+enum { ALP_FLUX_SPLITTING = 0, ALP_FINITE_VOLUME = 1 };
+enum { ALP_RECON_CONSERVATIVE = 0, ALP_RECON_PRIMITIVE = 1, ALP_RECON_CHARACTERISTIC = 2 };
+enum { ALP_STENCIL_WENO5 = 4 };
+enum { ALP_RIEMANN_HLLC = 0 };
+enum { ALP_SIGNAL_SPEED_EINFELDT = 0 };
+enum { ALP_FLUX_SPLITTING_ROE = 0 };
+enum { ALP_RK3 = 1 };
+enum { ALP_FP64 = 0, ALP_FP32_FLUX = 1 };
+
+typedef struct {
+  int convective_term_solver;
+  int state_reconstruction;
+  int reconstruction_stencil;
+  int riemann_solver;
+  int signal_speed;
+  int flux_splitting;
+  int time_integrator;
+  int precision;
+} alp_scheme;
+
+/* Stiffened-gas material (materials/equations_of_state/stiffened_gas.cpp;
+ * ideal gas = B 0). Values are non-dimensional, as the reference holds them
+ * after UnitHandler (unit_handler.cpp:33-56). safe selects StiffenedGasSafe. */
+typedef struct {
+  double gamma;
+  double background_pressure;
+  int safe;
+} alp_material;
+
+/* Library version string and the message of the last failing call (per thread). */
+const char *alp_version(void);
+const char *alp_last_error(void);
+
+/* Fills *s with the reference's default-like selection: FiniteVolume,
+ * Characteristic, WENO5, HLLC, Einfeldt, Roe, RK3, FP64. */
+void alp_scheme_default(alp_scheme *s);
+
+/* ---- stateless drop-in calls --------------------------------------------- */
+
+/* Replaces ConvectiveTermSolver<D>::UpdateConvectiveFluxes
+ * (solvers/convective_term_contributions/convective_term_solver.h:67-81) for nb
+ * blocks at once: fluxes of the average buffer d_blocks (halos filled) are
+ * ADDED to the caller-zeroed reference arrays d_fx/d_fy/d_fz, each
+ * [nb][NE][ICX+1][ICY+1][ICZ+1]; d_fy / d_fz are ignored below 2 / 3 dims.
+ * cell_size as in the reference call. */
+int alp_convective_fluxes(int dim, const alp_scheme *scheme, const alp_material *mat,
+                          const double *d_blocks, int nb, double cell_size,
+                          double *d_fx, double *d_fy, double *d_fz, alp_stream_t stream);
+
+/* Bytes of scratch alp_space_rhs needs for nb blocks. */
+size_t alp_space_rhs_workspace_size(int dim, int nb);
+
+/* Replaces SpaceSolver::UpdateFluxes (solvers/space_solver.cpp:50-184) for
+ * single-phase blocks without source terms: d_rhs (reference layout) is zeroed
+ * and its interior set to the consistency-managed flux divergence / cell_size
+ * (space_solver.cpp:131-153). d_workspace: alp_space_rhs_workspace_size bytes. */
+int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
+                  const double *d_blocks, int nb, double cell_size, double *d_rhs,
+                  void *d_workspace, size_t workspace_bytes, alp_stream_t stream);
+
+/* Replaces PrimeStateHandler::ConvertConservativesToPrimeStates over every
+ * cell (prime_states/prime_state_handler.h:141-152): d_primes [nb][NE][cells]
+ * in the order Density, Pressure, VelocityX[, Y[, Z]]. */
+int alp_prime_states(int dim, const alp_material *mat, const double *d_blocks, int nb,
+                     double *d_primes, alp_stream_t stream);
+
+/* Replaces the same-level part of HaloManager::MaterialHaloUpdate
+ * (halo_manager.cpp:59-124, internal_halo_manager.cpp:439-459): d_nbr26
+ * [nb][26] holds the neighbour block of each of the 26 directions (offsets
+ * (ox,oy,oz) in {-1,0,1}^3 without the centre, x slowest) or -1 for a
+ * zero-gradient domain face. mode ALP_HALO_ALL: all 26 regions then the
+ * reference's full zero-gradient slabs; ALP_HALO_FACES: only the 2*dim face
+ * regions over the interior extent (all a dimension-split scheme reads). */
+enum { ALP_HALO_ALL = 0, ALP_HALO_FACES = 1 };
+int alp_halo_update(int dim, double *d_blocks, int nb, int nfields, const int *d_nbr26,
+                    int mode, alp_stream_t stream);
+
+/* Replaces ModularAlgorithmAssembler::ComputeTimestepSize
+ * (modular_algorithm_assembler.cpp:1777-1997) for one material on one level:
+ * *h_dt = min(CFL / (max_cells sum_d(|u_d| + c) / cell_size), t_end - t).
+ * d_workspace: 8 bytes of device scratch for the reduction. Synchronises
+ * the stream. */
+int alp_timestep_size(int dim, const alp_material *mat, const double *d_blocks, int nb,
+                      double cell_size, double cfl, double t, double t_end, double *h_dt,
+                      void *d_workspace, alp_stream_t stream);
+
+/* One RungeKutta3TVD stage on the interiors (time_integrator.h:98-113,
+ * 369-457; runge_kutta_3_TVD.h:41-59): stage 0 saves d_blocks to d_initial,
+ * then d_blocks = a0*d_blocks + a1*d_initial + c*dt*d_rhs. */
+int alp_rk3_stage(int dim, double *d_blocks, double *d_initial, const double *d_rhs, int nb,
+                  int stage, double dt, alp_stream_t stream);
+
+/* ---- engine: device-resident cases, fused step, CUDA graphs ------------- */
+
+typedef struct alp_engine alp_engine;
+
+/* Creates an engine for one dimension and scheme with room for
+ * capacity_blocks blocks and max_cases cases. All device memory is
+ * allocated here. */
+int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
+                      alp_engine **out);
+int alp_engine_destroy(alp_engine *e);
+
+/* Device bytes an engine of this size allocates. */
+size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases);
+
+/* Adds a case: nb blocks of one cell size and material. h_nbr26 [nb][26]
+ * gives neighbours as case-local block indices (-1 = zero-gradient domain
+ * face). h_blocks [nb][NE][cells]: only the interiors are read; halos are
+ * filled on the device. The case runs until t_end or max_steps (<= 0: no
+ * limit). Returns the case id in *case_id. Copies from host memory on the
+ * engine stream; h_blocks may be reused once the call returns. */
+int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size, double cfl,
+                        double t0, double t_end, int max_steps, int nb, const int *h_nbr26,
+                        const double *h_blocks, int *case_id);
+
+/* Removes a case and frees its blocks. */
+int alp_engine_remove_case(alp_engine *e, int case_id);
+
+/* Advances every active case by n steps (each: dt reduction, three RK3
+ * stages of flux / divergence+stage update / halo). Cases whose time reached
+ * t_end or whose step budget is spent do no work. Asynchronous. */
+int alp_engine_step(alp_engine *e, int n);
+
+/* Copies a case's state (reference layout, halos included) to h_blocks and
+ * its time / step count. Synchronises the engine stream. Any of the outputs
+ * may be null. */
+int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t, int *steps);
+
+/* True (1) when every case is done; synchronises. */
+int alp_engine_all_done(alp_engine *e, int *done);
+
+/* Engine stream, for callers that order their own work after the engine. */
+alp_stream_t alp_engine_stream(alp_engine *e);
+
+/* Enables (1) or disables (0) CUDA-graph replay of the step (default on). */
+int alp_engine_set_graph(alp_engine *e, int enabled);
+
+/* Number of kernel launches one engine step issues. */
+int alp_engine_launches_per_step(alp_engine *e);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -92,7 +92,7 @@ class Restatement(_Common):
                                              C.c_double, C.c_int, C.c_double, _D, _D, _D, _D, C.c_int]
             lib.oracle_timestep.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int,
                                             C.c_double, C.c_double, C.c_double, C.c_double, _D]
-            lib.oracle_halo_fill.argtypes = [C.c_int, _D, C.c_int, C.c_int, _I, C.c_int]
+            lib.oracle_halo_fill.argtypes = [C.c_int, _D, C.c_int, C.c_int, _I, C.c_int, C.c_int]
             lib.oracle_halo_update.argtypes = [C.c_int, _D, C.c_int, _I]
             lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
                                        C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
@@ -146,12 +146,13 @@ class Restatement(_Common):
                                  t, t_end, C.byref(dt))
         return dt.value
 
-    def halo_fill(self, u, nbr26, faces_only=False):
-        """In-place same-level halo copy over 26 (or 2*dim face) regions."""
+    def halo_fill(self, u, nbr26, faces_only=False, zero_gradient=False):
+        """In-place same-level halo copy over 26 (or 2*dim face) regions, then
+        optionally the zero-gradient slabs of domain faces."""
         assert u.dtype == np.float64 and u.flags.c_contiguous
         nbr26 = np.ascontiguousarray(nbr26, dtype=np.int32)
         self.lib.oracle_halo_fill(self.dim, _dp(u), u.shape[0], u.shape[1], _ip(nbr26),
-                                  int(faces_only))
+                                  int(faces_only), int(zero_gradient))
         return u
 
     def halo_update(self, u, nbr):

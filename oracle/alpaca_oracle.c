@@ -800,15 +800,48 @@ int oracle_timestep(int dim, const double *u, int nb, double gamma, double B,
   return 0;
 }
 
+/* Zero-gradient slabs of the domain faces (boundary_constants.h:103-160,
+ * 211-252): the full TCY x TCZ (etc.) halo slab takes the first / last
+ * interior plane. A face is a domain face when face_nbr(b, face) < 0. */
+static void zero_gradient_slabs(const Geom *g, double *u, int nb, int nfields,
+                                const int *nbr, int nbr_stride, const int *face_slot) {
+  for (int b = 0; b < nb; ++b)
+    for (int face = 0; face < 2 * g->dim; ++face) {
+      if (nbr[(long)nbr_stride * b + face_slot[face]] >= 0) continue;
+      int const dir = face / 2, high = face % 2;
+      int const s = high ? HS + IC - 1 : HS;
+      int const h0 = high ? HS + IC : 0, h1 = high ? TC : HS;
+      for (int f = 0; f < nfields; ++f) {
+        double *x = u + ((long)b * nfields + f) * g->cells;
+        for (int i = 0; i < g->tc[0]; ++i)
+          for (int j = 0; j < g->tc[1]; ++j)
+            for (int k = 0; k < g->tc[2]; ++k) {
+              int const idx[3] = {i, j, k};
+              if (idx[dir] < h0 || idx[dir] >= h1) continue;
+              int si = i, sj = j, sk = k;
+              if (dir == 0) si = s;
+              if (dir == 1) sj = s;
+              if (dir == 2) sk = s;
+              x[cidx(g, i, j, k)] = x[cidx(g, si, sj, sk)];
+            }
+      }
+    }
+}
+
+/* slot of face W,E,S,N,B,T in the 26-entry table */
+static const int face_slot26[6] = {4, 21, 10, 15, 12, 13};
+static const int face_slot6[6] = {0, 1, 2, 3, 4, 5};
+
 /* Same-level halo copy. nbr26 holds 26 neighbour indices per block (-1: none),
  * ordered by direction offsets (ox, oy, oz) in {-1,0,1}^3 \ {0} with ox slowest:
  * index = (ox+1)*9 + (oy+1)*3 + (oz+1), minus one past the centre (13). The
  * region for offset +1 is [HS+IC, TC) filled from the neighbour's [HS, 2HS),
  * for -1 it is [0, HS) from the neighbour's [IC, IC+HS), for 0 the interior
  * (communication_types.h:45-132; internal_halo_manager.cpp:439-459).
- * faces_only copies only the 2*dim planes. */
+ * faces_only copies only the 2*dim planes; zero_gradient then applies the
+ * domain-face slabs, external after internal as in halo_manager.cpp:87-124. */
 int oracle_halo_fill(int dim, double *u, int nb, int nfields, const int *nbr26,
-                     int faces_only) {
+                     int faces_only, int zero_gradient) {
   Geom g = make_geom(dim);
   for (int b = 0; b < nb; ++b) {
     for (int o = 0; o < 27; ++o) {
@@ -846,6 +879,7 @@ int oracle_halo_fill(int dim, double *u, int nb, int nfields, const int *nbr26,
       }
     }
   }
+  if (zero_gradient) zero_gradient_slabs(&g, u, nb, nfields, nbr26, 26, face_slot26);
   return 0;
 }
 
@@ -878,27 +912,7 @@ static void halo_update6(const Geom *g, double *u, int nb, const int *nbr) {
                   s[cidx(g, src[0] + i, src[1] + j, src[2] + k)];
       }
     }
-  for (int b = 0; b < nb; ++b)
-    for (int face = 0; face < 2 * g->dim; ++face) {
-      if (nbr[6 * b + face] >= 0) continue;
-      int const dir = face / 2, high = face % 2;
-      int const s = high ? HS + IC - 1 : HS;
-      int const h0 = high ? HS + IC : 0, h1 = high ? TC : HS;
-      for (int f = 0; f < ne; ++f) {
-        double *x = u + ((long)b * ne + f) * g->cells;
-        for (int i = 0; i < g->tc[0]; ++i)
-          for (int j = 0; j < g->tc[1]; ++j)
-            for (int k = 0; k < g->tc[2]; ++k) {
-              int const idx[3] = {i, j, k};
-              if (idx[dir] < h0 || idx[dir] >= h1) continue;
-              int si = i, sj = j, sk = k;
-              if (dir == 0) si = s;
-              if (dir == 1) sj = s;
-              if (dir == 2) sk = s;
-              x[cidx(g, i, j, k)] = x[cidx(g, si, sj, sk)];
-            }
-      }
-    }
+  zero_gradient_slabs(g, u, nb, ne, nbr, 6, face_slot6);
 }
 
 int oracle_halo_update(int dim, double *u, int nb, const int *nbr) {

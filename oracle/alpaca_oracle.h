@@ -48,7 +48,7 @@ int oracle_timestep(int dim, const double *u, int nb, double gamma, double B,
                     double t_end, double *dt);
 
 int oracle_halo_fill(int dim, double *u, int nb, int nfields, const int *nbr26,
-                     int faces_only);
+                     int faces_only, int zero_gradient);
 
 /* six-face halo copy (W,E,S,N,B,T neighbour table, -1 = domain face) followed
  * by zero-gradient slabs on domain faces */

@@ -1,0 +1,62 @@
+"""The C-ABI library without a GPU: it loads, exports every function the
+header declares, and rejects bad arguments before touching the device."""
+import ctypes as C
+
+import pytest
+
+from alpaca_b200 import native as N
+
+
+def test_library_exports_every_declared_symbol():
+    lib = N.lib()
+    declared = N.declared_symbols()
+    assert len(declared) >= 20
+    missing = [s for s in declared if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_version_and_default_scheme():
+    assert b"sm_100a" in N.lib().alp_version()
+    s = N.Scheme()
+    N.lib().alp_scheme_default(C.byref(s))
+    assert (s.convective_term_solver, s.state_reconstruction, s.reconstruction_stencil,
+            s.riemann_solver, s.signal_speed, s.flux_splitting, s.time_integrator,
+            s.precision) == (N.FINITE_VOLUME, N.RECON_CHARACTERISTIC, N.STENCIL_WENO5,
+                             N.RIEMANN_HLLC, N.SIGNAL_SPEED_EINFELDT, N.FLUX_SPLITTING_ROE,
+                             N.RK3, N.FP64)
+
+
+def test_invalid_arguments_are_rejected_without_gpu():
+    lib = N.lib()
+    mat = N.Material.make(1.4)
+    sch = N.Scheme.make("fvchar")
+    null = C.c_void_p(0)
+    rc = lib.alp_convective_fluxes(4, C.byref(sch), C.byref(mat), null, 1, 0.1, null, null, null, null)
+    assert rc == N.ALP_ERR_INVALID and b"dim" in lib.alp_last_error()
+    bad = N.Scheme.make("fvchar")
+    bad.reconstruction_stencil = 0  # FirstOrder is not compiled
+    rc = lib.alp_convective_fluxes(3, C.byref(bad), C.byref(mat), null, 1, 0.1, null, null, null, null)
+    assert rc == N.ALP_ERR_INVALID and b"WENO5" in lib.alp_last_error()
+    cons = N.Scheme.make("fvchar")
+    cons.state_reconstruction = N.RECON_CONSERVATIVE
+    rc = lib.alp_convective_fluxes(3, C.byref(cons), C.byref(mat), null, 1, 0.1, null, null, null, null)
+    assert rc == N.ALP_ERR_INVALID
+    badmat = N.Material.make(1.0)
+    rc = lib.alp_convective_fluxes(3, C.byref(sch), C.byref(badmat), null, 1, 0.1, null, null, null, null)
+    assert rc == N.ALP_ERR_INVALID and b"gamma" in lib.alp_last_error()
+    rc = lib.alp_rk3_stage(3, null, null, null, 1, 3, 0.1, null)
+    assert rc == N.ALP_ERR_INVALID
+    rc = lib.alp_halo_update(3, null, 1, 5, null, 7, null)
+    assert rc == N.ALP_ERR_INVALID
+    h = C.c_void_p()
+    assert lib.alp_engine_create(3, C.byref(sch), 0, 1, C.byref(h)) == N.ALP_ERR_INVALID
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_workspace_and_engine_sizes(dim):
+    lib = N.lib()
+    faces = 17 * (17 if dim > 1 else 2) * (17 if dim > 2 else 2)
+    assert lib.alp_space_rhs_workspace_size(dim, 7) == 7 * dim * (dim + 2) * faces * 8
+    cells = 24 ** dim
+    per_block = 2 * (dim + 2) * cells * 8 + dim * (dim + 2) * faces * 8
+    assert lib.alp_engine_bytes(dim, 10, 2) >= 10 * per_block

@@ -1,0 +1,277 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle and with the
+golden fixtures generated from the reference itself.
+
+Tolerances (FP64 form):
+  * one right-hand-side evaluation: per field, max|gpu - ref| / max|ref| <= 1e-12
+  * after a time loop: per field, sum|gpu - ref| / sum|ref| <= 1e-10 (L1)
+The only arithmetic difference from the reference is FMA contraction on the GPU.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from alpaca_b200 import api, cases
+from alpaca_b200 import native as N
+from helpers import field_rel_err, filled, l1_rel, small_cases
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+RHS_TOL = 1e-12
+RUN_TOL = 1e-10
+VARIANTS = list(oracle.VARIANTS)
+
+
+def to_dev(a, dev):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+
+
+def l1_per_field(a, b):
+    return max(l1_rel(a[:, f], b[:, f]) for f in range(a.shape[1]))
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_convective_fluxes_and_rhs(cuda, dim, variant):
+    case = small_cases()[dim]
+    u = filled(case)
+    h = case.grid.cell_size
+    mat = N.Material.make(case.gamma)
+    fx, fy, fz, rhs = oracle.Restatement(dim, variant).space_rhs(u, case.gamma, 0.0, False, h)
+    ud = to_dev(u, cuda)
+    f = api.convective_fluxes(ud, dim, variant, mat, h)
+    for d, ref in enumerate((fx, fy, fz)[:dim]):
+        err = field_rel_err(f[d].cpu().numpy(), ref)
+        assert err.max() <= RHS_TOL, (d, err)
+    r = api.space_rhs(ud, dim, variant, mat, h).cpu().numpy()
+    I = cases.interior(dim)
+    assert field_rel_err(r[I], rhs[I]).max() <= RHS_TOL
+    # halos of the RHS buffer are zero as after SpaceSolver's zeroing
+    mask = np.ones(r.shape, bool)
+    mask[I] = False
+    assert not r[mask].any()
+    # the reference's own output (golden fixture)
+    z = np.load(os.path.join(GOLDEN, f"rhs_d{dim}_{variant}.npz"))
+    assert field_rel_err(r[I], z["rhs"]).max() <= RHS_TOL
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+@pytest.mark.parametrize("safe", [False, True])
+def test_stiffened_gas_rhs(cuda, variant, safe):
+    case = cases.fourier_shock(1, dim=3, seed=11, gamma=6.12, B=3000.0)
+    u = filled(case)
+    h = case.grid.cell_size
+    rhs = oracle.Restatement(3, variant).space_rhs(u, 6.12, 3000.0, safe, h)[3]
+    r = api.space_rhs(to_dev(u, cuda), 3, variant, N.Material.make(6.12, 3000.0, safe), h)
+    I = cases.interior(3)
+    assert field_rel_err(r.cpu().numpy()[I], rhs[I]).max() <= RHS_TOL
+
+
+def test_accumulate_contract(cuda):
+    """UpdateConvectiveFluxes adds to the caller's arrays (convective_term_solver.h:67-81)."""
+    case = small_cases()[2]
+    ud = to_dev(filled(case), cuda)
+    mat = N.Material.make(1.4)
+    f1 = api.convective_fluxes(ud, 2, "fvchar", mat, case.grid.cell_size)
+    import ctypes as C
+    sch = N.Scheme.make("fvchar")
+    N.check(N.lib().alp_convective_fluxes(2, C.byref(sch), C.byref(mat), api._ptr(ud), case.grid.nb,
+                                          case.grid.cell_size, api._ptr(f1[0]), api._ptr(f1[1]),
+                                          C.c_void_p(0), api._stream()))
+    f2 = api.convective_fluxes(ud, 2, "fvchar", mat, case.grid.cell_size)
+    assert np.array_equal(f1[0].cpu().numpy(), 2 * f2[0].cpu().numpy())
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_prime_states(cuda, dim):
+    case = small_cases()[dim]
+    u = filled(case)
+    p = api.prime_states(to_dev(u, cuda), dim, N.Material.make(case.gamma)).cpu().numpy()
+    ref = oracle.Restatement(dim).prime_states(u, case.gamma)
+    assert field_rel_err(p, ref).max() <= 1e-15
+
+
+def test_halo_known_answer(cuda):
+    """test_internal_halo_manager.cpp:76-140 through alp_halo_update (26 regions)."""
+    g = cases.BlockGrid(3, (2, 2, 2), (False, False, False), 1.0 / 32)
+    u = np.zeros((g.nb, 1) + cases.block_shape(3))
+    for b in range(g.nb):
+        u[b] = b
+    ud = to_dev(u, cuda)
+    api.halo_update(ud, 3, to_dev(g.nbr26, cuda), N.HALO_ALL)
+    got = ud.cpu().numpy()
+    for b in range(g.nb):
+        for s in range(26):
+            n = g.nbr26[b, s]
+            if n < 0:
+                continue
+            o = s if s < 13 else s + 1
+            off = (o // 9 - 1, (o // 3) % 3 - 1, o % 3 - 1)
+            sl = tuple(slice(20, 24) if x > 0 else slice(0, 4) if x < 0 else slice(4, 20)
+                       for x in off)
+            assert np.all(got[(b, 0) + sl] == n)
+    # every cell, domain sides included, as the oracle's 26 regions + zero-gradient slabs
+    ref = u.copy()
+    oracle.Restatement(3).halo_fill(ref, g.nbr26, zero_gradient=True)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_face_halo_update_matches_oracle(cuda, dim):
+    case = small_cases()[dim]
+    u = np.ascontiguousarray(case.u.copy())
+    ud = to_dev(u, cuda)
+    api.halo_update(ud, dim, to_dev(case.grid.nbr26, cuda), N.HALO_FACES)
+    ref = u.copy()
+    oracle.Restatement(dim).halo_update(ref, case.grid.nbr)
+    got = ud.cpu().numpy()
+    # compare interiors and the face slabs over the interior extent
+    for f in range(2 * dim):
+        d, hi = f // 2, f % 2
+        sl = [slice(4, 20) if x < dim else slice(0, 1) for x in range(3)]
+        sl[d] = slice(20, 24) if hi else slice(0, 4)
+        idx = (slice(None), slice(None)) + tuple(sl)
+        assert np.array_equal(got[idx], ref[idx]), f
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_timestep_size(cuda, dim):
+    case = small_cases()[dim]
+    u = filled(case)
+    mat = N.Material.make(case.gamma)
+    dt = api.timestep_size(to_dev(u, cuda), dim, mat, case.grid.cell_size, 0.6)
+    ref = oracle.Restatement(dim).timestep(u, case.gamma, 0.0, False, case.grid.cell_size, 0.6)
+    assert abs(dt - ref) <= 1e-15 * ref
+    # end-time clip (modular_algorithm_assembler.cpp:1971-1982)
+    dt2 = api.timestep_size(to_dev(u, cuda), dim, mat, case.grid.cell_size, 0.6, t=1.0,
+                            t_end=1.0 + ref / 3)
+    assert abs(dt2 - ref / 3) <= 1e-15
+
+
+def test_rk3_stage_from_rhs(cuda):
+    """TimeIntegrator stage on an oracle RHS buffer."""
+    import torch
+    case = small_cases()[3]
+    u = filled(case)
+    rhs = oracle.Restatement(3).space_rhs(u, 1.4, 0.0, False, case.grid.cell_size)[3]
+    ud, u0 = to_dev(u, cuda), torch.zeros(u.shape, dtype=torch.float64, device=cuda)
+    rd = to_dev(rhs, cuda)
+    api.rk3_stage(ud, u0, rd, 3, 0, 1e-3)
+    I = cases.interior(3)
+    exp = u + 1e-3 * rhs
+    assert np.allclose(ud.cpu().numpy()[I], exp[I], rtol=1e-15, atol=1e-15)
+    assert np.array_equal(u0.cpu().numpy()[I], u[I])
+    api.rk3_stage(ud, u0, rd, 3, 1, 1e-3)
+    exp2 = 0.25 * exp + 0.75 * u + 0.25 * 1e-3 * rhs
+    assert np.allclose(ud.cpu().numpy()[I], exp2[I], rtol=1e-15, atol=1e-15)
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_engine_sod_to_end_time(cuda, variant):
+    """Config 1: 1D Sod, 8 x 16 cells, WENO5 + SSP-RK3, CFL 0.6, t_end 0.2."""
+    z = np.load(os.path.join(GOLDEN, f"sod1d_{variant}.npz"))
+    case = cases.sod_1d()
+    eng = api.Engine(1, variant, capacity_blocks=16, max_cases=2)
+    cid = eng.add_case(case)
+    eng.run_to_end(chunk=8)
+    u, t, steps = eng.get(cid)
+    eng.close()
+    assert steps == int(z["steps"])
+    assert abs(t - float(z["t"])) <= 1e-15
+    I = cases.interior(1)
+    assert l1_per_field(u[I], z["final"]) <= RUN_TOL
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_engine_short_run_vs_reference(cuda, dim, variant):
+    z = np.load(os.path.join(GOLDEN, f"run5_d{dim}_{variant}.npz"))
+    case = small_cases()[dim]
+    eng = api.Engine(dim, variant, capacity_blocks=8, max_cases=2)
+    cid = eng.add_case(case, max_steps=5)
+    eng.run_to_end(chunk=5)
+    u, t, steps = eng.get(cid)
+    eng.close()
+    assert steps == 5 and abs(t - float(z["t"])) <= 1e-13 * t
+    I = cases.interior(dim)
+    assert field_rel_err(u[I], z["final"]).max() <= RHS_TOL * 10
+    assert l1_per_field(u[I], z["final"]) <= RUN_TOL
+
+
+@pytest.mark.parametrize("variant", ["fvchar", "fsroe"])
+def test_engine_100_steps_vs_oracle(cuda, variant):
+    """100 SSP-RK3 steps of a 2x2x2-block periodic Fourier + Mach-2 case."""
+    case = cases.fourier_shock(2, dim=3, seed=7)
+    ref, t_ref, n_ref, _ = oracle.Restatement(3, variant).run(
+        case.u, case.grid.nbr, case.gamma, 0.0, False, case.grid.cell_size, case.cfl, 1e300,
+        max_steps=100, nthreads=os.cpu_count() or 1)
+    eng = api.Engine(3, variant, capacity_blocks=8, max_cases=1)
+    cid = eng.add_case(case, max_steps=100)
+    eng.run_to_end(chunk=25)
+    u, t, steps = eng.get(cid)
+    eng.close()
+    assert steps == n_ref == 100
+    assert abs(t - t_ref) <= 1e-12 * t_ref
+    I = cases.interior(3)
+    assert l1_per_field(u[I], ref[I]) <= RUN_TOL
+
+
+def test_engine_mix_equals_alone(cuda):
+    """Cases sharing an engine give the same bits as each case alone."""
+    a = cases.fourier_shock(2, dim=3, seed=21, steps=7)
+    b = cases.fourier_shock(1, dim=3, seed=22, steps=4)
+    out = {}
+    for name, group in (("alone_a", [a]), ("alone_b", [b]), ("mix", [a, b])):
+        eng = api.Engine(3, "fvchar", capacity_blocks=16, max_cases=4)
+        ids = [eng.add_case(c) for c in group]
+        eng.run_to_end(chunk=4)
+        out[name] = [eng.get(i) for i in ids]
+        eng.close()
+    assert np.array_equal(out["mix"][0][0], out["alone_a"][0][0])
+    assert np.array_equal(out["mix"][1][0], out["alone_b"][0][0])
+    assert out["mix"][0][2] == 7 and out["mix"][1][2] == 4
+
+
+def test_engine_graph_equals_eager(cuda):
+    c = cases.fourier_shock(1, dim=3, seed=5, steps=3)
+    res = []
+    for graph in (True, False):
+        eng = api.Engine(3, "fvprim", capacity_blocks=2, max_cases=1, graph=graph)
+        cid = eng.add_case(c)
+        eng.run_to_end(chunk=3)
+        res.append(eng.get(cid)[0])
+        eng.close()
+    assert np.array_equal(res[0], res[1])
+
+
+def test_engine_numeric_fault_is_reported(cuda):
+    """A negative density stops the case and is reported through the status
+    word (ALP_ERR_NUMERIC), without a device fault."""
+    c = cases.fourier_shock(1, dim=3, seed=5, steps=3)
+    c.u[0, 0, 10, 10, 10] = -1.0
+    eng = api.Engine(3, "fvchar", capacity_blocks=2, max_cases=1)
+    cid = eng.add_case(c)
+    eng.step(2)
+    with pytest.raises(N.AlpacaError) as e:
+        eng.get(cid)
+    assert e.value.code == N.ALP_ERR_NUMERIC
+    assert eng.all_done()
+    eng.close()
+
+
+def test_engine_capacity_and_removal(cuda):
+    c = cases.fourier_shock(1, dim=3, seed=5, steps=1)
+    eng = api.Engine(3, "fvchar", capacity_blocks=2, max_cases=4)
+    i0 = eng.add_case(c)
+    i1 = eng.add_case(c)
+    with pytest.raises(N.AlpacaError) as e:
+        eng.add_case(c)
+    assert e.value.code == N.ALP_ERR_CAPACITY
+    eng.remove_case(i0)
+    i2 = eng.add_case(c)
+    eng.run_to_end()
+    assert np.array_equal(eng.get(i1)[0], eng.get(i2)[0])
+    eng.close()

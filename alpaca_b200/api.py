@@ -29,7 +29,7 @@ def flux_shape(dim: int, nb: int):
 
 
 def convective_fluxes(u, dim: int, variant: str, material: N.Material, cell_size: float,
-                      precision: int = N.FP64, stream=None):
+                      precision: int = N.FP64, stream=None, strict: bool = False):
     """ConvectiveTermSolver::UpdateConvectiveFluxes on nb blocks (device tensor
     [nb, ne, TCX, TCY, TCZ] float64). Returns zero-initialised flux arrays with
     the fluxes added, in the reference layout."""
@@ -39,25 +39,26 @@ def convective_fluxes(u, dim: int, variant: str, material: N.Material, cell_size
     f = [torch.zeros(shp, dtype=torch.float64, device=u.device) if d < dim else None
          for d in range(3)]
     sch = N.Scheme.make(variant, precision)
-    N.check(N.lib().alp_convective_fluxes(dim, C.byref(sch), C.byref(material), _ptr(u), nb,
-                                          cell_size, _ptr(f[0]), _ptr(f[1]), _ptr(f[2]),
-                                          _stream(stream)))
+    N.check(N.lib(strict).alp_convective_fluxes(dim, C.byref(sch), C.byref(material), _ptr(u), nb,
+                                                cell_size, _ptr(f[0]), _ptr(f[1]), _ptr(f[2]),
+                                                _stream(stream)), strict)
     return f
 
 
 def space_rhs(u, dim: int, variant: str, material: N.Material, cell_size: float,
-              precision: int = N.FP64, stream=None, workspace=None):
+              precision: int = N.FP64, stream=None, workspace=None, strict: bool = False):
     """SpaceSolver::UpdateFluxes right-hand side (reference layout)."""
     import torch
     nb = u.shape[0]
     rhs = torch.empty_like(u)
-    nbytes = N.lib().alp_space_rhs_workspace_size(dim, nb)
+    lib = N.lib(strict)
+    nbytes = lib.alp_space_rhs_workspace_size(dim, nb)
     if workspace is None:
         workspace = torch.empty(max(nbytes // 8, 1), dtype=torch.float64, device=u.device)
     sch = N.Scheme.make(variant, precision)
-    N.check(N.lib().alp_space_rhs(dim, C.byref(sch), C.byref(material), _ptr(u), nb, cell_size,
-                                  _ptr(rhs), _ptr(workspace), workspace.numel() * 8,
-                                  _stream(stream)))
+    N.check(lib.alp_space_rhs(dim, C.byref(sch), C.byref(material), _ptr(u), nb, cell_size,
+                              _ptr(rhs), _ptr(workspace), workspace.numel() * 8,
+                              _stream(stream)), strict)
     return rhs
 
 
@@ -96,22 +97,28 @@ class Engine:
     """Device-resident cases advanced by the fused step (alp_engine_*)."""
 
     def __init__(self, dim: int, variant: str = "fvchar", precision: int = N.FP64,
-                 capacity_blocks: int = 1024, max_cases: int = 64, graph: bool = True):
+                 capacity_blocks: int = 1024, max_cases: int = 64, graph: bool = True,
+                 strict: bool = False):
         self.dim = dim
         self.ne = dim + 2
         self.variant = variant
+        self.strict = strict
+        self.lib = N.lib(strict)
         sch = N.Scheme.make(variant, precision)
         h = C.c_void_p()
-        N.check(N.lib().alp_engine_create(dim, C.byref(sch), capacity_blocks, max_cases,
-                                          C.byref(h)))
+        self._check(self.lib.alp_engine_create(dim, C.byref(sch), capacity_blocks, max_cases,
+                                               C.byref(h)))
         self.h = h
         self.nb = {}
         if not graph:
-            N.check(N.lib().alp_engine_set_graph(self.h, 0))
+            self._check(self.lib.alp_engine_set_graph(self.h, 0))
+
+    def _check(self, rc):
+        N.check(rc, self.strict)
 
     def close(self):
-        if self.h:
-            N.lib().alp_engine_destroy(self.h)
+        if getattr(self, "h", None):
+            self.lib.alp_engine_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -127,7 +134,7 @@ class Engine:
         mat = N.Material.make(case.gamma, case.B, False)
         cid = C.c_int()
         steps = case.steps if max_steps is None else max_steps
-        N.check(N.lib().alp_engine_add_case(
+        self._check(self.lib.alp_engine_add_case(
             self.h, C.byref(mat), g.cell_size, case.cfl, t0, case.t_end, steps, g.nb,
             nbr.ctypes.data_as(C.POINTER(C.c_int)), u.ctypes.data_as(C.POINTER(C.c_double)),
             C.byref(cid)))
@@ -135,24 +142,25 @@ class Engine:
         return cid.value
 
     def remove_case(self, cid: int):
-        N.check(N.lib().alp_engine_remove_case(self.h, cid))
+        self._check(self.lib.alp_engine_remove_case(self.h, cid))
         self.nb.pop(cid, None)
 
     def step(self, n: int = 1):
-        N.check(N.lib().alp_engine_step(self.h, n))
+        self._check(self.lib.alp_engine_step(self.h, n))
 
     def get(self, cid: int):
         nb, shp = self.nb[cid]
         out = np.empty(shp, dtype=np.float64)
         t = C.c_double()
         steps = C.c_int()
-        N.check(N.lib().alp_engine_get_case(self.h, cid, out.ctypes.data_as(C.POINTER(C.c_double)),
-                                            C.byref(t), C.byref(steps)))
+        self._check(self.lib.alp_engine_get_case(self.h, cid,
+                                                 out.ctypes.data_as(C.POINTER(C.c_double)),
+                                                 C.byref(t), C.byref(steps)))
         return out, t.value, steps.value
 
     def all_done(self) -> bool:
         d = C.c_int()
-        N.check(N.lib().alp_engine_all_done(self.h, C.byref(d)))
+        self._check(self.lib.alp_engine_all_done(self.h, C.byref(d)))
         return bool(d.value)
 
     def run_to_end(self, chunk: int = 16, max_chunks: int = 1 << 20):
@@ -164,4 +172,8 @@ class Engine:
 
     @property
     def launches_per_step(self) -> int:
-        return N.lib().alp_engine_launches_per_step(self.h)
+        return self.lib.alp_engine_launches_per_step(self.h)
+
+    @property
+    def stream_handle(self) -> int:
+        return self.lib.alp_engine_stream(self.h)

@@ -9,6 +9,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libalpaca_b200.so")
 PROBE_LIB = os.path.join(HERE, "libalpaca_b200_probe.so")
+# Same sources without FMA contraction: every multiply and add is rounded on
+# its own, as in the reference's x86-64 build. Tests use it to show that the
+# CUDA arithmetic follows the reference's operation order bit for bit.
+STRICT_LIB = os.path.join(HERE, "libalpaca_b200_strict.so")
 SOURCES = ["kernels.cu", "capi.cu"]
 PROBE_SOURCES = ["probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -35,8 +39,8 @@ def stale() -> bool:
     return os.path.getmtime(hdr) > t
 
 
-def _nvcc(out: str, sources: list[str], verbose: bool) -> None:
-    cmd = [nvcc()] + ARCH + FLAGS + ["-o", out] + [os.path.join(CSRC, s) for s in sources]
+def _nvcc(out: str, sources: list[str], verbose: bool, extra=()) -> None:
+    cmd = [nvcc()] + ARCH + FLAGS + list(extra) + ["-o", out] + [os.path.join(CSRC, s) for s in sources]
     if verbose:
         print(" ".join(cmd))
     r = subprocess.run(cmd, capture_output=True, text=True)
@@ -45,8 +49,9 @@ def _nvcc(out: str, sources: list[str], verbose: bool) -> None:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    if force or stale() or not os.path.exists(PROBE_LIB):
+    if force or stale() or not os.path.exists(PROBE_LIB) or not os.path.exists(STRICT_LIB):
         _nvcc(LIB, SOURCES, verbose)
+        _nvcc(STRICT_LIB, SOURCES, verbose, ["-fmad=false"])
         _nvcc(PROBE_LIB, PROBE_SOURCES, verbose)
     return LIB
 

@@ -434,7 +434,10 @@ halo_region_kernel(double *__restrict__ U, int const *__restrict__ work,
 // Zero-gradient halos of domain faces (boundary_constants.h:103-160, 211-252):
 // the halo takes the value of the first / last interior plane. With
 // faces_only the copy covers the interior extent of the face, otherwise the
-// reference's full TC x TC slab.
+// reference's full TC x TC slab. The faces of one block are applied one after
+// the other in x, y, z order (CommunicationManager::NeighborsOfNode lists
+// domain sides East, West, North, South, Top, Bottom), which fixes the values
+// the overlapping slabs leave in edge and corner halos.
 template <int DIM>
 __global__ void __launch_bounds__(256)
 zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
@@ -444,33 +447,35 @@ zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
   int const item = blockIdx.x;
   int const slot = slot_of(work, item);
   if (cases && meta && !(cases[meta[slot].case_id].dt > 0.0)) return;
-  int const face = blockIdx.y;
-  int const dir = face / 2, high = face & 1;
-  int off[3] = {0, 0, 0};
-  off[dir] = high ? 1 : -1;
-  int const o = (off[0] + 1) * 9 + (off[1] + 1) * 3 + (off[2] + 1);
-  if (nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)] >= 0) return;
-  int lo[3], ext[3];
-#pragma unroll
-  for (int d = 0; d < 3; ++d) {
-    lo[d] = faces_only ? G::fic(d) : 0;
-    ext[d] = faces_only ? G::ic(d) : G::tc(d);
-  }
-  lo[dir] = high ? HS + IC : 0;
-  ext[dir] = HS;
-  int const plane = high ? HS + IC - 1 : HS;
-  int const cells = ext[0] * ext[1] * ext[2];
   double *b = U + (size_t)slot * nfields * G::CELLS;
-  for (int x = threadIdx.x; x < cells * nfields; x += blockDim.x) {
-    int const f = x / cells;
-    int const r = x - f * cells;
-    int c[3];
-    c[2] = lo[2] + r % ext[2];
-    c[1] = lo[1] + (r / ext[2]) % ext[1];
-    c[0] = lo[0] + r / (ext[2] * ext[1]);
-    int s[3] = {c[0], c[1], c[2]};
-    s[dir] = plane;
-    b[f * G::CELLS + G::cell(c[0], c[1], c[2])] = b[f * G::CELLS + G::cell(s[0], s[1], s[2])];
+  for (int face = 0; face < 2 * DIM; ++face) {
+    int const dir = face / 2, high = face & 1;
+    int off[3] = {0, 0, 0};
+    off[dir] = high ? 1 : -1;
+    int const o = (off[0] + 1) * 9 + (off[1] + 1) * 3 + (off[2] + 1);
+    if (nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)] >= 0) continue;
+    int lo[3], ext[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = faces_only ? G::fic(d) : 0;
+      ext[d] = faces_only ? G::ic(d) : G::tc(d);
+    }
+    lo[dir] = high ? HS + IC : 0;
+    ext[dir] = HS;
+    int const plane = high ? HS + IC - 1 : HS;
+    int const cells = ext[0] * ext[1] * ext[2];
+    for (int x = threadIdx.x; x < cells * nfields; x += blockDim.x) {
+      int const f = x / cells;
+      int const r = x - f * cells;
+      int c[3];
+      c[2] = lo[2] + r % ext[2];
+      c[1] = lo[1] + (r / ext[2]) % ext[1];
+      c[0] = lo[0] + r / (ext[2] * ext[1]);
+      int s[3] = {c[0], c[1], c[2]};
+      s[dir] = plane;
+      b[f * G::CELLS + G::cell(c[0], c[1], c[2])] = b[f * G::CELLS + G::cell(s[0], s[1], s[2])];
+    }
+    __syncthreads();
   }
 }
 
@@ -698,7 +703,7 @@ cudaError_t launch_halo(Launch const &L, int const *nbr26, bool faces_only, int 
                         CaseState const *cases) {
   if (L.nwork <= 0) return cudaSuccess;
   int const regions = faces_only ? 2 * L.dim : 26;
-  dim3 g1(L.nwork, regions), g2(L.nwork, 2 * L.dim);
+  dim3 g1(L.nwork, regions), g2(L.nwork);
   int const fo = faces_only ? 1 : 0;
   switch (L.dim) {
     case 1:

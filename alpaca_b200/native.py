@@ -11,6 +11,7 @@ import re
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libalpaca_b200.so")
+STRICT_LIB_PATH = os.path.join(HERE, "libalpaca_b200_strict.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "alpaca_b200.h")
 
 ALP_OK, ALP_ERR_INVALID, ALP_ERR_CUDA, ALP_ERR_CAPACITY, ALP_ERR_NOT_FOUND, ALP_ERR_NUMERIC = range(6)
@@ -99,7 +100,7 @@ _SIGS = {
     "alp_engine_launches_per_step": (C.c_int, [_V]),
 }
 
-_lib = None
+_libs = {}
 
 
 def declared_symbols() -> list[str]:
@@ -108,21 +109,22 @@ def declared_symbols() -> list[str]:
     return sorted(set(re.findall(r"\b(alp_[a-z0-9_]+)\s*\(", text)))
 
 
-def lib() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            raise ImportError(f"{LIB_PATH} is missing: build it with "
+def lib(strict: bool = False) -> C.CDLL:
+    """The CUDA library; strict=True loads the build without FMA contraction."""
+    if strict not in _libs:
+        path = STRICT_LIB_PATH if strict else LIB_PATH
+        if not os.path.exists(path):
+            raise ImportError(f"{path} is missing: build it with "
                               "`python -c 'import __graft_entry__ as g; g.build()'`")
-        l = C.CDLL(LIB_PATH)
+        l = C.CDLL(path)
         for name, (res, args) in _SIGS.items():
             f = getattr(l, name)
             f.restype = res
             f.argtypes = args
-        _lib = l
-    return _lib
+        _libs[strict] = l
+    return _libs[strict]
 
 
-def check(rc: int) -> None:
+def check(rc: int, strict: bool = False) -> None:
     if rc != ALP_OK:
-        raise AlpacaError(rc, lib().alp_last_error().decode())
+        raise AlpacaError(rc, lib(strict).alp_last_error().decode())

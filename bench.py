@@ -221,7 +221,7 @@ def run_ours(args, ws, rank, local):
     case = cases.fourier_shock(nbd, dim=3, seed=1)
     cells = case.grid.nb * 4096
     eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
-    stream = torch.cuda.ExternalStream(N.lib().alp_engine_stream(eng.h))
+    stream = torch.cuda.ExternalStream(eng.stream_handle)
     cid = eng.add_case(case, max_steps=0)
     eng.step(args.warmup)
     torch.cuda.synchronize()
@@ -250,7 +250,7 @@ def run_ours(args, ws, rank, local):
                             case.t_end, 0)
         out = torch.empty_like(host).pin_memory()
         eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
-        stream = torch.cuda.ExternalStream(N.lib().alp_engine_stream(eng.h))
+        stream = torch.cuda.ExternalStream(eng.stream_handle)
         cid = eng.add_case(case_p, max_steps=0)
         eng.step(args.warmup)
         eng.remove_case(cid)

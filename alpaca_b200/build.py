@@ -51,7 +51,7 @@ def _nvcc(out: str, sources: list[str], verbose: bool, extra=()) -> None:
 def build(force: bool = False, verbose: bool = False) -> str:
     if force or stale() or not os.path.exists(PROBE_LIB) or not os.path.exists(STRICT_LIB):
         _nvcc(LIB, SOURCES, verbose)
-        _nvcc(STRICT_LIB, SOURCES, verbose, ["-fmad=false"])
+        _nvcc(STRICT_LIB, SOURCES, verbose, ["-fmad=false", "-DALP_STRICT"])
         _nvcc(PROBE_LIB, PROBE_SOURCES, verbose)
     return LIB
 

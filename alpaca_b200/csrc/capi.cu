@@ -219,11 +219,15 @@ int alp_rk3_stage(int dim, double *d_blocks, double *d_initial, const double *d_
 // engine
 // ---------------------------------------------------------------------------
 
+// The engine keeps every case in three block pools: A holds the state at the
+// start of a step (and at its end), B and C the first and second RK3 stages.
+// Stencils read neighbour blocks directly, so pool halos are only filled when
+// a case is exported.
 struct alp_engine {
   int dim = 3, scheme = FV_CHAR, precision = FP64;
   int capacity = 0, max_cases = 0;
   int ne = 5, cells = 0, faces = 0;
-  double *U = nullptr, *U0 = nullptr, *F = nullptr;
+  double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr;
   int *work = nullptr;
@@ -248,18 +252,30 @@ struct alp_engine {
   long long dstride() const { return (long long)ne * faces; }
   long long stride() const { return dstride() * dim; }
 
+  // dt, then per stage one face-flux launch (all directions) and one
+  // divergence + stage-update launch: A -> B, (B, A) -> C, (C, A) -> A.
   int record_step() {
     Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
     ALP_CUDA(launch_signal_speed(L, cases, nullptr));
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
+    double *in[3] = {U, UB, UC};
+    double *out[3] = {UB, UC, U};
     for (int s = 0; s < 3; ++s) {
-      for (int d = 0; d < dim; ++d)
-        ALP_CUDA(launch_face_flux(L, d, F + d * dstride(), stride(), false));
-      ALP_CUDA(launch_stage_update(L, U0, F, stride(), dstride(), s, cases, 0.0));
-      ALP_CUDA(launch_halo(L, nbr26, true, ne, cases));
+      Launch Ls = L;
+      Ls.U = in[s];
+      ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
+      ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
     }
     ALP_CUDA(launch_step_commit(cases, max_cases, stream));
     return ALP_OK;
+  }
+
+  // work-list offset of a case's blocks (cases are listed in id order)
+  int work_offset(int cid) const {
+    int off = 0;
+    for (int c = 0; c < cid; ++c)
+      if (case_rec[c].live) off += case_rec[c].nb;
+    return off;
   }
 
   int rebuild_work() {
@@ -307,7 +323,8 @@ struct alp_engine {
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
     cudaFree(U);
-    cudaFree(U0);
+    cudaFree(UB);
+    cudaFree(UC);
     cudaFree(F);
     cudaFree(meta);
     cudaFree(nbr26);
@@ -325,7 +342,7 @@ size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
   size_t const blk = ne * cells_of(dim) * sizeof(double);
   size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double);
   return (size_t)capacity_blocks *
-             (2 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
+             (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
          (size_t)max_cases * sizeof(CaseState);
 }
 
@@ -353,7 +370,8 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
     if (err == cudaSuccess) err = cudaMalloc(p, bytes);
   };
   grab((void **)&e->U, blk * capacity_blocks * sizeof(double));
-  grab((void **)&e->U0, blk * capacity_blocks * sizeof(double));
+  grab((void **)&e->UB, blk * capacity_blocks * sizeof(double));
+  grab((void **)&e->UC, blk * capacity_blocks * sizeof(double));
   grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
   grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
@@ -428,17 +446,8 @@ int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size
   cs.max_steps = max_steps;
   cs.status = 0;
   ALP_CUDA(cudaMemcpyAsync(e->cases + cid, &cs, sizeof(cs), cudaMemcpyHostToDevice, e->stream));
-  // fill the halos of the new blocks from their interiors
-  BlockMeta def{};
-  Launch L{e->dim, e->scheme, e->precision, e->U, nullptr, nb, nullptr, def, e->stream};
   if (int rc = e->rebuild_work()) return rc;
-  // the case's blocks are contiguous in h_work order; find its offset
-  int off = 0;
-  for (int c = 0; c < cid; ++c)
-    if (e->case_rec[c].live) off += e->case_rec[c].nb;
-  L.work = e->work + off;
-  ALP_CUDA(launch_halo(L, e->nbr26, true, e->ne, nullptr));
-  // cudaMemcpyAsync from pageable memory returns once the source is consumed
+  // the source may be pageable or reused by the caller right after the call
   ALP_CUDA(cudaStreamSynchronize(e->stream));
   *case_id = cid;
   return ALP_OK;
@@ -495,9 +504,16 @@ int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t,
   auto const &c = e->case_rec[case_id];
   size_t const blk = (size_t)e->ne * e->cells;
   CaseState cs;
-  if (h_blocks)
+  if (h_blocks) {
+    // the pool's halos are not maintained while stepping: fill them (all 26
+    // regions + zero gradient, as the reference's halo update) before export
+    BlockMeta def{};
+    Launch L{e->dim, e->scheme, e->precision, e->U, e->work + e->work_offset(case_id), c.nb,
+             nullptr, def, e->stream};
+    ALP_CUDA(launch_halo(L, e->nbr26, false, e->ne, nullptr));
     ALP_CUDA(cudaMemcpyAsync(h_blocks, e->U + blk * c.first, blk * c.nb * sizeof(double),
                              cudaMemcpyDeviceToHost, e->stream));
+  }
   ALP_CUDA(cudaMemcpyAsync(&cs, e->cases + case_id, sizeof(cs), cudaMemcpyDeviceToHost, e->stream));
   ALP_CUDA(cudaStreamSynchronize(e->stream));
   if (t) *t = cs.t;
@@ -534,8 +550,8 @@ int alp_engine_set_graph(alp_engine *e, int enabled) {
 
 int alp_engine_launches_per_step(alp_engine *e) {
   if (!e) return 0;
-  // signal speed, dt, 3 x (dim face fluxes, stage update, halo copy + zero gradient), commit
-  return 2 + 3 * (e->dim + 1 + 2) + 1;
+  // signal speed, dt, 3 x (face fluxes, stage update), commit
+  return 2 + 3 * 2 + 1;
 }
 
 }  // extern "C"

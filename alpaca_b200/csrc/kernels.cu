@@ -8,6 +8,10 @@
 #include <cstdio>
 
 #include "kernels.cuh"
+
+// The FP32-flux branches return early, which leaves the shared FP64 tail
+// unreachable in those instantiations.
+#pragma nv_diag_suppress 128
 #include "numerics.cuh"
 
 namespace alp {
@@ -54,19 +58,50 @@ template <int DIM, int DIR> struct FaceMap {
   }
 };
 
-template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM>
-__global__ void __launch_bounds__(128)
-face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
-                 BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
-                 long long stride) {
+// Minimum resident CTAs per SM for the 128-thread face kernels: caps the
+// registers so that FV kernels keep 16-20 warps per SM without spilling
+// (FV characteristic: 126 registers at 4 CTAs); flux splitting keeps its
+// registers (its 6-cell flux and state stencils are live together).
+template <int SCHEME> struct FaceOccupancy { static constexpr int min_ctas = 1; };
+template <> struct FaceOccupancy<FV_CHAR> { static constexpr int min_ctas = 4; };
+template <> struct FaceOccupancy<FV_PRIM> { static constexpr int min_ctas = 5; };
+
+// Stores one face's fluxes in the reference flux-array layout: = (zero for a
+// skipped face) or, for the drop-in contract, += (skipped faces untouched).
+template <int DIM, int DIR, bool ACCUM>
+__device__ __forceinline__ void write_flux(double *__restrict__ F, int item, long long stride,
+                                           int a, int p1, int p2, bool valid,
+                                           double const (&flux)[DIM + 2]) {
+  using G = Geo<DIM>;
+  using M = FaceMap<DIM, DIR>;
+  int fi[3];
+  fi[DIR] = a;
+  fi[M::O1] = p1 + 1;
+  fi[M::O2] = p2 + 1;
+  double *fo = F + (long long)item * stride + G::face(fi[0], fi[1], fi[2]);
+#pragma unroll
+  for (int f = 0; f < DIM + 2; ++f) {
+    double const v = valid ? flux[f] : 0.0;
+    if (ACCUM) {
+      if (valid) fo[f * G::FACES] += v;
+    } else {
+      fo[f * G::FACES] = v;
+    }
+  }
+}
+
+// Flux of the face with thread index t of direction DIR of the block in `slot`.
+// GATHER: stencil cells outside the interior along DIR come from the
+// neighbour blocks' interiors (nbr26; zero gradient at domain faces) instead of
+// the block's own halo cells, so no halo copy is needed between stages.
+template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER>
+__device__ __forceinline__ void face_flux(double const *__restrict__ U,
+                                          int const *__restrict__ nbr26, int slot, int item,
+                                          int t, BlockMeta const &bm, double *__restrict__ F,
+                                          long long stride) {
   using G = Geo<DIM>;
   using M = FaceMap<DIM, DIR>;
   constexpr int NE = G::NE;
-  int const item = blockIdx.x;
-  int const t = blockIdx.y * blockDim.x + threadIdx.x;
-  if (t >= M::COUNT) return;
-  int const slot = slot_of(work, item);
-  BlockMeta const bm = meta ? meta[slot] : def;
   Eos const eos{bm.gamma, bm.B, bm.safe};
 
   int a, p1, p2;
@@ -76,13 +111,38 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
   c0[M::O1] = G::fic(M::O1) + p1;
   c0[M::O2] = G::fic(M::O2) + p2;
   constexpr int step = DIR == 0 ? G::TCY * G::TCZ : (DIR == 1 ? G::TCZ : 1);
-  double const *ub = U + (size_t)slot * G::BLOCK_DOUBLES + G::cell(c0[0], c0[1], c0[2]);
+  double const *blk = U + (size_t)slot * G::BLOCK_DOUBLES;
+  double const *ub = blk + G::cell(c0[0], c0[1], c0[2]);
 
   double cons[6][NE];
+  if constexpr (GATHER) {
+    // low / high neighbour along DIR (26-table slots of W,E / S,N / B,T)
+    constexpr int lo_slot = DIR == 0 ? 4 : (DIR == 1 ? 10 : 12);
+    constexpr int hi_slot = DIR == 0 ? 21 : (DIR == 1 ? 15 : 13);
+    int const nlo = a < 3 ? __ldg(nbr26 + (size_t)slot * 26 + lo_slot) : 0;
+    int const nhi = a > 13 ? __ldg(nbr26 + (size_t)slot * 26 + hi_slot) : 0;
 #pragma unroll
-  for (int m = 0; m < 6; ++m)
+    for (int m = 0; m < 6; ++m) {
+      int const c = HS + a - 3 + m;  // cell index along DIR
+      double const *src;
+      if (c < HS) {
+        src = nlo >= 0 ? U + (size_t)nlo * G::BLOCK_DOUBLES + ((ub - blk) + (c + IC - c0[DIR]) * step)
+                       : blk + ((ub - blk) + (HS - c0[DIR]) * step);
+      } else if (c >= HS + IC) {
+        src = nhi >= 0 ? U + (size_t)nhi * G::BLOCK_DOUBLES + ((ub - blk) + (c - IC - c0[DIR]) * step)
+                       : blk + ((ub - blk) + (HS + IC - 1 - c0[DIR]) * step);
+      } else {
+        src = ub + m * step;
+      }
 #pragma unroll
-    for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(ub + f * G::CELLS + m * step);
+      for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(src + f * G::CELLS);
+    }
+  } else {
+#pragma unroll
+    for (int m = 0; m < 6; ++m)
+#pragma unroll
+      for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(ub + f * G::CELLS + m * step);
+  }
 
   T flux[NE];
   bool valid = true;
@@ -94,7 +154,50 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
     if (!(pt.rho > 0.0) || !(pn.rho > 0.0)) valid = false;
     Roe<T> const r = roe_average<DIM, DIR, T>(eos, pt, pn);
     T ch[2][NE];
-    if constexpr (SCHEME == FV_CHAR) {
+    if constexpr (SCHEME == FV_CHAR && sizeof(T) == 4) {
+      // FP32 form: characteristic projection and WENO5 of the increments
+      // U_m - U_i against the face's left cell i (WENO5 is translation
+      // invariant and R L = I), the left cell's state added back in double.
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        T L[NE];
+        left_row<DIM, DIR, T>(n, r, L);
+        T uc[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) {
+          T s = T(0);
+#pragma unroll
+          for (int q = 0; q < NE; ++q) {
+            int const l = sum_seq<DIM, DIR>(q);
+            if (!left_nonzero<DIM, DIR>(n, l)) continue;
+            s = fmaf(L[l], m == 2 ? 0.0f : float(cons[m][l] - cons[2][l]), s);
+          }
+          uc[m] = s;
+        }
+        ch[0][n] = weno5_left(uc);
+        ch[1][n] = weno5_right(uc);
+      }
+      T dm[NE], dp[NE];
+      to_physical<DIM, DIR, T>(r, ch[0], dm);
+      to_physical<DIM, DIR, T>(r, ch[1], dp);
+      double cm[NE], cp[NE];
+#pragma unroll
+      for (int f = 0; f < NE; ++f) {
+        cm[f] = cons[2][f] + double(dm[f]);
+        cp[f] = cons[2][f] + double(dp[f]);
+      }
+      if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
+      double const one_l = inv(cm[MASS]), one_r = inv(cp[MASS]);
+      double const pm = eos_pressure<DIM>(eos, cm[MASS], cm[MOMX], DIM > 1 ? cm[MOMX + (DIM > 1)] : 0.0,
+                                          DIM > 2 ? cm[MOMX + 2 * (DIM > 2)] : 0.0, cm[ENERGY], one_l);
+      double const pp = eos_pressure<DIM>(eos, cp[MASS], cp[MOMX], DIM > 1 ? cp[MOMX + (DIM > 1)] : 0.0,
+                                          DIM > 2 ? cp[MOMX + 2 * (DIM > 2)] : 0.0, cp[ENERGY], one_r);
+      if (!(pm > -bm.B) || !(pp > -bm.B)) valid = false;
+      double fd[NE];
+      hllc_mixed<DIM, DIR>(eos, cm, cp, pm, pp, cm[mP] * one_l, cp[mP] * one_r, one_l, one_r, fd);
+      write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
+      return;
+    } else if constexpr (SCHEME == FV_CHAR) {
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
         T L[NE];
@@ -123,40 +226,44 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
       if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
       // prime states of the reconstructed states (prime_state_handler.h:277-371),
       // pressure recovered in double
+      T const one_l = inv(cm[MASS]), one_r = inv(cp[MASS]);
       double const pm = eos_pressure<DIM>(eos, double(cm[MASS]), double(cm[MOMX]),
                                           DIM > 1 ? double(cm[MOMX + (DIM > 1)]) : 0.0,
                                           DIM > 2 ? double(cm[MOMX + 2 * (DIM > 2)]) : 0.0,
-                                          double(cm[ENERGY]));
+                                          double(cm[ENERGY]), double(one_l));
       double const pp = eos_pressure<DIM>(eos, double(cp[MASS]), double(cp[MOMX]),
                                           DIM > 1 ? double(cp[MOMX + (DIM > 1)]) : 0.0,
                                           DIM > 2 ? double(cp[MOMX + 2 * (DIM > 2)]) : 0.0,
-                                          double(cp[ENERGY]));
+                                          double(cp[ENERGY]), double(one_r));
       if (!(pm > -bm.B) || !(pp > -bm.B)) valid = false;
-      T const vl = cm[mP] * (T(1) / cm[MASS]);
-      T const vr = cp[mP] * (T(1) / cp[MASS]);
-      hllc<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, flux);
+      T const vl = cm[mP] * one_l;
+      T const vr = cp[mP] * one_r;
+      hllc<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
     } else {
       // Roe flux-vector splitting (flux_splitting_scheme.cpp:42-76, 185-315)
-      T adv[6][NE];
+      double advd[6][NE];
 #pragma unroll
       for (int m = 0; m < 6; ++m) {
-        double const one_rho = 1.0 / cons[m][MASS];
+        double const one_rho = inv(cons[m][MASS]);
         double const p = eos_pressure<DIM>(
             eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
-            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY]);
+            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY], one_rho);
         double const vel = cons[m][mP] * one_rho;
         double const rho = cons[m][MASS];
-        adv[m][MASS] = T(rho * vel);
-        adv[m][ENERGY] = T((cons[m][ENERGY] + p) * vel);
+        advd[m][MASS] = rho * vel;
+        advd[m][ENERGY] = (cons[m][ENERGY] + p) * vel;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
           double const vd = cons[m][MOMX + d] * one_rho;
           double v = rho * (vel * vd);
           if (d == DIR) v += p;
-          adv[m][MOMX + d] = T(v);
+          advd[m][MOMX + d] = v;
         }
       }
       T const ev_nl0 = fabs(r.up - r.c), ev_nl1 = fabs(r.up + r.c), ev_lin = fabs(r.up);
+      // FP32 form: increments against the face's left cell; the characteristic
+      // flux of that cell, L f_i, is restored by R as f_i in double
+      constexpr bool DELTA = sizeof(T) == 4;
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
         T L[NE];
@@ -171,8 +278,8 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            T const uct = T(cons[m][l]) * L[l];
-            T const act = adv[m][l] * L[l];
+            T const uct = (DELTA ? T(cons[m][l] - cons[2][l]) : T(cons[m][l])) * L[l];
+            T const act = (DELTA ? T(advd[m][l] - advd[2][l]) : T(advd[m][l])) * L[l];
             T const tp = act + alpha * uct;
             T const tn = act - alpha * uct;
             sp = first ? tp : sp + tp;
@@ -185,22 +292,59 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
         ch[0][n] = T(0.5) * (weno5_left(pos) + weno5_right(neg));
       }
       to_physical<DIM, DIR, T>(r, ch[0], flux);
+      if constexpr (DELTA) {
+        double fd[NE];
+#pragma unroll
+        for (int f = 0; f < NE; ++f) fd[f] = advd[2][f] + double(flux[f]);
+        write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
+        return;
+      }
     }
   } else {
     // FV primitive reconstruction (primitive_state_reconstruction.h:56-107)
-    T pm[NE], pp[NE];
-    {
-      double prim[6][NE];
+    double prim[6][NE];
 #pragma unroll
-      for (int m = 0; m < 6; ++m) {
-        prim[m][RHO] = cons[m][MASS];
-        double const one_rho = 1.0 / cons[m][MASS];
+    for (int m = 0; m < 6; ++m) {
+      prim[m][RHO] = cons[m][MASS];
+      double const one_rho = inv(cons[m][MASS]);
 #pragma unroll
-        for (int d = 0; d < DIM; ++d) prim[m][VELX + d] = cons[m][MOMX + d] * one_rho;
-        prim[m][PRES] = eos_pressure<DIM>(
-            eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
-            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY]);
+      for (int d = 0; d < DIM; ++d) prim[m][VELX + d] = cons[m][MOMX + d] * one_rho;
+      prim[m][PRES] = eos_pressure<DIM>(
+          eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
+          DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY], one_rho);
+    }
+    if constexpr (sizeof(T) == 4) {
+      // FP32 form: WENO5 of the increments against the left cell's primes
+      double pmd[NE], ppd[NE];
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        T arr[6];
+#pragma unroll
+        for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n] - prim[2][n]);
+        pmd[n] = prim[2][n] + double(weno5_left(arr));
+        ppd[n] = prim[2][n] + double(weno5_right(arr));
       }
+      double cm[NE], cp[NE];
+      cm[MASS] = pmd[RHO];
+      cp[MASS] = ppd[RHO];
+#pragma unroll
+      for (int d = 0; d < DIM; ++d) {
+        cm[MOMX + d] = pmd[VELX + d] * pmd[RHO];
+        cp[MOMX + d] = ppd[VELX + d] * ppd[RHO];
+      }
+      cm[ENERGY] = eos_energy<DIM, double>(eos, pmd[RHO], pmd[VELX], DIM > 1 ? pmd[VELX + (DIM > 1)] : 0.0,
+                                           DIM > 2 ? pmd[VELX + 2 * (DIM > 2)] : 0.0, pmd[PRES]);
+      cp[ENERGY] = eos_energy<DIM, double>(eos, ppd[RHO], ppd[VELX], DIM > 1 ? ppd[VELX + (DIM > 1)] : 0.0,
+                                           DIM > 2 ? ppd[VELX + 2 * (DIM > 2)] : 0.0, ppd[PRES]);
+      if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
+      if (!(pmd[PRES] > -bm.B) || !(ppd[PRES] > -bm.B)) valid = false;
+      double fd[NE];
+      hllc_mixed<DIM, DIR>(eos, cm, cp, pmd[PRES], ppd[PRES], pmd[VELX + DIR], ppd[VELX + DIR],
+                           inv(cm[MASS]), inv(cp[MASS]), fd);
+      write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
+      return;
+    } else {
+      T pm[NE], pp[NE];
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
         T arr[6];
@@ -209,38 +353,73 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
         pm[n] = weno5_left(arr);
         pp[n] = weno5_right(arr);
       }
-    }
-    // PrimeStatesToConservatives (prime_state_handler.h:195-275)
-    T cm[NE], cp[NE];
-    cm[MASS] = pm[RHO];
-    cp[MASS] = pp[RHO];
+      // PrimeStatesToConservatives (prime_state_handler.h:195-275)
+      T cm[NE], cp[NE];
+      cm[MASS] = pm[RHO];
+      cp[MASS] = pp[RHO];
 #pragma unroll
-    for (int d = 0; d < DIM; ++d) {
-      cm[MOMX + d] = pm[VELX + d] * pm[RHO];
-      cp[MOMX + d] = pp[VELX + d] * pp[RHO];
+      for (int d = 0; d < DIM; ++d) {
+        cm[MOMX + d] = pm[VELX + d] * pm[RHO];
+        cp[MOMX + d] = pp[VELX + d] * pp[RHO];
+      }
+      cm[ENERGY] = eos_energy<DIM, T>(eos, pm[RHO], pm[VELX], DIM > 1 ? pm[VELX + (DIM > 1)] : T(0),
+                                      DIM > 2 ? pm[VELX + 2 * (DIM > 2)] : T(0), pm[PRES]);
+      cp[ENERGY] = eos_energy<DIM, T>(eos, pp[RHO], pp[VELX], DIM > 1 ? pp[VELX + (DIM > 1)] : T(0),
+                                      DIM > 2 ? pp[VELX + 2 * (DIM > 2)] : T(0), pp[PRES]);
+      if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
+      if (!(double(pm[PRES]) > -bm.B) || !(double(pp[PRES]) > -bm.B)) valid = false;
+      // HLLC's own 1/density (hllc_riemann_solver.h:75-78)
+      hllc<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR],
+                        inv(cm[MASS]), inv(cp[MASS]), flux);
     }
-    cm[ENERGY] = eos_energy<DIM, T>(eos, pm[RHO], pm[VELX], DIM > 1 ? pm[VELX + (DIM > 1)] : T(0),
-                                    DIM > 2 ? pm[VELX + 2 * (DIM > 2)] : T(0), pm[PRES]);
-    cp[ENERGY] = eos_energy<DIM, T>(eos, pp[RHO], pp[VELX], DIM > 1 ? pp[VELX + (DIM > 1)] : T(0),
-                                    DIM > 2 ? pp[VELX + 2 * (DIM > 2)] : T(0), pp[PRES]);
-    if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
-    if (!(double(pm[PRES]) > -bm.B) || !(double(pp[PRES]) > -bm.B)) valid = false;
-    hllc<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR], flux);
   }
 
-  int fi[3];
-  fi[DIR] = a;
-  fi[M::O1] = p1 + 1;
-  fi[M::O2] = p2 + 1;
-  double *fo = F + (long long)item * stride + G::face(fi[0], fi[1], fi[2]);
+  double fd[NE];
 #pragma unroll
-  for (int f = 0; f < NE; ++f) {
-    double const v = valid ? double(flux[f]) : 0.0;
-    if (ACCUM) {
-      if (valid) fo[f * G::FACES] += v;
-    } else {
-      fo[f * G::FACES] = v;
-    }
+  for (int f = 0; f < NE; ++f) fd[f] = double(flux[f]);
+  write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
+}
+
+// One direction over all work items (drop-in calls: halos from the buffer).
+template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM>
+__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME>::min_ctas)
+face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                 BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
+                 long long stride) {
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= FaceMap<DIM, DIR>::COUNT) return;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  face_flux<DIM, DIR, SCHEME, T, ACCUM, false>(U, nullptr, slot, item, t, bm, F, stride);
+}
+
+// Every direction of every work item in one launch (engine): blockIdx.z is the
+// direction, stencils gathered from neighbours, direction d written to
+// F + d * dstride. Items whose case is inactive (dt == 0) are skipped.
+template <int DIM, int SCHEME, typename T>
+__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME>::min_ctas)
+face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                     BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
+                     CaseState const *__restrict__ cases, double *__restrict__ F,
+                     long long stride, long long dstride) {
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  int const item = blockIdx.x;
+  int const slot = work[item];
+  BlockMeta const bm = meta[slot];
+  if (!(cases[bm.case_id].dt > 0.0)) return;
+  int const dir = blockIdx.z;
+  if (dir == 0) {
+    if (t < FaceMap<DIM, 0>::COUNT)
+      face_flux<DIM, 0, SCHEME, T, false, true>(U, nbr26, slot, item, t, bm, F, stride);
+  } else if (DIM > 1 && dir == 1) {
+    if (t < FaceMap<DIM, 1>::COUNT)
+      face_flux<DIM, (DIM > 1 ? 1 : 0), SCHEME, T, false, true>(U, nbr26, slot, item, t, bm,
+                                                                 F + dstride, stride);
+  } else if (DIM > 2) {
+    if (t < FaceMap<DIM, 2>::COUNT)
+      face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, T, false, true>(U, nbr26, slot, item, t, bm,
+                                                                 F + 2 * dstride, stride);
   }
 }
 
@@ -292,7 +471,7 @@ divergence_kernel(int const *__restrict__ work, BlockMeta const *__restrict__ me
   for (int x = threadIdx.x; x < G::BLOCK_DOUBLES; x += blockDim.x) rb[x] = 0.0;
   __syncthreads();
   BlockMeta const bm = meta ? meta[slot] : def;
-  double const ocs = 1.0 / bm.cell_size;
+  double const ocs = inv(bm.cell_size);
   double const *Fb = F + (long long)item * stride;
   for (int t = threadIdx.x; t < G::INTERIOR; t += blockDim.x) {
     int i, j, k;
@@ -312,10 +491,13 @@ __constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
 __constant__ double kRkA0[3] = {0.0, 0.25, 2.0 / 3.0};
 __constant__ double kRkA1[3] = {0.0, 0.75, 1.0 / 3.0};
 
+// Uin: stage input, U0: state at the start of the step, Uout: stage output.
+// Uout may alias U0 (each cell is read and written by the same thread) but
+// not Uin, whose cells other blocks' stencils read during the stage.
 template <int DIM>
 __global__ void __launch_bounds__(256)
-stage_update_kernel(double *__restrict__ U, double *__restrict__ U0, int const *__restrict__ work,
-                    BlockMeta const *__restrict__ meta, BlockMeta def,
+stage_update_kernel(double const *Uin, double const *U0, double *Uout,
+                    int const *__restrict__ work, BlockMeta const *__restrict__ meta, BlockMeta def,
                     double const *__restrict__ F, long long stride, long long dstride, int stage,
                     CaseState const *__restrict__ cases, double dt_all) {
   using G = Geo<DIM>;
@@ -329,7 +511,7 @@ stage_update_kernel(double *__restrict__ U, double *__restrict__ U0, int const *
   int i, j, k;
   interior_coords<DIM>(t, i, j, k);
   int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
-  double const ocs = 1.0 / bm.cell_size;
+  double const ocs = inv(bm.cell_size);
   double const cdt = kRkC[stage] * (0.0 + dt);
   double const a0 = kRkA0[stage], a1 = kRkA1[stage];
   double const *Fb = F + (long long)item * stride;
@@ -339,13 +521,9 @@ stage_update_kernel(double *__restrict__ U, double *__restrict__ U0, int const *
     double const *fx = Fb + f * G::FACES;
     double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
     size_t const x = base + (size_t)f * G::CELLS;
-    double u = U[x];
-    if (stage == 0) {
-      U0[x] = u;
-    } else {
-      u = a0 * u + a1 * U0[x];
-    }
-    U[x] = u + cdt * rhs;
+    double u = Uin[x];
+    if (stage != 0) u = a0 * u + a1 * U0[x];
+    Uout[x] = u + cdt * rhs;
   }
 }
 
@@ -498,13 +676,14 @@ prime_states_kernel(double const *__restrict__ U, int const *__restrict__ work,
     double c[G::NE];
 #pragma unroll
     for (int f = 0; f < G::NE; ++f) c[f] = ub[f * G::CELLS + x];
-    double const one_density = 1.0 / c[MASS];
+    double const one_density = inv(c[MASS]);
     pb[RHO * G::CELLS + x] = c[MASS];
 #pragma unroll
     for (int d = 0; d < DIM; ++d) pb[(VELX + d) * G::CELLS + x] = c[MOMX + d] * one_density;
     pb[PRES * G::CELLS + x] = eos_pressure<DIM>(eos, c[MASS], c[MOMX],
                                                 DIM > 1 ? c[MOMX + (DIM > 1)] : 0.0,
-                                                DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY]);
+                                                DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY],
+                                                one_density);
   }
 }
 
@@ -530,10 +709,11 @@ signal_speed_kernel(double const *__restrict__ U, int const *__restrict__ work,
     double c[G::NE];
 #pragma unroll
     for (int f = 0; f < G::NE; ++f) c[f] = ub[f * G::CELLS + x];
-    double const one_density = 1.0 / c[MASS];
+    double const one_density = inv(c[MASS]);
     double const p = eos_pressure<DIM>(eos, c[MASS], c[MOMX], DIM > 1 ? c[MOMX + (DIM > 1)] : 0.0,
-                                       DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY]);
-    double const cs = eos_speed_of_sound<double>(eos, c[MASS], p);
+                                       DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY],
+                                       one_density);
+    double const cs = eos_speed_of_sound<double>(eos, c[MASS], p, one_density);
     double v[3] = {0.0, 0.0, 0.0};
 #pragma unroll
     for (int d = 0; d < DIM; ++d) v[d] = fabs(c[MOMX + d] * one_density) + cs;
@@ -670,19 +850,59 @@ cudaError_t launch_divergence(Launch const &L, double const *F, long long stride
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage_update(Launch const &L, double *U0, double const *F, long long stride,
-                                long long dstride, int stage, CaseState const *cases, double dt) {
+cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout, double const *F,
+                                long long stride, long long dstride, int stage,
+                                CaseState const *cases, double dt) {
   if (L.nwork <= 0) return cudaSuccess;
   if (stage < 0 || stage > 2) return cudaErrorInvalidValue;
   int const threads = 256;
   dim3 grid(L.nwork, (interior_of(L.dim) + threads - 1) / threads);
   switch (L.dim) {
-    case 1: stage_update_kernel<1><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
-    case 2: stage_update_kernel<2><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
-    case 3: stage_update_kernel<3><<<grid, threads, 0, L.stream>>>(L.U, U0, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    case 1: stage_update_kernel<1><<<grid, threads, 0, L.stream>>>(L.U, U0, Uout, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    case 2: stage_update_kernel<2><<<grid, threads, 0, L.stream>>>(L.U, U0, Uout, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
+    case 3: stage_update_kernel<3><<<grid, threads, 0, L.stream>>>(L.U, U0, Uout, L.work, L.meta, L.def, F, stride, dstride, stage, cases, dt); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();
+}
+
+namespace {
+template <int DIM, typename T>
+cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *cases, double *F,
+                            long long stride, long long dstride) {
+  int const count = (IC + 1) * (DIM > 1 ? IC : 1) * (DIM > 2 ? IC : 1);
+  dim3 grid(L.nwork, (count + 127) / 128, DIM);
+  switch (L.scheme) {
+    case FV_CHAR:
+      face_flux_all_kernel<DIM, FV_CHAR, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      break;
+    case FV_PRIM:
+      face_flux_all_kernel<DIM, FV_PRIM, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      break;
+    case FS_ROE:
+      face_flux_all_kernel<DIM, FS_ROE, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
+                                 double *F, long long stride, long long dstride) {
+  if (L.nwork <= 0) return cudaSuccess;
+  if (!L.work || !L.meta || !nbr26 || !cases) return cudaErrorInvalidValue;
+  bool const f32 = L.precision == FP32_FLUX;
+  switch (L.dim) {
+    case 1: return f32 ? face_flux_all_t<1, float>(L, nbr26, cases, F, stride, dstride)
+                       : face_flux_all_t<1, double>(L, nbr26, cases, F, stride, dstride);
+    case 2: return f32 ? face_flux_all_t<2, float>(L, nbr26, cases, F, stride, dstride)
+                       : face_flux_all_t<2, double>(L, nbr26, cases, F, stride, dstride);
+    case 3: return f32 ? face_flux_all_t<3, float>(L, nbr26, cases, F, stride, dstride)
+                       : face_flux_all_t<3, double>(L, nbr26, cases, F, stride, dstride);
+  }
+  return cudaErrorInvalidValue;
 }
 
 cudaError_t launch_rk_stage_rhs(int dim, double *U, double *U0, double const *rhs, int nb,

@@ -42,10 +42,17 @@ cudaError_t launch_face_flux(Launch const &L, int dir, double *F, long long flux
 cudaError_t launch_divergence(Launch const &L, double const *F, long long flux_item_stride,
                               long long dir_stride, double *rhs);
 
-// RK3 stage: U0 <- U on stage 0; U <- a0*U + a1*U0 + c*dt*div(F) on the
-// interior, dt per case from cases[meta.case_id].dt (skip when dt == 0).
-// When cases is null, `dt` is used for every block.
-cudaError_t launch_stage_update(Launch const &L, double *U0, double const *F,
+// Face fluxes of every direction of every work item in one launch (engine):
+// stencils gathered from neighbour interiors through nbr26 (zero gradient at
+// domain faces), so block halos are never read; items of inactive cases
+// (dt == 0) skipped. Direction d goes to F + d * dir_stride.
+cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
+                                 double *F, long long flux_item_stride, long long dir_stride);
+
+// RK3 stage on the interior: Uout = (stage ? a0*Uin + a1*U0 : Uin) + c*dt*div(F)
+// with Uin = L.U; dt per case from cases[meta.case_id].dt (skip when dt == 0),
+// or `dt` for every block when cases is null. Uout may alias U0, not Uin.
+cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout, double const *F,
                                 long long flux_item_stride, long long dir_stride, int stage,
                                 CaseState const *cases, double dt);
 

@@ -5,13 +5,59 @@
 // with the CPU reference to rounding (FMA contraction is the only difference).
 // T is the compute type of reconstruction and flux (double, or float in the
 // FP32-flux form); pressure recovery from total energy always runs in double.
+//
+// Two builds share this file. The strict build (ALP_STRICT, compiled with
+// -fmad=false) evaluates every expression exactly as the reference writes it,
+// IEEE division included, and reproduces the reference bit for bit. The fast
+// build replaces divisions by Newton-refined reciprocals (reused where the same
+// divisor recurs) and evaluates the WENO5 weights with a single reciprocal;
+// both change results only at the rounding level.
 #pragma once
 
 #include <cfloat>
 
 #include "layout.cuh"
 
+#ifdef ALP_STRICT
+#define ALP_FAST 0
+#else
+#define ALP_FAST 1
+#endif
+
 namespace alp {
+
+// Reciprocal by Newton-Raphson iteration on f(y) = 1/y - b (y <- y + y(1 - b y)),
+// seeded with the PTX approximate reciprocal; two iterations take the seed's
+// ~2^-20 relative error below one ulp.
+__device__ __forceinline__ double rcp_nr(double b) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(b));
+  double e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  e = fma(-b, y, 1.0);
+  y = fma(y, e, y);
+  return y;
+}
+
+// 1/x: IEEE division in the strict build, rcp_nr (double) or the hardware
+// approximate quotient (float) in the fast build.
+__device__ __forceinline__ double inv(double x) {
+  if constexpr (ALP_FAST) return rcp_nr(x);
+  else return 1.0 / x;
+}
+__device__ __forceinline__ float inv(float x) {
+  if constexpr (ALP_FAST) return __fdividef(1.0f, x);
+  else return 1.0f / x;
+}
+// a / b, where ib is 1/b as returned by inv(b): the strict build divides.
+template <typename T> __device__ __forceinline__ T quot(T a, T b, T ib) {
+  if constexpr (ALP_FAST) return a * ib;
+  else return a / b;
+}
+template <typename T> __device__ __forceinline__ T quot(T a, T b) {
+  if constexpr (ALP_FAST) return a * inv(b);
+  else return a / b;
+}
 
 template <typename T> __device__ __forceinline__ T dmin(T a, T b) { return (b < a) ? b : a; }
 template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return (a < b) ? b : a; }
@@ -47,32 +93,46 @@ struct Eos {
   int safe;
 };
 
+// one_mass = inv(mass) (unused by the strict build, which divides)
 template <int DIM>
 __device__ __forceinline__ double eos_pressure(Eos const &e, double mass, double mx, double my,
-                                               double mz, double energy) {
+                                               double mz, double energy, double one_mass) {
   if (e.safe) {
-    double const p = -e.gamma * e.B + (e.gamma - 1.0) *
-                                          (energy - 0.5 * dacms<DIM>(mx * mx, my * my, mz * mz) /
-                                                        dmax(mass, DBL_EPSILON));
+    double const m = dmax(mass, DBL_EPSILON);
+    double const p =
+        -e.gamma * e.B +
+        (e.gamma - 1.0) * (energy - quot(0.5 * dacms<DIM>(mx * mx, my * my, mz * mz), m,
+                                         mass > DBL_EPSILON ? one_mass : inv(m)));
     return dmax(p, -e.B + DBL_EPSILON);
   }
   double const q = 0.5 * dacms<DIM>(mx * mx, my * my, mz * mz);
-  return -e.gamma * e.B + (e.gamma - 1.0) * (energy - q / mass);
+  return -e.gamma * e.B + (e.gamma - 1.0) * (energy - quot(q, mass, one_mass));
+}
+template <int DIM>
+__device__ __forceinline__ double eos_pressure(Eos const &e, double mass, double mx, double my,
+                                               double mz, double energy) {
+  return eos_pressure<DIM>(e, mass, mx, my, mz, energy, ALP_FAST ? inv(mass) : 0.0);
 }
 
 template <int DIM, typename T>
 __device__ __forceinline__ T eos_energy(Eos const &e, T rho, T u, T v, T w, T p) {
   T const g = T(e.gamma), B = T(e.B);
-  return (p + g * B) / (g - T(1)) + (T(0.5) * dacms<DIM>(u * u, v * v, w * w) * rho);
+  return quot(p + g * B, g - T(1)) + (T(0.5) * dacms<DIM>(u * u, v * v, w * w) * rho);
 }
 
-template <typename T> __device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p) {
+// one_rho = inv(rho) (unused by the strict build)
+template <typename T>
+__device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p, T one_rho) {
   T const g = T(e.gamma), B = T(e.B);
   if (e.safe) {
-    T const c2 = g * (p + B) / dmax(rho, eps_of<T>());
+    T const r = dmax(rho, eps_of<T>());
+    T const c2 = quot(g * (p + B), r, rho > eps_of<T>() ? one_rho : inv(r));
     return sqrt(dmax(c2, eps_of<T>()));
   }
-  return sqrt(g * (p + B) / rho);
+  return sqrt(quot(g * (p + B), rho, one_rho));
+}
+template <typename T> __device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p) {
+  return eos_speed_of_sound<T>(e, rho, p, ALP_FAST ? inv(rho) : T(0));
 }
 
 // ---- WENO5-JS (stencils/spatial_reconstruction_stencils/weno5.h:88-158) --
@@ -91,16 +151,29 @@ __device__ __forceinline__ T weno5_core(T v1, T v2, T v3, T v4, T v5) {
   T const s32 = T(3.0) * v3 + T(-4.0) * v4 + v5;
   T const s3 = c1 * s31 * s31 + c2 * s32 * s32;
   T const eps = T(1.0e-6);
-  T const a1 = T(0.1) / ((s1 + eps) * (s1 + eps));
-  T const a2 = T(0.6) / ((s2 + eps) * (s2 + eps));
-  T const a3 = T(0.3) / ((s3 + eps) * (s3 + eps));
-  T const one_a_sum = T(1.0) / (a1 + a2 + a3);
-  T const w1 = a1 * one_a_sum;
-  T const w2 = a2 * one_a_sum;
-  T const w3 = a3 * one_a_sum;
-  return w1 * (T(2.0 / 6.0) * v1 + T(-7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3) +
-         w2 * (T(-1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(2.0 / 6.0) * v4) +
-         w3 * (T(2.0 / 6.0) * v3 + T(5.0 / 6.0) * v4 + T(-1.0 / 6.0) * v5);
+  T const q1 = T(2.0 / 6.0) * v1 + T(-7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3;
+  T const q2 = T(-1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(2.0 / 6.0) * v4;
+  T const q3 = T(2.0 / 6.0) * v3 + T(5.0 / 6.0) * v4 + T(-1.0 / 6.0) * v5;
+  T const t1 = (s1 + eps) * (s1 + eps);
+  T const t2 = (s2 + eps) * (s2 + eps);
+  T const t3 = (s3 + eps) * (s3 + eps);
+  if constexpr (ALP_FAST && sizeof(T) == 8) {
+    // alpha_k = d_k / t_k scaled by t1 t2 t3: one reciprocal instead of four
+    // divisions (t_k >= 1e-12 and the products stay far inside the double range)
+    T const b1 = T(0.1) * (t2 * t3);
+    T const b2 = T(0.6) * (t1 * t3);
+    T const b3 = T(0.3) * (t1 * t2);
+    return (b1 * q1 + b2 * q2 + b3 * q3) * inv(b1 + b2 + b3);
+  } else {
+    T const a1 = quot(T(0.1), t1);
+    T const a2 = quot(T(0.6), t2);
+    T const a3 = quot(T(0.3), t3);
+    T const one_a_sum = quot(T(1.0), a1 + a2 + a3);
+    T const w1 = a1 * one_a_sum;
+    T const w2 = a2 * one_a_sum;
+    T const w3 = a3 * one_a_sum;
+    return w1 * q1 + w2 * q2 + w3 * q3;
+  }
 }
 template <typename T> __device__ __forceinline__ T weno5_left(T const (&a)[6]) {
   return weno5_core(a[0], a[1], a[2], a[3], a[4]);
@@ -148,7 +221,7 @@ template <int DIM, int DIR>
 __device__ __forceinline__ CellPrims<DIM, DIR> cell_prims(Eos const &e, double const (&c)[DIM + 2]) {
   CellPrims<DIM, DIR> r;
   r.rho = c[MASS];
-  r.one_rho = 1.0 / c[MASS];
+  r.one_rho = inv(c[MASS]);
   double const mx = c[MOMX];
   double const my = DIM > 1 ? c[MOMX + (DIM > 1 ? 1 : 0)] : 0.0;
   double const mz = DIM > 2 ? c[MOMX + (DIM > 2 ? 2 : 0)] : 0.0;
@@ -157,9 +230,10 @@ __device__ __forceinline__ CellPrims<DIM, DIR> cell_prims(Eos const &e, double c
   r.up = c[MOMX + DIR] * r.one_rho;
   r.u1 = DIM > 1 ? c[MOMX + (DIM > 1 ? Minor<DIR>::m1 : 0)] * r.one_rho : 0.0;
   r.u2 = DIM > 2 ? c[MOMX + (DIM > 2 ? Minor<DIR>::m2 : 0)] * r.one_rho : 0.0;
-  r.p = eos_pressure<DIM>(e, c[MASS], mx, my, mz, c[ENERGY]);
+  r.p = eos_pressure<DIM>(e, c[MASS], mx, my, mz, c[ENERGY], r.one_rho);
   // Enthalpy (stiffened_gas.cpp:88-96 / stiffened_gas_safe.cpp:77-84)
-  r.H = e.safe ? (c[ENERGY] + r.p) / dmax(c[MASS], DBL_EPSILON) : (c[ENERGY] + r.p) / c[MASS];
+  r.H = e.safe ? quot(c[ENERGY] + r.p, dmax(c[MASS], DBL_EPSILON))
+               : quot(c[ENERGY] + r.p, c[MASS], r.one_rho);
   return r;
 }
 
@@ -173,9 +247,9 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   T const psi_n = (T(n.p) + gB) * T(n.one_rho);
   T const sr_t = sqrt(T(t.rho));
   T const sr_n = sqrt(T(n.rho));
-  T const rho_div = T(1) / (sr_t + sr_n);
+  T const rho_div = quot(T(1), sr_t + sr_n);
   r.rho = sr_t * sr_n;
-  r.one_rho = T(1) / r.rho;
+  r.one_rho = quot(T(1), r.rho);
   r.up = ((T(t.up) * sr_t) + (T(n.up) * sr_n)) * rho_div;
   r.u1 = ((T(t.u1) * sr_t) + (T(n.u1) * sr_n)) * rho_div;
   r.u2 = ((T(t.u2) * sr_t) + (T(n.u2) * sr_n)) * rho_div;
@@ -188,7 +262,7 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   T const p_over_rho = ((T(t.p) * T(t.one_rho)) * sr_t + (T(n.p) * T(n.one_rho)) * sr_n) * rho_div +
                        T(0.5) * r.rho * (rho_div * rho_div) * tmp;
   r.cc = psi + r.gru * p_over_rho;
-  r.one_cc = T(1) / r.cc;
+  r.one_cc = quot(T(1), r.cc);
   r.c = sqrt(r.cc);
   r.half_cc = T(0.5) * r.one_cc;
   return r;
@@ -277,29 +351,29 @@ __device__ __forceinline__ void to_physical(Roe<T> const &r, T const (&ch)[DIM +
 // ---- HLLC with Einfeldt signal speeds -------------------------------------
 // CalculateSignalSpeed, Einfeldt (hll_signal_speed_calculator.h:77-101) and
 // HllcRiemannSolver::SolveRiemannProblemImplementation (hllc_riemann_solver.h:52-198)
+// one_rl, one_rr: 1/density of the two states as returned by inv()
 template <int DIM, int DIR, typename T>
 __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T const (&cr)[DIM + 2],
-                                     T pres_l, T pres_r, T vel_l, T vel_r,
+                                     T pres_l, T pres_r, T vel_l, T vel_r, T one_rl, T one_rr,
                                      T (&flux)[DIM + 2]) {
   constexpr int NE = DIM + 2;
   constexpr int mP = MOMX + DIR;
-  T const one_rl = T(1) / cl[MASS], one_rr = T(1) / cr[MASS];
-  T const c_l = eos_speed_of_sound(e, cl[MASS], pres_l);
-  T const c_r = eos_speed_of_sound(e, cr[MASS], pres_r);
+  T const c_l = eos_speed_of_sound<T>(e, cl[MASS], pres_l, one_rl);
+  T const c_r = eos_speed_of_sound<T>(e, cr[MASS], pres_r, one_rr);
   T const srl = sqrt(cl[MASS]);
   T const srr = sqrt(cr[MASS]);
-  T const rho_div = T(1) / (srl + srr);
+  T const rho_div = quot(T(1), srl + srr);
   T const u_roe = ((vel_l * srl) + (vel_r * srr)) * rho_div;
   T const c_e = sqrt(((c_l * c_l * srl) + (c_r * c_r * srr)) * rho_div +
                      (T(0.5) * srl * srr * rho_div * rho_div) * (vel_r - vel_l) * (vel_r - vel_l));
   T const sls = dmin(u_roe - c_e, vel_l - c_l);
   T const srs = dmax(u_roe + c_e, vel_r + c_r);
-  T const s_star = ((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r))) /
-                   (cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
+  T const s_star = quot((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r)),
+                        cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
   T const sl = dmin(sls, T(0));
   T const sr = dmax(srs, T(0));
-  T const chi_l = (sls - vel_l) / (sls - s_star);
-  T const chi_r = (srs - vel_r) / (srs - s_star);
+  T const chi_l = quot(sls - vel_l, sls - s_star);
+  T const chi_r = quot(srs - vel_r, srs - s_star);
   T const rchi_l = cl[MASS] * chi_l, rchi_r = cr[MASS] * chi_r;
   T const sg = T((T(0) < s_star) - (s_star < T(0)));
   T const wl = T(0.5) * (T(1) + sg), wr = T(0.5) * (T(1) - sg);
@@ -320,9 +394,9 @@ __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T con
   // energy (the star-state pressure term uses the clamped speeds, :131-144)
   {
     T const el = rchi_l * (cl[ENERGY] * one_rl +
-                           (s_star - vel_l) * (s_star + pres_l / (cl[MASS] * (sl - vel_l))));
+                           (s_star - vel_l) * (s_star + quot(pres_l, cl[MASS] * (sl - vel_l))));
     T const er = rchi_r * (cr[ENERGY] * one_rr +
-                           (s_star - vel_r) * (s_star + pres_r / (cr[MASS] * (sr - vel_r))));
+                           (s_star - vel_r) * (s_star + quot(pres_r, cr[MASS] * (sr - vel_r))));
     T const fl = vel_l * (cl[ENERGY] + pres_l);
     T const fr = vel_r * (cr[ENERGY] + pres_r);
     T const fsl = fl + (sl * (el - cl[ENERGY]));
@@ -338,6 +412,76 @@ __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T con
     flux[mm] = wl * fsl + wr * fsr;
   }
   (void)NE;
+}
+
+// HLLC for the FP32-flux form (same approximate Riemann solver as hllc():
+// Einfeldt speeds, Toro star states, the reference's clamped-speed energy
+// term). Wave speeds, the contact speed and the star-state increments
+// q* - q are computed in float; the physical fluxes F(q) that carry the mean
+// and their sum F + S (q* - q) are evaluated in double. Uses
+// chi - 1 = (S* - u) / (S - S*), so no increment is formed by cancellation.
+template <int DIM, int DIR>
+__device__ __forceinline__ void hllc_mixed(Eos const &e, double const (&cl)[DIM + 2],
+                                           double const (&cr)[DIM + 2], double pres_l,
+                                           double pres_r, double vel_l, double vel_r,
+                                           double one_rl, double one_rr, double (&flux)[DIM + 2]) {
+  constexpr int mP = MOMX + DIR;
+  float const g = float(e.gamma), B = float(e.B);
+  float const rl = float(cl[MASS]), rr = float(cr[MASS]);
+  float const ul = float(vel_l), ur = float(vel_r);
+  float const c_l = sqrtf(g * (float(pres_l) + B) * float(one_rl));
+  float const c_r = sqrtf(g * (float(pres_r) + B) * float(one_rr));
+  float const srl = sqrtf(rl), srr = sqrtf(rr);
+  float const rho_div = __fdividef(1.0f, srl + srr);
+  float const u_roe = (ul * srl + ur * srr) * rho_div;
+  float const c_e = sqrtf((c_l * c_l * srl + c_r * c_r * srr) * rho_div +
+                          (0.5f * srl * srr * rho_div * rho_div) * (ur - ul) * (ur - ul));
+  float const sls = dmin(u_roe - c_e, ul - c_l);
+  float const srs = dmax(u_roe + c_e, ur + c_r);
+  float const dpr = float(pres_r - pres_l);
+  float const s_star = __fdividef(dpr + (rl * ul * (sls - ul) - rr * ur * (srs - ur)),
+                                  rl * (sls - ul) - rr * (srs - ur));
+  float const sl = dmin(sls, 0.0f), sr = dmax(srs, 0.0f);
+  float const dchi_l = __fdividef(s_star - ul, sls - s_star);  // chi_l - 1
+  float const dchi_r = __fdividef(s_star - ur, srs - s_star);
+  float const chi_l = 1.0f + dchi_l, chi_r = 1.0f + dchi_r;
+  float const sg = float((0.0f < s_star) - (s_star < 0.0f));
+  double const wl = 0.5 * (1.0 + sg), wr = 0.5 * (1.0 - sg);
+  // star-state increments q* - q
+  float dq_l[DIM + 2], dq_r[DIM + 2];
+  dq_l[MASS] = rl * dchi_l;
+  dq_r[MASS] = rr * dchi_r;
+  dq_l[mP] = rl * ((s_star - ul) + dchi_l * s_star);
+  dq_r[mP] = rr * ((s_star - ur) + dchi_r * s_star);
+  dq_l[ENERGY] = float(cl[ENERGY]) * dchi_l +
+                 rl * chi_l * (s_star - ul) *
+                     (s_star + __fdividef(float(pres_l), rl * (sl - ul)));
+  dq_r[ENERGY] = float(cr[ENERGY]) * dchi_r +
+                 rr * chi_r * (s_star - ur) *
+                     (s_star + __fdividef(float(pres_r), rr * (sr - ur)));
+#pragma unroll
+  for (int d = 0; d < DIM - 1; ++d) {
+    int const mm = MOMX + (d == 0 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+    dq_l[mm] = dchi_l * float(cl[mm]);
+    dq_r[mm] = dchi_r * float(cr[mm]);
+  }
+  // physical fluxes in double
+  double fl[DIM + 2], fr[DIM + 2];
+  fl[MASS] = cl[mP];
+  fr[MASS] = cr[mP];
+  fl[mP] = cl[mP] * cl[mP] * one_rl + pres_l;
+  fr[mP] = cr[mP] * cr[mP] * one_rr + pres_r;
+  fl[ENERGY] = vel_l * (cl[ENERGY] + pres_l);
+  fr[ENERGY] = vel_r * (cr[ENERGY] + pres_r);
+#pragma unroll
+  for (int d = 0; d < DIM - 1; ++d) {
+    int const mm = MOMX + (d == 0 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+    fl[mm] = vel_l * cl[mm];
+    fr[mm] = vel_r * cr[mm];
+  }
+#pragma unroll
+  for (int n = 0; n < DIM + 2; ++n)
+    flux[n] = wl * (fl[n] + double(sl * dq_l[n])) + wr * (fr[n] + double(sr * dq_r[n]));
 }
 
 }  // namespace alp

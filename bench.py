@@ -39,6 +39,8 @@ def parse():
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--variant", default="fvchar", choices=["fvchar", "fvprim", "fsroe"])
+    p.add_argument("--precision", default="fp64", choices=["fp64", "fp32"],
+                   help="fp32: FP32 reconstruction/Riemann arithmetic, FP64 state")
     p.add_argument("--blocks", type=int, default=8, help="blocks per dimension")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -220,7 +222,8 @@ def run_ours(args, ws, rank, local):
     nbd = args.blocks
     case = cases.fourier_shock(nbd, dim=3, seed=1)
     cells = case.grid.nb * 4096
-    eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
+    prec = N.FP32_FLUX if args.precision == "fp32" else N.FP64
+    eng = api.Engine(3, args.variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
     stream = torch.cuda.ExternalStream(eng.stream_handle)
     cid = eng.add_case(case, max_steps=0)
     eng.step(args.warmup)
@@ -249,7 +252,8 @@ def run_ours(args, ws, rank, local):
         case_p = cases.Case(case.name, case.grid, host.numpy(), case.gamma, case.B, case.cfl,
                             case.t_end, 0)
         out = torch.empty_like(host).pin_memory()
-        eng = api.Engine(3, args.variant, capacity_blocks=case.grid.nb, max_cases=1)
+        eng = api.Engine(3, args.variant, precision=prec, capacity_blocks=case.grid.nb,
+                         max_cases=1)
         stream = torch.cuda.ExternalStream(eng.stream_handle)
         cid = eng.add_case(case_p, max_steps=0)
         eng.step(args.warmup)
@@ -288,7 +292,8 @@ def run_ours(args, ws, rank, local):
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-state", "data": "synthetic",
         "config": {"workload": "3d_periodic_fourier_mach2_128cubed", "blocks": case.grid.nb,
                    "cells_per_gpu": cells, "variant": args.variant,
                    "scheme": "WENO5-JS characteristic + HLLC/Einfeldt + SSP-RK3" if args.variant == "fvchar" else args.variant,

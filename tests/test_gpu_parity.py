@@ -387,3 +387,53 @@ def test_strict_engine_c2_bit_exact(cuda):
     glob = case.grid.gather(u)
     assert np.array_equal(glob[:, ::8, ::8, ::8], z["sub"])
     assert np.array_equal(u[cases.interior(3)].sum(axis=(2, 3, 4)), z["block_sums"])
+
+
+# ---- FP32-flux form ---------------------------------------------------------
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_fp32_flux_rhs(cuda, variant):
+    """Reconstruction and Riemann arithmetic in FP32 (increments against the
+    face's left cell), state and pressure recovery in FP64: one RHS within
+    1e-5 of the FP64 oracle, per field, normwise."""
+    case = small_cases()[3]
+    u = filled(case)
+    h = case.grid.cell_size
+    rhs = oracle.Restatement(3, variant).space_rhs(u, case.gamma, 0.0, False, h)[3]
+    r = api.space_rhs(to_dev(u, cuda), 3, variant, N.Material.make(case.gamma), h,
+                      precision=N.FP32_FLUX).cpu().numpy()
+    I = cases.interior(3)
+    err = field_rel_err(r[I], rhs[I])
+    print(variant, "fp32 rhs rel err per field", err)
+    assert err.max() <= 1e-5
+
+
+@pytest.mark.parametrize("variant", VARIANTS)
+def test_fp32_flux_sod_density_l1(cuda, variant):
+    """The precision target: relative L1 density error <= 1e-5 against the
+    FP64 reference after a full run (1D Sod to t = 0.2)."""
+    z = np.load(os.path.join(GOLDEN, f"sod1d_{variant}.npz"))
+    eng = api.Engine(1, variant, precision=N.FP32_FLUX, capacity_blocks=16, max_cases=1)
+    cid = eng.add_case(cases.sod_1d())
+    eng.run_to_end(chunk=16)
+    u, t, steps = eng.get(cid)
+    eng.close()
+    rho = u[cases.interior(1)][:, 0]
+    err = l1_rel(rho, z["final"][:, 0])
+    print(variant, "fp32 sod density L1", err, "steps", steps, int(z["steps"]))
+    assert abs(t - 0.2) <= 1e-15 and err <= 1e-5
+
+
+@pytest.mark.parametrize("variant", ["fvchar", "fsroe"])
+def test_fp32_flux_3d_100_steps(cuda, variant):
+    z = np.load(os.path.join(GOLDEN, f"c2_128_{variant}_100steps.npz"))
+    case = cases.fourier_shock(8, dim=3, seed=1, steps=100)
+    eng = api.Engine(3, variant, precision=N.FP32_FLUX, capacity_blocks=512, max_cases=1)
+    cid = eng.add_case(case)
+    eng.run_to_end(chunk=50)
+    u, t, steps = eng.get(cid)
+    eng.close()
+    sub = case.grid.gather(u)[:, ::8, ::8, ::8]
+    errs = [l1_rel(sub[f], z["sub"][f]) for f in range(5)]
+    print(variant, "fp32 128^3 100-step L1 per field", errs)
+    assert steps == 100 and errs[0] <= 1e-5

@@ -141,6 +141,21 @@ class Engine:
         self.nb[cid.value] = (g.nb, u.shape)
         return cid.value
 
+    def add_case_ic(self, ic_type: int, params, nblocks, cell_size: float, material: N.Material,
+                    periodic=(0, 0, 0), cfl: float = 0.6, t_end: float = 1e300,
+                    max_steps: int = 0, t0: float = 0.0) -> int:
+        """Case with a device-evaluated initial condition on a regular block grid."""
+        nbl = (C.c_int * 3)(*(list(nblocks) + [1, 1, 1])[:3])
+        per = (C.c_int * 3)(*(list(periodic) + [0, 0, 0])[:3])
+        prm = (C.c_double * 24)(*params)
+        cid = C.c_int()
+        self._check(self.lib.alp_engine_add_case_ic(self.h, C.byref(material), cell_size, cfl, t0,
+                                                    t_end, max_steps, nbl, per, ic_type, prm,
+                                                    len(params), C.byref(cid)))
+        nb = nbl[0] * nbl[1] * nbl[2]
+        self.nb[cid.value] = (nb, (nb, self.ne) + block_shape(self.dim))
+        return cid.value
+
     def remove_case(self, cid: int):
         self._check(self.lib.alp_engine_remove_case(self.h, cid))
         self.nb.pop(cid, None)
@@ -177,3 +192,51 @@ class Engine:
     @property
     def stream_handle(self) -> int:
         return self.lib.alp_engine_stream(self.h)
+
+
+def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: int = N.FP64,
+          share_3d: float = 0.9, max_cases: int = 256, steps_per_poll: int = 8,
+          one_at_a_time: bool = False, keep_results: bool = False):
+    """Runs the C++ request loop (alp_serve) over a list of serving.Request
+    specs. Returns (results as dicts, makespan seconds, final states or None)."""
+    n = len(requests)
+    reqs = (N.Request * n)()
+    outs = []
+    for i, r in enumerate(requests):
+        q = reqs[i]
+        q.dim = r.dim
+        for d in range(3):
+            q.nblocks[d] = r.nblocks[d]
+            q.periodic[d] = r.periodic[d]
+        q.cell_size = r.cell_size
+        q.material = N.Material.make(r.gamma, r.B)
+        q.cfl = r.cfl
+        q.t_end = r.t_end
+        q.max_steps = r.max_steps
+        q.ic_type = r.ic_type
+        for k, v in enumerate(r.params):
+            q.ic_params[k] = v
+        q.n_params = len(r.params)
+        q.arrival_s = r.arrival_s
+        if keep_results:
+            nb = r.nblocks[0] * r.nblocks[1] * r.nblocks[2]
+            buf = np.zeros((nb, r.dim + 2) + block_shape(r.dim))
+            outs.append(buf)
+            q.h_result = buf.ctypes.data_as(C.POINTER(C.c_double))
+        else:
+            outs.append(None)
+    res = (N.Result * n)()
+    cfg = N.ServerConfig()
+    cfg.hbm_budget_bytes = int(hbm_budget_bytes)
+    cfg.share_3d = share_3d
+    cfg.scheme = N.Scheme.make(variant, precision)
+    cfg.max_cases = max_cases
+    cfg.steps_per_poll = steps_per_poll
+    cfg.one_at_a_time = int(one_at_a_time)
+    mk = C.c_double()
+    rc = N.lib().alp_serve(C.byref(cfg), reqs, n, res, C.byref(mk))
+    if rc not in (N.ALP_OK, N.ALP_ERR_CAPACITY):
+        N.check(rc)
+    results = [dict(arrival_s=x.arrival_s, admitted_s=x.admitted_s, finished_s=x.finished_s, t=x.t,
+                    steps=x.steps, status=x.status) for x in res]
+    return results, mk.value, (outs if keep_results else None)

@@ -13,10 +13,7 @@
 #include "../../include/alpaca_b200.h"
 #include "kernels.cuh"
 
-using namespace alp;
-
-namespace {
-
+namespace alp {
 thread_local std::string g_last_error;
 
 int fail(int code, std::string const &msg) {
@@ -27,12 +24,13 @@ int fail(int code, std::string const &msg) {
 int cuda_fail(cudaError_t e, char const *where) {
   return fail(ALP_ERR_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
+}  // namespace alp
 
-#define ALP_CUDA(call)                                   \
-  do {                                                   \
-    cudaError_t const e_ = (call);                       \
-    if (e_ != cudaSuccess) return cuda_fail(e_, #call);  \
-  } while (0)
+using namespace alp;
+
+#include "engine.hpp"
+
+namespace {
 
 int faces_of(int dim) {
   return 17 * (dim > 1 ? 17 : 2) * (dim > 2 ? 17 : 2);
@@ -219,120 +217,96 @@ int alp_rk3_stage(int dim, double *d_blocks, double *d_initial, const double *d_
 // engine
 // ---------------------------------------------------------------------------
 
-// The engine keeps every case in three block pools: A holds the state at the
-// start of a step (and at its end), B and C the first and second RK3 stages.
-// Stencils read neighbour blocks directly, so pool halos are only filled when
-// a case is exported.
-struct alp_engine {
-  int dim = 3, scheme = FV_CHAR, precision = FP64;
-  int capacity = 0, max_cases = 0;
-  int ne = 5, cells = 0, faces = 0;
-  double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
-  BlockMeta *meta = nullptr;
-  int *nbr26 = nullptr;
-  int *work = nullptr;
-  CaseState *cases = nullptr;
-  cudaStream_t stream = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  bool use_graph = true;
-  bool graph_dirty = true;
+namespace alp {
 
-  // host mirrors
-  std::vector<BlockMeta> h_meta;
-  std::vector<int> h_nbr26;
-  std::map<int, int> free_ranges;  // start -> length
-  struct CaseRec {
-    bool live = false;
-    int first = 0, nb = 0;
-  };
-  std::vector<CaseRec> case_rec;
-  std::vector<int> h_work;
-  int nwork = 0;
-
-  long long dstride() const { return (long long)ne * faces; }
-  long long stride() const { return dstride() * dim; }
-
-  // dt, then per stage one face-flux launch (all directions) and one
-  // divergence + stage-update launch: A -> B, (B, A) -> C, (C, A) -> A.
-  int record_step() {
-    Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
-    ALP_CUDA(launch_signal_speed(L, cases, nullptr));
-    ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
-    double *in[3] = {U, UB, UC};
-    double *out[3] = {UB, UC, U};
-    for (int s = 0; s < 3; ++s) {
-      Launch Ls = L;
-      Ls.U = in[s];
-      ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
-      ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
-    }
-    ALP_CUDA(launch_step_commit(cases, max_cases, stream));
-    return ALP_OK;
-  }
-
-  // work-list offset of a case's blocks (cases are listed in id order)
-  int work_offset(int cid) const {
-    int off = 0;
-    for (int c = 0; c < cid; ++c)
-      if (case_rec[c].live) off += case_rec[c].nb;
-    return off;
-  }
-
-  int rebuild_work() {
-    h_work.clear();
-    for (auto const &c : case_rec)
-      if (c.live)
-        for (int b = 0; b < c.nb; ++b) h_work.push_back(c.first + b);
-    nwork = (int)h_work.size();
-    if (nwork)
-      ALP_CUDA(cudaMemcpyAsync(work, h_work.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice,
-                               stream));
-    graph_dirty = true;
-    return ALP_OK;
-  }
-
-  int alloc_range(int n, int *first) {
-    for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
-      if (it->second >= n) {
-        *first = it->first;
-        int const rest = it->second - n, start = it->first + n;
-        free_ranges.erase(it);
-        if (rest > 0) free_ranges[start] = rest;
-        return ALP_OK;
+std::vector<int> regular_grid_neighbours(int dim, int const n[3], int const periodic[3]) {
+  int const nb = n[0] * n[1] * n[2];
+  std::vector<int> nbr((size_t)nb * 26, -1);
+  for (int b = 0; b < nb; ++b) {
+    int const c[3] = {b / (n[1] * n[2]), (b / n[2]) % n[1], b % n[2]};
+    int slot = 0;
+    for (int o = 0; o < 27; ++o) {
+      if (o == 13) continue;
+      int const off[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+      int q[3] = {c[0], c[1], c[2]};
+      bool ok = true;
+      for (int d = 0; d < 3 && ok; ++d) {
+        if (off[d] == 0) continue;
+        if (d >= dim) {
+          ok = false;
+          break;
+        }
+        q[d] += off[d];
+        if (q[d] < 0 || q[d] >= n[d]) {
+          if (periodic[d])
+            q[d] = (q[d] + n[d]) % n[d];
+          else
+            ok = false;
+        }
       }
+      if (ok) nbr[(size_t)b * 26 + slot] = (q[0] * n[1] + q[1]) * n[2] + q[2];
+      ++slot;
     }
-    return fail(ALP_ERR_CAPACITY, "no contiguous free block range of the requested size");
   }
+  return nbr;
+}
 
-  void free_range(int first, int n) {
-    auto it = free_ranges.emplace(first, n).first;
-    auto nx = std::next(it);
-    if (nx != free_ranges.end() && it->first + it->second == nx->first) {
-      it->second += nx->second;
-      free_ranges.erase(nx);
+int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_size, double cfl,
+                         double t0, double t_end, int max_steps, int nb, int const *h_nbr26,
+                         int *case_id, int *first_out) {
+  if (int rc = check_material(mat)) return rc;
+  if (!(cell_size > 0.0) || !(cfl > 0.0)) return fail(ALP_ERR_INVALID, "bad cell size / cfl");
+  for (size_t i = 0; i < (size_t)nb * 26; ++i)
+    if (h_nbr26[i] < -1 || h_nbr26[i] >= nb) return fail(ALP_ERR_INVALID, "neighbour out of range");
+  int cid = -1;
+  for (int c = 0; c < e->max_cases; ++c)
+    if (!e->case_rec[c].live) {
+      cid = c;
+      break;
     }
-    if (it != free_ranges.begin()) {
-      auto pv = std::prev(it);
-      if (pv->first + pv->second == it->first) {
-        pv->second += it->second;
-        free_ranges.erase(it);
-      }
+  if (cid < 0) return fail(ALP_ERR_CAPACITY, "case table full");
+  int first;
+  if (int rc = e->alloc_range(nb, &first)) return rc;
+  e->case_rec[cid] = {true, first, nb};
+  for (int b = 0; b < nb; ++b) {
+    e->h_meta[first + b] = meta_of(mat, cell_size, cid);
+    for (int s = 0; s < 26; ++s) {
+      int const n = h_nbr26[(size_t)b * 26 + s];
+      e->h_nbr26[(size_t)(first + b) * 26 + s] = n < 0 ? -1 : first + n;
     }
   }
+  ALP_CUDA(cudaMemcpyAsync(e->meta + first, e->h_meta.data() + first, sizeof(BlockMeta) * nb,
+                           cudaMemcpyHostToDevice, e->stream));
+  ALP_CUDA(cudaMemcpyAsync(e->nbr26 + (size_t)first * 26, e->h_nbr26.data() + (size_t)first * 26,
+                           sizeof(int) * 26 * nb, cudaMemcpyHostToDevice, e->stream));
+  CaseState cs{};
+  cs.t = t0;
+  cs.t_end = t_end;
+  cs.cfl = cfl;
+  cs.dt = 0.0;
+  cs.h_min = cell_size;
+  cs.smax_bits = 0ull;
+  cs.steps = 0;
+  cs.max_steps = max_steps;
+  cs.status = 0;
+  e->h_case_state[cid] = cs;
+  ALP_CUDA(cudaMemcpyAsync(e->cases + cid, &e->h_case_state[cid], sizeof(cs),
+                           cudaMemcpyHostToDevice, e->stream));
+  if (int rc = e->rebuild_work()) return rc;
+  *case_id = cid;
+  *first_out = first;
+  return ALP_OK;
+}
 
-  void release() {
-    if (graph) cudaGraphExecDestroy(graph);
-    cudaFree(U);
-    cudaFree(UB);
-    cudaFree(UC);
-    cudaFree(F);
-    cudaFree(meta);
-    cudaFree(nbr26);
-    cudaFree(work);
-    cudaFree(cases);
-    if (stream) cudaStreamDestroy(stream);
-  }
-};
+int engine_case_states(alp_engine *e, std::vector<CaseState> &out) {
+  out.resize(e->max_cases);
+  ALP_CUDA(cudaMemcpyAsync(out.data(), e->cases, sizeof(CaseState) * e->max_cases,
+                           cudaMemcpyDeviceToHost, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  return ALP_OK;
+}
+
+}  // namespace alp
 
 extern "C" {
 
@@ -390,6 +364,7 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   e->h_nbr26.assign((size_t)capacity_blocks * 26, -1);
   e->free_ranges[0] = capacity_blocks;
   e->case_rec.assign(max_cases, {});
+  e->h_case_state.assign(max_cases, CaseState{});
   *out = e;
   return ALP_OK;
 }
@@ -406,49 +381,46 @@ int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size
                         double t0, double t_end, int max_steps, int nb, const int *h_nbr26,
                         const double *h_blocks, int *case_id) {
   if (!e || !case_id) return fail(ALP_ERR_INVALID, "null argument");
-  if (int rc = check_material(mat)) return rc;
   if (nb <= 0 || !h_nbr26 || !h_blocks) return fail(ALP_ERR_INVALID, "bad case blocks");
-  if (!(cell_size > 0.0) || !(cfl > 0.0)) return fail(ALP_ERR_INVALID, "bad cell size / cfl");
-  for (size_t i = 0; i < (size_t)nb * 26; ++i)
-    if (h_nbr26[i] < -1 || h_nbr26[i] >= nb) return fail(ALP_ERR_INVALID, "neighbour out of range");
-  int cid = -1;
-  for (int c = 0; c < e->max_cases; ++c)
-    if (!e->case_rec[c].live) {
-      cid = c;
-      break;
-    }
-  if (cid < 0) return fail(ALP_ERR_CAPACITY, "case table full");
-  int first;
-  if (int rc = e->alloc_range(nb, &first)) return rc;
-  e->case_rec[cid] = {true, first, nb};
-  for (int b = 0; b < nb; ++b) {
-    e->h_meta[first + b] = meta_of(mat, cell_size, cid);
-    for (int s = 0; s < 26; ++s) {
-      int const n = h_nbr26[(size_t)b * 26 + s];
-      e->h_nbr26[(size_t)(first + b) * 26 + s] = n < 0 ? -1 : first + n;
-    }
-  }
+  int cid, first;
+  if (int rc = engine_add_case_core(e, mat, cell_size, cfl, t0, t_end, max_steps, nb, h_nbr26,
+                                    &cid, &first))
+    return rc;
   size_t const blk = (size_t)e->ne * e->cells;
   ALP_CUDA(cudaMemcpyAsync(e->U + blk * first, h_blocks, blk * nb * sizeof(double),
                            cudaMemcpyHostToDevice, e->stream));
-  ALP_CUDA(cudaMemcpyAsync(e->meta + first, e->h_meta.data() + first, sizeof(BlockMeta) * nb,
-                           cudaMemcpyHostToDevice, e->stream));
-  ALP_CUDA(cudaMemcpyAsync(e->nbr26 + (size_t)first * 26, e->h_nbr26.data() + (size_t)first * 26,
-                           sizeof(int) * 26 * nb, cudaMemcpyHostToDevice, e->stream));
-  CaseState cs{};
-  cs.t = t0;
-  cs.t_end = t_end;
-  cs.cfl = cfl;
-  cs.dt = 0.0;
-  cs.h_min = cell_size;
-  cs.smax_bits = 0ull;
-  cs.steps = 0;
-  cs.max_steps = max_steps;
-  cs.status = 0;
-  ALP_CUDA(cudaMemcpyAsync(e->cases + cid, &cs, sizeof(cs), cudaMemcpyHostToDevice, e->stream));
-  if (int rc = e->rebuild_work()) return rc;
   // the source may be pageable or reused by the caller right after the call
   ALP_CUDA(cudaStreamSynchronize(e->stream));
+  *case_id = cid;
+  return ALP_OK;
+}
+
+int alp_engine_add_case_ic(alp_engine *e, const alp_material *mat, double cell_size, double cfl,
+                           double t0, double t_end, int max_steps, const int *nblocks,
+                           const int *periodic, int ic_type, const double *ic_params,
+                           int n_params, int *case_id) {
+  if (!e || !case_id || !nblocks || !periodic || (n_params > 0 && !ic_params))
+    return fail(ALP_ERR_INVALID, "null argument");
+  if (ic_type != ALP_IC_QUADRANTS && ic_type != ALP_IC_BLAST)
+    return fail(ALP_ERR_INVALID, "unknown initial-condition type");
+  if (n_params < 0 || n_params > 24) return fail(ALP_ERR_INVALID, "at most 24 parameters");
+  if (ic_type == ALP_IC_QUADRANTS && e->dim != 2)
+    return fail(ALP_ERR_INVALID, "the four-quadrant problem is two-dimensional");
+  int n[3] = {1, 1, 1};
+  for (int d = 0; d < e->dim; ++d) {
+    if (nblocks[d] <= 0) return fail(ALP_ERR_INVALID, "block counts must be positive");
+    n[d] = nblocks[d];
+  }
+  std::vector<int> nbr = regular_grid_neighbours(e->dim, n, periodic);
+  int const nb = n[0] * n[1] * n[2];
+  int cid, first;
+  if (int rc = engine_add_case_core(e, mat, cell_size, cfl, t0, t_end, max_steps, nb, nbr.data(),
+                                    &cid, &first))
+    return rc;
+  IcParams p{};
+  for (int i = 0; i < n_params; ++i) p.v[i] = ic_params[i];
+  ALP_CUDA(launch_initial_condition(e->dim, e->U, first, n, cell_size, mat->gamma,
+                                    mat->background_pressure, ic_type, p, e->stream));
   *case_id = cid;
   return ALP_OK;
 }
@@ -461,8 +433,9 @@ int alp_engine_remove_case(alp_engine *e, int case_id) {
   auto &c = e->case_rec[case_id];
   e->free_range(c.first, c.nb);
   c = {};
-  CaseState cs{};
-  ALP_CUDA(cudaMemcpyAsync(e->cases + case_id, &cs, sizeof(cs), cudaMemcpyHostToDevice, e->stream));
+  e->h_case_state[case_id] = CaseState{};
+  ALP_CUDA(cudaMemcpyAsync(e->cases + case_id, &e->h_case_state[case_id], sizeof(CaseState),
+                           cudaMemcpyHostToDevice, e->stream));
   return e->rebuild_work();
 }
 

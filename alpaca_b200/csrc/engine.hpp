@@ -1,0 +1,163 @@
+// Engine internals shared by the C ABI (capi.cu) and the request loop (server.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/alpaca_b200.h"
+#include "kernels.cuh"
+
+namespace alp {
+int fail(int code, std::string const &msg);
+int cuda_fail(cudaError_t e, char const *where);
+}  // namespace alp
+
+#define ALP_CUDA(call)                                        \
+  do {                                                        \
+    cudaError_t const e_ = (call);                            \
+    if (e_ != cudaSuccess) return alp::cuda_fail(e_, #call);  \
+  } while (0)
+
+using alp::BlockMeta;
+using alp::CaseState;
+using alp::Launch;
+using alp::FP64;
+using alp::FV_CHAR;
+using alp::fail;
+using alp::launch_face_flux_all;
+using alp::launch_stage_update;
+using alp::launch_signal_speed;
+using alp::launch_dt_finalize;
+using alp::launch_step_commit;
+
+// The engine keeps every case in three block pools: A holds the state at the
+// start of a step (and at its end), B and C the first and second RK3 stages.
+// Stencils read neighbour blocks directly, so pool halos are only filled when
+// a case is exported.
+struct alp_engine {
+  int dim = 3, scheme = FV_CHAR, precision = FP64;
+  int capacity = 0, max_cases = 0;
+  int ne = 5, cells = 0, faces = 0;
+  double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
+  BlockMeta *meta = nullptr;
+  int *nbr26 = nullptr;
+  int *work = nullptr;
+  CaseState *cases = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+  bool use_graph = true;
+  bool graph_dirty = true;
+
+  // host mirrors
+  std::vector<BlockMeta> h_meta;
+  std::vector<int> h_nbr26;
+  std::map<int, int> free_ranges;  // start -> length
+  struct CaseRec {
+    bool live = false;
+    int first = 0, nb = 0;
+  };
+  std::vector<CaseRec> case_rec;
+  std::vector<int> h_work;
+  std::vector<CaseState> h_case_state;  // staging for case records sent to the device
+  int nwork = 0;
+
+  long long dstride() const { return (long long)ne * faces; }
+  long long stride() const { return dstride() * dim; }
+
+  // dt, then per stage one face-flux launch (all directions) and one
+  // divergence + stage-update launch: A -> B, (B, A) -> C, (C, A) -> A.
+  int record_step() {
+    Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
+    ALP_CUDA(launch_signal_speed(L, cases, nullptr));
+    ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
+    double *in[3] = {U, UB, UC};
+    double *out[3] = {UB, UC, U};
+    for (int s = 0; s < 3; ++s) {
+      Launch Ls = L;
+      Ls.U = in[s];
+      ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
+      ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
+    }
+    ALP_CUDA(launch_step_commit(cases, max_cases, stream));
+    return ALP_OK;
+  }
+
+  // work-list offset of a case's blocks (cases are listed in id order)
+  int work_offset(int cid) const {
+    int off = 0;
+    for (int c = 0; c < cid; ++c)
+      if (case_rec[c].live) off += case_rec[c].nb;
+    return off;
+  }
+
+  int rebuild_work() {
+    h_work.clear();
+    for (auto const &c : case_rec)
+      if (c.live)
+        for (int b = 0; b < c.nb; ++b) h_work.push_back(c.first + b);
+    nwork = (int)h_work.size();
+    if (nwork)
+      ALP_CUDA(cudaMemcpyAsync(work, h_work.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice,
+                               stream));
+    graph_dirty = true;
+    return ALP_OK;
+  }
+
+  int alloc_range(int n, int *first) {
+    for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
+      if (it->second >= n) {
+        *first = it->first;
+        int const rest = it->second - n, start = it->first + n;
+        free_ranges.erase(it);
+        if (rest > 0) free_ranges[start] = rest;
+        return ALP_OK;
+      }
+    }
+    return fail(ALP_ERR_CAPACITY, "no contiguous free block range of the requested size");
+  }
+
+  void free_range(int first, int n) {
+    auto it = free_ranges.emplace(first, n).first;
+    auto nx = std::next(it);
+    if (nx != free_ranges.end() && it->first + it->second == nx->first) {
+      it->second += nx->second;
+      free_ranges.erase(nx);
+    }
+    if (it != free_ranges.begin()) {
+      auto pv = std::prev(it);
+      if (pv->first + pv->second == it->first) {
+        pv->second += it->second;
+        free_ranges.erase(it);
+      }
+    }
+  }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    cudaFree(U);
+    cudaFree(UB);
+    cudaFree(UC);
+    cudaFree(F);
+    cudaFree(meta);
+    cudaFree(nbr26);
+    cudaFree(work);
+    cudaFree(cases);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+
+namespace alp {
+// Neighbour table (26 directions, x slowest; -1 = domain face) of a regular
+// nx x ny x nz block grid in C order, periodic per dimension.
+std::vector<int> regular_grid_neighbours(int dim, int const n[3], int const periodic[3]);
+// Adds a case's blocks, metadata and state record; returns its id and first slot.
+int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_size, double cfl,
+                         double t0, double t_end, int max_steps, int nb, int const *nbr26,
+                         int *case_id, int *first);
+// Copies the device case table to host.
+int engine_case_states(alp_engine *e, std::vector<CaseState> &out);
+}  // namespace alp

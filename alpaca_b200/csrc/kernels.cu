@@ -772,6 +772,57 @@ __global__ void step_commit_kernel(CaseState *cases, int n) {
 
 }  // namespace
 
+// Initial conditions evaluated on the device for a regular block grid whose
+// blocks occupy consecutive slots from `first` in C order (x slowest). Cell
+// centres are ((block index * 16 + i + 0.5) * cell_size, ...). Prime states
+// are converted with PrimeStatesToConservatives (prime_state_handler.h:195-275).
+// Every cell of the block (halos too) is written; halos are refreshed before
+// they are read.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+initial_condition_kernel(double *__restrict__ U, int first, int nbx, int nby, int nbz,
+                         double cell_size, double gamma, double B, int type,
+                         IcParams params) {
+  using G = Geo<DIM>;
+  int const b = blockIdx.x;
+  int const bx = b / (nby * nbz), by = (b / nbz) % nby, bz = b % nbz;
+  double *ub = U + (size_t)(first + b) * G::BLOCK_DOUBLES;
+  Eos const eos{gamma, B, 0};
+  for (int x = threadIdx.x; x < G::CELLS; x += blockDim.x) {
+    int const k = x % G::TCZ, j = (x / G::TCZ) % G::TCY, i = x / (G::TCZ * G::TCY);
+    double pos[3] = {0.0, 0.0, 0.0};
+    pos[0] = (bx * IC + i - HS + 0.5) * cell_size;
+    if (DIM > 1) pos[1] = (by * IC + j - HS + 0.5) * cell_size;
+    if (DIM > 2) pos[2] = (bz * IC + k - HS + 0.5) * cell_size;
+    double const *q = params.v;
+    double rho, p, vel[3] = {0.0, 0.0, 0.0};
+    if (type == IC_QUADRANTS) {
+      // q: x0, y0, then (rho, u, v, p) for quadrants (x<x0,y<y0), (x>=x0,y<y0),
+      // (x<x0,y>=y0), (x>=x0,y>=y0)
+      int const quad = (pos[0] >= q[0] ? 1 : 0) + (pos[1] >= q[1] ? 2 : 0);
+      double const *s = q + 2 + 4 * quad;
+      rho = s[0];
+      vel[0] = s[1];
+      vel[1] = s[2];
+      p = s[3];
+    } else {
+      // IC_BLAST: q: centre (3), radius, (rho, p) inside, (rho, p) outside
+      double r2 = 0.0;
+      for (int d = 0; d < DIM; ++d) r2 += (pos[d] - q[d]) * (pos[d] - q[d]);
+      bool const in = r2 < q[3] * q[3];
+      rho = in ? q[4] : q[6];
+      p = in ? q[5] : q[7];
+    }
+    double c[G::NE];
+    c[MASS] = rho;
+#pragma unroll
+    for (int d = 0; d < DIM; ++d) c[MOMX + d] = vel[d] * rho;
+    c[ENERGY] = eos_energy<DIM, double>(eos, rho, vel[0], vel[1], vel[2], p);
+#pragma unroll
+    for (int f = 0; f < G::NE; ++f) ub[f * G::CELLS + x] = c[f];
+  }
+}
+
 // ---------------------------------------------------------------------------
 // launchers
 // ---------------------------------------------------------------------------
@@ -963,6 +1014,21 @@ cudaError_t launch_signal_speed(Launch const &L, CaseState *cases, unsigned long
     case 1: signal_speed_kernel<1><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
     case 2: signal_speed_kernel<2><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
     case 3: signal_speed_kernel<3><<<grid, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, cases, out); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_initial_condition(int dim, double *U, int first, int const nblocks[3],
+                                     double cell_size, double gamma, double B, int type,
+                                     IcParams const &params, cudaStream_t stream) {
+  int const nb = nblocks[0] * nblocks[1] * nblocks[2];
+  if (nb <= 0) return cudaSuccess;
+  if (type != IC_QUADRANTS && type != IC_BLAST) return cudaErrorInvalidValue;
+  switch (dim) {
+    case 1: initial_condition_kernel<1><<<nb, 256, 0, stream>>>(U, first, nblocks[0], nblocks[1], nblocks[2], cell_size, gamma, B, type, params); break;
+    case 2: initial_condition_kernel<2><<<nb, 256, 0, stream>>>(U, first, nblocks[0], nblocks[1], nblocks[2], cell_size, gamma, B, type, params); break;
+    case 3: initial_condition_kernel<3><<<nb, 256, 0, stream>>>(U, first, nblocks[0], nblocks[1], nblocks[2], cell_size, gamma, B, type, params); break;
     default: return cudaErrorInvalidValue;
   }
   return cudaGetLastError();

@@ -77,6 +77,17 @@ cudaError_t launch_prime_states(Launch const &L, double *P);
 cudaError_t launch_signal_speed(Launch const &L, CaseState *cases,
                                 unsigned long long *smax_bits_out);
 
+// Device-evaluated initial conditions (parameters by value).
+enum IcType { IC_QUADRANTS = 1, IC_BLAST = 2 };
+struct IcParams {
+  double v[24];
+};
+// Fills the nblocks[0] x nblocks[1] x nblocks[2] blocks stored from slot
+// `first` (C order) with the initial condition `type` (stiffened gas gamma, B).
+cudaError_t launch_initial_condition(int dim, double *U, int first, int const nblocks[3],
+                                     double cell_size, double gamma, double B, int type,
+                                     IcParams const &params, cudaStream_t stream);
+
 // dt for every case from its smax (ComputeTimestepSize), then resets smax.
 cudaError_t launch_dt_finalize(CaseState *cases, int ncases, cudaStream_t stream);
 // t += dt, steps += (dt > 0) for every case.

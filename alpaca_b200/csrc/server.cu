@@ -1,0 +1,182 @@
+// Request loop of the serving form (alp_serve, include/alpaca_b200.h).
+//
+// Continuous batching over the engines: cases arrive on a wall-clock
+// schedule, are admitted as soon as their blocks fit into the engine pool of
+// their dimension (FIFO order with backfill: a later request that fits is
+// admitted while an earlier one waits for room), advance together in the
+// engine's batched step (one launch per kernel for all resident blocks of all
+// cases, each case with its own dt), and leave the pool when their end time or
+// step budget is reached. The 2D and 3D engines step on their own streams, so
+// their work overlaps on the device. Device memory is sized once from the HBM
+// budget; nothing is allocated while serving.
+#include <algorithm>
+#include <chrono>
+#include <deque>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "engine.hpp"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Active {
+  int req;
+};
+
+struct DimPool {
+  alp_engine *eng = nullptr;
+  std::vector<int> req_of_case;  // case id -> request index (-1 free)
+  int active = 0;
+};
+
+}  // namespace
+
+extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, int n,
+                         alp_result *results, double *makespan_s) {
+  using namespace alp;
+  if (!cfg || (n > 0 && (!reqs || !results))) return fail(ALP_ERR_INVALID, "null argument");
+  if (cfg->steps_per_poll <= 0 || cfg->max_cases <= 0)
+    return fail(ALP_ERR_INVALID, "steps_per_poll and max_cases must be positive");
+  if (!(cfg->share_3d >= 0.0 && cfg->share_3d <= 1.0))
+    return fail(ALP_ERR_INVALID, "share_3d must lie in [0, 1]");
+  bool need[4] = {false, false, false, false};
+  for (int i = 0; i < n; ++i) {
+    if (reqs[i].dim < 1 || reqs[i].dim > 3) return fail(ALP_ERR_INVALID, "request dim");
+    need[reqs[i].dim] = true;
+  }
+  // size the pools from the budget
+  DimPool pool[4];
+  auto cleanup = [&]() {
+    for (auto &p : pool)
+      if (p.eng) alp_engine_destroy(p.eng);
+  };
+  double const share[4] = {0.0, 0.0, 1.0 - cfg->share_3d, cfg->share_3d};
+  for (int d = 1; d <= 3; ++d) {
+    if (!need[d]) continue;
+    double const s = d == 1 ? 1.0 : (need[2] && need[3] ? share[d] : 1.0);
+    size_t const per_block = alp_engine_bytes(d, 1, 0);
+    size_t const cap = (size_t)(s * (double)cfg->hbm_budget_bytes) / per_block;
+    if (cap < 1) {
+      cleanup();
+      return fail(ALP_ERR_CAPACITY, "HBM budget below one block");
+    }
+    if (int rc = alp_engine_create(d, &cfg->scheme, (int)std::min<size_t>(cap, 1 << 30),
+                                   cfg->max_cases, &pool[d].eng)) {
+      cleanup();
+      return rc;
+    }
+    pool[d].req_of_case.assign(cfg->max_cases, -1);
+  }
+
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](int a, int b) { return reqs[a].arrival_s < reqs[b].arrival_s; });
+  std::deque<int> queue;
+  int next = 0, done = 0;
+  Clock::time_point const t0 = Clock::now();
+  auto elapsed = [&]() { return std::chrono::duration<double>(Clock::now() - t0).count(); };
+  std::vector<CaseState> states;
+  int rc_all = ALP_OK;
+
+  while (done < n) {
+    double const now = elapsed();
+    while (next < n && reqs[order[next]].arrival_s <= now) queue.push_back(order[next++]);
+
+    // admission: FIFO with backfill; one-at-a-time admits only into an idle GPU
+    int total_active = 0;
+    for (auto &p : pool) total_active += p.active;
+    for (auto it = queue.begin(); it != queue.end();) {
+      if (cfg->one_at_a_time && total_active > 0) break;
+      alp_request const &r = reqs[*it];
+      DimPool &p = pool[r.dim];
+      int cid = -1;
+      int const rc = alp_engine_add_case_ic(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
+                                            r.max_steps, r.nblocks, r.periodic, r.ic_type,
+                                            r.ic_params, r.n_params, &cid);
+      if (rc == ALP_OK) {
+        p.req_of_case[cid] = *it;
+        ++p.active;
+        ++total_active;
+        results[*it].arrival_s = r.arrival_s;
+        results[*it].admitted_s = elapsed();
+        it = queue.erase(it);
+      } else if (rc == ALP_ERR_CAPACITY) {
+        if (total_active == 0 && it == queue.begin()) {
+          // does not fit even into an empty pool: fail the request
+          results[*it] = alp_result{r.arrival_s, now, now, 0.0, 0, ALP_ERR_CAPACITY};
+          ++done;
+          it = queue.erase(it);
+          rc_all = ALP_ERR_CAPACITY;
+        } else {
+          ++it;
+        }
+      } else {
+        cleanup();
+        return rc;
+      }
+    }
+
+    if (total_active == 0) {
+      if (next < n && queue.empty()) {
+        double const wait = reqs[order[next]].arrival_s - elapsed();
+        if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 1e-3)));
+      }
+      continue;
+    }
+
+    // advance every pool with resident cases (asynchronous, one stream each)
+    for (auto &p : pool)
+      if (p.active > 0) {
+        if (int rc = alp_engine_step(p.eng, cfg->steps_per_poll)) {
+          cleanup();
+          return rc;
+        }
+      }
+    // retire finished cases
+    for (auto &p : pool) {
+      if (p.active == 0) continue;
+      if (int rc = engine_case_states(p.eng, states)) {
+        cleanup();
+        return rc;
+      }
+      double const t_now = elapsed();
+      for (int c = 0; c < cfg->max_cases; ++c) {
+        int const ri = p.req_of_case[c];
+        if (ri < 0) continue;
+        CaseState const &s = states[c];
+        bool const finished = !(s.t < s.t_end) || (s.max_steps > 0 && s.steps >= s.max_steps) ||
+                              s.status != 0;
+        if (!finished) continue;
+        alp_request const &r = reqs[ri];
+        alp_result &out = results[ri];
+        out.finished_s = t_now;
+        out.t = s.t;
+        out.steps = s.steps;
+        out.status = s.status ? ALP_ERR_NUMERIC : ALP_OK;
+        if (r.h_result) {
+          double t;
+          int st;
+          int const grc = alp_engine_get_case(p.eng, c, r.h_result, &t, &st);
+          if (grc != ALP_OK && grc != ALP_ERR_NUMERIC) {
+            cleanup();
+            return grc;
+          }
+        }
+        if (int rc = alp_engine_remove_case(p.eng, c)) {
+          cleanup();
+          return rc;
+        }
+        p.req_of_case[c] = -1;
+        --p.active;
+        ++done;
+      }
+    }
+  }
+  if (makespan_s) *makespan_s = elapsed();
+  cleanup();
+  return rc_all;
+}

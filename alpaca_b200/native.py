@@ -68,6 +68,28 @@ class Material(C.Structure):
         return cls(gamma, B, int(safe))
 
 
+IC_QUADRANTS, IC_BLAST = 1, 2
+
+
+class Request(C.Structure):
+    """alp_request: one served case (device-evaluated initial condition)."""
+    _fields_ = [("dim", C.c_int), ("nblocks", C.c_int * 3), ("periodic", C.c_int * 3),
+                ("cell_size", C.c_double), ("material", Material), ("cfl", C.c_double),
+                ("t_end", C.c_double), ("max_steps", C.c_int), ("ic_type", C.c_int),
+                ("ic_params", C.c_double * 24), ("n_params", C.c_int), ("arrival_s", C.c_double),
+                ("h_result", C.POINTER(C.c_double))]
+
+
+class Result(C.Structure):
+    _fields_ = [("arrival_s", C.c_double), ("admitted_s", C.c_double), ("finished_s", C.c_double),
+                ("t", C.c_double), ("steps", C.c_int), ("status", C.c_int)]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("share_3d", C.c_double), ("scheme", Scheme),
+                ("max_cases", C.c_int), ("steps_per_poll", C.c_int), ("one_at_a_time", C.c_int)]
+
+
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
 _V = C.c_void_p
@@ -91,6 +113,10 @@ _SIGS = {
     "alp_engine_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
     "alp_engine_add_case": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _I, _D, _I]),
+    "alp_engine_add_case_ic": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_int, _I, _I, C.c_int, _D, C.c_int, _I]),
+    "alp_serve": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(Request), C.c_int, C.POINTER(Result),
+                            _D]),
     "alp_engine_remove_case": (C.c_int, [_V, C.c_int]),
     "alp_engine_step": (C.c_int, [_V, C.c_int]),
     "alp_engine_get_case": (C.c_int, [_V, C.c_int, _D, _D, _I]),

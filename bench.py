@@ -43,6 +43,10 @@ def parse():
                    help="fp32: FP32 reconstruction/Riemann arithmetic, FP64 state")
     p.add_argument("--blocks", type=int, default=8, help="blocks per dimension")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-serving", action="store_true")
+    p.add_argument("--serving-requests", type=int, default=32)
+    p.add_argument("--serving-only", action="store_true",
+                   help="run only the serving comparison and print its JSON")
     p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
@@ -210,6 +214,36 @@ def fp64_peak():
     return v.value
 
 
+def serving_report(args):
+    """Serving form: one seeded request stream (2D four-quadrant problems and 3D
+    gas / water blasts, log-uniform 4-2048 blocks, 200-2000 steps, Poisson
+    arrivals at 50/s) served one case at a time in FP64, and with continuous
+    batching in FP64 and in the FP32-flux form; time-to-solution percentiles
+    and cases/s per mode."""
+    import numpy as np
+
+    from alpaca_b200 import api, serving
+    from alpaca_b200 import native as N
+    reqs = serving.request_stream(args.serving_requests, seed=11, rate_hz=50.0)
+    budget = 160 << 30
+    out = {"requests": len(reqs), "arrival_rate_hz": 50.0, "hbm_budget_gb": 160,
+           "mix": {k: sum(1 for r in reqs if r.kind == k) for k in
+                   ("quadrants2d", "blast3d_gas", "blast3d_water")},
+           "cell_updates": int(sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs))}
+    for name, prec, one in (("one_at_a_time_fp64", N.FP64, True), ("batched_fp64", N.FP64, False),
+                            ("batched_fp32_flux", N.FP32_FLUX, False)):
+        res, mk, _ = api.serve(reqs, budget, precision=prec, one_at_a_time=one)
+        tts = np.array([r["finished_s"] - r["arrival_s"] for r in res])
+        ok = sum(1 for r in res if r["status"] == 0)
+        out[name] = {"cases_per_s": ok / mk, "makespan_s": mk, "p50_tts_s": float(np.percentile(tts, 50)),
+                     "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok,
+                     "cell_updates_per_s": out["cell_updates"] / mk}
+    base = out["one_at_a_time_fp64"]["cases_per_s"]
+    for k in ("batched_fp64", "batched_fp32_flux"):
+        out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base
+    return out
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -289,6 +323,9 @@ def run_ours(args, ws, rank, local):
         cpu = reference_cpu_sample(args.variant, 15.0, os.cpu_count() or 1)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     clk = clocks.summary()
+    serv = None
+    if not args.no_serving and ws == 1:
+        serv = serving_report(args)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
@@ -309,6 +346,7 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk,
+        "serving": serv,
     }
     print(json.dumps(line), flush=True)
 
@@ -319,6 +357,10 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, ws, rank)
+        elif args.serving_only:
+            import torch
+            torch.cuda.set_device(local)
+            print(json.dumps(serving_report(args)), flush=True)
         else:
             run_ours(args, ws, rank, local)
     finally:

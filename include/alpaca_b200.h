@@ -168,6 +168,24 @@ int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size
                         double t0, double t_end, int max_steps, int nb, const int *h_nbr26,
                         const double *h_blocks, int *case_id);
 
+/* Adds a case whose initial condition is evaluated on the device, on a
+ * regular grid of nblocks[0] x nblocks[1] x nblocks[2] blocks (entries past
+ * the engine's dimension ignored), periodic[d] != 0 wrapping dimension d and
+ * zero-gradient domain faces otherwise. Block (bx, by, bz) has index
+ * (bx * ny + by) * nz + bz; cell centres are ((16 b + i + 1/2) cell_size).
+ * Initial conditions (prime states converted with PrimeStatesToConservatives,
+ * prime_states/prime_state_handler.h:195-275):
+ *   ALP_IC_QUADRANTS (2D): params x0, y0, then rho, u, v, p of the quadrants
+ *     (x<x0, y<y0), (x>=x0, y<y0), (x<x0, y>=y0), (x>=x0, y>=y0)   (18 values)
+ *   ALP_IC_BLAST: params centre x, y, z, radius, rho and p inside, rho and p
+ *     outside, at rest                                               (8 values)
+ * Nothing is copied from the host but the parameters (at most 24). */
+enum { ALP_IC_QUADRANTS = 1, ALP_IC_BLAST = 2 };
+int alp_engine_add_case_ic(alp_engine *e, const alp_material *mat, double cell_size, double cfl,
+                           double t0, double t_end, int max_steps, const int *nblocks,
+                           const int *periodic, int ic_type, const double *ic_params,
+                           int n_params, int *case_id);
+
 /* Removes a case and frees its blocks. */
 int alp_engine_remove_case(alp_engine *e, int case_id);
 
@@ -192,6 +210,57 @@ int alp_engine_set_graph(alp_engine *e, int enabled);
 
 /* Number of kernel launches one engine step issues. */
 int alp_engine_launches_per_step(alp_engine *e);
+
+/* ---- serving: continuous batching of independent cases ------------------ */
+
+/* One request: a case on a regular block grid with a device-evaluated initial
+ * condition (see alp_engine_add_case_ic), arriving arrival_s seconds after
+ * alp_serve starts. h_result, when not null, receives the final state
+ * (reference layout, halos filled) before the case leaves the pool. */
+typedef struct {
+  int dim;
+  int nblocks[3];
+  int periodic[3];
+  double cell_size;
+  alp_material material;
+  double cfl;
+  double t_end;
+  int max_steps;
+  int ic_type;
+  double ic_params[24];
+  int n_params;
+  double arrival_s;
+  double *h_result;
+} alp_request;
+
+/* Wall-clock times are seconds after the start of alp_serve. */
+typedef struct {
+  double arrival_s;
+  double admitted_s;
+  double finished_s;
+  double t;       /* simulated time reached */
+  int steps;      /* SSP-RK3 steps taken */
+  int status;     /* ALP_OK, ALP_ERR_NUMERIC or ALP_ERR_CAPACITY */
+} alp_result;
+
+typedef struct {
+  size_t hbm_budget_bytes;  /* device memory for case state (all engines) */
+  double share_3d;          /* fraction of the budget given to 3D blocks when both occur */
+  alp_scheme scheme;
+  int max_cases;            /* resident cases per dimension */
+  int steps_per_poll;       /* steps between completion checks */
+  int one_at_a_time;        /* 1: admit a case only into an idle GPU (baseline) */
+} alp_server_config;
+
+/* Serves n requests: admits arrived requests whose blocks fit (FIFO with
+ * backfill), advances all resident cases in the engines' batched steps (2D and
+ * 3D on separate streams), retires finished cases. Blocks until every request
+ * has finished; results[i] belongs to reqs[i]. *makespan_s (may be null)
+ * receives the wall time from start to the last completion. Returns ALP_OK, or
+ * ALP_ERR_CAPACITY when a request could not fit into an empty pool (its result
+ * carries that status; the others are served). */
+int alp_serve(const alp_server_config *cfg, const alp_request *reqs, int n, alp_result *results,
+              double *makespan_s);
 
 #ifdef __cplusplus
 }

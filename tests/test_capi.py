@@ -60,3 +60,44 @@ def test_workspace_and_engine_sizes(dim):
     cells = 24 ** dim
     per_block = 2 * (dim + 2) * cells * 8 + dim * (dim + 2) * faces * 8
     assert lib.alp_engine_bytes(dim, 10, 2) >= 10 * per_block
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """ctypes mirrors of the ABI structs have the C sizes and field offsets."""
+    import os
+    import subprocess
+    src = tmp_path / "sizes.c"
+    src.write_text(
+        '#include <stdio.h>\n#include <stddef.h>\n#include "alpaca_b200.h"\n'
+        'int main(void){printf("%zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(alp_scheme),'
+        ' sizeof(alp_material), sizeof(alp_request), sizeof(alp_result), sizeof(alp_server_config),'
+        ' offsetof(alp_request, ic_params), offsetof(alp_request, arrival_s),'
+        ' offsetof(alp_server_config, scheme)); return 0;}\n')
+    inc = os.path.join(os.path.dirname(N.HEADER))
+    exe = tmp_path / "sizes"
+    subprocess.run(["gcc", "-I", inc, str(src), "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    want = [C.sizeof(N.Scheme), C.sizeof(N.Material), C.sizeof(N.Request), C.sizeof(N.Result),
+            C.sizeof(N.ServerConfig), N.Request.ic_params.offset, N.Request.arrival_s.offset,
+            N.ServerConfig.scheme.offset]
+    assert got == want
+
+
+def test_serve_rejects_bad_config_without_gpu():
+    cfg = N.ServerConfig()
+    cfg.steps_per_poll = 0
+    cfg.max_cases = 4
+    rc = N.lib().alp_serve(C.byref(cfg), None, 0, None, None)
+    assert rc == N.ALP_ERR_INVALID
+
+
+def test_request_stream_is_seeded_and_in_range():
+    from alpaca_b200 import serving
+    a = serving.request_stream(40, seed=3)
+    b = serving.request_stream(40, seed=3)
+    assert [(r.kind, r.nblocks, r.max_steps) for r in a] == [(r.kind, r.nblocks, r.max_steps) for r in b]
+    assert all(1 <= r.blocks <= 2600 and 200 <= r.max_steps <= 2000 for r in a)
+    assert all(a[i].arrival_s < a[i + 1].arrival_s for i in range(39))
+    water = [r for r in a if r.kind == "blast3d_water"]
+    assert water and abs(water[0].B - 3430.0) < 1e-9 and water[0].gamma == 6.12

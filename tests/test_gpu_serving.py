@@ -1,0 +1,123 @@
+"""Device-evaluated initial conditions and the serving request loop (alp_serve)."""
+import numpy as np
+import pytest
+
+import oracle
+from alpaca_b200 import api, cases, serving
+from alpaca_b200 import native as N
+from helpers import l1_rel
+
+pytestmark = pytest.mark.gpu
+
+
+def host_ic(req: serving.Request) -> np.ndarray:
+    """The request's initial condition evaluated with numpy (same formulas)."""
+    dim = req.dim
+    g = cases.BlockGrid(dim, req.nblocks[:dim], tuple(bool(p) for p in req.periodic[:dim]),
+                        req.cell_size)
+    x = g.cell_centres()
+    q = req.params
+    if req.ic_type == N.IC_QUADRANTS:
+        quad = (x[0] >= q[0]).astype(int) + 2 * (x[1] >= q[1]).astype(int)
+        s = np.array(q[2:18]).reshape(4, 4)
+        rho, u, v, p = (s[quad, i] for i in range(4))
+        vel = [u, v]
+    else:
+        r2 = sum((x[d] - q[d]) ** 2 for d in range(dim))
+        inside = r2 < q[3] * q[3]
+        rho = np.where(inside, q[4], q[6])
+        p = np.where(inside, q[5], q[7])
+        vel = [np.zeros_like(rho) for _ in range(dim)]
+    glob = cases.primes_to_conservatives(dim, rho, p, vel, req.gamma, req.B)
+    return g.scatter(glob), g
+
+
+@pytest.mark.parametrize("kind", ["quadrants", "blast_gas", "blast_water"])
+def test_device_initial_condition_matches_host(cuda, kind):
+    rng = np.random.default_rng(4)
+    if kind == "quadrants":
+        req = serving.quadrant_request(rng, 6, 5)
+    else:
+        req = serving.blast_request(rng, 8, 5, water=kind == "blast_water")
+    u_host, g = host_ic(req)
+    eng = api.Engine(req.dim, "fvchar", capacity_blocks=g.nb, max_cases=1)
+    cid = eng.add_case_ic(req.ic_type, req.params, req.nblocks, req.cell_size,
+                          N.Material.make(req.gamma, req.B), max_steps=5)
+    u_dev = eng.get(cid)[0]
+    I = cases.interior(req.dim)
+    np.testing.assert_allclose(u_dev[I], u_host[I], rtol=1e-15, atol=0)
+    # the device-generated case steps exactly like the oracle on the same state
+    eng.run_to_end(chunk=5)
+    got, t, steps = eng.get(cid)
+    eng.close()
+    ref = oracle.Restatement(req.dim, "fvchar").run(u_dev, g.nbr, req.gamma, req.B, False,
+                                                    req.cell_size, 0.6, 1e300, max_steps=5)[0]
+    assert steps == 5
+    for f in range(req.dim + 2):
+        assert l1_rel(got[I][:, f], ref[I][:, f]) <= 1e-12
+
+
+def small_stream(seed=2):
+    rng = np.random.default_rng(seed)
+    reqs = [serving.quadrant_request(rng, 4, 30), serving.blast_request(rng, 8, 20, water=False),
+            serving.blast_request(rng, 27, 12, water=True), serving.quadrant_request(rng, 12, 25),
+            serving.blast_request(rng, 8, 16, water=False)]
+    for i, r in enumerate(reqs):
+        r.arrival_s = 0.002 * i
+    return reqs
+
+
+def test_serving_mix_equals_alone(cuda):
+    """Continuous batching gives each case the same bits it gets alone."""
+    reqs = small_stream()
+    budget = 2 << 30
+    mix, _, states_mix = api.serve(reqs, budget, keep_results=True)
+    alone, _, states_alone = api.serve(reqs, budget, one_at_a_time=True, keep_results=True)
+    for i, r in enumerate(reqs):
+        assert mix[i]["status"] == 0 and alone[i]["status"] == 0
+        assert mix[i]["steps"] == alone[i]["steps"] == r.max_steps
+        assert np.array_equal(states_mix[i][cases.interior(r.dim)],
+                              states_alone[i][cases.interior(r.dim)]), i
+    # one at a time: no two cases resident together
+    spans = sorted((x["admitted_s"], x["finished_s"]) for x in alone)
+    for (a0, f0), (a1, _) in zip(spans, spans[1:]):
+        assert a1 >= f0
+    # batched: cases overlap on the device
+    mspans = sorted((x["admitted_s"], x["finished_s"]) for x in mix)
+    assert any(a1 < f0 for (a0, f0), (a1, _) in zip(mspans, mspans[1:]))
+
+
+def test_serving_budget_bounds_admission(cuda):
+    """With a budget for one 8-block 3D case, requests are admitted one after
+    the other and all complete."""
+    rng = np.random.default_rng(9)
+    reqs = [serving.blast_request(rng, 8, 6, water=False) for _ in range(3)]
+    per_block = N.lib().alp_engine_bytes(3, 1, 0)
+    res, makespan, _ = api.serve(reqs, 9 * per_block, share_3d=1.0)
+    assert all(r["status"] == 0 and r["steps"] == 6 for r in res)
+    spans = sorted((x["admitted_s"], x["finished_s"]) for x in res)
+    for (a0, f0), (a1, _) in zip(spans, spans[1:]):
+        assert a1 >= f0
+    assert makespan >= spans[-1][1]
+
+
+def test_serving_fp32_flux_within_target(cuda):
+    """The FP32-flux form serves the same cases within 1e-5 relative L1 density."""
+    reqs = small_stream(5)
+    budget = 2 << 30
+    r64, _, s64 = api.serve(reqs, budget, keep_results=True)
+    r32, _, s32 = api.serve(reqs, budget, precision=N.FP32_FLUX, keep_results=True)
+    for i, r in enumerate(reqs):
+        I = cases.interior(r.dim)
+        err = l1_rel(s32[i][I][:, 0], s64[i][I][:, 0])
+        assert r32[i]["steps"] == r64[i]["steps"] and err <= 1e-5, (i, err)
+
+
+def test_serving_request_too_large_is_reported(cuda):
+    rng = np.random.default_rng(1)
+    big = serving.blast_request(rng, 64, 3, water=False)
+    small = serving.blast_request(rng, 1, 3, water=False)
+    per_block = N.lib().alp_engine_bytes(3, 1, 0)
+    res, _, _ = api.serve([big, small], 8 * per_block, share_3d=1.0)
+    assert res[0]["status"] == N.ALP_ERR_CAPACITY
+    assert res[1]["status"] == 0 and res[1]["steps"] == 3

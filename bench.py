@@ -45,6 +45,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serving-requests", type=int, default=32)
+    p.add_argument("--precision-report", action="store_true",
+                   help="FP32-flux vs FP64 errors per field after 200 steps (128^3, 256^3, water)")
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving comparison and print its JSON")
     p.add_argument("--no-e2e", action="store_true")
@@ -244,6 +246,39 @@ def serving_report(args):
     return out
 
 
+def precision_report(steps: int = 200):
+    """L1 and Linf error of every field of the FP32-flux form against the FP64
+    path after `steps` SSP-RK3 steps (the FP64 path is the one checked against
+    the reference: per RHS <= 1e-12, 100-step L1 <= 1e-10)."""
+    import numpy as np
+
+    from alpaca_b200 import api, cases
+    from alpaca_b200 import native as N
+    names = ["density", "energy", "momentum_x", "momentum_y", "momentum_z"]
+    rows = []
+    for label, case in (("ideal gas 128^3 (512 blocks)", cases.fourier_shock(8, 3, seed=1)),
+                        ("ideal gas 256^3 (4096 blocks)", cases.fourier_shock(16, 3, seed=1)),
+                        ("stiffened-gas water 128^3", cases.water_spheres(8, seed=3))):
+        for variant in ("fvchar", "fsroe"):
+            out = {}
+            for prec in (N.FP64, N.FP32_FLUX):
+                eng = api.Engine(3, variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
+                cid = eng.add_case(case, max_steps=steps)
+                eng.run_to_end(chunk=50)
+                out[prec] = eng.get(cid)
+                eng.close()
+            I = cases.interior(3)
+            a, b = out[N.FP32_FLUX][0][I], out[N.FP64][0][I]
+            err = {}
+            for f, nm in enumerate(names):
+                d = np.abs(a[:, f] - b[:, f])
+                err[nm] = {"l1": float(d.sum() / max(np.abs(b[:, f]).sum(), 1e-300)),
+                           "linf": float(d.max() / max(np.abs(b[:, f]).max(), 1e-300))}
+            rows.append({"case": label, "variant": variant, "steps": out[N.FP64][2],
+                         "t_fp64": out[N.FP64][1], "t_fp32": out[N.FP32_FLUX][1], "errors": err})
+    return rows
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -357,6 +392,11 @@ def main():
     try:
         if args.impl == "reference":
             run_reference_arm(args, ws, rank)
+        elif args.precision_report:
+            import torch
+            torch.cuda.set_device(local)
+            for row in precision_report():
+                print(json.dumps(row), flush=True)
         elif args.serving_only:
             import torch
             torch.cuda.set_device(local)

@@ -314,7 +314,11 @@ size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
   if (dim < 1 || dim > 3) return 0;
   size_t const ne = dim + 2;
   size_t const blk = ne * cells_of(dim) * sizeof(double);
+#ifdef ALP_STRICT
   size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double);
+#else
+  size_t const flux = ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
+#endif
   return (size_t)capacity_blocks *
              (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
          (size_t)max_cases * sizeof(CaseState);
@@ -346,7 +350,16 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   grab((void **)&e->U, blk * capacity_blocks * sizeof(double));
   grab((void **)&e->UB, blk * capacity_blocks * sizeof(double));
   grab((void **)&e->UC, blk * capacity_blocks * sizeof(double));
+  // The strict build reproduces the reference's three-order symmetric flux
+  // sum, so it keeps the face-flux arrays; the fast build sweeps pencils.
+#ifdef ALP_STRICT
+  e->path = 1;
   grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
+#else
+  e->path = 0;
+  grab((void **)&e->R, (size_t)e->ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) *
+                           capacity_blocks * sizeof(double));
+#endif
   grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
@@ -523,8 +536,9 @@ int alp_engine_set_graph(alp_engine *e, int enabled) {
 
 int alp_engine_launches_per_step(alp_engine *e) {
   if (!e) return 0;
-  // signal speed, dt, 3 x (face fluxes, stage update), commit
-  return 2 + 3 * 2 + 1;
+  // signal speed, dt, 3 stages x (one pencil sweep per direction, or face
+  // fluxes + stage update), commit
+  return 2 + 3 * (e->path == 0 ? e->dim : 2) + 1;
 }
 
 }  // extern "C"

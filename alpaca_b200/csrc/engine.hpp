@@ -41,7 +41,10 @@ struct alp_engine {
   int dim = 3, scheme = FV_CHAR, precision = FP64;
   int capacity = 0, max_cases = 0;
   int ne = 5, cells = 0, faces = 0;
-  double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
+  double *U = nullptr, *UB = nullptr, *UC = nullptr;
+  double *F = nullptr;  // face fluxes [slot][dim][NE][faces] (face-flux path)
+  double *R = nullptr;  // per-cell flux differences [slot][NE][interior] (pencil path)
+  int path = 0;         // 0: pencil sweeps, 1: face fluxes + stage update
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr;
   int *work = nullptr;
@@ -78,8 +81,12 @@ struct alp_engine {
     for (int s = 0; s < 3; ++s) {
       Launch Ls = L;
       Ls.U = in[s];
-      ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
-      ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
+      if (path == 0) {
+        ALP_CUDA(alp::launch_pencil_stage(Ls, U, out[s], R, nbr26, cases, s));
+      } else {
+        ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
+        ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
+      }
     }
     ALP_CUDA(launch_step_commit(cases, max_cases, stream));
     return ALP_OK;
@@ -141,6 +148,7 @@ struct alp_engine {
     cudaFree(UB);
     cudaFree(UC);
     cudaFree(F);
+    cudaFree(R);
     cudaFree(meta);
     cudaFree(nbr26);
     cudaFree(work);

@@ -22,6 +22,12 @@ __device__ __forceinline__ int slot_of(int const *work, int item) {
   return work ? work[item] : item;
 }
 
+// SSP-RK3 stage coefficients (runge_kutta_3_TVD.h:41-59): Uout = a0 U + a1 U0 +
+// c dt RHS (time_integrator.h:98-113, 434-457)
+__constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
+__constant__ double kRkA0[3] = {0.0, 0.25, 2.0 / 3.0};
+__constant__ double kRkA1[3] = {0.0, 0.75, 1.0 / 3.0};
+
 // Structural nonzeros of the left eigenvector matrix row n, column l
 // (eigendecomposition.h:316-359).
 template <int DIM, int DIR>
@@ -90,60 +96,55 @@ __device__ __forceinline__ void write_flux(double *__restrict__ F, int item, lon
   }
 }
 
-// Flux of the face with thread index t of direction DIR of the block in `slot`.
-// GATHER: stencil cells outside the interior along DIR come from the
-// neighbour blocks' interiors (nbr26; zero gradient at domain faces) instead of
-// the block's own halo cells, so no halo copy is needed between stages.
-template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER>
-__device__ __forceinline__ void face_flux(double const *__restrict__ U,
-                                          int const *__restrict__ nbr26, int slot, int item,
-                                          int t, BlockMeta const &bm, double *__restrict__ F,
-                                          long long stride) {
+// Stencil of the face a (between cells a-1 and a along DIR) at transverse
+// position (p1, p2): cells a-3 .. a+2 in interior numbering, all fields.
+// GATHER: cells outside the interior along DIR come from the neighbour blocks'
+// interiors (nbr26; zero gradient at domain faces) instead of the block's own
+// halo cells, so no halo copy is needed between stages.
+template <int DIM, int DIR, bool GATHER>
+__device__ __forceinline__ double const *stencil_cell(double const *__restrict__ U,
+                                                      double const *blk, int c, int cell0,
+                                                      int nlo, int nhi) {
+  using G = Geo<DIM>;
+  constexpr int step = DIR == 0 ? G::TCY * G::TCZ : (DIR == 1 ? G::TCZ : 1);
+  // cell0: offset of (transverse position, DIR index 0) in the block
+  if (GATHER && c < HS)
+    return nlo >= 0 ? U + (size_t)nlo * G::BLOCK_DOUBLES + cell0 + (c + IC) * step
+                    : blk + cell0 + HS * step;
+  if (GATHER && c >= HS + IC)
+    return nhi >= 0 ? U + (size_t)nhi * G::BLOCK_DOUBLES + cell0 + (c - IC) * step
+                    : blk + cell0 + (HS + IC - 1) * step;
+  return blk + cell0 + c * step;
+}
+
+template <int DIM, int DIR>
+__device__ __forceinline__ int line_origin(int p1, int p2) {
   using G = Geo<DIM>;
   using M = FaceMap<DIM, DIR>;
-  constexpr int NE = G::NE;
-  Eos const eos{bm.gamma, bm.B, bm.safe};
+  int c[3];
+  c[DIR] = 0;
+  c[M::O1] = G::fic(M::O1) + p1;
+  c[M::O2] = G::fic(M::O2) + p2;
+  return G::cell(c[0], c[1], c[2]);
+}
 
-  int a, p1, p2;
-  M::decode(t, a, p1, p2);
-  int c0[3];
-  c0[DIR] = HS + a - 3;
-  c0[M::O1] = G::fic(M::O1) + p1;
-  c0[M::O2] = G::fic(M::O2) + p2;
-  constexpr int step = DIR == 0 ? G::TCY * G::TCZ : (DIR == 1 ? G::TCZ : 1);
-  double const *blk = U + (size_t)slot * G::BLOCK_DOUBLES;
-  double const *ub = blk + G::cell(c0[0], c0[1], c0[2]);
+template <int DIM, int DIR>
+__device__ __forceinline__ void load_cell(double const *src, double (&dst)[DIM + 2]) {
+#pragma unroll
+  for (int f = 0; f < DIM + 2; ++f) dst[f] = __ldg(src + f * Geo<DIM>::CELLS);
+}
 
-  double cons[6][NE];
-  if constexpr (GATHER) {
-    // low / high neighbour along DIR (26-table slots of W,E / S,N / B,T)
-    constexpr int lo_slot = DIR == 0 ? 4 : (DIR == 1 ? 10 : 12);
-    constexpr int hi_slot = DIR == 0 ? 21 : (DIR == 1 ? 15 : 13);
-    int const nlo = a < 3 ? __ldg(nbr26 + (size_t)slot * 26 + lo_slot) : 0;
-    int const nhi = a > 13 ? __ldg(nbr26 + (size_t)slot * 26 + hi_slot) : 0;
-#pragma unroll
-    for (int m = 0; m < 6; ++m) {
-      int const c = HS + a - 3 + m;  // cell index along DIR
-      double const *src;
-      if (c < HS) {
-        src = nlo >= 0 ? U + (size_t)nlo * G::BLOCK_DOUBLES + ((ub - blk) + (c + IC - c0[DIR]) * step)
-                       : blk + ((ub - blk) + (HS - c0[DIR]) * step);
-      } else if (c >= HS + IC) {
-        src = nhi >= 0 ? U + (size_t)nhi * G::BLOCK_DOUBLES + ((ub - blk) + (c - IC - c0[DIR]) * step)
-                       : blk + ((ub - blk) + (HS + IC - 1 - c0[DIR]) * step);
-      } else {
-        src = ub + m * step;
-      }
-#pragma unroll
-      for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(src + f * G::CELLS);
-    }
-  } else {
-#pragma unroll
-    for (int m = 0; m < 6; ++m)
-#pragma unroll
-      for (int f = 0; f < NE; ++f) cons[m][f] = __ldg(ub + f * G::CELLS + m * step);
-  }
-
+// Flux of one face from its 6-cell stencil (the reference's per-face work:
+// FiniteVolumeScheme::ComputeFluxes<DIR> with the selected reconstruction and
+// HLLC, or FluxSplittingScheme::ComputeFluxes<DIR>). Writes the flux in double
+// to fd and returns false for a face the reference skips (invalid
+// reconstructed state, finite_volume_scheme.cpp:218-225) or whose Roe average
+// has a non-positive density (eigendecomposition.h:244).
+template <int DIM, int DIR, int SCHEME, typename T>
+__device__ __forceinline__ bool face_compute(Eos const &eos, double B,
+                                             double const (&cons)[6][DIM + 2],
+                                             double (&fd)[DIM + 2]) {
+  constexpr int NE = DIM + 2;
   T flux[NE];
   bool valid = true;
   constexpr int mP = MOMX + DIR;
@@ -192,11 +193,9 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
                                           DIM > 2 ? cm[MOMX + 2 * (DIM > 2)] : 0.0, cm[ENERGY], one_l);
       double const pp = eos_pressure<DIM>(eos, cp[MASS], cp[MOMX], DIM > 1 ? cp[MOMX + (DIM > 1)] : 0.0,
                                           DIM > 2 ? cp[MOMX + 2 * (DIM > 2)] : 0.0, cp[ENERGY], one_r);
-      if (!(pm > -bm.B) || !(pp > -bm.B)) valid = false;
-      double fd[NE];
+      if (!(pm > -B) || !(pp > -B)) valid = false;
       hllc_mixed<DIM, DIR>(eos, cm, cp, pm, pp, cm[mP] * one_l, cp[mP] * one_r, one_l, one_r, fd);
-      write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
-      return;
+      return valid;
     } else if constexpr (SCHEME == FV_CHAR) {
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
@@ -235,7 +234,7 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
                                           DIM > 1 ? double(cp[MOMX + (DIM > 1)]) : 0.0,
                                           DIM > 2 ? double(cp[MOMX + 2 * (DIM > 2)]) : 0.0,
                                           double(cp[ENERGY]), double(one_r));
-      if (!(pm > -bm.B) || !(pp > -bm.B)) valid = false;
+      if (!(pm > -B) || !(pp > -B)) valid = false;
       T const vl = cm[mP] * one_l;
       T const vr = cp[mP] * one_r;
       hllc<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
@@ -293,11 +292,9 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
       }
       to_physical<DIM, DIR, T>(r, ch[0], flux);
       if constexpr (DELTA) {
-        double fd[NE];
 #pragma unroll
         for (int f = 0; f < NE; ++f) fd[f] = advd[2][f] + double(flux[f]);
-        write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
-        return;
+        return valid;
       }
     }
   } else {
@@ -337,12 +334,10 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
       cp[ENERGY] = eos_energy<DIM, double>(eos, ppd[RHO], ppd[VELX], DIM > 1 ? ppd[VELX + (DIM > 1)] : 0.0,
                                            DIM > 2 ? ppd[VELX + 2 * (DIM > 2)] : 0.0, ppd[PRES]);
       if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
-      if (!(pmd[PRES] > -bm.B) || !(ppd[PRES] > -bm.B)) valid = false;
-      double fd[NE];
+      if (!(pmd[PRES] > -B) || !(ppd[PRES] > -B)) valid = false;
       hllc_mixed<DIM, DIR>(eos, cm, cp, pmd[PRES], ppd[PRES], pmd[VELX + DIR], ppd[VELX + DIR],
                            inv(cm[MASS]), inv(cp[MASS]), fd);
-      write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
-      return;
+      return valid;
     } else {
       T pm[NE], pp[NE];
 #pragma unroll
@@ -367,16 +362,44 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
       cp[ENERGY] = eos_energy<DIM, T>(eos, pp[RHO], pp[VELX], DIM > 1 ? pp[VELX + (DIM > 1)] : T(0),
                                       DIM > 2 ? pp[VELX + 2 * (DIM > 2)] : T(0), pp[PRES]);
       if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
-      if (!(double(pm[PRES]) > -bm.B) || !(double(pp[PRES]) > -bm.B)) valid = false;
+      if (!(double(pm[PRES]) > -B) || !(double(pp[PRES]) > -B)) valid = false;
       // HLLC's own 1/density (hllc_riemann_solver.h:75-78)
       hllc<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR],
                         inv(cm[MASS]), inv(cp[MASS]), flux);
     }
   }
 
-  double fd[NE];
 #pragma unroll
   for (int f = 0; f < NE; ++f) fd[f] = double(flux[f]);
+  return valid;
+}
+
+// Flux of the face with thread index t of direction DIR of the block in `slot`.
+template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER>
+__device__ __forceinline__ void face_flux(double const *__restrict__ U,
+                                          int const *__restrict__ nbr26, int slot, int item,
+                                          int t, BlockMeta const &bm, double *__restrict__ F,
+                                          long long stride) {
+  using G = Geo<DIM>;
+  using M = FaceMap<DIM, DIR>;
+  constexpr int NE = G::NE;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+  int a, p1, p2;
+  M::decode(t, a, p1, p2);
+  double const *blk = U + (size_t)slot * G::BLOCK_DOUBLES;
+  int const cell0 = line_origin<DIM, DIR>(p1, p2);
+  // low / high neighbour along DIR (26-table slots of W,E / S,N / B,T)
+  constexpr int lo_slot = DIR == 0 ? 4 : (DIR == 1 ? 10 : 12);
+  constexpr int hi_slot = DIR == 0 ? 21 : (DIR == 1 ? 15 : 13);
+  int const nlo = GATHER && a < 3 ? __ldg(nbr26 + (size_t)slot * 26 + lo_slot) : 0;
+  int const nhi = GATHER && a > 13 ? __ldg(nbr26 + (size_t)slot * 26 + hi_slot) : 0;
+  double cons[6][NE];
+#pragma unroll
+  for (int m = 0; m < 6; ++m)
+    load_cell<DIM, DIR>(stencil_cell<DIM, DIR, GATHER>(U, blk, HS + a - 3 + m, cell0, nlo, nhi),
+                        cons[m]);
+  double fd[NE];
+  bool const valid = face_compute<DIM, DIR, SCHEME, T>(eos, bm.B, cons, fd);
   write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
 }
 
@@ -420,6 +443,108 @@ face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
     if (t < FaceMap<DIM, 2>::COUNT)
       face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, T, false, true>(U, nbr26, slot, item, t, bm,
                                                                  F + 2 * dstride, stride);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// pencil sweeps (engine fast path)
+// ---------------------------------------------------------------------------
+
+// Interior linear index of the cell with index c along DIR at transverse (p1, p2).
+template <int DIM, int DIR>
+__device__ __forceinline__ int interior_index(int c, int p1, int p2) {
+  using M = FaceMap<DIM, DIR>;
+  int ci[3] = {0, 0, 0};
+  ci[DIR] = c;
+  ci[M::O1] = p1;
+  ci[M::O2] = p2;
+  if constexpr (DIM == 3) return (ci[0] * IC + ci[1]) * IC + ci[2];
+  else if constexpr (DIM == 2) return ci[0] * IC + ci[1];
+  else return ci[0];
+}
+
+// One thread walks a line of 16 cells along DIR: it computes the 17 face
+// fluxes in order with a sliding 6-cell stencil window (each cell is loaded
+// once per line instead of six times) and forms each cell's flux difference
+// F(a-1/2) - F(a+1/2) as soon as both faces are known. The directions run one
+// after the other: MODE 0 stores the difference in R, MODE 1 adds to R, MODE 2
+// (the last direction) adds, scales by 1/cell size and applies the SSP-RK3
+// stage: Uout = (stage ? a0 Uin + a1 U0 : Uin) + c dt rhs. The summation order
+// is therefore (dx + dy) + dz instead of the reference's three-order symmetric
+// sum (the strict build keeps that one). Stencils are gathered from neighbour
+// interiors; cases with dt == 0 are skipped.
+template <int DIM, int DIR, int SCHEME, typename T, int MODE>
+__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME>::min_ctas)
+pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
+              int const *__restrict__ work, int nwork, BlockMeta const *__restrict__ meta,
+              int const *__restrict__ nbr26, CaseState const *__restrict__ cases, int stage) {
+  using G = Geo<DIM>;
+  using M = FaceMap<DIM, DIR>;
+  constexpr int NE = G::NE;
+  constexpr int P = M::E1 * M::E2;  // lines per block
+  constexpr int step = DIR == 0 ? G::TCY * G::TCZ : (DIR == 1 ? G::TCZ : 1);
+  constexpr int lo_slot = DIR == 0 ? 4 : (DIR == 1 ? 10 : 12);
+  constexpr int hi_slot = DIR == 0 ? 21 : (DIR == 1 ? 15 : 13);
+  int const g = blockIdx.x * blockDim.x + threadIdx.x;
+  int const item = g / P;
+  if (item >= nwork) return;
+  int const p = g - item * P;
+  int const p1 = p / M::E2, p2 = p - (p / M::E2) * M::E2;
+  int const slot = work[item];
+  BlockMeta const bm = meta[slot];
+  double const dt = cases[bm.case_id].dt;
+  if (!(dt > 0.0)) return;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+  double const *blk = Uin + (size_t)slot * G::BLOCK_DOUBLES;
+  int const cell0 = line_origin<DIM, DIR>(p1, p2);
+  int const nlo = __ldg(nbr26 + (size_t)slot * 26 + lo_slot);
+  int const nhi = __ldg(nbr26 + (size_t)slot * 26 + hi_slot);
+  double *Rb = R ? R + (size_t)slot * NE * G::INTERIOR : nullptr;
+
+  double w[6][NE];
+#pragma unroll
+  for (int m = 0; m < 6; ++m)
+    load_cell<DIM, DIR>(stencil_cell<DIM, DIR, true>(Uin, blk, HS - 3 + m, cell0, nlo, nhi), w[m]);
+  double const ocs = inv(bm.cell_size);
+  double const cdt = kRkC[stage] * (0.0 + dt);
+  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+  double fprev[NE];
+#pragma unroll 1
+  for (int a = 0; a <= IC; ++a) {
+    double f[NE];
+    bool const valid = face_compute<DIM, DIR, SCHEME, T>(eos, bm.B, w, f);
+#pragma unroll
+    for (int n = 0; n < NE; ++n)
+      if (!valid) f[n] = 0.0;
+    if (a > 0) {
+      int const ix = interior_index<DIM, DIR>(a - 1, p1, p2);
+      size_t const x = (size_t)slot * G::BLOCK_DOUBLES + cell0 + (HS + a - 1) * step;
+#pragma unroll
+      for (int n = 0; n < NE; ++n) {
+        double const d = fprev[n] - f[n];
+        if constexpr (MODE == 0) {
+          Rb[n * G::INTERIOR + ix] = d;
+        } else if constexpr (MODE == 1) {
+          Rb[n * G::INTERIOR + ix] += d;
+        } else {
+          double const sum = DIM > 1 ? Rb[n * G::INTERIOR + ix] + d : d;
+          double const rhs = 0.0 + sum * ocs;
+          size_t const xf = x + (size_t)n * G::CELLS;
+          double u = Uin[xf];
+          if (stage != 0) u = a0 * u + a1 * U0[xf];
+          Uout[xf] = u + cdt * rhs;
+        }
+      }
+    }
+#pragma unroll
+    for (int n = 0; n < NE; ++n) fprev[n] = f[n];
+    if (a < IC) {
+#pragma unroll
+      for (int m = 0; m < 5; ++m)
+#pragma unroll
+        for (int n = 0; n < NE; ++n) w[m][n] = w[m + 1][n];
+      load_cell<DIM, DIR>(stencil_cell<DIM, DIR, true>(Uin, blk, HS + a + 3, cell0, nlo, nhi), w[5]);
+    }
   }
 }
 
@@ -486,10 +611,6 @@ divergence_kernel(int const *__restrict__ work, BlockMeta const *__restrict__ me
   }
 }
 
-// SSP-RK3 stage (runge_kutta_3_TVD.h:41-59; time_integrator.h:98-113, 369-457)
-__constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
-__constant__ double kRkA0[3] = {0.0, 0.25, 2.0 / 3.0};
-__constant__ double kRkA1[3] = {0.0, 0.75, 1.0 / 3.0};
 
 // Uin: stage input, U0: state at the start of the step, Uout: stage output.
 // Uout may alias U0 (each cell is read and written by the same thread) but
@@ -939,6 +1060,61 @@ cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *
   return cudaGetLastError();
 }
 }  // namespace
+
+namespace {
+template <int DIM, int DIR, typename T, int MODE>
+cudaError_t pencil_t(Launch const &L, double const *U0, double *Uout, double *R, int const *nbr26,
+                     CaseState const *cases, int stage) {
+  constexpr int P = FaceMap<DIM, DIR>::E1 * FaceMap<DIM, DIR>::E2;
+  long long const threads = (long long)L.nwork * P;
+  dim3 grid((unsigned)((threads + 127) / 128));
+  switch (L.scheme) {
+    case FV_CHAR:
+      pencil_kernel<DIM, DIR, FV_CHAR, T, MODE><<<grid, 128, 0, L.stream>>>(L.U, U0, Uout, R, L.work, L.nwork, L.meta, nbr26, cases, stage);
+      break;
+    case FV_PRIM:
+      pencil_kernel<DIM, DIR, FV_PRIM, T, MODE><<<grid, 128, 0, L.stream>>>(L.U, U0, Uout, R, L.work, L.nwork, L.meta, nbr26, cases, stage);
+      break;
+    case FS_ROE:
+      pencil_kernel<DIM, DIR, FS_ROE, T, MODE><<<grid, 128, 0, L.stream>>>(L.U, U0, Uout, R, L.work, L.nwork, L.meta, nbr26, cases, stage);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+template <int DIM, typename T>
+cudaError_t pencil_dim(Launch const &L, double const *U0, double *Uout, double *R, int const *nbr26,
+                       CaseState const *cases, int stage) {
+  if (cudaError_t e = pencil_t<DIM, 0, T, DIM == 1 ? 2 : 0>(L, U0, Uout, R, nbr26, cases, stage))
+    return e;
+  if constexpr (DIM > 1)
+    if (cudaError_t e = pencil_t<DIM, (DIM > 1 ? 1 : 0), T, DIM == 2 ? 2 : 1>(L, U0, Uout, R, nbr26, cases, stage))
+      return e;
+  if constexpr (DIM > 2)
+    if (cudaError_t e = pencil_t<DIM, (DIM > 2 ? 2 : 0), T, 2>(L, U0, Uout, R, nbr26, cases, stage))
+      return e;
+  return cudaSuccess;
+}
+}  // namespace
+
+cudaError_t launch_pencil_stage(Launch const &L, double const *U0, double *Uout, double *R,
+                                int const *nbr26, CaseState const *cases, int stage) {
+  if (L.nwork <= 0) return cudaSuccess;
+  if (!L.work || !L.meta || !nbr26 || !cases || stage < 0 || stage > 2) return cudaErrorInvalidValue;
+  if (L.dim > 1 && !R) return cudaErrorInvalidValue;
+  bool const f32 = L.precision == FP32_FLUX;
+  switch (L.dim) {
+    case 1: return f32 ? pencil_dim<1, float>(L, U0, Uout, R, nbr26, cases, stage)
+                       : pencil_dim<1, double>(L, U0, Uout, R, nbr26, cases, stage);
+    case 2: return f32 ? pencil_dim<2, float>(L, U0, Uout, R, nbr26, cases, stage)
+                       : pencil_dim<2, double>(L, U0, Uout, R, nbr26, cases, stage);
+    case 3: return f32 ? pencil_dim<3, float>(L, U0, Uout, R, nbr26, cases, stage)
+                       : pencil_dim<3, double>(L, U0, Uout, R, nbr26, cases, stage);
+  }
+  return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
                                  double *F, long long stride, long long dstride) {

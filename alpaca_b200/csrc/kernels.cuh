@@ -49,6 +49,14 @@ cudaError_t launch_divergence(Launch const &L, double const *F, long long flux_i
 cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
                                  double *F, long long flux_item_stride, long long dir_stride);
 
+// One SSP-RK3 stage of every work item by pencil sweeps (engine fast path):
+// the faces of each line of cells along x, then y, then z, with the
+// per-cell flux differences accumulated in R ([slot][NE][interior cells]) and
+// the last direction applying Uout = (stage ? a0 Uin + a1 U0 : Uin) + c dt
+// ((dFx + dFy) + dFz) / h, Uin = L.U. Uout may alias U0, not Uin.
+cudaError_t launch_pencil_stage(Launch const &L, double const *U0, double *Uout, double *R,
+                                int const *nbr26, CaseState const *cases, int stage);
+
 // RK3 stage on the interior: Uout = (stage ? a0*Uin + a1*U0 : Uin) + c*dt*div(F)
 // with Uin = L.U; dt per case from cases[meta.case_id].dt (skip when dt == 0),
 // or `dt` for every block when cases is null. Uout may alias U0, not Uin.

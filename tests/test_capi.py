@@ -58,7 +58,7 @@ def test_workspace_and_engine_sizes(dim):
     faces = 17 * (17 if dim > 1 else 2) * (17 if dim > 2 else 2)
     assert lib.alp_space_rhs_workspace_size(dim, 7) == 7 * dim * (dim + 2) * faces * 8
     cells = 24 ** dim
-    per_block = 2 * (dim + 2) * cells * 8 + dim * (dim + 2) * faces * 8
+    per_block = 3 * (dim + 2) * cells * 8 + (dim + 2) * 16 ** dim * 8
     assert lib.alp_engine_bytes(dim, 10, 2) >= 10 * per_block
 
 

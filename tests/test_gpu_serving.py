@@ -58,12 +58,13 @@ def test_device_initial_condition_matches_host(cuda, kind):
 
 
 def small_stream(seed=2):
+    """Five small cases that all arrive at once (so the batched run overlaps them)."""
     rng = np.random.default_rng(seed)
     reqs = [serving.quadrant_request(rng, 4, 30), serving.blast_request(rng, 8, 20, water=False),
             serving.blast_request(rng, 27, 12, water=True), serving.quadrant_request(rng, 12, 25),
             serving.blast_request(rng, 8, 16, water=False)]
-    for i, r in enumerate(reqs):
-        r.arrival_s = 0.002 * i
+    for r in reqs:
+        r.arrival_s = 0.0
     return reqs
 
 

@@ -185,6 +185,17 @@ class Engine:
             self.step(chunk)
         raise RuntimeError("engine did not finish")
 
+    def autotune(self, trial_steps: int = 3):
+        """Times the stepping candidates on the resident cases (state unchanged)
+        and keeps the fastest; returns (chosen index, ms per step per candidate)."""
+        chosen = C.c_int()
+        ms = (C.c_float * 3)()
+        self._check(self.lib.alp_engine_autotune(self.h, trial_steps, C.byref(chosen), ms))
+        return chosen.value, [float(x) for x in ms]
+
+    def set_path(self, candidate: int):
+        self._check(self.lib.alp_engine_set_path(self.h, candidate))
+
     @property
     def launches_per_step(self) -> int:
         return self.lib.alp_engine_launches_per_step(self.h)

@@ -314,11 +314,8 @@ size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
   if (dim < 1 || dim > 3) return 0;
   size_t const ne = dim + 2;
   size_t const blk = ne * cells_of(dim) * sizeof(double);
-#ifdef ALP_STRICT
-  size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double);
-#else
-  size_t const flux = ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
-#endif
+  size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double) +
+                      ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
   return (size_t)capacity_blocks *
              (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
          (size_t)max_cases * sizeof(CaseState);
@@ -352,14 +349,13 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   grab((void **)&e->UC, blk * capacity_blocks * sizeof(double));
   // The strict build reproduces the reference's three-order symmetric flux
   // sum, so it keeps the face-flux arrays; the fast build sweeps pencils.
-#ifdef ALP_STRICT
+  // Both stepping paths keep their scratch so the autotuner can switch; the
+  // strict build always uses the face-flux path, whose three-order symmetric
+  // flux sum matches the reference bit for bit.
   e->path = 1;
   grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
-#else
-  e->path = 0;
   grab((void **)&e->R, (size_t)e->ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) *
                            capacity_blocks * sizeof(double));
-#endif
   grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
@@ -527,6 +523,73 @@ int alp_engine_all_done(alp_engine *e, int *done) {
 }
 
 alp_stream_t alp_engine_stream(alp_engine *e) { return e ? (alp_stream_t)e->stream : nullptr; }
+
+int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (trial_steps <= 0) return fail(ALP_ERR_INVALID, "trial_steps must be positive");
+  // candidates: face fluxes with 128- or 64-thread blocks, pencil sweeps
+  struct Cand {
+    int path, threads;
+  };
+  Cand const cands[3] = {{1, 128}, {1, 64}, {0, 128}};
+  int const ncand = 3;
+#ifdef ALP_STRICT
+  int const allowed = 2;  // the pencil path changes the flux summation order
+#else
+  int const allowed = ncand;
+#endif
+  int const saved_path = e->path, saved_threads = e->face_threads;
+  float best = 0.f;
+  int best_i = 0;
+  cudaEvent_t t0, t1;
+  ALP_CUDA(cudaEventCreate(&t0));
+  ALP_CUDA(cudaEventCreate(&t1));
+  for (int i = 0; i < ncand; ++i) {
+    float ms = -1.f;
+    if (i < allowed && e->nwork > 0) {
+      e->path = cands[i].path;
+      e->face_threads = cands[i].threads;
+      if (int rc = e->record_step(true)) return rc;  // warm-up
+      ALP_CUDA(cudaEventRecord(t0, e->stream));
+      for (int k = 0; k < trial_steps; ++k)
+        if (int rc = e->record_step(true)) return rc;
+      ALP_CUDA(cudaEventRecord(t1, e->stream));
+      ALP_CUDA(cudaEventSynchronize(t1));
+      ALP_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+      ms /= trial_steps;
+      if (best == 0.f || ms < best) {
+        best = ms;
+        best_i = i;
+      }
+    }
+    if (ms_per_step) ms_per_step[i] = ms;
+  }
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  if (e->nwork > 0) {
+    e->path = cands[best_i].path;
+    e->face_threads = cands[best_i].threads;
+  } else {
+    e->path = saved_path;
+    e->face_threads = saved_threads;
+  }
+  e->graph_dirty = true;
+  if (chosen) *chosen = e->nwork > 0 ? best_i : -1;
+  return ALP_OK;
+}
+
+int alp_engine_set_path(alp_engine *e, int candidate) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  int const paths[3] = {1, 1, 0}, threads[3] = {128, 64, 128};
+  if (candidate < 0 || candidate > 2) return fail(ALP_ERR_INVALID, "candidate must be 0, 1 or 2");
+#ifdef ALP_STRICT
+  if (candidate == 2) return fail(ALP_ERR_INVALID, "the strict build steps the face-flux path");
+#endif
+  e->path = paths[candidate];
+  e->face_threads = threads[candidate];
+  e->graph_dirty = true;
+  return ALP_OK;
+}
 
 int alp_engine_set_graph(alp_engine *e, int enabled) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");

@@ -44,7 +44,8 @@ struct alp_engine {
   double *U = nullptr, *UB = nullptr, *UC = nullptr;
   double *F = nullptr;  // face fluxes [slot][dim][NE][faces] (face-flux path)
   double *R = nullptr;  // per-cell flux differences [slot][NE][interior] (pencil path)
-  int path = 0;         // 0: pencil sweeps, 1: face fluxes + stage update
+  int path = 1;         // 0: pencil sweeps, 1: face fluxes + stage update
+  int face_threads = 128;
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr;
   int *work = nullptr;
@@ -70,25 +71,26 @@ struct alp_engine {
   long long dstride() const { return (long long)ne * faces; }
   long long stride() const { return dstride() * dim; }
 
-  // dt, then per stage one face-flux launch (all directions) and one
-  // divergence + stage-update launch: A -> B, (B, A) -> C, (C, A) -> A.
-  int record_step() {
+  // dt, then per stage the fluxes and the stage update: A -> B, (B, A) -> C,
+  // (C, A) -> A. trial: the last stage writes B instead of A and the step is
+  // not committed, so the case state is left as it was (autotuning).
+  int record_step(bool trial = false) {
     Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
     ALP_CUDA(launch_signal_speed(L, cases, nullptr));
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
     double *in[3] = {U, UB, UC};
-    double *out[3] = {UB, UC, U};
+    double *out[3] = {UB, UC, trial ? UB : U};
     for (int s = 0; s < 3; ++s) {
       Launch Ls = L;
       Ls.U = in[s];
       if (path == 0) {
         ALP_CUDA(alp::launch_pencil_stage(Ls, U, out[s], R, nbr26, cases, s));
       } else {
-        ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride()));
+        ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride(), face_threads));
         ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
       }
     }
-    ALP_CUDA(launch_step_commit(cases, max_cases, stream));
+    if (!trial) ALP_CUDA(launch_step_commit(cases, max_cases, stream));
     return ALP_OK;
   }
 

@@ -1041,18 +1041,18 @@ cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout,
 namespace {
 template <int DIM, typename T>
 cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *cases, double *F,
-                            long long stride, long long dstride) {
+                            long long stride, long long dstride, int threads) {
   int const count = (IC + 1) * (DIM > 1 ? IC : 1) * (DIM > 2 ? IC : 1);
-  dim3 grid(L.nwork, (count + 127) / 128, DIM);
+  dim3 grid(L.nwork, (count + threads - 1) / threads, DIM);
   switch (L.scheme) {
     case FV_CHAR:
-      face_flux_all_kernel<DIM, FV_CHAR, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FV_CHAR, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
       break;
     case FV_PRIM:
-      face_flux_all_kernel<DIM, FV_PRIM, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FV_PRIM, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
       break;
     case FS_ROE:
-      face_flux_all_kernel<DIM, FS_ROE, T><<<grid, 128, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FS_ROE, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -1117,17 +1117,19 @@ cudaError_t launch_pencil_stage(Launch const &L, double const *U0, double *Uout,
 }
 
 cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
-                                 double *F, long long stride, long long dstride) {
+                                 double *F, long long stride, long long dstride, int threads) {
   if (L.nwork <= 0) return cudaSuccess;
   if (!L.work || !L.meta || !nbr26 || !cases) return cudaErrorInvalidValue;
+  if (threads <= 0) threads = 128;
+  if (threads > 128 || (threads & 31)) return cudaErrorInvalidValue;
   bool const f32 = L.precision == FP32_FLUX;
   switch (L.dim) {
-    case 1: return f32 ? face_flux_all_t<1, float>(L, nbr26, cases, F, stride, dstride)
-                       : face_flux_all_t<1, double>(L, nbr26, cases, F, stride, dstride);
-    case 2: return f32 ? face_flux_all_t<2, float>(L, nbr26, cases, F, stride, dstride)
-                       : face_flux_all_t<2, double>(L, nbr26, cases, F, stride, dstride);
-    case 3: return f32 ? face_flux_all_t<3, float>(L, nbr26, cases, F, stride, dstride)
-                       : face_flux_all_t<3, double>(L, nbr26, cases, F, stride, dstride);
+    case 1: return f32 ? face_flux_all_t<1, float>(L, nbr26, cases, F, stride, dstride, threads)
+                       : face_flux_all_t<1, double>(L, nbr26, cases, F, stride, dstride, threads);
+    case 2: return f32 ? face_flux_all_t<2, float>(L, nbr26, cases, F, stride, dstride, threads)
+                       : face_flux_all_t<2, double>(L, nbr26, cases, F, stride, dstride, threads);
+    case 3: return f32 ? face_flux_all_t<3, float>(L, nbr26, cases, F, stride, dstride, threads)
+                       : face_flux_all_t<3, double>(L, nbr26, cases, F, stride, dstride, threads);
   }
   return cudaErrorInvalidValue;
 }

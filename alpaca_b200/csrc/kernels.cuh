@@ -47,7 +47,8 @@ cudaError_t launch_divergence(Launch const &L, double const *F, long long flux_i
 // domain faces), so block halos are never read; items of inactive cases
 // (dt == 0) skipped. Direction d goes to F + d * dir_stride.
 cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState const *cases,
-                                 double *F, long long flux_item_stride, long long dir_stride);
+                                 double *F, long long flux_item_stride, long long dir_stride,
+                                 int threads = 128);
 
 // One SSP-RK3 stage of every work item by pencil sweeps (engine fast path):
 // the faces of each line of cells along x, then y, then z, with the

@@ -124,6 +124,8 @@ _SIGS = {
     "alp_engine_stream": (_S, [_V]),
     "alp_engine_set_graph": (C.c_int, [_V, C.c_int]),
     "alp_engine_launches_per_step": (C.c_int, [_V]),
+    "alp_engine_autotune": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_float)]),
+    "alp_engine_set_path": (C.c_int, [_V, C.c_int]),
 }
 
 _libs = {}

@@ -246,7 +246,7 @@ def serving_report(args):
     return out
 
 
-def precision_report(steps: int = 200):
+def precision_report(steps: int = 200, emit=None):
     """L1 and Linf error of every field of the FP32-flux form against the FP64
     path after `steps` SSP-RK3 steps (the FP64 path is the one checked against
     the reference: per RHS <= 1e-12, 100-step L1 <= 1e-10)."""
@@ -261,12 +261,22 @@ def precision_report(steps: int = 200):
                         ("stiffened-gas water 128^3", cases.water_spheres(8, seed=3))):
         for variant in ("fvchar", "fsroe"):
             out = {}
+            failed = None
             for prec in (N.FP64, N.FP32_FLUX):
                 eng = api.Engine(3, variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
                 cid = eng.add_case(case, max_steps=steps)
                 eng.run_to_end(chunk=50)
-                out[prec] = eng.get(cid)
+                try:
+                    out[prec] = eng.get(cid)
+                except N.AlpacaError as err:
+                    failed = f"{'fp64' if prec == N.FP64 else 'fp32-flux'}: {err}"
                 eng.close()
+            if failed:
+                row = {"case": label, "variant": variant, "failed": failed}
+                rows.append(row)
+                if emit:
+                    emit(row)
+                continue
             I = cases.interior(3)
             a, b = out[N.FP32_FLUX][0][I], out[N.FP64][0][I]
             err = {}
@@ -274,8 +284,11 @@ def precision_report(steps: int = 200):
                 d = np.abs(a[:, f] - b[:, f])
                 err[nm] = {"l1": float(d.sum() / max(np.abs(b[:, f]).sum(), 1e-300)),
                            "linf": float(d.max() / max(np.abs(b[:, f]).max(), 1e-300))}
-            rows.append({"case": label, "variant": variant, "steps": out[N.FP64][2],
-                         "t_fp64": out[N.FP64][1], "t_fp32": out[N.FP32_FLUX][1], "errors": err})
+            row = {"case": label, "variant": variant, "steps": out[N.FP64][2],
+                   "t_fp64": out[N.FP64][1], "t_fp32": out[N.FP32_FLUX][1], "errors": err}
+            rows.append(row)
+            if emit:
+                emit(row)
     return rows
 
 
@@ -295,6 +308,7 @@ def run_ours(args, ws, rank, local):
     eng = api.Engine(3, args.variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
     stream = torch.cuda.ExternalStream(eng.stream_handle)
     cid = eng.add_case(case, max_steps=0)
+    chosen, cand_ms = eng.autotune(trial_steps=3)
     eng.step(args.warmup)
     torch.cuda.synchronize()
     barrier(ws, dev)
@@ -325,6 +339,7 @@ def run_ours(args, ws, rank, local):
                          max_cases=1)
         stream = torch.cuda.ExternalStream(eng.stream_handle)
         cid = eng.add_case(case_p, max_steps=0)
+        eng.set_path(chosen)
         eng.step(args.warmup)
         eng.remove_case(cid)
         torch.cuda.synchronize()
@@ -371,7 +386,11 @@ def run_ours(args, ws, rank, local):
                    "scheme": "WENO5-JS characteristic + HLLC/Einfeldt + SSP-RK3" if args.variant == "fvchar" else args.variant,
                    "cfl": 0.6, "l2": "state 283 MB per buffer > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{ws}", "sim_time_reached": t_sim,
-                   "steps_done": steps_done},
+                   "steps_done": steps_done,
+                   "autotune": {"chosen": ["face fluxes, 128-thread blocks",
+                                           "face fluxes, 64-thread blocks",
+                                           "pencil sweeps"][chosen],
+                                "ms_per_step": cand_ms}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "traffic": None,
                      "peak_source": src,
@@ -395,8 +414,7 @@ def main():
         elif args.precision_report:
             import torch
             torch.cuda.set_device(local)
-            for row in precision_report():
-                print(json.dumps(row), flush=True)
+            precision_report(emit=lambda row: print(json.dumps(row), flush=True))
         elif args.serving_only:
             import torch
             torch.cuda.set_device(local)

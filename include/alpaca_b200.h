@@ -208,6 +208,21 @@ alp_stream_t alp_engine_stream(alp_engine *e);
 /* Enables (1) or disables (0) CUDA-graph replay of the step (default on). */
 int alp_engine_set_graph(alp_engine *e, int enabled);
 
+/* Times the stepping candidates on the engine's resident cases and keeps the
+ * fastest: 0 = face fluxes (128-thread blocks, all directions in one launch)
+ * + divergence/stage update, 1 = the same with 64-thread blocks, 2 = pencil
+ * sweeps (one thread per line of cells, 17 faces with a sliding stencil
+ * window, flux differences summed in the kernels and the RK stage applied by
+ * the last direction; not available in the strict build). Each candidate runs
+ * trial_steps steps whose last stage writes scratch memory and that are not
+ * committed, so the cases' state and time are unchanged. *chosen receives the
+ * candidate (-1 when no case is resident), ms_per_step[3] (may be null) the
+ * measured time per step of each candidate (-1 when not run). Synchronises. */
+int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step);
+
+/* Selects a stepping candidate (as numbered for alp_engine_autotune). */
+int alp_engine_set_path(alp_engine *e, int candidate);
+
 /* Number of kernel launches one engine step issues. */
 int alp_engine_launches_per_step(alp_engine *e);
 

@@ -437,3 +437,33 @@ def test_fp32_flux_3d_100_steps(cuda, variant):
     errs = [l1_rel(sub[f], z["sub"][f]) for f in range(5)]
     print(variant, "fp32 128^3 100-step L1 per field", errs)
     assert steps == 100 and errs[0] <= 1e-5
+
+
+# ---- stepping candidates and the autotuner -----------------------------------
+
+def test_autotune_leaves_state_and_candidates_agree(cuda):
+    """Autotuning runs uncommitted trial steps (state and time unchanged); every
+    candidate advances the case to the same result within the FP64 tolerance
+    (face paths bit-identical to each other; the pencil path sums the three
+    flux differences in a different order)."""
+    case = cases.fourier_shock(2, dim=3, seed=31, steps=6)
+    eng = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
+    cid = eng.add_case(case)
+    eng.step(2)
+    before = eng.get(cid)
+    chosen, ms = eng.autotune(trial_steps=2)
+    after = eng.get(cid)
+    assert chosen in (0, 1, 2) and all(m > 0 for m in ms)
+    assert np.array_equal(before[0], after[0]) and before[1:] == after[1:]
+    results = []
+    for cand in (0, 1, 2):
+        e = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
+        i = e.add_case(case)
+        e.set_path(cand)
+        e.run_to_end(chunk=6)
+        results.append(e.get(i)[0])
+        e.close()
+    eng.close()
+    I = cases.interior(3)
+    assert np.array_equal(results[0], results[1])
+    assert l1_per_field(results[2][I], results[0][I]) <= 1e-13

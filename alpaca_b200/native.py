@@ -103,6 +103,8 @@ _SIGS = {
     "alp_space_rhs_workspace_size": (C.c_size_t, [C.c_int, C.c_int]),
     "alp_space_rhs": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _V, C.c_int,
                                 C.c_double, _V, _V, C.c_size_t, _S]),
+    "alp_space_rhs_static": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _V,
+                                       C.c_int, C.c_double, _V, _S]),
     "alp_prime_states": (C.c_int, [C.c_int, C.POINTER(Material), _V, C.c_int, _V, _S]),
     "alp_halo_update": (C.c_int, [C.c_int, _V, C.c_int, C.c_int, _V, C.c_int, _S]),
     "alp_timestep_size": (C.c_int, [C.c_int, C.POINTER(Material), _V, C.c_int, C.c_double,

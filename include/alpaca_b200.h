@@ -112,6 +112,21 @@ int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
                   const double *d_blocks, int nb, double cell_size, double *d_rhs,
                   void *d_workspace, size_t workspace_bytes, alp_stream_t stream);
 
+/* alp_space_rhs for callers that may not allocate device memory; it has no
+ * counterpart in the reference. The face-flux scratch is a 16 MiB array of
+ * this library in device memory instead of a caller workspace, so at most 28
+ * blocks in 3D, 453 in 2D and 10,280 in 1D per call; a larger nb returns
+ * ALP_ERR_CAPACITY and launches nothing. Nothing is allocated by the call. The
+ * first call on each device (with that device current) looks up the array's
+ * address, which may load the library's module: make that first call before
+ * any stream capture. All calls on a device share the one array and it keeps
+ * the last call's contents (no call relies on them): calls that may overlap
+ * (different streams or threads without ordering) race on it, so order them.
+ * Results are those of alp_space_rhs on the same inputs. */
+int alp_space_rhs_static(int dim, const alp_scheme *scheme, const alp_material *mat,
+                         const double *d_blocks, int nb, double cell_size, double *d_rhs,
+                         alp_stream_t stream);
+
 /* Replaces PrimeStateHandler::ConvertConservativesToPrimeStates over every
  * cell (prime_states/prime_state_handler.h:141-152): d_primes [nb][NE][cells]
  * in the order Density, Pressure, VelocityX[, Y[, Z]]. */

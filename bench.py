@@ -30,6 +30,15 @@ sys.path.insert(0, ROOT)
 
 METRIC = "cell-updates/s"
 B_ALG_3D = 320.0  # algorithmic HBM bytes per 3D cell-update (64 * N_eq, FP64 state)
+# Floating-point operations (add + mul + div + sqrt) of the reference algorithm
+# per 3D cell-update (one full SSP-RK3 step incl. prime states and dt), counted
+# by the operation-counting build of the oracle on a seeded one-block case;
+# tests/test_oracle.py::test_op_counts_match_bench_constants re-counts them.
+FLOPS_PER_CELL_UPDATE_3D = {"fvchar": 15767, "fvprim": 10192, "fsroe": 22478}
+# DRAM bytes per SSP-RK3 step of the 128^3 workload (sum of dram__bytes_read.sum
+# and dram__bytes_write.sum over the step's kernels, one ncu capture; summary in
+# profiles/step_fvchar_128cubed.md)
+TRAFFIC_PER_STEP = {("fvchar", "fp64"): 4.348e9}
 
 
 def parse():
@@ -261,7 +270,7 @@ def precision_report(steps: int = 200, emit=None):
                         ("stiffened-gas water 128^3", cases.water_spheres(8, seed=3))):
         for variant in ("fvchar", "fsroe"):
             out = {}
-            failed = None
+            failed = []
             for prec in (N.FP64, N.FP32_FLUX):
                 eng = api.Engine(3, variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
                 cid = eng.add_case(case, max_steps=steps)
@@ -269,10 +278,10 @@ def precision_report(steps: int = 200, emit=None):
                 try:
                     out[prec] = eng.get(cid)
                 except N.AlpacaError as err:
-                    failed = f"{'fp64' if prec == N.FP64 else 'fp32-flux'}: {err}"
+                    failed.append(f"{'fp64' if prec == N.FP64 else 'fp32-flux'}: {err}")
                 eng.close()
             if failed:
-                row = {"case": label, "variant": variant, "failed": failed}
+                row = {"case": label, "variant": variant, "failed": "; ".join(failed)}
                 rows.append(row)
                 if emit:
                     emit(row)
@@ -368,6 +377,18 @@ def run_ours(args, ws, rank, local):
     hbm, src = peaks()
     achieved = cells * args.steps / (ms * 1e-3) * B_ALG_3D / 1e9
     fp64 = fp64_peak()
+    flops = FLOPS_PER_CELL_UPDATE_3D[args.variant]
+    fp64_compute = None
+    if fp64:
+        fp64_compute = {
+            "flops_per_cell_update": flops,
+            "achieved_tflops": value / ws * flops / 1e12,
+            "peak_tflops": fp64, "peak_source": "measured FP64 FMA chains (2 flops per FMA)",
+            "frac": value / ws * flops / 1e12 / fp64,
+            "ceiling_cell_updates_per_s": fp64 * 1e12 / flops,
+            "count": "add+mul+div+sqrt of the reference algorithm, counted by the oracle's "
+                     "operation-counting build" + ("" if args.precision == "fp64" else
+                                                   "; the FP32-flux form runs part of them in FP32")}
     cpu = None
     if not args.no_cpu_baseline:
         cpu = reference_cpu_sample(args.variant, 15.0, os.cpu_count() or 1)
@@ -392,10 +413,12 @@ def run_ours(args, ws, rank, local):
                                            "pencil sweeps"][chosen],
                                 "ms_per_step": cand_ms}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "traffic": None,
+                     "frac": achieved / hbm,
+                     "traffic": TRAFFIC_PER_STEP.get((args.variant, args.precision)),
                      "peak_source": src,
                      "kernel": "whole SSP-RK3 step (one CUDA-graph launch), 320 B/cell-update",
-                     "fp64_pipe_peak_tflops_measured": fp64},
+                     "fp64_pipe_peak_tflops_measured": fp64,
+                     "fp64_compute": fp64_compute},
         "cpu_baseline": cpu,
         "e2e": e2e,
         "gpu_launches": launches,

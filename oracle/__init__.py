@@ -23,6 +23,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 RESTATEMENT_SO = os.path.join(HERE, "_build", "liboracle.so")
+# the same restatement with every double replaced by an operation-counting scalar
+OPCOUNT_SO = os.path.join(HERE, "_build", "liboracle_ops.so")
 REF_DIR = os.path.join(HERE, "_ref")
 
 FLUX_SPLITTING, FINITE_VOLUME = 0, 1
@@ -75,30 +77,37 @@ class _Common:
         return (nb, self.ne) + tc, (nb, self.ne) + tuple(n + 1 for n in ic)
 
 
+def _load(path: str):
+    """Loads a build of alpaca_oracle.c and declares its entry points."""
+    lib = C.CDLL(path)
+    lib.oracle_weno5.argtypes = [_D, _D, _D]
+    lib.oracle_eos.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, _D, _D, _D]
+    lib.oracle_prime_states.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int, _D]
+    lib.oracle_space_rhs.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, C.c_double,
+                                     C.c_double, C.c_int, C.c_double, _D, _D, _D, _D, C.c_int]
+    lib.oracle_timestep.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int,
+                                    C.c_double, C.c_double, C.c_double, C.c_double, _D]
+    lib.oracle_halo_fill.argtypes = [C.c_int, _D, C.c_int, C.c_int, _I, C.c_int, C.c_int]
+    lib.oracle_halo_update.argtypes = [C.c_int, _D, C.c_int, _I]
+    lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
+                               C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
+                               C.c_int, C.c_int, _D, _I, _D]
+    return lib
+
+
 class Restatement(_Common):
     """The plain-C restatement, for one dimension and scheme variant."""
 
     _lib = None
+    _path = RESTATEMENT_SO
 
     def __init__(self, dim: int, variant: str = "fvchar"):
-        if Restatement._lib is None:
-            if not os.path.exists(RESTATEMENT_SO):
+        cls = type(self)
+        if cls._lib is None:
+            if not os.path.exists(cls._path):
                 build()
-            lib = C.CDLL(RESTATEMENT_SO)
-            lib.oracle_weno5.argtypes = [_D, _D, _D]
-            lib.oracle_eos.argtypes = [C.c_int, C.c_double, C.c_double, C.c_int, _D, _D, _D]
-            lib.oracle_prime_states.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int, _D]
-            lib.oracle_space_rhs.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, C.c_double,
-                                             C.c_double, C.c_int, C.c_double, _D, _D, _D, _D, C.c_int]
-            lib.oracle_timestep.argtypes = [C.c_int, _D, C.c_int, C.c_double, C.c_double, C.c_int,
-                                            C.c_double, C.c_double, C.c_double, C.c_double, _D]
-            lib.oracle_halo_fill.argtypes = [C.c_int, _D, C.c_int, C.c_int, _I, C.c_int, C.c_int]
-            lib.oracle_halo_update.argtypes = [C.c_int, _D, C.c_int, _I]
-            lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
-                                       C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
-                                       C.c_int, C.c_int, _D, _I, _D]
-            Restatement._lib = lib
-        self.lib = Restatement._lib
+            cls._lib = _load(cls._path)
+        self.lib = cls._lib
         self.dim = dim
         self.ne = dim + 2
         self.variant = variant
@@ -177,6 +186,29 @@ class Restatement(_Common):
         if rc:
             raise RuntimeError(f"oracle_run rc={rc}")
         return u, t.value, steps.value, dts[: steps.value].copy()
+
+
+class OpCounting(Restatement):
+    """The restatement compiled with an operation-counting scalar
+    (oracle/flop_count.cpp): same results, plus the floating-point operations
+    the reference algorithm executes. Single-threaded (nthreads must stay 1)."""
+
+    _lib = None
+    _path = OPCOUNT_SO
+    FIELDS = ("add", "mul", "div", "sqrt", "cmp", "abs")
+
+    def __init__(self, dim: int, variant: str = "fvchar"):
+        super().__init__(dim, variant)
+        self.lib.oracle_op_counts.argtypes = [C.POINTER(C.c_longlong)]
+        self.lib.oracle_op_reset.argtypes = []
+
+    def reset(self) -> None:
+        self.lib.oracle_op_reset()
+
+    def counts(self) -> dict:
+        out = (C.c_longlong * 6)()
+        self.lib.oracle_op_counts(out)
+        return dict(zip(self.FIELDS, (int(x) for x in out)))
 
 
 class Reference(_Common):

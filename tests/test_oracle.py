@@ -215,3 +215,25 @@ def test_sod_physics_sanity():
     assert abs(float(z["t"]) - 0.2) < 1e-15
     assert rho.min() > 0.124 and rho.max() < 1.001  # WENO over/undershoots stay small
     assert rho[0] == pytest.approx(1.0, abs=1e-6) and rho[-1] == pytest.approx(0.125, abs=1e-6)
+
+
+# ---- 4. operation counts (the FP64 compute ceiling of the path) --------------
+
+def test_op_counts_match_bench_constants():
+    """The operation-counting build computes the restatement's results bit for
+    bit, and its flops per 3D cell-update are the constants bench.py reports."""
+    import bench
+    case = cases.fourier_shock(1, dim=3, seed=5)
+    u = filled(case)
+    for variant, expected in bench.FLOPS_PER_CELL_UPDATE_3D.items():
+        O = oracle.OpCounting(3, variant)
+        a = oracle.Restatement(3, variant).space_rhs(u, case.gamma, 0.0, False,
+                                                     case.grid.cell_size)[3]
+        b = O.space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)[3]
+        assert np.array_equal(a, b)
+        O.reset()
+        O.run(case.u, case.grid.nbr, case.gamma, 0.0, False, case.grid.cell_size, case.cfl,
+              1e300, max_steps=1)
+        c = O.counts()
+        flops = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / 4096
+        assert abs(flops - expected) <= 0.01 * expected, (variant, flops)

@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 
 from . import native as N
-from .cases import Case, block_shape
+from .cases import Case, LevelCase, block_shape
 
 VARIANTS = ("fvchar", "fvprim", "fsroe")
 
@@ -203,6 +203,66 @@ class Engine:
     @property
     def stream_handle(self) -> int:
         return self.lib.alp_engine_stream(self.h)
+
+
+class LevelEngine:
+    """A multi-level case (alp_levels_*): the leaves of a block tree advanced
+    with local time stepping; one CUDA graph per macro step."""
+
+    def __init__(self, case: LevelCase, variant: str = "fvchar", precision: int = N.FP64,
+                 max_macro: int = 0, strict: bool = False):
+        self.lib = N.lib(strict)
+        self.strict = strict
+        self.dim = case.dim
+        self.nleaf = case.nleaf
+        self.shape = case.u.shape
+        sch = N.Scheme.make(variant, precision)
+        mat = N.Material.make(case.gamma, case.B)
+        level = np.ascontiguousarray(case.level, dtype=np.int32)
+        coord = np.ascontiguousarray(case.coord, dtype=np.int32).reshape(-1, 3)
+        n0 = np.ascontiguousarray(list(case.n0) + [1] * (3 - len(case.n0)), dtype=np.int32)
+        u = np.ascontiguousarray(case.u, dtype=np.float64)
+        h = C.c_void_p()
+        N.check(self.lib.alp_levels_create(
+            case.dim, C.byref(sch), C.byref(mat), n0.ctypes.data_as(N._I), case.h0, case.nleaf,
+            level.ctypes.data_as(N._I), coord.ctypes.data_as(N._I), case.cfl, 0.0, case.t_end,
+            max_macro, u.ctypes.data_as(N._D), C.byref(h)), strict)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.alp_levels_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def step(self, n: int = 1):
+        N.check(self.lib.alp_levels_step(self.h, n), self.strict)
+
+    def get(self):
+        """(blocks [nleaf, ne, TC...] with valid interiors, t, macro steps)."""
+        out = np.empty(self.shape)
+        t = C.c_double()
+        m = C.c_int()
+        N.check(self.lib.alp_levels_get(self.h, out.ctypes.data_as(N._D), C.byref(t), C.byref(m)),
+                self.strict)
+        return out, t.value, m.value
+
+    def info(self) -> dict:
+        ng, lm, lp = C.c_int(), C.c_int(), C.c_int()
+        cu = C.c_longlong()
+        N.check(self.lib.alp_levels_info(self.h, C.byref(ng), C.byref(lm), C.byref(cu),
+                                         C.byref(lp)), self.strict)
+        return {"ghosts": ng.value, "max_level": lm.value,
+                "cell_updates_per_macro_step": cu.value, "launches_per_macro_step": lp.value}
+
+    @property
+    def stream_handle(self) -> int:
+        return self.lib.alp_levels_stream(self.h) or 0
 
 
 def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: int = N.FP64,

@@ -37,6 +37,10 @@ int faces_of(int dim) {
 }
 int cells_of(int dim) { return 24 * (dim > 1 ? 24 : 1) * (dim > 2 ? 24 : 1); }
 
+}  // namespace
+
+namespace alp {
+
 int scheme_id(alp_scheme const *s, int *id, int *precision) {
   if (!s) return fail(ALP_ERR_INVALID, "scheme is null");
   if (s->reconstruction_stencil != ALP_STENCIL_WENO5)
@@ -85,7 +89,7 @@ BlockMeta meta_of(alp_material const *m, double cell_size, int case_id) {
   return b;
 }
 
-}  // namespace
+}  // namespace alp
 
 extern "C" {
 

@@ -170,4 +170,10 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
                          int *case_id, int *first);
 // Copies the device case table to host.
 int engine_case_states(alp_engine *e, std::vector<CaseState> &out);
+// Compiled scheme id and precision of a selection (ALP_ERR_INVALID otherwise).
+int scheme_id(alp_scheme const *s, int *id, int *precision);
+// Rejects gamma <= 1 and negative background pressure.
+int check_material(alp_material const *m);
+// Block metadata of one material and cell size.
+BlockMeta meta_of(alp_material const *m, double cell_size, int case_id);
 }  // namespace alp

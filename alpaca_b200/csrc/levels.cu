@@ -1,0 +1,603 @@
+// Multi-level cases: the leaves of a block tree (levels of the reference's
+// multiresolution hierarchy) advanced with its local time stepping, all levels
+// batched into the engine's face-flux and stage-update launches.
+//
+// Time stepping (ModularAlgorithmAssembler::Advance,
+// modular_algorithm_assembler.cpp:575-874): a macro step is 2^lmax micro steps;
+// micro step t integrates the levels GetLevels(t) returns (:2564-2573), level l
+// with the sum of its last 2^(lmax-l) micro time steps (Integrate :1068-1098,
+// time_integrator.h:312-340); a level's stage-0 right-hand side is evaluated at
+// the start of its interval, i.e. during micro step t for the levels of
+// GetLevels(t-1) (all levels at t = 0), and kept in the face-flux scratch until
+// the level integrates. The micro time step is ComputeTimestepSize over all
+// leaves with the finest cell size, clipped to the end time with the micro
+// steps already taken (:1925-1982).
+//
+// Leaves are ordered finest level first in the work list, so the levels of
+// GetLevels(t) (always the finest `height` levels) are a prefix of it and every
+// launch covers exactly the leaves that work.
+//
+// Jumps: the face kernels gather stencil cells from a neighbour block's
+// interior. Where the face neighbour of a leaf is one level coarser or finer,
+// the neighbour slot is a ghost block: a virtual node of the leaf's level whose
+// three cell layers next to the shared face are filled before each stage, by
+// injection from the coarser leaf, or by averaging the finer leaves with
+// Multiresolution::Average (multiresolution.h:94-166). The reference predicts
+// the finer side with a fifth-order interpolation (Multiresolution::Prediction,
+// multiresolution.cpp:146) and corrects coarse fluxes at jumps
+// (JumpFluxAdjustment, modular_algorithm_assembler.cpp:1347); neither is done
+// here. Face neighbours may differ by one level at most.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cfloat>
+#include <map>
+#include <new>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "../../include/alpaca_b200.h"
+#include "engine.hpp"
+
+namespace {
+
+using alp::Geo;
+using alp::HS;
+using alp::IC;
+
+constexpr int kMaxLevels = 7;            // lmax <= 6: 64 micro steps per macro step
+constexpr int kMaxMicro = 1 << (kMaxLevels - 1);
+
+struct LevelState {
+  double t, t_end, cfl, h_fine;
+  double hist[kMaxMicro];  // micro time steps of the macro step in flight
+  int macro, max_macro, micro, active, status, pad;
+};
+
+// A ghost block: type 0 takes its cells from the coarser leaf src[0]
+// (octant bits src[1]), type 1 averages the finer leaves src[o] (child o has
+// x in bit 0, y in bit 1, z in bit 2; -1 where a child is not a leaf). Only
+// the cell layers next to the faces in `faces` (bits W, E, S, N, B, T) are
+// read by neighbours and filled.
+struct GhostRec {
+  int slot, type, level, src_level, faces;
+  int src[8];
+};
+
+__device__ __forceinline__ double ghost_average3(double a0, double a1, double a2, double a3,
+                                                 double a4, double a5, double a6, double a7) {
+  // children (x,y,z) = bits of the index; pairs of Multiresolution::Average
+  double const a = a0 + a7;  // (0,0,0) + (1,1,1)
+  double const b = a4 + a3;  // (0,0,1) + (1,1,0)
+  double const c = a2 + a5;  // (0,1,0) + (1,0,1)
+  double const d = a6 + a1;  // (0,1,1) + (1,0,0)
+  double const s1 = (a + b) + (c + d);
+  double const s2 = (a + c) + (b + d);
+  double const s3 = (a + d) + (b + c);
+  // min / max as std::min / std::max order them (first argument on ties)
+  double const i1 = s3 < s2 ? s3 : s2, mn = i1 < s1 ? i1 : s1;
+  double const i2 = s2 < s3 ? s3 : s2, mx = s1 < i2 ? i2 : s1;
+  return 0.125 * (0.5 * (mn + mx));
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+ghost_fill_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
+                  double const *Us, CaseState const *__restrict__ gate,
+                  CaseState const *__restrict__ cu, int stage) {
+  using G = Geo<DIM>;
+  GhostRec const g = ghosts[blockIdx.x];
+  int const f = blockIdx.y;
+  if (!((g.faces >> f) & 1)) return;
+  if (!(gate[g.level].dt > 0.0)) return;  // no leaf reading this ghost computes now
+  double const *src = (stage > 0 && cu[g.src_level].dt > 0.0) ? Us : UA;
+  int const d = f / 2, high = f % 2;
+  constexpr int T1 = DIM > 1 ? IC : 1, T2 = DIM > 2 ? IC : 1;
+  int const count = 3 * T1 * T2;
+  double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
+  for (int t = threadIdx.x; t < count; t += blockDim.x) {
+    // slab cell (layer, transverse 1, transverse 2) -> node cell a[3]
+    int const layer = t / (T1 * T2), r = t % (T1 * T2);
+    int a[3] = {0, 0, 0};
+    int const tr[2] = {r / T2, r % T2};
+    int q = 0;
+    for (int e = 0; e < DIM; ++e) {
+      if (e == d) a[e] = high ? IC - 3 + layer : layer;
+      else a[e] = tr[q++];
+    }
+    int const x = G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2));
+    if (g.type == 0) {
+      int c[3] = {0, 0, 0};
+      for (int e = 0; e < DIM; ++e) c[e] = (IC / 2) * ((g.src[1] >> e) & 1) + a[e] / 2;
+      double const *sb = src + (size_t)g.src[0] * G::BLOCK_DOUBLES;
+      int const y = G::cell(c[0] + G::fic(0), c[1] + G::fic(1), c[2] + G::fic(2));
+#pragma unroll
+      for (int e = 0; e < G::NE; ++e) dst[e * G::CELLS + x] = sb[e * G::CELLS + y];
+    } else {
+      int o = 0, c[3] = {0, 0, 0};
+      for (int e = 0; e < DIM; ++e) {
+        o |= (a[e] / (IC / 2)) << e;
+        c[e] = 2 * (a[e] % (IC / 2)) + G::fic(e);
+      }
+      int const child = g.src[o];
+      if (child < 0) continue;  // never read: the host checks face children are leaves
+      double const *sb = src + (size_t)child * G::BLOCK_DOUBLES;
+#pragma unroll
+      for (int e = 0; e < G::NE; ++e) {
+        double const *s = sb + e * G::CELLS;
+        double v;
+        if constexpr (DIM == 1) {
+          v = (s[G::cell(c[0], 0, 0)] + s[G::cell(c[0] + 1, 0, 0)]) * 0.5;
+        } else if constexpr (DIM == 2) {
+          v = ((s[G::cell(c[0], c[1], 0)] + s[G::cell(c[0] + 1, c[1] + 1, 0)]) +
+               (s[G::cell(c[0] + 1, c[1], 0)] + s[G::cell(c[0], c[1] + 1, 0)])) * 0.25;
+        } else {
+          double w[8];
+#pragma unroll
+          for (int k = 0; k < 8; ++k)
+            w[k] = s[G::cell(c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + ((k >> 2) & 1))];
+          v = ghost_average3(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7]);
+        }
+        dst[e * G::CELLS + x] = v;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ int levels_height(int t) { return __popc((t + 1) ^ t); }
+
+// Micro time step from the per-level signal speeds, the per-level step sizes
+// (cu: integrating levels, dt = sum of their micro steps) and the stage-0 flux
+// gate (cf: levels whose interval starts now, dt = 1).
+__global__ void levels_dt_kernel(LevelState *ls, CaseState *cu, CaseState *cf, int lmax, int tm) {
+  LevelState &S = *ls;
+  if (tm == 0)
+    S.active = S.t < S.t_end && (S.max_macro <= 0 || S.macro < S.max_macro) && !S.status;
+  double smax = 0.0;
+  int st = 0;
+  for (int l = 0; l <= lmax; ++l) {
+    smax = fmax(smax, __longlong_as_double((long long)cu[l].smax_bits));
+    cu[l].smax_bits = 0ull;
+    st |= cu[l].status;
+  }
+  S.status |= st;
+  bool const run = S.active && !S.status;
+  double dt = 0.0;
+  if (run) {
+    double cur = S.t;
+    for (int k = 0; k < tm; ++k) cur = cur + S.hist[k];
+    double const rate = smax / S.h_fine;
+    double local = rate == 0.0 ? DBL_MAX : S.cfl / rate;
+    if (cur + local > S.t_end) local = fmax(S.t_end - cur, 0.0);
+    dt = local;
+  }
+  S.hist[tm] = dt;
+  int const lu = lmax - levels_height(tm) + 1;
+  int const lf = tm == 0 ? 0 : lmax - levels_height(tm - 1) + 1;
+  for (int l = 0; l <= lmax; ++l) {
+    double dtl = 0.0;
+    if (l >= lu)
+      for (int k = tm; k > tm - (1 << (lmax - l)); --k) dtl += S.hist[k];
+    cu[l].dt = run ? dtl : 0.0;
+    cf[l].dt = (run && l >= lf) ? 1.0 : 0.0;
+  }
+}
+
+__global__ void levels_commit_kernel(LevelState *ls, int tm, int nmicro) {
+  LevelState &S = *ls;
+  if (!S.active) return;
+  S.micro += 1;
+  if (tm == nmicro - 1) {
+    double sum = 0.0;
+    for (int k = 0; k < nmicro; ++k) sum = sum + S.hist[k];
+    S.t = S.t + sum;
+    S.macro += 1;
+  }
+}
+
+struct NodeKey {
+  int l, c[3];
+  bool operator<(NodeKey const &o) const {
+    return std::tie(l, c[0], c[1], c[2]) < std::tie(o.l, o.c[0], o.c[1], o.c[2]);
+  }
+};
+
+}  // namespace
+
+struct alp_levels {
+  int dim = 3, scheme = 0, precision = 0, lmax = 0, nlev = 1, nmicro = 1;
+  int nleaf = 0, nghost = 0, nslots = 0, ne = 5, cells = 0, faces = 0;
+  long long cell_updates_per_macro = 0;
+  double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
+  BlockMeta *meta = nullptr;
+  int *nbr26 = nullptr, *work = nullptr;
+  GhostRec *ghosts = nullptr;
+  CaseState *cu = nullptr, *cf = nullptr;
+  LevelState *ls = nullptr;
+  std::vector<int> nwork_ge;  // work items of level >= l
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph = nullptr;
+
+  long long dstride() const { return (long long)ne * faces; }
+  long long stride() const { return dstride() * dim; }
+
+  int record_macro() {
+    Launch L{dim, scheme, precision, U, work, nleaf, meta, BlockMeta{}, stream};
+    double *in[3] = {U, UB, UC};
+    double *out[3] = {UB, UC, U};
+    for (int tm = 0; tm < nmicro; ++tm) {
+      Launch La = L;
+      ALP_CUDA(launch_signal_speed(La, cu, nullptr));
+      levels_dt_kernel<<<1, 1, 0, stream>>>(ls, cu, cf, lmax, tm);
+      ALP_CUDA(cudaGetLastError());
+      auto height = [](int t) { return __builtin_popcount((unsigned)((t + 1) ^ t)); };
+      int const lu = lmax - height(tm) + 1;
+      int const lf = tm == 0 ? 0 : lmax - height(tm - 1) + 1;
+      for (int s = 0; s < 3; ++s) {
+        CaseState const *gate = s == 0 ? cf : cu;
+        if (nghost > 0) {
+          dim3 grid(nghost, 2 * dim);
+          switch (dim) {
+            case 1: ghost_fill_kernel<1><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
+            case 2: ghost_fill_kernel<2><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
+            default: ghost_fill_kernel<3><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
+          }
+          ALP_CUDA(cudaGetLastError());
+        }
+        Launch Ls = L;
+        Ls.U = in[s];
+        Ls.nwork = nwork_ge[s == 0 ? lf : lu];
+        if (Ls.nwork > 0)
+          ALP_CUDA(launch_face_flux_all(Ls, nbr26, gate, F, stride(), dstride(), 128));
+        Ls.nwork = nwork_ge[lu];
+        if (Ls.nwork > 0)
+          ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cu, 0.0));
+      }
+      levels_commit_kernel<<<1, 1, 0, stream>>>(ls, tm, nmicro);
+      ALP_CUDA(cudaGetLastError());
+    }
+    return ALP_OK;
+  }
+
+  void release() {
+    if (graph) cudaGraphExecDestroy(graph);
+    cudaFree(U);
+    cudaFree(UB);
+    cudaFree(UC);
+    cudaFree(F);
+    cudaFree(meta);
+    cudaFree(nbr26);
+    cudaFree(work);
+    cudaFree(ghosts);
+    cudaFree(cu);
+    cudaFree(cf);
+    cudaFree(ls);
+    if (stream) cudaStreamDestroy(stream);
+  }
+};
+
+namespace {
+
+// Validates the tree and builds the per-slot neighbour table and the ghosts.
+int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const *coord,
+               std::vector<int> &nbr26, std::vector<GhostRec> &ghosts, int *lmax_out) {
+  using alp::fail;
+  int lmax = 0;
+  for (int b = 0; b < nleaf; ++b) {
+    if (level[b] < 0 || level[b] >= kMaxLevels)
+      return fail(ALP_ERR_INVALID, "leaf level outside 0.." + std::to_string(kMaxLevels - 1));
+    lmax = std::max(lmax, level[b]);
+  }
+  std::map<NodeKey, int> leaf, refined;  // refined: value unused
+  auto key = [&](int l, int const *c) {
+    NodeKey k{l, {0, 0, 0}};
+    for (int d = 0; d < dim; ++d) k.c[d] = c[d];
+    return k;
+  };
+  auto extent = [&](int l, int d) { return d < dim ? n0[d] << l : 1; };
+  for (int b = 0; b < nleaf; ++b) {
+    int const *c = coord + 3 * b;
+    for (int d = 0; d < dim; ++d)
+      if (c[d] < 0 || c[d] >= extent(level[b], d))
+        return fail(ALP_ERR_INVALID, "leaf " + std::to_string(b) + " lies outside the box");
+    if (!leaf.emplace(key(level[b], c), b).second)
+      return fail(ALP_ERR_INVALID, "two leaves share node " + std::to_string(b));
+  }
+  for (int b = 0; b < nleaf; ++b)
+    for (int a = level[b] - 1; a >= 0; --a) {
+      int c[3] = {0, 0, 0};
+      for (int d = 0; d < dim; ++d) c[d] = coord[3 * b + d] >> (level[b] - a);
+      NodeKey const k = key(a, c);
+      if (leaf.count(k)) return fail(ALP_ERR_INVALID, "a leaf overlaps leaf " + std::to_string(b));
+      refined.emplace(k, 0);
+    }
+  // tiling: level-0 nodes all present; refined nodes have all children
+  long long n0tot = 1;
+  for (int d = 0; d < dim; ++d) n0tot *= n0[d];
+  long long covered = 0;
+  for (auto const &kv : leaf)
+    if (kv.first.l == 0) ++covered;
+  for (auto const &kv : refined)
+    if (kv.first.l == 0) ++covered;
+  if (covered != n0tot) return fail(ALP_ERR_INVALID, "leaves do not cover every level-0 node");
+  for (auto const &kv : refined)
+    for (int o = 0; o < (1 << dim); ++o) {
+      int c[3] = {0, 0, 0};
+      for (int d = 0; d < dim; ++d) c[d] = 2 * kv.first.c[d] + ((o >> d) & 1);
+      NodeKey const k = key(kv.first.l + 1, c);
+      if (!leaf.count(k) && !refined.count(k))
+        return fail(ALP_ERR_INVALID, "a refined node misses a child");
+    }
+  // face neighbours: same-level leaf, ghost of a refined node (finer leaves),
+  // ghost inside a coarser leaf, or -1 (domain face)
+  static int const face_slot[6] = {4, 21, 10, 15, 12, 13};
+  nbr26.assign((size_t)nleaf * 26, -1);
+  std::map<NodeKey, int> ghost_of;
+  for (int b = 0; b < nleaf; ++b) {
+    int const l = level[b];
+    for (int f = 0; f < 2 * dim; ++f) {
+      int const d = f / 2, s = (f % 2) ? 1 : -1;
+      int p[3] = {0, 0, 0};
+      for (int e = 0; e < dim; ++e) p[e] = coord[3 * b + e];
+      p[d] += s;
+      if (p[d] < 0 || p[d] >= extent(l, d)) continue;
+      NodeKey const k = key(l, p);
+      auto it = leaf.find(k);
+      if (it != leaf.end()) {
+        nbr26[(size_t)b * 26 + face_slot[f]] = it->second;
+        continue;
+      }
+      GhostRec gr{};
+      gr.level = l;
+      for (int o = 0; o < 8; ++o) gr.src[o] = -1;
+      if (refined.count(k)) {
+        gr.type = 1;
+        gr.src_level = l + 1;
+        for (int o = 0; o < (1 << dim); ++o) {
+          int c[3] = {0, 0, 0};
+          for (int e = 0; e < dim; ++e) c[e] = 2 * p[e] + ((o >> e) & 1);
+          auto ci = leaf.find(key(l + 1, c));
+          bool const face_child = ((o >> d) & 1) == (s > 0 ? 0 : 1);
+          if (ci == leaf.end() && face_child)
+            return fail(ALP_ERR_INVALID, "face neighbours more than one level apart at leaf " +
+                                             std::to_string(b));
+          gr.src[o] = ci == leaf.end() ? -1 : ci->second;
+        }
+      } else {
+        int q[3] = {0, 0, 0};
+        for (int e = 0; e < dim; ++e) q[e] = p[e] >> 1;
+        auto ci = l > 0 ? leaf.find(key(l - 1, q)) : leaf.end();
+        if (ci == leaf.end())
+          return fail(ALP_ERR_INVALID, "face neighbours more than one level apart at leaf " +
+                                           std::to_string(b));
+        gr.type = 0;
+        gr.src_level = l - 1;
+        gr.src[0] = ci->second;
+        int oct = 0;
+        for (int e = 0; e < dim; ++e) oct |= (p[e] & 1) << e;
+        gr.src[1] = oct;
+      }
+      // the leaf sits on the (s < 0 ? high : low) side of the ghost
+      int const ghost_face = 2 * d + (s < 0 ? 1 : 0);
+      auto gi = ghost_of.find(k);
+      int idx;
+      if (gi == ghost_of.end()) {
+        idx = (int)ghosts.size();
+        gr.slot = nleaf + idx;
+        gr.faces = 0;
+        ghosts.push_back(gr);
+        ghost_of.emplace(k, idx);
+      } else {
+        idx = gi->second;
+      }
+      ghosts[idx].faces |= 1 << ghost_face;
+      nbr26[(size_t)b * 26 + face_slot[f]] = nleaf + idx;
+    }
+  }
+  *lmax_out = lmax;
+  return ALP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat, const int *n0,
+                      double h0, int nleaf, const int *h_level, const int *h_coord, double cfl,
+                      double t0, double t_end, int max_macro_steps, const double *h_blocks,
+                      alp_levels **out) {
+  using namespace alp;
+  if (!out) return fail(ALP_ERR_INVALID, "out is null");
+  *out = nullptr;
+  if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  int sid, prec;
+  if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  if (int rc = check_material(mat)) return rc;
+  if (!n0 || !h_level || !h_coord || !h_blocks || nleaf <= 0)
+    return fail(ALP_ERR_INVALID, "empty or null tree description");
+  for (int d = 0; d < dim; ++d)
+    if (n0[d] <= 0) return fail(ALP_ERR_INVALID, "n0 must be positive");
+  if (!(h0 > 0.0) || !(cfl > 0.0)) return fail(ALP_ERR_INVALID, "h0 and cfl must be positive");
+  int n0v[3] = {1, 1, 1};
+  for (int d = 0; d < dim; ++d) n0v[d] = n0[d];
+  std::vector<int> nbr;
+  std::vector<GhostRec> gh;
+  int lmax = 0;
+  if (int rc = build_tree(dim, n0v, nleaf, h_level, h_coord, nbr, gh, &lmax)) return rc;
+
+  alp_levels *m = new (std::nothrow) alp_levels;
+  if (!m) return fail(ALP_ERR_CUDA, "host allocation failed");
+  m->dim = dim;
+  m->scheme = sid;
+  m->precision = prec;
+  m->lmax = lmax;
+  m->nlev = lmax + 1;
+  m->nmicro = 1 << lmax;
+  m->nleaf = nleaf;
+  m->nghost = (int)gh.size();
+  m->nslots = nleaf + m->nghost;
+  m->ne = dim + 2;
+  m->cells = 24 * (dim > 1 ? 24 : 1) * (dim > 2 ? 24 : 1);
+  m->faces = 17 * (dim > 1 ? 17 : 2) * (dim > 2 ? 17 : 2);
+  int const icells = 16 * (dim > 1 ? 16 : 1) * (dim > 2 ? 16 : 1);
+  for (int b = 0; b < nleaf; ++b) m->cell_updates_per_macro += (long long)icells << h_level[b];
+
+  // work list: finest level first (stable), prefix counts per level
+  std::vector<int> work(nleaf);
+  for (int b = 0; b < nleaf; ++b) work[b] = b;
+  std::stable_sort(work.begin(), work.end(),
+                   [&](int a, int b) { return h_level[a] > h_level[b]; });
+  m->nwork_ge.assign(m->nlev + 1, 0);
+  for (int l = 0; l <= lmax; ++l)
+    for (int b = 0; b < nleaf; ++b)
+      if (h_level[b] >= l) ++m->nwork_ge[l];
+
+  std::vector<BlockMeta> meta(m->nslots);
+  for (int b = 0; b < nleaf; ++b)
+    meta[b] = meta_of(mat, h0 / (double)(1 << h_level[b]), h_level[b]);
+  for (int g = 0; g < m->nghost; ++g)
+    meta[nleaf + g] = meta_of(mat, h0 / (double)(1 << gh[g].level), gh[g].level);
+  nbr.resize((size_t)m->nslots * 26, -1);
+
+  size_t const blk = (size_t)m->ne * m->cells * sizeof(double);
+  size_t const pool = blk * m->nslots;
+  auto cleanup = [&](int rc) {
+    m->release();
+    delete m;
+    return rc;
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaStreamCreate"));
+  void **bufs[] = {(void **)&m->U, (void **)&m->UB, (void **)&m->UC};
+  for (void **b : bufs) {
+    e = cudaMalloc(b, pool);
+    if (e == cudaSuccess) e = cudaMemsetAsync(*b, 0, pool, m->stream);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaMalloc(level pools)"));
+  }
+  size_t const fbytes = (size_t)m->stride() * nleaf * sizeof(double);
+  if ((e = cudaMalloc(&m->F, fbytes)) != cudaSuccess ||
+      (e = cudaMalloc(&m->meta, sizeof(BlockMeta) * m->nslots)) != cudaSuccess ||
+      (e = cudaMalloc(&m->nbr26, sizeof(int) * nbr.size())) != cudaSuccess ||
+      (e = cudaMalloc(&m->work, sizeof(int) * nleaf)) != cudaSuccess ||
+      (e = cudaMalloc(&m->ghosts, sizeof(GhostRec) * std::max(m->nghost, 1))) != cudaSuccess ||
+      (e = cudaMalloc(&m->cu, sizeof(CaseState) * m->nlev)) != cudaSuccess ||
+      (e = cudaMalloc(&m->cf, sizeof(CaseState) * m->nlev)) != cudaSuccess ||
+      (e = cudaMalloc(&m->ls, sizeof(LevelState))) != cudaSuccess)
+    return cleanup(cuda_fail(e, "cudaMalloc(level tables)"));
+  std::vector<CaseState> cs(m->nlev);
+  for (auto &c : cs) {
+    c = CaseState{};
+    c.t = t0;
+    c.t_end = t_end;
+    c.cfl = cfl;
+    c.h_min = h0 / (double)m->nmicro;
+  }
+  LevelState st{};
+  st.t = t0;
+  st.t_end = t_end;
+  st.cfl = cfl;
+  st.h_fine = h0 / (double)m->nmicro;
+  st.max_macro = max_macro_steps;
+  for (int b = 0; b < nleaf; ++b) {
+    e = cudaMemcpyAsync(m->U + (size_t)b * m->ne * m->cells, h_blocks + (size_t)b * m->ne * m->cells,
+                        blk, cudaMemcpyHostToDevice, m->stream);
+    if (e != cudaSuccess) break;
+  }
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->meta, meta.data(), sizeof(BlockMeta) * m->nslots,
+                        cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->nbr26, nbr.data(), sizeof(int) * nbr.size(), cudaMemcpyHostToDevice,
+                        m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->work, work.data(), sizeof(int) * nleaf, cudaMemcpyHostToDevice,
+                        m->stream);
+  if (e == cudaSuccess && m->nghost)
+    e = cudaMemcpyAsync(m->ghosts, gh.data(), sizeof(GhostRec) * m->nghost,
+                        cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->cu, cs.data(), sizeof(CaseState) * m->nlev, cudaMemcpyHostToDevice,
+                        m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->cf, cs.data(), sizeof(CaseState) * m->nlev, cudaMemcpyHostToDevice,
+                        m->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(m->ls, &st, sizeof(st), cudaMemcpyHostToDevice, m->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(m->stream);
+  if (e != cudaSuccess) return cleanup(cuda_fail(e, "level case upload"));
+  *out = m;
+  return ALP_OK;
+}
+
+int alp_levels_destroy(alp_levels *m) {
+  if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  cudaStreamSynchronize(m->stream);
+  m->release();
+  delete m;
+  return ALP_OK;
+}
+
+int alp_levels_step(alp_levels *m, int n_macro) {
+  if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  if (n_macro <= 0) return ALP_OK;
+  if (!m->graph) {
+    cudaGraph_t g;
+    ALP_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+    int const rc = m->record_macro();
+    cudaError_t const e = cudaStreamEndCapture(m->stream, &g);
+    if (rc) {
+      if (e == cudaSuccess) cudaGraphDestroy(g);
+      return rc;
+    }
+    if (e != cudaSuccess) return alp::cuda_fail(e, "cudaStreamEndCapture");
+    cudaError_t const ei = cudaGraphInstantiate(&m->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ei != cudaSuccess) return alp::cuda_fail(ei, "cudaGraphInstantiate");
+  }
+  for (int i = 0; i < n_macro; ++i) ALP_CUDA(cudaGraphLaunch(m->graph, m->stream));
+  return ALP_OK;
+}
+
+int alp_levels_get(alp_levels *m, double *h_blocks, double *t, int *macro_steps) {
+  if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  if (h_blocks)
+    ALP_CUDA(cudaMemcpyAsync(h_blocks, m->U, sizeof(double) * m->ne * m->cells * m->nleaf,
+                             cudaMemcpyDeviceToHost, m->stream));
+  LevelState st;
+  ALP_CUDA(cudaMemcpyAsync(&st, m->ls, sizeof(st), cudaMemcpyDeviceToHost, m->stream));
+  ALP_CUDA(cudaStreamSynchronize(m->stream));
+  if (t) *t = st.t;
+  if (macro_steps) *macro_steps = st.macro;
+  if (st.status) return alp::fail(ALP_ERR_NUMERIC, "non-finite or non-positive state; case stopped");
+  return ALP_OK;
+}
+
+int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
+                    long long *cell_updates_per_macro_step, int *launches_per_macro_step) {
+  if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  if (n_ghosts) *n_ghosts = m->nghost;
+  if (max_level) *max_level = m->lmax;
+  if (cell_updates_per_macro_step) *cell_updates_per_macro_step = m->cell_updates_per_macro;
+  if (launches_per_macro_step) {
+    int per_micro = 2 + 1;  // signal speed, micro dt, commit
+    auto height = [](int t) { return __builtin_popcount((unsigned)((t + 1) ^ t)); };
+    int n = 0;
+    for (int tm = 0; tm < m->nmicro; ++tm) {
+      int const lu = m->lmax - height(tm) + 1;
+      int const lf = tm == 0 ? 0 : m->lmax - height(tm - 1) + 1;
+      n += per_micro;
+      for (int s = 0; s < 3; ++s) {
+        n += m->nghost > 0 ? 1 : 0;
+        n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? 1 : 0;
+        n += m->nwork_ge[lu] > 0 ? 1 : 0;
+      }
+    }
+    *launches_per_macro_step = n;
+  }
+  return ALP_OK;
+}
+
+alp_stream_t alp_levels_stream(alp_levels *m) { return m ? (alp_stream_t)m->stream : nullptr; }
+
+}  // extern "C"

@@ -128,6 +128,14 @@ _SIGS = {
     "alp_engine_launches_per_step": (C.c_int, [_V]),
     "alp_engine_autotune": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_float)]),
     "alp_engine_set_path": (C.c_int, [_V, C.c_int]),
+    "alp_levels_create": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _I, C.c_double,
+                                    C.c_int, _I, _I, C.c_double, C.c_double, C.c_double, C.c_int,
+                                    _D, C.POINTER(_V)]),
+    "alp_levels_destroy": (C.c_int, [_V]),
+    "alp_levels_step": (C.c_int, [_V, C.c_int]),
+    "alp_levels_get": (C.c_int, [_V, _D, _D, _I]),
+    "alp_levels_info": (C.c_int, [_V, _I, _I, C.POINTER(C.c_longlong), _I]),
+    "alp_levels_stream": (_S, [_V]),
 }
 
 _libs = {}

@@ -59,6 +59,9 @@ def parse():
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving comparison and print its JSON")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--levels", action="store_true",
+                   help="multi-level batching: 3-level spherical-shock hierarchy with local "
+                        "time stepping (one line; steps are macro steps)")
     return p.parse_args()
 
 
@@ -301,6 +304,54 @@ def precision_report(steps: int = 200, emit=None):
     return rows
 
 
+def levels_report(args):
+    """Multi-level batching form: the 48 / 469 / 1176-leaf three-level
+    spherical-shock hierarchy advanced with local time stepping (a macro step
+    is 4 micro steps; level l takes 2^l RK3 steps per macro step), all levels
+    in the same batched launches, one CUDA graph per macro step. Timed with
+    CUDA events on the case's stream after W warm-up macro steps."""
+    import torch
+
+    from alpaca_b200 import api, cases
+    case = cases.spherical_shock_levels()
+    prec = 1 if args.precision == "fp32" else 0
+    eng = api.LevelEngine(case, args.variant, precision=prec)
+    info = eng.info()
+    stream = torch.cuda.ExternalStream(eng.stream_handle)
+    eng.step(max(args.warmup, 3))
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        e0.record(stream)
+        eng.step(args.steps)
+        e1.record(stream)
+        e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, t, macro = eng.get()
+    eng.close()
+    cu = info["cell_updates_per_macro_step"] * args.steps
+    value = cu / (ms * 1e-3)
+    hbm, src = peaks()
+    return {
+        "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": 1, "steps": args.steps,
+        "warmup": max(args.warmup, 3), "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64" if args.precision == "fp64" else "f32-flux/f64-state", "data": "synthetic",
+        "config": {"workload": "3d_spherical_shock_3_levels", "leaves_per_level": case.leaves_per_level(),
+                   "ghost_blocks": info["ghosts"], "variant": args.variant,
+                   "step": "macro step = 4 micro steps (local time stepping)",
+                   "cell_updates_per_macro_step": info["cell_updates_per_macro_step"],
+                   "jumps": "injection / Multiresolution::Average halos, no jump-flux correction",
+                   "sim_time_reached": t, "macro_steps_done": macro,
+                   "l2": "state %.2f GB per pool > 126 MB L2 (no flush needed)"
+                         % ((case.nleaf + info["ghosts"]) * 5 * 24 ** 3 * 8 / 1e9)},
+        "roofline": {"bound": "hbm", "achieved": value * B_ALG_3D / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": value * B_ALG_3D / 1e9 / hbm, "traffic": None, "peak_source": src},
+        "gpu_launches": info["launches_per_macro_step"] * args.steps,
+        "clocks": clocks.summary(),
+    }
+
+
 def run_ours(args, ws, rank, local):
     import numpy as np
     import torch
@@ -438,6 +489,11 @@ def main():
             import torch
             torch.cuda.set_device(local)
             precision_report(emit=lambda row: print(json.dumps(row), flush=True))
+        elif args.levels:
+            import torch
+            torch.cuda.set_device(local)
+            if rank == 0:
+                print(json.dumps(levels_report(args)), flush=True)
         elif args.serving_only:
             import torch
             torch.cuda.set_device(local)

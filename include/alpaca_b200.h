@@ -241,6 +241,42 @@ int alp_engine_set_path(alp_engine *e, int candidate);
 /* Number of kernel launches one engine step issues. */
 int alp_engine_launches_per_step(alp_engine *e);
 
+/* ---- multi-level cases: leaves of a block tree, local time stepping ----- */
+
+/* A case whose blocks are the leaves of a block tree (the reference's
+ * multiresolution levels, topology/node.cpp) over a box of n0[0] x n0[1] x
+ * n0[2] level-0 nodes with zero-gradient domain faces. Leaf b has level
+ * h_level[b] (0..6) and integer node coordinates h_coord[3b..3b+2] in units of
+ * its own node size; its cell size is h0 / 2^level. Face neighbours may differ
+ * by one level at most. Time stepping as ModularAlgorithmAssembler::Advance
+ * (modular_algorithm_assembler.cpp:575-874): a macro step is 2^lmax micro
+ * steps, micro step t integrates the levels of GetLevels(t) (:2564-2573), each
+ * with the sum of its last 2^(lmax-level) micro time steps (Integrate,
+ * :1068-1098); the micro time step is ComputeTimestepSize over all leaves with
+ * the finest cell size (:1925-1982). Halo cells across a level jump are the
+ * average of the finer leaves (Multiresolution::Average,
+ * multiresolution/multiresolution.h:94-166) or the coarser leaf's cell
+ * (injection); the reference's fifth-order prediction
+ * (multiresolution.cpp:146) and jump-flux correction (:1347) are not applied.
+ * h_blocks: [nleaf][NE][cells], interiors read. All levels run in the same
+ * batched launches; one CUDA graph per macro step. */
+typedef struct alp_levels alp_levels;
+int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat, const int *n0,
+                      double h0, int nleaf, const int *h_level, const int *h_coord, double cfl,
+                      double t0, double t_end, int max_macro_steps, const double *h_blocks,
+                      alp_levels **out);
+int alp_levels_destroy(alp_levels *m);
+/* Advances n macro steps (asynchronous). */
+int alp_levels_step(alp_levels *m, int n_macro);
+/* Copies the leaves (interiors valid) and the time / macro steps reached;
+ * synchronises. ALP_ERR_NUMERIC once a non-finite state stopped the case. */
+int alp_levels_get(alp_levels *m, double *h_blocks, double *t, int *macro_steps);
+/* Ghost blocks at level jumps, finest level, interior cells x RK3 steps per
+ * macro step summed over the leaves, kernel launches per macro step. */
+int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
+                    long long *cell_updates_per_macro_step, int *launches_per_macro_step);
+alp_stream_t alp_levels_stream(alp_levels *m);
+
 /* ---- serving: continuous batching of independent cases ------------------ */
 
 /* One request: a case on a regular block grid with a device-evaluated initial

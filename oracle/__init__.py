@@ -92,6 +92,9 @@ def _load(path: str):
     lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                C.c_int, C.c_int, _D, _I, _D]
+    lib.oracle_levels_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, _I, _I,
+                                      C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
+                                      C.c_double, C.c_int, C.c_int, _D, _I, _D]
     return lib
 
 
@@ -186,6 +189,27 @@ class Restatement(_Common):
         if rc:
             raise RuntimeError(f"oracle_run rc={rc}")
         return u, t.value, steps.value, dts[: steps.value].copy()
+
+    def levels_run(self, u, level, coord, n0, h0, gamma, B, safe, cfl, t_end, max_macro=0,
+                   t0=0.0, nthreads=1):
+        """Multi-level time loop with local time stepping (leaves of a block
+        tree). Returns (u_final, t, macro_steps, micro_dt_log)."""
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        level = np.ascontiguousarray(level, dtype=np.int32)
+        coord = np.ascontiguousarray(coord, dtype=np.int32).reshape(-1, 3)
+        n0 = np.ascontiguousarray(list(n0) + [1] * (3 - len(n0)), dtype=np.int32)
+        nmicro = 1 << int(level.max())
+        cap = (max_macro if max_macro > 0 else 100000) * nmicro
+        dts = np.zeros(cap)
+        t = C.c_double(t0)
+        macro = C.c_int()
+        rc = self.lib.oracle_levels_run(self.dim, self.solver, self.recon, _dp(u), u.shape[0],
+                                        _ip(level), _ip(coord), _ip(n0), h0, gamma, B, int(safe),
+                                        cfl, t_end, max_macro, nthreads, C.byref(t),
+                                        C.byref(macro), _dp(dts))
+        if rc:
+            raise RuntimeError(f"oracle_levels_run rc={rc}")
+        return u, t.value, macro.value, dts[: macro.value * nmicro].copy()
 
 
 class OpCounting(Restatement):

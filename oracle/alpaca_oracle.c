@@ -1006,3 +1006,336 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr
   *steps_done = steps;
   return 0;
 }
+
+/* ---- multi-level cases: a block tree with local time stepping ------------
+ *
+ * Leaves of levels 0..lmax tile a box of n0[0] x n0[1] x n0[2] level-0 nodes
+ * (inactive dimensions 1); a node of level l has cell size h0 / 2^l and
+ * integer coordinates in units of its own size. Time stepping restates
+ * ModularAlgorithmAssembler::Advance (modular_algorithm_assembler.cpp:575-874):
+ * a macro step is 2^lmax micro steps; micro step t integrates the levels of
+ * GetLevels(t) (:2564-2573), level l with the sum of its last 2^(lmax-l) micro
+ * time steps (Integrate :1068-1098, time_integrator.h:312-340); the stage-0
+ * right-hand side of a level is evaluated at the start of its interval
+ * (levels of GetLevels(t-1), all levels at t = 0). The micro time step is
+ * ComputeTimestepSize over all leaves with the finest cell size, clipped to
+ * the end time with the micro steps taken so far (:1925-1982); the macro time
+ * advances by their sum (FinishMacroTimestep, time_integrator.h:247-252).
+ * A level whose time step is zero is not integrated.
+ *
+ * Halo cells across a jump (a face neighbour one level coarser or finer) are
+ * filled by averaging the finer leaves with Multiresolution::Average
+ * (multiresolution.h:94-166) and by injection from the coarser leaf. The
+ * reference predicts the finer side with a fifth-order interpolation
+ * (Multiresolution::Prediction, multiresolution.cpp:146) and corrects coarse
+ * fluxes at jumps (JumpFluxAdjustment, modular_algorithm_assembler.cpp:1347);
+ * neither is restated. Face neighbours must differ by at most one level.
+ */
+
+#define MAXLEV 8
+
+typedef struct {
+  int dim, lmax, nleaf;
+  int ext[MAXLEV][3];
+  int *grid[MAXLEV]; /* >= 0 leaf index, -1 inside a coarser leaf, -2 refined */
+  const int *level, *coord;
+} Tree;
+
+static long tree_at(const Tree *t, int l, const int c[3]) {
+  return ((long)c[0] * t->ext[l][1] + c[1]) * t->ext[l][2] + c[2];
+}
+
+static void tree_free(Tree *t) {
+  for (int l = 0; l < MAXLEV; ++l) free(t->grid[l]);
+}
+
+/* 0 ok, 4 not a tiling of the box, 5 face neighbours more than one level apart */
+static int tree_build(Tree *t, int dim, int nleaf, const int *level, const int *coord,
+                      const int *n0) {
+  memset(t, 0, sizeof(*t));
+  t->dim = dim;
+  t->nleaf = nleaf;
+  t->level = level;
+  t->coord = coord;
+  int lmax = 0;
+  for (int b = 0; b < nleaf; ++b) {
+    if (level[b] < 0 || level[b] >= MAXLEV) return 4;
+    if (level[b] > lmax) lmax = level[b];
+  }
+  t->lmax = lmax;
+  for (int l = 0; l <= lmax; ++l) {
+    long n = 1;
+    for (int d = 0; d < 3; ++d) {
+      t->ext[l][d] = d < dim ? n0[d] << l : 1;
+      n *= t->ext[l][d];
+    }
+    t->grid[l] = (int *)malloc(sizeof(int) * n);
+    if (!t->grid[l]) return 3;
+    for (long x = 0; x < n; ++x) t->grid[l][x] = -1;
+  }
+  for (int b = 0; b < nleaf; ++b) {
+    int const l = level[b];
+    int c[3];
+    for (int d = 0; d < 3; ++d) {
+      c[d] = d < dim ? coord[3 * b + d] : 0;
+      if (c[d] < 0 || c[d] >= t->ext[l][d]) return 4;
+    }
+    long const x = tree_at(t, l, c);
+    if (t->grid[l][x] != -1) return 4;
+    t->grid[l][x] = b;
+  }
+  for (int b = 0; b < nleaf; ++b)
+    for (int a = level[b] - 1; a >= 0; --a) {
+      int c[3];
+      for (int d = 0; d < 3; ++d) c[d] = d < dim ? coord[3 * b + d] >> (level[b] - a) : 0;
+      long const x = tree_at(t, a, c);
+      if (t->grid[a][x] >= 0) return 4;
+      t->grid[a][x] = -2;
+    }
+  /* every level-0 node present, every refined node has all its children */
+  for (int l = 0; l <= lmax; ++l) {
+    for (int i = 0; i < t->ext[l][0]; ++i)
+      for (int j = 0; j < t->ext[l][1]; ++j)
+        for (int k = 0; k < t->ext[l][2]; ++k) {
+          int const c[3] = {i, j, k};
+          int const v = t->grid[l][tree_at(t, l, c)];
+          if (l == 0 && v == -1) return 4;
+          if (v == -2) {
+            if (l == lmax) return 4;
+            for (int o = 0; o < (1 << dim); ++o) {
+              int cc[3];
+              for (int d = 0; d < 3; ++d) cc[d] = d < dim ? 2 * c[d] + ((o >> d) & 1) : 0;
+              if (t->grid[l + 1][tree_at(t, l + 1, cc)] == -1) return 4;
+            }
+          }
+        }
+  }
+  /* face balance: the neighbour region of a leaf is a leaf of its level, a
+   * refined node whose face children are leaves, or lies in a leaf one level
+   * coarser */
+  for (int b = 0; b < nleaf; ++b) {
+    int const l = level[b];
+    for (int f = 0; f < 2 * dim; ++f) {
+      int const d = f / 2, s = (f % 2) ? 1 : -1;
+      int p[3];
+      for (int e = 0; e < 3; ++e) p[e] = e < dim ? coord[3 * b + e] : 0;
+      p[d] += s;
+      if (p[d] < 0 || p[d] >= t->ext[l][d]) continue;
+      int const v = t->grid[l][tree_at(t, l, p)];
+      if (v == -1) {
+        int q[3];
+        for (int e = 0; e < 3; ++e) q[e] = e < dim ? p[e] >> 1 : 0;
+        if (l == 0 || t->grid[l - 1][tree_at(t, l - 1, q)] < 0) return 5;
+      } else if (v == -2) {
+        for (int o = 0; o < (1 << dim); ++o) {
+          if (((o >> d) & 1) != (s > 0 ? 0 : 1)) continue;
+          int cc[3];
+          for (int e = 0; e < 3; ++e) cc[e] = e < dim ? 2 * p[e] + ((o >> e) & 1) : 0;
+          if (t->grid[l + 1][tree_at(t, l + 1, cc)] < 0) return 5;
+        }
+      }
+    }
+  }
+  return 0;
+}
+
+/* 3D / 2D / 1D conservative average of the 2^dim children cells of a parent
+ * cell (Multiresolution::Average, multiresolution.h:133-158). c points at the
+ * child cell (2a, 2b, 2c) of field buffer f. */
+static double child_average(const Geom *g, const double *f, int i, int j, int k) {
+  if (g->dim == 1) return (f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j, k)]) * 0.5;
+  if (g->dim == 2)
+    return ((f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j + 1, k)]) +
+            (f[cidx(g, i + 1, j, k)] + f[cidx(g, i, j + 1, k)])) * 0.25;
+  double const a = f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j + 1, k + 1)];
+  double const b = f[cidx(g, i, j, k + 1)] + f[cidx(g, i + 1, j + 1, k)];
+  double const c = f[cidx(g, i, j + 1, k)] + f[cidx(g, i + 1, j, k + 1)];
+  double const d = f[cidx(g, i, j + 1, k + 1)] + f[cidx(g, i + 1, j, k)];
+  double const s1 = (a + b) + (c + d);
+  double const s2 = (a + c) + (b + d);
+  double const s3 = (a + d) + (b + c);
+  double const mn = dmin(s1, dmin(s2, s3)), mx = dmax(s1, dmax(s2, s3));
+  return 0.125 * (0.5 * (mn + mx));
+}
+
+/* Face halos (HS layers over the interior extent) of leaf b in pool dst; the
+ * neighbours' values come from src[level] (a pool per level). */
+static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double *const *src) {
+  int const l = t->level[b], ne = g->ne;
+  long const blk = (long)ne * g->cells;
+  double *ub = dst + b * blk;
+  for (int f = 0; f < 2 * g->dim; ++f) {
+    int const d = f / 2, s = (f % 2) ? 1 : -1;
+    int p[3];
+    for (int e = 0; e < 3; ++e) p[e] = e < g->dim ? t->coord[3 * b + e] : 0;
+    p[d] += s;
+    int kind, v = -1;
+    if (p[d] < 0 || p[d] >= t->ext[l][d]) {
+      kind = 0; /* domain face: zero gradient */
+    } else {
+      v = t->grid[l][tree_at(t, l, p)];
+      kind = v >= 0 ? 1 : (v == -2 ? 2 : 3);
+    }
+    int ext[3];
+    for (int e = 0; e < 3; ++e) ext[e] = g->ic[e];
+    ext[d] = HS;
+    for (int h0 = 0; h0 < ext[0]; ++h0)
+      for (int h1 = 0; h1 < ext[1]; ++h1)
+        for (int h2 = 0; h2 < ext[2]; ++h2) {
+          int hh[3] = {h0, h1, h2};
+          /* halo cell in this block, and the neighbour node's interior cell */
+          int hc[3], a[3];
+          for (int e = 0; e < 3; ++e) {
+            hc[e] = fic(g, e) + hh[e];
+            a[e] = hh[e];
+          }
+          hc[d] = s > 0 ? HS + IC + hh[d] : hh[d];
+          a[d] = s > 0 ? hh[d] : IC - HS + hh[d];
+          long const x = cidx(g, hc[0], hc[1], hc[2]);
+          for (int e = 0; e < ne; ++e) {
+            double *fo = ub + (long)e * g->cells;
+            double val;
+            if (kind == 0) {
+              int zc[3] = {hc[0], hc[1], hc[2]};
+              zc[d] = s > 0 ? HS + IC - 1 : HS;
+              val = fo[cidx(g, zc[0], zc[1], zc[2])];
+            } else if (kind == 1) {
+              const double *fs = src[l] + v * blk + (long)e * g->cells;
+              val = fs[cidx(g, fic(g, 0) + a[0], fic(g, 1) + a[1], fic(g, 2) + a[2])];
+            } else if (kind == 2) {
+              int cc[3], ci[3];
+              for (int q = 0; q < 3; ++q) {
+                int const o = q < g->dim ? a[q] / (IC / 2) : 0;
+                cc[q] = q < g->dim ? 2 * p[q] + o : 0;
+                ci[q] = q < g->dim ? fic(g, q) + 2 * (a[q] % (IC / 2)) : 0;
+              }
+              int const c = t->grid[l + 1][tree_at(t, l + 1, cc)];
+              const double *fs = src[l + 1] + c * blk + (long)e * g->cells;
+              val = child_average(g, fs, ci[0], ci[1], ci[2]);
+            } else {
+              int q3[3], ci[3];
+              for (int q = 0; q < 3; ++q) {
+                q3[q] = q < g->dim ? p[q] >> 1 : 0;
+                ci[q] = q < g->dim ? fic(g, q) + (IC / 2) * (p[q] & 1) + a[q] / 2 : 0;
+              }
+              int const c = t->grid[l - 1][tree_at(t, l - 1, q3)];
+              const double *fs = src[l - 1] + c * blk + (long)e * g->cells;
+              val = fs[cidx(g, ci[0], ci[1], ci[2])];
+            }
+            fo[x] = val;
+          }
+        }
+  }
+}
+
+/* number of levels GetLevels(t) returns (modular_algorithm_assembler.cpp:2564-2573) */
+static int get_levels_height(unsigned t) { return __builtin_popcount((t + 1) ^ t); }
+
+typedef struct {
+  const Geom *g;
+  const Eos *e;
+  int solver, recon;
+  const Tree *t;
+  const int *items;
+  double *pool;
+  double *rhs;
+  double h0;
+} LevelRhsCtx;
+
+static void level_rhs_task(void *vctx, int i, Work *w, double *f[3]) {
+  LevelRhsCtx *c = (LevelRhsCtx *)vctx;
+  int const b = c->items[i];
+  long const blk = (long)c->g->ne * c->g->cells;
+  double const h = c->h0 / (double)(1 << c->t->level[b]);
+  block_fluxes(c->g, c->e, c->solver, c->recon, c->pool + b * blk, w, f);
+  block_divergence(c->g, h, f, c->rhs + b * blk);
+}
+
+int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, const int *level,
+                      const int *coord, const int *n0, double h0, double gamma, double B,
+                      int safe, double cfl, double t_end, int max_macro, int nthreads,
+                      double *t_io, int *macro_done, double *dt_log) {
+  if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
+  Geom g = make_geom(dim);
+  Eos e = {dim, gamma, B, safe};
+  Tree tr;
+  int rc = tree_build(&tr, dim, nleaf, level, coord, n0);
+  if (rc) {
+    tree_free(&tr);
+    return rc;
+  }
+  int const lmax = tr.lmax, nmicro = 1 << lmax;
+  long const blk = (long)g.ne * g.cells, n = (long)nleaf * blk;
+  double *pb = (double *)malloc(sizeof(double) * n);
+  double *pc = (double *)malloc(sizeof(double) * n);
+  double *rhs = (double *)calloc((size_t)n, sizeof(double));
+  int *items = (int *)malloc(sizeof(int) * nleaf);
+  double *hist = (double *)malloc(sizeof(double) * nmicro);
+  if (!pb || !pc || !rhs || !items || !hist) {
+    free(pb); free(pc); free(rhs); free(items); free(hist);
+    tree_free(&tr);
+    return 3;
+  }
+  memcpy(pb, u, sizeof(double) * n);
+  memcpy(pc, u, sizeof(double) * n);
+  double *pool_in[3] = {u, pb, pc};
+  double *pool_out[3] = {pb, pc, u};
+  double const h_fine = h0 / (double)nmicro;
+  double t = *t_io;
+  int macro = 0, logged = 0;
+  while (t < t_end && (max_macro <= 0 || macro < max_macro)) {
+    for (int tm = 0; tm < nmicro; ++tm) {
+      double cur = t;
+      for (int k = 0; k < tm; ++k) cur = cur + hist[k];
+      double dt;
+      oracle_timestep(dim, u, nleaf, gamma, B, safe, h_fine, cfl, cur, t_end, &dt);
+      hist[tm] = dt;
+      if (dt_log) dt_log[logged] = dt;
+      ++logged;
+      int const lu = lmax - get_levels_height((unsigned)tm) + 1;
+      int const lf0 = tm == 0 ? 0 : lmax - get_levels_height((unsigned)(tm - 1)) + 1;
+      for (int s = 0; s < 3; ++s) {
+        int const lflux = s == 0 ? lf0 : lu;
+        double *src[MAXLEV];
+        for (int l = 0; l <= lmax; ++l) src[l] = (s > 0 && l >= lu) ? pool_in[s] : u;
+        int ni = 0;
+        for (int b = 0; b < nleaf; ++b)
+          if (level[b] >= lflux) {
+            level_halos(&g, &tr, b, pool_in[s], src);
+            items[ni++] = b;
+          }
+        LevelRhsCtx c = {&g, &e, solver, recon, &tr, items, pool_in[s], rhs, h0};
+        parallel_blocks(&g, ni, nthreads, level_rhs_task, &c);
+        for (int b = 0; b < nleaf; ++b) {
+          int const l = level[b];
+          if (l < lu) continue;
+          double dtl = 0.0;
+          for (int k = tm; k > tm - (1 << (lmax - l)); --k) dtl += hist[k];
+          if (!(dtl > 0.0)) continue;
+          double const step = rk_c[s] * (0.0 + dtl);
+          double const m0 = rk_a[s][0], m1 = rk_a[s][1];
+          const double *ui = pool_in[s] + b * blk, *u0 = u + b * blk, *r = rhs + b * blk;
+          double *uo = pool_out[s] + b * blk;
+          for (int f = 0; f < g.ne; ++f)
+            for (int i = fic(&g, 0); i <= lic(&g, 0); ++i)
+              for (int j = fic(&g, 1); j <= lic(&g, 1); ++j)
+                for (int k = fic(&g, 2); k <= lic(&g, 2); ++k) {
+                  long const x = (long)f * g.cells + cidx(&g, i, j, k);
+                  double v = ui[x];
+                  if (s != 0) v = m0 * v + m1 * u0[x];
+                  uo[x] = v + step * r[x];
+                }
+        }
+      }
+    }
+    double sum = 0.0;
+    for (int k = 0; k < nmicro; ++k) sum = sum + hist[k];
+    t = t + sum;
+    ++macro;
+  }
+  free(pb); free(pc); free(rhs); free(items); free(hist);
+  tree_free(&tr);
+  *t_io = t;
+  *macro_done = macro;
+  return 0;
+}

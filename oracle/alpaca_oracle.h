@@ -59,6 +59,19 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb,
                double cell_size, double cfl, double t_end, int max_steps,
                int nthreads, double *t_io, int *steps_done, double *dt_log);
 
+/* Multi-level case: nleaf leaves, leaf b of level level[b] at integer node
+ * coordinates coord[3b..3b+2] (units of its own node size) in a box of
+ * n0[0] x n0[1] x n0[2] level-0 nodes with level-0 cell size h0; zero-gradient
+ * domain faces. u [nleaf] blocks (interiors read and written). Local time
+ * stepping over macro steps of 2^lmax micro steps; dt_log receives every
+ * micro time step. Returns 0, or 4 (leaves do not tile the box) or 5 (face
+ * neighbours more than one level apart). */
+int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf,
+                      const int *level, const int *coord, const int *n0, double h0,
+                      double gamma, double B, int safe, double cfl, double t_end,
+                      int max_macro, int nthreads, double *t_io, int *macro_done,
+                      double *dt_log);
+
 #ifdef __cplusplus
 }
 #endif

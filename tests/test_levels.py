@@ -1,0 +1,106 @@
+"""Multi-level cases on the CPU: the oracle's local time stepping reduces to the
+single-level loop where it must, and the C ABI rejects trees that are not a
+face-balanced tiling before touching the device."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from alpaca_b200 import cases
+from alpaca_b200 import native as N
+
+
+def smooth_grid_case(dim, nblocks, cell_size, seed):
+    g = cases.BlockGrid(dim, nblocks, (False,) * dim, cell_size)
+    rng = np.random.default_rng(seed)
+    x = g.cell_centres()
+    shp = g.cells_shape()
+    rho = 1 + 0.1 * cases.fourier_modes(rng, shp, x, dim)
+    p = 1 + 0.1 * cases.fourier_modes(rng, shp, x, dim)
+    vel = [0.2 * cases.fourier_modes(rng, shp, x, dim) for _ in range(dim)]
+    return g, g.scatter(cases.primes_to_conservatives(dim, rho, p, vel, 1.4))
+
+
+def test_single_level_tree_is_the_single_level_loop():
+    """lmax = 0: one micro step per macro step, same bits as oracle_run."""
+    g, u = smooth_grid_case(2, (3, 2), 1.0 / 48, 2)
+    R = oracle.Restatement(2, "fvchar")
+    a = R.run(u, g.nbr, 1.4, 0.0, False, g.cell_size, 0.6, 1e300, max_steps=3)
+    b = R.levels_run(u, np.zeros(g.nb, np.int32), g.coords, (3, 2), g.cell_size, 1.4, 0.0, False,
+                     0.6, 1e300, max_macro=3)
+    I = cases.interior(2)
+    assert np.array_equal(a[0][I], b[0][I])
+    assert a[1] == b[1] and np.array_equal(a[3], b[3])
+
+
+def test_uniform_finer_level_takes_two_micro_steps():
+    """All leaves on level 1: two micro steps per macro step, each the
+    single-level step with the level-1 cell size (final time may differ in the
+    last bit: the macro time adds the micro steps as one sum)."""
+    g, u = smooth_grid_case(2, (4, 2), 1.0 / 64, 3)
+    R = oracle.Restatement(2, "fsroe")
+    a = R.run(u, g.nbr, 1.4, 0.0, False, g.cell_size, 0.6, 1e300, max_steps=4)
+    b = R.levels_run(u, np.ones(g.nb, np.int32), g.coords, (2, 1), 2 * g.cell_size, 1.4, 0.0,
+                     False, 0.6, 1e300, max_macro=2)
+    I = cases.interior(2)
+    assert np.array_equal(a[0][I], b[0][I])
+    assert np.array_equal(a[3], b[3]) and abs(a[1] - b[1]) <= 1e-15 * a[1]
+
+
+def test_three_level_tree_runs_and_nearly_conserves():
+    """2D three-level tree: finite states; mass changes only through the jumps
+    (no jump-flux correction), by far less than its round-off-free scale."""
+    c = cases.spherical_shock_levels(n0=4, dim=2, lmax=2)
+    u, t, macro, dts = oracle.Restatement(2, "fvchar").levels_run(
+        c.u, c.level, c.coord, c.n0, c.h0, c.gamma, 0.0, False, 0.6, 1e300, max_macro=1)
+    I = cases.interior(2)
+    assert macro == 1 and len(dts) == 4 and np.all(dts > 0) and t == pytest.approx(dts.sum())
+    assert np.isfinite(u[I]).all() and (u[I][:, 0] > 0).all()
+    vol = (c.h0 / (1 << c.level)) ** 2
+    m0 = (c.u[I][:, 0].reshape(c.nleaf, -1).sum(1) * vol).sum()
+    m1 = (u[I][:, 0].reshape(c.nleaf, -1).sum(1) * vol).sum()
+    assert abs(m1 - m0) <= 1e-6 * m0
+
+
+def test_leaves_per_level_of_the_spherical_shock_hierarchy():
+    c = cases.spherical_shock_levels()
+    assert c.leaves_per_level() == [48, 469, 1176]
+    assert c.cell_updates_per_macro_step() == 4096 * (48 + 2 * 469 + 4 * 1176)
+
+
+# ---- the C ABI validates the tree on the host --------------------------------
+
+def _create(dim, n0, level, coord, h0=1.0 / 32):
+    lib = N.lib()
+    sch = N.Scheme.make("fvchar")
+    mat = N.Material.make(1.4)
+    level = np.ascontiguousarray(level, dtype=np.int32)
+    coord = np.ascontiguousarray(coord, dtype=np.int32).reshape(-1, 3)
+    n0 = np.ascontiguousarray(list(n0) + [1] * (3 - len(n0)), dtype=np.int32)
+    u = np.zeros((len(level), dim + 2) + cases.block_shape(dim))
+    h = C.c_void_p()
+    rc = lib.alp_levels_create(dim, C.byref(sch), C.byref(mat), n0.ctypes.data_as(N._I), h0,
+                               len(level), level.ctypes.data_as(N._I),
+                               coord.ctypes.data_as(N._I), 0.6, 0.0, 1.0, 1,
+                               u.ctypes.data_as(N._D), C.byref(h))
+    return rc, lib.alp_last_error().decode()
+
+
+@pytest.mark.parametrize("what", ["overlap", "gap", "unbalanced", "level", "outside"])
+def test_invalid_trees_are_rejected(what):
+    if what == "overlap":  # a leaf and its parent
+        rc, msg = _create(1, (2,), [0, 0, 1, 1], [[0, 0, 0], [1, 0, 0], [0, 0, 0], [1, 0, 0]])
+    elif what == "gap":  # level-0 node 1 missing
+        rc, msg = _create(1, (2,), [0], [[0, 0, 0]])
+    elif what == "unbalanced":  # level-2 leaves next to a level-0 leaf
+        lv = [0, 1, 2, 2]
+        co = [[1, 0, 0], [0, 0, 0], [2, 0, 0], [3, 0, 0]]
+        rc, msg = _create(1, (2,), lv, co)
+        assert "more than one level" in msg
+    elif what == "level":
+        rc, msg = _create(1, (1,), [9], [[0, 0, 0]])
+    else:
+        rc, msg = _create(1, (2,), [0, 0], [[0, 0, 0], [2, 0, 0]])
+    assert rc == N.ALP_ERR_INVALID, (what, rc, msg)
+    assert msg

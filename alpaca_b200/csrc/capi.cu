@@ -43,33 +43,51 @@ namespace alp {
 
 int scheme_id(alp_scheme const *s, int *id, int *precision) {
   if (!s) return fail(ALP_ERR_INVALID, "scheme is null");
-  if (s->reconstruction_stencil != ALP_STENCIL_WENO5)
-    return fail(ALP_ERR_INVALID, "only ReconstructionStencils::WENO5 is compiled");
+  int const st = s->reconstruction_stencil;
+  if (st != ST_WENO5 && st != ST_WENO5Z && st != ST_TENO5 && st != ST_WENO3 && st != ST_FIRST_ORDER)
+    return fail(ALP_ERR_INVALID,
+                "compiled ReconstructionStencils: FirstOrder, WENO3, WENO5, WENO5Z, TENO5");
   if (s->time_integrator != ALP_RK3)
     return fail(ALP_ERR_INVALID, "only TimeIntegrators::RK3 is compiled");
   if (s->precision != ALP_FP64 && s->precision != ALP_FP32_FLUX)
     return fail(ALP_ERR_INVALID, "precision must be ALP_FP64 or ALP_FP32_FLUX");
   *precision = s->precision;
   if (s->convective_term_solver == ALP_FINITE_VOLUME) {
-    if (s->riemann_solver != ALP_RIEMANN_HLLC || s->signal_speed != ALP_SIGNAL_SPEED_EINFELDT)
-      return fail(ALP_ERR_INVALID, "FiniteVolume is compiled with Hllc + Einfeldt only");
-    if (s->state_reconstruction == ALP_RECON_CHARACTERISTIC) {
-      *id = FV_CHAR;
-      return ALP_OK;
-    }
-    if (s->state_reconstruction == ALP_RECON_PRIMITIVE) {
-      *id = FV_PRIM;
-      return ALP_OK;
-    }
-    return fail(ALP_ERR_INVALID, "FiniteVolume needs Primitive or Characteristic reconstruction");
-  }
-  if (s->convective_term_solver == ALP_FLUX_SPLITTING) {
-    if (s->flux_splitting != ALP_FLUX_SPLITTING_ROE)
-      return fail(ALP_ERR_INVALID, "FluxSplitting is compiled with FluxSplitting::Roe only");
+    if (s->riemann_solver < RS_HLLC || s->riemann_solver > RS_HLL)
+      return fail(ALP_ERR_INVALID, "RiemannSolvers must be Hllc, Hllc_LM or Hll");
+    if (s->signal_speed < SS_EINFELDT || s->signal_speed > SS_ARITHMETIC)
+      return fail(ALP_ERR_INVALID, "SignalSpeed must be Einfeldt, Davis, Toro or Arithmetic");
+    if (s->state_reconstruction == ALP_RECON_CHARACTERISTIC) *id = FV_CHAR;
+    else if (s->state_reconstruction == ALP_RECON_PRIMITIVE) *id = FV_PRIM;
+    else return fail(ALP_ERR_INVALID, "FiniteVolume needs Primitive or Characteristic reconstruction");
+  } else if (s->convective_term_solver == ALP_FLUX_SPLITTING) {
+    int const fs = s->flux_splitting;
+    if (fs == FSP_GLF)
+      return fail(ALP_ERR_INVALID,
+                  "FluxSplitting::GlobalLaxFriedrichs (a domain-wide eigenvalue reduction) is not compiled");
+    if (fs != FSP_ROE && fs != FSP_LLF && fs != FSP_ROE_M && fs != FSP_LLF_M)
+      return fail(ALP_ERR_INVALID,
+                  "FluxSplitting must be Roe, LocalLaxFriedrichs, Roe_M or LocalLaxFriedrichs_M");
     *id = FS_ROE;
-    return ALP_OK;
+  } else {
+    return fail(ALP_ERR_INVALID, "unknown convective_term_solver");
   }
-  return fail(ALP_ERR_INVALID, "unknown convective_term_solver");
+  if (*precision == ALP_FP32_FLUX && !scheme_options(s).is_default())
+    return fail(ALP_ERR_INVALID,
+                "ALP_FP32_FLUX is compiled for WENO5 + HLLC/Einfeldt and Roe splitting only");
+  return ALP_OK;
+}
+
+SchemeOptions scheme_options(alp_scheme const *s) {
+  SchemeOptions o;
+  o.stencil = s->reconstruction_stencil;
+  if (s->convective_term_solver == ALP_FINITE_VOLUME) {
+    o.riemann = s->riemann_solver;
+    o.signal = s->signal_speed;
+  } else {
+    o.splitting = s->flux_splitting;
+  }
+  return o;
 }
 
 int check_material(alp_material const *m) {
@@ -120,6 +138,7 @@ int alp_convective_fluxes(int dim, const alp_scheme *scheme, const alp_material 
     if (!F[d] && nb > 0) return fail(ALP_ERR_INVALID, "flux buffer is null");
   Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
            meta_of(mat, cell_size, 0), (cudaStream_t)stream};
+  L.opt = scheme_options(scheme);
   long long const stride = (long long)(dim + 2) * faces_of(dim);
   for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F[d], stride, true));
   return ALP_OK;
@@ -144,6 +163,7 @@ int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
   double *F = static_cast<double *>(d_workspace);
   Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
            meta_of(mat, cell_size, 0), (cudaStream_t)stream};
+  L.opt = scheme_options(scheme);
   long long const dstride = (long long)(dim + 2) * faces_of(dim);
   long long const stride = dstride * dim;
   for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F + d * dstride, stride, false));
@@ -338,6 +358,7 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   e->dim = dim;
   e->scheme = sid;
   e->precision = prec;
+  e->opt = scheme_options(scheme);
   e->capacity = capacity_blocks;
   e->max_cases = max_cases;
   e->ne = dim + 2;
@@ -540,7 +561,8 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
 #ifdef ALP_STRICT
   int const allowed = 2;  // the pencil path changes the flux summation order
 #else
-  int const allowed = ncand;
+  // the pencil kernels are compiled for the default schemes only
+  int const allowed = e->opt.is_default() ? ncand : 2;
 #endif
   int const saved_path = e->path, saved_threads = e->face_threads;
   float best = 0.f;
@@ -589,6 +611,8 @@ int alp_engine_set_path(alp_engine *e, int candidate) {
 #ifdef ALP_STRICT
   if (candidate == 2) return fail(ALP_ERR_INVALID, "the strict build steps the face-flux path");
 #endif
+  if (candidate == 2 && !e->opt.is_default())
+    return fail(ALP_ERR_INVALID, "pencil sweeps are compiled for WENO5 + HLLC/Einfeldt and Roe only");
   e->path = paths[candidate];
   e->face_threads = threads[candidate];
   e->graph_dirty = true;

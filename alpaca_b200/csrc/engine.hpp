@@ -39,6 +39,7 @@ using alp::launch_step_commit;
 // a case is exported.
 struct alp_engine {
   int dim = 3, scheme = FV_CHAR, precision = FP64;
+  alp::SchemeOptions opt;  // run-time selected schemes (face-flux path only)
   int capacity = 0, max_cases = 0;
   int ne = 5, cells = 0, faces = 0;
   double *U = nullptr, *UB = nullptr, *UC = nullptr;
@@ -76,6 +77,7 @@ struct alp_engine {
   // not committed, so the case state is left as it was (autotuning).
   int record_step(bool trial = false) {
     Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
+    L.opt = opt;
     ALP_CUDA(launch_signal_speed(L, cases, nullptr));
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
     double *in[3] = {U, UB, UC};
@@ -172,6 +174,9 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
 int engine_case_states(alp_engine *e, std::vector<CaseState> &out);
 // Compiled scheme id and precision of a selection (ALP_ERR_INVALID otherwise).
 int scheme_id(alp_scheme const *s, int *id, int *precision);
+// Stencil / Riemann / signal-speed / splitting choices of a validated selection
+// (the fields the selected convective term solver does not use are default).
+SchemeOptions scheme_options(alp_scheme const *s);
 // Rejects gamma <= 1 and negative background pressure.
 int check_material(alp_material const *m);
 // Block metadata of one material and cell size.

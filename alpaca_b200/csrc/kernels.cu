@@ -13,6 +13,7 @@
 // unreachable in those instantiations.
 #pragma nv_diag_suppress 128
 #include "numerics.cuh"
+#include "schemes_ext.cuh"
 
 namespace alp {
 
@@ -140,10 +141,12 @@ __device__ __forceinline__ void load_cell(double const *src, double (&dst)[DIM +
 // to fd and returns false for a face the reference skips (invalid
 // reconstructed state, finite_volume_scheme.cpp:218-225) or whose Roe average
 // has a non-positive density (eigendecomposition.h:244).
-template <int DIM, int DIR, int SCHEME, typename T>
+// P selects reconstruction stencil, Riemann solver and splitting eigenvalues
+// (DefaultPolicy: WENO5, HLLC/Einfeldt, Roe; ExtPolicy: run-time choice, FP64).
+template <int DIM, int DIR, int SCHEME, typename T, typename P = DefaultPolicy>
 __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
                                              double const (&cons)[6][DIM + 2],
-                                             double (&fd)[DIM + 2]) {
+                                             double (&fd)[DIM + 2], P const &pol = P()) {
   constexpr int NE = DIM + 2;
   T flux[NE];
   bool valid = true;
@@ -216,8 +219,8 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           }
           uc[m] = s;
         }
-        ch[0][n] = weno5_left(uc);
-        ch[1][n] = weno5_right(uc);
+        ch[0][n] = pol.left(uc);
+        ch[1][n] = pol.right(uc);
       }
       T cm[NE], cp[NE];
       to_physical<DIM, DIR, T>(r, ch[0], cm);
@@ -237,7 +240,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       if (!(pm > -B) || !(pp > -B)) valid = false;
       T const vl = cm[mP] * one_l;
       T const vr = cp[mP] * one_r;
-      hllc<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
+      pol.template riemann<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
     } else {
       // Roe flux-vector splitting (flux_splitting_scheme.cpp:42-76, 185-315)
       double advd[6][NE];
@@ -259,7 +262,8 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           advd[m][MOMX + d] = v;
         }
       }
-      T const ev_nl0 = fabs(r.up - r.c), ev_nl1 = fabs(r.up + r.c), ev_lin = fabs(r.up);
+      T ev_nl0, ev_lin, ev_nl1;
+      pol.template fs_eigenvalues<DIM, DIR, T>(eos, r, pt, pn, ev_nl0, ev_lin, ev_nl1);
       // FP32 form: increments against the face's left cell; the characteristic
       // flux of that cell, L f_i, is restored by R as f_i in double
       constexpr bool DELTA = sizeof(T) == 4;
@@ -288,7 +292,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           pos[m] = sp;
           neg[m] = sn;
         }
-        ch[0][n] = T(0.5) * (weno5_left(pos) + weno5_right(neg));
+        ch[0][n] = T(0.5) * (pol.left(pos) + pol.right(neg));
       }
       to_physical<DIM, DIR, T>(r, ch[0], flux);
       if constexpr (DELTA) {
@@ -345,8 +349,8 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
         T arr[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n]);
-        pm[n] = weno5_left(arr);
-        pp[n] = weno5_right(arr);
+        pm[n] = pol.left(arr);
+        pp[n] = pol.right(arr);
       }
       // PrimeStatesToConservatives (prime_state_handler.h:195-275)
       T cm[NE], cp[NE];
@@ -364,7 +368,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
       if (!(double(pm[PRES]) > -B) || !(double(pp[PRES]) > -B)) valid = false;
       // HLLC's own 1/density (hllc_riemann_solver.h:75-78)
-      hllc<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR],
+      pol.template riemann<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR],
                         inv(cm[MASS]), inv(cp[MASS]), flux);
     }
   }
@@ -375,11 +379,12 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
 }
 
 // Flux of the face with thread index t of direction DIR of the block in `slot`.
-template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER>
+template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER,
+          typename P = DefaultPolicy>
 __device__ __forceinline__ void face_flux(double const *__restrict__ U,
                                           int const *__restrict__ nbr26, int slot, int item,
                                           int t, BlockMeta const &bm, double *__restrict__ F,
-                                          long long stride) {
+                                          long long stride, P const &pol = P()) {
   using G = Geo<DIM>;
   using M = FaceMap<DIM, DIR>;
   constexpr int NE = G::NE;
@@ -399,7 +404,7 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
     load_cell<DIM, DIR>(stencil_cell<DIM, DIR, GATHER>(U, blk, HS + a - 3 + m, cell0, nlo, nhi),
                         cons[m]);
   double fd[NE];
-  bool const valid = face_compute<DIM, DIR, SCHEME, T>(eos, bm.B, cons, fd);
+  bool const valid = face_compute<DIM, DIR, SCHEME, T, P>(eos, bm.B, cons, fd, pol);
   write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
 }
 
@@ -443,6 +448,48 @@ face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
     if (t < FaceMap<DIM, 2>::COUNT)
       face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, T, false, true>(U, nbr26, slot, item, t, bm,
                                                                  F + 2 * dstride, stride);
+  }
+}
+
+// The same two kernels for the run-time selected schemes (ExtPolicy, FP64).
+template <int DIM, int DIR, int SCHEME, bool ACCUM>
+__global__ void __launch_bounds__(128)
+face_flux_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                     BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
+                     long long stride, ExtPolicy pol) {
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= FaceMap<DIM, DIR>::COUNT) return;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  face_flux<DIM, DIR, SCHEME, double, ACCUM, false, ExtPolicy>(U, nullptr, slot, item, t, bm, F,
+                                                               stride, pol);
+}
+
+template <int DIM, int SCHEME>
+__global__ void __launch_bounds__(128)
+face_flux_all_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                         BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
+                         CaseState const *__restrict__ cases, double *__restrict__ F,
+                         long long stride, long long dstride, ExtPolicy pol) {
+  int const t = blockIdx.y * blockDim.x + threadIdx.x;
+  int const item = blockIdx.x;
+  int const slot = work[item];
+  BlockMeta const bm = meta[slot];
+  if (!(cases[bm.case_id].dt > 0.0)) return;
+  int const dir = blockIdx.z;
+  if (dir == 0) {
+    if (t < FaceMap<DIM, 0>::COUNT)
+      face_flux<DIM, 0, SCHEME, double, false, true, ExtPolicy>(U, nbr26, slot, item, t, bm, F,
+                                                                stride, pol);
+  } else if (DIM > 1 && dir == 1) {
+    if (t < FaceMap<DIM, 1>::COUNT)
+      face_flux<DIM, (DIM > 1 ? 1 : 0), SCHEME, double, false, true, ExtPolicy>(
+          U, nbr26, slot, item, t, bm, F + dstride, stride, pol);
+  } else if (DIM > 2) {
+    if (t < FaceMap<DIM, 2>::COUNT)
+      face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, double, false, true, ExtPolicy>(
+          U, nbr26, slot, item, t, bm, F + 2 * dstride, stride, pol);
   }
 }
 
@@ -954,6 +1001,26 @@ template <int DIM, int DIR, typename T, bool ACC>
 cudaError_t face_flux_dir(Launch const &L, double *F, long long stride, int threads) {
   using M = FaceMap<DIM, DIR>;
   dim3 grid(L.nwork, (M::COUNT + threads - 1) / threads);
+  if (!L.opt.is_default()) {
+    ExtPolicy const pol{L.opt};
+    switch (L.scheme) {
+      case FV_CHAR:
+        face_flux_ext_kernel<DIM, DIR, FV_CHAR, ACC>
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+        break;
+      case FV_PRIM:
+        face_flux_ext_kernel<DIM, DIR, FV_PRIM, ACC>
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+        break;
+      case FS_ROE:
+        face_flux_ext_kernel<DIM, DIR, FS_ROE, ACC>
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+        break;
+      default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  }
   switch (L.scheme) {
     case FV_CHAR:
       face_flux_kernel<DIM, DIR, FV_CHAR, T, ACC>
@@ -1002,6 +1069,7 @@ cudaError_t launch_face_flux(Launch const &L, int dir, double *F, long long stri
   if (L.nwork <= 0) return cudaSuccess;
   int const threads = block_threads > 0 ? block_threads : 128;
   if (threads > 128 || (threads & 31)) return cudaErrorInvalidValue;
+  if (!L.opt.is_default() && L.precision != FP64) return cudaErrorInvalidValue;
   if (L.precision == FP32_FLUX)
     return accumulate ? face_flux_t<float, true>(L, dir, F, stride, threads)
                       : face_flux_t<float, false>(L, dir, F, stride, threads);
@@ -1044,6 +1112,23 @@ cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *
                             long long stride, long long dstride, int threads) {
   int const count = (IC + 1) * (DIM > 1 ? IC : 1) * (DIM > 2 ? IC : 1);
   dim3 grid(L.nwork, (count + threads - 1) / threads, DIM);
+  if (!L.opt.is_default()) {
+    ExtPolicy const pol{L.opt};
+    switch (L.scheme) {
+      case FV_CHAR:
+        face_flux_all_ext_kernel<DIM, FV_CHAR><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        break;
+      case FV_PRIM:
+        face_flux_all_ext_kernel<DIM, FV_PRIM><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        break;
+      case FS_ROE:
+        face_flux_all_ext_kernel<DIM, FS_ROE><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        break;
+      default:
+        return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+  }
   switch (L.scheme) {
     case FV_CHAR:
       face_flux_all_kernel<DIM, FV_CHAR, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
@@ -1104,6 +1189,7 @@ cudaError_t launch_pencil_stage(Launch const &L, double const *U0, double *Uout,
   if (L.nwork <= 0) return cudaSuccess;
   if (!L.work || !L.meta || !nbr26 || !cases || stage < 0 || stage > 2) return cudaErrorInvalidValue;
   if (L.dim > 1 && !R) return cudaErrorInvalidValue;
+  if (!L.opt.is_default()) return cudaErrorInvalidValue;  // pencils: default schemes only
   bool const f32 = L.precision == FP32_FLUX;
   switch (L.dim) {
     case 1: return f32 ? pencil_dim<1, float>(L, U0, Uout, R, nbr26, cases, stage)
@@ -1122,6 +1208,7 @@ cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState co
   if (!L.work || !L.meta || !nbr26 || !cases) return cudaErrorInvalidValue;
   if (threads <= 0) threads = 128;
   if (threads > 128 || (threads & 31)) return cudaErrorInvalidValue;
+  if (!L.opt.is_default() && L.precision != FP64) return cudaErrorInvalidValue;
   bool const f32 = L.precision == FP32_FLUX;
   switch (L.dim) {
     case 1: return f32 ? face_flux_all_t<1, float>(L, nbr26, cases, F, stride, dstride, threads)

@@ -16,6 +16,23 @@ namespace alp {
 enum Scheme { FV_CHAR = 0, FV_PRIM = 1, FS_ROE = 2 };
 enum Precision { FP64 = 0, FP32_FLUX = 1 };
 
+// Further selections of the reference's plugin surface, dispatched at run time
+// in FP64 (schemes_ext.cuh); the values are those of the reference's enums
+// (stencil_setup.h:26-43, riemann_solver_settings.h:47, enums/signal_speed.h:31,
+// enums/flux_splitting.h:31).
+enum StencilId { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11 };
+enum RiemannId { RS_HLLC = 0, RS_HLLC_LM = 1, RS_HLL = 2 };
+enum SignalSpeedId { SS_EINFELDT = 0, SS_DAVIS = 1, SS_TORO = 2, SS_ARITHMETIC = 3 };
+enum SplittingId { FSP_ROE = 0, FSP_LLF = 1, FSP_GLF = 2, FSP_ROE_M = 3, FSP_LLF_M = 4 };
+
+struct SchemeOptions {
+  int stencil = ST_WENO5, riemann = RS_HLLC, signal = SS_EINFELDT, splitting = FSP_ROE;
+  __host__ __device__ bool is_default() const {
+    return stencil == ST_WENO5 && riemann == RS_HLLC && signal == SS_EINFELDT &&
+           splitting == FSP_ROE;
+  }
+};
+
 // Work description shared by the launchers. A null `work` means the identity
 // worklist (item i is slot i); a null `meta` means every block uses `def`.
 struct Launch {
@@ -28,6 +45,7 @@ struct Launch {
   BlockMeta const *meta;   // [slots], or null
   BlockMeta def;
   cudaStream_t stream;
+  SchemeOptions opt = SchemeOptions();  // non-default: FP64 run-time dispatch, face kernels only
 };
 
 // Face fluxes of direction `dir` for every work item into

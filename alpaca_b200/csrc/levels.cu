@@ -207,6 +207,7 @@ struct NodeKey {
 
 struct alp_levels {
   int dim = 3, scheme = 0, precision = 0, lmax = 0, nlev = 1, nmicro = 1;
+  alp::SchemeOptions opt;
   int nleaf = 0, nghost = 0, nslots = 0, ne = 5, cells = 0, faces = 0;
   long long cell_updates_per_macro = 0;
   double *U = nullptr, *UB = nullptr, *UC = nullptr, *F = nullptr;
@@ -224,6 +225,7 @@ struct alp_levels {
 
   int record_macro() {
     Launch L{dim, scheme, precision, U, work, nleaf, meta, BlockMeta{}, stream};
+    L.opt = opt;
     double *in[3] = {U, UB, UC};
     double *out[3] = {UB, UC, U};
     for (int tm = 0; tm < nmicro; ++tm) {
@@ -431,6 +433,7 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   m->dim = dim;
   m->scheme = sid;
   m->precision = prec;
+  m->opt = scheme_options(scheme);
   m->lmax = lmax;
   m->nlev = lmax + 1;
   m->nmicro = 1 << lmax;

@@ -17,10 +17,29 @@ HEADER = os.path.join(os.path.dirname(HERE), "include", "alpaca_b200.h")
 ALP_OK, ALP_ERR_INVALID, ALP_ERR_CUDA, ALP_ERR_CAPACITY, ALP_ERR_NOT_FOUND, ALP_ERR_NUMERIC = range(6)
 FLUX_SPLITTING, FINITE_VOLUME = 0, 1
 RECON_CONSERVATIVE, RECON_PRIMITIVE, RECON_CHARACTERISTIC = 0, 1, 2
-STENCIL_WENO5 = 4
-RIEMANN_HLLC = 0
-SIGNAL_SPEED_EINFELDT = 0
-FLUX_SPLITTING_ROE = 0
+STENCIL_FIRST_ORDER, STENCIL_WENO3, STENCIL_WENO5, STENCIL_WENO5Z, STENCIL_TENO5 = 0, 1, 4, 7, 11
+RIEMANN_HLLC, RIEMANN_HLLC_LM, RIEMANN_HLL = 0, 1, 2
+SIGNAL_SPEED_EINFELDT, SIGNAL_SPEED_DAVIS, SIGNAL_SPEED_TORO, SIGNAL_SPEED_ARITHMETIC = 0, 1, 2, 3
+FLUX_SPLITTING_ROE, FLUX_SPLITTING_LLF, FLUX_SPLITTING_GLF = 0, 1, 2
+FLUX_SPLITTING_ROE_M, FLUX_SPLITTING_LLF_M = 3, 4
+
+# Further selections by name: base variant and the alp_scheme fields changed
+EXT_SCHEMES = {
+    "fvchar_weno5z": ("fvchar", {"reconstruction_stencil": STENCIL_WENO5Z}),
+    "fvchar_teno5": ("fvchar", {"reconstruction_stencil": STENCIL_TENO5}),
+    "fvchar_weno3": ("fvchar", {"reconstruction_stencil": STENCIL_WENO3}),
+    "fvchar_first": ("fvchar", {"reconstruction_stencil": STENCIL_FIRST_ORDER}),
+    "fvchar_hll": ("fvchar", {"riemann_solver": RIEMANN_HLL}),
+    "fvchar_hllclm": ("fvchar", {"riemann_solver": RIEMANN_HLLC_LM}),
+    "fvchar_davis": ("fvchar", {"signal_speed": SIGNAL_SPEED_DAVIS}),
+    "fvchar_toro": ("fvchar", {"signal_speed": SIGNAL_SPEED_TORO}),
+    "fvchar_arith": ("fvchar", {"signal_speed": SIGNAL_SPEED_ARITHMETIC}),
+    "fvprim_teno5": ("fvprim", {"reconstruction_stencil": STENCIL_TENO5}),
+    "fs_llf": ("fsroe", {"flux_splitting": FLUX_SPLITTING_LLF}),
+    "fs_roem": ("fsroe", {"flux_splitting": FLUX_SPLITTING_ROE_M}),
+    "fs_llfm": ("fsroe", {"flux_splitting": FLUX_SPLITTING_LLF_M}),
+    "fs_teno5": ("fsroe", {"reconstruction_stencil": STENCIL_TENO5}),
+}
 RK3 = 1
 FP64, FP32_FLUX = 0, 1
 HALO_ALL, HALO_FACES = 0, 1
@@ -41,6 +60,12 @@ class Scheme(C.Structure):
 
     @classmethod
     def make(cls, variant: str = "fvchar", precision: int = FP64) -> "Scheme":
+        if variant in EXT_SCHEMES:
+            base, fields = EXT_SCHEMES[variant]
+            s = cls.make(base, precision)
+            for k, v in fields.items():
+                setattr(s, k, v)
+            return s
         s = cls()
         s.convective_term_solver = FINITE_VOLUME
         s.state_reconstruction = RECON_CHARACTERISTIC

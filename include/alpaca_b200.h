@@ -42,22 +42,46 @@ enum {
  * user_specifications/ selects the same combination:
  *   convective_term_solver   riemann_solver_settings.h:28  (FluxSplitting=0, FiniteVolume=1)
  *   state_reconstruction     state_reconstruction_settings.h:25 (Conservative=0, Primitive=1, Characteristic=2)
- *   reconstruction_stencil   stencil_setup.h:26-43 (WENO5 = 4)
+ *   reconstruction_stencil   stencil_setup.h:26-43 (FirstOrder=0, WENO3=1, WENO5=4, WENO5Z=7, TENO5=11)
  *   riemann_solver           riemann_solver_settings.h:47 (Hllc=0, Hllc_LM=1, Hll=2)
- *   signal_speed             enums/signal_speed.h:31 (Einfeldt = 0)
- *   flux_splitting           enums/flux_splitting.h:31 (Roe = 0)
+ *   signal_speed             enums/signal_speed.h:31 (Einfeldt=0, Davis=1, Toro=2, Arithmetic=3)
+ *   flux_splitting           enums/flux_splitting.h:31 (Roe=0, LLF=1, GLF=2, Roe_M=3, LLF_M=4)
  *   time_integrator          numerical_setup.h:26 (RK2=0, RK3=1)
- * Supported: FiniteVolume + {Primitive, Characteristic} + WENO5 + Hllc +
- * Einfeldt, and FluxSplitting + Roe + WENO5; RK3.
+ * Supported: FiniteVolume + {Primitive, Characteristic} reconstruction with
+ * the stencils FirstOrder, WENO3, WENO5, WENO5Z or TENO5, the Riemann solvers
+ * Hllc, Hllc_LM or Hll and the signal speeds Einfeldt, Davis, Toro or
+ * Arithmetic; FluxSplitting with Roe, LocalLaxFriedrichs, Roe_M or
+ * LocalLaxFriedrichs_M and the same stencils; RK3. WENO5 + Hllc + Einfeldt
+ * and WENO5 + Roe are the compiled fast path (FP64 and FP32_FLUX, pencil
+ * sweeps); the other choices run through one FP64 face kernel that selects
+ * them at run time. GlobalLaxFriedrichs (a domain-wide eigenvalue reduction)
+ * is rejected.
  * precision: ALP_FP64 (all arithmetic in double) or ALP_FP32_FLUX
  * (reconstruction, smoothness indicators and Riemann fluxes in float; state,
  * RK accumulation, pressure recovery and dt in double). */
 enum { ALP_FLUX_SPLITTING = 0, ALP_FINITE_VOLUME = 1 };
 enum { ALP_RECON_CONSERVATIVE = 0, ALP_RECON_PRIMITIVE = 1, ALP_RECON_CHARACTERISTIC = 2 };
-enum { ALP_STENCIL_WENO5 = 4 };
-enum { ALP_RIEMANN_HLLC = 0 };
-enum { ALP_SIGNAL_SPEED_EINFELDT = 0 };
-enum { ALP_FLUX_SPLITTING_ROE = 0 };
+enum {
+  ALP_STENCIL_FIRST_ORDER = 0,
+  ALP_STENCIL_WENO3 = 1,
+  ALP_STENCIL_WENO5 = 4,
+  ALP_STENCIL_WENO5Z = 7,
+  ALP_STENCIL_TENO5 = 11
+};
+enum { ALP_RIEMANN_HLLC = 0, ALP_RIEMANN_HLLC_LM = 1, ALP_RIEMANN_HLL = 2 };
+enum {
+  ALP_SIGNAL_SPEED_EINFELDT = 0,
+  ALP_SIGNAL_SPEED_DAVIS = 1,
+  ALP_SIGNAL_SPEED_TORO = 2,
+  ALP_SIGNAL_SPEED_ARITHMETIC = 3
+};
+enum {
+  ALP_FLUX_SPLITTING_ROE = 0,
+  ALP_FLUX_SPLITTING_LLF = 1,
+  ALP_FLUX_SPLITTING_GLF = 2,
+  ALP_FLUX_SPLITTING_ROE_M = 3,
+  ALP_FLUX_SPLITTING_LLF_M = 4
+};
 enum { ALP_RK3 = 1 };
 enum { ALP_FP64 = 0, ALP_FP32_FLUX = 1 };
 

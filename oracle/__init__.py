@@ -38,6 +38,38 @@ VARIANTS = {
     "fsroe": (FLUX_SPLITTING, RECON_CHARACTERISTIC),
 }
 
+# Further selections: name -> (base variant, (stencil, riemann solver, signal
+# speed, flux splitting)) with the values of the reference's enums.
+WENO5, WENO5Z, TENO5, WENO3, FIRST_ORDER = 4, 7, 11, 1, 0
+HLLC, HLLC_LM, HLL = 0, 1, 2
+EINFELDT, DAVIS, TORO, ARITHMETIC = 0, 1, 2, 3
+ROE, LLF, ROE_M, LLF_M = 0, 1, 3, 4
+DEFAULT_OPTIONS = (WENO5, HLLC, EINFELDT, ROE)
+EXT_VARIANTS = {
+    "fvchar_weno5z": ("fvchar", (WENO5Z, HLLC, EINFELDT, ROE)),
+    "fvchar_teno5": ("fvchar", (TENO5, HLLC, EINFELDT, ROE)),
+    "fvchar_weno3": ("fvchar", (WENO3, HLLC, EINFELDT, ROE)),
+    "fvchar_first": ("fvchar", (FIRST_ORDER, HLLC, EINFELDT, ROE)),
+    "fvchar_hll": ("fvchar", (WENO5, HLL, EINFELDT, ROE)),
+    "fvchar_hllclm": ("fvchar", (WENO5, HLLC_LM, EINFELDT, ROE)),
+    "fvchar_davis": ("fvchar", (WENO5, HLLC, DAVIS, ROE)),
+    "fvchar_toro": ("fvchar", (WENO5, HLLC, TORO, ROE)),
+    "fvchar_arith": ("fvchar", (WENO5, HLLC, ARITHMETIC, ROE)),
+    "fvprim_teno5": ("fvprim", (TENO5, HLLC, EINFELDT, ROE)),
+    "fs_llf": ("fsroe", (WENO5, HLLC, EINFELDT, LLF)),
+    "fs_roem": ("fsroe", (WENO5, HLLC, EINFELDT, ROE_M)),
+    "fs_llfm": ("fsroe", (WENO5, HLLC, EINFELDT, LLF_M)),
+    "fs_teno5": ("fsroe", (TENO5, HLLC, EINFELDT, ROE)),
+}
+
+
+def variant_spec(variant: str):
+    """(solver, reconstruction, options) of a variant name."""
+    if variant in VARIANTS:
+        return VARIANTS[variant] + (DEFAULT_OPTIONS,)
+    base, opts = EXT_VARIANTS[variant]
+    return VARIANTS[base] + (opts,)
+
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
 
@@ -92,6 +124,7 @@ def _load(path: str):
     lib.oracle_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, C.c_double,
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                C.c_int, C.c_int, _D, _I, _D]
+    lib.oracle_set_options.argtypes = [C.c_int] * 4
     lib.oracle_levels_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, _I, _I,
                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _D, _I, _D]
@@ -114,7 +147,13 @@ class Restatement(_Common):
         self.dim = dim
         self.ne = dim + 2
         self.variant = variant
-        self.solver, self.recon = VARIANTS[variant]
+        self.solver, self.recon, self.options = variant_spec(variant)
+        # every entry point below reads the process-wide selection: set it first
+        self._select()
+
+    def _select(self):
+        if self.lib.oracle_set_options(*self.options):
+            raise ValueError(f"unknown options {self.options}")
 
     # -- scalar kernels --
     def weno5(self, v):
@@ -139,6 +178,7 @@ class Restatement(_Common):
 
     def space_rhs(self, u, gamma, B, safe, cell_size, nthreads=1):
         """Returns (fx, fy, fz, rhs) for blocks whose halos are filled."""
+        self._select()
         u = np.ascontiguousarray(u, dtype=np.float64)
         nb = u.shape[0]
         _, fshape = self._shapes(nb)
@@ -177,6 +217,7 @@ class Restatement(_Common):
     def run(self, u, nbr, gamma, B, safe, cell_size, cfl, t_end, max_steps=0, t0=0.0,
             nthreads=1):
         """Single-level time loop. Returns (u_final, t, steps, dt_log)."""
+        self._select()
         u = np.array(u, dtype=np.float64, order="C", copy=True)
         nbr = np.ascontiguousarray(nbr, dtype=np.int32)
         cap = max_steps if max_steps > 0 else 1000000
@@ -194,6 +235,7 @@ class Restatement(_Common):
                    t0=0.0, nthreads=1):
         """Multi-level time loop with local time stepping (leaves of a block
         tree). Returns (u_final, t, macro_steps, micro_dt_log)."""
+        self._select()
         u = np.array(u, dtype=np.float64, order="C", copy=True)
         level = np.ascontiguousarray(level, dtype=np.int32)
         coord = np.ascontiguousarray(coord, dtype=np.int32).reshape(-1, 3)
@@ -219,7 +261,7 @@ class OpCounting(Restatement):
 
     _lib = None
     _path = OPCOUNT_SO
-    FIELDS = ("add", "mul", "div", "sqrt", "cmp", "abs")
+    FIELDS = ("add", "mul", "div", "sqrt", "cmp", "abs", "pow", "sin")
 
     def __init__(self, dim: int, variant: str = "fvchar"):
         super().__init__(dim, variant)
@@ -230,7 +272,7 @@ class OpCounting(Restatement):
         self.lib.oracle_op_reset()
 
     def counts(self) -> dict:
-        out = (C.c_longlong * 6)()
+        out = (C.c_longlong * 8)()
         self.lib.oracle_op_counts(out)
         return dict(zip(self.FIELDS, (int(x) for x in out)))
 

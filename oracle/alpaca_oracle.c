@@ -206,6 +206,113 @@ static double weno5(const double *a, int offset, int sign) {
 static inline double weno5_left(const double *a) { return weno5(a, 0, 1); }
 static inline double weno5_right(const double *a) { return weno5(a, 1, -1); }
 
+/* ---- further selections of the plugin surface (enum values of the
+ * reference: stencil_setup.h:26-43, riemann_solver_settings.h:47,
+ * enums/signal_speed.h:31, enums/flux_splitting.h:31) -------------------- */
+enum { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11 };
+enum { RS_HLLC = 0, RS_HLLC_LM = 1, RS_HLL = 2 };
+enum { SS_EINFELDT = 0, SS_DAVIS = 1, SS_TORO = 2, SS_ARITHMETIC = 3 };
+enum { FSP_ROE = 0, FSP_LLF = 1, FSP_ROE_M = 3, FSP_LLF_M = 4 };
+static int g_stencil = ST_WENO5, g_riemann = RS_HLLC, g_signal = SS_EINFELDT,
+           g_splitting = FSP_ROE;
+
+/* WENO5-Z (weno5_z.h:88-150) */
+static double weno5z(const double *a, int offset, int sign) {
+  double const v1 = a[2 + offset - 2 * sign];
+  double const v2 = a[2 + offset - 1 * sign];
+  double const v3 = a[2 + offset];
+  double const v4 = a[2 + offset + 1 * sign];
+  double const v5 = a[2 + offset + 2 * sign];
+  double const c1 = 13.0 / 12.0, c2 = 0.25;
+  double const s11 = 1.0 * v1 + -2.0 * v2 + 1.0 * v3;
+  double const s12 = 1.0 * v1 + -4.0 * v2 + 3.0 * v3;
+  double const s1 = c1 * s11 * s11 + c2 * s12 * s12;
+  double const s21 = 1.0 * v2 + -2.0 * v3 + 1.0 * v4;
+  double const s22 = 1.0 * v2 + -1.0 * v4;
+  double const s2 = c1 * s21 * s21 + c2 * s22 * s22;
+  double const s31 = 1.0 * v3 + -2.0 * v4 + 1.0 * v5;
+  double const s32 = 3.0 * v3 + -4.0 * v4 + 1.0 * v5;
+  double const s3 = c1 * s31 * s31 + c2 * s32 * s32;
+  double const tau = fabs(s1 - s3);
+  double const a1 = 0.1 * (1.0 + tau / (s1 + DBL_EPSILON));
+  double const a2 = 0.6 * (1.0 + tau / (s2 + DBL_EPSILON));
+  double const a3 = 0.3 * (1.0 + tau / (s3 + DBL_EPSILON));
+  double const one_a_sum = 1.0 / (a1 + a2 + a3);
+  double const w1 = a1 * one_a_sum, w2 = a2 * one_a_sum, w3 = a3 * one_a_sum;
+  return w1 * (2.0 / 6.0 * v1 + -7.0 / 6.0 * v2 + 11.0 / 6.0 * v3) +
+         w2 * (-1.0 / 6.0 * v2 + 5.0 / 6.0 * v3 + 2.0 / 6.0 * v4) +
+         w3 * (2.0 / 6.0 * v3 + 5.0 / 6.0 * v4 + -1.0 / 6.0 * v5);
+}
+
+/* TENO5 (teno5.h:98-180), cut-off C_T = 1e-5 */
+static double teno5(const double *a, int offset, int sign) {
+  double const v1 = a[2 + offset - 2 * sign];
+  double const v2 = a[2 + offset - 1 * sign];
+  double const v3 = a[2 + offset];
+  double const v4 = a[2 + offset + 1 * sign];
+  double const v5 = a[2 + offset + 2 * sign];
+  double const c1 = 13.0 / 12.0, c2 = 0.25;
+  double const s11 = 1.0 * v2 + -2.0 * v3 + 1.0 * v4;
+  double const s12 = 1.0 * v2 + -1.0 * v4;
+  double const s1 = c1 * s11 * s11 + c2 * s12 * s12;
+  double const s21 = 1.0 * v3 + -2.0 * v4 + 1.0 * v5;
+  double const s22 = 3.0 * v3 + -4.0 * v4 + 1.0 * v5;
+  double const s2 = c1 * s21 * s21 + c2 * s22 * s22;
+  double const s31 = 1.0 * v1 + -2.0 * v2 + 1.0 * v3;
+  double const s32 = 1.0 * v1 + -4.0 * v2 + 3.0 * v3;
+  double const s3 = c1 * s31 * s31 + c2 * s32 * s32;
+  double const tau5 = fabs(s3 - s2);
+  double a1 = 1.0 + tau5 / (s1 + DBL_EPSILON);
+  double a2 = 1.0 + tau5 / (s2 + DBL_EPSILON);
+  double a3 = 1.0 + tau5 / (s3 + DBL_EPSILON);
+  a1 *= (a1 * a1);
+  a2 *= (a2 * a2);
+  a3 *= (a3 * a3);
+  a1 *= a1;
+  a2 *= a2;
+  a3 *= a3;
+  double const one_a_sum = 1.0 / (a1 + a2 + a3);
+  double const b1 = a1 * one_a_sum < 1.0e-5 ? 0.0 : 1.0;
+  double const b2 = a2 * one_a_sum < 1.0e-5 ? 0.0 : 1.0;
+  double const b3 = a3 * one_a_sum < 1.0e-5 ? 0.0 : 1.0;
+  double const var1 = -1.0 * v2 + 5.0 * v3 + 2.0 * v4;
+  double const var2 = 2.0 * v3 + 5.0 * v4 + -1.0 * v5;
+  double const var3 = 2.0 * v1 + -7.0 * v2 + 11.0 * v3;
+  double const w1 = 0.6 * b1, w2 = 0.3 * b2, w3 = 0.1 * b3;
+  double const one_w_sum = 1.0 / (w1 + w2 + w3);
+  return (w1 * one_w_sum * var1 + w2 * one_w_sum * var2 + w3 * one_w_sum * var3) * (1.0 / 6.0);
+}
+
+/* WENO3 (weno3.h:66-100): cells i-1..i+2 are a[1..4]; downstream size 1 */
+static double weno3(const double *a, int offset, int sign) {
+  double const v1 = a[2 + offset - 1 * sign];
+  double const v2 = a[2 + offset];
+  double const v3 = a[2 + offset + 1 * sign];
+  double const s11 = -1.0 * v1 + 1.0 * v2;
+  double const s1 = s11 * s11;
+  double const s21 = -1.0 * v2 + 1.0 * v3;
+  double const s2 = s21 * s21;
+  double const a1 = (1.0 / 3.0) / ((s1 + DBL_EPSILON) * (s1 + DBL_EPSILON));
+  double const a2 = (2.0 / 3.0) / ((s2 + DBL_EPSILON) * (s2 + DBL_EPSILON));
+  double const one_a_sum = 1.0 / (a1 + a2);
+  double const w1 = a1 * one_a_sum, w2 = a2 * one_a_sum;
+  return w1 * (-1.0 / 2.0 * v1 + 3.0 / 2.0 * v2) + w2 * (1.0 / 2.0 * v2 + 1.0 / 2.0 * v3);
+}
+
+/* SU::Reconstruction with the selected stencil (stencils/stencil_utilities.h),
+ * UpwindLeft {0, 1} / UpwindRight {1, -1}; FirstOrder returns cell i / i+1. */
+static double recon(const double *a, int offset, int sign) {
+  switch (g_stencil) {
+    case ST_WENO5Z: return weno5z(a, offset, sign);
+    case ST_TENO5: return teno5(a, offset, sign);
+    case ST_WENO3: return weno3(a, offset, sign);
+    case ST_FIRST_ORDER: return a[2 + offset];
+    default: return weno5(a, offset, sign);
+  }
+}
+static inline double recon_left(const double *a) { return recon(a, 0, 1); }
+static inline double recon_right(const double *a) { return recon(a, 1, -1); }
+
 /* ---- Roe eigensystem (solvers/eigendecomposition.h:181-467) ------------ */
 
 /* minor directions (eigendecomposition.h:84-125) */
@@ -361,10 +468,32 @@ static void roe_eigen(const Geom *g, const Eos *e, int dir, const double *u,
   R[ENERGY][ev_principal] = gru * H - c * c;
   R[ENERGY][ne - 1] = H + up * c;
 
-  /* Roe flux-splitting wave speeds (eigendecomposition.h:416-421, 64-72) */
-  out->ev[0] = fabs(up - c);
-  out->ev[ne - 1] = fabs(up + c);
-  for (int l = 1; l < ne - 1; ++l) out->ev[l] = fabs(up);
+  /* flux-splitting wave speeds (eigendecomposition.h:416-454, 64-72): Roe,
+   * Roe-M, local Lax-Friedrichs, LLF-M; low-Mach limit factor 5 */
+  double e0, elin, e1;
+  if (g_splitting == FSP_ROE_M) {
+    double const cm = dmin(c, 5.0 * fabs(up));
+    e0 = fabs(up - cm);
+    elin = fabs(up);
+    e1 = fabs(up + cm);
+  } else if (g_splitting == FSP_LLF || g_splitting == FSP_LLF_M) {
+    double ct = eos_speed_of_sound(e, rho_t, p_t);
+    double cn = eos_speed_of_sound(e, rho_n, p_n);
+    if (g_splitting == FSP_LLF_M) {
+      ct = dmin(5.0 * fabs(up_t), ct);
+      cn = dmin(5.0 * fabs(up_n), cn);
+    }
+    e0 = dmax(fabs(up_t - ct), fabs(up_n - cn));
+    elin = dmax(fabs(up_t), fabs(up_n));
+    e1 = dmax(fabs(up_t + ct), fabs(up_n + cn));
+  } else {
+    e0 = fabs(up - c);
+    elin = fabs(up);
+    e1 = fabs(up + c);
+  }
+  out->ev[0] = e0;
+  out->ev[ne - 1] = e1;
+  for (int l = 1; l < ne - 1; ++l) out->ev[l] = elin;
 }
 
 /* TransformToPhysicalSpace (eigendecomposition.h:144-165) */
@@ -377,7 +506,7 @@ static void to_physical(int ne, const double *ch, double R[MAXNE][MAXNE],
   }
 }
 
-/* ---- HLLC with Einfeldt signal speeds ---------------------------------- */
+/* ---- HLL-type Riemann solvers and their signal speeds ------------------ */
 
 /* CalculateSignalSpeed, Einfeldt branch (hll_signal_speed_calculator.h:77-101) */
 static void einfeldt(double rl, double rr, double ul, double ur, double cl,
@@ -393,10 +522,38 @@ static void einfeldt(double rl, double rr, double ul, double ur, double cl,
   *sr = dmax(u_roe + c_e, ur + cr);
 }
 
+/* CalculateSignalSpeed, the other branches (hll_signal_speed_calculator.h:40-140) */
+static void signal_speeds(double rl, double rr, double ul, double ur, double pl,
+                          double pr, double cl, double cr, double gamma, double *sl,
+                          double *sr) {
+  if (g_signal == SS_ARITHMETIC) {
+    double const cf = 0.5 * (cl + cr);
+    double const uf = 0.5 * (ul + ur);
+    *sl = dmin(uf - cf, ul - cl);
+    *sr = dmax(uf + cf, ur + cr);
+  } else if (g_signal == SS_DAVIS) {
+    *sl = dmin(ul - cl, ur - cr);
+    *sr = dmax(ul + cl, ur + cr);
+  } else if (g_signal == SS_TORO) {
+    double const z = (gamma - 1.0) / (2.0 * gamma);
+    double const p_star =
+        pow(((cl + cr) - 0.5 * (ur - ul) * (gamma - 1.0)) / (cl / pow(pl, z) + cr / pow(pr, z)),
+            (1.0 / z));
+    double ql = 1.0, qr = 1.0;
+    if (p_star > pl) ql = sqrt(1.0 + (gamma + 1.0) / (2.0 * gamma) * (p_star / pl - 1.0));
+    if (p_star > pr) qr = sqrt(1.0 + (gamma + 1.0) / (2.0 * gamma) * (p_star / pr - 1.0));
+    *sl = ul - cl * ql;
+    *sr = ur + cr * qr;
+  } else {
+    einfeldt(rl, rr, ul, ur, cl, cr, sl, sr);
+  }
+}
+
 static inline int signum(double x) { return (0.0 < x) - (x < 0.0); }
 
 /* HllcRiemannSolver::SolveRiemannProblemImplementation
- * (riemann_solvers/hllc_riemann_solver.h:52-198) */
+ * (riemann_solvers/hllc_riemann_solver.h:52-198), or with the selection
+ * g_riemann the HLL or HLLC-LM solver; signal speeds per g_signal. */
 static void hllc(const Eos *e, int dir, const double *cl, const double *cr,
                  const double *pl, const double *pr, double *flux) {
   int const dim = e->dim, ne = dim + 2;
@@ -409,12 +566,31 @@ static void hllc(const Eos *e, int dir, const double *cl, const double *cr,
   double const c_l = eos_speed_of_sound(e, cl[MASS], pres_l);
   double const c_r = eos_speed_of_sound(e, cr[MASS], pres_r);
   double sls, srs;
-  einfeldt(cl[MASS], cr[MASS], vel_l, vel_r, c_l, c_r, &sls, &srs);
+  signal_speeds(cl[MASS], cr[MASS], vel_l, vel_r, pres_l, pres_r, c_l, c_r, e->gamma, &sls, &srs);
+  fl[MASS] = cl[mP];
+  fl[mP] = ((cl[mP] * cl[mP]) * one_rl) + pres_l;
+  fl[ENERGY] = vel_l * (cl[ENERGY] + pres_l);
+  fr[MASS] = cr[mP];
+  fr[mP] = ((cr[mP] * cr[mP]) * one_rr) + pres_r;
+  fr[ENERGY] = vel_r * (cr[ENERGY] + pres_r);
+  for (int d = 0; d < dim - 1; ++d) {
+    int const mm = MOMX + minor_dir(dir, d);
+    fl[mm] = vel_l * cl[mm];
+    fr[mm] = vel_r * cr[mm];
+  }
+  if (g_riemann == RS_HLL) {
+    /* HllRiemannSolver (hll_riemann_solver.h:96-150) */
+    double const sl = dmin(sls, 0.0), sr = dmax(srs, 0.0);
+    for (int n = 0; n < ne; ++n)
+      flux[n] = (((sr * fl[n]) - (sl * fr[n])) + ((sr * sl) * (cr[n] - cl[n]))) / (sr - sl);
+    return;
+  }
+  int const lm = g_riemann == RS_HLLC_LM; /* HllcLMRiemannSolver: unclamped speeds */
   double const s_star =
       ((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r))) /
       (cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
-  double const sl = dmin(sls, 0.0);
-  double const sr = dmax(srs, 0.0);
+  double const sl = lm ? sls : dmin(sls, 0.0);
+  double const sr = lm ? srs : dmax(srs, 0.0);
   double const chi_l = (sls - vel_l) / (sls - s_star);
   double const chi_r = (srs - vel_r) / (srs - s_star);
 
@@ -429,19 +605,26 @@ static void hllc(const Eos *e, int dir, const double *cl, const double *cr,
                 (cr[ENERGY] * one_rr +
                  (s_star - vel_r) * (s_star + pres_r / (cr[MASS] * (sr - vel_r))));
 
-  fl[MASS] = cl[mP];
-  fl[mP] = ((cl[mP] * cl[mP]) * one_rl) + pres_l;
-  fl[ENERGY] = vel_l * (cl[ENERGY] + pres_l);
-  fr[MASS] = cr[mP];
-  fr[mP] = ((cr[mP] * cr[mP]) * one_rr) + pres_r;
-  fr[ENERGY] = vel_r * (cr[ENERGY] + pres_r);
-
   for (int d = 0; d < dim - 1; ++d) {
     int const mm = MOMX + minor_dir(dir, d);
     qsl[mm] = chi_l * cl[mm];
     qsr[mm] = chi_r * cr[mm];
-    fl[mm] = vel_l * cl[mm];
-    fr[mm] = vel_r * cr[mm];
+  }
+  if (lm) {
+    /* low-Mach activation (hllc_lm_riemann_solver.h:180-198), Ma limit 0.1 */
+    double const ma = dmin(0.1, dmax(fabs(vel_l / c_l), fabs(vel_r / c_r)));
+    double const act = sin((ma / 0.1) * 1.57079632679489661923);
+    for (int n = 0; n < ne; ++n) {
+      if (sl >= 0.0)
+        flux[n] = fl[n];
+      else if (sr <= 0.0)
+        flux[n] = fr[n];
+      else
+        flux[n] = 0.5 * ((fl[n] + fr[n]) - (((act * sr) * (cr[n] - qsr[n]) +
+                                             (act * sl) * (cl[n] - qsl[n])) +
+                                            fabs(s_star) * (qsr[n] - qsl[n])));
+    }
+    return;
   }
   int const sg = signum(s_star);
   for (int n = 0; n < ne; ++n) {
@@ -533,8 +716,8 @@ static void fv_fluxes(const Geom *g, const Eos *e, int recon, int dir,
                 uc[m] += eig[fi].L[n][l] * u[l * C + cells6[m]];
               }
             }
-            chm[n] = weno5_left(uc);
-            chp[n] = weno5_right(uc);
+            chm[n] = recon_left(uc);
+            chp[n] = recon_right(uc);
           }
           to_physical(ne, chm, eig[fi].R, cm);
           to_physical(ne, chp, eig[fi].R, cp);
@@ -545,8 +728,8 @@ static void fv_fluxes(const Geom *g, const Eos *e, int recon, int dir,
           double arr[6];
           for (int n = 0; n < np; ++n) {
             for (int m = 0; m < 6; ++m) arr[m] = p[n * C + cells6[m]];
-            pm[n] = weno5_left(arr);
-            pp[n] = weno5_right(arr);
+            pm[n] = recon_left(arr);
+            pp[n] = recon_right(arr);
           }
           prim_to_cons(e, pm, cm);
           prim_to_cons(e, pp, cp);
@@ -606,7 +789,7 @@ static void fs_fluxes(const Geom *g, int dir, const double *u, const double *adv
               neg[m] += (act - alpha * uct);
             }
           }
-          chf[n] = 0.5 * (weno5_left(pos) + weno5_right(neg));
+          chf[n] = 0.5 * (recon_left(pos) + recon_right(neg));
         }
         to_physical(ne, chf, eig[fi].R, phys);
         for (int l = 0; l < ne; ++l) flux[l * g->faces + fi] += phys[l];
@@ -1337,5 +1520,23 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
   tree_free(&tr);
   *t_io = t;
   *macro_done = macro;
+  return 0;
+}
+
+/* Selects stencil, Riemann solver, signal speed and flux splitting (values of
+ * the reference's enums); 1 for an unknown value. */
+int oracle_set_options(int stencil, int riemann, int signal, int splitting) {
+  if (stencil != ST_WENO5 && stencil != ST_WENO5Z && stencil != ST_TENO5 &&
+      stencil != ST_WENO3 && stencil != ST_FIRST_ORDER)
+    return 1;
+  if (riemann < RS_HLLC || riemann > RS_HLL) return 1;
+  if (signal < SS_EINFELDT || signal > SS_ARITHMETIC) return 1;
+  if (splitting != FSP_ROE && splitting != FSP_LLF && splitting != FSP_ROE_M &&
+      splitting != FSP_LLF_M)
+    return 1;
+  g_stencil = stencil;
+  g_riemann = riemann;
+  g_signal = signal;
+  g_splitting = splitting;
   return 0;
 }

@@ -29,6 +29,13 @@ enum { ORACLE_RECON_CONSERVATIVE = 0, ORACLE_RECON_PRIMITIVE = 1,
 
 int oracle_weno5(const double *v6, double *left, double *right);
 
+/* Selects the reconstruction stencil, Riemann solver, signal speed and flux
+ * splitting for the calls that follow (values of the reference's enums,
+ * stencil_setup.h:26-43, riemann_solver_settings.h:47, enums/signal_speed.h:31,
+ * enums/flux_splitting.h:31). Default: WENO5, Hllc, Einfeldt, Roe. Process-wide
+ * setting: not to be changed while another thread runs a call. */
+int oracle_set_options(int stencil, int riemann, int signal, int splitting);
+
 /* cons = (mass, energy, mx, my, mz), prim = (rho, p, u, v, w);
  * out = pressure, enthalpy, energy, speed of sound, psi, gruneisen.
  * dim selects the dimension-aware sums as a DIMENSION=dim build does. */

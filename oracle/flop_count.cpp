@@ -20,7 +20,7 @@
 #include <cmath>
 
 namespace opcount {
-long long add, mul, div, sqrt_, cmp, abs_;
+long long add, mul, div, sqrt_, cmp, abs_, pow_, sin_;
 }
 
 struct cdouble {
@@ -50,6 +50,8 @@ inline bool operator==(cdouble a, cdouble b) { ++opcount::cmp; return a.v == b.v
 inline bool operator!=(cdouble a, cdouble b) { ++opcount::cmp; return a.v != b.v; }
 inline cdouble sqrt(cdouble a) { ++opcount::sqrt_; return std::sqrt(a.v); }
 inline cdouble fabs(cdouble a) { ++opcount::abs_; return std::fabs(a.v); }
+inline cdouble pow(cdouble a, cdouble b) { ++opcount::pow_; return std::pow(a.v, b.v); }
+inline cdouble sin(cdouble a) { ++opcount::sin_; return std::sin(a.v); }
 
 #define double cdouble
 #include "alpaca_oracle.c"
@@ -57,8 +59,8 @@ inline cdouble fabs(cdouble a) { ++opcount::abs_; return std::fabs(a.v); }
 
 extern "C" {
 
-/* out[0..5] = additions/subtractions, multiplications, divisions, square
- * roots, comparisons, absolute values since the last reset. */
+/* out[0..7] = additions/subtractions, multiplications, divisions, square
+ * roots, comparisons, absolute values, powers, sines since the last reset. */
 void oracle_op_counts(long long *out) {
   out[0] = opcount::add;
   out[1] = opcount::mul;
@@ -66,9 +68,12 @@ void oracle_op_counts(long long *out) {
   out[3] = opcount::sqrt_;
   out[4] = opcount::cmp;
   out[5] = opcount::abs_;
+  out[6] = opcount::pow_;
+  out[7] = opcount::sin_;
 }
 
 void oracle_op_reset(void) {
   opcount::add = opcount::mul = opcount::div = opcount::sqrt_ = opcount::cmp = opcount::abs_ = 0;
+  opcount::pow_ = opcount::sin_ = 0;
 }
 }

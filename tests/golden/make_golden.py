@@ -8,6 +8,7 @@ tell that the generator still reproduces it bit for bit.
 
     python tests/golden/make_golden.py            # small fixtures
     python tests/golden/make_golden.py --c2       # also the 128^3, 100-step run summary
+    python tests/golden/make_golden.py --ext      # the further selections (make -C oracle ref-ext)
 """
 from __future__ import annotations
 
@@ -74,6 +75,28 @@ def short_run_fixtures(nsteps: int = 5):
             print("wrote", path)
 
 
+def ext_fixtures():
+    """1D and 3D right-hand sides and the 1D Sod run of every further selection
+    (stencils, Riemann solvers, signal speeds, flux splittings)."""
+    for variant in oracle.EXT_VARIANTS:
+        for dim in (1, 3):
+            case = small_cases()[dim]
+            u = filled(case)
+            I = cases.interior(dim)
+            rhs = oracle.Reference(dim, variant).space_rhs(u, case.gamma, case.B, False,
+                                                           case.grid.cell_size)[3]
+            path = os.path.join(HERE, "ext", f"rhs_d{dim}_{variant}.npz")
+            np.savez_compressed(path, input_sha=sha(u), rhs=rhs[I])
+        case = cases.sod_1d()
+        u, t, steps, dts = oracle.Reference(1, variant).run(
+            case.u, case.grid.nbr, case.gamma, case.B, False, case.grid.cell_size, case.cfl,
+            case.t_end)
+        path = os.path.join(HERE, "ext", f"sod1d_{variant}.npz")
+        np.savez_compressed(path, input_sha=sha(case.u), final=u[cases.interior(1)], t=t,
+                            steps=steps, dts=dts)
+        print("wrote", variant, steps, t)
+
+
 def c2_summary(variant: str, steps: int = 100):
     """The 3D periodic 128^3 Fourier + Mach-2 shock case after `steps` RK3 steps:
     per-block per-field interior sums and every 8th cell, from the reference."""
@@ -95,6 +118,10 @@ def c2_summary(variant: str, steps: int = 100):
 if __name__ == "__main__":
     if not oracle.Reference.available():
         sys.exit("oracle/_ref is not built: run `make -C oracle ref` with the reference sources")
+    if "--ext" in sys.argv:
+        os.makedirs(os.path.join(HERE, "ext"), exist_ok=True)
+        ext_fixtures()
+        sys.exit(0)
     rhs_fixtures()
     sod_fixtures()
     short_run_fixtures()

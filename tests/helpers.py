@@ -22,6 +22,17 @@ def field_rel_err(a: np.ndarray, b: np.ndarray, field_axis: int = 1) -> np.ndarr
     return np.abs(a - b).max(axis=1) / scale
 
 
+def field_rel_err_floored(a: np.ndarray, b: np.ndarray, field_axis: int = 1) -> np.ndarray:
+    """field_rel_err, except that a field whose reference is identically zero
+    (e.g. the mass right-hand side of a scheme without dissipation on a fluid
+    at rest) is measured against the largest field's scale."""
+    a2 = np.moveaxis(a, field_axis, 0).reshape(a.shape[field_axis], -1)
+    b2 = np.moveaxis(b, field_axis, 0).reshape(b.shape[field_axis], -1)
+    scale = np.abs(b2).max(axis=1)
+    scale = np.where(scale > 0.0, scale, max(scale.max(), 1e-300))
+    return np.abs(a2 - b2).max(axis=1) / scale
+
+
 def l1_rel(a: np.ndarray, b: np.ndarray) -> float:
     return float(np.abs(a - b).sum() / max(np.abs(b).sum(), 1e-300))
 

@@ -34,7 +34,7 @@ def test_invalid_arguments_are_rejected_without_gpu():
     rc = lib.alp_convective_fluxes(4, C.byref(sch), C.byref(mat), null, 1, 0.1, null, null, null, null)
     assert rc == N.ALP_ERR_INVALID and b"dim" in lib.alp_last_error()
     bad = N.Scheme.make("fvchar")
-    bad.reconstruction_stencil = 0  # FirstOrder is not compiled
+    bad.reconstruction_stencil = 14  # WENO9 is not compiled
     rc = lib.alp_convective_fluxes(3, C.byref(bad), C.byref(mat), null, 1, 0.1, null, null, null, null)
     assert rc == N.ALP_ERR_INVALID and b"WENO5" in lib.alp_last_error()
     cons = N.Scheme.make("fvchar")
@@ -101,3 +101,27 @@ def test_request_stream_is_seeded_and_in_range():
     assert all(a[i].arrival_s < a[i + 1].arrival_s for i in range(39))
     water = [r for r in a if r.kind == "blast3d_water"]
     assert water and abs(water[0].B - 3430.0) < 1e-9 and water[0].gamma == 6.12
+
+
+def test_extension_selections_validated_on_the_host():
+    """Unknown values, GlobalLaxFriedrichs and FP32 with a further selection are
+    rejected before any device work; the further selections themselves pass
+    validation (the call then only fails on the null buffers)."""
+    lib = N.lib()
+    mat = N.Material.make(1.4)
+    ws = C.c_void_p(0)
+
+    def rhs(sch):
+        return lib.alp_space_rhs(3, C.byref(sch), C.byref(mat), None, 1, 0.1, None, ws, 0, None)
+
+    s = N.Scheme.make("fvchar")
+    s.reconstruction_stencil = 5  # WENO5AER: not compiled
+    assert rhs(s) == N.ALP_ERR_INVALID and b"WENO5Z" in lib.alp_last_error()
+    s = N.Scheme.make("fsroe")
+    s.flux_splitting = N.FLUX_SPLITTING_GLF
+    assert rhs(s) == N.ALP_ERR_INVALID and b"GlobalLaxFriedrichs" in lib.alp_last_error()
+    s = N.Scheme.make("fvchar_teno5", N.FP32_FLUX)
+    assert rhs(s) == N.ALP_ERR_INVALID and b"FP32_FLUX" in lib.alp_last_error()
+    for name in N.EXT_SCHEMES:
+        assert rhs(N.Scheme.make(name)) == N.ALP_ERR_INVALID
+        assert b"null buffer" in lib.alp_last_error(), name

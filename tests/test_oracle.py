@@ -237,3 +237,50 @@ def test_op_counts_match_bench_constants():
         c = O.counts()
         flops = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / 4096
         assert abs(flops - expected) <= 0.01 * expected, (variant, flops)
+
+
+# ---- 5. further selections: stencils, Riemann solvers, signal speeds, splittings
+
+EXT = list(oracle.EXT_VARIANTS)
+
+
+@pytest.mark.parametrize("dim", [1, 3])
+@pytest.mark.parametrize("variant", EXT)
+def test_ext_restatement_matches_reference_rhs(dim, variant):
+    if not oracle.Reference.available(dim, variant):
+        pytest.skip("oracle/_ref further selections not built (make -C oracle ref-ext)")
+    case = small_cases()[dim]
+    u = filled(case)
+    a = oracle.Restatement(dim, variant).space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)
+    b = oracle.Reference(dim, variant).space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)
+    for x, y in zip(a, b):
+        assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("variant", EXT)
+def test_ext_restatement_matches_golden(variant):
+    """RHS in 1D and 3D and the 1D Sod run to t = 0.2, from the reference."""
+    for dim in (1, 3):
+        z = np.load(os.path.join(GOLDEN, "ext", f"rhs_d{dim}_{variant}.npz"))
+        case = small_cases()[dim]
+        u = filled(case)
+        assert _sha(u) == str(z["input_sha"])
+        rhs = oracle.Restatement(dim, variant).space_rhs(u, case.gamma, 0.0, False,
+                                                         case.grid.cell_size)[3]
+        assert np.array_equal(rhs[cases.interior(dim)], z["rhs"])
+    z = np.load(os.path.join(GOLDEN, "ext", f"sod1d_{variant}.npz"))
+    case = cases.sod_1d()
+    u, t, steps, dts = oracle.Restatement(1, variant).run(case.u, case.grid.nbr, 1.4, 0.0, False,
+                                                          case.grid.cell_size, 0.6, 0.2)
+    assert steps == int(z["steps"]) and t == float(z["t"]) and np.array_equal(dts, z["dts"])
+    assert np.array_equal(u[cases.interior(1)], z["final"])
+
+
+@pytest.mark.parametrize("variant", EXT)
+def test_ext_selection_changes_the_scheme(variant):
+    base = oracle.EXT_VARIANTS[variant][0]
+    case = small_cases()[3]
+    u = filled(case)
+    a = oracle.Restatement(3, variant).space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)[3]
+    b = oracle.Restatement(3, base).space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)[3]
+    assert not np.array_equal(a, b)

@@ -267,7 +267,8 @@ class LevelEngine:
 
 def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: int = N.FP64,
           share_3d: float = 0.9, max_cases: int = 256, steps_per_poll: int = 8,
-          one_at_a_time: bool = False, keep_results: bool = False):
+          one_at_a_time: bool = False, keep_results: bool = False, shortest_first: bool = False,
+          step_set_cells: float = float(1 << 21)):
     """Runs the C++ request loop (alp_serve) over a list of serving.Request
     specs. Returns (results as dicts, makespan seconds, final states or None)."""
     n = len(requests)
@@ -304,6 +305,8 @@ def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: i
     cfg.max_cases = max_cases
     cfg.steps_per_poll = steps_per_poll
     cfg.one_at_a_time = int(one_at_a_time)
+    cfg.shortest_first = int(shortest_first)
+    cfg.step_set_cells = step_set_cells
     mk = C.c_double()
     rc = N.lib().alp_serve(C.byref(cfg), reqs, n, res, C.byref(mk))
     if rc not in (N.ALP_OK, N.ALP_ERR_CAPACITY):

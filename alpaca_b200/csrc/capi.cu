@@ -330,6 +330,14 @@ int engine_case_states(alp_engine *e, std::vector<CaseState> &out) {
   return ALP_OK;
 }
 
+int engine_set_hold(alp_engine *e, int case_id, int hold) {
+  // the staging record keeps the source alive until the copy has run
+  e->h_case_state[case_id].hold = hold;
+  ALP_CUDA(cudaMemcpyAsync(&e->cases[case_id].hold, &e->h_case_state[case_id].hold, sizeof(int),
+                           cudaMemcpyHostToDevice, e->stream));
+  return ALP_OK;
+}
+
 }  // namespace alp
 
 extern "C" {

@@ -172,6 +172,8 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
                          int *case_id, int *first);
 // Copies the device case table to host.
 int engine_case_states(alp_engine *e, std::vector<CaseState> &out);
+// Holds (1) or releases (0) a case: a held case takes no steps (dt 0).
+int engine_set_hold(alp_engine *e, int case_id, int hold);
 // Compiled scheme id and precision of a selection (ALP_ERR_INVALID otherwise).
 int scheme_id(alp_scheme const *s, int *id, int *precision);
 // Stencil / Riemann / signal-speed / splitting choices of a validated selection

@@ -924,7 +924,7 @@ __global__ void dt_finalize_kernel(CaseState *cases, int n) {
   if (s.t + local > s.t_end) local = dmax(s.t_end - s.t, 0.0);
   if (!(s.t < s.t_end)) local = 0.0;
   if (s.max_steps > 0 && s.steps >= s.max_steps) local = 0.0;
-  if (s.status) local = 0.0;
+  if (s.status || s.hold) local = 0.0;
   s.dt = local;
 }
 

@@ -73,7 +73,7 @@ struct CaseState {
   int steps;       // steps taken
   int max_steps;   // <= 0: unbounded
   int status;      // bit 0: non-finite or non-positive state seen (case stopped)
-  int pad;
+  int hold;        // 1: the case takes no steps until released (request scheduling)
 };
 
 }  // namespace alp

@@ -8,7 +8,11 @@
 // cases, each case with its own dt), and leave the pool when their end time or
 // step budget is reached. The 2D and 3D engines step on their own streams, so
 // their work overlaps on the device. Device memory is sized once from the HBM
-// budget; nothing is allocated while serving.
+// budget; nothing is allocated while serving. With shortest_first, only the
+// resident cases with the least remaining work (cells x steps left) step, up to
+// step_set_cells cells together, and the others are held (they keep their
+// state and take no steps): the GPU stays busy while short cases finish first.
+// Holding changes no arithmetic, so every case gets the same bits either way.
 #include <algorithm>
 #include <chrono>
 #include <deque>
@@ -29,6 +33,8 @@ struct Active {
 struct DimPool {
   alp_engine *eng = nullptr;
   std::vector<int> req_of_case;  // case id -> request index (-1 free)
+  std::vector<int> held;         // case id -> hold flag on the device
+  std::vector<CaseState> states; // last case records read back
   int active = 0;
 };
 
@@ -42,6 +48,8 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     return fail(ALP_ERR_INVALID, "steps_per_poll and max_cases must be positive");
   if (!(cfg->share_3d >= 0.0 && cfg->share_3d <= 1.0))
     return fail(ALP_ERR_INVALID, "share_3d must lie in [0, 1]");
+  if (cfg->shortest_first && !(cfg->step_set_cells > 0.0))
+    return fail(ALP_ERR_INVALID, "step_set_cells must be positive");
   bool need[4] = {false, false, false, false};
   for (int i = 0; i < n; ++i) {
     if (reqs[i].dim < 1 || reqs[i].dim > 3) return fail(ALP_ERR_INVALID, "request dim");
@@ -69,7 +77,10 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
       return rc;
     }
     pool[d].req_of_case.assign(cfg->max_cases, -1);
+    pool[d].held.assign(cfg->max_cases, 0);
+    pool[d].states.assign(cfg->max_cases, CaseState{});
   }
+
 
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
@@ -79,7 +90,6 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
   int next = 0, done = 0;
   Clock::time_point const t0 = Clock::now();
   auto elapsed = [&]() { return std::chrono::duration<double>(Clock::now() - t0).count(); };
-  std::vector<CaseState> states;
   int rc_all = ALP_OK;
 
   while (done < n) {
@@ -99,6 +109,8 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
                                             r.ic_params, r.n_params, &cid);
       if (rc == ALP_OK) {
         p.req_of_case[cid] = *it;
+        p.held[cid] = 0;
+        p.states[cid] = CaseState{};
         ++p.active;
         ++total_active;
         results[*it].arrival_s = r.arrival_s;
@@ -128,6 +140,45 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
       continue;
     }
 
+    // shortest remaining work first: release the shortest cases up to the
+    // step-set size, hold the rest
+    if (cfg->shortest_first && !cfg->one_at_a_time) {
+      struct Cand {
+        double work, cells;
+        int dim, cid, req;
+      };
+      std::vector<Cand> cands;
+      for (int d = 1; d <= 3; ++d) {
+        DimPool &p = pool[d];
+        if (!p.eng) continue;
+        for (int c = 0; c < cfg->max_cases; ++c) {
+          int const ri = p.req_of_case[c];
+          if (ri < 0) continue;
+          alp_request const &r = reqs[ri];
+          double cells = 1.0;
+          for (int k = 0; k < d; ++k) cells *= 16.0 * r.nblocks[k];
+          double const left = r.max_steps > 0 ? double(r.max_steps - p.states[c].steps) : 1e30;
+          cands.push_back({cells * left, cells, d, c, ri});
+        }
+      }
+      std::stable_sort(cands.begin(), cands.end(), [](Cand const &a, Cand const &b) {
+        return a.work < b.work || (a.work == b.work && a.req < b.req);
+      });
+      double acc = 0.0;
+      for (Cand const &c : cands) {
+        int const hold = acc >= cfg->step_set_cells ? 1 : 0;
+        if (!hold) acc += c.cells;
+        DimPool &p = pool[c.dim];
+        if (p.held[c.cid] != hold) {
+          if (int rc = engine_set_hold(p.eng, c.cid, hold)) {
+            cleanup();
+            return rc;
+          }
+          p.held[c.cid] = hold;
+        }
+      }
+    }
+
     // advance every pool with resident cases (asynchronous, one stream each)
     for (auto &p : pool)
       if (p.active > 0) {
@@ -139,10 +190,11 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     // retire finished cases
     for (auto &p : pool) {
       if (p.active == 0) continue;
-      if (int rc = engine_case_states(p.eng, states)) {
+      if (int rc = engine_case_states(p.eng, p.states)) {
         cleanup();
         return rc;
       }
+      std::vector<CaseState> const &states = p.states;
       double const t_now = elapsed();
       for (int c = 0; c < cfg->max_cases; ++c) {
         int const ri = p.req_of_case[c];

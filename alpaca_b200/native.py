@@ -112,7 +112,8 @@ class Result(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("share_3d", C.c_double), ("scheme", Scheme),
-                ("max_cases", C.c_int), ("steps_per_poll", C.c_int), ("one_at_a_time", C.c_int)]
+                ("max_cases", C.c_int), ("steps_per_poll", C.c_int), ("one_at_a_time", C.c_int),
+                ("shortest_first", C.c_int), ("step_set_cells", C.c_double)]
 
 
 _D = C.POINTER(C.c_double)

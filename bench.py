@@ -54,6 +54,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serving-requests", type=int, default=32)
+    p.add_argument("--step-set-cells", type=float, default=float(1 << 22),
+                   help="cells stepping together under shortest-remaining-work-first serving")
     p.add_argument("--precision-report", action="store_true",
                    help="FP32-flux vs FP64 errors per field after 200 steps (128^3, 256^3, water)")
     p.add_argument("--serving-only", action="store_true",
@@ -232,8 +234,9 @@ def serving_report(args):
     """Serving form: one seeded request stream (2D four-quadrant problems and 3D
     gas / water blasts, log-uniform 4-2048 blocks, 200-2000 steps, Poisson
     arrivals at 50/s) served one case at a time in FP64, and with continuous
-    batching in FP64 and in the FP32-flux form; time-to-solution percentiles
-    and cases/s per mode."""
+    batching in FP64 and in the FP32-flux form, every resident case stepping or
+    shortest remaining work first (--step-set-cells stepping together); time-
+    to-solution percentiles and cases/s per mode."""
     import numpy as np
 
     from alpaca_b200 import api, serving
@@ -244,17 +247,24 @@ def serving_report(args):
            "mix": {k: sum(1 for r in reqs if r.kind == k) for k in
                    ("quadrants2d", "blast3d_gas", "blast3d_water")},
            "cell_updates": int(sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs))}
-    for name, prec, one in (("one_at_a_time_fp64", N.FP64, True), ("batched_fp64", N.FP64, False),
-                            ("batched_fp32_flux", N.FP32_FLUX, False)):
-        res, mk, _ = api.serve(reqs, budget, precision=prec, one_at_a_time=one)
+    out["step_set_cells"] = float(args.step_set_cells)
+    modes = (("one_at_a_time_fp64", N.FP64, True, False), ("batched_fp64", N.FP64, False, False),
+             ("batched_fp32_flux", N.FP32_FLUX, False, False),
+             ("batched_shortest_first_fp64", N.FP64, False, True),
+             ("batched_shortest_first_fp32_flux", N.FP32_FLUX, False, True))
+    for name, prec, one, srpt in modes:
+        res, mk, _ = api.serve(reqs, budget, precision=prec, one_at_a_time=one,
+                               shortest_first=srpt, step_set_cells=out["step_set_cells"])
         tts = np.array([r["finished_s"] - r["arrival_s"] for r in res])
         ok = sum(1 for r in res if r["status"] == 0)
         out[name] = {"cases_per_s": ok / mk, "makespan_s": mk, "p50_tts_s": float(np.percentile(tts, 50)),
                      "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok,
                      "cell_updates_per_s": out["cell_updates"] / mk}
-    base = out["one_at_a_time_fp64"]["cases_per_s"]
-    for k in ("batched_fp64", "batched_fp32_flux"):
-        out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base
+    base = out["one_at_a_time_fp64"]
+    for k, _, one, _ in modes:
+        if not one:
+            out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base["cases_per_s"]
+            out[k]["p50_tts_vs_one_at_a_time"] = out[k]["p50_tts_s"] / base["p50_tts_s"]
     return out
 
 

@@ -340,6 +340,10 @@ typedef struct {
   int max_cases;            /* resident cases per dimension */
   int steps_per_poll;       /* steps between completion checks */
   int one_at_a_time;        /* 1: admit a case only into an idle GPU (baseline) */
+  int shortest_first;       /* 1: step only the resident cases with the least remaining
+                               work (cells x steps left) up to step_set_cells cells, holding
+                               the others; 0: every resident case steps */
+  double step_set_cells;    /* cells stepped together under shortest_first (>= one case) */
 } alp_server_config;
 
 /* Serves n requests: admits arrived requests whose blocks fit (FIFO with

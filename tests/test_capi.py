@@ -90,6 +90,11 @@ def test_serve_rejects_bad_config_without_gpu():
     cfg.max_cases = 4
     rc = N.lib().alp_serve(C.byref(cfg), None, 0, None, None)
     assert rc == N.ALP_ERR_INVALID
+    cfg.steps_per_poll = 4
+    cfg.shortest_first = 1
+    cfg.step_set_cells = 0.0
+    rc = N.lib().alp_serve(C.byref(cfg), None, 0, None, None)
+    assert rc == N.ALP_ERR_INVALID and b"step_set_cells" in N.lib().alp_last_error()
 
 
 def test_request_stream_is_seeded_and_in_range():

@@ -88,6 +88,29 @@ def test_serving_mix_equals_alone(cuda):
     assert any(a1 < f0 for (a0, f0), (a1, _) in zip(mspans, mspans[1:]))
 
 
+def test_shortest_first_finishes_short_cases_first_with_the_same_bits(cuda):
+    """Shortest remaining work first: a small case that arrives with large ones
+    finishes before them, and every case keeps the bits it gets alone."""
+    rng = np.random.default_rng(12)
+    big = [serving.blast_request(rng, 27, 60, water=False) for _ in range(2)]
+    small = serving.quadrant_request(rng, 4, 20)
+    reqs = big + [small]
+    for r in reqs:
+        r.arrival_s = 0.0
+    budget = 2 << 30
+    # step set of one big case: the small case and one big case step, the
+    # other big case waits
+    res, _, st = api.serve(reqs, budget, keep_results=True, shortest_first=True,
+                           step_set_cells=27 * 4096.0, steps_per_poll=4)
+    alone, _, st_alone = api.serve(reqs, budget, one_at_a_time=True, keep_results=True)
+    for i, r in enumerate(reqs):
+        assert res[i]["status"] == 0 and res[i]["steps"] == r.max_steps
+        assert np.array_equal(st[i][cases.interior(r.dim)], st_alone[i][cases.interior(r.dim)]), i
+    assert res[2]["finished_s"] < min(res[0]["finished_s"], res[1]["finished_s"])
+    # the held big case finishes after the other one (it waited)
+    assert res[1]["finished_s"] > res[0]["finished_s"]
+
+
 def test_serving_budget_bounds_admission(cuda):
     """With a budget for one 8-block 3D case, requests are admitted one after
     the other and all complete."""

@@ -188,8 +188,8 @@ class Engine:
     def autotune(self, trial_steps: int = 3):
         """Times the stepping candidates on the resident cases (state unchanged)
         and keeps the fastest; returns (chosen index, ms per step per candidate)."""
-        chosen = C.c_int()
-        ms = (C.c_float * 3)()
+        chosen = C.c_int()  # candidates 0..3
+        ms = (C.c_float * 4)()
         self._check(self.lib.alp_engine_autotune(self.h, trial_steps, C.byref(chosen), ms))
         return chosen.value, [float(x) for x in ms]
 

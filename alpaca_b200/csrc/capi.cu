@@ -394,6 +394,10 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
   grab((void **)&e->cases, sizeof(CaseState) * max_cases);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
+  if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking);
+  for (cudaEvent_t &ev : e->ev_batch)
+    if (err == cudaSuccess) err = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+  if (err == cudaSuccess) err = cudaEventCreateWithFlags(&e->ev_join, cudaEventDisableTiming);
   if (err == cudaSuccess)
     err = cudaMemsetAsync(e->cases, 0, sizeof(CaseState) * max_cases, e->stream);
   if (err == cudaSuccess) err = cudaStreamSynchronize(e->stream);
@@ -560,18 +564,22 @@ alp_stream_t alp_engine_stream(alp_engine *e) { return e ? (alp_stream_t)e->stre
 int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");
   if (trial_steps <= 0) return fail(ALP_ERR_INVALID, "trial_steps must be positive");
-  // candidates: face fluxes with 128- or 64-thread blocks, pencil sweeps
+  // candidates: face fluxes with 128- or 64-thread blocks, pencil sweeps,
+  // face fluxes and stage updates overlapped in batches
   struct Cand {
     int path, threads;
   };
-  Cand const cands[3] = {{1, 128}, {1, 64}, {0, 128}};
-  int const ncand = 3;
+  Cand const cands[4] = {{1, 128}, {1, 64}, {0, 128}, {2, 128}};
+  int const ncand = 4;
+  auto allowed = [&](int i) {
+    if (i != 2) return true;
+    if (!e->opt.is_default()) return false;  // pencils: default schemes only
 #ifdef ALP_STRICT
-  int const allowed = 2;  // the pencil path changes the flux summation order
+    return false;  // the pencil path changes the flux summation order
 #else
-  // the pencil kernels are compiled for the default schemes only
-  int const allowed = e->opt.is_default() ? ncand : 2;
+    return true;
 #endif
+  };
   int const saved_path = e->path, saved_threads = e->face_threads;
   float best = 0.f;
   int best_i = 0;
@@ -580,7 +588,7 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
   ALP_CUDA(cudaEventCreate(&t1));
   for (int i = 0; i < ncand; ++i) {
     float ms = -1.f;
-    if (i < allowed && e->nwork > 0) {
+    if (allowed(i) && e->nwork > 0) {
       e->path = cands[i].path;
       e->face_threads = cands[i].threads;
       if (int rc = e->record_step(true)) return rc;  // warm-up
@@ -614,8 +622,9 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
 
 int alp_engine_set_path(alp_engine *e, int candidate) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");
-  int const paths[3] = {1, 1, 0}, threads[3] = {128, 64, 128};
-  if (candidate < 0 || candidate > 2) return fail(ALP_ERR_INVALID, "candidate must be 0, 1 or 2");
+  int const paths[4] = {1, 1, 0, 2}, threads[4] = {128, 64, 128, 128};
+  if (candidate < 0 || candidate > 3)
+    return fail(ALP_ERR_INVALID, "candidate must be 0, 1, 2 or 3");
 #ifdef ALP_STRICT
   if (candidate == 2) return fail(ALP_ERR_INVALID, "the strict build steps the face-flux path");
 #endif
@@ -636,8 +645,9 @@ int alp_engine_set_graph(alp_engine *e, int enabled) {
 int alp_engine_launches_per_step(alp_engine *e) {
   if (!e) return 0;
   // signal speed, dt, 3 stages x (one pencil sweep per direction, or face
-  // fluxes + stage update), commit
-  return 2 + 3 * (e->path == 0 ? e->dim : 2) + 1;
+  // fluxes + stage update, per batch on the overlapped path), commit
+  int const batches = e->path == 2 ? std::min(alp_engine::kMaxBatches, std::max(1, e->nwork / 64)) : 1;
+  return 2 + 3 * (e->path == 0 ? e->dim : 2 * batches) + 1;
 }
 
 }  // extern "C"

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <string>
 #include <vector>
@@ -45,7 +46,12 @@ struct alp_engine {
   double *U = nullptr, *UB = nullptr, *UC = nullptr;
   double *F = nullptr;  // face fluxes [slot][dim][NE][faces] (face-flux path)
   double *R = nullptr;  // per-cell flux differences [slot][NE][interior] (pencil path)
-  int path = 1;         // 0: pencil sweeps, 1: face fluxes + stage update
+  int path = 1;         // 0: pencil sweeps, 1: face fluxes + stage update, 2: the same in
+                        // overlapped batches
+  cudaStream_t stream2 = nullptr;  // stage updates of the overlapped path
+  static constexpr int kMaxBatches = 16;
+  cudaEvent_t ev_batch[kMaxBatches] = {};
+  cudaEvent_t ev_join = nullptr;
   int face_threads = 128;
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr;
@@ -87,12 +93,38 @@ struct alp_engine {
       Ls.U = in[s];
       if (path == 0) {
         ALP_CUDA(alp::launch_pencil_stage(Ls, U, out[s], R, nbr26, cases, s));
+      } else if (path == 2) {
+        if (int rc = record_overlapped_stage(Ls, out[s], s)) return rc;
       } else {
         ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride(), face_threads));
         ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
       }
     }
     if (!trial) ALP_CUDA(launch_step_commit(cases, max_cases, stream));
+    return ALP_OK;
+  }
+
+  // One stage in batches of work items: the faces of batch k+1 run on `stream`
+  // while the stage update of batch k runs on stream2 (the update is bound by
+  // HBM, the faces by the FP64 pipe). Faces read only the stage input and the
+  // updates write the stage output, so batches do not interfere; the next
+  // stage waits for every update. Same kernels and arithmetic as path 1.
+  int record_overlapped_stage(Launch const &Ls, double *Uout, int s) {
+    int const nb = std::min(kMaxBatches, std::max(1, nwork / 64));
+    int const per = (nwork + nb - 1) / nb;
+    for (int k = 0, off = 0; off < nwork; ++k, off += per) {
+      Launch Lk = Ls;
+      Lk.work = work + off;
+      Lk.nwork = std::min(per, nwork - off);
+      double *Fk = F + (size_t)off * stride();
+      ALP_CUDA(launch_face_flux_all(Lk, nbr26, cases, Fk, stride(), dstride(), face_threads));
+      ALP_CUDA(cudaEventRecord(ev_batch[k], stream));
+      ALP_CUDA(cudaStreamWaitEvent(stream2, ev_batch[k], 0));
+      Lk.stream = stream2;
+      ALP_CUDA(launch_stage_update(Lk, U, Uout, Fk, stride(), dstride(), s, cases, 0.0));
+    }
+    ALP_CUDA(cudaEventRecord(ev_join, stream2));
+    ALP_CUDA(cudaStreamWaitEvent(stream, ev_join, 0));
     return ALP_OK;
   }
 
@@ -157,6 +189,10 @@ struct alp_engine {
     cudaFree(nbr26);
     cudaFree(work);
     cudaFree(cases);
+    for (cudaEvent_t &ev : ev_batch)
+      if (ev) cudaEventDestroy(ev);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (stream2) cudaStreamDestroy(stream2);
     if (stream) cudaStreamDestroy(stream);
   }
 };

@@ -471,7 +471,8 @@ def run_ours(args, ws, rank, local):
                    "steps_done": steps_done,
                    "autotune": {"chosen": ["face fluxes, 128-thread blocks",
                                            "face fluxes, 64-thread blocks",
-                                           "pencil sweeps"][chosen],
+                                           "pencil sweeps",
+                                           "face fluxes and stage updates overlapped in batches"][chosen],
                                 "ms_per_step": cand_ms}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm,

@@ -252,11 +252,14 @@ int alp_engine_set_graph(alp_engine *e, int enabled);
  * + divergence/stage update, 1 = the same with 64-thread blocks, 2 = pencil
  * sweeps (one thread per line of cells, 17 faces with a sliding stencil
  * window, flux differences summed in the kernels and the RK stage applied by
- * the last direction; not available in the strict build). Each candidate runs
- * trial_steps steps whose last stage writes scratch memory and that are not
- * committed, so the cases' state and time are unchanged. *chosen receives the
- * candidate (-1 when no case is resident), ms_per_step[3] (may be null) the
- * measured time per step of each candidate (-1 when not run). Synchronises. */
+ * the last direction; not available in the strict build; default schemes
+ * only), 3 = candidate 0 in batches of about 64 blocks, the stage update of
+ * one batch on a second stream overlapping the face fluxes of the next (same
+ * arithmetic). Each candidate runs trial_steps steps
+ * whose last stage writes scratch memory and that are not committed, so the
+ * cases' state and time are unchanged. *chosen receives the candidate (-1 when
+ * no case is resident), ms_per_step[4] (may be null) the measured time per
+ * step of each candidate (-1 when not run). Synchronises. */
 int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step);
 
 /* Selects a stepping candidate (as numbered for alp_engine_autotune). */

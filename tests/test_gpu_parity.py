@@ -444,8 +444,8 @@ def test_fp32_flux_3d_100_steps(cuda, variant):
 def test_autotune_leaves_state_and_candidates_agree(cuda):
     """Autotuning runs uncommitted trial steps (state and time unchanged); every
     candidate advances the case to the same result within the FP64 tolerance
-    (face paths bit-identical to each other; the pencil path sums the three
-    flux differences in a different order)."""
+    (face paths, one launch or overlapped batches, bit-identical to each other;
+    the pencil path sums the three flux differences in a different order)."""
     case = cases.fourier_shock(2, dim=3, seed=31, steps=6)
     eng = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
     cid = eng.add_case(case)
@@ -453,10 +453,10 @@ def test_autotune_leaves_state_and_candidates_agree(cuda):
     before = eng.get(cid)
     chosen, ms = eng.autotune(trial_steps=2)
     after = eng.get(cid)
-    assert chosen in (0, 1, 2) and all(m > 0 for m in ms)
+    assert chosen in (0, 1, 2, 3) and all(m > 0 for m in ms)
     assert np.array_equal(before[0], after[0]) and before[1:] == after[1:]
     results = []
-    for cand in (0, 1, 2):
+    for cand in (0, 1, 2, 3):
         e = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
         i = e.add_case(case)
         e.set_path(cand)
@@ -466,4 +466,25 @@ def test_autotune_leaves_state_and_candidates_agree(cuda):
     eng.close()
     I = cases.interior(3)
     assert np.array_equal(results[0], results[1])
+    assert np.array_equal(results[0][I], results[3][I])
     assert l1_per_field(results[2][I], results[0][I]) <= 1e-13
+
+
+@pytest.mark.parametrize("variant", ["fvchar", "fsroe"])
+def test_overlapped_batches_strict_bit_exact(cuda, variant):
+    """Face fluxes and stage updates overlapped in batches (strict build)
+    reproduce the oracle bit for bit over 6 steps of a 6x6x6-block 3D case
+    (216 blocks: three batches)."""
+    case = cases.fourier_shock(6, dim=3, seed=32, steps=6)
+    ref = oracle.Restatement(3, variant).run(case.u, case.grid.nbr, case.gamma, 0.0, False,
+                                             case.grid.cell_size, case.cfl, 1e300, max_steps=6,
+                                             nthreads=os.cpu_count() or 8)
+    e = api.Engine(3, variant, capacity_blocks=case.grid.nb, max_cases=1, strict=True)
+    i = e.add_case(case)
+    e.set_path(3)
+    e.run_to_end(chunk=6)
+    got, t, steps = e.get(i)
+    e.close()
+    I = cases.interior(3)
+    assert steps == 6 and t == ref[1]
+    assert np.array_equal(got[I], ref[0][I])

@@ -69,9 +69,20 @@ template <int DIM, int DIR> struct FaceMap {
 // registers so that FV kernels keep 16-20 warps per SM without spilling
 // (FV characteristic: 126 registers at 4 CTAs); flux splitting keeps its
 // registers (its 6-cell flux and state stencils are live together).
-template <int SCHEME> struct FaceOccupancy { static constexpr int min_ctas = 1; };
-template <> struct FaceOccupancy<FV_CHAR> { static constexpr int min_ctas = 4; };
-template <> struct FaceOccupancy<FV_PRIM> { static constexpr int min_ctas = 5; };
+// Minimum resident 128-thread CTAs per SM of the face kernels (register caps
+// 256 / 128 / 96 at 1-2 / 4 / 5); compile-time tunable.
+#ifndef ALP_FS_ROE_CTAS
+#define ALP_FS_ROE_CTAS 1
+#endif
+#ifndef ALP_FV_CHAR_CTAS
+#define ALP_FV_CHAR_CTAS 4
+#endif
+#ifndef ALP_FV_PRIM_CTAS
+#define ALP_FV_PRIM_CTAS 5
+#endif
+template <int SCHEME> struct FaceOccupancy { static constexpr int min_ctas = ALP_FS_ROE_CTAS; };
+template <> struct FaceOccupancy<FV_CHAR> { static constexpr int min_ctas = ALP_FV_CHAR_CTAS; };
+template <> struct FaceOccupancy<FV_PRIM> { static constexpr int min_ctas = ALP_FV_PRIM_CTAS; };
 
 // Stores one face's fluxes in the reference flux-array layout: = (zero for a
 // skipped face) or, for the drop-in contract, += (skipped faces untouched).

@@ -22,11 +22,19 @@
 // the neighbour slot is a ghost block: a virtual node of the leaf's level whose
 // three cell layers next to the shared face are filled before each stage, by
 // injection from the coarser leaf, or by averaging the finer leaves with
-// Multiresolution::Average (multiresolution.h:94-166). The reference predicts
+// Multiresolution::Average (multiresolution.h:94-166); the reference predicts
 // the finer side with a fifth-order interpolation (Multiresolution::Prediction,
-// multiresolution.cpp:146) and corrects coarse fluxes at jumps
-// (JumpFluxAdjustment, modular_algorithm_assembler.cpp:1347); neither is done
-// here. Face neighbours may differ by one level at most.
+// multiresolution.cpp:146), which is not done here. Face neighbours may differ
+// by one level at most.
+//
+// Conservation at jumps as in the reference: after each stage update the
+// leaves integrate their jump-face fluxes with the RK3 jump multipliers times
+// their level step (space_solver.cpp:155-182, time_integrator.h:64-80); at the
+// end of each fine step these sums are averaged onto the parent's face
+// (Multiresolution::AverageJumpBuffer, multiresolution.cpp:47-128); at the end
+// of a coarse step the cells next to a refined neighbour get
+// - CMS(coarse sums) + CMS(fine sums) per unit cell size (JumpFluxAdjustment,
+// modular_algorithm_assembler.cpp:1347-1636).
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -39,9 +47,11 @@
 
 #include "../../include/alpaca_b200.h"
 #include "engine.hpp"
+#include "numerics.cuh"
 
 namespace {
 
+using alp::cms3;
 using alp::Geo;
 using alp::HS;
 using alp::IC;
@@ -145,6 +155,160 @@ ghost_fill_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const 
   }
 }
 
+// A jump face of a leaf: kind 2 (coarse side: the neighbour is refined) or 3
+// (fine side: the neighbour lies in a coarser leaf). Face loc: East 0, West 1,
+// North 2, South 3, Top 4, Bottom 5 (boundary_specifications.h:56-63). acc:
+// the parent-face accumulator the coarse side reads and the fine side fills;
+// o1, o2: offsets of the fine face on the parent face (transverse cells).
+struct JumpRec {
+  int item, slot, loc, level, kind, acc, o1, o2;
+};
+// A coarse leaf with jump faces: its record per face location (-1: none).
+struct CorrectRec {
+  int slot, level, rec[6];
+};
+
+template <int DIM>
+__device__ __forceinline__ void interior_coords_of(int t, int &i, int &j, int &k) {
+  if constexpr (DIM == 3) {
+    i = t >> 8;
+    j = (t >> 4) & 15;
+    k = t & 15;
+  } else if constexpr (DIM == 2) {
+    i = t >> 4;
+    j = t & 15;
+    k = 0;
+  } else {
+    i = t;
+    j = 0;
+    k = 0;
+  }
+}
+
+// RK3 jump multipliers (runge_kutta_3_TVD.h:42-46)
+__constant__ double kRkJump[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+
+template <int DIM> struct FaceCells {
+  __host__ __device__ static int t1(int d) { return d == 0 ? 1 : 0; }
+  __host__ __device__ static int t2(int d) { return d == 2 ? 1 : 2; }
+  __host__ __device__ static int n(int t) { return t < DIM ? IC : 1; }
+};
+
+// IntegrateJumpConservatives: J += (w_stage * dt_level) * F for the jump faces
+// of the leaves that integrated in this stage.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+jump_accumulate_kernel(JumpRec const *__restrict__ recs, double const *__restrict__ F,
+                       long long stride, long long dstride, double *__restrict__ jbuf,
+                       CaseState const *__restrict__ cu, int stage) {
+  using G = Geo<DIM>;
+  using FC = FaceCells<DIM>;
+  JumpRec const r = recs[blockIdx.x];
+  double const dtl = cu[r.level].dt;
+  if (!(dtl > 0.0)) return;
+  double const jstep = kRkJump[stage] * dtl;
+  int const d = r.loc / 2, a = (r.loc % 2) ? 0 : IC;
+  int const t1 = FC::t1(d), t2 = FC::t2(d), n1 = FC::n(t1), n2 = FC::n(t2);
+  double const *Fd = F + (long long)r.item * stride + d * dstride;
+  double *J = jbuf + (size_t)blockIdx.x * G::NE * IC * IC;
+  for (int x = threadIdx.x; x < G::NE * n1 * n2; x += blockDim.x) {
+    int const e = x / (n1 * n2), q = x % (n1 * n2), p1 = q / n2, p2 = q % n2;
+    int fi[3];
+    fi[d] = a;
+    fi[t1] = p1 + 1;
+    fi[t2] = p2 + 1;
+    J[e * IC * IC + p1 * IC + p2] += jstep * Fd[e * G::FACES + G::face(fi[0], fi[1], fi[2])];
+  }
+}
+
+// AverageJumpBuffer of the fine faces of leaves that finished a step onto the
+// parent faces, then their reset.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+jump_average_kernel(int const *__restrict__ fine, JumpRec const *__restrict__ recs,
+                    double *__restrict__ jbuf, double *__restrict__ acc,
+                    CaseState const *__restrict__ cu) {
+  using G = Geo<DIM>;
+  using FC = FaceCells<DIM>;
+  int const ri = fine[blockIdx.x];
+  JumpRec const r = recs[ri];
+  if (!(cu[r.level].dt > 0.0)) return;
+  int const d = r.loc / 2, t1 = FC::t1(d), t2 = FC::t2(d);
+  int const h1 = t1 < DIM ? IC / 2 : 1, h2 = t2 < DIM ? IC / 2 : 1;
+  double *J = jbuf + (size_t)ri * G::NE * IC * IC;
+  double *A = acc + (size_t)r.acc * G::NE * IC * IC;
+  for (int x = threadIdx.x; x < G::NE * h1 * h2; x += blockDim.x) {
+    int const e = x / (h1 * h2), q = x % (h1 * h2), i = q / h2, j = q % h2;
+    double const *c = J + e * IC * IC;
+    double v;
+    if constexpr (DIM == 1) v = c[0];
+    else if constexpr (DIM == 2) v = (c[(2 * i) * IC] + c[(2 * i + 1) * IC]) * 0.5;
+    else
+      v = ((c[(2 * i) * IC + 2 * j] + c[(2 * i + 1) * IC + 2 * j + 1]) +
+           (c[(2 * i + 1) * IC + 2 * j] + c[(2 * i) * IC + 2 * j + 1])) * 0.25;
+    A[e * IC * IC + (r.o1 + i) * IC + (r.o2 + j)] += v;
+  }
+  __syncthreads();
+  for (int x = threadIdx.x; x < G::NE * IC * IC; x += blockDim.x) J[x] = 0.0;
+}
+
+// JumpFluxAdjustment of the coarse leaves that finished a step: cells next to
+// a refined neighbour get - CMS(coarse) + CMS(fine) of their face sums divided
+// by the cell size (signs: +1 on West / South / Bottom faces, -1 on East /
+// North / Top), then the sums are reset.
+template <int DIM>
+__global__ void __launch_bounds__(256)
+jump_correct_kernel(CorrectRec const *__restrict__ corr, JumpRec const *__restrict__ recs,
+                    double *__restrict__ jbuf, double *__restrict__ acc, double *U,
+                    BlockMeta const *__restrict__ meta, CaseState const *__restrict__ cu) {
+  using G = Geo<DIM>;
+  using FC = FaceCells<DIM>;
+  CorrectRec const cr = corr[blockIdx.x];
+  if (!(cu[cr.level].dt > 0.0)) return;
+  double const ocs = 1.0 / meta[cr.slot].cell_size;
+  double *ub = U + (size_t)cr.slot * G::BLOCK_DOUBLES;
+  for (int t = threadIdx.x; t < G::INTERIOR; t += blockDim.x) {
+    int a[3];
+    interior_coords_of<DIM>(t, a[0], a[1], a[2]);
+    bool touched = false;
+#pragma unroll
+    for (int loc = 0; loc < 2 * DIM; ++loc) {
+      int const d = loc / 2;
+      touched |= cr.rec[loc] >= 0 && a[d] == ((loc % 2) ? 0 : IC - 1);
+    }
+    if (!touched) continue;
+    int const cell = G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2));
+    for (int e = 0; e < G::NE; ++e) {
+      double cf[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, ff[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+      for (int loc = 0; loc < 2 * DIM; ++loc) {
+        int const d = loc / 2, high = (loc % 2) == 0;
+        int const ri = cr.rec[loc];
+        if (ri < 0 || a[d] != (high ? IC - 1 : 0)) continue;
+        int const t1 = FC::t1(d), t2 = FC::t2(d);
+        int const x = e * IC * IC + a[t1] * IC + a[t2];
+        double const dir = high ? -1.0 : 1.0;
+        cf[loc] = jbuf[(size_t)ri * G::NE * IC * IC + x] * ocs * dir;
+        ff[loc] = acc[(size_t)recs[ri].acc * G::NE * IC * IC + x] * ocs * dir;
+      }
+      double &u = ub[e * G::CELLS + cell];
+      u -= cms3(cf[0] + cf[1], cf[2] + cf[3], cf[4] + cf[5]);
+      u += cms3(ff[0] + ff[1], ff[2] + ff[3], ff[4] + ff[5]);
+    }
+  }
+  __syncthreads();
+  for (int loc = 0; loc < 2 * DIM; ++loc) {
+    int const ri = cr.rec[loc];
+    if (ri < 0) continue;
+    double *J = jbuf + (size_t)ri * G::NE * IC * IC;
+    double *A = acc + (size_t)recs[ri].acc * G::NE * IC * IC;
+    for (int x = threadIdx.x; x < G::NE * IC * IC; x += blockDim.x) {
+      J[x] = 0.0;
+      A[x] = 0.0;
+    }
+  }
+}
+
 __device__ __forceinline__ int levels_height(int t) { return __popc((t + 1) ^ t); }
 
 // Micro time step from the per-level signal speeds, the per-level step sizes
@@ -203,6 +367,15 @@ struct NodeKey {
   }
 };
 
+// A leaf face at a level jump, as the tree builder finds it: kind 2 (coarse
+// side) or 3 (fine side); the parent face (node, face location) whose
+// accumulator the two sides share; the fine face's offsets on it.
+struct JumpFace {
+  int leaf, loc, kind;
+  NodeKey node;
+  int node_loc, o1, o2;
+};
+
 }  // namespace
 
 struct alp_levels {
@@ -214,6 +387,13 @@ struct alp_levels {
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr, *work = nullptr;
   GhostRec *ghosts = nullptr;
+  // jump-flux conservation: records, per-record sums, parent-face sums,
+  // fine-side record list, coarse leaves to correct
+  int nrec = 0, nfine = 0, ncorr = 0, nacc = 0;
+  JumpRec *jrecs = nullptr;
+  double *jbuf = nullptr, *jacc = nullptr;
+  int *jfine = nullptr;
+  CorrectRec *jcorr = nullptr;
   CaseState *cu = nullptr, *cf = nullptr;
   LevelState *ls = nullptr;
   std::vector<int> nwork_ge;  // work items of level >= l
@@ -255,6 +435,32 @@ struct alp_levels {
         Ls.nwork = nwork_ge[lu];
         if (Ls.nwork > 0)
           ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cu, 0.0));
+        if (nrec > 0) {
+          switch (dim) {
+            case 1: jump_accumulate_kernel<1><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
+            case 2: jump_accumulate_kernel<2><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
+            default: jump_accumulate_kernel<3><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
+          }
+          ALP_CUDA(cudaGetLastError());
+        }
+      }
+      // the levels that integrated have finished a step: fine sums onto the
+      // parent faces, then the coarse corrections
+      if (nfine > 0) {
+        switch (dim) {
+          case 1: jump_average_kernel<1><<<nfine, 256, 0, stream>>>(jfine, jrecs, jbuf, jacc, cu); break;
+          case 2: jump_average_kernel<2><<<nfine, 256, 0, stream>>>(jfine, jrecs, jbuf, jacc, cu); break;
+          default: jump_average_kernel<3><<<nfine, 256, 0, stream>>>(jfine, jrecs, jbuf, jacc, cu); break;
+        }
+        ALP_CUDA(cudaGetLastError());
+      }
+      if (ncorr > 0) {
+        switch (dim) {
+          case 1: jump_correct_kernel<1><<<ncorr, 256, 0, stream>>>(jcorr, jrecs, jbuf, jacc, U, meta, cu); break;
+          case 2: jump_correct_kernel<2><<<ncorr, 256, 0, stream>>>(jcorr, jrecs, jbuf, jacc, U, meta, cu); break;
+          default: jump_correct_kernel<3><<<ncorr, 256, 0, stream>>>(jcorr, jrecs, jbuf, jacc, U, meta, cu); break;
+        }
+        ALP_CUDA(cudaGetLastError());
       }
       levels_commit_kernel<<<1, 1, 0, stream>>>(ls, tm, nmicro);
       ALP_CUDA(cudaGetLastError());
@@ -272,6 +478,11 @@ struct alp_levels {
     cudaFree(nbr26);
     cudaFree(work);
     cudaFree(ghosts);
+    cudaFree(jrecs);
+    cudaFree(jbuf);
+    cudaFree(jacc);
+    cudaFree(jfine);
+    cudaFree(jcorr);
     cudaFree(cu);
     cudaFree(cf);
     cudaFree(ls);
@@ -283,7 +494,8 @@ namespace {
 
 // Validates the tree and builds the per-slot neighbour table and the ghosts.
 int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const *coord,
-               std::vector<int> &nbr26, std::vector<GhostRec> &ghosts, int *lmax_out) {
+               std::vector<int> &nbr26, std::vector<GhostRec> &ghosts,
+               std::vector<JumpFace> &jumps, int *lmax_out) {
   using alp::fail;
   int lmax = 0;
   for (int b = 0; b < nleaf; ++b) {
@@ -353,7 +565,10 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
       GhostRec gr{};
       gr.level = l;
       for (int o = 0; o < 8; ++o) gr.src[o] = -1;
+      int const loc = f ^ 1;  // East 0, West 1, North 2, South 3, Top 4, Bottom 5
       if (refined.count(k)) {
+        // coarse side: the neighbour's opposite face collects the fine sums
+        jumps.push_back({b, loc, 2, k, loc ^ 1, 0, 0});
         gr.type = 1;
         gr.src_level = l + 1;
         for (int o = 0; o < (1 << dim); ++o) {
@@ -376,6 +591,16 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
         gr.type = 0;
         gr.src_level = l - 1;
         gr.src[0] = ci->second;
+        // fine side: this leaf's face lies on its parent's face of the same location
+        NodeKey parent{l - 1, {0, 0, 0}};
+        int oc[3] = {0, 0, 0};
+        for (int e = 0; e < dim; ++e) {
+          parent.c[e] = coord[3 * b + e] >> 1;
+          oc[e] = coord[3 * b + e] & 1;
+        }
+        int const t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+        jumps.push_back({b, loc, 3, parent, loc, t1 < dim ? oc[t1] * (IC / 2) : 0,
+                         t2 < dim ? oc[t2] * (IC / 2) : 0});
         int oct = 0;
         for (int e = 0; e < dim; ++e) oct |= (p[e] & 1) << e;
         gr.src[1] = oct;
@@ -425,8 +650,9 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   for (int d = 0; d < dim; ++d) n0v[d] = n0[d];
   std::vector<int> nbr;
   std::vector<GhostRec> gh;
+  std::vector<JumpFace> jf;
   int lmax = 0;
-  if (int rc = build_tree(dim, n0v, nleaf, h_level, h_coord, nbr, gh, &lmax)) return rc;
+  if (int rc = build_tree(dim, n0v, nleaf, h_level, h_coord, nbr, gh, jf, &lmax)) return rc;
 
   alp_levels *m = new (std::nothrow) alp_levels;
   if (!m) return fail(ALP_ERR_CUDA, "host allocation failed");
@@ -455,6 +681,38 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   for (int l = 0; l <= lmax; ++l)
     for (int b = 0; b < nleaf; ++b)
       if (h_level[b] >= l) ++m->nwork_ge[l];
+
+  // jump records: one per jump face, an accumulator per parent face
+  std::vector<int> item_of(nleaf);
+  for (int i = 0; i < nleaf; ++i) item_of[work[i]] = i;
+  std::vector<JumpRec> recs;
+  std::vector<int> fine;
+  std::vector<CorrectRec> corr;
+  std::map<std::pair<NodeKey, int>, int> acc_of;
+  std::map<int, int> corr_of;  // leaf -> CorrectRec index
+  for (JumpFace const &j : jf) {
+    auto key = std::make_pair(j.node, j.node_loc);
+    auto it = acc_of.find(key);
+    int const acc = it == acc_of.end() ? (int)acc_of.size() : it->second;
+    if (it == acc_of.end()) acc_of.emplace(key, acc);
+    int const ri = (int)recs.size();
+    recs.push_back({item_of[j.leaf], j.leaf, j.loc, h_level[j.leaf], j.kind, acc, j.o1, j.o2});
+    if (j.kind == 3) {
+      fine.push_back(ri);
+    } else {
+      auto ci = corr_of.find(j.leaf);
+      if (ci == corr_of.end()) {
+        CorrectRec c{j.leaf, h_level[j.leaf], {-1, -1, -1, -1, -1, -1}};
+        ci = corr_of.emplace(j.leaf, (int)corr.size()).first;
+        corr.push_back(c);
+      }
+      corr[ci->second].rec[j.loc] = ri;
+    }
+  }
+  m->nrec = (int)recs.size();
+  m->nfine = (int)fine.size();
+  m->ncorr = (int)corr.size();
+  m->nacc = (int)acc_of.size();
 
   std::vector<BlockMeta> meta(m->nslots);
   for (int b = 0; b < nleaf; ++b)
@@ -488,6 +746,23 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
       (e = cudaMalloc(&m->cf, sizeof(CaseState) * m->nlev)) != cudaSuccess ||
       (e = cudaMalloc(&m->ls, sizeof(LevelState))) != cudaSuccess)
     return cleanup(cuda_fail(e, "cudaMalloc(level tables)"));
+  size_t const jface = (size_t)m->ne * IC * IC * sizeof(double);
+  if (m->nrec > 0) {
+    if ((e = cudaMalloc(&m->jrecs, sizeof(JumpRec) * m->nrec)) != cudaSuccess ||
+        (e = cudaMalloc(&m->jbuf, jface * m->nrec)) != cudaSuccess ||
+        (e = cudaMalloc(&m->jacc, jface * std::max(m->nacc, 1))) != cudaSuccess ||
+        (e = cudaMalloc(&m->jfine, sizeof(int) * std::max(m->nfine, 1))) != cudaSuccess ||
+        (e = cudaMalloc(&m->jcorr, sizeof(CorrectRec) * std::max(m->ncorr, 1))) != cudaSuccess ||
+        (e = cudaMemsetAsync(m->jbuf, 0, jface * m->nrec, m->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(m->jacc, 0, jface * std::max(m->nacc, 1), m->stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(m->jrecs, recs.data(), sizeof(JumpRec) * m->nrec,
+                             cudaMemcpyHostToDevice, m->stream)) != cudaSuccess ||
+        (m->nfine > 0 && (e = cudaMemcpyAsync(m->jfine, fine.data(), sizeof(int) * m->nfine,
+                                              cudaMemcpyHostToDevice, m->stream)) != cudaSuccess) ||
+        (m->ncorr > 0 && (e = cudaMemcpyAsync(m->jcorr, corr.data(), sizeof(CorrectRec) * m->ncorr,
+                                              cudaMemcpyHostToDevice, m->stream)) != cudaSuccess))
+      return cleanup(cuda_fail(e, "jump-flux tables"));
+  }
   std::vector<CaseState> cs(m->nlev);
   for (auto &c : cs) {
     c = CaseState{};
@@ -594,7 +869,9 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
         n += m->nghost > 0 ? 1 : 0;
         n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? 1 : 0;
         n += m->nwork_ge[lu] > 0 ? 1 : 0;
+        n += m->nrec > 0 ? 1 : 0;
       }
+      n += (m->nfine > 0 ? 1 : 0) + (m->ncorr > 0 ? 1 : 0);
     }
     *launches_per_macro_step = n;
   }

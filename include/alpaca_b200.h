@@ -283,8 +283,11 @@ int alp_engine_launches_per_step(alp_engine *e);
  * the finest cell size (:1925-1982). Halo cells across a level jump are the
  * average of the finer leaves (Multiresolution::Average,
  * multiresolution/multiresolution.h:94-166) or the coarser leaf's cell
- * (injection); the reference's fifth-order prediction
- * (multiresolution.cpp:146) and jump-flux correction (:1347) are not applied.
+ * (injection; the reference's fifth-order prediction, multiresolution.cpp:146,
+ * is not applied). Conservation at jumps as JumpFluxAdjustment
+ * (modular_algorithm_assembler.cpp:1347-1636): jump-face fluxes integrated
+ * with the RK3 jump multipliers, fine sums averaged onto the parent faces
+ * after each fine step, coarse cells corrected after each coarse step.
  * h_blocks: [nleaf][NE][cells], interiors read. All levels run in the same
  * batched launches; one CUDA graph per macro step. */
 typedef struct alp_levels alp_levels;

@@ -1208,11 +1208,19 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr
  *
  * Halo cells across a jump (a face neighbour one level coarser or finer) are
  * filled by averaging the finer leaves with Multiresolution::Average
- * (multiresolution.h:94-166) and by injection from the coarser leaf. The
- * reference predicts the finer side with a fifth-order interpolation
- * (Multiresolution::Prediction, multiresolution.cpp:146) and corrects coarse
- * fluxes at jumps (JumpFluxAdjustment, modular_algorithm_assembler.cpp:1347);
- * neither is restated. Face neighbours must differ by at most one level.
+ * (multiresolution.h:94-166) and by injection from the coarser leaf (the
+ * reference predicts the finer side with a fifth-order interpolation,
+ * Multiresolution::Prediction, multiresolution.cpp:146, not restated here).
+ * Conservation at jumps follows the reference: every leaf integrates its
+ * boundary face fluxes at jump faces with the RK3 jump multipliers (1/6, 1/6,
+ * 2/3) times its level step (SpaceSolver::UpdateFluxes space_solver.cpp:155-182,
+ * IntegrateJumpConservatives time_integrator.h:64-80, runge_kutta_3_TVD.h:42-46);
+ * at the end of each fine step these sums are averaged onto the parent's face
+ * (Multiresolution::AverageJumpBuffer, multiresolution.cpp:47-128) and reset;
+ * at the end of a coarse step the cells of a coarse leaf next to a refined
+ * neighbour get - CMS(coarse sums) + CMS(fine sums) per unit cell size
+ * (JumpFluxAdjustment, modular_algorithm_assembler.cpp:1347-1636) and the sums
+ * are reset. Face neighbours must differ by at most one level.
  */
 
 #define MAXLEV 8
@@ -1411,6 +1419,40 @@ static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double
   }
 }
 
+/* Face neighbour kind of leaf b across face loc (East 0, West 1, North 2,
+ * South 3, Top 4, Bottom 5; boundary_specifications.h:56-63): 0 domain face,
+ * 1 same-level leaf, 2 refined node (finer leaves), 3 inside a coarser leaf.
+ * p receives the neighbour position at the leaf's level. */
+static int face_kind(const Tree *t, int b, int loc, int p[3]) {
+  int const l = t->level[b], d = loc / 2, s = (loc % 2) ? -1 : 1;
+  for (int e = 0; e < 3; ++e) p[e] = e < t->dim ? t->coord[3 * b + e] : 0;
+  p[d] += s;
+  if (p[d] < 0 || p[d] >= t->ext[l][d]) return 0;
+  int const v = t->grid[l][tree_at(t, l, p)];
+  return v >= 0 ? 1 : (v == -2 ? 2 : 3);
+}
+
+/* Boundary face fluxes of a leaf, per location and field over the transverse
+ * face cells (p1, p2) in increasing dimension order (the jump-buffer layout,
+ * space_solver.cpp:155-182), from the flux arrays of block_fluxes. */
+static void boundary_fluxes(const Geom *g, double *f[3], double *out) {
+  int const ne = g->ne, n2 = IC * IC;
+  for (int loc = 0; loc < 2 * g->dim; ++loc) {
+    int const d = loc / 2, a = (loc % 2) ? 0 : g->ic[d];
+    int const t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+    for (int e = 0; e < ne; ++e)
+      for (int p1 = 0; p1 < g->ic[t1]; ++p1)
+        for (int p2 = 0; p2 < g->ic[t2]; ++p2) {
+          int fi[3];
+          fi[d] = a;
+          fi[t1] = p1 + 1;
+          fi[t2] = p2 + 1;
+          out[((long)loc * ne + e) * n2 + p1 * IC + p2] =
+              f[d][(long)e * g->faces + fidx(g, fi[0], fi[1], fi[2])];
+        }
+  }
+}
+
 /* number of levels GetLevels(t) returns (modular_algorithm_assembler.cpp:2564-2573) */
 static int get_levels_height(unsigned t) { return __builtin_popcount((t + 1) ^ t); }
 
@@ -1422,6 +1464,7 @@ typedef struct {
   const int *items;
   double *pool;
   double *rhs;
+  double *bflux; /* per leaf [6][NE][IC*IC] boundary face fluxes */
   double h0;
 } LevelRhsCtx;
 
@@ -1432,6 +1475,116 @@ static void level_rhs_task(void *vctx, int i, Work *w, double *f[3]) {
   double const h = c->h0 / (double)(1 << c->t->level[b]);
   block_fluxes(c->g, c->e, c->solver, c->recon, c->pool + b * blk, w, f);
   block_divergence(c->g, h, f, c->rhs + b * blk);
+  boundary_fluxes(c->g, f, c->bflux + (long)b * 6 * c->g->ne * IC * IC);
+}
+
+/* RK3 jump multipliers (runge_kutta_3_TVD.h:42-46) */
+static const double rk_jump[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+
+/* End of micro step tm for the levels >= lu (they just finished a step with
+ * a positive level step): AverageJumpBuffer of the finished fine leaves onto
+ * their parents' faces, then JumpFluxAdjustment of the finished coarse leaves,
+ * then the reset. */
+static void level_jump_fluxes(const Geom *g, const Tree *t, double *u, double *jump,
+                              double **pjump[MAXLEV], const double *hist, int tm, int lu,
+                              double h0) {
+  int const ne = g->ne, n2 = IC * IC, dim = g->dim;
+  long const jsz = 6L * ne * n2, fsz = (long)ne * n2;
+  long const blk = (long)ne * g->cells;
+  int done[MAXLEV];
+  for (int l = 0; l <= t->lmax; ++l) {
+    double dtl = 0.0;
+    if (l >= lu)
+      for (int k = tm; k > tm - (1 << (t->lmax - l)); --k) dtl += hist[k];
+    done[l] = dtl > 0.0;
+  }
+  /* averaging down (multiresolution.cpp:47-128), finished fine leaves */
+  for (int b = 0; b < t->nleaf; ++b) {
+    int const l = t->level[b];
+    if (l == 0 || !done[l]) continue;
+    for (int loc = 0; loc < 2 * dim; ++loc) {
+      int pn[3];
+      if (face_kind(t, b, loc, pn) != 3) continue;
+      int pc[3] = {0, 0, 0}, oc[3] = {0, 0, 0};
+      for (int e = 0; e < dim; ++e) {
+        pc[e] = t->coord[3 * b + e] >> 1;
+        oc[e] = t->coord[3 * b + e] & 1;
+      }
+      long const pidx = tree_at(t, l - 1, pc);
+      double **slot = &pjump[l - 1][pidx];
+      if (!*slot) *slot = (double *)calloc((size_t)jsz, sizeof(double));
+      double *pj = *slot + (long)loc * fsz;
+      double *cj = jump + (long)b * jsz + (long)loc * fsz;
+      int const d = loc / 2, t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+      int const n1 = g->ic[t1] > 1 ? IC / 2 : 1, n2c = g->ic[t2] > 1 ? IC / 2 : 1;
+      int const o1 = t1 < dim ? oc[t1] * (IC / 2) : 0, o2 = t2 < dim ? oc[t2] * (IC / 2) : 0;
+      for (int e = 0; e < ne; ++e)
+        for (int i = 0; i < n1; ++i)
+          for (int j = 0; j < n2c; ++j) {
+            const double *c = cj + (long)e * n2;
+            double v;
+            if (dim == 1)
+              v = c[0];
+            else if (dim == 2)
+              v = (c[(2 * i) * IC] + c[(2 * i + 1) * IC]) * 0.5;
+            else
+              v = ((c[(2 * i) * IC + 2 * j] + c[(2 * i + 1) * IC + 2 * j + 1]) +
+                   (c[(2 * i + 1) * IC + 2 * j] + c[(2 * i) * IC + 2 * j + 1])) * 0.25;
+            pj[(long)e * n2 + (o1 + i) * IC + (o2 + j)] += v;
+          }
+      for (long x = 0; x < fsz; ++x) cj[x] = 0.0;
+    }
+  }
+  /* exchange and correction (modular_algorithm_assembler.cpp:1410-1636) */
+  for (int b = 0; b < t->nleaf; ++b) {
+    int const l = t->level[b];
+    if (!done[l]) continue;
+    int kinds[6] = {0, 0, 0, 0, 0, 0}, any = 0;
+    double *pj[6] = {0, 0, 0, 0, 0, 0};
+    for (int loc = 0; loc < 2 * dim; ++loc) {
+      int pn[3];
+      kinds[loc] = face_kind(t, b, loc, pn);
+      if (kinds[loc] != 2) continue;
+      any = 1;
+      double **slot = &pjump[l][tree_at(t, l, pn)];
+      if (!*slot) *slot = (double *)calloc((size_t)jsz, sizeof(double));
+      pj[loc] = *slot + (long)(loc ^ 1) * fsz; /* the neighbour's opposite face */
+    }
+    if (!any) continue;
+    double const ocs = 1.0 / (h0 / (double)(1 << l));
+    double *ub = u + b * blk;
+    for (int e = 0; e < ne; ++e)
+      for (int i = 0; i < g->ic[0]; ++i)
+        for (int j = 0; j < g->ic[1]; ++j)
+          for (int k = 0; k < g->ic[2]; ++k) {
+            int const a[3] = {i, j, k};
+            double cf[6] = {0, 0, 0, 0, 0, 0}, ff[6] = {0, 0, 0, 0, 0, 0};
+            int touched = 0;
+            for (int loc = 0; loc < 2 * dim; ++loc) {
+              if (kinds[loc] != 2) continue;
+              int const d = loc / 2, high = (loc % 2) == 0;
+              if (a[d] != (high ? IC - 1 : 0)) continue;
+              int const t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
+              long const x = (long)e * n2 + a[t1] * IC + (t2 < 3 ? a[t2] : 0);
+              double const dir = high ? -1.0 : 1.0;
+              cf[loc] = jump[(long)b * jsz + (long)loc * fsz + x] * ocs * dir;
+              ff[loc] = pj[loc][x] * ocs * dir;
+              touched = 1;
+            }
+            if (!touched) continue;
+            double *cell = ub + (long)e * g->cells + cidx(g, i + fic(g, 0), j + fic(g, 1), k + fic(g, 2));
+            *cell -= cms3(cf[0] + cf[1], cf[2] + cf[3], cf[4] + cf[5]);
+            *cell += cms3(ff[0] + ff[1], ff[2] + ff[3], ff[4] + ff[5]);
+          }
+    for (int loc = 0; loc < 2 * dim; ++loc) {
+      if (kinds[loc] != 2) continue;
+      double *cj = jump + (long)b * jsz + (long)loc * fsz;
+      for (long x = 0; x < fsz; ++x) {
+        cj[x] = 0.0;
+        pj[loc][x] = 0.0;
+      }
+    }
+  }
 }
 
 int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, const int *level,
@@ -1454,8 +1607,19 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
   double *rhs = (double *)calloc((size_t)n, sizeof(double));
   int *items = (int *)malloc(sizeof(int) * nleaf);
   double *hist = (double *)malloc(sizeof(double) * nmicro);
-  if (!pb || !pc || !rhs || !items || !hist) {
-    free(pb); free(pc); free(rhs); free(items); free(hist);
+  long const jsz = 6L * g.ne * IC * IC; /* one leaf's six jump buffers */
+  double *bflux = (double *)calloc((size_t)nleaf * jsz, sizeof(double));
+  double *jump = (double *)calloc((size_t)nleaf * jsz, sizeof(double));
+  /* jump buffers of refined nodes (the parents' faces), per level and node */
+  double **pjump[MAXLEV] = {0};
+  int ok = pb && pc && rhs && items && hist && bflux && jump;
+  for (int l = 0; ok && l <= tr.lmax; ++l) {
+    pjump[l] = (double **)calloc((size_t)tr.ext[l][0] * tr.ext[l][1] * tr.ext[l][2], sizeof(double *));
+    ok = pjump[l] != NULL;
+  }
+  if (!ok) {
+    free(pb); free(pc); free(rhs); free(items); free(hist); free(bflux); free(jump);
+    for (int l = 0; l < MAXLEV; ++l) free(pjump[l]);
     tree_free(&tr);
     return 3;
   }
@@ -1487,7 +1651,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
             level_halos(&g, &tr, b, pool_in[s], src);
             items[ni++] = b;
           }
-        LevelRhsCtx c = {&g, &e, solver, recon, &tr, items, pool_in[s], rhs, h0};
+        LevelRhsCtx c = {&g, &e, solver, recon, &tr, items, pool_in[s], rhs, bflux, h0};
         parallel_blocks(&g, ni, nthreads, level_rhs_task, &c);
         for (int b = 0; b < nleaf; ++b) {
           int const l = level[b];
@@ -1508,15 +1672,31 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                   if (s != 0) v = m0 * v + m1 * u0[x];
                   uo[x] = v + step * r[x];
                 }
+          /* IntegrateJumpConservatives: jump faces integrate their fluxes */
+          double const jstep = rk_jump[s] * dtl;
+          for (int loc = 0; loc < 2 * dim; ++loc) {
+            int pn[3];
+            int const kind = face_kind(&tr, b, loc, pn);
+            if (kind < 2) continue;
+            double *jb = jump + (long)b * jsz + (long)loc * g.ne * IC * IC;
+            const double *fb = bflux + (long)b * jsz + (long)loc * g.ne * IC * IC;
+            for (long x = 0; x < (long)g.ne * IC * IC; ++x) jb[x] += jstep * fb[x];
+          }
         }
       }
+      level_jump_fluxes(&g, &tr, u, jump, pjump, hist, tm, lu, h0);
     }
     double sum = 0.0;
     for (int k = 0; k < nmicro; ++k) sum = sum + hist[k];
     t = t + sum;
     ++macro;
   }
-  free(pb); free(pc); free(rhs); free(items); free(hist);
+  free(pb); free(pc); free(rhs); free(items); free(hist); free(bflux); free(jump);
+  for (int l = 0; l < MAXLEV; ++l) {
+    if (pjump[l])
+      for (long x = 0; x < (long)tr.ext[l][0] * tr.ext[l][1] * tr.ext[l][2]; ++x) free(pjump[l][x]);
+    free(pjump[l]);
+  }
   tree_free(&tr);
   *t_io = t;
   *macro_done = macro;

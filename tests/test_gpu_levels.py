@@ -68,6 +68,24 @@ def test_levels_strict_bit_exact(cuda, name):
     assert np.array_equal(got[I], ref[I])
 
 
+def test_levels_conserve_mass_and_energy(cuda):
+    """Jump-flux correction on the GPU: mass and energy of the 2D three-level
+    tree change by round-off only over two macro steps."""
+    c = small_trees()["2d_three_levels"]
+    eng = api.LevelEngine(c, "fvchar", max_macro=2)
+    eng.step(2)
+    got, t, m = eng.get()
+    eng.close()
+    I = cases.interior(2)
+    vol = (c.h0 / (1 << c.level)) ** 2
+
+    def tot(u, f):
+        return (u[I][:, f].reshape(c.nleaf, -1).sum(1) * vol).sum()
+
+    for f in (0, 1):
+        assert abs(tot(got, f) - tot(c.u, f)) <= 1e-14 * tot(c.u, f)
+
+
 def test_single_level_tree_equals_engine(cuda):
     """A tree without refinement is the single-level engine on the same grid."""
     g = cases.BlockGrid(3, (2, 2, 2), (False,) * 3, 1.0 / 32)

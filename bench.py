@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-serving", action="store_true")
     p.add_argument("--serving-requests", type=int, default=32)
-    p.add_argument("--step-set-cells", type=float, default=float(1 << 22),
+    p.add_argument("--step-set-cells", type=float, default=float(1 << 21),
                    help="cells stepping together under shortest-remaining-work-first serving")
     p.add_argument("--precision-report", action="store_true",
                    help="FP32-flux vs FP64 errors per field after 200 steps (128^3, 256^3, water)")

@@ -80,9 +80,25 @@ template <int DIM, int DIR> struct FaceMap {
 #ifndef ALP_FV_PRIM_CTAS
 #define ALP_FV_PRIM_CTAS 5
 #endif
-template <int SCHEME> struct FaceOccupancy { static constexpr int min_ctas = ALP_FS_ROE_CTAS; };
-template <> struct FaceOccupancy<FV_CHAR> { static constexpr int min_ctas = ALP_FV_CHAR_CTAS; };
-template <> struct FaceOccupancy<FV_PRIM> { static constexpr int min_ctas = ALP_FV_PRIM_CTAS; };
+// FP32-flux instantiations (fewer live doubles) have their own limits
+// (measured on the 128^3 step: FS 4 CTAs 2.05 ms vs 3: 2.23, 2: 2.86; FV
+// char 5 CTAs 1.56 ms vs 4: 1.64, 6: 1.59; FV prim 5: 1.455 vs 6: 1.48).
+#ifndef ALP_FS_ROE_CTAS_F32
+#define ALP_FS_ROE_CTAS_F32 4
+#endif
+#ifndef ALP_FV_CHAR_CTAS_F32
+#define ALP_FV_CHAR_CTAS_F32 5
+#endif
+#ifndef ALP_FV_PRIM_CTAS_F32
+#define ALP_FV_PRIM_CTAS_F32 ALP_FV_PRIM_CTAS
+#endif
+template <int SCHEME, typename T = double> struct FaceOccupancy {
+  static constexpr bool f32 = sizeof(T) == 4;
+  static constexpr int min_ctas =
+      SCHEME == FV_CHAR ? (f32 ? ALP_FV_CHAR_CTAS_F32 : ALP_FV_CHAR_CTAS)
+      : SCHEME == FV_PRIM ? (f32 ? ALP_FV_PRIM_CTAS_F32 : ALP_FV_PRIM_CTAS)
+                          : (f32 ? ALP_FS_ROE_CTAS_F32 : ALP_FS_ROE_CTAS);
+};
 
 // Stores one face's fluxes in the reference flux-array layout: = (zero for a
 // skipped face) or, for the drop-in contract, += (skipped faces untouched).
@@ -421,7 +437,7 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
 
 // One direction over all work items (drop-in calls: halos from the buffer).
 template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM>
-__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME>::min_ctas)
+__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME, T>::min_ctas)
 face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
                  BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
                  long long stride) {
@@ -437,7 +453,7 @@ face_flux_kernel(double const *__restrict__ U, int const *__restrict__ work,
 // direction, stencils gathered from neighbours, direction d written to
 // F + d * dstride. Items whose case is inactive (dt == 0) are skipped.
 template <int DIM, int SCHEME, typename T>
-__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME>::min_ctas)
+__global__ void __launch_bounds__(128, FaceOccupancy<SCHEME, T>::min_ctas)
 face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
                      BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
                      CaseState const *__restrict__ cases, double *__restrict__ F,

@@ -39,6 +39,13 @@ EXT_SCHEMES = {
     "fs_roem": ("fsroe", {"flux_splitting": FLUX_SPLITTING_ROE_M}),
     "fs_llfm": ("fsroe", {"flux_splitting": FLUX_SPLITTING_LLF_M}),
     "fs_teno5": ("fsroe", {"reconstruction_stencil": STENCIL_TENO5}),
+    "fvchar_weno3_hll": ("fvchar", {"reconstruction_stencil": STENCIL_WENO3,
+                                    "riemann_solver": RIEMANN_HLL}),
+    "fs_weno3": ("fsroe", {"reconstruction_stencil": STENCIL_WENO3}),
+    "fs_llf_weno3": ("fsroe", {"reconstruction_stencil": STENCIL_WENO3,
+                               "flux_splitting": FLUX_SPLITTING_LLF}),
+    "fs_llfm_weno3": ("fsroe", {"reconstruction_stencil": STENCIL_WENO3,
+                                "flux_splitting": FLUX_SPLITTING_LLF_M}),
 }
 RK3 = 1
 FP64, FP32_FLUX = 0, 1

@@ -60,6 +60,12 @@ EXT_VARIANTS = {
     "fs_roem": ("fsroe", (WENO5, HLLC, EINFELDT, ROE_M)),
     "fs_llfm": ("fsroe", (WENO5, HLLC, EINFELDT, LLF_M)),
     "fs_teno5": ("fsroe", (TENO5, HLLC, EINFELDT, ROE)),
+    # the four single-phase selections of the reference testsuite's DetailedSod
+    # table (32-cell blocks, RK3) that differ from the defaults in two places
+    "fvchar_weno3_hll": ("fvchar", (WENO3, HLL, EINFELDT, ROE)),
+    "fs_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, ROE)),
+    "fs_llf_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, LLF)),
+    "fs_llfm_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, LLF_M)),
 }
 
 

@@ -9,6 +9,7 @@ tell that the generator still reproduces it bit for bit.
     python tests/golden/make_golden.py            # small fixtures
     python tests/golden/make_golden.py --c2       # also the 128^3, 100-step run summary
     python tests/golden/make_golden.py --ext      # the further selections (make -C oracle ref-ext)
+    python tests/golden/make_golden.py --ext fs_weno3   # only the named selections
 """
 from __future__ import annotations
 
@@ -75,10 +76,11 @@ def short_run_fixtures(nsteps: int = 5):
             print("wrote", path)
 
 
-def ext_fixtures():
+def ext_fixtures(only=()):
     """1D and 3D right-hand sides and the 1D Sod run of every further selection
-    (stencils, Riemann solvers, signal speeds, flux splittings)."""
-    for variant in oracle.EXT_VARIANTS:
+    (stencils, Riemann solvers, signal speeds, flux splittings), or of the
+    named ones."""
+    for variant in only or oracle.EXT_VARIANTS:
         for dim in (1, 3):
             case = small_cases()[dim]
             u = filled(case)
@@ -120,7 +122,9 @@ if __name__ == "__main__":
         sys.exit("oracle/_ref is not built: run `make -C oracle ref` with the reference sources")
     if "--ext" in sys.argv:
         os.makedirs(os.path.join(HERE, "ext"), exist_ok=True)
-        ext_fixtures()
+        # --ext [name ...]: all further selections, or only the named ones
+        ext_fixtures(tuple(a for a in sys.argv[sys.argv.index("--ext") + 1:]
+                           if not a.startswith("--")))
         sys.exit(0)
     rhs_fixtures()
     sod_fixtures()

@@ -44,3 +44,37 @@ def small_cases():
         2: cases.fourier_shock(2, dim=2, seed=3),
         3: cases.fourier_shock(1, dim=3, seed=5),
     }
+
+
+# The reference testsuite's DetailedSod error table
+# (testsuite/ReferenceValues/DetailedSod/1D_DetailedSod_errors_reference.csv):
+# (DensityL1, DensityL2, DensityLinf, PressureL1, PressureL2, PressureLinf) at
+# t = 0.2 of the single-level runs on 128 cells (4 blocks of 32, RK3) whose
+# schemes this library compiles, keyed by variant name with the CSV line.
+SOD_REFERENCE_NORMS = {
+    "fvchar": (58, (6.90089530e-07, 2.05275093e-07, 1.39620303e-07,
+                    5.95487513e-07, 2.49384854e-07, 2.28787992e-07)),
+    "fvchar_weno3_hll": (42, (1.02264424e-06, 2.58609513e-07, 1.78590815e-07,
+                              8.47004465e-07, 3.27459497e-07, 2.99812686e-07)),
+    "fs_weno3": (30, (9.64420466e-07, 2.53172573e-07, 1.78922953e-07,
+                      8.43317388e-07, 3.33634664e-07, 3.05663996e-07)),
+    "fs_llf_weno3": (22, (1.02774396e-06, 2.58481190e-07, 1.81214189e-07,
+                          9.21920404e-07, 3.41063398e-07, 3.09256115e-07)),
+    "fs_llfm_weno3": (74, (9.60803571e-07, 2.56417781e-07, 1.82571444e-07,
+                           8.29079300e-07, 3.39286859e-07, 3.11954844e-07)),
+}
+
+
+def sod_error_norms(case: cases.Case, u: np.ndarray, t: float) -> np.ndarray:
+    """The six DetailedSod norms of a 1D Sod result ``u`` (block layout) at
+    time ``t``; the weight is the reference's cell volume, h^3 in 1D too."""
+    from oracle.sod_exact import relative_error_norms, sod_exact
+    g = case.grid
+    glob = g.gather(u)
+    rho, energy, mom = glob[0, :, 0, 0], glob[1, :, 0, 0], glob[2, :, 0, 0]
+    p = (case.gamma - 1.0) * (energy - 0.5 * mom * mom / rho)
+    x = g.cell_centres()[0][:, 0, 0]
+    rho_x, _, p_x = sod_exact(x, t, case.gamma)
+    vol = g.cell_size ** 3
+    return np.concatenate([relative_error_norms(rho, rho_x, vol),
+                           relative_error_norms(p, p_x, vol)])

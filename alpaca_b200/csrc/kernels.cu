@@ -205,8 +205,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           }
           uc[m] = s;
         }
-        ch[0][n] = weno5_left(uc);
-        ch[1][n] = weno5_right(uc);
+        weno5_pair(uc, ch[0][n], ch[1][n]);
       }
       T dm[NE], dp[NE];
       to_physical<DIM, DIR, T>(r, ch[0], dm);
@@ -246,8 +245,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           }
           uc[m] = s;
         }
-        ch[0][n] = pol.left(uc);
-        ch[1][n] = pol.right(uc);
+        pol.pair(uc, ch[0][n], ch[1][n]);
       }
       T cm[NE], cp[NE];
       to_physical<DIM, DIR, T>(r, ch[0], cm);
@@ -319,7 +317,9 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           pos[m] = sp;
           neg[m] = sn;
         }
-        ch[0][n] = T(0.5) * (pol.left(pos) + pol.right(neg));
+        T wl, wr;
+        pol.two(pos, neg, wl, wr);
+        ch[0][n] = T(0.5) * (wl + wr);
       }
       to_physical<DIM, DIR, T>(r, ch[0], flux);
       if constexpr (DELTA) {
@@ -349,8 +349,10 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
         T arr[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n] - prim[2][n]);
-        pmd[n] = prim[2][n] + double(weno5_left(arr));
-        ppd[n] = prim[2][n] + double(weno5_right(arr));
+        T wl, wr;
+        weno5_pair(arr, wl, wr);
+        pmd[n] = prim[2][n] + double(wl);
+        ppd[n] = prim[2][n] + double(wr);
       }
       double cm[NE], cp[NE];
       cm[MASS] = pmd[RHO];
@@ -376,8 +378,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
         T arr[6];
 #pragma unroll
         for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n]);
-        pm[n] = pol.left(arr);
-        pp[n] = pol.right(arr);
+        pol.pair(arr, pm[n], pp[n]);
       }
       // PrimeStatesToConservatives (prime_state_handler.h:195-275)
       T cm[NE], cp[NE];

@@ -10,8 +10,10 @@
 // -fmad=false) evaluates every expression exactly as the reference writes it,
 // IEEE division included, and reproduces the reference bit for bit. The fast
 // build replaces divisions by Newton-refined reciprocals (reused where the same
-// divisor recurs) and evaluates the WENO5 weights with a single reciprocal;
-// both change results only at the rounding level.
+// divisor recurs), evaluates the WENO5 weights of a face's two reconstructions
+// with shared second differences and one reciprocal, and takes float square
+// roots from the hardware approximation; all change results only at the
+// rounding level.
 #pragma once
 
 #include <cfloat>
@@ -57,6 +59,20 @@ template <typename T> __device__ __forceinline__ T quot(T a, T b, T ib) {
 template <typename T> __device__ __forceinline__ T quot(T a, T b) {
   if constexpr (ALP_FAST) return a * inv(b);
   else return a / b;
+}
+
+// Square root: IEEE in double and in the strict build; in the fast build's
+// float arithmetic (the FP32-flux form) the PTX approximate square root, one
+// instruction with a few ulp of error against the IEEE sequence.
+__device__ __forceinline__ double tsqrt(double x) { return sqrt(x); }
+__device__ __forceinline__ float tsqrt(float x) {
+  if constexpr (ALP_FAST) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  } else {
+    return sqrtf(x);
+  }
 }
 
 template <typename T> __device__ __forceinline__ T dmin(T a, T b) { return (b < a) ? b : a; }
@@ -127,9 +143,9 @@ __device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p, T one_
   if (e.safe) {
     T const r = dmax(rho, eps_of<T>());
     T const c2 = quot(g * (p + B), r, rho > eps_of<T>() ? one_rho : inv(r));
-    return sqrt(dmax(c2, eps_of<T>()));
+    return tsqrt(dmax(c2, eps_of<T>()));
   }
-  return sqrt(quot(g * (p + B), rho, one_rho));
+  return tsqrt(quot(g * (p + B), rho, one_rho));
 }
 template <typename T> __device__ __forceinline__ T eos_speed_of_sound(Eos const &e, T rho, T p) {
   return eos_speed_of_sound<T>(e, rho, p, ALP_FAST ? inv(rho) : T(0));
@@ -180,6 +196,96 @@ template <typename T> __device__ __forceinline__ T weno5_left(T const (&a)[6]) {
 }
 template <typename T> __device__ __forceinline__ T weno5_right(T const (&a)[6]) {
   return weno5_core(a[5], a[4], a[3], a[2], a[1]);
+}
+
+// Fast-build WENO5-JS as numerator and denominator (value = num / den).
+// d1..d3 are the second differences of the three sub-stencils (v1 v2 v3),
+// (v2 v3 v4), (v3 v4 v5). The smoothness indicators come out four times
+// larger (13/3 d^2 + e^2) with eps four times larger too: every
+// (beta + eps)^2 is scaled by 16, so the normalised weights do not change.
+// Double: the weights are scaled by t1 t2 t3 (no reciprocal here); float keeps
+// one reciprocal per weight, as products of the t_k leave the float range.
+template <typename T> struct Weno5Frac { T num, den; };
+
+template <typename T>
+__device__ __forceinline__ Weno5Frac<T> weno5_frac(T v1, T v2, T v3, T v4, T v5, T d1, T d2,
+                                                   T d3) {
+  T const c = T(13.0 / 3.0);
+  T const e1 = (v1 + T(-4.0) * v2) + T(3.0) * v3;
+  T const e2 = v2 - v4;
+  T const e3 = (v5 + T(-4.0) * v4) + T(3.0) * v3;
+  T const eps = T(4.0e-6);
+  T const s1 = (c * d1) * d1 + (e1 * e1 + eps);
+  T const s2 = (c * d2) * d2 + (e2 * e2 + eps);
+  T const s3 = (c * d3) * d3 + (e3 * e3 + eps);
+  T const t1 = s1 * s1, t2 = s2 * s2, t3 = s3 * s3;
+  T const q1 = T(2.0 / 6.0) * v1 + T(-7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3;
+  T const q2 = T(-1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(2.0 / 6.0) * v4;
+  T const q3 = T(2.0 / 6.0) * v3 + T(5.0 / 6.0) * v4 + T(-1.0 / 6.0) * v5;
+  T b1, b2, b3;
+  if constexpr (sizeof(T) == 8) {
+    b1 = T(0.1) * (t2 * t3);
+    b2 = T(0.6) * (t1 * t3);
+    b3 = T(0.3) * (t1 * t2);
+  } else {
+    b1 = T(0.1) * inv(t1);
+    b2 = T(0.6) * inv(t2);
+    b3 = T(0.3) * inv(t3);
+  }
+  return {b1 * q1 + b2 * q2 + b3 * q3, b1 + b2 + b3};
+}
+
+// second difference centred on b, symmetric in its outer arguments
+template <typename T> __device__ __forceinline__ T d2c(T a, T b, T c) {
+  return (a + c) + T(-2.0) * b;
+}
+
+// num_l / den_l and num_r / den_r. Double: one reciprocal of the product of
+// the two denominators (each <= ~1e3 |v|^8, so the product stays in range
+// for |v| up to ~1e18).
+template <typename T>
+__device__ __forceinline__ void weno5_divide(Weno5Frac<T> const &l, Weno5Frac<T> const &r,
+                                             T &left, T &right) {
+  if constexpr (sizeof(T) == 8) {
+    T const rr = inv(l.den * r.den);
+    left = l.num * (r.den * rr);
+    right = r.num * (l.den * rr);
+  } else {
+    left = l.num * inv(l.den);
+    right = r.num * inv(r.den);
+  }
+}
+
+// UpwindLeft and UpwindRight of one face from the same six cells a[0..5]
+// (i-2..i+3). The fast build shares the second differences centred on a[2]
+// and a[3] between the two.
+template <typename T>
+__device__ __forceinline__ void weno5_pair(T const (&a)[6], T &left, T &right) {
+  if constexpr (!ALP_FAST) {
+    left = weno5_left(a);
+    right = weno5_right(a);
+  } else {
+    T const D1 = d2c(a[0], a[1], a[2]), D2 = d2c(a[1], a[2], a[3]);
+    T const D3 = d2c(a[2], a[3], a[4]), D4 = d2c(a[3], a[4], a[5]);
+    weno5_divide(weno5_frac(a[0], a[1], a[2], a[3], a[4], D1, D2, D3),
+                 weno5_frac(a[5], a[4], a[3], a[2], a[1], D4, D3, D2), left, right);
+  }
+}
+
+// UpwindLeft of a and UpwindRight of b (flux splitting: the positive and
+// negative split fluxes).
+template <typename T>
+__device__ __forceinline__ void weno5_two(T const (&a)[6], T const (&b)[6], T &left, T &right) {
+  if constexpr (!ALP_FAST) {
+    left = weno5_left(a);
+    right = weno5_right(b);
+  } else {
+    weno5_divide(weno5_frac(a[0], a[1], a[2], a[3], a[4], d2c(a[0], a[1], a[2]),
+                            d2c(a[1], a[2], a[3]), d2c(a[2], a[3], a[4])),
+                 weno5_frac(b[5], b[4], b[3], b[2], b[1], d2c(b[5], b[4], b[3]),
+                            d2c(b[4], b[3], b[2]), d2c(b[3], b[2], b[1])),
+                 left, right);
+  }
 }
 
 // ---- Roe eigensystem (solvers/eigendecomposition.h:181-467) --------------
@@ -245,8 +351,8 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   T const gB = T(e.gamma * e.B);
   T const psi_t = (T(t.p) + gB) * T(t.one_rho);
   T const psi_n = (T(n.p) + gB) * T(n.one_rho);
-  T const sr_t = sqrt(T(t.rho));
-  T const sr_n = sqrt(T(n.rho));
+  T const sr_t = tsqrt(T(t.rho));
+  T const sr_n = tsqrt(T(n.rho));
   T const rho_div = quot(T(1), sr_t + sr_n);
   r.rho = sr_t * sr_n;
   r.one_rho = quot(T(1), r.rho);
@@ -263,7 +369,7 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
                        T(0.5) * r.rho * (rho_div * rho_div) * tmp;
   r.cc = psi + r.gru * p_over_rho;
   r.one_cc = quot(T(1), r.cc);
-  r.c = sqrt(r.cc);
+  r.c = tsqrt(r.cc);
   r.half_cc = T(0.5) * r.one_cc;
   return r;
 }
@@ -360,11 +466,11 @@ __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T con
   constexpr int mP = MOMX + DIR;
   T const c_l = eos_speed_of_sound<T>(e, cl[MASS], pres_l, one_rl);
   T const c_r = eos_speed_of_sound<T>(e, cr[MASS], pres_r, one_rr);
-  T const srl = sqrt(cl[MASS]);
-  T const srr = sqrt(cr[MASS]);
+  T const srl = tsqrt(cl[MASS]);
+  T const srr = tsqrt(cr[MASS]);
   T const rho_div = quot(T(1), srl + srr);
   T const u_roe = ((vel_l * srl) + (vel_r * srr)) * rho_div;
-  T const c_e = sqrt(((c_l * c_l * srl) + (c_r * c_r * srr)) * rho_div +
+  T const c_e = tsqrt(((c_l * c_l * srl) + (c_r * c_r * srr)) * rho_div +
                      (T(0.5) * srl * srr * rho_div * rho_div) * (vel_r - vel_l) * (vel_r - vel_l));
   T const sls = dmin(u_roe - c_e, vel_l - c_l);
   T const srs = dmax(u_roe + c_e, vel_r + c_r);
@@ -429,12 +535,13 @@ __device__ __forceinline__ void hllc_mixed(Eos const &e, double const (&cl)[DIM 
   float const g = float(e.gamma), B = float(e.B);
   float const rl = float(cl[MASS]), rr = float(cr[MASS]);
   float const ul = float(vel_l), ur = float(vel_r);
-  float const c_l = sqrtf(g * (float(pres_l) + B) * float(one_rl));
-  float const c_r = sqrtf(g * (float(pres_r) + B) * float(one_rr));
-  float const srl = sqrtf(rl), srr = sqrtf(rr);
+  float const cc_l = g * (float(pres_l) + B) * float(one_rl);
+  float const cc_r = g * (float(pres_r) + B) * float(one_rr);
+  float const c_l = tsqrt(cc_l), c_r = tsqrt(cc_r);
+  float const srl = tsqrt(rl), srr = tsqrt(rr);
   float const rho_div = __fdividef(1.0f, srl + srr);
   float const u_roe = (ul * srl + ur * srr) * rho_div;
-  float const c_e = sqrtf((c_l * c_l * srl + c_r * c_r * srr) * rho_div +
+  float const c_e = tsqrt((cc_l * srl + cc_r * srr) * rho_div +
                           (0.5f * srl * srr * rho_div * rho_div) * (ur - ul) * (ur - ul));
   float const sls = dmin(u_roe - c_e, ul - c_l);
   float const srs = dmax(u_roe + c_e, ur + c_r);

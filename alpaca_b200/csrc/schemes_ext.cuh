@@ -248,6 +248,14 @@ struct DefaultPolicy {
   template <typename T> __device__ __forceinline__ T right(T const (&a)[6]) const {
     return weno5_right(a);
   }
+  template <typename T>
+  __device__ __forceinline__ void pair(T const (&a)[6], T &l, T &r) const {
+    weno5_pair(a, l, r);
+  }
+  template <typename T>
+  __device__ __forceinline__ void two(T const (&a)[6], T const (&b)[6], T &l, T &r) const {
+    weno5_two(a, b, l, r);
+  }
   template <int DIM, int DIR, typename T>
   __device__ __forceinline__ void riemann(Eos const &e, T const (&cl)[DIM + 2],
                                           T const (&cr)[DIM + 2], T pl, T pr, T vl, T vr,
@@ -273,6 +281,15 @@ struct ExtPolicy {
   }
   __device__ __forceinline__ double right(double const (&a)[6]) const {
     return reconstruct(o.stencil, a, true);
+  }
+  __device__ __forceinline__ void pair(double const (&a)[6], double &l, double &r) const {
+    l = left(a);
+    r = right(a);
+  }
+  __device__ __forceinline__ void two(double const (&a)[6], double const (&b)[6], double &l,
+                                      double &r) const {
+    l = left(a);
+    r = right(b);
   }
   template <int DIM, int DIR, typename T>
   __device__ __forceinline__ void riemann(Eos const &e, double const (&cl)[DIM + 2],

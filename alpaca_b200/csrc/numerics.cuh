@@ -476,6 +476,32 @@ __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T con
   T const srs = dmax(u_roe + c_e, vel_r + c_r);
   T const s_star = quot((pres_r - pres_l) + (cl[mP] * (sls - vel_l) - cr[mP] * (srs - vel_r)),
                         cl[MASS] * (sls - vel_l) - cr[MASS] * (srs - vel_r));
+  if constexpr (ALP_FAST) {
+    // The upwind star flux alone. Where the reference averages the two (S* = 0)
+    // they are equal up to rounding: F*_L - F*_R = S* (U*_L - U*_R).
+    bool const rs = s_star < T(0);
+    T const rho = rs ? cr[MASS] : cl[MASS];
+    T const mp = rs ? cr[mP] : cl[mP];
+    T const E = rs ? cr[ENERGY] : cl[ENERGY];
+    T const p = rs ? pres_r : pres_l;
+    T const v = rs ? vel_r : vel_l;
+    T const one_r = rs ? one_rr : one_rl;
+    T const s = rs ? srs : sls;
+    T const sc = rs ? dmax(srs, T(0)) : dmin(sls, T(0));
+    T const chi = quot(s - v, s - s_star);
+    T const rchi = rho * chi;
+    flux[MASS] = mp + (sc * (rchi - rho));
+    flux[mP] = ((mp * mp) * one_r + p) + (sc * (rchi * s_star - mp));
+    T const es = rchi * (E * one_r + (s_star - v) * (s_star + quot(p, rho * (sc - v))));
+    flux[ENERGY] = v * (E + p) + (sc * (es - E));
+#pragma unroll
+    for (int d = 0; d < DIM - 1; ++d) {
+      int const mm = MOMX + (d == 0 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+      T const q = rs ? cr[mm] : cl[mm];
+      flux[mm] = v * q + (sc * (chi * q - q));
+    }
+    return;
+  }
   T const sl = dmin(sls, T(0));
   T const sr = dmax(srs, T(0));
   T const chi_l = quot(sls - vel_l, sls - s_star);
@@ -549,6 +575,35 @@ __device__ __forceinline__ void hllc_mixed(Eos const &e, double const (&cl)[DIM 
   float const s_star = __fdividef(dpr + (rl * ul * (sls - ul) - rr * ur * (srs - ur)),
                                   rl * (sls - ul) - rr * (srs - ur));
   float const sl = dmin(sls, 0.0f), sr = dmax(srs, 0.0f);
+  if constexpr (ALP_FAST) {
+    // the upwind star flux alone (as in hllc())
+    bool const rs = s_star < 0.0f;
+    float const rho = rs ? rr : rl, u = rs ? ur : ul;
+    float const s = rs ? srs : sls, sc = rs ? sr : sl;
+    double const p = rs ? pres_r : pres_l, v = rs ? vel_r : vel_l;
+    double const one_r = rs ? one_rr : one_rl;
+    double const mp = rs ? cr[mP] : cl[mP], E = rs ? cr[ENERGY] : cl[ENERGY];
+    float const dchi = __fdividef(s_star - u, s - s_star);  // chi - 1
+    float dq[DIM + 2];
+    double f[DIM + 2];
+    dq[MASS] = rho * dchi;
+    dq[mP] = rho * ((s_star - u) + dchi * s_star);
+    dq[ENERGY] = float(E) * dchi + rho * (1.0f + dchi) * (s_star - u) *
+                                       (s_star + __fdividef(float(p), rho * (sc - u)));
+    f[MASS] = mp;
+    f[mP] = mp * mp * one_r + p;
+    f[ENERGY] = v * (E + p);
+#pragma unroll
+    for (int d = 0; d < DIM - 1; ++d) {
+      int const mm = MOMX + (d == 0 ? Minor<DIR>::m1 : Minor<DIR>::m2);
+      double const q = rs ? cr[mm] : cl[mm];
+      dq[mm] = dchi * float(q);
+      f[mm] = v * q;
+    }
+#pragma unroll
+    for (int n = 0; n < DIM + 2; ++n) flux[n] = f[n] + double(sc * dq[n]);
+    return;
+  }
   float const dchi_l = __fdividef(s_star - ul, sls - s_star);  // chi_l - 1
   float const dchi_r = __fdividef(s_star - ur, srs - s_star);
   float const chi_l = 1.0f + dchi_l, chi_r = 1.0f + dchi_r;

@@ -277,12 +277,13 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
             DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY], one_rho);
         double const vel = cons[m][mP] * one_rho;
         double const rho = cons[m][MASS];
-        advd[m][MASS] = rho * vel;
+        // the fast build uses rho u = m for the mass and momentum fluxes
+        advd[m][MASS] = ALP_FAST ? cons[m][mP] : rho * vel;
         advd[m][ENERGY] = (cons[m][ENERGY] + p) * vel;
 #pragma unroll
         for (int d = 0; d < DIM; ++d) {
           double const vd = cons[m][MOMX + d] * one_rho;
-          double v = rho * (vel * vd);
+          double v = ALP_FAST ? cons[m][mP] * vd : rho * (vel * vd);
           if (d == DIR) v += p;
           advd[m][MOMX + d] = v;
         }
@@ -308,14 +309,26 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
             T const uct = (DELTA ? T(cons[m][l] - cons[2][l]) : T(cons[m][l])) * L[l];
             T const act = (DELTA ? T(advd[m][l] - advd[2][l]) : T(advd[m][l])) * L[l];
-            T const tp = act + alpha * uct;
-            T const tn = act - alpha * uct;
-            sp = first ? tp : sp + tp;
-            sn = first ? tn : sn + tn;
+            if constexpr (ALP_FAST) {
+              // project state (into sp) and flux (into sn), split afterwards:
+              // L (f +/- alpha u) = L f +/- alpha L u
+              sp = first ? uct : sp + uct;
+              sn = first ? act : sn + act;
+            } else {
+              T const tp = act + alpha * uct;
+              T const tn = act - alpha * uct;
+              sp = first ? tp : sp + tp;
+              sn = first ? tn : sn + tn;
+            }
             first = false;
           }
-          pos[m] = sp;
-          neg[m] = sn;
+          if constexpr (ALP_FAST) {
+            pos[m] = sn + alpha * sp;
+            neg[m] = sn - alpha * sp;
+          } else {
+            pos[m] = sp;
+            neg[m] = sn;
+          }
         }
         T wl, wr;
         pol.two(pos, neg, wl, wr);

@@ -41,6 +41,20 @@ __device__ __forceinline__ double rcp_nr(double b) {
   return y;
 }
 
+// 1/sqrt(x) by Newton-Raphson iteration on f(y) = 1/y^2 - x
+// (y <- y + y (1 - x y^2) / 2), seeded with the PTX approximate reciprocal
+// square root; each iteration squares the relative error, two take it below
+// the rounding of the last steps (fast build only).
+__device__ __forceinline__ double rsqrt_nr(double x) {
+  double y;
+  asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  double e = fma(-x * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  e = fma(-x * y, y, 1.0);
+  y = fma(0.5 * y, e, y);
+  return y;
+}
+
 // 1/x: IEEE division in the strict build, rcp_nr (double) or the hardware
 // approximate quotient (float) in the fast build.
 __device__ __forceinline__ double inv(double x) {
@@ -351,11 +365,28 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   T const gB = T(e.gamma * e.B);
   T const psi_t = (T(t.p) + gB) * T(t.one_rho);
   T const psi_n = (T(n.p) + gB) * T(n.one_rho);
-  T const sr_t = tsqrt(T(t.rho));
-  T const sr_n = tsqrt(T(n.rho));
-  T const rho_div = quot(T(1), sr_t + sr_n);
-  r.rho = sr_t * sr_n;
-  r.one_rho = quot(T(1), r.rho);
+  // sr_k * rho_div are the Roe weights sqrt(rho_k) / (sqrt(rho_t) + sqrt(rho_n))
+  constexpr bool WEIGHTS = ALP_FAST && sizeof(T) == 8;
+  T sr_t, sr_n, rho_div;
+  if constexpr (WEIGHTS) {
+    // the weights themselves (rho_div = 1) from one reciprocal square root:
+    // mu = sqrt(rho_t / rho_n), lambda = 1 / mu, w_t = 1 / (1 + lambda),
+    // w_n = lambda w_t, Roe density rho_t lambda and its inverse mu / rho_t
+    T const ratio = n.rho * t.one_rho;
+    T const mu = rsqrt_nr(ratio);
+    T const lambda = ratio * mu;
+    sr_t = inv(T(1) + lambda);
+    sr_n = lambda * sr_t;
+    rho_div = T(1);
+    r.rho = t.rho * lambda;
+    r.one_rho = t.one_rho * mu;
+  } else {
+    sr_t = tsqrt(T(t.rho));
+    sr_n = tsqrt(T(n.rho));
+    rho_div = quot(T(1), sr_t + sr_n);
+    r.rho = sr_t * sr_n;
+    r.one_rho = quot(T(1), r.rho);
+  }
   r.up = ((T(t.up) * sr_t) + (T(n.up) * sr_n)) * rho_div;
   r.u1 = ((T(t.u1) * sr_t) + (T(n.u1) * sr_n)) * rho_div;
   r.u2 = ((T(t.u2) * sr_t) + (T(n.u2) * sr_n)) * rho_div;
@@ -365,8 +396,11 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   r.q2 = dacms<DIM>(r.up * r.up, r.u1 * r.u1, r.u2 * r.u2);
   T const dup = T(t.up) - T(n.up), du1 = T(t.u1) - T(n.u1), du2 = T(t.u2) - T(n.u2);
   T const tmp = dacms<DIM>(dup * dup, du1 * du1, du2 * du2);
-  T const p_over_rho = ((T(t.p) * T(t.one_rho)) * sr_t + (T(n.p) * T(n.one_rho)) * sr_n) * rho_div +
-                       T(0.5) * r.rho * (rho_div * rho_div) * tmp;
+  // 0.5 rho_roe rho_div^2 = 0.5 w_t w_n
+  T const jump = WEIGHTS ? T(0.5) * (sr_t * sr_n) * tmp
+                         : T(0.5) * r.rho * (rho_div * rho_div) * tmp;
+  T const p_over_rho =
+      ((T(t.p) * T(t.one_rho)) * sr_t + (T(n.p) * T(n.one_rho)) * sr_n) * rho_div + jump;
   r.cc = psi + r.gru * p_over_rho;
   r.one_cc = quot(T(1), r.cc);
   r.c = tsqrt(r.cc);
@@ -466,9 +500,19 @@ __device__ __forceinline__ void hllc(Eos const &e, T const (&cl)[DIM + 2], T con
   constexpr int mP = MOMX + DIR;
   T const c_l = eos_speed_of_sound<T>(e, cl[MASS], pres_l, one_rl);
   T const c_r = eos_speed_of_sound<T>(e, cr[MASS], pres_r, one_rr);
-  T const srl = tsqrt(cl[MASS]);
-  T const srr = tsqrt(cr[MASS]);
-  T const rho_div = quot(T(1), srl + srr);
+  T srl, srr, rho_div;
+  if constexpr (ALP_FAST && sizeof(T) == 8) {
+    // the Roe weights themselves (rho_div = 1): lambda = sqrt(rho_r / rho_l),
+    // w_l = 1 / (1 + lambda), w_r = lambda w_l
+    T const lambda = tsqrt(cr[MASS] * one_rl);
+    srl = inv(T(1) + lambda);
+    srr = lambda * srl;
+    rho_div = T(1);
+  } else {
+    srl = tsqrt(cl[MASS]);
+    srr = tsqrt(cr[MASS]);
+    rho_div = quot(T(1), srl + srr);
+  }
   T const u_roe = ((vel_l * srl) + (vel_r * srr)) * rho_div;
   T const c_e = tsqrt(((c_l * c_l * srl) + (c_r * c_r * srr)) * rho_div +
                      (T(0.5) * srl * srr * rho_div * rho_div) * (vel_r - vel_l) * (vel_r - vel_l));

@@ -212,77 +212,77 @@ template <typename T> __device__ __forceinline__ T weno5_right(T const (&a)[6]) 
   return weno5_core(a[5], a[4], a[3], a[2], a[1]);
 }
 
-// Fast-build WENO5-JS as numerator and denominator (value = num / den).
-// d1..d3 are the second differences of the three sub-stencils (v1 v2 v3),
-// (v2 v3 v4), (v3 v4 v5). The smoothness indicators come out four times
-// larger (13/3 d^2 + e^2) with eps four times larger too: every
-// (beta + eps)^2 is scaled by 16, so the normalised weights do not change.
-// Double: the weights are scaled by t1 t2 t3 (no reciprocal here); float keeps
-// one reciprocal per weight, as products of the t_k leave the float range.
+// Fast-build WENO5-JS from first differences. For a stencil v1..v5 around
+// the face of v3, with g1..g4 = v2-v1, v3-v2, v4-v3, v5-v4 and the second
+// differences d1..d3 = g2-g1, g3-g2, g4-g3, the three candidate values are
+//   q1 = v3 + (5 g2 - 2 g1) / 6, q2 = v3 + (g2 + 2 g3) / 6, q3 = v3 + (4 g3 - g4) / 6
+// and the smoothness indicators, four times larger with eps four times larger
+// (every (beta + eps)^2 scaled alike, so the weights do not change),
+//   13/3 d_k^2 + e_k^2 with e = 3 g2 - g1, g2 + g3, g4 - 3 g3.
+// The ideal weights 0.1, 0.6, 0.3 enter as 1, 6, 3. The result is
+// v3 + num / (6 den); passing the differences of the mirrored stencil without
+// their sign change (g_k' = -g) negates num and leaves den unchanged.
+// Double: alpha_k scaled by t1 t2 t3 (no reciprocal here); float keeps one
+// reciprocal per weight, as products of the t_k leave the float range.
 template <typename T> struct Weno5Frac { T num, den; };
 
 template <typename T>
-__device__ __forceinline__ Weno5Frac<T> weno5_frac(T v1, T v2, T v3, T v4, T v5, T d1, T d2,
-                                                   T d3) {
+__device__ __forceinline__ Weno5Frac<T> weno5_frac(T g1, T g2, T g3, T g4, T d1, T d2, T d3) {
   T const c = T(13.0 / 3.0);
-  T const e1 = (v1 + T(-4.0) * v2) + T(3.0) * v3;
-  T const e2 = v2 - v4;
-  T const e3 = (v5 + T(-4.0) * v4) + T(3.0) * v3;
+  T const e1 = T(3.0) * g2 - g1;
+  T const e2 = g2 + g3;
+  T const e3 = g4 + T(-3.0) * g3;
   T const eps = T(4.0e-6);
   T const s1 = (c * d1) * d1 + (e1 * e1 + eps);
   T const s2 = (c * d2) * d2 + (e2 * e2 + eps);
   T const s3 = (c * d3) * d3 + (e3 * e3 + eps);
   T const t1 = s1 * s1, t2 = s2 * s2, t3 = s3 * s3;
-  T const q1 = T(2.0 / 6.0) * v1 + T(-7.0 / 6.0) * v2 + T(11.0 / 6.0) * v3;
-  T const q2 = T(-1.0 / 6.0) * v2 + T(5.0 / 6.0) * v3 + T(2.0 / 6.0) * v4;
-  T const q3 = T(2.0 / 6.0) * v3 + T(5.0 / 6.0) * v4 + T(-1.0 / 6.0) * v5;
+  T const r1 = T(5.0) * g2 + T(-2.0) * g1;
+  T const r2 = g2 + T(2.0) * g3;
+  T const r3 = T(4.0) * g3 - g4;
   T b1, b2, b3;
   if constexpr (sizeof(T) == 8) {
-    b1 = T(0.1) * (t2 * t3);
-    b2 = T(0.6) * (t1 * t3);
-    b3 = T(0.3) * (t1 * t2);
+    b1 = t2 * t3;
+    b2 = T(6.0) * (t1 * t3);
+    b3 = T(3.0) * (t1 * t2);
   } else {
-    b1 = T(0.1) * inv(t1);
-    b2 = T(0.6) * inv(t2);
-    b3 = T(0.3) * inv(t3);
+    b1 = inv(t1);
+    b2 = T(6.0) * inv(t2);
+    b3 = T(3.0) * inv(t3);
   }
-  return {b1 * q1 + b2 * q2 + b3 * q3, b1 + b2 + b3};
+  return {b1 * r1 + b2 * r2 + b3 * r3, b1 + b2 + b3};
 }
 
-// second difference centred on b, symmetric in its outer arguments
-template <typename T> __device__ __forceinline__ T d2c(T a, T b, T c) {
-  return (a + c) + T(-2.0) * b;
-}
-
-// num_l / den_l and num_r / den_r. Double: one reciprocal of the product of
-// the two denominators (each <= ~1e3 |v|^8, so the product stays in range
-// for |v| up to ~1e18).
+// v_l + num_l / (6 den_l) and v_r - num_r / (6 den_r). Double: one reciprocal
+// of the product of the two denominators (each between ~1e-22 and ~1e7 |g|^8,
+// so the product stays in range for differences up to ~1e17).
 template <typename T>
-__device__ __forceinline__ void weno5_divide(Weno5Frac<T> const &l, Weno5Frac<T> const &r,
-                                             T &left, T &right) {
+__device__ __forceinline__ void weno5_finish(T v_l, Weno5Frac<T> const &l, T v_r,
+                                             Weno5Frac<T> const &r, T &left, T &right) {
   if constexpr (sizeof(T) == 8) {
-    T const rr = inv(l.den * r.den);
-    left = l.num * (r.den * rr);
-    right = r.num * (l.den * rr);
+    T const rr = inv((T(6.0) * l.den) * r.den);
+    left = v_l + l.num * (r.den * rr);
+    right = v_r - r.num * (l.den * rr);
   } else {
-    left = l.num * inv(l.den);
-    right = r.num * inv(r.den);
+    left = v_l + l.num * inv(T(6.0) * l.den);
+    right = v_r - r.num * inv(T(6.0) * r.den);
   }
 }
 
 // UpwindLeft and UpwindRight of one face from the same six cells a[0..5]
-// (i-2..i+3). The fast build shares the second differences centred on a[2]
-// and a[3] between the two.
+// (i-2..i+3). The fast build shares the first differences and the second
+// differences centred on a[2] and a[3] between the two.
 template <typename T>
 __device__ __forceinline__ void weno5_pair(T const (&a)[6], T &left, T &right) {
   if constexpr (!ALP_FAST) {
     left = weno5_left(a);
     right = weno5_right(a);
   } else {
-    T const D1 = d2c(a[0], a[1], a[2]), D2 = d2c(a[1], a[2], a[3]);
-    T const D3 = d2c(a[2], a[3], a[4]), D4 = d2c(a[3], a[4], a[5]);
-    weno5_divide(weno5_frac(a[0], a[1], a[2], a[3], a[4], D1, D2, D3),
-                 weno5_frac(a[5], a[4], a[3], a[2], a[1], D4, D3, D2), left, right);
+    T const G0 = a[1] - a[0], G1 = a[2] - a[1], G2 = a[3] - a[2], G3 = a[4] - a[3];
+    T const G4 = a[5] - a[4];
+    T const D1 = G1 - G0, D2 = G2 - G1, D3 = G3 - G2, D4 = G4 - G3;
+    weno5_finish(a[2], weno5_frac(G0, G1, G2, G3, D1, D2, D3), a[3],
+                 weno5_frac(G4, G3, G2, G1, D4, D3, D2), left, right);
   }
 }
 
@@ -294,11 +294,10 @@ __device__ __forceinline__ void weno5_two(T const (&a)[6], T const (&b)[6], T &l
     left = weno5_left(a);
     right = weno5_right(b);
   } else {
-    weno5_divide(weno5_frac(a[0], a[1], a[2], a[3], a[4], d2c(a[0], a[1], a[2]),
-                            d2c(a[1], a[2], a[3]), d2c(a[2], a[3], a[4])),
-                 weno5_frac(b[5], b[4], b[3], b[2], b[1], d2c(b[5], b[4], b[3]),
-                            d2c(b[4], b[3], b[2]), d2c(b[3], b[2], b[1])),
-                 left, right);
+    T const A0 = a[1] - a[0], A1 = a[2] - a[1], A2 = a[3] - a[2], A3 = a[4] - a[3];
+    T const B1 = b[2] - b[1], B2 = b[3] - b[2], B3 = b[4] - b[3], B4 = b[5] - b[4];
+    weno5_finish(a[2], weno5_frac(A0, A1, A2, A3, A1 - A0, A2 - A1, A3 - A2), b[3],
+                 weno5_frac(B4, B3, B2, B1, B4 - B3, B3 - B2, B2 - B1), left, right);
   }
 }
 

@@ -115,6 +115,31 @@ template <int DIM, typename T> __device__ __forceinline__ T dacms(T a, T b, T c)
   else return cms3(a, b, c);
 }
 
+// Sum of three squares, independent of the order of its terms as the
+// consistency-managed sum is. The fast build sorts them (the bit patterns of
+// non-negative floating-point values order like the values) and adds the two
+// smaller first: two additions and integer compares instead of seven
+// additions and four floating-point compares. The strict build and 1D/2D keep
+// DimensionAwareConsistencyManagedSum.
+template <int DIM, typename T> __device__ __forceinline__ T sum_sq(T a, T b, T c) {
+  if constexpr (!ALP_FAST || DIM < 3) {
+    return dacms<DIM>(a, b, c);
+  } else if constexpr (sizeof(T) == 8) {
+    long long const ia = __double_as_longlong(a), ib = __double_as_longlong(b);
+    long long const ic = __double_as_longlong(c);
+    long long const lo = min(ia, ib), hi = max(ia, ib);
+    long long const x0 = min(lo, ic), t = max(lo, ic);
+    long long const x1 = min(t, hi), x2 = max(t, hi);
+    return (__longlong_as_double(x0) + __longlong_as_double(x1)) + __longlong_as_double(x2);
+  } else {
+    int const ia = __float_as_int(a), ib = __float_as_int(b), ic = __float_as_int(c);
+    int const lo = min(ia, ib), hi = max(ia, ib);
+    int const x0 = min(lo, ic), t = max(lo, ic);
+    int const x1 = min(t, hi), x2 = max(t, hi);
+    return (__int_as_float(x0) + __int_as_float(x1)) + __int_as_float(x2);
+  }
+}
+
 // ---- stiffened gas (generic_stiffened_gas.h:40-102, stiffened_gas.cpp:62-149,
 //      stiffened_gas_safe.cpp:61-146) --------------------------------------
 
@@ -131,11 +156,11 @@ __device__ __forceinline__ double eos_pressure(Eos const &e, double mass, double
     double const m = dmax(mass, DBL_EPSILON);
     double const p =
         -e.gamma * e.B +
-        (e.gamma - 1.0) * (energy - quot(0.5 * dacms<DIM>(mx * mx, my * my, mz * mz), m,
+        (e.gamma - 1.0) * (energy - quot(0.5 * sum_sq<DIM>(mx * mx, my * my, mz * mz), m,
                                          mass > DBL_EPSILON ? one_mass : inv(m)));
     return dmax(p, -e.B + DBL_EPSILON);
   }
-  double const q = 0.5 * dacms<DIM>(mx * mx, my * my, mz * mz);
+  double const q = 0.5 * sum_sq<DIM>(mx * mx, my * my, mz * mz);
   return -e.gamma * e.B + (e.gamma - 1.0) * (energy - quot(q, mass, one_mass));
 }
 template <int DIM>
@@ -147,7 +172,7 @@ __device__ __forceinline__ double eos_pressure(Eos const &e, double mass, double
 template <int DIM, typename T>
 __device__ __forceinline__ T eos_energy(Eos const &e, T rho, T u, T v, T w, T p) {
   T const g = T(e.gamma), B = T(e.B);
-  return quot(p + g * B, g - T(1)) + (T(0.5) * dacms<DIM>(u * u, v * v, w * w) * rho);
+  return quot(p + g * B, g - T(1)) + (T(0.5) * sum_sq<DIM>(u * u, v * v, w * w) * rho);
 }
 
 // one_rho = inv(rho) (unused by the strict build)
@@ -392,9 +417,9 @@ __device__ __forceinline__ Roe<T> roe_average(Eos const &e, CellPrims<DIM, DIR> 
   T const psi = ((psi_t * sr_t) + (psi_n * sr_n)) * rho_div;
   r.H = (T(t.H) * sr_t + T(n.H) * sr_n) * rho_div;
   r.gru = T(e.gamma - 1.0);
-  r.q2 = dacms<DIM>(r.up * r.up, r.u1 * r.u1, r.u2 * r.u2);
+  r.q2 = sum_sq<DIM>(r.up * r.up, r.u1 * r.u1, r.u2 * r.u2);
   T const dup = T(t.up) - T(n.up), du1 = T(t.u1) - T(n.u1), du2 = T(t.u2) - T(n.u2);
-  T const tmp = dacms<DIM>(dup * dup, du1 * du1, du2 * du2);
+  T const tmp = sum_sq<DIM>(dup * dup, du1 * du1, du2 * du2);
   // 0.5 rho_roe rho_div^2 = 0.5 w_t w_n
   T const jump = WEIGHTS ? T(0.5) * (sr_t * sr_n) * tmp
                          : T(0.5) * r.rho * (rho_div * rho_div) * tmp;

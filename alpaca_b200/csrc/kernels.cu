@@ -65,14 +65,13 @@ template <int DIM, int DIR> struct FaceMap {
   }
 };
 
-// Minimum resident CTAs per SM for the 128-thread face kernels: caps the
-// registers so that FV kernels keep 16-20 warps per SM without spilling
-// (FV characteristic: 126 registers at 4 CTAs); flux splitting keeps its
-// registers (its 6-cell flux and state stencils are live together).
-// Minimum resident 128-thread CTAs per SM of the face kernels (register caps
-// 256 / 128 / 96 at 1-2 / 4 / 5); compile-time tunable.
+// Minimum resident 128-thread CTAs per SM of the face kernels, which caps
+// their registers (168 / 128 / 102 at 3 / 4 / 5); compile-time tunable.
+// Measured on the FP64 128^3 step: FV char 4 CTAs 1.60 ms vs 3: 1.71, 5: 1.66;
+// FV prim 5: 1.37 vs 4: 1.46, 6: 1.37; flux splitting 3: 1.91 vs 1-2: 2.23
+// (at 4 it spills ~0.7 KB per thread).
 #ifndef ALP_FS_ROE_CTAS
-#define ALP_FS_ROE_CTAS 1
+#define ALP_FS_ROE_CTAS 3
 #endif
 #ifndef ALP_FV_CHAR_CTAS
 #define ALP_FV_CHAR_CTAS 4

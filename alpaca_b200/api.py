@@ -156,6 +156,23 @@ class Engine:
         self.nb[cid.value] = (nb, (nb, self.ne) + block_shape(self.dim))
         return cid.value
 
+    def add_case_expr(self, program: "IcProgram", nblocks, cell_size: float,
+                      material: N.Material, periodic=(0, 0, 0), cfl: float = 0.6,
+                      t_end: float = 1e300, max_steps: int = 0, t0: float = 0.0,
+                      origin=(0.0, 0.0, 0.0), units: N.Units | None = None) -> int:
+        """Case whose initial condition is a compiled expression program,
+        evaluated on the device over a regular block grid."""
+        nbl = (C.c_int * 3)(*(list(nblocks) + [1, 1, 1])[:3])
+        per = (C.c_int * 3)(*(list(periodic) + [0, 0, 0])[:3])
+        org = (C.c_double * 3)(*(list(origin) + [0.0, 0.0, 0.0])[:3])
+        cid = C.c_int()
+        self._check(self.lib.alp_engine_add_case_expr(
+            self.h, C.byref(material), cell_size, cfl, t0, t_end, max_steps, nbl, per, org,
+            C.byref(units) if units is not None else None, program.h, C.byref(cid)))
+        nb = nbl[0] * nbl[1] * nbl[2]
+        self.nb[cid.value] = (nb, (nb, self.ne) + block_shape(self.dim))
+        return cid.value
+
     def remove_case(self, cid: int):
         self._check(self.lib.alp_engine_remove_case(self.h, cid))
         self.nb.pop(cid, None)
@@ -314,3 +331,52 @@ def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: i
     results = [dict(arrival_s=x.arrival_s, admitted_s=x.admitted_s, finished_s=x.finished_s, t=x.t,
                     steps=x.steps, status=x.status) for x in res]
     return results, mk.value, (outs if keep_results else None)
+
+
+class IcProgram:
+    """An initial condition given as expression statements (alp_ic_program_*),
+    compiled once on the host; see include/alpaca_b200.h for the language."""
+
+    def __init__(self, text: str, strict: bool = False):
+        self.lib = N.lib(strict)
+        self.strict = strict
+        h = C.c_void_p()
+        N.check(self.lib.alp_ic_program_create(text.encode(), C.byref(h)), strict)
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.alp_ic_program_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        n, st, nv = C.c_int(), C.c_int(), C.c_int()
+        N.check(self.lib.alp_ic_program_info(self.h, C.byref(n), C.byref(st), C.byref(nv)),
+                self.strict)
+        return {"instructions": n.value, "max_stack": st.value, "variables": nv.value}
+
+    def listing(self) -> list[str]:
+        size = 64 * (self.info()["instructions"] + 1)
+        buf = C.create_string_buffer(size)
+        w = C.c_int()
+        N.check(self.lib.alp_ic_program_listing(self.h, buf, size, C.byref(w)), self.strict)
+        return buf.value.decode().splitlines()
+
+    def evaluate(self, origins, dim: int, cell_size: float, units: N.Units | None = None,
+                 stream=None):
+        """Prime states [nb, dim + 2, 16^dim] (non-dimensional) of nodes whose
+        origins are the rows of the device tensor origins [nb, 3]."""
+        import torch
+        nb = origins.shape[0]
+        cells = 16 ** dim
+        out = torch.empty((nb, dim + 2, cells), dtype=torch.float64, device=origins.device)
+        N.check(self.lib.alp_ic_evaluate(self.h, dim, nb, _ptr(origins.contiguous()), cell_size,
+                                         C.byref(units) if units is not None else None,
+                                         _ptr(out), _stream(stream)), self.strict)
+        return out

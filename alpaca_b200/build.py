@@ -13,7 +13,7 @@ PROBE_LIB = os.path.join(HERE, "libalpaca_b200_probe.so")
 # its own, as in the reference's x86-64 build. Tests use it to show that the
 # CUDA arithmetic follows the reference's operation order bit for bit.
 STRICT_LIB = os.path.join(HERE, "libalpaca_b200_strict.so")
-SOURCES = ["kernels.cu", "capi.cu", "server.cu", "levels.cu", "static_scratch.cu"]
+SOURCES = ["kernels.cu", "capi.cu", "server.cu", "levels.cu", "static_scratch.cu", "ic_expr.cu"]
 PROBE_SOURCES = ["probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # only the alp_* C ABI is exported (exports.map)

@@ -103,6 +103,11 @@ class Material(C.Structure):
 IC_QUADRANTS, IC_BLAST = 1, 2
 
 
+class Units(C.Structure):
+    """alp_units: UnitHandler references (density, velocity, length)."""
+    _fields_ = [("density", C.c_double), ("velocity", C.c_double), ("length", C.c_double)]
+
+
 class Request(C.Structure):
     """alp_request: one served case (device-evaluated initial condition)."""
     _fields_ = [("dim", C.c_int), ("nblocks", C.c_int * 3), ("periodic", C.c_int * 3),
@@ -150,6 +155,14 @@ _SIGS = {
                                       C.c_double, C.c_int, C.c_int, _I, _D, _I]),
     "alp_engine_add_case_ic": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int, _I, _I, C.c_int, _D, C.c_int, _I]),
+    "alp_ic_program_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
+    "alp_ic_program_destroy": (None, [_V]),
+    "alp_ic_program_info": (C.c_int, [_V, _I, _I, _I]),
+    "alp_ic_program_listing": (C.c_int, [_V, C.c_char_p, C.c_int, _I]),
+    "alp_ic_evaluate": (C.c_int, [_V, C.c_int, C.c_int, _V, C.c_double, C.POINTER(Units), _V, _S]),
+    "alp_engine_add_case_expr": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double,
+                                           C.c_double, C.c_double, C.c_int, _I, _I, _D,
+                                           C.POINTER(Units), _V, _I]),
     "alp_serve": (C.c_int, [C.POINTER(ServerConfig), C.POINTER(Request), C.c_int, C.POINTER(Result),
                             _D]),
     "alp_engine_remove_case": (C.c_int, [_V, C.c_int]),

@@ -225,6 +225,60 @@ int alp_engine_add_case_ic(alp_engine *e, const alp_material *mat, double cell_s
                            const int *periodic, int ic_type, const double *ic_params,
                            int n_params, int *case_id);
 
+/* ---- initial conditions as expressions -------------------------------------
+ * Replaces PrimeStateInitializer (initial_condition/prime_state_initializer.h,
+ * GetInitialPrimeStates at prime_state_initializer.cpp:34-85) and the exprtk
+ * UserExpression it evaluates (user_expression.h): a material's initial
+ * condition as the statements of the reference's input files, e.g.
+ *     if (x < 0.5) { density := 1.0; velocityX := 0.0; pressure := 1.0; }
+ *     else { density := 0.125; velocityX := 0.0; pressure := 0.1; }
+ * compiled once on the host and evaluated per cell on the device. The program
+ * reads x, y, z (the cell centre in the units of the expression) and assigns
+ * density, velocityX, velocityY, velocityZ, pressure (0 when not assigned).
+ * The language is the exprtk subset the reference's inputs use: statements
+ * ":=" (also written ": ="), "+=" ... "%=", "var", "if (c) S else S", blocks;
+ * expressions with ?:, if(c, a, b), and/or/not (& | !), comparisons, + - * / %
+ * ^, implicit multiplication after a number or ')', the usual one- and
+ * two-argument functions, variadic min/max, pi; comments // # and block. */
+typedef struct alp_ic_program alp_ic_program;
+
+/* UnitHandler references (unit_handler.cpp:33-56): values are divided by
+ * density, velocity and density * velocity^2 (pressure); cell centres are in
+ * units of length. A null pointer means 1, 1, 1. */
+typedef struct {
+  double density, velocity, length;
+} alp_units;
+
+/* Compiles an initial-condition program (host only). ALP_ERR_INVALID, with
+ * the position and the cause in alp_last_error, for a syntax error, an unknown
+ * symbol or function, an assignment to a name that is neither a prime state
+ * nor declared with var, or nesting deeper than 32 values; the reference's
+ * UserExpression throws in those cases. */
+int alp_ic_program_create(const char *text, alp_ic_program **out);
+void alp_ic_program_destroy(alp_ic_program *p);
+/* Instructions, largest stack depth and variable slots of a compiled program. */
+int alp_ic_program_info(const alp_ic_program *p, int *n_instructions, int *max_stack,
+                        int *n_variables);
+/* The compiled program as text, one instruction per line ("CONST 0.5",
+ * "LOAD x", "JZ 12", ...), NUL-terminated; *written = its length. */
+int alp_ic_program_listing(const alp_ic_program *p, char *buf, int size, int *written);
+
+/* GetInitialPrimeStates for nb nodes of 16^dim cells: node b's cell (i, j, k)
+ * has centre d_origins[3b + d] + (index_d + 1/2) cell_size * units->length;
+ * the non-dimensional prime states rho, u_1 .. u_dim, p go to
+ * d_prims[b][dim + 2][16^dim] (cells in C order). Device pointers, stream
+ * order; the program is copied to the device on its first use. */
+int alp_ic_evaluate(const alp_ic_program *p, int dim, int nb, const double *d_origins,
+                    double cell_size, const alp_units *units, double *d_prims, void *stream);
+
+/* alp_engine_add_case_ic with the initial condition given by a program on the
+ * regular grid of nblocks blocks whose first cell has its corner at origin
+ * (units of length; null: 0), cell_size non-dimensional. */
+int alp_engine_add_case_expr(alp_engine *e, const alp_material *mat, double cell_size,
+                             double cfl, double t0, double t_end, int max_steps,
+                             const int *nblocks, const int *periodic, const double *origin,
+                             const alp_units *units, const alp_ic_program *prog, int *case_id);
+
 /* Removes a case and frees its blocks. */
 int alp_engine_remove_case(alp_engine *e, int case_id);
 

@@ -307,6 +307,12 @@ def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: i
             q.ic_params[k] = v
         q.n_params = len(r.params)
         q.arrival_s = r.arrival_s
+        if r.ic_type == N.IC_PROGRAM:
+            q.program = r.program.h
+            for d in range(3):
+                q.origin[d] = r.origin[d]
+            if r.units is not None:
+                q.units = N.Units(*r.units)
         if keep_results:
             nb = r.nblocks[0] * r.nblocks[1] * r.nblocks[2]
             buf = np.zeros((nb, r.dim + 2) + block_shape(r.dim))

@@ -603,7 +603,7 @@ struct ExprLaunch {
   int nby, nbz;           // nodes along y and z of the regular grid
   double h;               // dimensional cell size
   double rho_ref, vel_ref, p_ref;
-  double *prims;  // [nb][DIM+2][IC^d] non-dimensional rho, u.., p
+  double *prims;  // [nb][DIM+2][IC^d] non-dimensional rho, p, u.. (the reference's order)
   double *U;      // or the engine's block pool, blocks first.. first+nb-1
   int first;
   double gamma, B;
@@ -683,10 +683,11 @@ __global__ void expr_ic_kernel(ExprLaunch L) {
   for (int d = 0; d < DIM; ++d) vel[d] = var[SLOT_PRIME + 1 + d] / L.vel_ref;
   double const p = var[SLOT_PRIME + 4] / L.p_ref;
   if (L.prims) {
+    // PrimeState order Density, Pressure, VelocityX.. (block_definitions/field_details.h:201-212)
     double *out = L.prims + (size_t)b * (DIM + 2) * CELLS;
     out[c] = rho;
-    for (int d = 0; d < DIM; ++d) out[(1 + d) * CELLS + c] = vel[d];
-    out[(DIM + 1) * CELLS + c] = p;
+    out[CELLS + c] = p;
+    for (int d = 0; d < DIM; ++d) out[(2 + d) * CELLS + c] = vel[d];
   } else {
     // PrimeStatesToConservatives (prime_states/prime_state_handler.h:195-275)
     Eos const eos{L.gamma, L.B, 0};

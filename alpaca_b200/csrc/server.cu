@@ -104,9 +104,15 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
       alp_request const &r = reqs[*it];
       DimPool &p = pool[r.dim];
       int cid = -1;
-      int const rc = alp_engine_add_case_ic(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
-                                            r.max_steps, r.nblocks, r.periodic, r.ic_type,
-                                            r.ic_params, r.n_params, &cid);
+      bool const unit = r.units.density == 0.0 && r.units.velocity == 0.0 && r.units.length == 0.0;
+      int const rc =
+          r.ic_type == ALP_IC_PROGRAM
+              ? alp_engine_add_case_expr(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
+                                         r.max_steps, r.nblocks, r.periodic, r.origin,
+                                         unit ? nullptr : &r.units, r.program, &cid)
+              : alp_engine_add_case_ic(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
+                                       r.max_steps, r.nblocks, r.periodic, r.ic_type,
+                                       r.ic_params, r.n_params, &cid);
       if (rc == ALP_OK) {
         p.req_of_case[cid] = *it;
         p.held[cid] = 0;

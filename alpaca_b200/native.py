@@ -100,7 +100,7 @@ class Material(C.Structure):
         return cls(gamma, B, int(safe))
 
 
-IC_QUADRANTS, IC_BLAST = 1, 2
+IC_QUADRANTS, IC_BLAST, IC_PROGRAM = 1, 2, 3
 
 
 class Units(C.Structure):
@@ -114,7 +114,8 @@ class Request(C.Structure):
                 ("cell_size", C.c_double), ("material", Material), ("cfl", C.c_double),
                 ("t_end", C.c_double), ("max_steps", C.c_int), ("ic_type", C.c_int),
                 ("ic_params", C.c_double * 24), ("n_params", C.c_int), ("arrival_s", C.c_double),
-                ("h_result", C.POINTER(C.c_double))]
+                ("h_result", C.POINTER(C.c_double)), ("program", C.c_void_p),
+                ("origin", C.c_double * 3), ("units", Units)]
 
 
 class Result(C.Structure):

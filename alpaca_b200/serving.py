@@ -52,6 +52,9 @@ class Request:
     t_end: float = 1e300
     periodic: tuple = (0, 0, 0)
     kind: str = field(default="")
+    program: object = None  # api.IcProgram for ic_type IC_PROGRAM
+    origin: tuple = (0.0, 0.0, 0.0)
+    units: tuple | None = None  # (density, velocity, length) references
 
     @property
     def blocks(self) -> int:

@@ -265,8 +265,10 @@ int alp_ic_program_listing(const alp_ic_program *p, char *buf, int size, int *wr
 
 /* GetInitialPrimeStates for nb nodes of 16^dim cells: node b's cell (i, j, k)
  * has centre d_origins[3b + d] + (index_d + 1/2) cell_size * units->length;
- * the non-dimensional prime states rho, u_1 .. u_dim, p go to
- * d_prims[b][dim + 2][16^dim] (cells in C order). Device pointers, stream
+ * the non-dimensional prime states go to d_prims[b][dim + 2][16^dim] in the
+ * reference's prime-state order Density, Pressure, VelocityX[, Y[, Z]]
+ * (block_definitions/field_details.h:201-212), cells in C order, as
+ * GetInitialPrimeStates fills its prime_state_buffer. Device pointers, stream
  * order; the program is copied to the device on its first use. */
 int alp_ic_evaluate(const alp_ic_program *p, int dim, int nb, const double *d_origins,
                     double cell_size, const alp_units *units, double *d_prims, void *stream);
@@ -364,9 +366,12 @@ alp_stream_t alp_levels_stream(alp_levels *m);
 /* ---- serving: continuous batching of independent cases ------------------ */
 
 /* One request: a case on a regular block grid with a device-evaluated initial
- * condition (see alp_engine_add_case_ic), arriving arrival_s seconds after
- * alp_serve starts. h_result, when not null, receives the final state
- * (reference layout, halos filled) before the case leaves the pool. */
+ * condition (see alp_engine_add_case_ic; ic_type ALP_IC_PROGRAM: the program,
+ * origin and units of alp_engine_add_case_expr, ic_params unused, units all 0
+ * meaning 1), arriving arrival_s seconds after alp_serve starts. h_result,
+ * when not null, receives the final state (reference layout, halos filled)
+ * before the case leaves the pool. */
+enum { ALP_IC_PROGRAM = 3 };
 typedef struct {
   int dim;
   int nblocks[3];
@@ -381,6 +386,9 @@ typedef struct {
   int n_params;
   double arrival_s;
   double *h_result;
+  const alp_ic_program *program;
+  double origin[3];
+  alp_units units;
 } alp_request;
 
 /* Wall-clock times are seconds after the start of alp_serve. */

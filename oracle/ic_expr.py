@@ -417,7 +417,8 @@ def check_syntax(text: str, inputs=("x", "y", "z"), outputs=PRIMES) -> None:
 def initial_prime_states(text: str, dim: int, origins, cell_size: float,
                          units=(1.0, 1.0, 1.0)) -> np.ndarray:
     """GetInitialPrimeStates for nodes of 16^dim cells with the given origins
-    [nb, 3] and dimensional cell size: non-dimensional (rho, u_1..u_dim, p)
+    [nb, 3] and dimensional cell size: non-dimensional prime states in the
+    reference's order (Density, Pressure, VelocityX.., field_details.h:201-212)
     as [nb, dim + 2, 16^dim], cells in C order."""
     rho_ref, vel_ref, _ = units
     origins = np.asarray(origins, dtype=np.float64).reshape(-1, 3)
@@ -429,9 +430,9 @@ def initial_prime_states(text: str, dim: int, origins, cell_size: float,
                for d, c in enumerate("xyz")}
         v = evaluate(text, xyz)
         out[b, 0] = v["density"] / rho_ref
+        out[b, 1] = v["pressure"] / (rho_ref * vel_ref * vel_ref)
         for d in range(dim):
-            out[b, 1 + d] = v[("velocityX", "velocityY", "velocityZ")[d]] / vel_ref
-        out[b, dim + 1] = v["pressure"] / (rho_ref * vel_ref * vel_ref)
+            out[b, 2 + d] = v[("velocityX", "velocityY", "velocityZ")[d]] / vel_ref
     return out
 
 

@@ -77,7 +77,7 @@ def test_engine_expression_case_matches_array_case(cuda):
     prims = X.initial_prime_states(text, 3, np.array(g.coords) * 16 * g.cell_size, g.cell_size)
     u = np.zeros((g.nb, 5) + cases.block_shape(3))
     I = cases.interior(3)
-    rho, vel, p = prims[:, 0], [prims[:, 1], prims[:, 2], prims[:, 3]], prims[:, 4]
+    rho, p, vel = prims[:, 0], prims[:, 1], [prims[:, 2], prims[:, 3], prims[:, 4]]
     cons = cases.primes_to_conservatives(3, rho, p, vel, 1.4)
     u[I] = np.moveaxis(np.asarray(cons), 0, 1).reshape((g.nb, 5, 16, 16, 16))
     mat = N.Material.make(1.4)

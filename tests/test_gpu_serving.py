@@ -88,6 +88,40 @@ def test_serving_mix_equals_alone(cuda):
     assert any(a1 < f0 for (a0, f0), (a1, _) in zip(mspans, mspans[1:]))
 
 
+def test_serving_program_requests(cuda):
+    """Requests whose initial condition is an expression program: batched with
+    fixed-form requests they get the bits they get alone and the bits of the
+    engine's own expression case."""
+    prog2 = api.IcProgram("""if ((x < 0.5) & (y < 0.5)) { density := 1; pressure := 1; }
+        else { density := 0.125 + 0.1 * sin(2 * pi * y); pressure := 0.1; velocityX := 0.2; }""")
+    prog3 = api.IcProgram("""var r := sqrt((x - 0.25)^2 + (y - 0.25)^2 + (z - 0.25)^2);
+        density := r < 0.1 ? 2.0 : 1.0; pressure := r < 0.1 ? 10.0 : 1.0;""")
+    reqs = [
+        serving.Request(2, (4, 4, 1), 1.0 / 64, 1.4, 0.0, N.IC_PROGRAM, [], 20, program=prog2),
+        serving.Request(3, (2, 2, 2), 1.0 / 64, 1.4, 0.0, N.IC_PROGRAM, [], 12, arrival_s=0.01,
+                        program=prog3, units=(1.0, 1.0, 2.0)),
+    ] + small_stream()[:3]
+    budget = 2 << 30
+    mix, _, states_mix = api.serve(reqs, budget, keep_results=True)
+    alone, _, states_alone = api.serve(reqs, budget, one_at_a_time=True, keep_results=True)
+    for i, r in enumerate(reqs):
+        assert mix[i]["status"] == 0 and alone[i]["status"] == 0
+        I = cases.interior(r.dim)
+        assert np.array_equal(states_mix[i][I], states_alone[i][I]), i
+    for i, (prog, units) in enumerate(((prog2, None), (prog3, N.Units(1.0, 1.0, 2.0)))):
+        r = reqs[i]
+        eng = api.Engine(r.dim, "fvchar", capacity_blocks=r.blocks, max_cases=1)
+        cid = eng.add_case_expr(prog, r.nblocks, r.cell_size, N.Material.make(1.4),
+                                max_steps=r.max_steps, units=units)
+        eng.step(r.max_steps)
+        u = eng.get(cid)[0]
+        eng.close()
+        I = cases.interior(r.dim)
+        assert np.array_equal(u[I], states_mix[i][I]), i
+    prog2.close()
+    prog3.close()
+
+
 def test_shortest_first_finishes_short_cases_first_with_the_same_bits(cuda):
     """Shortest remaining work first: a small case that arrives with large ones
     finishes before them, and every case keeps the bits it gets alone."""

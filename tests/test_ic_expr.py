@@ -107,7 +107,7 @@ def _initializer_program(material: int, factors, dim: int):
     """CreateMaterialInitialConditions (test_prime_state_initializer.cpp:80-98):
     prime state p of material m := (m + 1)(p + 1)(f0 x + f1 y + f2 z), numbers
     written as std::to_string writes them."""
-    names = ["density", "velocityX", "velocityY", "velocityZ"][: dim + 1] + ["pressure"]
+    names = ["density", "pressure", "velocityX", "velocityY", "velocityZ"][: dim + 2]
     s = ""
     for p, n in enumerate(names):
         k = float((material + 1) * (p + 1))
@@ -136,8 +136,8 @@ def test_units_scale_the_prime_states():
     velocity / u_ref, pressure / (rho_ref u_ref^2); coordinates in length units."""
     prog = "density := 1000; velocityX := 20; pressure := 1e5 + x;"
     a = X.initial_prime_states(prog, 1, np.zeros((1, 3)), 0.5, units=(1000.0, 10.0, 2.0))
-    assert np.allclose(a[0, 0], 1.0) and np.allclose(a[0, 1], 2.0)
-    assert np.allclose(a[0, 2], (1e5 + (np.arange(16) + 0.5) * 0.5) / 1e5)
+    assert np.allclose(a[0, 0], 1.0) and np.allclose(a[0, 2], 2.0)
+    assert np.allclose(a[0, 1], (1e5 + (np.arange(16) + 0.5) * 0.5) / 1e5)
 
 
 # ---- the library's compiler against the oracle -------------------------------

@@ -470,9 +470,13 @@ __global__ void __launch_bounds__(128, FaceOccupancy<SCHEME, T>::min_ctas)
 face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
                      BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
                      CaseState const *__restrict__ cases, double *__restrict__ F,
-                     long long stride, long long dstride) {
-  int const t = blockIdx.y * blockDim.x + threadIdx.x;
-  int const item = blockIdx.x;
+                     long long stride, long long dstride, int chunks) {
+  // grid (items x chunks, 1, dir): an item's chunks are consecutive, so the
+  // CTAs resident at any time share few blocks' stencils (a few MB of L2
+  // instead of one stencil plane of every item in the launch)
+  int const chunk = (int)(blockIdx.x % chunks);
+  int const item = (int)(blockIdx.x / chunks);
+  int const t = chunk * blockDim.x + threadIdx.x;
   int const slot = work[item];
   BlockMeta const bm = meta[slot];
   if (!(cases[bm.case_id].dt > 0.0)) return;
@@ -1169,15 +1173,19 @@ cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *
     }
     return cudaGetLastError();
   }
+  // items x chunks < 2^31 for up to 2^31 / 68 items (64-thread chunks)
+  int const chunks = (count + threads - 1) / threads;
+  if ((long long)L.nwork * chunks > 0x7fffffffLL) return cudaErrorInvalidValue;
+  dim3 const g2((unsigned)(L.nwork * chunks), 1, DIM);
   switch (L.scheme) {
     case FV_CHAR:
-      face_flux_all_kernel<DIM, FV_CHAR, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FV_CHAR, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
       break;
     case FV_PRIM:
-      face_flux_all_kernel<DIM, FV_PRIM, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FV_PRIM, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
       break;
     case FS_ROE:
-      face_flux_all_kernel<DIM, FS_ROE, T><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride);
+      face_flux_all_kernel<DIM, FS_ROE, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
       break;
     default:
       return cudaErrorInvalidValue;

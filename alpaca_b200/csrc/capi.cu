@@ -62,12 +62,10 @@ int scheme_id(alp_scheme const *s, int *id, int *precision) {
     else return fail(ALP_ERR_INVALID, "FiniteVolume needs Primitive or Characteristic reconstruction");
   } else if (s->convective_term_solver == ALP_FLUX_SPLITTING) {
     int const fs = s->flux_splitting;
-    if (fs == FSP_GLF)
+    if (fs != FSP_ROE && fs != FSP_LLF && fs != FSP_GLF && fs != FSP_ROE_M && fs != FSP_LLF_M)
       return fail(ALP_ERR_INVALID,
-                  "FluxSplitting::GlobalLaxFriedrichs (a domain-wide eigenvalue reduction) is not compiled");
-    if (fs != FSP_ROE && fs != FSP_LLF && fs != FSP_ROE_M && fs != FSP_LLF_M)
-      return fail(ALP_ERR_INVALID,
-                  "FluxSplitting must be Roe, LocalLaxFriedrichs, Roe_M or LocalLaxFriedrichs_M");
+                  "FluxSplitting must be Roe, LocalLaxFriedrichs, GlobalLaxFriedrichs, Roe_M or "
+                  "LocalLaxFriedrichs_M");
     *id = FS_ROE;
   } else {
     return fail(ALP_ERR_INVALID, "unknown convective_term_solver");
@@ -109,6 +107,20 @@ BlockMeta meta_of(alp_material const *m, double cell_size, int case_id) {
 
 }  // namespace alp
 
+namespace {
+// GlobalLaxFriedrichs in the stateless calls: the maxima over the call's blocks
+// (all leaves handed to one call, as ComputeRightHandSide takes them over all
+// leaves) in the library's slot, before the fluxes.
+int stateless_glf(Launch &L) {
+  if (L.scheme != FS_ROE || L.opt.splitting != FSP_GLF || L.nwork <= 0) return ALP_OK;
+  unsigned long long *slot = glf_stateless_slot();
+  if (!slot) return fail(ALP_ERR_CUDA, "GlobalLaxFriedrichs: no device slot");
+  ALP_CUDA(launch_glf_maxima(L, slot, 1));
+  L.glf = slot;
+  return ALP_OK;
+}
+}  // namespace
+
 extern "C" {
 
 const char *alp_version(void) { return "alpaca_b200 0.1 (sm_100a)"; }
@@ -139,6 +151,7 @@ int alp_convective_fluxes(int dim, const alp_scheme *scheme, const alp_material 
   Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
            meta_of(mat, cell_size, 0), (cudaStream_t)stream};
   L.opt = scheme_options(scheme);
+  if (int rc = stateless_glf(L)) return rc;
   long long const stride = (long long)(dim + 2) * faces_of(dim);
   for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F[d], stride, true));
   return ALP_OK;
@@ -164,6 +177,7 @@ int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
   Launch L{dim, sid, prec, const_cast<double *>(d_blocks), nullptr, nb, nullptr,
            meta_of(mat, cell_size, 0), (cudaStream_t)stream};
   L.opt = scheme_options(scheme);
+  if (int rc = stateless_glf(L)) return rc;
   long long const dstride = (long long)(dim + 2) * faces_of(dim);
   long long const stride = dstride * dim;
   for (int d = 0; d < dim; ++d) ALP_CUDA(launch_face_flux(L, d, F + d * dstride, stride, false));
@@ -393,6 +407,7 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
   grab((void **)&e->cases, sizeof(CaseState) * max_cases);
+  grab((void **)&e->glf, sizeof(unsigned long long) * 4 * max_cases);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking);
   for (cudaEvent_t &ev : e->ev_batch)

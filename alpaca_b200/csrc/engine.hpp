@@ -57,6 +57,7 @@ struct alp_engine {
   int *nbr26 = nullptr;
   int *work = nullptr;
   CaseState *cases = nullptr;
+  unsigned long long *glf = nullptr;  // GlobalLaxFriedrichs wave speeds [case][4]
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
   bool use_graph = true;
@@ -88,9 +89,15 @@ struct alp_engine {
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
     double *in[3] = {U, UB, UC};
     double *out[3] = {UB, UC, trial ? UB : U};
+    bool const glf_due = scheme == alp::FS_ROE && opt.splitting == alp::FSP_GLF;
     for (int s = 0; s < 3; ++s) {
       Launch Ls = L;
       Ls.U = in[s];
+      if (glf_due) {
+        // the case's maxima over its blocks before this stage's fluxes
+        ALP_CUDA(launch_glf_maxima(Ls, glf, max_cases));
+        Ls.glf = glf;
+      }
       if (path == 0) {
         ALP_CUDA(alp::launch_pencil_stage(Ls, U, out[s], R, nbr26, cases, s));
       } else if (path == 2) {
@@ -189,6 +196,7 @@ struct alp_engine {
     cudaFree(nbr26);
     cudaFree(work);
     cudaFree(cases);
+    cudaFree(glf);
     for (cudaEvent_t &ev : ev_batch)
       if (ev) cudaEventDestroy(ev);
     if (ev_join) cudaEventDestroy(ev_join);

@@ -7,6 +7,8 @@
 #include <cfloat>
 #include <cstdio>
 
+#include <mutex>
+
 #include "kernels.cuh"
 
 // The FP32-flux branches return early, which leaves the shared FP64 tail
@@ -495,19 +497,27 @@ face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
   }
 }
 
+// The policy of one block: the GlobalLaxFriedrichs wave speeds of its case.
+__device__ __forceinline__ ExtPolicy block_policy(ExtPolicy pol, BlockMeta const &bm,
+                                                  unsigned long long const *glf) {
+  if (glf && pol.o.splitting == FSP_GLF)
+    for (int k = 0; k < 3; ++k) pol.glf[k] = __longlong_as_double(glf[4 * bm.case_id + k]);
+  return pol;
+}
+
 // The same two kernels for the run-time selected schemes (ExtPolicy, FP64).
 template <int DIM, int DIR, int SCHEME, bool ACCUM>
 __global__ void __launch_bounds__(128)
 face_flux_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
                      BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
-                     long long stride, ExtPolicy pol) {
+                     long long stride, ExtPolicy pol, unsigned long long const *__restrict__ glf) {
   int const t = blockIdx.y * blockDim.x + threadIdx.x;
   if (t >= FaceMap<DIM, DIR>::COUNT) return;
   int const item = blockIdx.x;
   int const slot = slot_of(work, item);
   BlockMeta const bm = meta ? meta[slot] : def;
   face_flux<DIM, DIR, SCHEME, double, ACCUM, false, ExtPolicy>(U, nullptr, slot, item, t, bm, F,
-                                                               stride, pol);
+                                                               stride, block_policy(pol, bm, glf));
 }
 
 template <int DIM, int SCHEME>
@@ -515,12 +525,14 @@ __global__ void __launch_bounds__(128)
 face_flux_all_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
                          BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
                          CaseState const *__restrict__ cases, double *__restrict__ F,
-                         long long stride, long long dstride, ExtPolicy pol) {
+                         long long stride, long long dstride, ExtPolicy pol0,
+                         unsigned long long const *__restrict__ glf) {
   int const t = blockIdx.y * blockDim.x + threadIdx.x;
   int const item = blockIdx.x;
   int const slot = work[item];
   BlockMeta const bm = meta[slot];
   if (!(cases[bm.case_id].dt > 0.0)) return;
+  ExtPolicy const pol = block_policy(pol0, bm, glf);
   int const dir = blockIdx.z;
   if (dir == 0) {
     if (t < FaceMap<DIM, 0>::COUNT)
@@ -1050,15 +1062,15 @@ cudaError_t face_flux_dir(Launch const &L, double *F, long long stride, int thre
     switch (L.scheme) {
       case FV_CHAR:
         face_flux_ext_kernel<DIM, DIR, FV_CHAR, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
         break;
       case FV_PRIM:
         face_flux_ext_kernel<DIM, DIR, FV_PRIM, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
         break;
       case FS_ROE:
         face_flux_ext_kernel<DIM, DIR, FS_ROE, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol);
+            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
         break;
       default:
         return cudaErrorInvalidValue;
@@ -1160,13 +1172,13 @@ cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *
     ExtPolicy const pol{L.opt};
     switch (L.scheme) {
       case FV_CHAR:
-        face_flux_all_ext_kernel<DIM, FV_CHAR><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        face_flux_all_ext_kernel<DIM, FV_CHAR><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
         break;
       case FV_PRIM:
-        face_flux_all_ext_kernel<DIM, FV_PRIM><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        face_flux_all_ext_kernel<DIM, FV_PRIM><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
         break;
       case FS_ROE:
-        face_flux_all_ext_kernel<DIM, FS_ROE><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol);
+        face_flux_all_ext_kernel<DIM, FS_ROE><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
         break;
       default:
         return cudaErrorInvalidValue;
@@ -1357,6 +1369,80 @@ cudaError_t launch_step_commit(CaseState *cases, int n, cudaStream_t stream) {
   if (n <= 0) return cudaSuccess;
   step_commit_kernel<<<(n + 127) / 128, 128, 0, stream>>>(cases, n);
   return cudaGetLastError();
+}
+
+namespace {
+__device__ unsigned long long g_glf_stateless[4];
+
+__device__ __forceinline__ double max_keep(double m, double v) { return (m < v) ? v : m; }
+
+// One CTA per block: the block's maxima of |u - c|, |u|, |u + c| (x velocity,
+// interior cells with positive density; std::max keeps the running maximum
+// against a NaN as the reference's does), then one atomicMax per value on
+// its case's slot (bit patterns of non-negative doubles order like the values).
+template <int DIM>
+__global__ void __launch_bounds__(256)
+glf_maxima_kernel(double const *__restrict__ U, int const *__restrict__ work,
+                  BlockMeta const *__restrict__ meta, BlockMeta def,
+                  unsigned long long *__restrict__ glf) {
+  using G = Geo<DIM>;
+  int const item = blockIdx.x;
+  int const slot = slot_of(work, item);
+  BlockMeta const bm = meta ? meta[slot] : def;
+  Eos const eos{bm.gamma, bm.B, bm.safe};
+  double const *ub = U + (size_t)slot * G::BLOCK_DOUBLES;
+  double m[3] = {0.0, 0.0, 0.0};
+  for (int c = threadIdx.x; c < G::INTERIOR; c += blockDim.x) {
+    int const k = c % G::ICZ, j = (c / G::ICZ) % G::ICY, i = c / (G::ICZ * G::ICY);
+    int const x = ((i + HS) * G::TCY + (j + (DIM > 1 ? HS : 0))) * G::TCZ + (k + (DIM > 2 ? HS : 0));
+    double cons[G::NE];
+#pragma unroll
+    for (int f = 0; f < G::NE; ++f) cons[f] = ub[f * G::CELLS + x];
+    auto const pr = cell_prims<DIM, 0>(eos, cons);
+    if (!(pr.rho > 0.0)) continue;
+    double const cs = eos_speed_of_sound<double>(eos, pr.rho, pr.p, pr.one_rho);
+    m[0] = max_keep(m[0], fabs(pr.up - cs));
+    m[1] = max_keep(m[1], fabs(pr.up));
+    m[2] = max_keep(m[2], fabs(pr.up + cs));
+  }
+  __shared__ double red[3][8];
+#pragma unroll
+  for (int q = 0; q < 3; ++q) {
+    double v = m[q];
+    for (int o = 16; o > 0; o >>= 1) v = max_keep(v, __shfl_down_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    double v = 0.0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v = max_keep(v, red[threadIdx.x][w]);
+    atomicMax(&glf[4 * bm.case_id + threadIdx.x], (unsigned long long)__double_as_longlong(v));
+  }
+}
+}  // namespace
+
+cudaError_t launch_glf_maxima(Launch const &L, unsigned long long *glf, int ncases) {
+  if (ncases <= 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(glf, 0, sizeof(unsigned long long) * 4 * ncases, L.stream);
+  if (e != cudaSuccess || L.nwork <= 0) return e;
+  switch (L.dim) {
+    case 1: glf_maxima_kernel<1><<<L.nwork, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, glf); break;
+    case 2: glf_maxima_kernel<2><<<L.nwork, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, glf); break;
+    default: glf_maxima_kernel<3><<<L.nwork, 256, 0, L.stream>>>(L.U, L.work, L.meta, L.def, glf); break;
+  }
+  return cudaGetLastError();
+}
+
+// The address is looked up once per device (the lookup may load the module).
+unsigned long long *glf_stateless_slot() {
+  static std::mutex mu;
+  static void *addr[64] = {};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev] && cudaGetSymbolAddress(&addr[dev], g_glf_stateless) != cudaSuccess)
+    addr[dev] = nullptr;
+  return static_cast<unsigned long long *>(addr[dev]);
 }
 
 }  // namespace alp

@@ -46,7 +46,19 @@ struct Launch {
   BlockMeta def;
   cudaStream_t stream;
   SchemeOptions opt = SchemeOptions();  // non-default: FP64 run-time dispatch, face kernels only
+  // GlobalLaxFriedrichs wave speeds |u-c|, |u|, |u+c| per case, as the bit
+  // patterns of non-negative doubles, 4 words per case (launch_glf_maxima)
+  unsigned long long const *glf = nullptr;
 };
+
+// GlobalLaxFriedrichs: zeroes glf[0 .. 4 ncases) and sets, per case, the
+// largest |u - c|, |u|, |u + c| of the x velocity over the interior cells of
+// the launch's blocks with positive density (ComputeMaxEigenvaluesOnBlock,
+// eigendecomposition.cpp:46-110, maxima over blocks as
+// modular_algorithm_assembler.cpp:957-985).
+cudaError_t launch_glf_maxima(Launch const &L, unsigned long long *glf, int ncases);
+// The library's slot for the stateless calls (one case, id 0).
+unsigned long long *glf_stateless_slot();
 
 // Face fluxes of direction `dir` for every work item into
 // F[item * flux_item_stride + field * FACES + face] (reference flux-array

@@ -640,6 +640,10 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
   int sid, prec;
   if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  if (sid == FS_ROE && scheme->flux_splitting == FSP_GLF)
+    return fail(ALP_ERR_INVALID,
+                "GlobalLaxFriedrichs takes its maxima over the levels integrated in each micro "
+                "step; multi-level cases do not support it");
   if (int rc = check_material(mat)) return rc;
   if (!n0 || !h_level || !h_coord || !h_blocks || nleaf <= 0)
     return fail(ALP_ERR_INVALID, "empty or null tree description");

@@ -276,6 +276,7 @@ struct DefaultPolicy {
 
 struct ExtPolicy {
   SchemeOptions o;
+  double glf[3] = {0.0, 0.0, 0.0};  // GlobalLaxFriedrichs wave speeds of the block's case
   __device__ __forceinline__ double left(double const (&a)[6]) const {
     return reconstruct(o.stencil, a, false);
   }
@@ -320,6 +321,11 @@ struct ExtPolicy {
       e0 = dmax(fabs(pt.up - ct), fabs(pn.up - cn));
       elin = dmax(fabs(pt.up), fabs(pn.up));
       e1 = dmax(fabs(pt.up + ct), fabs(pn.up + cn));
+    } else if (o.splitting == FSP_GLF) {
+      // the x maxima in every direction (eigendecomposition.h:457-460)
+      e0 = glf[0];
+      elin = glf[1];
+      e1 = glf[2];
     } else {
       e0 = fabs(r.up - r.c);
       e1 = fabs(r.up + r.c);

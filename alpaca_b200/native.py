@@ -46,6 +46,9 @@ EXT_SCHEMES = {
                                "flux_splitting": FLUX_SPLITTING_LLF}),
     "fs_llfm_weno3": ("fsroe", {"reconstruction_stencil": STENCIL_WENO3,
                                 "flux_splitting": FLUX_SPLITTING_LLF_M}),
+    "fs_glf": ("fsroe", {"flux_splitting": FLUX_SPLITTING_GLF}),
+    "fs_glf_weno5z": ("fsroe", {"reconstruction_stencil": STENCIL_WENO5Z,
+                                "flux_splitting": FLUX_SPLITTING_GLF}),
 }
 RK3 = 1
 FP64, FP32_FLUX = 0, 1

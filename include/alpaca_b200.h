@@ -50,12 +50,17 @@ enum {
  * Supported: FiniteVolume + {Primitive, Characteristic} reconstruction with
  * the stencils FirstOrder, WENO3, WENO5, WENO5Z or TENO5, the Riemann solvers
  * Hllc, Hllc_LM or Hll and the signal speeds Einfeldt, Davis, Toro or
- * Arithmetic; FluxSplitting with Roe, LocalLaxFriedrichs, Roe_M or
- * LocalLaxFriedrichs_M and the same stencils; RK3. WENO5 + Hllc + Einfeldt
- * and WENO5 + Roe are the compiled fast path (FP64 and FP32_FLUX, pencil
- * sweeps); the other choices run through one FP64 face kernel that selects
- * them at run time. GlobalLaxFriedrichs (a domain-wide eigenvalue reduction)
- * is rejected.
+ * Arithmetic; FluxSplitting with Roe, LocalLaxFriedrichs, GlobalLaxFriedrichs,
+ * Roe_M or LocalLaxFriedrichs_M and the same stencils; RK3. WENO5 + Hllc +
+ * Einfeldt and WENO5 + Roe are the compiled fast path (FP64 and FP32_FLUX,
+ * pencil sweeps); the other choices run through one FP64 face kernel that
+ * selects them at run time. GlobalLaxFriedrichs takes the largest |u - c|,
+ * |u|, |u + c| of the x velocity over all interior cells before every flux
+ * evaluation and uses them in every direction, as the reference does
+ * (modular_algorithm_assembler.cpp:957-985, eigendecomposition.h:457-460):
+ * over the case in the engine, over the blocks of the call in the stateless
+ * calls (which then share one library slot per device, so GLF calls that may
+ * overlap must be ordered); multi-level cases reject it.
  * precision: ALP_FP64 (all arithmetic in double) or ALP_FP32_FLUX
  * (reconstruction, smoothness indicators and Riemann fluxes in float; state,
  * RK accumulation, pressure recovery and dt in double). */

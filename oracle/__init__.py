@@ -43,7 +43,7 @@ VARIANTS = {
 WENO5, WENO5Z, TENO5, WENO3, FIRST_ORDER = 4, 7, 11, 1, 0
 HLLC, HLLC_LM, HLL = 0, 1, 2
 EINFELDT, DAVIS, TORO, ARITHMETIC = 0, 1, 2, 3
-ROE, LLF, ROE_M, LLF_M = 0, 1, 3, 4
+ROE, LLF, GLF, ROE_M, LLF_M = 0, 1, 2, 3, 4
 DEFAULT_OPTIONS = (WENO5, HLLC, EINFELDT, ROE)
 EXT_VARIANTS = {
     "fvchar_weno5z": ("fvchar", (WENO5Z, HLLC, EINFELDT, ROE)),
@@ -66,6 +66,9 @@ EXT_VARIANTS = {
     "fs_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, ROE)),
     "fs_llf_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, LLF)),
     "fs_llfm_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, LLF_M)),
+    # global Lax-Friedrichs (maxima over all blocks of the call / case)
+    "fs_glf": ("fsroe", (WENO5, HLLC, EINFELDT, GLF)),
+    "fs_glf_weno5z": ("fsroe", (WENO5Z, HLLC, EINFELDT, GLF)),
 }
 
 

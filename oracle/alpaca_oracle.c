@@ -212,9 +212,10 @@ static inline double weno5_right(const double *a) { return weno5(a, 1, -1); }
 enum { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11 };
 enum { RS_HLLC = 0, RS_HLLC_LM = 1, RS_HLL = 2 };
 enum { SS_EINFELDT = 0, SS_DAVIS = 1, SS_TORO = 2, SS_ARITHMETIC = 3 };
-enum { FSP_ROE = 0, FSP_LLF = 1, FSP_ROE_M = 3, FSP_LLF_M = 4 };
+enum { FSP_ROE = 0, FSP_LLF = 1, FSP_GLF = 2, FSP_ROE_M = 3, FSP_LLF_M = 4 };
 static int g_stencil = ST_WENO5, g_riemann = RS_HLLC, g_signal = SS_EINFELDT,
            g_splitting = FSP_ROE;
+static double g_glf[3]; /* global Lax-Friedrichs wave speeds (glf_maxima) */
 
 /* WENO5-Z (weno5_z.h:88-150) */
 static double weno5z(const double *a, int offset, int sign) {
@@ -476,6 +477,11 @@ static void roe_eigen(const Geom *g, const Eos *e, int dir, const double *u,
     e0 = fabs(up - cm);
     elin = fabs(up);
     e1 = fabs(up + cm);
+  } else if (g_splitting == FSP_GLF) {
+    /* the x maxima in every direction (eigendecomposition.h:457-460) */
+    e0 = g_glf[0];
+    elin = g_glf[1];
+    e1 = g_glf[2];
   } else if (g_splitting == FSP_LLF || g_splitting == FSP_LLF_M) {
     double ct = eos_speed_of_sound(e, rho_t, p_t);
     double cn = eos_speed_of_sound(e, rho_n, p_n);
@@ -654,6 +660,39 @@ static void work_free(Work *w) {
 }
 
 /* block-wide prime states (prime_state_handler.h:141-152) */
+/* Global Lax-Friedrichs wave speeds: the largest |u - c|, |u|, |u + c| of the
+ * x velocity over the interior cells of all blocks whose density is positive
+ * (EigenDecomposition::ComputeMaxEigenvaluesOnBlock, eigendecomposition.cpp:
+ * 46-110; maxima across blocks before the fluxes of every stage in
+ * ComputeRightHandSide, modular_algorithm_assembler.cpp:957-985). Only the x
+ * maxima are kept (g_glf): the flux uses them in every direction. */
+
+static void glf_maxima(const Geom *g, const Eos *e, const double *u, int nb) {
+  double m[3] = {0.0, 0.0, 0.0};
+  double c[MAXNE], p[MAXNE];
+  for (int b = 0; b < nb; ++b) {
+    const double *ub = u + (long)b * g->ne * g->cells;
+    for (int i = fic(g, 0); i <= lic(g, 0); ++i)
+      for (int j = fic(g, 1); j <= lic(g, 1); ++j)
+        for (int k = fic(g, 2); k <= lic(g, 2); ++k) {
+          long const x = cidx(g, i, j, k);
+          for (int f = 0; f < g->ne; ++f) c[f] = ub[f * g->cells + x];
+          cons_to_prim(e, c, p);
+          if (p[RHO] <= 0.0) continue;
+          double const cs = eos_speed_of_sound(e, p[RHO], p[PRES]);
+          double const vx = p[VELX];
+          m[0] = dmax(m[0], fabs(vx - cs));
+          m[1] = dmax(m[1], fabs(vx));
+          m[2] = dmax(m[2], fabs(vx + cs));
+        }
+  }
+  for (int q = 0; q < 3; ++q) g_glf[q] = m[q];
+}
+
+static int glf_selected(int solver) {
+  return solver == ORACLE_FLUX_SPLITTING && g_splitting == FSP_GLF;
+}
+
 static void block_primes(const Geom *g, const Eos *e, const double *u, double *p) {
   double c[MAXNE], q[MAXNE];
   for (long x = 0; x < g->cells; ++x) {
@@ -944,6 +983,7 @@ int oracle_space_rhs(int dim, int solver, int recon, const double *u, int nb,
   Geom g = make_geom(dim);
   Eos e = {dim, gamma, B, safe};
   RhsCtx c = {&g, &e, solver, recon, u, cell_size, fx, fy, fz, rhs};
+  if (glf_selected(solver)) glf_maxima(&g, &e, u, nb);
   parallel_blocks(&g, nb, nthreads, rhs_task, &c);
   return 0;
 }
@@ -1173,6 +1213,7 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr
     if (dt_log) dt_log[steps] = dt;
     for (int stage = 0; stage < 3; ++stage) {
       StageCtx c = {&g, &e, solver, recon, stage, cur, u0, other, cell_size, dt};
+      if (glf_selected(solver)) glf_maxima(&g, &e, cur, nb);
       parallel_blocks(&g, nb, nthreads, stage_task, &c);
       halo_update6(&g, other, nb, nbr);
       double *tmp = cur;
@@ -1592,6 +1633,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                       int safe, double cfl, double t_end, int max_macro, int nthreads,
                       double *t_io, int *macro_done, double *dt_log) {
   if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
+  if (glf_selected(solver)) return 4; /* global maxima over the levels due: not restated */
   Geom g = make_geom(dim);
   Eos e = {dim, gamma, B, safe};
   Tree tr;
@@ -1711,8 +1753,8 @@ int oracle_set_options(int stencil, int riemann, int signal, int splitting) {
     return 1;
   if (riemann < RS_HLLC || riemann > RS_HLL) return 1;
   if (signal < SS_EINFELDT || signal > SS_ARITHMETIC) return 1;
-  if (splitting != FSP_ROE && splitting != FSP_LLF && splitting != FSP_ROE_M &&
-      splitting != FSP_LLF_M)
+  if (splitting != FSP_ROE && splitting != FSP_LLF && splitting != FSP_GLF &&
+      splitting != FSP_ROE_M && splitting != FSP_LLF_M)
     return 1;
   g_stencil = stencil;
   g_riemann = riemann;

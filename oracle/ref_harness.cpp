@@ -165,6 +165,35 @@ void SpaceRhs(Context const &ctx, std::pair<MaterialName const, Block> &mb,
   }
 }
 
+// Global Lax-Friedrichs: ComputeRightHandSide (modular_algorithm_assembler.cpp:
+// 957-985) takes the maxima of EigenDecomposition::ComputeMaxEigenvaluesOnBlock
+// over all blocks (then over MPI ranks, one rank here) and hands them to
+// SetGlobalEigenvalues before the fluxes of each stage. block(b) returns the
+// (material, block) pair of block b with its prime states up to date.
+template <class BlockOf>
+void SetGlobalLaxFriedrichs(Context const &ctx, int nb, BlockOf block) {
+  if constexpr (convective_term_solver == ConvectiveTermSolvers::FluxSplitting &&
+                FluxSplittingSettings::flux_splitting_scheme ==
+                    FluxSplitting::GlobalLaxFriedrichs) {
+    double max_eigenvalues[DTI(CC::DIM())][MF::ANOE()];
+    for (unsigned d = 0; d < DTI(CC::DIM()); ++d)
+      for (unsigned e = 0; e < MF::ANOE(); ++e)
+        max_eigenvalues[d][e] = 0.0;
+    double current[DTI(CC::DIM())][MF::ANOE()];
+    for (int b = 0; b < nb; ++b) {
+      ctx.eigen->ComputeMaxEigenvaluesOnBlock(block(b), current);
+      for (unsigned d = 0; d < DTI(CC::DIM()); ++d)
+        for (unsigned e = 0; e < MF::ANOE(); ++e)
+          max_eigenvalues[d][e] = std::max(max_eigenvalues[d][e], current[d][e]);
+    }
+    ctx.eigen->SetGlobalEigenvalues(max_eigenvalues);
+  } else {
+    (void)ctx;
+    (void)nb;
+    (void)block;
+  }
+}
+
 struct ScratchBuffers {
   FluxArray fx, fy, fz;
   ForceArray vf;
@@ -354,6 +383,19 @@ int ref_space_rhs(double const *u, int nb, double gamma, double B, int safe,
   Context ctx(gamma, B, safe);
   if (nthreads < 1)
     nthreads = 1;
+  {
+    // prime states of every block first (global Lax-Friedrichs maxima)
+    auto mb = std::make_unique<std::pair<MaterialName const, Block>>(
+        std::piecewise_construct, std::forward_as_tuple(kMat),
+        std::forward_as_tuple());
+    SetGlobalLaxFriedrichs(ctx, nb, [&](int b) -> std::pair<MaterialName const, Block> const & {
+      Block &blk = mb->second;
+      LoadAverages(blk, u + std::size_t(b) * NE * CELLS);
+      ctx.primes->ConvertConservativesToPrimeStates(kMat, blk.GetAverageBuffer(),
+                                                    blk.GetPrimeStateBuffer());
+      return *mb;
+    });
+  }
   ParallelFor(nthreads, [&](int t) {
     auto mb = std::make_unique<std::pair<MaterialName const, Block>>(
         std::piecewise_construct, std::forward_as_tuple(kMat),
@@ -429,8 +471,11 @@ int ref_run(double *u, int nb, int const *nbr, double gamma, double B, int safe,
       dt_log[steps] = dt;
     rk.AppendMicroTimestep(dt);
     for (unsigned stage = 0; stage < rk.NumberOfStages(); ++stage) {
-      // ComputeRightHandSide (:954-1008): FillInitialBuffer, UpdateFluxes,
-      // PrepareBufferForIntegration.
+      // ComputeRightHandSide (:954-1008): global Lax-Friedrichs maxima,
+      // FillInitialBuffer, UpdateFluxes, PrepareBufferForIntegration.
+      SetGlobalLaxFriedrichs(ctx, nb, [&](int b) -> std::pair<MaterialName const, Block> const & {
+        return *nodes[b]->GetPhases().begin();
+      });
       ParallelFor(nthreads, [&](int th) {
         Scratch s;
         for (int b = th; b < nb; b += nthreads) {

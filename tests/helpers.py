@@ -62,6 +62,8 @@ SOD_REFERENCE_NORMS = {
                           9.21920404e-07, 3.41063398e-07, 3.09256115e-07)),
     "fs_llfm_weno3": (74, (9.60803571e-07, 2.56417781e-07, 1.82571444e-07,
                            8.29079300e-07, 3.39286859e-07, 3.11954844e-07)),
+    "fs_glf_weno5z": (70, (6.11467178e-07, 1.86248795e-07, 1.19883696e-07,
+                           5.70962203e-07, 2.28544959e-07, 2.03433021e-07)),
 }
 
 

@@ -109,9 +109,9 @@ def test_request_stream_is_seeded_and_in_range():
 
 
 def test_extension_selections_validated_on_the_host():
-    """Unknown values, GlobalLaxFriedrichs and FP32 with a further selection are
-    rejected before any device work; the further selections themselves pass
-    validation (the call then only fails on the null buffers)."""
+    """Unknown values and FP32 with a further selection are rejected before any
+    device work; the further selections themselves pass validation (the call
+    then only fails on the null buffers)."""
     lib = N.lib()
     mat = N.Material.make(1.4)
     ws = C.c_void_p(0)
@@ -123,7 +123,7 @@ def test_extension_selections_validated_on_the_host():
     s.reconstruction_stencil = 5  # WENO5AER: not compiled
     assert rhs(s) == N.ALP_ERR_INVALID and b"WENO5Z" in lib.alp_last_error()
     s = N.Scheme.make("fsroe")
-    s.flux_splitting = N.FLUX_SPLITTING_GLF
+    s.flux_splitting = 5  # no such splitting
     assert rhs(s) == N.ALP_ERR_INVALID and b"GlobalLaxFriedrichs" in lib.alp_last_error()
     s = N.Scheme.make("fvchar_teno5", N.FP32_FLUX)
     assert rhs(s) == N.ALP_ERR_INVALID and b"FP32_FLUX" in lib.alp_last_error()

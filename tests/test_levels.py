@@ -122,3 +122,20 @@ def test_invalid_trees_are_rejected(what):
         rc, msg = _create(1, (2,), [0, 0], [[0, 0, 0], [2, 0, 0]])
     assert rc == N.ALP_ERR_INVALID, (what, rc, msg)
     assert msg
+
+
+def test_global_lax_friedrichs_is_rejected_for_levels():
+    """The reference takes the GLF maxima over the levels integrated in each
+    micro step; the multi-level engine does not restate that and says so."""
+    lib = N.lib()
+    sch = N.Scheme.make("fs_glf")
+    mat = N.Material.make(1.4)
+    level = np.zeros(2, dtype=np.int32)
+    coord = np.array([[0, 0, 0], [1, 0, 0]], dtype=np.int32)
+    n0 = np.array([2, 1, 1], dtype=np.int32)
+    u = np.zeros((2, 3) + cases.block_shape(1))
+    h = C.c_void_p()
+    rc = lib.alp_levels_create(1, C.byref(sch), C.byref(mat), n0.ctypes.data_as(N._I), 1 / 32,
+                               2, level.ctypes.data_as(N._I), coord.ctypes.data_as(N._I), 0.6,
+                               0.0, 1.0, 1, u.ctypes.data_as(N._D), C.byref(h))
+    assert rc == N.ALP_ERR_INVALID and b"GlobalLaxFriedrichs" in lib.alp_last_error()

@@ -47,8 +47,8 @@ int scheme_id(alp_scheme const *s, int *id, int *precision) {
   if (st != ST_WENO5 && st != ST_WENO5Z && st != ST_TENO5 && st != ST_WENO3 && st != ST_FIRST_ORDER)
     return fail(ALP_ERR_INVALID,
                 "compiled ReconstructionStencils: FirstOrder, WENO3, WENO5, WENO5Z, TENO5");
-  if (s->time_integrator != ALP_RK3)
-    return fail(ALP_ERR_INVALID, "only TimeIntegrators::RK3 is compiled");
+  if (s->time_integrator != ALP_RK3 && s->time_integrator != ALP_RK2)
+    return fail(ALP_ERR_INVALID, "TimeIntegrators must be RK2 or RK3");
   if (s->precision != ALP_FP64 && s->precision != ALP_FP32_FLUX)
     return fail(ALP_ERR_INVALID, "precision must be ALP_FP64 or ALP_FP32_FLUX");
   *precision = s->precision;
@@ -267,7 +267,8 @@ std::vector<int> regular_grid_neighbours(int dim, int const n[3], int const peri
       if (o == 13) continue;
       int const off[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
       int q[3] = {c[0], c[1], c[2]};
-      bool ok = true;
+      bool ok = true, wall = false;
+      int const nonzero = (off[0] != 0) + (off[1] != 0) + (off[2] != 0);
       for (int d = 0; d < 3 && ok; ++d) {
         if (off[d] == 0) continue;
         if (d >= dim) {
@@ -276,13 +277,18 @@ std::vector<int> regular_grid_neighbours(int dim, int const n[3], int const peri
         }
         q[d] += off[d];
         if (q[d] < 0 || q[d] >= n[d]) {
-          if (periodic[d])
-            q[d] = (q[d] + n[d]) % n[d];
-          else
+          if (periodic[d] == ALP_BOUNDARY_SYMMETRY) {
+            wall = nonzero == 1;  // face slots only (edges and corners stay -1)
             ok = false;
+          } else if (periodic[d]) {
+            q[d] = (q[d] + n[d]) % n[d];
+          } else {
+            ok = false;
+          }
         }
       }
       if (ok) nbr[(size_t)b * 26 + slot] = (q[0] * n[1] + q[1]) * n[2] + q[2];
+      else if (wall) nbr[(size_t)b * 26 + slot] = -2;
       ++slot;
     }
   }
@@ -294,8 +300,13 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
                          int *case_id, int *first_out) {
   if (int rc = check_material(mat)) return rc;
   if (!(cell_size > 0.0) || !(cfl > 0.0)) return fail(ALP_ERR_INVALID, "bad cell size / cfl");
-  for (size_t i = 0; i < (size_t)nb * 26; ++i)
-    if (h_nbr26[i] < -1 || h_nbr26[i] >= nb) return fail(ALP_ERR_INVALID, "neighbour out of range");
+  for (size_t i = 0; i < (size_t)nb * 26; ++i) {
+    // -2 (symmetry wall) only in the six face slots 4, 10, 12, 13, 15, 21
+    int const s = (int)(i % 26);
+    bool const face = s == 4 || s == 10 || s == 12 || s == 13 || s == 15 || s == 21;
+    if (h_nbr26[i] < (face ? -2 : -1) || h_nbr26[i] >= nb)
+      return fail(ALP_ERR_INVALID, "neighbour out of range");
+  }
   int cid = -1;
   for (int c = 0; c < e->max_cases; ++c)
     if (!e->case_rec[c].live) {
@@ -310,7 +321,7 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
     e->h_meta[first + b] = meta_of(mat, cell_size, cid);
     for (int s = 0; s < 26; ++s) {
       int const n = h_nbr26[(size_t)b * 26 + s];
-      e->h_nbr26[(size_t)(first + b) * 26 + s] = n < 0 ? -1 : first + n;
+      e->h_nbr26[(size_t)(first + b) * 26 + s] = n < 0 ? n : first + n;  // -1 / -2 kept
     }
   }
   ALP_CUDA(cudaMemcpyAsync(e->meta + first, e->h_meta.data() + first, sizeof(BlockMeta) * nb,
@@ -381,6 +392,7 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   e->scheme = sid;
   e->precision = prec;
   e->opt = scheme_options(scheme);
+  e->rk2 = scheme->time_integrator == ALP_RK2;
   e->capacity = capacity_blocks;
   e->max_cases = max_cases;
   e->ne = dim + 2;
@@ -588,7 +600,7 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
   int const ncand = 4;
   auto allowed = [&](int i) {
     if (i != 2) return true;
-    if (!e->opt.is_default()) return false;  // pencils: default schemes only
+    if (!e->opt.is_default() || e->rk2) return false;  // pencils: default schemes, RK3
 #ifdef ALP_STRICT
     return false;  // the pencil path changes the flux summation order
 #else
@@ -643,8 +655,9 @@ int alp_engine_set_path(alp_engine *e, int candidate) {
 #ifdef ALP_STRICT
   if (candidate == 2) return fail(ALP_ERR_INVALID, "the strict build steps the face-flux path");
 #endif
-  if (candidate == 2 && !e->opt.is_default())
-    return fail(ALP_ERR_INVALID, "pencil sweeps are compiled for WENO5 + HLLC/Einfeldt and Roe only");
+  if (candidate == 2 && (!e->opt.is_default() || e->rk2))
+    return fail(ALP_ERR_INVALID,
+                "pencil sweeps are compiled for WENO5 + HLLC/Einfeldt and Roe with RK3 only");
   e->path = paths[candidate];
   e->face_threads = threads[candidate];
   e->graph_dirty = true;
@@ -662,7 +675,7 @@ int alp_engine_launches_per_step(alp_engine *e) {
   // signal speed, dt, 3 stages x (one pencil sweep per direction, or face
   // fluxes + stage update, per batch on the overlapped path), commit
   int const batches = e->path == 2 ? std::min(alp_engine::kMaxBatches, std::max(1, e->nwork / 64)) : 1;
-  return 2 + 3 * (e->path == 0 ? e->dim : 2 * batches) + 1;
+  return 2 + (e->rk2 ? 2 : 3) * (e->path == 0 ? e->dim : 2 * batches) + 1;
 }
 
 }  // extern "C"

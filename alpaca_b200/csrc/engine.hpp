@@ -41,6 +41,7 @@ using alp::launch_step_commit;
 struct alp_engine {
   int dim = 3, scheme = FV_CHAR, precision = FP64;
   alp::SchemeOptions opt;  // run-time selected schemes (face-flux path only)
+  int rk2 = 0;             // 1: TVD-RK2 (2 stages, face-flux paths), 0: SSP-RK3
   int capacity = 0, max_cases = 0;
   int ne = 5, cells = 0, faces = 0;
   double *U = nullptr, *UB = nullptr, *UC = nullptr;
@@ -87,10 +88,13 @@ struct alp_engine {
     L.opt = opt;
     ALP_CUDA(launch_signal_speed(L, cases, nullptr));
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream));
+    // RK3: A -> B, (B, A) -> C, (C, A) -> A; RK2: A -> B, (B, A) -> A (trial: C)
     double *in[3] = {U, UB, UC};
     double *out[3] = {UB, UC, trial ? UB : U};
+    if (rk2) out[1] = trial ? UC : U;
+    int const nst = rk2 ? 2 : 3, s0 = rk2 ? 3 : 0;
     bool const glf_due = scheme == alp::FS_ROE && opt.splitting == alp::FSP_GLF;
-    for (int s = 0; s < 3; ++s) {
+    for (int s = 0; s < nst; ++s) {
       Launch Ls = L;
       Ls.U = in[s];
       if (glf_due) {
@@ -101,10 +105,10 @@ struct alp_engine {
       if (path == 0) {
         ALP_CUDA(alp::launch_pencil_stage(Ls, U, out[s], R, nbr26, cases, s));
       } else if (path == 2) {
-        if (int rc = record_overlapped_stage(Ls, out[s], s)) return rc;
+        if (int rc = record_overlapped_stage(Ls, out[s], s0 + s)) return rc;
       } else {
         ALP_CUDA(launch_face_flux_all(Ls, nbr26, cases, F, stride(), dstride(), face_threads));
-        ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cases, 0.0));
+        ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s0 + s, cases, 0.0));
       }
     }
     if (!trial) ALP_CUDA(launch_step_commit(cases, max_cases, stream));

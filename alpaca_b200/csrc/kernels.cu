@@ -27,9 +27,14 @@ __device__ __forceinline__ int slot_of(int const *work, int item) {
 
 // SSP-RK3 stage coefficients (runge_kutta_3_TVD.h:41-59): Uout = a0 U + a1 U0 +
 // c dt RHS (time_integrator.h:98-113, 434-457)
-__constant__ double kRkC[3] = {1.0, 0.25, 2.0 / 3.0};
-__constant__ double kRkA0[3] = {0.0, 0.25, 2.0 / 3.0};
-__constant__ double kRkA1[3] = {0.0, 0.75, 1.0 / 3.0};
+// Stage coefficients: indices 0-2 the SSP-RK3 stages (runge_kutta_3_TVD.h:
+// 41-59), 3-4 the TVD-RK2 stages (runge_kutta_2_TVD.h:37-56); per stage the
+// multiplier of dt and the buffer multipliers of the stage input and of the
+// step's initial state (unused in a first stage).
+__constant__ double kRkC[5] = {1.0, 0.25, 2.0 / 3.0, 1.0, 0.5};
+__constant__ double kRkA0[5] = {0.0, 0.25, 2.0 / 3.0, 0.0, 0.5};
+__constant__ double kRkA1[5] = {0.0, 0.75, 1.0 / 3.0, 0.0, 0.5};
+__host__ __device__ constexpr bool rk_first_stage(int stage) { return stage == 0 || stage == 3; }
 
 // Structural nonzeros of the left eigenvector matrix row n, column l
 // (eigendecomposition.h:316-359).
@@ -161,6 +166,24 @@ template <int DIM, int DIR>
 __device__ __forceinline__ void load_cell(double const *src, double (&dst)[DIM + 2]) {
 #pragma unroll
   for (int f = 0; f < DIM + 2; ++f) dst[f] = __ldg(src + f * Geo<DIM>::CELLS);
+}
+
+// Cell c of a stencil line (stencil_cell), with symmetry walls: a neighbour
+// entry of -2 across the block face mirrors the line about the wall and negates
+// the momentum normal to it (symmetry_boundary_condition.h:60-113, 148-217;
+// boundary_constants.h:35-46, 167-209); -1 is zero gradient.
+template <int DIM, int DIR, bool GATHER>
+__device__ __forceinline__ void stencil_load(double const *__restrict__ U, double const *blk,
+                                             int c, int cell0, int nlo, int nhi,
+                                             double (&dst)[DIM + 2]) {
+  constexpr int step = DIR == 0 ? Geo<DIM>::TCY * Geo<DIM>::TCZ : (DIR == 1 ? Geo<DIM>::TCZ : 1);
+  if (GATHER && ((c < HS && nlo == -2) || (c >= HS + IC && nhi == -2))) {
+    int const m = c < HS ? 2 * HS - 1 - c : 2 * (HS + IC) - 1 - c;
+    load_cell<DIM, DIR>(blk + cell0 + m * step, dst);
+    dst[MOMX + DIR] = -1.0 * dst[MOMX + DIR];
+    return;
+  }
+  load_cell<DIM, DIR>(stencil_cell<DIM, DIR, GATHER>(U, blk, c, cell0, nlo, nhi), dst);
 }
 
 // Flux of one face from its 6-cell stencil (the reference's per-face work:
@@ -443,8 +466,7 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
   double cons[6][NE];
 #pragma unroll
   for (int m = 0; m < 6; ++m)
-    load_cell<DIM, DIR>(stencil_cell<DIM, DIR, GATHER>(U, blk, HS + a - 3 + m, cell0, nlo, nhi),
-                        cons[m]);
+    stencil_load<DIM, DIR, GATHER>(U, blk, HS + a - 3 + m, cell0, nlo, nhi, cons[m]);
   double fd[NE];
   bool const valid = face_compute<DIM, DIR, SCHEME, T, P>(eos, bm.B, cons, fd, pol);
   write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
@@ -607,7 +629,7 @@ pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
   double w[6][NE];
 #pragma unroll
   for (int m = 0; m < 6; ++m)
-    load_cell<DIM, DIR>(stencil_cell<DIM, DIR, true>(Uin, blk, HS - 3 + m, cell0, nlo, nhi), w[m]);
+    stencil_load<DIM, DIR, true>(Uin, blk, HS - 3 + m, cell0, nlo, nhi, w[m]);
   double const ocs = inv(bm.cell_size);
   double const cdt = kRkC[stage] * (0.0 + dt);
   double const a0 = kRkA0[stage], a1 = kRkA1[stage];
@@ -646,7 +668,7 @@ pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
       for (int m = 0; m < 5; ++m)
 #pragma unroll
         for (int n = 0; n < NE; ++n) w[m][n] = w[m + 1][n];
-      load_cell<DIM, DIR>(stencil_cell<DIM, DIR, true>(Uin, blk, HS + a + 3, cell0, nlo, nhi), w[5]);
+      stencil_load<DIM, DIR, true>(Uin, blk, HS + a + 3, cell0, nlo, nhi, w[5]);
     }
   }
 }
@@ -746,7 +768,7 @@ stage_update_kernel(double const *Uin, double const *U0, double *Uout,
     double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
     size_t const x = base + (size_t)f * G::CELLS;
     double u = Uin[x];
-    if (stage != 0) u = a0 * u + a1 * U0[x];
+    if (!rk_first_stage(stage)) u = a0 * u + a1 * U0[x];
     Uout[x] = u + cdt * rhs;
   }
 }
@@ -855,7 +877,9 @@ zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
     int off[3] = {0, 0, 0};
     off[dir] = high ? 1 : -1;
     int const o = (off[0] + 1) * 9 + (off[1] + 1) * 3 + (off[2] + 1);
-    if (nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)] >= 0) continue;
+    int const nface = nbr26[(size_t)slot * 26 + (o < 13 ? o : o - 1)];
+    if (nface >= 0) continue;
+    bool const sym = nface == -2;  // symmetry wall: mirror, normal momentum negated
     int lo[3], ext[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -865,6 +889,7 @@ zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
     lo[dir] = high ? HS + IC : 0;
     ext[dir] = HS;
     int const plane = high ? HS + IC - 1 : HS;
+    int const mirror = high ? 2 * (HS + IC) - 1 : 2 * HS - 1;
     int const cells = ext[0] * ext[1] * ext[2];
     for (int x = threadIdx.x; x < cells * nfields; x += blockDim.x) {
       int const f = x / cells;
@@ -874,8 +899,10 @@ zero_gradient_kernel(double *__restrict__ U, int const *__restrict__ work,
       c[1] = lo[1] + (r / ext[2]) % ext[1];
       c[0] = lo[0] + r / (ext[2] * ext[1]);
       int s[3] = {c[0], c[1], c[2]};
-      s[dir] = plane;
-      b[f * G::CELLS + G::cell(c[0], c[1], c[2])] = b[f * G::CELLS + G::cell(s[0], s[1], s[2])];
+      s[dir] = sym ? mirror - c[dir] : plane;
+      double const v = b[f * G::CELLS + G::cell(s[0], s[1], s[2])];
+      // the momentum (or, for prime states, the velocity) normal to the wall is field 2 + dir
+      b[f * G::CELLS + G::cell(c[0], c[1], c[2])] = (sym && f == 2 + dir) ? -1.0 * v : v;
     }
     __syncthreads();
   }
@@ -1150,7 +1177,7 @@ cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout,
                                 long long stride, long long dstride, int stage,
                                 CaseState const *cases, double dt) {
   if (L.nwork <= 0) return cudaSuccess;
-  if (stage < 0 || stage > 2) return cudaErrorInvalidValue;
+  if (stage < 0 || stage > 4) return cudaErrorInvalidValue;
   int const threads = 256;
   dim3 grid(L.nwork, (interior_of(L.dim) + threads - 1) / threads);
   switch (L.dim) {

@@ -88,8 +88,9 @@ cudaError_t launch_face_flux_all(Launch const &L, int const *nbr26, CaseState co
 cudaError_t launch_pencil_stage(Launch const &L, double const *U0, double *Uout, double *R,
                                 int const *nbr26, CaseState const *cases, int stage);
 
-// RK3 stage on the interior: Uout = (stage ? a0*Uin + a1*U0 : Uin) + c*dt*div(F)
-// with Uin = L.U; dt per case from cases[meta.case_id].dt (skip when dt == 0),
+// Runge-Kutta stage on the interior: Uout = (first stage ? Uin : a0*Uin +
+// a1*U0) + c*dt*div(F) with Uin = L.U; stage 0-2 the SSP-RK3 stages, 3-4 the
+// TVD-RK2 stages; dt per case from cases[meta.case_id].dt (skip when dt == 0),
 // or `dt` for every block when cases is null. Uout may alias U0, not Uin.
 cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout, double const *F,
                                 long long flux_item_stride, long long dir_stride, int stage,

@@ -24,6 +24,7 @@ FLUX_SPLITTING_ROE, FLUX_SPLITTING_LLF, FLUX_SPLITTING_GLF = 0, 1, 2
 FLUX_SPLITTING_ROE_M, FLUX_SPLITTING_LLF_M = 3, 4
 
 # Further selections by name: base variant and the alp_scheme fields changed
+RK2, RK3 = 0, 1  # TimeIntegrators (numerical_setup.h:26)
 EXT_SCHEMES = {
     "fvchar_weno5z": ("fvchar", {"reconstruction_stencil": STENCIL_WENO5Z}),
     "fvchar_teno5": ("fvchar", {"reconstruction_stencil": STENCIL_TENO5}),
@@ -49,8 +50,22 @@ EXT_SCHEMES = {
     "fs_glf": ("fsroe", {"flux_splitting": FLUX_SPLITTING_GLF}),
     "fs_glf_weno5z": ("fsroe", {"reconstruction_stencil": STENCIL_WENO5Z,
                                 "flux_splitting": FLUX_SPLITTING_GLF}),
+    # TVD-RK2 selections of the reference's DetailedSod table
+    "rk2_fvchar_weno3": ("fvchar", {"reconstruction_stencil": STENCIL_WENO3,
+                                    "time_integrator": RK2}),
+    "rk2_fvchar_hll_weno5z": ("fvchar", {"reconstruction_stencil": STENCIL_WENO5Z,
+                                         "riemann_solver": RIEMANN_HLL, "time_integrator": RK2}),
+    "rk2_fs_glf": ("fsroe", {"flux_splitting": FLUX_SPLITTING_GLF, "time_integrator": RK2}),
+    "rk2_fs_llf_weno5z": ("fsroe", {"reconstruction_stencil": STENCIL_WENO5Z,
+                                    "flux_splitting": FLUX_SPLITTING_LLF, "time_integrator": RK2}),
+    "rk2_fs_roem_weno3": ("fsroe", {"reconstruction_stencil": STENCIL_WENO3,
+                                    "flux_splitting": FLUX_SPLITTING_ROE_M,
+                                    "time_integrator": RK2}),
+    "rk2_fs_llfm": ("fsroe", {"flux_splitting": FLUX_SPLITTING_LLF_M, "time_integrator": RK2}),
+    "rk2_fs_llfm_weno5z": ("fsroe", {"reconstruction_stencil": STENCIL_WENO5Z,
+                                     "flux_splitting": FLUX_SPLITTING_LLF_M,
+                                     "time_integrator": RK2}),
 }
-RK3 = 1
 FP64, FP32_FLUX = 0, 1
 HALO_ALL, HALO_FACES = 0, 1
 

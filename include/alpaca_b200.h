@@ -51,7 +51,9 @@ enum {
  * the stencils FirstOrder, WENO3, WENO5, WENO5Z or TENO5, the Riemann solvers
  * Hllc, Hllc_LM or Hll and the signal speeds Einfeldt, Davis, Toro or
  * Arithmetic; FluxSplitting with Roe, LocalLaxFriedrichs, GlobalLaxFriedrichs,
- * Roe_M or LocalLaxFriedrichs_M and the same stencils; RK3. WENO5 + Hllc +
+ * Roe_M or LocalLaxFriedrichs_M and the same stencils; RK3, or RK2 (TVD, two
+ * stages) in the engine and serving forms (alp_rk3_stage and multi-level
+ * cases: RK3). WENO5 + Hllc +
  * Einfeldt and WENO5 + Roe are the compiled fast path (FP64 and FP32_FLUX,
  * pencil sweeps); the other choices run through one FP64 face kernel that
  * selects them at run time. GlobalLaxFriedrichs takes the largest |u - c|,
@@ -87,7 +89,7 @@ enum {
   ALP_FLUX_SPLITTING_ROE_M = 3,
   ALP_FLUX_SPLITTING_LLF_M = 4
 };
-enum { ALP_RK3 = 1 };
+enum { ALP_RK2 = 0, ALP_RK3 = 1 };
 enum { ALP_FP64 = 0, ALP_FP32_FLUX = 1 };
 
 typedef struct {
@@ -165,10 +167,13 @@ int alp_prime_states(int dim, const alp_material *mat, const double *d_blocks, i
 /* Replaces the same-level part of HaloManager::MaterialHaloUpdate
  * (halo_manager.cpp:59-124, internal_halo_manager.cpp:439-459): d_nbr26
  * [nb][26] holds the neighbour block of each of the 26 directions (offsets
- * (ox,oy,oz) in {-1,0,1}^3 without the centre, x slowest) or -1 for a
- * zero-gradient domain face. mode ALP_HALO_ALL: all 26 regions then the
- * reference's full zero-gradient slabs; ALP_HALO_FACES: only the 2*dim face
- * regions over the interior extent (all a dimension-split scheme reads). */
+ * (ox,oy,oz) in {-1,0,1}^3 without the centre, x slowest), -1 for a
+ * zero-gradient domain face or, in a face slot, -2 for a symmetry wall
+ * (SymmetryBoundaryCondition: mirror image with field 2 + d, the momentum or
+ * velocity normal to the wall, negated). mode ALP_HALO_ALL: all 26 regions
+ * then the reference's full zero-gradient / symmetry slabs; ALP_HALO_FACES:
+ * only the 2*dim face regions over the interior extent (all a
+ * dimension-split scheme reads). */
 enum { ALP_HALO_ALL = 0, ALP_HALO_FACES = 1 };
 int alp_halo_update(int dim, double *d_blocks, int nb, int nfields, const int *d_nbr26,
                     int mode, alp_stream_t stream);
@@ -204,7 +209,7 @@ size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases);
 
 /* Adds a case: nb blocks of one cell size and material. h_nbr26 [nb][26]
  * gives neighbours as case-local block indices (-1 = zero-gradient domain
- * face). h_blocks [nb][NE][cells]: only the interiors are read; halos are
+ * face, -2 in a face slot = symmetry wall). h_blocks [nb][NE][cells]: only the interiors are read; halos are
  * filled on the device. The case runs until t_end or max_steps (<= 0: no
  * limit). Returns the case id in *case_id. Copies from host memory on the
  * engine stream; h_blocks may be reused once the call returns. */
@@ -212,10 +217,15 @@ int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size
                         double t0, double t_end, int max_steps, int nb, const int *h_nbr26,
                         const double *h_blocks, int *case_id);
 
+/* Boundary types of a regular grid, per dimension (periodic[d] below). */
+enum { ALP_BOUNDARY_ZERO_GRADIENT = 0, ALP_BOUNDARY_PERIODIC = 1, ALP_BOUNDARY_SYMMETRY = 2 };
+
 /* Adds a case whose initial condition is evaluated on the device, on a
  * regular grid of nblocks[0] x nblocks[1] x nblocks[2] blocks (entries past
- * the engine's dimension ignored), periodic[d] != 0 wrapping dimension d and
- * zero-gradient domain faces otherwise. Block (bx, by, bz) has index
+ * the engine's dimension ignored); periodic[d] is the boundary type of both
+ * domain faces of dimension d: ALP_BOUNDARY_PERIODIC wraps, ALP_BOUNDARY_SYMMETRY
+ * puts symmetry walls (SymmetryBoundaryCondition: mirror image, momentum normal
+ * to the wall negated), ALP_BOUNDARY_ZERO_GRADIENT (0) zero-gradient faces. Block (bx, by, bz) has index
  * (bx * ny + by) * nz + bz; cell centres are ((16 b + i + 1/2) cell_size).
  * Initial conditions (prime states converted with PrimeStatesToConservatives,
  * prime_states/prime_state_handler.h:195-275):
@@ -289,7 +299,7 @@ int alp_engine_add_case_expr(alp_engine *e, const alp_material *mat, double cell
 /* Removes a case and frees its blocks. */
 int alp_engine_remove_case(alp_engine *e, int case_id);
 
-/* Advances every active case by n steps (each: dt reduction, three RK3
+/* Advances every active case by n steps (each: dt reduction, the RK3 (or RK2)
  * stages of flux / divergence+stage update / halo). Cases whose time reached
  * t_end or whose step budget is spent do no work. Asynchronous. */
 int alp_engine_step(alp_engine *e, int n);

@@ -44,7 +44,8 @@ WENO5, WENO5Z, TENO5, WENO3, FIRST_ORDER = 4, 7, 11, 1, 0
 HLLC, HLLC_LM, HLL = 0, 1, 2
 EINFELDT, DAVIS, TORO, ARITHMETIC = 0, 1, 2, 3
 ROE, LLF, GLF, ROE_M, LLF_M = 0, 1, 2, 3, 4
-DEFAULT_OPTIONS = (WENO5, HLLC, EINFELDT, ROE)
+RK2, RK3 = 0, 1  # TimeIntegrators (numerical_setup.h:26)
+DEFAULT_OPTIONS = (WENO5, HLLC, EINFELDT, ROE, RK3)
 EXT_VARIANTS = {
     "fvchar_weno5z": ("fvchar", (WENO5Z, HLLC, EINFELDT, ROE)),
     "fvchar_teno5": ("fvchar", (TENO5, HLLC, EINFELDT, ROE)),
@@ -69,6 +70,14 @@ EXT_VARIANTS = {
     # global Lax-Friedrichs (maxima over all blocks of the call / case)
     "fs_glf": ("fsroe", (WENO5, HLLC, EINFELDT, GLF)),
     "fs_glf_weno5z": ("fsroe", (WENO5Z, HLLC, EINFELDT, GLF)),
+    # TVD-RK2 selections of the DetailedSod table (fifth option: time integrator)
+    "rk2_fvchar_weno3": ("fvchar", (WENO3, HLLC, EINFELDT, ROE, RK2)),
+    "rk2_fvchar_hll_weno5z": ("fvchar", (WENO5Z, HLL, EINFELDT, ROE, RK2)),
+    "rk2_fs_glf": ("fsroe", (WENO5, HLLC, EINFELDT, GLF, RK2)),
+    "rk2_fs_llf_weno5z": ("fsroe", (WENO5Z, HLLC, EINFELDT, LLF, RK2)),
+    "rk2_fs_roem_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, ROE_M, RK2)),
+    "rk2_fs_llfm": ("fsroe", (WENO5, HLLC, EINFELDT, LLF_M, RK2)),
+    "rk2_fs_llfm_weno5z": ("fsroe", (WENO5Z, HLLC, EINFELDT, LLF_M, RK2)),
 }
 
 
@@ -77,7 +86,7 @@ def variant_spec(variant: str):
     if variant in VARIANTS:
         return VARIANTS[variant] + (DEFAULT_OPTIONS,)
     base, opts = EXT_VARIANTS[variant]
-    return VARIANTS[base] + (opts,)
+    return VARIANTS[base] + (tuple(opts) + DEFAULT_OPTIONS[len(opts):],)
 
 _D = C.POINTER(C.c_double)
 _I = C.POINTER(C.c_int)
@@ -134,6 +143,7 @@ def _load(path: str):
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                C.c_int, C.c_int, _D, _I, _D]
     lib.oracle_set_options.argtypes = [C.c_int] * 4
+    lib.oracle_set_time_integrator.argtypes = [C.c_int]
     lib.oracle_levels_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, _I, _I,
                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _D, _I, _D]
@@ -161,7 +171,8 @@ class Restatement(_Common):
         self._select()
 
     def _select(self):
-        if self.lib.oracle_set_options(*self.options):
+        if self.lib.oracle_set_options(*self.options[:4]) or \
+                self.lib.oracle_set_time_integrator(self.options[4]):
             raise ValueError(f"unknown options {self.options}")
 
     # -- scalar kernels --

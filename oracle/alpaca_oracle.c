@@ -1026,26 +1026,36 @@ int oracle_timestep(int dim, const double *u, int nb, double gamma, double B,
 /* Zero-gradient slabs of the domain faces (boundary_constants.h:103-160,
  * 211-252): the full TCY x TCZ (etc.) halo slab takes the first / last
  * interior plane. A face is a domain face when face_nbr(b, face) < 0. */
+/* A neighbour entry of -2 marks a symmetry wall instead
+ * (symmetry_boundary_condition.h:60-113, boundary_constants.h:35-46, 167-209):
+ * the halo cell at distance q from the wall takes the interior cell at
+ * distance q on the other side, the momentum normal to the wall negated
+ * (SymmetrySign -1.0, symmetry_boundary_condition.h:148-217). */
 static void zero_gradient_slabs(const Geom *g, double *u, int nb, int nfields,
                                 const int *nbr, int nbr_stride, const int *face_slot) {
   for (int b = 0; b < nb; ++b)
     for (int face = 0; face < 2 * g->dim; ++face) {
-      if (nbr[(long)nbr_stride * b + face_slot[face]] >= 0) continue;
+      int const nb_face = nbr[(long)nbr_stride * b + face_slot[face]];
+      if (nb_face >= 0) continue;
+      int const sym = nb_face == -2;
       int const dir = face / 2, high = face % 2;
       int const s = high ? HS + IC - 1 : HS;
+      int const mirror = high ? 2 * (HS + IC) - 1 : 2 * HS - 1;
       int const h0 = high ? HS + IC : 0, h1 = high ? TC : HS;
       for (int f = 0; f < nfields; ++f) {
         double *x = u + ((long)b * nfields + f) * g->cells;
+        double const sign = (sym && f == MOMX + dir) ? -1.0 : 1.0;
         for (int i = 0; i < g->tc[0]; ++i)
           for (int j = 0; j < g->tc[1]; ++j)
             for (int k = 0; k < g->tc[2]; ++k) {
               int const idx[3] = {i, j, k};
               if (idx[dir] < h0 || idx[dir] >= h1) continue;
               int si = i, sj = j, sk = k;
-              if (dir == 0) si = s;
-              if (dir == 1) sj = s;
-              if (dir == 2) sk = s;
-              x[cidx(g, i, j, k)] = x[cidx(g, si, sj, sk)];
+              int const src = sym ? mirror - idx[dir] : s;
+              if (dir == 0) si = src;
+              if (dir == 1) sj = src;
+              if (dir == 2) sk = src;
+              x[cidx(g, i, j, k)] = sym ? sign * x[cidx(g, si, sj, sk)] : x[cidx(g, si, sj, sk)];
             }
       }
     }
@@ -1145,9 +1155,26 @@ int oracle_halo_update(int dim, double *u, int nb, const int *nbr) {
   return 0;
 }
 
-/* SSP-RK3 (runge_kutta_3_TVD.h:41-59) */
-static const double rk_c[3] = {1.0, 0.25, 2.0 / 3.0};
-static const double rk_a[3][2] = {{0.0, 0.0}, {0.25, 0.75}, {2.0 / 3.0, 1.0 / 3.0}};
+/* SSP-RK3 (runge_kutta_3_TVD.h:41-59) and TVD-RK2 (runge_kutta_2_TVD.h:37-56):
+ * per stage the multiplier of dt and the buffer multipliers of the stage input
+ * and of the step's initial state; the integrator is selected at run time
+ * (TimeIntegrators of numerical_setup.h: RK2 = 0, RK3 = 1). */
+enum { TI_RK2 = 0, TI_RK3 = 1 };
+static int g_integrator = TI_RK3;
+static const double rk3_c[3] = {1.0, 0.25, 2.0 / 3.0};
+static const double rk3_a[3][2] = {{0.0, 0.0}, {0.25, 0.75}, {2.0 / 3.0, 1.0 / 3.0}};
+static const double rk2_c[3] = {1.0, 0.5, 0.0};
+static const double rk2_a[3][2] = {{0.0, 0.0}, {0.5, 0.5}, {0.0, 0.0}};
+/* the multi-level loop is RK3 only */
+static const double *const rk_c = rk3_c;
+static const double (*const rk_a)[2] = rk3_a;
+static int rk_stages(void) { return g_integrator == TI_RK2 ? 2 : 3; }
+
+int oracle_set_time_integrator(int integrator) {
+  if (integrator != TI_RK2 && integrator != TI_RK3) return 1;
+  g_integrator = integrator;
+  return 0;
+}
 
 typedef struct {
   const Geom *g;
@@ -1169,11 +1196,13 @@ static void stage_task(void *vctx, int b, Work *w, double *f[3]) {
   if (c->stage == 0) memcpy(u0, u, sizeof(double) * n);
   block_fluxes(g, c->e, c->solver, c->recon, u, w, f);
   block_divergence(g, c->cell_size, f, r);
+  const double(*rka)[2] = g_integrator == TI_RK2 ? rk2_a : rk3_a;
+  const double *const rkc = g_integrator == TI_RK2 ? rk2_c : rk3_c;
   if (c->stage != 0) {
-    double const m0 = rk_a[c->stage][0], m1 = rk_a[c->stage][1];
+    double const m0 = rka[c->stage][0], m1 = rka[c->stage][1];
     for (long x = 0; x < n; ++x) u[x] = m0 * u[x] + m1 * u0[x];
   }
-  double const step = rk_c[c->stage] * (0.0 + c->dt);
+  double const step = rkc[c->stage] * (0.0 + c->dt);
   for (int e = 0; e < g->ne; ++e)
     for (int i = fic(g, 0); i <= lic(g, 0); ++i)
       for (int j = fic(g, 1); j <= lic(g, 1); ++j)
@@ -1211,7 +1240,7 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr
     double dt;
     oracle_timestep(dim, cur, nb, gamma, B, safe, cell_size, cfl, t, t_end, &dt);
     if (dt_log) dt_log[steps] = dt;
-    for (int stage = 0; stage < 3; ++stage) {
+    for (int stage = 0; stage < rk_stages(); ++stage) {
       StageCtx c = {&g, &e, solver, recon, stage, cur, u0, other, cell_size, dt};
       if (glf_selected(solver)) glf_maxima(&g, &e, cur, nb);
       parallel_blocks(&g, nb, nthreads, stage_task, &c);
@@ -1634,6 +1663,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                       double *t_io, int *macro_done, double *dt_log) {
   if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
   if (glf_selected(solver)) return 4; /* global maxima over the levels due: not restated */
+  if (g_integrator != TI_RK3) return 5; /* RK3 jump multipliers only */
   Geom g = make_geom(dim);
   Eos e = {dim, gamma, B, safe};
   Tree tr;

@@ -35,6 +35,8 @@ int oracle_weno5(const double *v6, double *left, double *right);
  * enums/flux_splitting.h:31). Default: WENO5, Hllc, Einfeldt, Roe. Process-wide
  * setting: not to be changed while another thread runs a call. */
 int oracle_set_options(int stencil, int riemann, int signal, int splitting);
+/* TimeIntegrators (numerical_setup.h:26): RK2 = 0, RK3 = 1 (default). */
+int oracle_set_time_integrator(int integrator);
 
 /* cons = (mass, energy, mx, my, mz), prim = (rho, p, u, v, w);
  * out = pressure, enthalpy, energy, speed of sound, psi, gruneisen.

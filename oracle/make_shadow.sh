@@ -9,10 +9,13 @@
 #   STENCIL: WENO5 (default) | WENO5Z | TENO5 | WENO3 | FirstOrder
 #   RIEMANN: Hllc (default) | Hllc_LM | Hll
 #   SIGNAL: Einfeldt (default) | Davis | Toro | Arithmetic
-#   SPLITTING: Roe (default) | LocalLaxFriedrichs | Roe_M | LocalLaxFriedrichs_M
+#   SPLITTING: Roe (default) | LocalLaxFriedrichs | GlobalLaxFriedrichs | Roe_M |
+#              LocalLaxFriedrichs_M
+#   INTEGRATOR: RK3 (default) | RK2   (numerical_setup.h)
 set -e
 SRC="$1"; OUT="$2"; SOLVER="$3"; RECON="$4"
 STENCIL="${5:-WENO5}"; RIEMANN="${6:-Hllc}"; SIGNAL="${7:-Einfeldt}"; SPLITTING="${8:-Roe}"
+INTEGRATOR="${9:-RK3}"
 mkdir -p "$OUT/user_specifications"
 U="$SRC/user_specifications"
 D="$OUT/user_specifications"
@@ -31,6 +34,9 @@ sed -e ':a' -e 'N' -e '$!ba' \
 sed -e ':a' -e 'N' -e '$!ba' \
   -e "s/ReconstructionStencils reconstruction_stencil =[[:space:]]*ReconstructionStencils::[A-Za-z0-9]*;/ReconstructionStencils reconstruction_stencil = ReconstructionStencils::$STENCIL;/" \
   "$U/stencil_setup.h" > "$D/stencil_setup.h"
+sed -e "s/time_integrator = TimeIntegrators::RK[0-9];/time_integrator = TimeIntegrators::$INTEGRATOR;/" \
+  "$U/numerical_setup.h" > "$D/numerical_setup.h"
+grep -q "time_integrator = TimeIntegrators::$INTEGRATOR;" "$D/numerical_setup.h"
 grep -q "EquationSet::Euler;" "$D/equation_settings.h"
 grep -q "convective_term_solver = ConvectiveTermSolvers::$SOLVER;" "$D/riemann_solver_settings.h"
 grep -q "flux_splitting_scheme = FluxSplitting::$SPLITTING;" "$D/riemann_solver_settings.h"

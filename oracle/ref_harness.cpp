@@ -15,7 +15,9 @@
 //     state reconstruction, WENO5 and HLLC/Einfeldt classes,
 //   * StiffenedGas / StiffenedGasSafe (materials/equations_of_state/),
 //   * PrimeStateHandler::ConvertConservativesToPrimeStates (prime_state_handler.h:141),
-//   * RungeKutta3TVD + TimeIntegrator on Node objects (integrator/time_integrator.h).
+//   * RungeKutta3TVD or RungeKutta2TVD (TimeIntegratorSetup::Concretize of the
+//     shadow numerical_setup.h) + TimeIntegrator on Node objects
+//     (integrator/time_integrator.h).
 // What is restated (the reference's versions need mpi.h, which is absent):
 //   * the divergence of SpaceSolver::UpdateFluxes (space_solver.cpp:58-70, 131-153),
 //   * the same-level halo copy (internal_halo_manager.cpp:439-459 with the plane
@@ -23,7 +25,10 @@
 //     zero-gradient slabs (boundary_constants.h:103-160, 211-252),
 //   * ComputeTimestepSize (modular_algorithm_assembler.cpp:1777-1997),
 //   * the single-level stage sequence of Advance (modular_algorithm_assembler.cpp:575-874).
+#include "boundary_condition/boundary_constants.h"
+#include "integrator/runge_kutta_2_TVD.h"
 #include "integrator/runge_kutta_3_TVD.h"
+#include "integrator/time_integrator_setup.h"
 #include "materials/equations_of_state/stiffened_gas.h"
 #include "materials/equations_of_state/stiffened_gas_safe.h"
 #include "materials/material_manager.h"
@@ -209,6 +214,39 @@ struct Scratch {
 // slabs for domain faces (boundary_constants.h:103-160, 211-252). nbr holds six
 // entries per block ordered W,E,S,N,B,T; -1 marks a zero-gradient domain face.
 // Reads the interiors and writes the halos of the buffer selected by get().
+// Symmetry wall at location LOC: the reference's mirror indices and halo
+// slab (BoundaryConstants<LOC>::SymmetryInternalValue / HaloStart/EndIndices,
+// boundary_constants.h:35-46, 167-209) with the sign of
+// SymmetryBoundaryCondition<LOC>::SymmetrySign (-1.0 for the momentum normal
+// to the wall, symmetry_boundary_condition.h:148-217).
+template <BoundaryLocation LOC>
+void SymmetrySlab(Field &f, double const sign) {
+  constexpr auto lo = BoundaryConstants<LOC>::HaloStartIndices();
+  constexpr auto hi = BoundaryConstants<LOC>::HaloEndIndices();
+  for (unsigned i = lo[0]; i < hi[0]; ++i)
+    for (unsigned j = lo[1]; j < hi[1]; ++j)
+      for (unsigned k = lo[2]; k < hi[2]; ++k)
+        f[i][j][k] = sign * BoundaryConstants<LOC>::SymmetryInternalValue(f, i, j, k);
+}
+
+void SymmetryFace(Field &f, int dir, int high, Equation eq) {
+  Equation const normal = dir == 0 ? Equation::MomentumX
+                                   : (dir == 1 ? Equation::MomentumY : Equation::MomentumZ);
+  double const sign = eq == normal ? -1.0 : 1.0;
+  if (dir == 0) {
+    if (high) SymmetrySlab<BoundaryLocation::East>(f, sign);
+    else SymmetrySlab<BoundaryLocation::West>(f, sign);
+  } else if (dir == 1) {
+    if (high) SymmetrySlab<BoundaryLocation::North>(f, sign);
+    else SymmetrySlab<BoundaryLocation::South>(f, sign);
+  } else {
+    if (high) SymmetrySlab<BoundaryLocation::Top>(f, sign);
+    else SymmetrySlab<BoundaryLocation::Bottom>(f, sign);
+  }
+}
+
+// Same-level halos from the six face neighbours nbr[6 b + face] (W, E, S, N,
+// B, T): >= 0 a neighbour, -1 a zero-gradient domain face, -2 a symmetry wall.
 void HaloUpdate(std::vector<std::unique_ptr<Node>> &nodes, int const *nbr,
                 std::function<Field &(Block &, Equation)> const &get) {
   int const nb = int(nodes.size());
@@ -242,7 +280,7 @@ void HaloUpdate(std::vector<std::unique_ptr<Node>> &nodes, int const *nbr,
       }
     }
   }
-  // External (zero-gradient) boundaries after all internal halos, as in
+  // External (zero-gradient, symmetry) boundaries after all internal halos, as in
   // HaloManager::MaterialHaloUpdateOnLevel (halo_manager.cpp:87-124).
   for (int b = 0; b < nb; ++b) {
     Block &me = nodes[b]->GetSinglePhase();
@@ -252,6 +290,10 @@ void HaloUpdate(std::vector<std::unique_ptr<Node>> &nodes, int const *nbr,
       int const dir = face / 2, high = face % 2;
       for (Equation const eq : MF::ASOE()) {
         Field &f = get(me, eq);
+        if (nbr[6 * b + face] == -2) {
+          SymmetryFace(f, dir, high, eq);
+          continue;
+        }
         if (dir == 0) {
           unsigned const s = high ? CC::FHHX() - 1 : CC::HSSX();
           unsigned const i0 = high ? CC::FHHX() : 0, i1 = high ? TCX : CC::HSSX();
@@ -437,7 +479,7 @@ int ref_run(double *u, int nb, int const *nbr, double gamma, double B, int safe,
   Context ctx(gamma, B, safe);
   if (nthreads < 1)
     nthreads = 1;
-  RungeKutta3TVD rk(*t_io);
+  TimeIntegratorSetup::Concretize<time_integrator>::type rk(*t_io);
   std::vector<std::unique_ptr<Node>> nodes(nb);
   double const node_size = cell_size * ICX;
   for (int b = 0; b < nb; ++b) {

@@ -49,21 +49,37 @@ def small_cases():
 # The reference testsuite's DetailedSod error table
 # (testsuite/ReferenceValues/DetailedSod/1D_DetailedSod_errors_reference.csv):
 # (DensityL1, DensityL2, DensityLinf, PressureL1, PressureL2, PressureLinf) at
-# t = 0.2 of the single-level runs on 128 cells (4 blocks of 32, RK3) whose
-# schemes this library compiles, keyed by variant name with the CSV line.
+# t = 0.2 of the single-level runs whose schemes this library compiles, keyed
+# by variant name: (CSV line, norms, blocks of 16 cells). The grids are the
+# reference's: 4 nodes of 32 (RK3), 24 or 8 cells, i.e. 128, 96 or 32 cells,
+# with the symmetry walls of testsuite/InputFiles/DetailedSod/1D/SodX.xml.
 SOD_REFERENCE_NORMS = {
     "fvchar": (58, (6.90089530e-07, 2.05275093e-07, 1.39620303e-07,
-                    5.95487513e-07, 2.49384854e-07, 2.28787992e-07)),
+                    5.95487513e-07, 2.49384854e-07, 2.28787992e-07), 8),
     "fvchar_weno3_hll": (42, (1.02264424e-06, 2.58609513e-07, 1.78590815e-07,
-                              8.47004465e-07, 3.27459497e-07, 2.99812686e-07)),
+                              8.47004465e-07, 3.27459497e-07, 2.99812686e-07), 8),
     "fs_weno3": (30, (9.64420466e-07, 2.53172573e-07, 1.78922953e-07,
-                      8.43317388e-07, 3.33634664e-07, 3.05663996e-07)),
+                      8.43317388e-07, 3.33634664e-07, 3.05663996e-07), 8),
     "fs_llf_weno3": (22, (1.02774396e-06, 2.58481190e-07, 1.81214189e-07,
-                          9.21920404e-07, 3.41063398e-07, 3.09256115e-07)),
+                          9.21920404e-07, 3.41063398e-07, 3.09256115e-07), 8),
     "fs_llfm_weno3": (74, (9.60803571e-07, 2.56417781e-07, 1.82571444e-07,
-                           8.29079300e-07, 3.39286859e-07, 3.11954844e-07)),
+                           8.29079300e-07, 3.39286859e-07, 3.11954844e-07), 8),
     "fs_glf_weno5z": (70, (6.11467178e-07, 1.86248795e-07, 1.19883696e-07,
-                           5.70962203e-07, 2.28544959e-07, 2.03433021e-07)),
+                           5.70962203e-07, 2.28544959e-07, 2.03433021e-07), 8),
+    "rk2_fs_glf": (6, (1.79790069e-06, 4.81072783e-07, 2.95788755e-07,
+                       1.70715046e-06, 5.93024051e-07, 4.98112838e-07), 6),
+    "rk2_fs_llf_weno5z": (10, (4.20347064e-05, 1.71242192e-05, 1.50718666e-05,
+                               4.95227518e-05, 2.76342072e-05, 2.66893986e-05), 2),
+    "rk2_fvchar_weno3": (34, (2.20465992e-06, 5.65708847e-07, 3.71935085e-07,
+                              1.91570490e-06, 6.99942603e-07, 6.14275684e-07), 6),
+    "rk2_fvchar_hll_weno5z": (46, (4.18500391e-05, 1.69155498e-05, 1.48248685e-05,
+                                   4.66086932e-05, 2.66536675e-05, 2.58109384e-05), 2),
+    "rk2_fs_roem_weno3": (50, (2.50746878e-06, 6.35908633e-07, 3.86180985e-07,
+                               2.36985780e-06, 8.19966693e-07, 6.63064934e-07), 6),
+    "rk2_fs_llfm": (62, (4.73109368e-05, 1.91201415e-05, 1.68388893e-05,
+                         5.45096592e-05, 3.08180236e-05, 2.97142519e-05), 2),
+    "rk2_fs_llfm_weno5z": (82, (1.28201009e-06, 3.86170496e-07, 1.92486130e-07,
+                                1.12651026e-06, 4.31014301e-07, 3.36644260e-07), 6),
 }
 
 

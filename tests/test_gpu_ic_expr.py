@@ -49,12 +49,14 @@ def test_device_prime_states_match_oracle(cuda, dim, name):
 
 def test_engine_sod_from_expression_meets_reference_table(cuda):
     """The Sod program of the reference's DetailedSod input, evaluated on the
-    device into an engine case, run to t = 0.2: the reference's error table."""
+    device into an engine case with its symmetry walls, run to t = 0.2: the
+    reference's error table."""
     case = cases.sod_1d()
     prog = api.IcProgram(SOD)
     eng = api.Engine(1, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
     cid = eng.add_case_expr(prog, (case.grid.nb,), case.grid.cell_size,
-                            N.Material.make(case.gamma), cfl=case.cfl, t_end=case.t_end)
+                            N.Material.make(case.gamma), periodic=(cases.SYMMETRY, 0, 0),
+                            cfl=case.cfl, t_end=case.t_end)
     u0 = eng.get(cid)[0]
     I = cases.interior(1)
     np.testing.assert_allclose(u0[I], case.u[I], rtol=1e-15, atol=0)

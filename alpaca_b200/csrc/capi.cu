@@ -44,9 +44,10 @@ namespace alp {
 int scheme_id(alp_scheme const *s, int *id, int *precision) {
   if (!s) return fail(ALP_ERR_INVALID, "scheme is null");
   int const st = s->reconstruction_stencil;
-  if (st != ST_WENO5 && st != ST_WENO5Z && st != ST_TENO5 && st != ST_WENO3 && st != ST_FIRST_ORDER)
+  if (st != ST_WENO5 && st != ST_WENO5Z && st != ST_TENO5 && st != ST_WENO3 &&
+      st != ST_FIRST_ORDER && st != ST_WENO7)
     return fail(ALP_ERR_INVALID,
-                "compiled ReconstructionStencils: FirstOrder, WENO3, WENO5, WENO5Z, TENO5");
+                "compiled ReconstructionStencils: FirstOrder, WENO3, WENO5, WENO5Z, TENO5, WENO7");
   if (s->time_integrator != ALP_RK3 && s->time_integrator != ALP_RK2)
     return fail(ALP_ERR_INVALID, "TimeIntegrators must be RK2 or RK3");
   if (s->precision != ALP_FP64 && s->precision != ALP_FP32_FLUX)

@@ -194,18 +194,19 @@ __device__ __forceinline__ void stencil_load(double const *__restrict__ U, doubl
 // has a non-positive density (eigendecomposition.h:244).
 // P selects reconstruction stencil, Riemann solver and splitting eigenvalues
 // (DefaultPolicy: WENO5, HLLC/Einfeldt, Roe; ExtPolicy: run-time choice, FP64).
-template <int DIM, int DIR, int SCHEME, typename T, typename P = DefaultPolicy>
+template <int DIM, int DIR, int SCHEME, typename T, typename P = DefaultPolicy, int W = 6>
 __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
-                                             double const (&cons)[6][DIM + 2],
+                                             double const (&cons)[W][DIM + 2],
                                              double (&fd)[DIM + 2], P const &pol = P()) {
   constexpr int NE = DIM + 2;
   T flux[NE];
   bool valid = true;
   constexpr int mP = MOMX + DIR;
+  constexpr int C = W / 2 - 1;  // the face's left cell i in the stencil
 
   if constexpr (SCHEME == FV_CHAR || SCHEME == FS_ROE) {
-    auto const pt = cell_prims<DIM, DIR>(eos, cons[2]);
-    auto const pn = cell_prims<DIM, DIR>(eos, cons[3]);
+    auto const pt = cell_prims<DIM, DIR>(eos, cons[C]);
+    auto const pn = cell_prims<DIM, DIR>(eos, cons[C + 1]);
     if (!(pt.rho > 0.0) || !(pn.rho > 0.0)) valid = false;
     Roe<T> const r = roe_average<DIM, DIR, T>(eos, pt, pn);
     T ch[2][NE];
@@ -217,15 +218,15 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       for (int n = 0; n < NE; ++n) {
         T L[NE];
         left_row<DIM, DIR, T>(n, r, L);
-        T uc[6];
+        T uc[W];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
+        for (int m = 0; m < W; ++m) {
           T s = T(0);
 #pragma unroll
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            s = fmaf(L[l], m == 2 ? 0.0f : float(cons[m][l] - cons[2][l]), s);
+            s = fmaf(L[l], m == C ? 0.0f : float(cons[m][l] - cons[C][l]), s);
           }
           uc[m] = s;
         }
@@ -237,8 +238,8 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       double cm[NE], cp[NE];
 #pragma unroll
       for (int f = 0; f < NE; ++f) {
-        cm[f] = cons[2][f] + double(dm[f]);
-        cp[f] = cons[2][f] + double(dp[f]);
+        cm[f] = cons[C][f] + double(dm[f]);
+        cp[f] = cons[C][f] + double(dp[f]);
       }
       if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
       double const one_l = inv(cm[MASS]), one_r = inv(cp[MASS]);
@@ -254,9 +255,9 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       for (int n = 0; n < NE; ++n) {
         T L[NE];
         left_row<DIM, DIR, T>(n, r, L);
-        T uc[6];
+        T uc[W];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
+        for (int m = 0; m < W; ++m) {
           T s = T(0);
           bool first = true;
 #pragma unroll
@@ -292,9 +293,9 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       pol.template riemann<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
     } else {
       // Roe flux-vector splitting (flux_splitting_scheme.cpp:42-76, 185-315)
-      double advd[6][NE];
+      double advd[W][NE];
 #pragma unroll
-      for (int m = 0; m < 6; ++m) {
+      for (int m = 0; m < W; ++m) {
         double const one_rho = inv(cons[m][MASS]);
         double const p = eos_pressure<DIM>(
             eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
@@ -322,17 +323,17 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
         T L[NE];
         left_row<DIM, DIR, T>(n, r, L);
         T const alpha = n == 0 ? ev_nl0 : (n == NE - 1 ? ev_nl1 : ev_lin);
-        T pos[6], neg[6];
+        T pos[W], neg[W];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) {
+        for (int m = 0; m < W; ++m) {
           T sp = T(0), sn = T(0);
           bool first = true;
 #pragma unroll
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            T const uct = (DELTA ? T(cons[m][l] - cons[2][l]) : T(cons[m][l])) * L[l];
-            T const act = (DELTA ? T(advd[m][l] - advd[2][l]) : T(advd[m][l])) * L[l];
+            T const uct = (DELTA ? T(cons[m][l] - cons[C][l]) : T(cons[m][l])) * L[l];
+            T const act = (DELTA ? T(advd[m][l] - advd[C][l]) : T(advd[m][l])) * L[l];
             if constexpr (ALP_FAST) {
               // project state (into sp) and flux (into sn), split afterwards:
               // L (f +/- alpha u) = L f +/- alpha L u
@@ -361,15 +362,15 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       to_physical<DIM, DIR, T>(r, ch[0], flux);
       if constexpr (DELTA) {
 #pragma unroll
-        for (int f = 0; f < NE; ++f) fd[f] = advd[2][f] + double(flux[f]);
+        for (int f = 0; f < NE; ++f) fd[f] = advd[C][f] + double(flux[f]);
         return valid;
       }
     }
   } else {
     // FV primitive reconstruction (primitive_state_reconstruction.h:56-107)
-    double prim[6][NE];
+    double prim[W][NE];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) {
+    for (int m = 0; m < W; ++m) {
       prim[m][RHO] = cons[m][MASS];
       double const one_rho = inv(cons[m][MASS]);
 #pragma unroll
@@ -383,13 +384,13 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       double pmd[NE], ppd[NE];
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
-        T arr[6];
+        T arr[W];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n] - prim[2][n]);
+        for (int m = 0; m < W; ++m) arr[m] = T(prim[m][n] - prim[C][n]);
         T wl, wr;
         weno5_pair(arr, wl, wr);
-        pmd[n] = prim[2][n] + double(wl);
-        ppd[n] = prim[2][n] + double(wr);
+        pmd[n] = prim[C][n] + double(wl);
+        ppd[n] = prim[C][n] + double(wr);
       }
       double cm[NE], cp[NE];
       cm[MASS] = pmd[RHO];
@@ -412,9 +413,9 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       T pm[NE], pp[NE];
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
-        T arr[6];
+        T arr[W];
 #pragma unroll
-        for (int m = 0; m < 6; ++m) arr[m] = T(prim[m][n]);
+        for (int m = 0; m < W; ++m) arr[m] = T(prim[m][n]);
         pol.pair(arr, pm[n], pp[n]);
       }
       // PrimeStatesToConservatives (prime_state_handler.h:195-275)
@@ -445,7 +446,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
 
 // Flux of the face with thread index t of direction DIR of the block in `slot`.
 template <int DIM, int DIR, int SCHEME, typename T, bool ACCUM, bool GATHER,
-          typename P = DefaultPolicy>
+          typename P = DefaultPolicy, int W = 6>
 __device__ __forceinline__ void face_flux(double const *__restrict__ U,
                                           int const *__restrict__ nbr26, int slot, int item,
                                           int t, BlockMeta const &bm, double *__restrict__ F,
@@ -461,14 +462,14 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
   // low / high neighbour along DIR (26-table slots of W,E / S,N / B,T)
   constexpr int lo_slot = DIR == 0 ? 4 : (DIR == 1 ? 10 : 12);
   constexpr int hi_slot = DIR == 0 ? 21 : (DIR == 1 ? 15 : 13);
-  int const nlo = GATHER && a < 3 ? __ldg(nbr26 + (size_t)slot * 26 + lo_slot) : 0;
-  int const nhi = GATHER && a > 13 ? __ldg(nbr26 + (size_t)slot * 26 + hi_slot) : 0;
-  double cons[6][NE];
+  int const nlo = GATHER && a < W / 2 ? __ldg(nbr26 + (size_t)slot * 26 + lo_slot) : 0;
+  int const nhi = GATHER && a > IC - W / 2 ? __ldg(nbr26 + (size_t)slot * 26 + hi_slot) : 0;
+  double cons[W][NE];
 #pragma unroll
-  for (int m = 0; m < 6; ++m)
-    stencil_load<DIM, DIR, GATHER>(U, blk, HS + a - 3 + m, cell0, nlo, nhi, cons[m]);
+  for (int m = 0; m < W; ++m)
+    stencil_load<DIM, DIR, GATHER>(U, blk, HS + a - W / 2 + m, cell0, nlo, nhi, cons[m]);
   double fd[NE];
-  bool const valid = face_compute<DIM, DIR, SCHEME, T, P>(eos, bm.B, cons, fd, pol);
+  bool const valid = face_compute<DIM, DIR, SCHEME, T, P, W>(eos, bm.B, cons, fd, pol);
   write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
 }
 
@@ -519,6 +520,12 @@ face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
   }
 }
 
+// The run-time selected schemes read 6-cell stencils (i-2 .. i+3), or 8-cell
+// stencils (i-3 .. i+4) when the stencil is WENO7; the narrower stencils use
+// the middle cells. The 8-wide instantiation holds 33 % more stencil state, so
+// the launchers pick it only for WENO7.
+inline bool ext_wide(SchemeOptions const &o) { return o.stencil == ST_WENO7; }
+
 // The policy of one block: the GlobalLaxFriedrichs wave speeds of its case.
 __device__ __forceinline__ ExtPolicy block_policy(ExtPolicy pol, BlockMeta const &bm,
                                                   unsigned long long const *glf) {
@@ -528,7 +535,7 @@ __device__ __forceinline__ ExtPolicy block_policy(ExtPolicy pol, BlockMeta const
 }
 
 // The same two kernels for the run-time selected schemes (ExtPolicy, FP64).
-template <int DIM, int DIR, int SCHEME, bool ACCUM>
+template <int DIM, int DIR, int SCHEME, bool ACCUM, int W>
 __global__ void __launch_bounds__(128)
 face_flux_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
                      BlockMeta const *__restrict__ meta, BlockMeta def, double *__restrict__ F,
@@ -538,11 +545,11 @@ face_flux_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
   int const item = blockIdx.x;
   int const slot = slot_of(work, item);
   BlockMeta const bm = meta ? meta[slot] : def;
-  face_flux<DIM, DIR, SCHEME, double, ACCUM, false, ExtPolicy>(U, nullptr, slot, item, t, bm, F,
+  face_flux<DIM, DIR, SCHEME, double, ACCUM, false, ExtPolicy, W>(U, nullptr, slot, item, t, bm, F,
                                                                stride, block_policy(pol, bm, glf));
 }
 
-template <int DIM, int SCHEME>
+template <int DIM, int SCHEME, int W>
 __global__ void __launch_bounds__(128)
 face_flux_all_ext_kernel(double const *__restrict__ U, int const *__restrict__ work,
                          BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
@@ -558,15 +565,15 @@ face_flux_all_ext_kernel(double const *__restrict__ U, int const *__restrict__ w
   int const dir = blockIdx.z;
   if (dir == 0) {
     if (t < FaceMap<DIM, 0>::COUNT)
-      face_flux<DIM, 0, SCHEME, double, false, true, ExtPolicy>(U, nbr26, slot, item, t, bm, F,
+      face_flux<DIM, 0, SCHEME, double, false, true, ExtPolicy, W>(U, nbr26, slot, item, t, bm, F,
                                                                 stride, pol);
   } else if (DIM > 1 && dir == 1) {
     if (t < FaceMap<DIM, 1>::COUNT)
-      face_flux<DIM, (DIM > 1 ? 1 : 0), SCHEME, double, false, true, ExtPolicy>(
+      face_flux<DIM, (DIM > 1 ? 1 : 0), SCHEME, double, false, true, ExtPolicy, W>(
           U, nbr26, slot, item, t, bm, F + dstride, stride, pol);
   } else if (DIM > 2) {
     if (t < FaceMap<DIM, 2>::COUNT)
-      face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, double, false, true, ExtPolicy>(
+      face_flux<DIM, (DIM > 2 ? 2 : 0), SCHEME, double, false, true, ExtPolicy, W>(
           U, nbr26, slot, item, t, bm, F + 2 * dstride, stride, pol);
   }
 }
@@ -1080,30 +1087,36 @@ initial_condition_kernel(double *__restrict__ U, int first, int nbx, int nby, in
 
 namespace {
 
+template <int DIM, int DIR, bool ACC, int W>
+cudaError_t face_flux_ext_dir(Launch const &L, dim3 grid, double *F, long long stride,
+                              int threads) {
+  ExtPolicy const pol{L.opt};
+  switch (L.scheme) {
+    case FV_CHAR:
+      face_flux_ext_kernel<DIM, DIR, FV_CHAR, ACC, W>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
+      break;
+    case FV_PRIM:
+      face_flux_ext_kernel<DIM, DIR, FV_PRIM, ACC, W>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
+      break;
+    case FS_ROE:
+      face_flux_ext_kernel<DIM, DIR, FS_ROE, ACC, W>
+          <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 template <int DIM, int DIR, typename T, bool ACC>
 cudaError_t face_flux_dir(Launch const &L, double *F, long long stride, int threads) {
   using M = FaceMap<DIM, DIR>;
   dim3 grid(L.nwork, (M::COUNT + threads - 1) / threads);
-  if (!L.opt.is_default()) {
-    ExtPolicy const pol{L.opt};
-    switch (L.scheme) {
-      case FV_CHAR:
-        face_flux_ext_kernel<DIM, DIR, FV_CHAR, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
-        break;
-      case FV_PRIM:
-        face_flux_ext_kernel<DIM, DIR, FV_PRIM, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
-        break;
-      case FS_ROE:
-        face_flux_ext_kernel<DIM, DIR, FS_ROE, ACC>
-            <<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, L.def, F, stride, pol, L.glf);
-        break;
-      default:
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-  }
+  if (!L.opt.is_default())
+    return ext_wide(L.opt) ? face_flux_ext_dir<DIM, DIR, ACC, 8>(L, grid, F, stride, threads)
+                           : face_flux_ext_dir<DIM, DIR, ACC, 6>(L, grid, F, stride, threads);
   switch (L.scheme) {
     case FV_CHAR:
       face_flux_kernel<DIM, DIR, FV_CHAR, T, ACC>
@@ -1190,28 +1203,35 @@ cudaError_t launch_stage_update(Launch const &L, double const *U0, double *Uout,
 }
 
 namespace {
+template <int DIM, int W>
+cudaError_t face_flux_all_ext(Launch const &L, dim3 grid, int const *nbr26, CaseState const *cases,
+                              double *F, long long stride, long long dstride, int threads) {
+  ExtPolicy const pol{L.opt};
+  switch (L.scheme) {
+    case FV_CHAR:
+      face_flux_all_ext_kernel<DIM, FV_CHAR, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      break;
+    case FV_PRIM:
+      face_flux_all_ext_kernel<DIM, FV_PRIM, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      break;
+    case FS_ROE:
+      face_flux_all_ext_kernel<DIM, FS_ROE, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      break;
+    default:
+      return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
 template <int DIM, typename T>
 cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *cases, double *F,
                             long long stride, long long dstride, int threads) {
   int const count = (IC + 1) * (DIM > 1 ? IC : 1) * (DIM > 2 ? IC : 1);
   dim3 grid(L.nwork, (count + threads - 1) / threads, DIM);
-  if (!L.opt.is_default()) {
-    ExtPolicy const pol{L.opt};
-    switch (L.scheme) {
-      case FV_CHAR:
-        face_flux_all_ext_kernel<DIM, FV_CHAR><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
-        break;
-      case FV_PRIM:
-        face_flux_all_ext_kernel<DIM, FV_PRIM><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
-        break;
-      case FS_ROE:
-        face_flux_all_ext_kernel<DIM, FS_ROE><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
-        break;
-      default:
-        return cudaErrorInvalidValue;
-    }
-    return cudaGetLastError();
-  }
+  if (!L.opt.is_default())
+    return ext_wide(L.opt)
+               ? face_flux_all_ext<DIM, 8>(L, grid, nbr26, cases, F, stride, dstride, threads)
+               : face_flux_all_ext<DIM, 6>(L, grid, nbr26, cases, F, stride, dstride, threads);
   // items x chunks < 2^31 for up to 2^31 / 68 items (64-thread chunks)
   int const chunks = (count + threads - 1) / threads;
   if ((long long)L.nwork * chunks > 0x7fffffffLL) return cudaErrorInvalidValue;

@@ -20,7 +20,14 @@ enum Precision { FP64 = 0, FP32_FLUX = 1 };
 // in FP64 (schemes_ext.cuh); the values are those of the reference's enums
 // (stencil_setup.h:26-43, riemann_solver_settings.h:47, enums/signal_speed.h:31,
 // enums/flux_splitting.h:31).
-enum StencilId { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11 };
+enum StencilId {
+  ST_FIRST_ORDER = 0,
+  ST_WENO3 = 1,
+  ST_WENO5 = 4,
+  ST_WENO5Z = 7,
+  ST_TENO5 = 11,
+  ST_WENO7 = 13
+};
 enum RiemannId { RS_HLLC = 0, RS_HLLC_LM = 1, RS_HLL = 2 };
 enum SignalSpeedId { SS_EINFELDT = 0, SS_DAVIS = 1, SS_TORO = 2, SS_ARITHMETIC = 3 };
 enum SplittingId { FSP_ROE = 0, FSP_LLF = 1, FSP_GLF = 2, FSP_ROE_M = 3, FSP_LLF_M = 4 };

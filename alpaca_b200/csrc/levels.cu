@@ -640,6 +640,9 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
   int sid, prec;
   if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
+  if (scheme->reconstruction_stencil == ST_WENO7)
+    return fail(ALP_ERR_INVALID,
+                "WENO7 reads four cells across a face; multi-level ghost blocks hold three");
   if (scheme->time_integrator != ALP_RK3)
     return fail(ALP_ERR_INVALID, "multi-level cases integrate with RK3 (its jump multipliers)");
   if (sid == FS_ROE && scheme->flux_splitting == FSP_GLF)

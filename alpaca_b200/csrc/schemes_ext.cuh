@@ -99,20 +99,72 @@ __device__ __forceinline__ double weno3_core(double v1, double v2, double v3) {
 // Reconstruction of the 6-cell array a (cells i-2..i+3 around face i+1/2) with
 // UpwindLeft (right = false) or UpwindRight evaluation properties
 // (stencils/apply_wrapper.h:47-57); narrower stencils use the middle cells.
-__device__ __forceinline__ double reconstruct(int stencil, double const (&a)[6], bool right) {
+// WENO7-JS (weno7.h:21-212; coefficients of Balsara & Shu 2000): v1..v7 the
+// cells i-3..i+3 seen from the upwind side, eps 1e-10, the reference's
+// association order.
+__device__ __forceinline__ double weno7_core(double v1, double v2, double v3, double v4,
+                                             double v5, double v6, double v7) {
+  double const s11 = 547.0 * v1 + -3882.0 * v2 + 4642.0 * v3 + -1854.0 * v4;
+  double const s12 = 7043.0 * v2 + -17246.0 * v3 + 7042.0 * v4;
+  double const s13 = 11003.0 * v3 + -9402.0 * v4;
+  double const s14 = 2107.0 * v4;
+  double const s1 = v1 * s11 + v2 * s12 + v3 * s13 + v4 * s14;
+  double const s21 = 267.0 * v2 + -1642.0 * v3 + 1602.0 * v4 + -494.0 * v5;
+  double const s22 = 2843.0 * v3 + -5966.0 * v4 + 1922.0 * v5;
+  double const s23 = 3443.0 * v4 + -2522.0 * v5;
+  double const s24 = 547.0 * v5;
+  double const s2 = v2 * s21 + v3 * s22 + v4 * s23 + v5 * s24;
+  double const s31 = 547.0 * v3 + -2522.0 * v4 + 1922.0 * v5 + -494.0 * v6;
+  double const s32 = 3443.0 * v4 + -5966.0 * v5 + 1602.0 * v6;
+  double const s33 = 2843.0 * v5 + -1642.0 * v6;
+  double const s34 = 267.0 * v6;
+  double const s3 = v3 * s31 + v4 * s32 + v5 * s33 + v6 * s34;
+  double const s41 = 2107.0 * v4 + -9402.0 * v5 + 7042.0 * v6 + -1854.0 * v7;
+  double const s42 = 11003.0 * v5 + -17246.0 * v6 + 4642.0 * v7;
+  double const s43 = 7043.0 * v6 + -3882.0 * v7;
+  double const s44 = 547.0 * v7;
+  double const s4 = v4 * s41 + v5 * s42 + v6 * s43 + v7 * s44;
+  double const eps = 1.0e-10;
+  double const a1 = quot(1.0 / 35.0, (s1 + eps) * (s1 + eps));
+  double const a2 = quot(12.0 / 35.0, (s2 + eps) * (s2 + eps));
+  double const a3 = quot(18.0 / 35.0, (s3 + eps) * (s3 + eps));
+  double const a4 = quot(4.0 / 35.0, (s4 + eps) * (s4 + eps));
+  double const one_a_sum = quot(1.0, a1 + a2 + a3 + a4);
+  double const w1 = a1 * one_a_sum, w2 = a2 * one_a_sum, w3 = a3 * one_a_sum,
+               w4 = a4 * one_a_sum;
+  return w1 * (-3.0 / 12.0 * v1 + 13.0 / 12.0 * v2 + -23.0 / 12.0 * v3 + 25.0 / 12.0 * v4) +
+         w2 * (1.0 / 12.0 * v2 + -5.0 / 12.0 * v3 + 13.0 / 12.0 * v4 + 3.0 / 12.0 * v5) +
+         w3 * (-1.0 / 12.0 * v3 + 7.0 / 12.0 * v4 + 7.0 / 12.0 * v5 + -1.0 / 12.0 * v6) +
+         w4 * (3.0 / 12.0 * v4 + 13.0 / 12.0 * v5 + -5.0 / 12.0 * v6 + 1.0 / 12.0 * v7);
+}
+
+// a: the N cells of the stencil line with the face's left cell i at N/2 - 1
+// (N = 6: i-2..i+3, N = 8: i-3..i+4); the five- and three-point stencils read
+// the middle cells.
+template <int N>
+__device__ __forceinline__ double reconstruct(int stencil, double const (&a)[N], bool right) {
+  constexpr int o = N / 2 - 3;  // a[o + k]: cell i - 2 + k
   switch (stencil) {
+    case ST_WENO7:
+      if constexpr (N >= 8)
+        return right ? weno7_core(a[o + 6], a[o + 5], a[o + 4], a[o + 3], a[o + 2], a[o + 1], a[o])
+                     : weno7_core(a[o - 1], a[o], a[o + 1], a[o + 2], a[o + 3], a[o + 4], a[o + 5]);
+      else
+        return 0.0;  // not reachable: WENO7 runs with 8-cell stencils
     case ST_WENO5Z:
-      return right ? weno5z_core(a[5], a[4], a[3], a[2], a[1])
-                   : weno5z_core(a[0], a[1], a[2], a[3], a[4]);
+      return right ? weno5z_core(a[o + 5], a[o + 4], a[o + 3], a[o + 2], a[o + 1])
+                   : weno5z_core(a[o], a[o + 1], a[o + 2], a[o + 3], a[o + 4]);
     case ST_TENO5:
-      return right ? teno5_core(a[5], a[4], a[3], a[2], a[1])
-                   : teno5_core(a[0], a[1], a[2], a[3], a[4]);
+      return right ? teno5_core(a[o + 5], a[o + 4], a[o + 3], a[o + 2], a[o + 1])
+                   : teno5_core(a[o], a[o + 1], a[o + 2], a[o + 3], a[o + 4]);
     case ST_WENO3:
-      return right ? weno3_core(a[4], a[3], a[2]) : weno3_core(a[1], a[2], a[3]);
+      return right ? weno3_core(a[o + 4], a[o + 3], a[o + 2])
+                   : weno3_core(a[o + 1], a[o + 2], a[o + 3]);
     case ST_FIRST_ORDER:
-      return right ? a[3] : a[2];
+      return right ? a[o + 3] : a[o + 2];
     default:
-      return right ? weno5_right(a) : weno5_left(a);
+      return right ? weno5_core(a[o + 5], a[o + 4], a[o + 3], a[o + 2], a[o + 1])
+                   : weno5_core(a[o], a[o + 1], a[o + 2], a[o + 3], a[o + 4]);
   }
 }
 
@@ -277,17 +329,19 @@ struct DefaultPolicy {
 struct ExtPolicy {
   SchemeOptions o;
   double glf[3] = {0.0, 0.0, 0.0};  // GlobalLaxFriedrichs wave speeds of the block's case
-  __device__ __forceinline__ double left(double const (&a)[6]) const {
+  template <int N> __device__ __forceinline__ double left(double const (&a)[N]) const {
     return reconstruct(o.stencil, a, false);
   }
-  __device__ __forceinline__ double right(double const (&a)[6]) const {
+  template <int N> __device__ __forceinline__ double right(double const (&a)[N]) const {
     return reconstruct(o.stencil, a, true);
   }
-  __device__ __forceinline__ void pair(double const (&a)[6], double &l, double &r) const {
+  template <int N>
+  __device__ __forceinline__ void pair(double const (&a)[N], double &l, double &r) const {
     l = left(a);
     r = right(a);
   }
-  __device__ __forceinline__ void two(double const (&a)[6], double const (&b)[6], double &l,
+  template <int N>
+  __device__ __forceinline__ void two(double const (&a)[N], double const (&b)[N], double &l,
                                       double &r) const {
     l = left(a);
     r = right(b);

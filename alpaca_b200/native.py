@@ -18,6 +18,7 @@ ALP_OK, ALP_ERR_INVALID, ALP_ERR_CUDA, ALP_ERR_CAPACITY, ALP_ERR_NOT_FOUND, ALP_
 FLUX_SPLITTING, FINITE_VOLUME = 0, 1
 RECON_CONSERVATIVE, RECON_PRIMITIVE, RECON_CHARACTERISTIC = 0, 1, 2
 STENCIL_FIRST_ORDER, STENCIL_WENO3, STENCIL_WENO5, STENCIL_WENO5Z, STENCIL_TENO5 = 0, 1, 4, 7, 11
+STENCIL_WENO7 = 13
 RIEMANN_HLLC, RIEMANN_HLLC_LM, RIEMANN_HLL = 0, 1, 2
 SIGNAL_SPEED_EINFELDT, SIGNAL_SPEED_DAVIS, SIGNAL_SPEED_TORO, SIGNAL_SPEED_ARITHMETIC = 0, 1, 2, 3
 FLUX_SPLITTING_ROE, FLUX_SPLITTING_LLF, FLUX_SPLITTING_GLF = 0, 1, 2
@@ -65,6 +66,15 @@ EXT_SCHEMES = {
     "rk2_fs_llfm_weno5z": ("fsroe", {"reconstruction_stencil": STENCIL_WENO5Z,
                                      "flux_splitting": FLUX_SPLITTING_LLF_M,
                                      "time_integrator": RK2}),
+    # WENO7 (8-cell stencils)
+    "fvchar_weno7": ("fvchar", {"reconstruction_stencil": STENCIL_WENO7}),
+    "fs_roem_weno7": ("fsroe", {"reconstruction_stencil": STENCIL_WENO7,
+                                "flux_splitting": FLUX_SPLITTING_ROE_M}),
+    "rk2_fvchar_weno7": ("fvchar", {"reconstruction_stencil": STENCIL_WENO7,
+                                    "time_integrator": RK2}),
+    "rk2_fs_glf_weno7": ("fsroe", {"reconstruction_stencil": STENCIL_WENO7,
+                                   "flux_splitting": FLUX_SPLITTING_GLF, "time_integrator": RK2}),
+    "rk2_fs_weno7": ("fsroe", {"reconstruction_stencil": STENCIL_WENO7, "time_integrator": RK2}),
 }
 FP64, FP32_FLUX = 0, 1
 HALO_ALL, HALO_FACES = 0, 1

@@ -42,13 +42,15 @@ enum {
  * user_specifications/ selects the same combination:
  *   convective_term_solver   riemann_solver_settings.h:28  (FluxSplitting=0, FiniteVolume=1)
  *   state_reconstruction     state_reconstruction_settings.h:25 (Conservative=0, Primitive=1, Characteristic=2)
- *   reconstruction_stencil   stencil_setup.h:26-43 (FirstOrder=0, WENO3=1, WENO5=4, WENO5Z=7, TENO5=11)
+ *   reconstruction_stencil   stencil_setup.h:26-43 (FirstOrder=0, WENO3=1, WENO5=4, WENO5Z=7, TENO5=11,
+ *                                                  WENO7=13)
  *   riemann_solver           riemann_solver_settings.h:47 (Hllc=0, Hllc_LM=1, Hll=2)
  *   signal_speed             enums/signal_speed.h:31 (Einfeldt=0, Davis=1, Toro=2, Arithmetic=3)
  *   flux_splitting           enums/flux_splitting.h:31 (Roe=0, LLF=1, GLF=2, Roe_M=3, LLF_M=4)
  *   time_integrator          numerical_setup.h:26 (RK2=0, RK3=1)
  * Supported: FiniteVolume + {Primitive, Characteristic} reconstruction with
- * the stencils FirstOrder, WENO3, WENO5, WENO5Z or TENO5, the Riemann solvers
+ * the stencils FirstOrder, WENO3, WENO5, WENO5Z, TENO5 or WENO7 (8-cell
+ * stencils; not in multi-level cases), the Riemann solvers
  * Hllc, Hllc_LM or Hll and the signal speeds Einfeldt, Davis, Toro or
  * Arithmetic; FluxSplitting with Roe, LocalLaxFriedrichs, GlobalLaxFriedrichs,
  * Roe_M or LocalLaxFriedrichs_M and the same stencils; RK3, or RK2 (TVD, two
@@ -73,7 +75,8 @@ enum {
   ALP_STENCIL_WENO3 = 1,
   ALP_STENCIL_WENO5 = 4,
   ALP_STENCIL_WENO5Z = 7,
-  ALP_STENCIL_TENO5 = 11
+  ALP_STENCIL_TENO5 = 11,
+  ALP_STENCIL_WENO7 = 13
 };
 enum { ALP_RIEMANN_HLLC = 0, ALP_RIEMANN_HLLC_LM = 1, ALP_RIEMANN_HLL = 2 };
 enum {

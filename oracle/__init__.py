@@ -40,7 +40,7 @@ VARIANTS = {
 
 # Further selections: name -> (base variant, (stencil, riemann solver, signal
 # speed, flux splitting)) with the values of the reference's enums.
-WENO5, WENO5Z, TENO5, WENO3, FIRST_ORDER = 4, 7, 11, 1, 0
+WENO5, WENO5Z, TENO5, WENO3, FIRST_ORDER, WENO7 = 4, 7, 11, 1, 0, 13
 HLLC, HLLC_LM, HLL = 0, 1, 2
 EINFELDT, DAVIS, TORO, ARITHMETIC = 0, 1, 2, 3
 ROE, LLF, GLF, ROE_M, LLF_M = 0, 1, 2, 3, 4
@@ -78,6 +78,12 @@ EXT_VARIANTS = {
     "rk2_fs_roem_weno3": ("fsroe", (WENO3, HLLC, EINFELDT, ROE_M, RK2)),
     "rk2_fs_llfm": ("fsroe", (WENO5, HLLC, EINFELDT, LLF_M, RK2)),
     "rk2_fs_llfm_weno5z": ("fsroe", (WENO5Z, HLLC, EINFELDT, LLF_M, RK2)),
+    # WENO7 (8-cell stencils) and the WENO7 rows of the DetailedSod table
+    "fvchar_weno7": ("fvchar", (WENO7, HLLC, EINFELDT, ROE)),
+    "fs_roem_weno7": ("fsroe", (WENO7, HLLC, EINFELDT, ROE_M)),
+    "rk2_fvchar_weno7": ("fvchar", (WENO7, HLLC, EINFELDT, ROE, RK2)),
+    "rk2_fs_glf_weno7": ("fsroe", (WENO7, HLLC, EINFELDT, GLF, RK2)),
+    "rk2_fs_weno7": ("fsroe", (WENO7, HLLC, EINFELDT, ROE, RK2)),
 }
 
 

@@ -209,7 +209,9 @@ static inline double weno5_right(const double *a) { return weno5(a, 1, -1); }
 /* ---- further selections of the plugin surface (enum values of the
  * reference: stencil_setup.h:26-43, riemann_solver_settings.h:47,
  * enums/signal_speed.h:31, enums/flux_splitting.h:31) -------------------- */
-enum { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11 };
+enum { ST_FIRST_ORDER = 0, ST_WENO3 = 1, ST_WENO5 = 4, ST_WENO5Z = 7, ST_TENO5 = 11,
+       ST_WENO7 = 13 };
+#define MAXW 8 /* widest stencil: WENO7, cells i-3 .. i+4 */
 enum { RS_HLLC = 0, RS_HLLC_LM = 1, RS_HLL = 2 };
 enum { SS_EINFELDT = 0, SS_DAVIS = 1, SS_TORO = 2, SS_ARITHMETIC = 3 };
 enum { FSP_ROE = 0, FSP_LLF = 1, FSP_GLF = 2, FSP_ROE_M = 3, FSP_LLF_M = 4 };
@@ -300,10 +302,61 @@ static double weno3(const double *a, int offset, int sign) {
   return w1 * (-1.0 / 2.0 * v1 + 3.0 / 2.0 * v2) + w2 * (1.0 / 2.0 * v2 + 1.0 / 2.0 * v3);
 }
 
+/* WENO7-JS (stencils/spatial_reconstruction_stencils/weno7.h:21-212; the
+ * coefficients of Balsara & Shu 2000): a[0..7] are cells i-3..i+4 around face
+ * i+1/2 (downstream stencil size 3), eps 1e-10. */
+static double weno7(const double *a, int offset, int sign) {
+  double const v1 = a[3 + offset - 3 * sign];
+  double const v2 = a[3 + offset - 2 * sign];
+  double const v3 = a[3 + offset - 1 * sign];
+  double const v4 = a[3 + offset];
+  double const v5 = a[3 + offset + 1 * sign];
+  double const v6 = a[3 + offset + 2 * sign];
+  double const v7 = a[3 + offset + 3 * sign];
+  double const s11 = 547.0 * v1 + -3882.0 * v2 + 4642.0 * v3 + -1854.0 * v4;
+  double const s12 = 7043.0 * v2 + -17246.0 * v3 + 7042.0 * v4;
+  double const s13 = 11003.0 * v3 + -9402.0 * v4;
+  double const s14 = 2107.0 * v4;
+  double const s1 = v1 * s11 + v2 * s12 + v3 * s13 + v4 * s14;
+  double const s21 = 267.0 * v2 + -1642.0 * v3 + 1602.0 * v4 + -494.0 * v5;
+  double const s22 = 2843.0 * v3 + -5966.0 * v4 + 1922.0 * v5;
+  double const s23 = 3443.0 * v4 + -2522.0 * v5;
+  double const s24 = 547.0 * v5;
+  double const s2 = v2 * s21 + v3 * s22 + v4 * s23 + v5 * s24;
+  double const s31 = 547.0 * v3 + -2522.0 * v4 + 1922.0 * v5 + -494.0 * v6;
+  double const s32 = 3443.0 * v4 + -5966.0 * v5 + 1602.0 * v6;
+  double const s33 = 2843.0 * v5 + -1642.0 * v6;
+  double const s34 = 267.0 * v6;
+  double const s3 = v3 * s31 + v4 * s32 + v5 * s33 + v6 * s34;
+  double const s41 = 2107.0 * v4 + -9402.0 * v5 + 7042.0 * v6 + -1854.0 * v7;
+  double const s42 = 11003.0 * v5 + -17246.0 * v6 + 4642.0 * v7;
+  double const s43 = 7043.0 * v6 + -3882.0 * v7;
+  double const s44 = 547.0 * v7;
+  double const s4 = v4 * s41 + v5 * s42 + v6 * s43 + v7 * s44;
+  double const eps = 1.0e-10;
+  double const a1 = (1.0 / 35.0) / ((s1 + eps) * (s1 + eps));
+  double const a2 = (12.0 / 35.0) / ((s2 + eps) * (s2 + eps));
+  double const a3 = (18.0 / 35.0) / ((s3 + eps) * (s3 + eps));
+  double const a4 = (4.0 / 35.0) / ((s4 + eps) * (s4 + eps));
+  double const one_a_sum = 1.0 / (a1 + a2 + a3 + a4);
+  double const w1 = a1 * one_a_sum, w2 = a2 * one_a_sum, w3 = a3 * one_a_sum,
+               w4 = a4 * one_a_sum;
+  return w1 * (-3.0 / 12.0 * v1 + 13.0 / 12.0 * v2 + -23.0 / 12.0 * v3 + 25.0 / 12.0 * v4) +
+         w2 * (1.0 / 12.0 * v2 + -5.0 / 12.0 * v3 + 13.0 / 12.0 * v4 + 3.0 / 12.0 * v5) +
+         w3 * (-1.0 / 12.0 * v3 + 7.0 / 12.0 * v4 + 7.0 / 12.0 * v5 + -1.0 / 12.0 * v6) +
+         w4 * (3.0 / 12.0 * v4 + 13.0 / 12.0 * v5 + -5.0 / 12.0 * v6 + 1.0 / 12.0 * v7);
+}
+
+/* Cells of the selected stencil around face i+1/2 (the reference's
+ * stencil_size_): 8 for WENO7 (cell i at index 3), else 6 (cell i at 2). */
+static int stencil_width(void) { return g_stencil == ST_WENO7 ? 8 : 6; }
+
 /* SU::Reconstruction with the selected stencil (stencils/stencil_utilities.h),
- * UpwindLeft {0, 1} / UpwindRight {1, -1}; FirstOrder returns cell i / i+1. */
+ * UpwindLeft {0, 1} / UpwindRight {1, -1}; FirstOrder returns cell i / i+1.
+ * a holds stencil_width() cells. */
 static double recon(const double *a, int offset, int sign) {
   switch (g_stencil) {
+    case ST_WENO7: return weno7(a, offset, sign);
     case ST_WENO5Z: return weno5z(a, offset, sign);
     case ST_TENO5: return teno5(a, offset, sign);
     case ST_WENO3: return weno3(a, offset, sign);
@@ -739,16 +792,17 @@ static void fv_fluxes(const Geom *g, const Eos *e, int recon, int dir,
     for (int j = lo[1]; j <= hi[1]; ++j)
       for (int k = lo[2]; k <= hi[2]; ++k) {
         long const fi = fidx(g, i - off[0], j - off[1], k - off[2]);
-        long cells6[6];
-        for (int m = 0; m < 6; ++m) {
-          int const s = m - 2;
+        int const W = stencil_width(), D = W / 2 - 1;
+        long cells6[MAXW];
+        for (int m = 0; m < W; ++m) {
+          int const s = m - D;
           cells6[m] = cidx(g, i + (dir == 0) * s, j + (dir == 1) * s, k + (dir == 2) * s);
         }
         double cm[MAXNE], cp[MAXNE], pm[MAXNE], pp[MAXNE];
         if (recon == ORACLE_RECON_CHARACTERISTIC) {
-          double chm[MAXNE], chp[MAXNE], uc[6];
+          double chm[MAXNE], chp[MAXNE], uc[MAXW];
           for (int n = 0; n < ne; ++n) {
-            for (int m = 0; m < 6; ++m) {
+            for (int m = 0; m < W; ++m) {
               uc[m] = 0.0;
               for (int s = 0; s < ne; ++s) {
                 int const l = seq[s];
@@ -764,9 +818,9 @@ static void fv_fluxes(const Geom *g, const Eos *e, int recon, int dir,
           cons_to_prim(e, cm, pm);
           cons_to_prim(e, cp, pp);
         } else {
-          double arr[6];
+          double arr[MAXW];
           for (int n = 0; n < np; ++n) {
-            for (int m = 0; m < 6; ++m) arr[m] = p[n * C + cells6[m]];
+            for (int m = 0; m < W; ++m) arr[m] = p[n * C + cells6[m]];
             pm[n] = recon_left(arr);
             pp[n] = recon_right(arr);
           }
@@ -809,15 +863,16 @@ static void fs_fluxes(const Geom *g, int dir, const double *u, const double *adv
     for (int j = lo[1]; j <= hi[1]; ++j)
       for (int k = lo[2]; k <= hi[2]; ++k) {
         long const fi = fidx(g, i - off[0], j - off[1], k - off[2]);
-        long cells6[6];
-        for (int m = 0; m < 6; ++m) {
-          int const s = m - 2;
+        int const W = stencil_width(), D = W / 2 - 1;
+        long cells6[MAXW];
+        for (int m = 0; m < W; ++m) {
+          int const s = m - D;
           cells6[m] = cidx(g, i + (dir == 0) * s, j + (dir == 1) * s, k + (dir == 2) * s);
         }
-        double chf[MAXNE], pos[6], neg[6], phys[MAXNE];
+        double chf[MAXNE], pos[MAXW], neg[MAXW], phys[MAXNE];
         for (int n = 0; n < ne; ++n) {
           double const alpha = eig[fi].ev[n];
-          for (int m = 0; m < 6; ++m) {
+          for (int m = 0; m < W; ++m) {
             pos[m] = 0.0;
             neg[m] = 0.0;
             for (int s = 0; s < ne; ++s) {
@@ -1778,7 +1833,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
 /* Selects stencil, Riemann solver, signal speed and flux splitting (values of
  * the reference's enums); 1 for an unknown value. */
 int oracle_set_options(int stencil, int riemann, int signal, int splitting) {
-  if (stencil != ST_WENO5 && stencil != ST_WENO5Z && stencil != ST_TENO5 &&
+  if (stencil != ST_WENO5 && stencil != ST_WENO5Z && stencil != ST_TENO5 && stencil != ST_WENO7 &&
       stencil != ST_WENO3 && stencil != ST_FIRST_ORDER)
     return 1;
   if (riemann < RS_HLLC || riemann > RS_HLL) return 1;

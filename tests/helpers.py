@@ -80,6 +80,14 @@ SOD_REFERENCE_NORMS = {
                          5.45096592e-05, 3.08180236e-05, 2.97142519e-05), 2),
     "rk2_fs_llfm_weno5z": (82, (1.28201009e-06, 3.86170496e-07, 1.92486130e-07,
                                 1.12651026e-06, 4.31014301e-07, 3.36644260e-07), 6),
+    "fs_roem_weno7": (26, (5.41078087e-07, 1.78701534e-07, 1.18724621e-07,
+                           4.74130387e-07, 2.22922105e-07, 2.03218512e-07), 8),
+    "rk2_fvchar_weno7": (18, (4.53331444e-05, 1.84825089e-05, 1.64356637e-05,
+                              5.15861558e-05, 2.92978943e-05, 2.83574250e-05), 2),
+    "rk2_fs_glf_weno7": (38, (4.94093395e-05, 1.98145425e-05, 1.74995495e-05,
+                              5.98894516e-05, 3.19034136e-05, 3.04606609e-05), 2),
+    "rk2_fs_weno7": (54, (1.48258118e-06, 4.43012783e-07, 3.01900864e-07,
+                          1.45519660e-06, 5.83116890e-07, 5.16433858e-07), 6),
 }
 
 

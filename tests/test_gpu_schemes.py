@@ -10,6 +10,16 @@ low-Mach splittings on a fluid at rest, against the largest field's scale);
 runs per field L1 <= 1e-10. The strict build is bit-exact except
 where the reference calls std::pow (Toro signal speeds) or std::sin (HLLC-LM),
 whose CUDA versions may differ in the last bit: there <= 1e-13.
+
+WENO7's smoothness indicators are quadratic forms with coefficients up to
+17246 that cancel on smooth data; the fast build's fused multiply-adds round
+them differently, and the nonlinear weights amplify that to a few 1e-12 of the
+flux. Its fast-build RHS bound is 2e-11 (the strict build stays bit-exact).
+Its epsilon is 1e-10, against a rounding residue of the indicators near 1e-12
+on flat data, so over a whole Sod run those differences move the weights by up
+to a percent in nearly flat regions (more under Roe-M, which does not damp a
+fluid at rest): fast runs <= 1e-6 in L1, and the strict build's run is held to
+the reference's final state at <= 1e-12.
 """
 import os
 
@@ -30,6 +40,14 @@ EXT = list(N.EXT_SCHEMES)
 LIBM = {"fvchar_toro": "pow", "fvchar_hllclm": "sin"}
 
 
+def rhs_tol(variant):
+    return 2e-11 if "weno7" in variant else RHS_TOL
+
+
+def run_tol(variant):
+    return 1e-6 if "weno7" in variant else RUN_TOL
+
+
 def to_dev(a, dev):
     import torch
     return torch.from_numpy(np.ascontiguousarray(a)).to(dev)
@@ -45,14 +63,15 @@ def test_ext_fluxes_and_rhs_match_oracle(cuda, dim, variant):
     fx, fy, fz, rhs = oracle.Restatement(dim, variant).space_rhs(u, case.gamma, 0.0, False, h)
     ud = to_dev(u, cuda)
     f = api.convective_fluxes(ud, dim, variant, mat, h)
+    tol = rhs_tol(variant)
     for d, ref in enumerate((fx, fy, fz)[:dim]):
-        assert field_rel_err(f[d].cpu().numpy(), ref).max() <= RHS_TOL, d
+        assert field_rel_err(f[d].cpu().numpy(), ref).max() <= tol, d
     r = api.space_rhs(ud, dim, variant, mat, h).cpu().numpy()
     I = cases.interior(dim)
-    assert field_rel_err(r[I], rhs[I]).max() <= RHS_TOL
+    assert field_rel_err(r[I], rhs[I]).max() <= tol
     if dim != 2:
         z = np.load(os.path.join(GOLDEN, f"rhs_d{dim}_{variant}.npz"))
-        assert field_rel_err(r[I], z["rhs"]).max() <= RHS_TOL
+        assert field_rel_err(r[I], z["rhs"]).max() <= tol
 
 
 @pytest.mark.parametrize("variant", EXT)
@@ -70,20 +89,32 @@ def test_ext_strict_build(cuda, variant):
         assert np.array_equal(r[I], rhs[I])
 
 
-@pytest.mark.parametrize("variant", EXT)
-def test_ext_engine_sod_matches_reference(cuda, variant):
-    """1D Sod to t = 0.2 in the engine against the reference's run."""
+def engine_sod(variant, strict=False):
     case = cases.sod_1d()
     z = np.load(os.path.join(GOLDEN, f"sod1d_{variant}.npz"))
-    eng = api.Engine(1, variant, capacity_blocks=case.grid.nb, max_cases=1)
+    eng = api.Engine(1, variant, capacity_blocks=case.grid.nb, max_cases=1, strict=strict)
     cid = eng.add_case(case)
     eng.run_to_end(chunk=50)
     got, t, steps = eng.get(cid)
     eng.close()
     assert steps == int(z["steps"]) and t == pytest.approx(float(z["t"]), rel=1e-14)
-    g = got[cases.interior(1)]
+    return got[cases.interior(1)], z["final"]
+
+
+@pytest.mark.parametrize("variant", EXT)
+def test_ext_engine_sod_matches_reference(cuda, variant):
+    """1D Sod to t = 0.2 in the engine against the reference's run."""
+    g, ref = engine_sod(variant)
     for f in range(3):
-        assert l1_rel(g[:, f], z["final"][:, f]) <= RUN_TOL, f
+        assert l1_rel(g[:, f], ref[:, f]) <= run_tol(variant), f
+
+
+@pytest.mark.parametrize("variant", [v for v in EXT if "weno7" in v])
+def test_weno7_strict_engine_sod_matches_reference(cuda, variant):
+    """The strict build's WENO7 Sod runs against the reference's runs."""
+    g, ref = engine_sod(variant, strict=True)
+    for f in range(3):
+        assert l1_rel(g[:, f], ref[:, f]) <= 1e-12, f
 
 
 @pytest.mark.parametrize("variant", ["fvchar_teno5", "fvchar_hll", "fs_llf", "fs_roem"])

@@ -7,7 +7,11 @@ Grids as in test_sod_exact.py (symmetry walls; SSP-RK3 and TVD-RK2 rows).
 Tolerances: the strict build reproduces the oracle bit for bit, so its norms
 meet the table's 9 digits (<= 1e-8 relative); the fast build's runs differ by
 <= 1e-10 relative in L1, which moves norms of errors near 1e-2 per cell by
-<= 1e-7 relative.
+<= 1e-7 relative. WENO7 is the exception: its epsilon is 1e-10 and its
+smoothness indicators cancel to a rounding residue near 1e-12 on flat data, so
+the fast build's fused multiply-adds move its nonlinear weights by up to a
+percent wherever the flow is nearly flat; its fast runs differ by <= 1e-6 in
+L1 and its norms by <= 1e-6 relative (the strict build still meets 1e-8).
 """
 import numpy as np
 import pytest
@@ -30,5 +34,5 @@ def test_engine_sod_norms_match_reference_table(cuda, variant, strict):
     eng.close()
     assert t == pytest.approx(case.t_end, rel=1e-14)
     got = sod_error_norms(case, u, t)
-    tol = 1e-8 if strict else 1e-7
+    tol = 1e-8 if strict else (1e-6 if "weno7" in variant else 1e-7)
     assert np.max(np.abs(got / np.array(ref) - 1.0)) <= tol, (variant, line, got)

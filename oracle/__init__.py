@@ -133,6 +133,18 @@ class _Common:
         return (nb, self.ne) + tc, (nb, self.ne) + tuple(n + 1 for n in ic)
 
 
+def _prediction(fn, parent, octant, start, count, child):
+    parent = np.ascontiguousarray(parent, dtype=np.float64)
+    child = np.zeros_like(parent) if child is None else np.ascontiguousarray(child, dtype=np.float64)
+    st = np.zeros(3, dtype=np.int32)
+    ct = np.zeros(3, dtype=np.int32)
+    st[:len(start)] = start
+    ct[:len(count)] = count
+    if fn(_dp(parent), int(octant), st.ctypes.data_as(_I), ct.ctypes.data_as(_I), _dp(child)):
+        raise ValueError("prediction: bad range")
+    return child
+
+
 def _load(path: str):
     """Loads a build of alpaca_oracle.c and declares its entry points."""
     lib = C.CDLL(path)
@@ -149,6 +161,7 @@ def _load(path: str):
                                C.c_double, C.c_int, C.c_double, C.c_double, C.c_double,
                                C.c_int, C.c_int, _D, _I, _D]
     lib.oracle_set_options.argtypes = [C.c_int] * 4
+    lib.oracle_prediction.argtypes = [C.c_int, _D, C.c_int, _I, _I, _D]
     lib.oracle_set_time_integrator.argtypes = [C.c_int]
     lib.oracle_levels_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, _I, _I,
                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
@@ -194,6 +207,12 @@ class Restatement(_Common):
         out = np.zeros(6)
         self.lib.oracle_eos(self.dim, gamma, B, int(safe), _dp(cons), _dp(prim), _dp(out))
         return out
+
+    def prediction(self, parent, octant, start, count, child=None):
+        """Multiresolution::Prediction of one field buffer (tc shape) into the
+        child cells start .. start + count of a child at position octant."""
+        return _prediction(lambda *a: self.lib.oracle_prediction(self.dim, *a),
+                           parent, octant, start, count, child)
 
     # -- block kernels --
     def prime_states(self, u, gamma, B=0.0, safe=False):
@@ -327,6 +346,7 @@ class Reference(_Common):
                                           _D, _D, _D, _D, C.c_int]
             lib.ref_run.argtypes = [_D, C.c_int, _I, C.c_double, C.c_double, C.c_int, C.c_double,
                                     C.c_double, C.c_double, C.c_int, C.c_int, _D, _I, _D]
+            lib.ref_prediction.argtypes = [_D, C.c_int, _I, _I, _D]
             Reference._libs[key] = lib
         self.lib = Reference._libs[key]
         vals = [C.c_int() for _ in range(5)]
@@ -340,6 +360,9 @@ class Reference(_Common):
         l, r = C.c_double(), C.c_double()
         self.lib.ref_weno5(_dp(v), C.byref(l), C.byref(r))
         return l.value, r.value
+
+    def prediction(self, parent, octant, start, count, child=None):
+        return _prediction(self.lib.ref_prediction, parent, octant, start, count, child)
 
     def eos(self, gamma, B, safe, cons, prim):
         cons = np.ascontiguousarray(cons, dtype=np.float64)

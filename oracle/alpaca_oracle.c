@@ -1474,6 +1474,137 @@ static double child_average(const Geom *g, const double *f, int i, int j, int k)
   return 0.125 * (0.5 * (mn + mx));
 }
 
+/* ConsistencyManagedSum of four values (mathematical_functions.h:115-125) */
+static double cms4(double a, double b, double c, double d) {
+  double const s1 = (a + b) + (c + d);
+  double const s2 = (a + c) + (b + d);
+  double const s3 = (a + d) + (b + c);
+  double mn = s1, mx = s1;
+  if (s2 < mn) mn = s2;
+  if (s3 < mn) mn = s3;
+  if (mx < s2) mx = s2;
+  if (mx < s3) mx = s3;
+  return 0.5 * (mn + mx);
+}
+
+/* Fifth-order prediction of the children of one parent cell
+ * (Multiresolution::Prediction, multiresolution.cpp:146-283, after Harten 1993).
+ * v: the parent values at offsets -2..2 around the cell, v[(a+2)*25 + (b+2)*5 +
+ * (c+2)] for offsets (a, b, c) along x, y, z (offsets of absent dimensions 0).
+ * out[o]: child o, bit d of o set for the high-index child along d. The terms
+ * and their evaluation order are the reference's: differences along one axis
+ * (Qx, Qy, Qz), pairs of axes (Qxy, Qxz, Qyz) and the consistency-managed
+ * triple term (Qxyz), combined per child with the child's signs. */
+#define PRED_V(a, b, c) v[((a) + 2) * 25 + ((b) + 2) * 5 + ((c) + 2)]
+static const double pc0 = -22.0 / 128.0, pc1 = 3.0 / 128.0;
+
+/* value at offset s along dimension d */
+static double pred_at1(const double *v, int d, int s) {
+  int o[3] = {0, 0, 0};
+  o[d] = s;
+  return PRED_V(o[0], o[1], o[2]);
+}
+
+/* value at offsets s along d and t along e */
+static double pred_at2(const double *v, int d, int s, int e, int t) {
+  int o[3] = {0, 0, 0};
+  o[d] = s;
+  o[e] = t;
+  return PRED_V(o[0], o[1], o[2]);
+}
+
+static double pred_q1(const double *v, int d) {
+  return pc0 * (pred_at1(v, d, 1) - pred_at1(v, d, -1)) +
+         pc1 * (pred_at1(v, d, 2) - pred_at1(v, d, -2));
+}
+
+/* one coefficient's cross difference: (v(+a,+b) + v(-a,-b)) - (v(-a,+b) + v(+a,-b)) */
+static double pred_x2(const double *v, int d, int e, int a, int b) {
+  return (pred_at2(v, d, a, e, b) + pred_at2(v, d, -a, e, -b)) -
+         (pred_at2(v, d, -a, e, b) + pred_at2(v, d, a, e, -b));
+}
+
+static double pred_q2(const double *v, int d, int e) {
+  double const c00 = pc0 * pc0, c01 = pc0 * pc1, c11 = pc1 * pc1;
+  return (c00 * pred_x2(v, d, e, 1, 1) + c11 * pred_x2(v, d, e, 2, 2)) +
+         (c01 * pred_x2(v, d, e, 1, 2) + c01 * pred_x2(v, d, e, 2, 1));
+}
+
+/* the four antisymmetric differences of offsets (a, b, c), summed consistently */
+static double pred_x3(const double *v, int a, int b, int c) {
+  return cms4(PRED_V(a, b, c) - PRED_V(-a, -b, -c), PRED_V(-a, -b, c) - PRED_V(a, b, -c),
+              PRED_V(a, -b, -c) - PRED_V(-a, b, c), PRED_V(-a, b, -c) - PRED_V(a, -b, c));
+}
+
+static double pred_q3(const double *v) {
+  double const c00 = pc0 * pc0, c11 = pc1 * pc1;
+  double const c000 = c00 * pc0, c001 = c00 * pc1, c011 = pc0 * c11, c111 = pc1 * c11;
+  return cms4(c000 * pred_x3(v, 1, 1, 1) + c111 * pred_x3(v, 2, 2, 2),
+              c001 * pred_x3(v, 1, 1, 2) + c011 * pred_x3(v, 2, 2, 1),
+              c011 * pred_x3(v, 1, 2, 2) + c001 * pred_x3(v, 2, 1, 1),
+              c001 * pred_x3(v, 1, 2, 1) + c011 * pred_x3(v, 2, 1, 2));
+}
+
+static void predict_children(int dim, const double *v, double out[8]) {
+  double qx = 0.0, qy = 0.0, qz = 0.0, qxy = 0.0, qxz = 0.0, qyz = 0.0, qxyz = 0.0;
+  qx = pred_q1(v, 0);
+  if (dim > 1) {
+    qy = pred_q1(v, 1);
+    qxy = pred_q2(v, 0, 1);
+  }
+  if (dim > 2) {
+    qz = pred_q1(v, 2);
+    qxz = pred_q2(v, 0, 2);
+    qyz = pred_q2(v, 1, 2);
+    qxyz = pred_q3(v);
+  }
+  double const p = PRED_V(0, 0, 0);
+  for (int o = 0; o < (1 << dim); ++o) {
+    double const sx = (o & 1) ? -1.0 : 1.0, sy = (o & 2) ? -1.0 : 1.0, sz = (o & 4) ? -1.0 : 1.0;
+    out[o] = p + dacms(dim, sx * qx, sy * qy, sz * qz) +
+             dacms(dim, sx * sy * qxy, sx * sz * qxz, sy * sz * qyz) + sx * sy * sz * qxyz;
+  }
+}
+
+/* Multiresolution::Prediction over a cell range of one field buffer: parent
+ * and child are [tc] buffers of one field; the child has position octant among
+ * its siblings; start / count give the child cells to fill (start even). */
+int oracle_prediction(int dim, const double *parent, int octant, const int *start,
+                      const int *count, double *child) {
+  if (dim < 1 || dim > 3) return 1;
+  Geom const gg = make_geom(dim);
+  Geom const *g = &gg;
+  int ps[3], pn[3];
+  for (int d = 0; d < 3; ++d) {
+    if (d < dim && (start[d] % 2 || count[d] % 2)) return 1;
+    int const off = ((octant >> d) & 1) ? g->tc[0] / 2 - HS / 2 : HS / 2;
+    ps[d] = d < dim ? start[d] / 2 + off : 0;
+    pn[d] = d < dim ? count[d] / 2 : 1;
+  }
+  double v[125];
+  for (int i = 0; i < pn[0]; ++i)
+    for (int j = 0; j < pn[1]; ++j)
+      for (int k = 0; k < pn[2]; ++k) {
+        int const c[3] = {ps[0] + i, ps[1] + j, ps[2] + k};
+        for (int a = -2; a <= 2; ++a)
+          for (int b = -2; b <= 2; ++b)
+            for (int e = -2; e <= 2; ++e) {
+              int const q[3] = {c[0] + a, c[1] + (dim > 1 ? b : 0), c[2] + (dim > 2 ? e : 0)};
+              int inside = 1;
+              for (int d = 0; d < dim; ++d) inside &= q[d] >= 0 && q[d] < g->tc[d];
+              PRED_V(a, b, e) = inside ? parent[cidx(g, q[0], q[1], q[2])] : 0.0;
+            }
+        double out[8];
+        predict_children(dim, v, out);
+        for (int o = 0; o < (1 << dim); ++o) {
+          int x[3] = {0, 0, 0};
+          for (int d = 0; d < dim; ++d) x[d] = start[d] + 2 * (d == 0 ? i : d == 1 ? j : k) + ((o >> d) & 1);
+          child[cidx(g, x[0], x[1], x[2])] = out[o];
+        }
+      }
+  return 0;
+}
+
 /* Face halos (HS layers over the interior extent) of leaf b in pool dst; the
  * neighbours' values come from src[level] (a pool per level). */
 static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double *const *src) {

@@ -75,6 +75,10 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb,
  * stepping over macro steps of 2^lmax micro steps; dt_log receives every
  * micro time step. Returns 0, or 4 (leaves do not tile the box) or 5 (face
  * neighbours more than one level apart). */
+/* Multiresolution::Prediction (multiresolution.cpp:146-283) of one field
+ * buffer [tc] into a child's cells start .. start + count (even numbers). */
+int oracle_prediction(int dim, const double *parent, int octant, const int *start,
+                      const int *count, double *child);
 int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf,
                       const int *level, const int *coord, const int *n0, double h0,
                       double gamma, double B, int safe, double cfl, double t_end,

@@ -32,6 +32,7 @@
 #include "materials/equations_of_state/stiffened_gas.h"
 #include "materials/equations_of_state/stiffened_gas_safe.h"
 #include "materials/material_manager.h"
+#include "multiresolution/multiresolution.h"
 #include "prime_states/prime_state_handler.h"
 #include "solvers/convective_term_contributions/convective_term_solver_setup.h"
 #include "solvers/eigendecomposition.h"
@@ -375,6 +376,28 @@ int ref_weno5(double const *v, double *left, double *right) {
     a[i] = v[i];
   *left = SU::Reconstruction<WENO5, SP::UpwindLeft>(a, 1.0);
   *right = SU::Reconstruction<WENO5, SP::UpwindRight>(a, 1.0);
+  return 0;
+}
+
+// Multiresolution::Prediction (multiresolution.cpp:146-283) of one field:
+// parent and child are full [TCX][TCY][TCZ] buffers; octant is the child's
+// position among its siblings (bit 0 x, bit 1 y, bit 2 z); start and count
+// give the child cells to fill, as the reference's halo managers pass them.
+int ref_prediction(double const *parent, int octant, int const *start, int const *count,
+                   double *child) {
+  using Buf = double[CC::TCX()][CC::TCY()][CC::TCZ()];
+  nid_t child_id = 0;
+  bool found = false;
+  for (nid_t const id : IdsOfChildren(IdSeed()))
+    if (int(PositionOfNodeAmongSiblings(id)) == octant) {
+      child_id = id;
+      found = true;
+    }
+  if (!found) return 1;
+  Multiresolution::Prediction(*reinterpret_cast<Buf const *>(parent),
+                              *reinterpret_cast<Buf *>(child), child_id,
+                              unsigned(start[0]), unsigned(count[0]), unsigned(start[1]),
+                              unsigned(count[1]), unsigned(start[2]), unsigned(count[2]));
   return 0;
 }
 

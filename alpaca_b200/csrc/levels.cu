@@ -20,12 +20,19 @@
 // Jumps: the face kernels gather stencil cells from a neighbour block's
 // interior. Where the face neighbour of a leaf is one level coarser or finer,
 // the neighbour slot is a ghost block: a virtual node of the leaf's level whose
-// three cell layers next to the shared face are filled before each stage, by
-// injection from the coarser leaf, or by averaging the finer leaves with
-// Multiresolution::Average (multiresolution.h:94-166); the reference predicts
-// the finer side with a fifth-order interpolation (Multiresolution::Prediction,
-// multiresolution.cpp:146), which is not done here. Face neighbours may differ
-// by one level at most.
+// three cell layers next to the shared face are filled before each stage. On
+// the coarse side they average the finer leaves (Multiresolution::Average,
+// multiresolution.h:94-166); on the fine side they are the fifth-order
+// prediction from the coarser level (Multiresolution::Prediction,
+// multiresolution.cpp:146-283), which is what the reference's jump halos hold
+// (InternalHaloManager::UpdateMaterialJumpNoMpi, internal_halo_manager.cpp:
+// 230-290, predicting from the parent's buffer: its interior the average of
+// its children, its halos its neighbours' cells). The prediction reads two
+// parent-level cells around each parent cell, so the parent position's
+// neighbours that are not leaves become ghosts filled whole: averages of their
+// children, or predictions from one level coarser still. Averaged ghosts are
+// filled finest level first, predicted ones coarsest first. Face neighbours may
+// differ by one level at most.
 //
 // Conservation at jumps as in the reference: after each stage update the
 // leaves integrate their jump-face fluxes with the RK3 jump multipliers times
@@ -65,14 +72,23 @@ struct LevelState {
   int macro, max_macro, micro, active, status, pad;
 };
 
-// A ghost block: type 0 takes its cells from the coarser leaf src[0]
-// (octant bits src[1]), type 1 averages the finer leaves src[o] (child o has
-// x in bit 0, y in bit 1, z in bit 2; -1 where a child is not a leaf). Only
-// the cell layers next to the faces in `faces` (bits W, E, S, N, B, T) are
-// read by neighbours and filled.
+// A ghost block: a node position of a leaf's level that is not a leaf, filled
+// before every stage in which a block reading it computes. Type 1 (a refined
+// node): the average of its children src[o] (child o has x in bit 0, y in bit
+// 1, z in bit 2; Multiresolution::Average). Type 0 (inside a coarser leaf): the
+// fifth-order prediction from the parent level (Multiresolution::Prediction),
+// which reads the 3^dim nodes nb[] around the parent position q (nb index
+// (dx+1)*9 + (dy+1)*3 + (dz+1); cells beyond the domain take the value of the
+// nearest domain cell, zero gradient); oct is the ghost's octant in its parent.
+// A ghost the face kernels read fills the three cell layers next to each face
+// in `faces` (bits W, E, S, N, B, T); a ghost other ghosts read is filled whole
+// (`full`). Slots below nleaf are leaves, read from the pool of their level.
+// gate: the finest level whose computing needs the ghost.
 struct GhostRec {
-  int slot, type, level, src_level, faces;
+  int slot, type, level, gate, faces, full, oct;
+  int q[3], ext[3];  // parent position (nodes) and level extent (cells) of the parent level
   int src[8];
+  int nb[27];
 };
 
 __device__ __forceinline__ double ghost_average3(double a0, double a1, double a2, double a3,
@@ -91,67 +107,219 @@ __device__ __forceinline__ double ghost_average3(double a0, double a1, double a2
   return 0.125 * (0.5 * (mn + mx));
 }
 
+// The pool a slot's cells are read from in this stage.
+__device__ __forceinline__ double const *ghost_source(int slot, int nleaf, int leaf_level,
+                                                      double const *Ug, double const *UA,
+                                                      CaseState const *cu, int stage) {
+  if (slot >= nleaf) return Ug;
+  return (stage > 0 && cu[leaf_level].dt > 0.0) ? Ug : UA;
+}
+
+// The cells a part of the fill covers: part < 2 DIM, the three layers next to
+// face part (if served); part == 2 DIM, the whole block (if full).
+template <int DIM>
+__device__ __forceinline__ bool ghost_part(GhostRec const &g, int part, int lo[3], int hi[3]) {
+  bool const whole = part == 2 * DIM;
+  if (whole ? !g.full : (g.full || !((g.faces >> part) & 1))) return false;
+  for (int e = 0; e < 3; ++e) {
+    lo[e] = 0;
+    hi[e] = e < DIM ? IC : 1;
+  }
+  if (!whole) {
+    int const d = part / 2;
+    lo[d] = (part & 1) ? IC - 3 : 0;
+    hi[d] = lo[d] + 3;
+  }
+  return true;
+}
+
+// Type 1 ghosts of one level: averages of the children.
 template <int DIM>
 __global__ void __launch_bounds__(256)
-ghost_fill_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
-                  double const *Us, CaseState const *__restrict__ gate,
-                  CaseState const *__restrict__ cu, int stage) {
+ghost_average_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
+                     int nleaf, CaseState const *__restrict__ gate,
+                     CaseState const *__restrict__ cu, int stage) {
   using G = Geo<DIM>;
-  GhostRec const g = ghosts[blockIdx.x];
-  int const f = blockIdx.y;
-  if (!((g.faces >> f) & 1)) return;
-  if (!(gate[g.level].dt > 0.0)) return;  // no leaf reading this ghost computes now
-  double const *src = (stage > 0 && cu[g.src_level].dt > 0.0) ? Us : UA;
-  int const d = f / 2, high = f % 2;
-  constexpr int T1 = DIM > 1 ? IC : 1, T2 = DIM > 2 ? IC : 1;
-  int const count = 3 * T1 * T2;
+  GhostRec const &g = ghosts[blockIdx.x];
+  int lo[3], hi[3];
+  if (!ghost_part<DIM>(g, blockIdx.y, lo, hi)) return;
+  if (!(gate[g.gate].dt > 0.0)) return;  // no block reading this ghost computes now
+  int const n1 = hi[1] - lo[1], n2 = hi[2] - lo[2];
+  int const count = (hi[0] - lo[0]) * n1 * n2;
   double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
   for (int t = threadIdx.x; t < count; t += blockDim.x) {
-    // slab cell (layer, transverse 1, transverse 2) -> node cell a[3]
-    int const layer = t / (T1 * T2), r = t % (T1 * T2);
-    int a[3] = {0, 0, 0};
-    int const tr[2] = {r / T2, r % T2};
-    int q = 0;
-    for (int e = 0; e < DIM; ++e) {
-      if (e == d) a[e] = high ? IC - 3 + layer : layer;
-      else a[e] = tr[q++];
-    }
+    int const a[3] = {lo[0] + t / (n1 * n2), lo[1] + (t / n2) % n1, lo[2] + t % n2};
     int const x = G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2));
-    if (g.type == 0) {
-      int c[3] = {0, 0, 0};
-      for (int e = 0; e < DIM; ++e) c[e] = (IC / 2) * ((g.src[1] >> e) & 1) + a[e] / 2;
-      double const *sb = src + (size_t)g.src[0] * G::BLOCK_DOUBLES;
-      int const y = G::cell(c[0] + G::fic(0), c[1] + G::fic(1), c[2] + G::fic(2));
+    int o = 0, c[3] = {0, 0, 0};
+    for (int e = 0; e < DIM; ++e) {
+      o |= (a[e] / (IC / 2)) << e;
+      c[e] = 2 * (a[e] % (IC / 2)) + G::fic(e);
+    }
+    int const child = g.src[o];
+    if (child < 0) continue;  // never read: the host checks face children are leaves
+    double const *sb =
+        ghost_source(child, nleaf, g.level + 1, Ug, UA, cu, stage) + (size_t)child * G::BLOCK_DOUBLES;
 #pragma unroll
-      for (int e = 0; e < G::NE; ++e) dst[e * G::CELLS + x] = sb[e * G::CELLS + y];
-    } else {
-      int o = 0, c[3] = {0, 0, 0};
-      for (int e = 0; e < DIM; ++e) {
-        o |= (a[e] / (IC / 2)) << e;
-        c[e] = 2 * (a[e] % (IC / 2)) + G::fic(e);
+    for (int e = 0; e < G::NE; ++e) {
+      double const *s = sb + e * G::CELLS;
+      double v;
+      if constexpr (DIM == 1) {
+        v = (s[G::cell(c[0], 0, 0)] + s[G::cell(c[0] + 1, 0, 0)]) * 0.5;
+      } else if constexpr (DIM == 2) {
+        v = ((s[G::cell(c[0], c[1], 0)] + s[G::cell(c[0] + 1, c[1] + 1, 0)]) +
+             (s[G::cell(c[0] + 1, c[1], 0)] + s[G::cell(c[0], c[1] + 1, 0)])) * 0.25;
+      } else {
+        double w[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k)
+          w[k] = s[G::cell(c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + ((k >> 2) & 1))];
+        v = ghost_average3(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7]);
       }
-      int const child = g.src[o];
-      if (child < 0) continue;  // never read: the host checks face children are leaves
-      double const *sb = src + (size_t)child * G::BLOCK_DOUBLES;
+      dst[e * G::CELLS + x] = v;
+    }
+  }
+}
+
+// Fifth-order prediction of the children of one parent cell
+// (Multiresolution::Prediction, multiresolution.cpp:146-283): V(a, b, c) is the
+// parent value at offsets (a, b, c) in -2..2 along x, y, z. The terms and their
+// order are the reference's: one-axis differences, pairs of axes, and the
+// consistency-managed triple term, combined per child with its signs.
+constexpr double kPc0 = -22.0 / 128.0, kPc1 = 3.0 / 128.0;
+constexpr double kPc00 = kPc0 * kPc0, kPc01 = kPc0 * kPc1, kPc11 = kPc1 * kPc1;
+constexpr double kPc000 = kPc00 * kPc0, kPc001 = kPc00 * kPc1, kPc011 = kPc0 * kPc11,
+                 kPc111 = kPc1 * kPc11;
+
+__device__ __forceinline__ double cms4(double a, double b, double c, double d) {
+  double const s1 = (a + b) + (c + d);
+  double const s2 = (a + c) + (b + d);
+  double const s3 = (a + d) + (b + c);
+  double const i1 = s2 < s1 ? s2 : s1, mn = s3 < i1 ? s3 : i1;
+  double const i2 = s1 < s2 ? s2 : s1, mx = i2 < s3 ? s3 : i2;
+  return 0.5 * (mn + mx);
+}
+
+template <int DIM, typename V>
+__device__ __forceinline__ void predict_children(V const &val, double (&out)[1 << DIM]) {
+  auto at1 = [&](int d, int s) { return val(d == 0 ? s : 0, d == 1 ? s : 0, d == 2 ? s : 0); };
+  auto at2 = [&](int d, int sd, int e, int se) {
+    int o[3] = {0, 0, 0};
+    o[d] = sd;
+    o[e] = se;
+    return val(o[0], o[1], o[2]);
+  };
+  auto q1 = [&](int d) {
+    return kPc0 * (at1(d, 1) - at1(d, -1)) + kPc1 * (at1(d, 2) - at1(d, -2));
+  };
+  auto x2 = [&](int d, int e, int a, int b) {
+    return (at2(d, a, e, b) + at2(d, -a, e, -b)) - (at2(d, -a, e, b) + at2(d, a, e, -b));
+  };
+  auto q2 = [&](int d, int e) {
+    return (kPc00 * x2(d, e, 1, 1) + kPc11 * x2(d, e, 2, 2)) +
+           (kPc01 * x2(d, e, 1, 2) + kPc01 * x2(d, e, 2, 1));
+  };
+  auto x3 = [&](int a, int b, int c) {
+    return cms4(val(a, b, c) - val(-a, -b, -c), val(-a, -b, c) - val(a, b, -c),
+                val(a, -b, -c) - val(-a, b, c), val(-a, b, -c) - val(a, -b, c));
+  };
+  double qx = 0.0, qy = 0.0, qz = 0.0, qxy = 0.0, qxz = 0.0, qyz = 0.0, qxyz = 0.0;
+  qx = q1(0);
+  if constexpr (DIM > 1) {
+    qy = q1(1);
+    qxy = q2(0, 1);
+  }
+  if constexpr (DIM > 2) {
+    qz = q1(2);
+    qxz = q2(0, 2);
+    qyz = q2(1, 2);
+    qxyz = cms4(kPc000 * x3(1, 1, 1) + kPc111 * x3(2, 2, 2),
+                kPc001 * x3(1, 1, 2) + kPc011 * x3(2, 2, 1),
+                kPc011 * x3(1, 2, 2) + kPc001 * x3(2, 1, 1),
+                kPc001 * x3(1, 2, 1) + kPc011 * x3(2, 1, 2));
+  }
+  double const p = val(0, 0, 0);
 #pragma unroll
-      for (int e = 0; e < G::NE; ++e) {
-        double const *s = sb + e * G::CELLS;
-        double v;
-        if constexpr (DIM == 1) {
-          v = (s[G::cell(c[0], 0, 0)] + s[G::cell(c[0] + 1, 0, 0)]) * 0.5;
-        } else if constexpr (DIM == 2) {
-          v = ((s[G::cell(c[0], c[1], 0)] + s[G::cell(c[0] + 1, c[1] + 1, 0)]) +
-               (s[G::cell(c[0] + 1, c[1], 0)] + s[G::cell(c[0], c[1] + 1, 0)])) * 0.25;
-        } else {
-          double w[8];
-#pragma unroll
-          for (int k = 0; k < 8; ++k)
-            w[k] = s[G::cell(c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + ((k >> 2) & 1))];
-          v = ghost_average3(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7]);
+  for (int o = 0; o < (1 << DIM); ++o) {
+    double const sx = (o & 1) ? -1.0 : 1.0, sy = (o & 2) ? -1.0 : 1.0, sz = (o & 4) ? -1.0 : 1.0;
+    double s1, s2;
+    if constexpr (DIM == 1) {
+      s1 = sx * qx;
+      s2 = sx * sy * qxy;
+    } else if constexpr (DIM == 2) {
+      s1 = sx * qx + sy * qy;
+      s2 = sx * sy * qxy + sx * sz * qxz;
+    } else {
+      s1 = cms3(sx * qx, sy * qy, sz * qz);
+      s2 = cms3(sx * sy * qxy, sx * sz * qxz, sy * sz * qyz);
+    }
+    out[o] = ((p + s1) + s2) + sx * sy * sz * qxyz;
+  }
+}
+
+// Type 0 ghosts of one level: predicted from the parent level. Per field, the
+// parent cells under the filled part plus two on every side are staged in
+// shared memory; one thread per parent cell writes its children.
+constexpr int kBox = IC / 2 + 4;  // parent cells of a whole octant plus the stencil reach
+
+template <int DIM>
+__global__ void __launch_bounds__(256)
+ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
+                     int nleaf, CaseState const *__restrict__ gate,
+                     CaseState const *__restrict__ cu, int stage) {
+  using G = Geo<DIM>;
+  constexpr int B1 = DIM > 1 ? kBox : 1, B2 = DIM > 2 ? kBox : 1;
+  __shared__ double box[kBox * B1 * B2];
+  GhostRec const &g = ghosts[blockIdx.x];
+  int lo[3], hi[3];
+  if (!ghost_part<DIM>(g, blockIdx.y, lo, hi)) return;
+  if (!(gate[g.gate].dt > 0.0)) return;
+  // parent cells (relative to the parent node's origin) under the part
+  int plo[3] = {0, 0, 0}, pn[3] = {1, 1, 1}, bn[3] = {1, 1, 1};
+  for (int e = 0; e < DIM; ++e) {
+    int const base = (IC / 2) * ((g.oct >> e) & 1);
+    plo[e] = base + lo[e] / 2;
+    pn[e] = (hi[e] + 1) / 2 - lo[e] / 2;
+    bn[e] = pn[e] + 4;
+  }
+  int const nbox = bn[0] * bn[1] * bn[2], npar = pn[0] * pn[1] * pn[2];
+  double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
+  for (int e = 0; e < G::NE; ++e) {
+    for (int t = threadIdx.x; t < nbox; t += blockDim.x) {
+      int const r[3] = {t / (bn[1] * bn[2]), (t / bn[2]) % bn[1], t % bn[2]};
+      int y[3] = {0, 0, 0}, k = 0;
+      for (int d = 0; d < 3; ++d) {
+        int dn = 0;
+        if (d < DIM) {
+          int gc = g.q[d] * IC + plo[d] - 2 + r[d];  // parent-level cell
+          gc = gc < 0 ? 0 : (gc >= g.ext[d] ? g.ext[d] - 1 : gc);
+          dn = gc / IC - g.q[d];
+          y[d] = gc - (g.q[d] + dn) * IC + G::fic(d);
         }
-        dst[e * G::CELLS + x] = v;
+        k = 3 * k + dn + 1;
+      }
+      int const slot = g.nb[k];
+      double const *sb =
+          ghost_source(slot, nleaf, g.level - 1, Ug, UA, cu, stage) + (size_t)slot * G::BLOCK_DOUBLES;
+      box[(r[0] * B1 + r[1]) * B2 + r[2]] = sb[e * G::CELLS + G::cell(y[0], y[1], y[2])];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < npar; t += blockDim.x) {
+      int const r[3] = {t / (pn[1] * pn[2]) + 2, (t / pn[2]) % pn[1] + (DIM > 1 ? 2 : 0),
+                        t % pn[2] + (DIM > 2 ? 2 : 0)};
+      auto val = [&](int a, int b, int c) {
+        return box[((r[0] + a) * B1 + (DIM > 1 ? r[1] + b : 0)) * B2 + (DIM > 2 ? r[2] + c : 0)];
+      };
+      double out[1 << DIM];
+      predict_children<DIM>(val, out);
+#pragma unroll
+      for (int o = 0; o < (1 << DIM); ++o) {
+        int a[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; ++d)
+          a[d] = 2 * (plo[d] + r[d] - 2 - (IC / 2) * ((g.oct >> d) & 1)) + ((o >> d) & 1);
+        dst[e * G::CELLS + G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2))] = out[o];
       }
     }
+    __syncthreads();
   }
 }
 
@@ -378,6 +546,11 @@ struct JumpFace {
 
 }  // namespace
 
+// A run of ghost records of one type and level, filled by one launch.
+struct GhostGroup {
+  int type, level, first, count;
+};
+
 struct alp_levels {
   int dim = 3, scheme = 0, precision = 0, lmax = 0, nlev = 1, nmicro = 1;
   alp::SchemeOptions opt;
@@ -387,6 +560,7 @@ struct alp_levels {
   BlockMeta *meta = nullptr;
   int *nbr26 = nullptr, *work = nullptr;
   GhostRec *ghosts = nullptr;
+  std::vector<GhostGroup> ghost_groups;  // launch order of the ghost records
   // jump-flux conservation: records, per-record sums, parent-face sums,
   // fine-side record list, coarse leaves to correct
   int nrec = 0, nfine = 0, ncorr = 0, nacc = 0;
@@ -418,12 +592,22 @@ struct alp_levels {
       int const lf = tm == 0 ? 0 : lmax - height(tm - 1) + 1;
       for (int s = 0; s < 3; ++s) {
         CaseState const *gate = s == 0 ? cf : cu;
-        if (nghost > 0) {
-          dim3 grid(nghost, 2 * dim);
-          switch (dim) {
-            case 1: ghost_fill_kernel<1><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
-            case 2: ghost_fill_kernel<2><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
-            default: ghost_fill_kernel<3><<<grid, 256, 0, stream>>>(ghosts, in[s], U, in[s], gate, cu, s); break;
+        // averaged ghosts finest level first, then predicted ones coarsest first
+        for (GhostGroup const &gg : ghost_groups) {
+          dim3 grid(gg.count, 2 * dim + 1);
+          GhostRec const *g0 = ghosts + gg.first;
+          if (gg.type == 1) {
+            switch (dim) {
+              case 1: ghost_average_kernel<1><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              case 2: ghost_average_kernel<2><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              default: ghost_average_kernel<3><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+            }
+          } else {
+            switch (dim) {
+              case 1: ghost_predict_kernel<1><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              case 2: ghost_predict_kernel<2><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              default: ghost_predict_kernel<3><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+            }
           }
           ALP_CUDA(cudaGetLastError());
         }
@@ -548,6 +732,45 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
   static int const face_slot[6] = {4, 21, 10, 15, 12, 13};
   nbr26.assign((size_t)nleaf * 26, -1);
   std::map<NodeKey, int> ghost_of;
+  std::vector<NodeKey> ghost_key;
+  std::vector<int> pending;  // ghosts to be filled whole whose sources are not resolved yet
+  // the ghost of node position k (created on first use: refined -> type 1,
+  // otherwise inside a coarser leaf -> type 0)
+  auto ghost_for = [&](NodeKey const &k) {
+    auto gi = ghost_of.find(k);
+    if (gi != ghost_of.end()) return gi->second;
+    GhostRec gr{};
+    gr.slot = nleaf + (int)ghosts.size();
+    gr.level = k.l;
+    gr.gate = -1;
+    for (int o = 0; o < 8; ++o) gr.src[o] = -1;
+    for (int o = 0; o < 27; ++o) gr.nb[o] = -1;
+    if (refined.count(k)) {
+      gr.type = 1;
+    } else {
+      gr.type = 0;
+      for (int e = 0; e < dim; ++e) {
+        gr.q[e] = k.c[e] >> 1;
+        gr.oct |= (k.c[e] & 1) << e;
+        gr.ext[e] = extent(k.l - 1, e) * IC;
+      }
+    }
+    ghosts.push_back(gr);
+    ghost_key.push_back(k);
+    ghost_of.emplace(k, (int)ghosts.size() - 1);
+    return (int)ghosts.size() - 1;
+  };
+  // the slot holding node position k whole: a leaf, or a ghost filled whole
+  auto whole = [&](NodeKey const &k) {
+    auto it = leaf.find(k);
+    if (it != leaf.end()) return it->second;
+    int const idx = ghost_for(k);
+    if (!ghosts[idx].full) {
+      ghosts[idx].full = 1;
+      pending.push_back(idx);
+    }
+    return nleaf + idx;
+  };
   for (int b = 0; b < nleaf; ++b) {
     int const l = level[b];
     for (int f = 0; f < 2 * dim; ++f) {
@@ -562,35 +785,24 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
         nbr26[(size_t)b * 26 + face_slot[f]] = it->second;
         continue;
       }
-      GhostRec gr{};
-      gr.level = l;
-      for (int o = 0; o < 8; ++o) gr.src[o] = -1;
       int const loc = f ^ 1;  // East 0, West 1, North 2, South 3, Top 4, Bottom 5
       if (refined.count(k)) {
         // coarse side: the neighbour's opposite face collects the fine sums
         jumps.push_back({b, loc, 2, k, loc ^ 1, 0, 0});
-        gr.type = 1;
-        gr.src_level = l + 1;
         for (int o = 0; o < (1 << dim); ++o) {
           int c[3] = {0, 0, 0};
           for (int e = 0; e < dim; ++e) c[e] = 2 * p[e] + ((o >> e) & 1);
-          auto ci = leaf.find(key(l + 1, c));
           bool const face_child = ((o >> d) & 1) == (s > 0 ? 0 : 1);
-          if (ci == leaf.end() && face_child)
+          if (face_child && !leaf.count(key(l + 1, c)))
             return fail(ALP_ERR_INVALID, "face neighbours more than one level apart at leaf " +
                                              std::to_string(b));
-          gr.src[o] = ci == leaf.end() ? -1 : ci->second;
         }
       } else {
         int q[3] = {0, 0, 0};
         for (int e = 0; e < dim; ++e) q[e] = p[e] >> 1;
-        auto ci = l > 0 ? leaf.find(key(l - 1, q)) : leaf.end();
-        if (ci == leaf.end())
+        if (l == 0 || !leaf.count(key(l - 1, q)))
           return fail(ALP_ERR_INVALID, "face neighbours more than one level apart at leaf " +
                                            std::to_string(b));
-        gr.type = 0;
-        gr.src_level = l - 1;
-        gr.src[0] = ci->second;
         // fine side: this leaf's face lies on its parent's face of the same location
         NodeKey parent{l - 1, {0, 0, 0}};
         int oc[3] = {0, 0, 0};
@@ -601,27 +813,77 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
         int const t1 = d == 0 ? 1 : 0, t2 = d == 2 ? 1 : 2;
         jumps.push_back({b, loc, 3, parent, loc, t1 < dim ? oc[t1] * (IC / 2) : 0,
                          t2 < dim ? oc[t2] * (IC / 2) : 0});
-        int oct = 0;
-        for (int e = 0; e < dim; ++e) oct |= (p[e] & 1) << e;
-        gr.src[1] = oct;
       }
+      int const idx = ghost_for(k);
+      GhostRec &gr = ghosts[idx];
+      if (gr.type == 1)
+        for (int o = 0; o < (1 << dim); ++o) {
+          int c[3] = {0, 0, 0};
+          for (int e = 0; e < dim; ++e) c[e] = 2 * p[e] + ((o >> e) & 1);
+          auto ci = leaf.find(key(l + 1, c));
+          if (ci != leaf.end()) gr.src[o] = ci->second;
+        }
+      else if (gr.full == 0 && gr.nb[13] < 0)
+        pending.push_back(idx);
       // the leaf sits on the (s < 0 ? high : low) side of the ghost
-      int const ghost_face = 2 * d + (s < 0 ? 1 : 0);
-      auto gi = ghost_of.find(k);
-      int idx;
-      if (gi == ghost_of.end()) {
-        idx = (int)ghosts.size();
-        gr.slot = nleaf + idx;
-        gr.faces = 0;
-        ghosts.push_back(gr);
-        ghost_of.emplace(k, idx);
-      } else {
-        idx = gi->second;
-      }
-      ghosts[idx].faces |= 1 << ghost_face;
-      nbr26[(size_t)b * 26 + face_slot[f]] = nleaf + idx;
+      gr.faces |= 1 << (2 * d + (s < 0 ? 1 : 0));
+      gr.gate = l;
+      nbr26[(size_t)b * 26 + face_slot[f]] = gr.slot;
     }
   }
+  // sources of the ghosts: a predicted ghost reads its parent position's 3^dim
+  // neighbours whole, an averaged ghost filled whole reads all its children
+  // whole; both may add further ghosts
+  while (!pending.empty()) {
+    int const idx = pending.back();
+    pending.pop_back();
+    GhostRec const g = ghosts[idx];
+    if (g.type == 0) {
+      if (g.nb[13] >= 0) continue;  // resolved already
+      int nb[27];
+      for (int o = 0; o < 27; ++o) {
+        int const off[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+        bool ok = true;
+        int c[3] = {0, 0, 0};
+        for (int e = 0; e < 3; ++e) {
+          if (e >= dim) {
+            ok = ok && off[e] == 0;
+            continue;
+          }
+          c[e] = g.q[e] + off[e];
+          ok = ok && c[e] >= 0 && c[e] < extent(g.level - 1, e);
+        }
+        nb[o] = ok ? whole(key(g.level - 1, c)) : -1;
+      }
+      for (int o = 0; o < 27; ++o) ghosts[idx].nb[o] = nb[o];
+    } else {
+      NodeKey const k = ghost_key[idx];
+      int src[8];
+      for (int o = 0; o < (1 << dim); ++o) {
+        int c[3] = {0, 0, 0};
+        for (int e = 0; e < dim; ++e) c[e] = 2 * k.c[e] + ((o >> e) & 1);
+        src[o] = whole(key(g.level + 1, c));
+      }
+      for (int o = 0; o < (1 << dim); ++o) ghosts[idx].src[o] = src[o];
+    }
+  }
+  // a ghost is needed whenever a ghost reading it is: its gate is the finest
+  // gate of its readers (a level computes whenever a coarser one does)
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (GhostRec const &g : ghosts) {
+      if (g.gate < 0) continue;
+      int const *deps = g.type == 0 ? g.nb : g.src;
+      int const n = g.type == 0 ? 27 : 8;
+      for (int o = 0; o < n; ++o)
+        if (deps[o] >= nleaf && ghosts[deps[o] - nleaf].gate < g.gate) {
+          ghosts[deps[o] - nleaf].gate = g.gate;
+          changed = true;
+        }
+    }
+  }
+  for (GhostRec const &g : ghosts)
+    if (g.gate < 0 || g.gate > lmax) return fail(ALP_ERR_INVALID, "a ghost block has no reader");
   *lmax_out = lmax;
   return ALP_OK;
 }
@@ -800,8 +1062,21 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(m->work, work.data(), sizeof(int) * nleaf, cudaMemcpyHostToDevice,
                         m->stream);
+  // launch order: averaged ghosts finest level first (their children may be
+  // averaged ghosts one level finer), then predicted ghosts coarsest level
+  // first (their sources may be predicted ghosts one level coarser)
+  std::vector<GhostRec> order;
+  auto group = [&](int type, int lev) {
+    int const first = (int)order.size();
+    for (GhostRec const &g : gh)
+      if (g.type == type && g.level == lev) order.push_back(g);
+    if ((int)order.size() > first)
+      m->ghost_groups.push_back({type, lev, first, (int)order.size() - first});
+  };
+  for (int l = lmax; l >= 0; --l) group(1, l);
+  for (int l = 0; l <= lmax; ++l) group(0, l);
   if (e == cudaSuccess && m->nghost)
-    e = cudaMemcpyAsync(m->ghosts, gh.data(), sizeof(GhostRec) * m->nghost,
+    e = cudaMemcpyAsync(m->ghosts, order.data(), sizeof(GhostRec) * m->nghost,
                         cudaMemcpyHostToDevice, m->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(m->cu, cs.data(), sizeof(CaseState) * m->nlev, cudaMemcpyHostToDevice,
@@ -875,7 +1150,7 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
       int const lf = tm == 0 ? 0 : m->lmax - height(tm - 1) + 1;
       n += per_micro;
       for (int s = 0; s < 3; ++s) {
-        n += m->nghost > 0 ? 1 : 0;
+        n += (int)m->ghost_groups.size();
         n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? 1 : 0;
         n += m->nwork_ge[lu] > 0 ? 1 : 0;
         n += m->nrec > 0 ? 1 : 0;

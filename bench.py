@@ -315,7 +315,7 @@ def precision_report(steps: int = 200, emit=None):
 
 
 def levels_report(args):
-    """Multi-level batching form: the 48 / 469 / 1176-leaf three-level
+    """Multi-level batching form: the 8 / 294 / 1232-leaf three-level
     spherical-shock hierarchy advanced with local time stepping (a macro step
     is 4 micro steps; level l takes 2^l RK3 steps per macro step), all levels
     in the same batched launches, one CUDA graph per macro step. Timed with

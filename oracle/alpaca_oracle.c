@@ -1333,9 +1333,9 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb, const int *nbr
  *
  * Halo cells across a jump (a face neighbour one level coarser or finer) are
  * filled by averaging the finer leaves with Multiresolution::Average
- * (multiresolution.h:94-166) and by injection from the coarser leaf (the
- * reference predicts the finer side with a fifth-order interpolation,
- * Multiresolution::Prediction, multiresolution.cpp:146, not restated here).
+ * (multiresolution.h:94-166) and, on the finer side, by the fifth-order
+ * prediction from the coarser level (Multiresolution::Prediction,
+ * multiresolution.cpp:146-283), through the level field below.
  * Conservation at jumps follows the reference: every leaf integrates its
  * boundary face fluxes at jump faces with the RK3 jump multipliers (1/6, 1/6,
  * 2/3) times its level step (SpaceSolver::UpdateFluxes space_solver.cpp:155-182,
@@ -1458,20 +1458,26 @@ static int tree_build(Tree *t, int dim, int nleaf, const int *level, const int *
 /* 3D / 2D / 1D conservative average of the 2^dim children cells of a parent
  * cell (Multiresolution::Average, multiresolution.h:133-158). c points at the
  * child cell (2a, 2b, 2c) of field buffer f. */
-static double child_average(const Geom *g, const double *f, int i, int j, int k) {
-  if (g->dim == 1) return (f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j, k)]) * 0.5;
-  if (g->dim == 2)
-    return ((f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j + 1, k)]) +
-            (f[cidx(g, i + 1, j, k)] + f[cidx(g, i, j + 1, k)])) * 0.25;
-  double const a = f[cidx(g, i, j, k)] + f[cidx(g, i + 1, j + 1, k + 1)];
-  double const b = f[cidx(g, i, j, k + 1)] + f[cidx(g, i + 1, j + 1, k)];
-  double const c = f[cidx(g, i, j + 1, k)] + f[cidx(g, i + 1, j, k + 1)];
-  double const d = f[cidx(g, i, j + 1, k + 1)] + f[cidx(g, i + 1, j, k)];
+/* w[o]: child o (bit d of o: high half along d) */
+static double average_values(int dim, const double *w) {
+  if (dim == 1) return (w[0] + w[1]) * 0.5;
+  if (dim == 2) return ((w[0] + w[3]) + (w[1] + w[2])) * 0.25;
+  double const a = w[0] + w[7];
+  double const b = w[4] + w[3];
+  double const c = w[2] + w[5];
+  double const d = w[6] + w[1];
   double const s1 = (a + b) + (c + d);
   double const s2 = (a + c) + (b + d);
   double const s3 = (a + d) + (b + c);
   double const mn = dmin(s1, dmin(s2, s3)), mx = dmax(s1, dmax(s2, s3));
   return 0.125 * (0.5 * (mn + mx));
+}
+
+static double child_average(const Geom *g, const double *f, int i, int j, int k) {
+  double w[8];
+  for (int o = 0; o < (1 << g->dim); ++o)
+    w[o] = f[cidx(g, i + (o & 1), j + ((o >> 1) & 1), k + ((o >> 2) & 1))];
+  return average_values(g->dim, w);
 }
 
 /* ConsistencyManagedSum of four values (mathematical_functions.h:115-125) */
@@ -1605,9 +1611,129 @@ int oracle_prediction(int dim, const double *parent, int octant, const int *star
   return 0;
 }
 
+/* The cell values a node buffer of level L holds in the reference, for every
+ * node position of level L: a leaf's own cells; a refined node's interior is
+ * the average of its children (Averager, Multiresolution::Average); a node
+ * position inside a coarser leaf is what a node there receives in its jump
+ * halos, the prediction from the next coarser level (Multiresolution::
+ * Prediction from the parent's buffer, internal_halo_manager.cpp:230-290);
+ * beyond the domain, the zero-gradient value of the nearest domain cell. Refined
+ * and predicted nodes are computed whole on first use and kept for the pass
+ * (the leaves' values come from src[level], fixed during a pass). */
+typedef struct {
+  const Geom *g;
+  const Tree *t;
+  double *const *src;
+  double **node[MAXLEV]; /* per level and node position: NULL or [ne][IC^dim] */
+} LevelField;
+
+static void lf_init(LevelField *F, const Geom *g, const Tree *t, double *const *src) {
+  memset(F, 0, sizeof(*F));
+  F->g = g;
+  F->t = t;
+  F->src = src;
+}
+
+static void lf_free(LevelField *F) {
+  for (int l = 0; l < MAXLEV; ++l) {
+    if (!F->node[l]) continue;
+    long const n = (long)F->t->ext[l][0] * F->t->ext[l][1] * F->t->ext[l][2];
+    for (long x = 0; x < n; ++x) free(F->node[l][x]);
+    free(F->node[l]);
+  }
+}
+
+static long lf_cell(int dim, const int y[3]) {
+  long c = 0;
+  for (int d = 0; d < dim; ++d) c = c * IC + y[d];
+  return c;
+}
+
+static const double *lf_node(LevelField *F, int L, const int n[3]);
+
+/* value of field e at global cell Y of level L */
+static double lf_value(LevelField *F, int L, const int Y0[3], int e) {
+  const Geom *g = F->g;
+  const Tree *t = F->t;
+  int Y[3] = {0, 0, 0}, n[3] = {0, 0, 0}, y[3] = {0, 0, 0};
+  for (int d = 0; d < g->dim; ++d) {
+    int const top = t->ext[L][d] * IC - 1;
+    Y[d] = Y0[d] < 0 ? 0 : (Y0[d] > top ? top : Y0[d]);
+    n[d] = Y[d] / IC;
+    y[d] = Y[d] - n[d] * IC;
+  }
+  int const v = t->grid[L][tree_at(t, L, n)];
+  if (v >= 0) {
+    const double *f = F->src[L] + ((long)v * g->ne + e) * g->cells;
+    return f[cidx(g, fic(g, 0) + y[0], fic(g, 1) + y[1], fic(g, 2) + y[2])];
+  }
+  long const icd = g->dim == 3 ? IC * IC * IC : (g->dim == 2 ? IC * IC : IC);
+  return lf_node(F, L, n)[(long)e * icd + lf_cell(g->dim, y)];
+}
+
+static const double *lf_node(LevelField *F, int L, const int n[3]) {
+  const Geom *g = F->g;
+  const Tree *t = F->t;
+  int const dim = g->dim;
+  long const x = tree_at(t, L, n);
+  if (!F->node[L]) {
+    long const cnt = (long)t->ext[L][0] * t->ext[L][1] * t->ext[L][2];
+    F->node[L] = (double **)calloc((size_t)cnt, sizeof(double *));
+  }
+  if (F->node[L][x]) return F->node[L][x];
+  long const icd = dim == 3 ? IC * IC * IC : (dim == 2 ? IC * IC : IC);
+  double *blk = (double *)malloc(sizeof(double) * g->ne * icd);
+  int const ext1 = dim > 1 ? IC : 1, ext2 = dim > 2 ? IC : 1;
+  if (t->grid[L][x] == -2) {
+    /* refined: average of the 2^dim children cells of level L + 1 */
+    for (int e = 0; e < g->ne; ++e)
+      for (int a = 0; a < IC; ++a)
+        for (int b = 0; b < ext1; ++b)
+          for (int c = 0; c < ext2; ++c) {
+            int const y[3] = {a, b, c};
+            double w[8];
+            for (int o = 0; o < (1 << dim); ++o) {
+              int Y[3] = {0, 0, 0};
+              for (int d = 0; d < dim; ++d) Y[d] = 2 * (n[d] * IC + y[d]) + ((o >> d) & 1);
+              w[o] = lf_value(F, L + 1, Y, e);
+            }
+            blk[(long)e * icd + lf_cell(dim, y)] = average_values(dim, w);
+          }
+  } else {
+    /* inside a coarser leaf: predicted from level L - 1 */
+    for (int e = 0; e < g->ne; ++e)
+      for (int a = 0; a < IC / 2; ++a)
+        for (int b = 0; b < (dim > 1 ? IC / 2 : 1); ++b)
+          for (int c = 0; c < (dim > 2 ? IC / 2 : 1); ++c) {
+            int const q[3] = {a, b, c};
+            int P[3] = {0, 0, 0};
+            for (int d = 0; d < dim; ++d) P[d] = n[d] * (IC / 2) + q[d];
+            double v[125];
+            for (int i = -2; i <= 2; ++i)
+              for (int j = -2; j <= 2; ++j)
+                for (int k = -2; k <= 2; ++k) {
+                  int const o[3] = {i, dim > 1 ? j : 0, dim > 2 ? k : 0};
+                  int Y[3] = {0, 0, 0};
+                  for (int d = 0; d < dim; ++d) Y[d] = P[d] + o[d];
+                  PRED_V(i, j, k) = lf_value(F, L - 1, Y, e);
+                }
+            double out[8];
+            predict_children(dim, v, out);
+            for (int o = 0; o < (1 << dim); ++o) {
+              int y[3] = {0, 0, 0};
+              for (int d = 0; d < dim; ++d) y[d] = 2 * q[d] + ((o >> d) & 1);
+              blk[(long)e * icd + lf_cell(dim, y)] = out[o];
+            }
+          }
+  }
+  F->node[L][x] = blk;
+  return blk;
+}
+
 /* Face halos (HS layers over the interior extent) of leaf b in pool dst; the
  * neighbours' values come from src[level] (a pool per level). */
-static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double *const *src) {
+static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double *const *src,
+                        LevelField *F) {
   int const l = t->level[b], ne = g->ne;
   long const blk = (long)ne * g->cells;
   double *ub = dst + b * blk;
@@ -1660,14 +1786,9 @@ static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double
               const double *fs = src[l + 1] + c * blk + (long)e * g->cells;
               val = child_average(g, fs, ci[0], ci[1], ci[2]);
             } else {
-              int q3[3], ci[3];
-              for (int q = 0; q < 3; ++q) {
-                q3[q] = q < g->dim ? p[q] >> 1 : 0;
-                ci[q] = q < g->dim ? fic(g, q) + (IC / 2) * (p[q] & 1) + a[q] / 2 : 0;
-              }
-              int const c = t->grid[l - 1][tree_at(t, l - 1, q3)];
-              const double *fs = src[l - 1] + c * blk + (long)e * g->cells;
-              val = fs[cidx(g, ci[0], ci[1], ci[2])];
+              int X[3] = {0, 0, 0};
+              for (int q = 0; q < g->dim; ++q) X[q] = p[q] * IC + a[q];
+              val = lf_value(F, l, X, e);
             }
             fo[x] = val;
           }
@@ -1904,11 +2025,14 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
         double *src[MAXLEV];
         for (int l = 0; l <= lmax; ++l) src[l] = (s > 0 && l >= lu) ? pool_in[s] : u;
         int ni = 0;
+        LevelField field;
+        lf_init(&field, &g, &tr, src);
         for (int b = 0; b < nleaf; ++b)
           if (level[b] >= lflux) {
-            level_halos(&g, &tr, b, pool_in[s], src);
+            level_halos(&g, &tr, b, pool_in[s], src, &field);
             items[ni++] = b;
           }
+        lf_free(&field);
         LevelRhsCtx c = {&g, &e, solver, recon, &tr, items, pool_in[s], rhs, bflux, h0};
         parallel_blocks(&g, ni, nthreads, level_rhs_task, &c);
         for (int b = 0; b < nleaf; ++b) {

@@ -104,3 +104,19 @@ def sod_error_norms(case: cases.Case, u: np.ndarray, t: float) -> np.ndarray:
     vol = g.cell_size ** 3
     return np.concatenate([relative_error_norms(rho, rho_x, vol),
                            relative_error_norms(p, p_x, vol)])
+
+
+def smooth_bump(c, centre=0.5, radius=0.2):
+    """A level case's leaves filled with a pressure and density bump at rest,
+    cos^2 in the distance from the centre, zero outside the radius: smooth
+    across the level jumps, and uniform at the domain faces."""
+    I = cases.interior(c.dim)
+    u = c.u.copy()
+    for b in range(c.nleaf):
+        x = c.cell_centres(b)
+        r = np.sqrt(sum((x[d] - centre) ** 2 for d in range(c.dim)))
+        w = np.where(r < radius, np.cos(0.5 * np.pi * r / radius) ** 2, 0.0)
+        vel = [np.zeros_like(r) for _ in range(c.dim)]
+        u[(b, slice(None)) + I[1:]] = cases.primes_to_conservatives(
+            c.dim, 1.0 + 0.5 * w, 1.0 + 2.0 * w, vel, c.gamma)
+    return u

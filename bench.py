@@ -351,8 +351,8 @@ def levels_report(args):
                    "ghost_blocks": info["ghosts"], "variant": args.variant,
                    "step": "macro step = 4 micro steps (local time stepping)",
                    "cell_updates_per_macro_step": info["cell_updates_per_macro_step"],
-                   "jumps": "injection / Multiresolution::Average halos, JumpFluxAdjustment "
-                            "conservation",
+                   "jumps": "Multiresolution::Prediction / Average halos, "
+                            "JumpFluxAdjustment conservation",
                    "sim_time_reached": t, "macro_steps_done": macro,
                    "l2": "state %.2f GB per pool > 126 MB L2 (no flush needed)"
                          % ((case.nleaf + info["ghosts"]) * 5 * 24 ** 3 * 8 / 1e9)},

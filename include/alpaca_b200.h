@@ -356,9 +356,11 @@ int alp_engine_launches_per_step(alp_engine *e);
  * :1068-1098); the micro time step is ComputeTimestepSize over all leaves with
  * the finest cell size (:1925-1982). Halo cells across a level jump are the
  * average of the finer leaves (Multiresolution::Average,
- * multiresolution/multiresolution.h:94-166) or the coarser leaf's cell
- * (injection; the reference's fifth-order prediction, multiresolution.cpp:146,
- * is not applied). Conservation at jumps as JumpFluxAdjustment
+ * multiresolution/multiresolution.h:94-166) or, on the finer side, the
+ * fifth-order prediction from the coarser level (Multiresolution::Prediction,
+ * multiresolution.cpp:146-283), as the reference's jump halos hold them; node
+ * positions the prediction reads that are not leaves are averaged or predicted
+ * in turn. Conservation at jumps as JumpFluxAdjustment
  * (modular_algorithm_assembler.cpp:1347-1636): jump-face fluxes integrated
  * with the RK3 jump multipliers, fine sums averaged onto the parent faces
  * after each fine step, coarse cells corrected after each coarse step.

@@ -81,11 +81,13 @@ struct LevelState {
 // (dx+1)*9 + (dy+1)*3 + (dz+1); cells beyond the domain take the value of the
 // nearest domain cell, zero gradient); oct is the ghost's octant in its parent.
 // A ghost the face kernels read fills the three cell layers next to each face
-// in `faces` (bits W, E, S, N, B, T); a ghost other ghosts read is filled whole
-// (`full`). Slots below nleaf are leaves, read from the pool of their level.
-// gate: the finest level whose computing needs the ghost.
+// in `faces` (bits W, E, S, N, B, T); a ghost other ghosts read (`full`: its
+// sources are all resolved) also fills the box of cells those reads reach,
+// lo[e] <= cell < hi[e]. Slots below nleaf are leaves, read from the pool of
+// their level. gate: the finest level whose computing needs the ghost.
 struct GhostRec {
   int slot, type, level, gate, faces, full, oct;
+  int lo[3], hi[3];  // the box other ghosts read (empty: lo >= hi)
   int q[3], ext[3];  // parent position (nodes) and level extent (cells) of the parent level
   int src[8];
   int nb[27];
@@ -116,20 +118,26 @@ __device__ __forceinline__ double const *ghost_source(int slot, int nleaf, int l
 }
 
 // The cells a part of the fill covers: part < 2 DIM, the three layers next to
-// face part (if served); part == 2 DIM, the whole block (if full).
+// face part (if served); part == 2 DIM, the box other ghosts read (if any).
 template <int DIM>
 __device__ __forceinline__ bool ghost_part(GhostRec const &g, int part, int lo[3], int hi[3]) {
-  bool const whole = part == 2 * DIM;
-  if (whole ? !g.full : (g.full || !((g.faces >> part) & 1))) return false;
+  if (part == 2 * DIM) {
+    bool any = true;
+    for (int e = 0; e < 3; ++e) {
+      lo[e] = e < DIM ? g.lo[e] : 0;
+      hi[e] = e < DIM ? g.hi[e] : 1;
+      any = any && lo[e] < hi[e];
+    }
+    return any;
+  }
+  if (!((g.faces >> part) & 1)) return false;
   for (int e = 0; e < 3; ++e) {
     lo[e] = 0;
     hi[e] = e < DIM ? IC : 1;
   }
-  if (!whole) {
-    int const d = part / 2;
-    lo[d] = (part & 1) ? IC - 3 : 0;
-    hi[d] = lo[d] + 3;
-  }
+  int const d = part / 2;
+  lo[d] = (part & 1) ? IC - 3 : 0;
+  hi[d] = lo[d] + 3;
   return true;
 }
 
@@ -884,6 +892,88 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
   }
   for (GhostRec const &g : ghosts)
     if (g.gate < 0 || g.gate > lmax) return fail(ALP_ERR_INVALID, "a ghost block has no reader");
+  // the box of each ghost other ghosts read: grown from the cells its readers
+  // hold (face layers and their own boxes) until nothing changes
+  for (GhostRec &g : ghosts)
+    for (int e = 0; e < 3; ++e) {
+      g.lo[e] = e < dim ? IC : 0;
+      g.hi[e] = e < dim ? 0 : 1;
+    }
+  auto grow = [&](int slot, int const lo[3], int const hi[3]) {
+    GhostRec &t = ghosts[slot - nleaf];
+    bool changed = false;
+    for (int e = 0; e < dim; ++e) {
+      if (lo[e] < t.lo[e]) t.lo[e] = lo[e], changed = true;
+      if (hi[e] > t.hi[e]) t.hi[e] = hi[e], changed = true;
+    }
+    return changed;
+  };
+  for (bool changed = true; changed;) {
+    changed = false;
+    for (size_t gi = 0; gi < ghosts.size(); ++gi) {
+      GhostRec const g = ghosts[gi];
+      if (g.type == 1 && !g.full) continue;  // an averaged face ghost reads leaves only
+      // bounding box of the cells g holds
+      int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+      bool any = false;
+      for (int e = 0; e < dim; ++e) lo[e] = IC, hi[e] = 0;
+      auto add = [&](int const *a, int const *b) {
+        bool ok = true;
+        for (int e = 0; e < dim; ++e) ok = ok && a[e] < b[e];
+        if (!ok) return;
+        any = true;
+        for (int e = 0; e < dim; ++e) lo[e] = std::min(lo[e], a[e]), hi[e] = std::max(hi[e], b[e]);
+      };
+      add(g.lo, g.hi);
+      for (int f = 0; f < 2 * dim; ++f)
+        if ((g.faces >> f) & 1) {
+          int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+          for (int e = 0; e < dim; ++e) b[e] = IC;
+          a[f / 2] = (f & 1) ? IC - 3 : 0;
+          b[f / 2] = a[f / 2] + 3;
+          add(a, b);
+        }
+      if (!any) continue;
+      if (g.type == 0) {
+        // parent-level cells read: the parent cells under the box, two more on
+        // each side, clamped to the domain (global cells of the parent level)
+        int plo[3] = {0, 0, 0}, phi[3] = {1, 1, 1};
+        for (int e = 0; e < dim; ++e) {
+          int const base = g.q[e] * IC + (IC / 2) * ((g.oct >> e) & 1);
+          plo[e] = std::max(0, base + lo[e] / 2 - 2);
+          phi[e] = std::min(g.ext[e], base + (hi[e] + 1) / 2 + 2);
+        }
+        for (int o = 0; o < 27; ++o) {
+          int const src = g.nb[o];
+          if (src < nleaf) continue;
+          int const off[3] = {o / 9 - 1, (o / 3) % 3 - 1, o % 3 - 1};
+          int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+          bool ok = true;
+          for (int e = 0; e < dim; ++e) {
+            int const n0c = (g.q[e] + off[e]) * IC;
+            a[e] = std::max(plo[e], n0c) - n0c;
+            b[e] = std::min(phi[e], n0c + IC) - n0c;
+            ok = ok && a[e] < b[e];
+          }
+          if (ok && grow(src, a, b)) changed = true;
+        }
+      } else {
+        for (int o = 0; o < (1 << dim); ++o) {
+          int const src = g.src[o];
+          if (src < nleaf) continue;
+          int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
+          bool ok = true;
+          for (int e = 0; e < dim; ++e) {
+            int const base = (IC / 2) * ((o >> e) & 1);
+            a[e] = 2 * (std::max(lo[e], base) - base);
+            b[e] = 2 * (std::min(hi[e], base + IC / 2) - base);
+            ok = ok && a[e] < b[e];
+          }
+          if (ok && grow(src, a, b)) changed = true;
+        }
+      }
+    }
+  }
   *lmax_out = lmax;
   return ALP_OK;
 }

@@ -190,6 +190,37 @@ class Engine:
                                                  C.byref(t), C.byref(steps)))
         return out, t.value, steps.value
 
+    def checkpoint(self, cid: int) -> dict:
+        """The state that resumes case cid exactly (alp_engine_checkpoint_case):
+        its blocks, neighbour table, time, step count and settings."""
+        nb, shp = self.nb[cid]
+        info = N.CaseCheckpoint()
+        nbr = np.empty((nb, 26), dtype=np.int32)
+        u = np.empty(shp, dtype=np.float64)
+        self._check(self.lib.alp_engine_checkpoint_case(
+            self.h, cid, C.byref(info), nbr.ctypes.data_as(C.POINTER(C.c_int)),
+            u.ctypes.data_as(C.POINTER(C.c_double))))
+        return {"dim": info.dim, "steps": info.steps, "max_steps": info.max_steps, "t": info.t,
+                "t_end": info.t_end, "cfl": info.cfl, "cell_size": info.cell_size,
+                "gamma": info.material.gamma, "background_pressure": info.material.background_pressure,
+                "safe": info.material.safe, "nbr26": nbr, "blocks": u}
+
+    def restore(self, ck: dict) -> int:
+        """Adds the case a checkpoint describes; it continues where it stopped."""
+        u = np.ascontiguousarray(ck["blocks"], dtype=np.float64)
+        nbr = np.ascontiguousarray(ck["nbr26"], dtype=np.int32)
+        info = N.CaseCheckpoint(int(ck["dim"]), u.shape[0], int(ck["steps"]), int(ck["max_steps"]),
+                                float(ck["t"]), float(ck["t_end"]), float(ck["cfl"]),
+                                float(ck["cell_size"]),
+                                N.Material.make(float(ck["gamma"]), float(ck["background_pressure"]),
+                                                bool(ck["safe"])))
+        cid = C.c_int()
+        self._check(self.lib.alp_engine_restore_case(
+            self.h, C.byref(info), nbr.ctypes.data_as(C.POINTER(C.c_int)),
+            u.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cid)))
+        self.nb[cid.value] = (u.shape[0], u.shape)
+        return cid.value
+
     def all_done(self) -> bool:
         d = C.c_int()
         self._check(self.lib.alp_engine_all_done(self.h, C.byref(d)))
@@ -386,3 +417,43 @@ class IcProgram:
                                          C.byref(units) if units is not None else None,
                                          _ptr(out), _stream(stream)), self.strict)
         return out
+
+
+# Checkpoint files. The reference writes its restart snapshots as HDF5
+# (RestartManager::WriteRestartFile, input_output/restart_manager.cpp:301-485):
+# group simulation_data with the attributes Time, Dimensions, InternalCells,
+# HaloSize and MaximumLevel, and group node_cell_data with the dataset
+# Conservatives [node][equation][cells]. These files keep the same names and
+# layout in a NumPy archive (no HDF5 library here), plus a case group with what
+# resuming a case of this library needs.
+_CASE_KEYS = ("steps", "max_steps", "t_end", "cfl", "cell_size", "gamma", "background_pressure",
+              "safe")
+
+
+def save_checkpoint(path: str, ck: dict) -> None:
+    """Writes one case checkpoint (Engine.checkpoint) to path (.npz)."""
+    out = {"simulation_data/Time": np.float64(ck["t"]),
+           "simulation_data/Dimensions": np.uint32(ck["dim"]),
+           "simulation_data/InternalCells": np.uint32(16),
+           "simulation_data/HaloSize": np.uint32(4),
+           "simulation_data/MaximumLevel": np.uint32(0),
+           "node_cell_data/Conservatives": np.ascontiguousarray(ck["blocks"], dtype=np.float64),
+           "case/Neighbours": np.ascontiguousarray(ck["nbr26"], dtype=np.int32)}
+    for k in _CASE_KEYS:
+        out["case/" + k] = np.asarray(ck[k])
+    with open(path, "wb") as f:
+        np.savez(f, **out)
+
+
+def load_checkpoint(path: str) -> dict:
+    """Reads a checkpoint file written by save_checkpoint (for Engine.restore)."""
+    with np.load(path) as z:
+        if int(z["simulation_data/InternalCells"]) != 16 or int(z["simulation_data/HaloSize"]) != 4:
+            raise ValueError("checkpoint of another block layout")
+        ck = {"t": float(z["simulation_data/Time"]), "dim": int(z["simulation_data/Dimensions"]),
+              "blocks": z["node_cell_data/Conservatives"].copy(),
+              "nbr26": z["case/Neighbours"].copy()}
+        for k in _CASE_KEYS:
+            v = z["case/" + k]
+            ck[k] = v.item()
+    return ck

@@ -317,7 +317,7 @@ int engine_add_case_core(alp_engine *e, alp_material const *mat, double cell_siz
   if (cid < 0) return fail(ALP_ERR_CAPACITY, "case table full");
   int first;
   if (int rc = e->alloc_range(nb, &first)) return rc;
-  e->case_rec[cid] = {true, first, nb};
+  e->case_rec[cid] = {true, first, nb, *mat, cell_size};
   for (int b = 0; b < nb; ++b) {
     e->h_meta[first + b] = meta_of(mat, cell_size, cid);
     for (int s = 0; s < 26; ++s) {
@@ -566,6 +566,52 @@ int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t,
   if (t) *t = cs.t;
   if (steps) *steps = cs.steps;
   if (cs.status) return fail(ALP_ERR_NUMERIC, "non-finite or non-positive state; case stopped");
+  return ALP_OK;
+}
+
+int alp_engine_checkpoint_case(alp_engine *e, int case_id, alp_case_checkpoint *info,
+                               int *h_nbr26, double *h_blocks) {
+  if (!e || !info) return fail(ALP_ERR_INVALID, "null argument");
+  if (case_id < 0 || case_id >= e->max_cases || !e->case_rec[case_id].live)
+    return fail(ALP_ERR_NOT_FOUND, "unknown case");
+  if (int rc = alp_engine_get_case(e, case_id, h_blocks, nullptr, nullptr)) return rc;
+  auto const &c = e->case_rec[case_id];
+  CaseState cs;
+  ALP_CUDA(cudaMemcpyAsync(&cs, e->cases + case_id, sizeof(cs), cudaMemcpyDeviceToHost, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  info->dim = e->dim;
+  info->nb = c.nb;
+  info->steps = cs.steps;
+  info->max_steps = cs.max_steps;
+  info->t = cs.t;
+  info->t_end = cs.t_end;
+  info->cfl = cs.cfl;
+  info->cell_size = c.cell_size;
+  info->material = c.mat;
+  if (h_nbr26)
+    for (size_t i = 0; i < (size_t)c.nb * 26; ++i) {
+      int const n = e->h_nbr26[(size_t)c.first * 26 + i];
+      h_nbr26[i] = n < 0 ? n : n - c.first;
+    }
+  return ALP_OK;
+}
+
+int alp_engine_restore_case(alp_engine *e, const alp_case_checkpoint *info, const int *h_nbr26,
+                            const double *h_blocks, int *case_id) {
+  if (!e || !info || !case_id) return fail(ALP_ERR_INVALID, "null argument");
+  if (info->dim != e->dim) return fail(ALP_ERR_INVALID, "checkpoint of another dimension");
+  if (info->steps < 0) return fail(ALP_ERR_INVALID, "negative step count");
+  int cid;
+  if (int rc = alp_engine_add_case(e, &info->material, info->cell_size, info->cfl, info->t,
+                                   info->t_end, info->max_steps, info->nb, h_nbr26, h_blocks,
+                                   &cid))
+    return rc;
+  // the step count carries on from the checkpoint (max_steps counts from the start)
+  e->h_case_state[cid].steps = info->steps;
+  ALP_CUDA(cudaMemcpyAsync(e->cases + cid, &e->h_case_state[cid], sizeof(CaseState),
+                           cudaMemcpyHostToDevice, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  *case_id = cid;
   return ALP_OK;
 }
 

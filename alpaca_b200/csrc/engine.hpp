@@ -71,6 +71,8 @@ struct alp_engine {
   struct CaseRec {
     bool live = false;
     int first = 0, nb = 0;
+    alp_material mat{};     // as given, for checkpoints
+    double cell_size = 0.0;
   };
   std::vector<CaseRec> case_rec;
   std::vector<int> h_work;

@@ -128,6 +128,14 @@ class Material(C.Structure):
         return cls(gamma, B, int(safe))
 
 
+class CaseCheckpoint(C.Structure):
+    """alp_case_checkpoint: what resuming one engine case needs beside its
+    neighbour table and blocks."""
+    _fields_ = [("dim", C.c_int), ("nb", C.c_int), ("steps", C.c_int), ("max_steps", C.c_int),
+                ("t", C.c_double), ("t_end", C.c_double), ("cfl", C.c_double),
+                ("cell_size", C.c_double), ("material", Material)]
+
+
 IC_QUADRANTS, IC_BLAST, IC_PROGRAM = 1, 2, 3
 
 
@@ -198,6 +206,8 @@ _SIGS = {
     "alp_engine_step": (C.c_int, [_V, C.c_int]),
     "alp_engine_get_case": (C.c_int, [_V, C.c_int, _D, _D, _I]),
     "alp_engine_all_done": (C.c_int, [_V, _I]),
+    "alp_engine_checkpoint_case": (C.c_int, [_V, C.c_int, C.POINTER(CaseCheckpoint), _I, _D]),
+    "alp_engine_restore_case": (C.c_int, [_V, C.POINTER(CaseCheckpoint), _I, _D, _I]),
     "alp_engine_stream": (_S, [_V]),
     "alp_engine_set_graph": (C.c_int, [_V, C.c_int]),
     "alp_engine_launches_per_step": (C.c_int, [_V]),

@@ -312,6 +312,30 @@ int alp_engine_step(alp_engine *e, int n);
  * may be null. */
 int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t, int *steps);
 
+/* Checkpoint and resume of one case: what the reference's restart file keeps
+ * of a simulation (RestartManager::WriteRestartFile / RestoreSimulation,
+ * input_output/restart_manager.h:66-68: the time, and every node's
+ * conservatives in the block layout), plus the case's own settings. A case
+ * restored from its checkpoint continues exactly as the uninterrupted case:
+ * state, time and step count are the same, and nothing else carries over
+ * between steps. */
+typedef struct {
+  int dim, nb;
+  int steps, max_steps;  /* steps taken; the step budget (<= 0: none) */
+  double t, t_end, cfl, cell_size;
+  alp_material material;
+} alp_case_checkpoint;
+
+/* Fills *info, and (when not null) h_nbr26 [nb][26] with the case-local
+ * neighbour table and h_blocks [nb][NE][cells] with the state (halos filled).
+ * Synchronises the engine stream. */
+int alp_engine_checkpoint_case(alp_engine *e, int case_id, alp_case_checkpoint *info,
+                               int *h_nbr26, double *h_blocks);
+/* Adds a case from a checkpoint (interiors of h_blocks read); its step count
+ * continues from info->steps. */
+int alp_engine_restore_case(alp_engine *e, const alp_case_checkpoint *info, const int *h_nbr26,
+                            const double *h_blocks, int *case_id);
+
 /* True (1) when every case is done; synchronises. */
 int alp_engine_all_done(alp_engine *e, int *done);
 

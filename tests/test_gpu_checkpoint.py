@@ -1,0 +1,54 @@
+"""Checkpoint and resume of engine cases (alp_engine_checkpoint_case /
+alp_engine_restore_case): a case written to a checkpoint file after some
+steps and restored into a new engine ends exactly where the uninterrupted case
+ends, bit for bit, with the same time and step count."""
+import numpy as np
+import pytest
+
+from alpaca_b200 import api, cases
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_resumed_case_equals_uninterrupted(cuda, tmp_path, dim):
+    case = {1: cases.sod_1d(), 2: cases.fourier_shock(2, dim=2, seed=3),
+            3: cases.fourier_shock(1, dim=3, seed=5)}[dim]
+    I = cases.interior(dim)
+    # uninterrupted: 20 steps, then the step budget of 25 ends the case
+    a = api.Engine(dim, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    ca = a.add_case(case, max_steps=25)
+    a.step(20)
+    mid_ref = a.get(ca)
+    a.step(10)
+    ua, ta, sa = a.get(ca)
+    a.close()
+    # interrupted after 20 steps, written to a file, resumed in a new engine
+    b = api.Engine(dim, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    cb = b.add_case(case, max_steps=25)
+    b.step(20)
+    path = str(tmp_path / "ck.npz")
+    api.save_checkpoint(path, b.checkpoint(cb))
+    b.close()
+    ck = api.load_checkpoint(path)
+    assert ck["steps"] == 20 and ck["t"] == mid_ref[1]
+    assert np.array_equal(ck["blocks"][I], mid_ref[0][I])
+    c = api.Engine(dim, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    cc = c.restore(ck)
+    c.step(10)
+    uc, tc, sc = c.get(cc)
+    c.close()
+    assert sa == sc == 25 and ta == tc
+    assert np.array_equal(ua[I], uc[I])
+
+
+def test_restore_rejects_another_dimension(cuda):
+    case = cases.sod_1d()
+    e = api.Engine(1, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    ck = e.checkpoint(e.add_case(case))
+    e.close()
+    e2 = api.Engine(2, "fvchar", capacity_blocks=64, max_cases=1)
+    from alpaca_b200 import native as N
+    with pytest.raises(N.AlpacaError):
+        e2.restore(ck)
+    e2.close()

@@ -258,8 +258,10 @@ class LevelEngine:
     with local time stepping; one CUDA graph per macro step."""
 
     def __init__(self, case: LevelCase, variant: str = "fvchar", precision: int = N.FP64,
-                 max_macro: int = 0, strict: bool = False):
+                 max_macro: int = 0, strict: bool = False, t0: float = 0.0):
         self.lib = N.lib(strict)
+        self.case, self.variant, self.precision = case, variant, precision
+        self.max_macro, self.t0 = max_macro, t0
         self.strict = strict
         self.dim = case.dim
         self.nleaf = case.nleaf
@@ -273,7 +275,7 @@ class LevelEngine:
         h = C.c_void_p()
         N.check(self.lib.alp_levels_create(
             case.dim, C.byref(sch), C.byref(mat), n0.ctypes.data_as(N._I), case.h0, case.nleaf,
-            level.ctypes.data_as(N._I), coord.ctypes.data_as(N._I), case.cfl, 0.0, case.t_end,
+            level.ctypes.data_as(N._I), coord.ctypes.data_as(N._I), case.cfl, t0, case.t_end,
             max_macro, u.ctypes.data_as(N._D), C.byref(h)), strict)
         self.h = h
 
@@ -299,6 +301,23 @@ class LevelEngine:
         N.check(self.lib.alp_levels_get(self.h, out.ctypes.data_as(N._D), C.byref(t), C.byref(m)),
                 self.strict)
         return out, t.value, m.value
+
+    def checkpoint(self) -> dict:
+        """The leaves, time and macro steps done (between macro steps nothing
+        else carries over: every jump-flux sum has been applied)."""
+        u, t, m = self.get()
+        return {"blocks": u, "t": t, "macro": m}
+
+    def restore(self, ck: dict, strict: bool = False) -> "LevelEngine":
+        """A new level engine for the same tree that continues from ck; the
+        macro-step budget counts the steps still to do."""
+        c = LevelCase(self.case.name, self.case.dim, self.case.n0, self.case.h0, self.case.level,
+                      self.case.coord, ck["blocks"], self.case.gamma, self.case.B, self.case.cfl,
+                      self.case.t_end)
+        left = self.max_macro - ck["macro"] if self.max_macro > 0 else 0
+        if self.max_macro > 0 and left <= 0:
+            raise ValueError("the checkpointed case has no macro steps left")
+        return LevelEngine(c, self.variant, self.precision, left, strict, ck["t"])
 
     def info(self) -> dict:
         ng, lm, lp = C.c_int(), C.c_int(), C.c_int()

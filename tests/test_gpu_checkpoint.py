@@ -52,3 +52,25 @@ def test_restore_rejects_another_dimension(cuda):
     with pytest.raises(N.AlpacaError):
         e2.restore(ck)
     e2.close()
+
+
+def test_resumed_level_case_equals_uninterrupted(cuda):
+    """A three-level 2D tree checkpointed after one macro step and resumed in a
+    new level engine ends where three uninterrupted macro steps end."""
+    c = cases.spherical_shock_levels(n0=4, dim=2, lmax=2)
+    a = api.LevelEngine(c, "fvchar", max_macro=3)
+    a.step(3)
+    ua, ta, ma = a.get()
+    a.close()
+    b = api.LevelEngine(c, "fvchar", max_macro=3)
+    b.step(1)
+    ck = b.checkpoint()
+    r = b.restore(ck)
+    b.close()
+    r.step(5)  # two macro steps are left
+    ur, tr, mr = r.get()
+    r.close()
+    I = cases.interior(2)
+    assert ma == 3 and ck["macro"] == 1 and mr == 2
+    assert ta == tr
+    assert np.array_equal(ua[I], ur[I])

@@ -264,10 +264,20 @@ __device__ __forceinline__ void predict_children(V const &val, double (&out)[1 <
   }
 }
 
-// Type 0 ghosts of one level: predicted from the parent level. Per field, the
-// parent cells under the filled part plus two on every side are staged in
-// shared memory; one thread per parent cell writes its children.
+// Type 0 ghosts of one level: predicted from the parent level. The parent
+// cells under the filled part plus two on every side are staged in shared
+// memory for all fields at once; then one thread per (field, parent cell)
+// writes the children.
 constexpr int kBox = IC / 2 + 4;  // parent cells of a whole octant plus the stencil reach
+
+template <int DIM>
+__host__ __device__ constexpr int predict_box_doubles() {
+  return kBox * (DIM > 1 ? kBox : 1) * (DIM > 2 ? kBox : 1);
+}
+template <int DIM>
+constexpr size_t predict_smem_bytes() {
+  return sizeof(double) * Geo<DIM>::NE * predict_box_doubles<DIM>();
+}
 
 template <int DIM>
 __global__ void __launch_bounds__(256)
@@ -276,7 +286,8 @@ ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double con
                      CaseState const *__restrict__ cu, int stage) {
   using G = Geo<DIM>;
   constexpr int B1 = DIM > 1 ? kBox : 1, B2 = DIM > 2 ? kBox : 1;
-  __shared__ double box[kBox * B1 * B2];
+  constexpr int BOX = predict_box_doubles<DIM>();
+  extern __shared__ double box[];  // [NE][kBox][B1][B2]
   GhostRec const &g = ghosts[blockIdx.x];
   int lo[3], hi[3];
   if (!ghost_part<DIM>(g, blockIdx.y, lo, hi)) return;
@@ -290,44 +301,46 @@ ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double con
     bn[e] = pn[e] + 4;
   }
   int const nbox = bn[0] * bn[1] * bn[2], npar = pn[0] * pn[1] * pn[2];
-  double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
-  for (int e = 0; e < G::NE; ++e) {
-    for (int t = threadIdx.x; t < nbox; t += blockDim.x) {
-      int const r[3] = {t / (bn[1] * bn[2]), (t / bn[2]) % bn[1], t % bn[2]};
-      int y[3] = {0, 0, 0}, k = 0;
-      for (int d = 0; d < 3; ++d) {
-        int dn = 0;
-        if (d < DIM) {
-          int gc = g.q[d] * IC + plo[d] - 2 + r[d];  // parent-level cell
-          gc = gc < 0 ? 0 : (gc >= g.ext[d] ? g.ext[d] - 1 : gc);
-          dn = gc / IC - g.q[d];
-          y[d] = gc - (g.q[d] + dn) * IC + G::fic(d);
-        }
-        k = 3 * k + dn + 1;
+  for (int t = threadIdx.x; t < nbox; t += blockDim.x) {
+    int const r[3] = {t / (bn[1] * bn[2]), (t / bn[2]) % bn[1], t % bn[2]};
+    int y[3] = {0, 0, 0}, k = 0;
+    for (int d = 0; d < 3; ++d) {
+      int dn = 0;
+      if (d < DIM) {
+        int gc = g.q[d] * IC + plo[d] - 2 + r[d];  // parent-level cell
+        gc = gc < 0 ? 0 : (gc >= g.ext[d] ? g.ext[d] - 1 : gc);
+        dn = gc / IC - g.q[d];
+        y[d] = gc - (g.q[d] + dn) * IC + G::fic(d);
       }
-      int const slot = g.nb[k];
-      double const *sb =
-          ghost_source(slot, nleaf, g.level - 1, Ug, UA, cu, stage) + (size_t)slot * G::BLOCK_DOUBLES;
-      box[(r[0] * B1 + r[1]) * B2 + r[2]] = sb[e * G::CELLS + G::cell(y[0], y[1], y[2])];
+      k = 3 * k + dn + 1;
     }
-    __syncthreads();
-    for (int t = threadIdx.x; t < npar; t += blockDim.x) {
-      int const r[3] = {t / (pn[1] * pn[2]) + 2, (t / pn[2]) % pn[1] + (DIM > 1 ? 2 : 0),
-                        t % pn[2] + (DIM > 2 ? 2 : 0)};
-      auto val = [&](int a, int b, int c) {
-        return box[((r[0] + a) * B1 + (DIM > 1 ? r[1] + b : 0)) * B2 + (DIM > 2 ? r[2] + c : 0)];
-      };
-      double out[1 << DIM];
-      predict_children<DIM>(val, out);
+    int const slot = g.nb[k];
+    double const *sb =
+        ghost_source(slot, nleaf, g.level - 1, Ug, UA, cu, stage) + (size_t)slot * G::BLOCK_DOUBLES;
+    int const c = G::cell(y[0], y[1], y[2]);
+    int const b = (r[0] * B1 + r[1]) * B2 + r[2];
 #pragma unroll
-      for (int o = 0; o < (1 << DIM); ++o) {
-        int a[3] = {0, 0, 0};
-        for (int d = 0; d < DIM; ++d)
-          a[d] = 2 * (plo[d] + r[d] - 2 - (IC / 2) * ((g.oct >> d) & 1)) + ((o >> d) & 1);
-        dst[e * G::CELLS + G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2))] = out[o];
-      }
+    for (int e = 0; e < G::NE; ++e) box[e * BOX + b] = sb[e * G::CELLS + c];
+  }
+  __syncthreads();
+  double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
+  for (int t = threadIdx.x; t < npar * G::NE; t += blockDim.x) {
+    int const e = t / npar, tp = t - e * npar;
+    int const r[3] = {tp / (pn[1] * pn[2]) + 2, (tp / pn[2]) % pn[1] + (DIM > 1 ? 2 : 0),
+                      tp % pn[2] + (DIM > 2 ? 2 : 0)};
+    double const *bx = box + e * BOX;
+    auto val = [&](int a, int b, int c) {
+      return bx[((r[0] + a) * B1 + (DIM > 1 ? r[1] + b : 0)) * B2 + (DIM > 2 ? r[2] + c : 0)];
+    };
+    double out[1 << DIM];
+    predict_children<DIM>(val, out);
+#pragma unroll
+    for (int o = 0; o < (1 << DIM); ++o) {
+      int a[3] = {0, 0, 0};
+      for (int d = 0; d < DIM; ++d)
+        a[d] = 2 * (plo[d] + r[d] - 2 - (IC / 2) * ((g.oct >> d) & 1)) + ((o >> d) & 1);
+      dst[e * G::CELLS + G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2))] = out[o];
     }
-    __syncthreads();
   }
 }
 
@@ -612,9 +625,9 @@ struct alp_levels {
             }
           } else {
             switch (dim) {
-              case 1: ghost_predict_kernel<1><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              case 2: ghost_predict_kernel<2><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              default: ghost_predict_kernel<3><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              case 1: ghost_predict_kernel<1><<<grid, 256, predict_smem_bytes<1>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              case 2: ghost_predict_kernel<2><<<grid, 256, predict_smem_bytes<2>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
+              default: ghost_predict_kernel<3><<<grid, 256, predict_smem_bytes<3>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
             }
           }
           ALP_CUDA(cudaGetLastError());
@@ -1091,6 +1104,13 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   };
   cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaStreamCreate"));
+  // the 3D prediction kernel stages 69 KB of parent cells: above the default
+  // 48 KB of dynamic shared memory, so it is allowed here, before any capture
+  if (dim == 3) {
+    e = cudaFuncSetAttribute(ghost_predict_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)predict_smem_bytes<3>());
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaFuncSetAttribute(ghost_predict_kernel)"));
+  }
   void **bufs[] = {(void **)&m->U, (void **)&m->UB, (void **)&m->UC};
   for (void **b : bufs) {
     e = cudaMalloc(b, pool);

@@ -20,7 +20,8 @@
 // Jumps: the face kernels gather stencil cells from a neighbour block's
 // interior. Where the face neighbour of a leaf is one level coarser or finer,
 // the neighbour slot is a ghost block: a virtual node of the leaf's level whose
-// three cell layers next to the shared face are filled before each stage. On
+// cell layers next to the shared face that the stencils reach (three, four for
+// WENO7) are filled before each stage. On
 // the coarse side they average the finer leaves (Multiresolution::Average,
 // multiresolution.h:94-166); on the fine side they are the fifth-order
 // prediction from the coarser level (Multiresolution::Prediction,
@@ -80,13 +81,14 @@ struct LevelState {
 // which reads the 3^dim nodes nb[] around the parent position q (nb index
 // (dx+1)*9 + (dy+1)*3 + (dz+1); cells beyond the domain take the value of the
 // nearest domain cell, zero gradient); oct is the ghost's octant in its parent.
-// A ghost the face kernels read fills the three cell layers next to each face
+// A ghost the face kernels read fills the `layers` cell layers next to each face
 // in `faces` (bits W, E, S, N, B, T); a ghost other ghosts read (`full`: its
 // sources are all resolved) also fills the box of cells those reads reach,
 // lo[e] <= cell < hi[e]. Slots below nleaf are leaves, read from the pool of
 // their level. gate: the finest level whose computing needs the ghost.
 struct GhostRec {
   int slot, type, level, gate, faces, full, oct;
+  int layers;        // cell layers next to a served face: the stencil's reach (3, WENO7 4)
   int lo[3], hi[3];  // the box other ghosts read (empty: lo >= hi)
   int q[3], ext[3];  // parent position (nodes) and level extent (cells) of the parent level
   int src[8];
@@ -136,8 +138,8 @@ __device__ __forceinline__ bool ghost_part(GhostRec const &g, int part, int lo[3
     hi[e] = e < DIM ? IC : 1;
   }
   int const d = part / 2;
-  lo[d] = (part & 1) ? IC - 3 : 0;
-  hi[d] = lo[d] + 3;
+  lo[d] = (part & 1) ? IC - g.layers : 0;
+  hi[d] = lo[d] + g.layers;
   return true;
 }
 
@@ -375,7 +377,9 @@ __device__ __forceinline__ void interior_coords_of(int t, int &i, int &j, int &k
 }
 
 // RK3 jump multipliers (runge_kutta_3_TVD.h:42-46)
-__constant__ double kRkJump[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+// jump multipliers per stage: SSP-RK3 (runge_kutta_3_TVD.h:42-46), then
+// TVD-RK2 (runge_kutta_2_TVD.h:40-44), as the stage tables of the update kernel
+__constant__ double kRkJump[5] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0, 0.5, 0.5};
 
 template <int DIM> struct FaceCells {
   __host__ __device__ static int t1(int d) { return d == 0 ? 1 : 0; }
@@ -574,6 +578,7 @@ struct GhostGroup {
 
 struct alp_levels {
   int dim = 3, scheme = 0, precision = 0, lmax = 0, nlev = 1, nmicro = 1;
+  bool rk2 = false;  // TVD-RK2: two stages (stage tables from entry 3)
   alp::SchemeOptions opt;
   int nleaf = 0, nghost = 0, nslots = 0, ne = 5, cells = 0, faces = 0;
   long long cell_updates_per_macro = 0;
@@ -603,6 +608,8 @@ struct alp_levels {
     L.opt = opt;
     double *in[3] = {U, UB, UC};
     double *out[3] = {UB, UC, U};
+    int const nst = rk2 ? 2 : 3, s0 = rk2 ? 3 : 0;
+    if (rk2) out[1] = U;
     for (int tm = 0; tm < nmicro; ++tm) {
       Launch La = L;
       ALP_CUDA(launch_signal_speed(La, cu, nullptr));
@@ -611,7 +618,7 @@ struct alp_levels {
       auto height = [](int t) { return __builtin_popcount((unsigned)((t + 1) ^ t)); };
       int const lu = lmax - height(tm) + 1;
       int const lf = tm == 0 ? 0 : lmax - height(tm - 1) + 1;
-      for (int s = 0; s < 3; ++s) {
+      for (int s = 0; s < nst; ++s) {
         CaseState const *gate = s == 0 ? cf : cu;
         // averaged ghosts finest level first, then predicted ones coarsest first
         for (GhostGroup const &gg : ghost_groups) {
@@ -639,12 +646,12 @@ struct alp_levels {
           ALP_CUDA(launch_face_flux_all(Ls, nbr26, gate, F, stride(), dstride(), 128));
         Ls.nwork = nwork_ge[lu];
         if (Ls.nwork > 0)
-          ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s, cu, 0.0));
+          ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s0 + s, cu, 0.0));
         if (nrec > 0) {
           switch (dim) {
-            case 1: jump_accumulate_kernel<1><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
-            case 2: jump_accumulate_kernel<2><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
-            default: jump_accumulate_kernel<3><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s); break;
+            case 1: jump_accumulate_kernel<1><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
+            case 2: jump_accumulate_kernel<2><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
+            default: jump_accumulate_kernel<3><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
           }
           ALP_CUDA(cudaGetLastError());
         }
@@ -698,7 +705,7 @@ struct alp_levels {
 namespace {
 
 // Validates the tree and builds the per-slot neighbour table and the ghosts.
-int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const *coord,
+int build_tree(int dim, int layers, int const n0[3], int nleaf, int const *level, int const *coord,
                std::vector<int> &nbr26, std::vector<GhostRec> &ghosts,
                std::vector<JumpFace> &jumps, int *lmax_out) {
   using alp::fail;
@@ -763,6 +770,7 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
     GhostRec gr{};
     gr.slot = nleaf + (int)ghosts.size();
     gr.level = k.l;
+    gr.layers = layers;
     gr.gate = -1;
     for (int o = 0; o < 8; ++o) gr.src[o] = -1;
     for (int o = 0; o < 27; ++o) gr.nb[o] = -1;
@@ -942,8 +950,8 @@ int build_tree(int dim, int const n0[3], int nleaf, int const *level, int const 
         if ((g.faces >> f) & 1) {
           int a[3] = {0, 0, 0}, b[3] = {1, 1, 1};
           for (int e = 0; e < dim; ++e) b[e] = IC;
-          a[f / 2] = (f & 1) ? IC - 3 : 0;
-          b[f / 2] = a[f / 2] + 3;
+          a[f / 2] = (f & 1) ? IC - layers : 0;
+          b[f / 2] = a[f / 2] + layers;
           add(a, b);
         }
       if (!any) continue;
@@ -1005,11 +1013,6 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
   int sid, prec;
   if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
-  if (scheme->reconstruction_stencil == ST_WENO7)
-    return fail(ALP_ERR_INVALID,
-                "WENO7 reads four cells across a face; multi-level ghost blocks hold three");
-  if (scheme->time_integrator != ALP_RK3)
-    return fail(ALP_ERR_INVALID, "multi-level cases integrate with RK3 (its jump multipliers)");
   if (sid == FS_ROE && scheme->flux_splitting == FSP_GLF)
     return fail(ALP_ERR_INVALID,
                 "GlobalLaxFriedrichs takes its maxima over the levels integrated in each micro "
@@ -1026,7 +1029,8 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   std::vector<GhostRec> gh;
   std::vector<JumpFace> jf;
   int lmax = 0;
-  if (int rc = build_tree(dim, n0v, nleaf, h_level, h_coord, nbr, gh, jf, &lmax)) return rc;
+  int const layers = scheme->reconstruction_stencil == ST_WENO7 ? 4 : 3;
+  if (int rc = build_tree(dim, layers, n0v, nleaf, h_level, h_coord, nbr, gh, jf, &lmax)) return rc;
 
   alp_levels *m = new (std::nothrow) alp_levels;
   if (!m) return fail(ALP_ERR_CUDA, "host allocation failed");
@@ -1034,6 +1038,7 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   m->scheme = sid;
   m->precision = prec;
   m->opt = scheme_options(scheme);
+  m->rk2 = scheme->time_integrator == ALP_RK2;
   m->lmax = lmax;
   m->nlev = lmax + 1;
   m->nmicro = 1 << lmax;
@@ -1259,7 +1264,7 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
       int const lu = m->lmax - height(tm) + 1;
       int const lf = tm == 0 ? 0 : m->lmax - height(tm - 1) + 1;
       n += per_micro;
-      for (int s = 0; s < 3; ++s) {
+      for (int s = 0; s < (m->rk2 ? 2 : 3); ++s) {
         n += (int)m->ghost_groups.size();
         n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? 1 : 0;
         n += m->nwork_ge[lu] > 0 ? 1 : 0;

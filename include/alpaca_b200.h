@@ -386,7 +386,8 @@ int alp_engine_launches_per_step(alp_engine *e);
  * positions the prediction reads that are not leaves are averaged or predicted
  * in turn. Conservation at jumps as JumpFluxAdjustment
  * (modular_algorithm_assembler.cpp:1347-1636): jump-face fluxes integrated
- * with the RK3 jump multipliers, fine sums averaged onto the parent faces
+ * with the integrator's jump multipliers (SSP-RK3 1/6, 1/6, 2/3; TVD-RK2 1/2, 1/2),
+ * fine sums averaged onto the parent faces
  * after each fine step, coarse cells corrected after each coarse step.
  * h_blocks: [nleaf][NE][cells], interiors read. All levels run in the same
  * batched launches; one CUDA graph per macro step. */

@@ -1857,6 +1857,8 @@ static void level_rhs_task(void *vctx, int i, Work *w, double *f[3]) {
 
 /* RK3 jump multipliers (runge_kutta_3_TVD.h:42-46) */
 static const double rk_jump[3] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0};
+/* TVD-RK2 jump multipliers (runge_kutta_2_TVD.h:40-44) */
+static const double rk2_jump[3] = {0.5, 0.5, 0.0};
 
 /* End of micro step tm for the levels >= lu (they just finished a step with
  * a positive level step): AverageJumpBuffer of the finished fine leaves onto
@@ -1970,7 +1972,6 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                       double *t_io, int *macro_done, double *dt_log) {
   if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
   if (glf_selected(solver)) return 4; /* global maxima over the levels due: not restated */
-  if (g_integrator != TI_RK3) return 5; /* RK3 jump multipliers only */
   Geom g = make_geom(dim);
   Eos e = {dim, gamma, B, safe};
   Tree tr;
@@ -2006,6 +2007,12 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
   memcpy(pc, u, sizeof(double) * n);
   double *pool_in[3] = {u, pb, pc};
   double *pool_out[3] = {pb, pc, u};
+  /* SSP-RK3 or TVD-RK2 (the last stage writes the state pool) */
+  int const nst = rk_stages();
+  const double(*rka)[2] = g_integrator == TI_RK2 ? rk2_a : rk3_a;
+  const double *const rkc = g_integrator == TI_RK2 ? rk2_c : rk3_c;
+  const double *const rkj = g_integrator == TI_RK2 ? rk2_jump : rk_jump;
+  if (nst == 2) pool_out[1] = u;
   double const h_fine = h0 / (double)nmicro;
   double t = *t_io;
   int macro = 0, logged = 0;
@@ -2020,7 +2027,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
       ++logged;
       int const lu = lmax - get_levels_height((unsigned)tm) + 1;
       int const lf0 = tm == 0 ? 0 : lmax - get_levels_height((unsigned)(tm - 1)) + 1;
-      for (int s = 0; s < 3; ++s) {
+      for (int s = 0; s < nst; ++s) {
         int const lflux = s == 0 ? lf0 : lu;
         double *src[MAXLEV];
         for (int l = 0; l <= lmax; ++l) src[l] = (s > 0 && l >= lu) ? pool_in[s] : u;
@@ -2041,8 +2048,8 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
           double dtl = 0.0;
           for (int k = tm; k > tm - (1 << (lmax - l)); --k) dtl += hist[k];
           if (!(dtl > 0.0)) continue;
-          double const step = rk_c[s] * (0.0 + dtl);
-          double const m0 = rk_a[s][0], m1 = rk_a[s][1];
+          double const step = rkc[s] * (0.0 + dtl);
+          double const m0 = rka[s][0], m1 = rka[s][1];
           const double *ui = pool_in[s] + b * blk, *u0 = u + b * blk, *r = rhs + b * blk;
           double *uo = pool_out[s] + b * blk;
           for (int f = 0; f < g.ne; ++f)
@@ -2055,7 +2062,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                   uo[x] = v + step * r[x];
                 }
           /* IntegrateJumpConservatives: jump faces integrate their fluxes */
-          double const jstep = rk_jump[s] * dtl;
+          double const jstep = rkj[s] * dtl;
           for (int loc = 0; loc < 2 * dim; ++loc) {
             int pn[3];
             int const kind = face_kind(&tr, b, loc, pn);

@@ -135,3 +135,35 @@ def test_spherical_shock_hierarchy_runs(cuda):
     assert np.isfinite(got[I]).all() and (got[I][:, 0] > 0).all()
     assert info["cell_updates_per_macro_step"] == c.cell_updates_per_macro_step()
     assert info["ghosts"] > 0 and info["launches_per_macro_step"] > 0
+
+
+@pytest.mark.parametrize("variant", ["rk2_fvchar_weno3", "rk2_fs_llf_weno5z", "fvchar_weno7",
+                                     "rk2_fvchar_weno7"])
+@pytest.mark.parametrize("name", ["2d_three_levels", "3d_corner_three_levels"])
+def test_levels_rk2_and_weno7_strict_bit_exact(cuda, name, variant):
+    """TVD-RK2 (two stages, jump multipliers 1/2, 1/2) and WENO7 (ghosts four
+    cells deep) on multi-level trees: the strict build against the oracle."""
+    c = small_trees()[name]
+    ref, t_ref, m_ref, _ = reference_run(c, variant, 1)
+    eng = api.LevelEngine(c, variant, max_macro=1, strict=True)
+    eng.step(1)
+    got, t, m = eng.get()
+    eng.close()
+    I = cases.interior(c.dim)
+    assert m == 1 and t == t_ref
+    assert np.isfinite(ref[I]).all()
+    assert np.array_equal(got[I], ref[I])
+
+
+def test_levels_rk2_conserve_mass_and_energy(cuda):
+    c = small_trees()["2d_three_levels"]
+    eng = api.LevelEngine(c, "rk2_fvchar_weno3", max_macro=2)
+    eng.step(2)
+    got = eng.get()[0]
+    eng.close()
+    I = cases.interior(2)
+    vol = (c.h0 / (1 << c.level)) ** 2
+    for f in (0, 1):
+        a = (c.u[I][:, f].reshape(c.nleaf, -1).sum(1) * vol).sum()
+        b = (got[I][:, f].reshape(c.nleaf, -1).sum(1) * vol).sum()
+        assert abs(b - a) <= 1e-14 * a, f

@@ -85,6 +85,19 @@ def test_three_level_tree_conserves_mass_and_energy(dim, macro):
     assert abs(b[0] - a[0]) <= 1e-14 * a[0] and abs(b[1] - a[1]) <= 1e-14 * a[1]
 
 
+def test_rk2_three_level_tree_conserves_mass_and_energy():
+    """TVD-RK2 on a three-level 2D tree: jump multipliers 1/2, 1/2 keep the
+    jump-flux correction exact."""
+    c = cases.spherical_shock_levels(n0=4, dim=2, lmax=2)
+    u, t, m, dts = oracle.Restatement(2, "rk2_fvchar_weno3").levels_run(
+        c.u, c.level, c.coord, c.n0, c.h0, c.gamma, 0.0, False, 0.6, 1e300, max_macro=2,
+        nthreads=4)
+    I = cases.interior(2)
+    assert m == 2 and np.isfinite(u[I]).all()
+    a, b = totals(c, c.u), totals(c, u)
+    assert abs(b[0] - a[0]) <= 1e-14 * a[0] and abs(b[1] - a[1]) <= 1e-14 * a[1]
+
+
 def test_leaves_per_level_of_the_spherical_shock_hierarchy():
     c = cases.spherical_shock_levels()
     assert c.leaves_per_level() == [8, 294, 1232]

@@ -346,6 +346,16 @@ ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double con
   }
 }
 
+// The GlobalLaxFriedrichs maxima of all levels into every level's words (bit
+// patterns of non-negative doubles order as the values).
+__global__ void glf_fold_kernel(unsigned long long *glf, int nlev) {
+  int const k = threadIdx.x;
+  if (k >= 3) return;
+  unsigned long long m = 0ull;
+  for (int l = 0; l < nlev; ++l) m = glf[4 * l + k] > m ? glf[4 * l + k] : m;
+  for (int l = 0; l < nlev; ++l) glf[4 * l + k] = m;
+}
+
 // A jump face of a leaf: kind 2 (coarse side: the neighbour is refined) or 3
 // (fine side: the neighbour lies in a coarser leaf). Face loc: East 0, West 1,
 // North 2, South 3, Top 4, Bottom 5 (boundary_specifications.h:56-63). acc:
@@ -596,6 +606,9 @@ struct alp_levels {
   CorrectRec *jcorr = nullptr;
   CaseState *cu = nullptr, *cf = nullptr;
   LevelState *ls = nullptr;
+  // GlobalLaxFriedrichs: wave-speed maxima, 4 words per level (all levels hold
+  // the maxima over the leaves computing in the stage); null unless selected
+  unsigned long long *glf = nullptr;
   std::vector<int> nwork_ge;  // work items of level >= l
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -606,6 +619,7 @@ struct alp_levels {
   int record_macro() {
     Launch L{dim, scheme, precision, U, work, nleaf, meta, BlockMeta{}, stream};
     L.opt = opt;
+    L.glf = glf;
     double *in[3] = {U, UB, UC};
     double *out[3] = {UB, UC, U};
     int const nst = rk2 ? 2 : 3, s0 = rk2 ? 3 : 0;
@@ -642,6 +656,14 @@ struct alp_levels {
         Launch Ls = L;
         Ls.U = in[s];
         Ls.nwork = nwork_ge[s == 0 ? lf : lu];
+        if (glf && Ls.nwork > 0) {
+          // maxima over the leaves computing now (ComputeRightHandSide over its
+          // levels, modular_algorithm_assembler.cpp:957-988): per level, then
+          // the largest into every level's words
+          ALP_CUDA(launch_glf_maxima(Ls, glf, nlev));
+          glf_fold_kernel<<<1, 32, 0, stream>>>(glf, nlev);
+          ALP_CUDA(cudaGetLastError());
+        }
         if (Ls.nwork > 0)
           ALP_CUDA(launch_face_flux_all(Ls, nbr26, gate, F, stride(), dstride(), 128));
         Ls.nwork = nwork_ge[lu];
@@ -698,6 +720,7 @@ struct alp_levels {
     cudaFree(cu);
     cudaFree(cf);
     cudaFree(ls);
+    cudaFree(glf);
     if (stream) cudaStreamDestroy(stream);
   }
 };
@@ -1013,10 +1036,6 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
   int sid, prec;
   if (int rc = scheme_id(scheme, &sid, &prec)) return rc;
-  if (sid == FS_ROE && scheme->flux_splitting == FSP_GLF)
-    return fail(ALP_ERR_INVALID,
-                "GlobalLaxFriedrichs takes its maxima over the levels integrated in each micro "
-                "step; multi-level cases do not support it");
   if (int rc = check_material(mat)) return rc;
   if (!n0 || !h_level || !h_coord || !h_blocks || nleaf <= 0)
     return fail(ALP_ERR_INVALID, "empty or null tree description");
@@ -1130,7 +1149,9 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
       (e = cudaMalloc(&m->ghosts, sizeof(GhostRec) * std::max(m->nghost, 1))) != cudaSuccess ||
       (e = cudaMalloc(&m->cu, sizeof(CaseState) * m->nlev)) != cudaSuccess ||
       (e = cudaMalloc(&m->cf, sizeof(CaseState) * m->nlev)) != cudaSuccess ||
-      (e = cudaMalloc(&m->ls, sizeof(LevelState))) != cudaSuccess)
+      (e = cudaMalloc(&m->ls, sizeof(LevelState))) != cudaSuccess ||
+      (sid == FS_ROE && scheme->flux_splitting == FSP_GLF &&
+       (e = cudaMalloc(&m->glf, sizeof(unsigned long long) * 4 * m->nlev)) != cudaSuccess))
     return cleanup(cuda_fail(e, "cudaMalloc(level tables)"));
   size_t const jface = (size_t)m->ne * IC * IC * sizeof(double);
   if (m->nrec > 0) {
@@ -1266,7 +1287,7 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
       n += per_micro;
       for (int s = 0; s < (m->rk2 ? 2 : 3); ++s) {
         n += (int)m->ghost_groups.size();
-        n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? 1 : 0;
+        n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? (m->glf ? 3 : 1) : 0;  // GLF: maxima, fold
         n += m->nwork_ge[lu] > 0 ? 1 : 0;
         n += m->nrec > 0 ? 1 : 0;
       }

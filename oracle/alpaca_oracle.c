@@ -742,6 +742,33 @@ static void glf_maxima(const Geom *g, const Eos *e, const double *u, int nb) {
   for (int q = 0; q < 3; ++q) g_glf[q] = m[q];
 }
 
+/* The same maxima over the leaves items[0..ni) whose right-hand side is
+ * computed (ComputeRightHandSide takes them over the leaves of the levels it
+ * is given, modular_algorithm_assembler.cpp:957-988); leaf b's state is src[level]. */
+static void glf_maxima_leaves(const Geom *g, const Eos *e, double *const *src, const int *level,
+                              const int *items, int ni) {
+  double m[3] = {0.0, 0.0, 0.0};
+  double c[MAXNE], p[MAXNE];
+  for (int n = 0; n < ni; ++n) {
+    int const b = items[n];
+    const double *ub = src[level[b]] + (long)b * g->ne * g->cells;
+    for (int i = fic(g, 0); i <= lic(g, 0); ++i)
+      for (int j = fic(g, 1); j <= lic(g, 1); ++j)
+        for (int k = fic(g, 2); k <= lic(g, 2); ++k) {
+          long const x = cidx(g, i, j, k);
+          for (int f = 0; f < g->ne; ++f) c[f] = ub[f * g->cells + x];
+          cons_to_prim(e, c, p);
+          if (p[RHO] <= 0.0) continue;
+          double const cs = eos_speed_of_sound(e, p[RHO], p[PRES]);
+          double const vx = p[VELX];
+          m[0] = dmax(m[0], fabs(vx - cs));
+          m[1] = dmax(m[1], fabs(vx));
+          m[2] = dmax(m[2], fabs(vx + cs));
+        }
+  }
+  for (int q = 0; q < 3; ++q) g_glf[q] = m[q];
+}
+
 static int glf_selected(int solver) {
   return solver == ORACLE_FLUX_SPLITTING && g_splitting == FSP_GLF;
 }
@@ -1220,9 +1247,6 @@ static const double rk3_c[3] = {1.0, 0.25, 2.0 / 3.0};
 static const double rk3_a[3][2] = {{0.0, 0.0}, {0.25, 0.75}, {2.0 / 3.0, 1.0 / 3.0}};
 static const double rk2_c[3] = {1.0, 0.5, 0.0};
 static const double rk2_a[3][2] = {{0.0, 0.0}, {0.5, 0.5}, {0.0, 0.0}};
-/* the multi-level loop is RK3 only */
-static const double *const rk_c = rk3_c;
-static const double (*const rk_a)[2] = rk3_a;
 static int rk_stages(void) { return g_integrator == TI_RK2 ? 2 : 3; }
 
 int oracle_set_time_integrator(int integrator) {
@@ -1971,7 +1995,6 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
                       int safe, double cfl, double t_end, int max_macro, int nthreads,
                       double *t_io, int *macro_done, double *dt_log) {
   if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
-  if (glf_selected(solver)) return 4; /* global maxima over the levels due: not restated */
   Geom g = make_geom(dim);
   Eos e = {dim, gamma, B, safe};
   Tree tr;
@@ -2040,6 +2063,7 @@ int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf, cons
             items[ni++] = b;
           }
         lf_free(&field);
+        if (glf_selected(solver)) glf_maxima_leaves(&g, &e, src, level, items, ni);
         LevelRhsCtx c = {&g, &e, solver, recon, &tr, items, pool_in[s], rhs, bflux, h0};
         parallel_blocks(&g, ni, nthreads, level_rhs_task, &c);
         for (int b = 0; b < nleaf; ++b) {

@@ -138,11 +138,12 @@ def test_spherical_shock_hierarchy_runs(cuda):
 
 
 @pytest.mark.parametrize("variant", ["rk2_fvchar_weno3", "rk2_fs_llf_weno5z", "fvchar_weno7",
-                                     "rk2_fvchar_weno7"])
+                                     "rk2_fvchar_weno7", "fs_glf", "rk2_fs_glf"])
 @pytest.mark.parametrize("name", ["2d_three_levels", "3d_corner_three_levels"])
 def test_levels_rk2_and_weno7_strict_bit_exact(cuda, name, variant):
-    """TVD-RK2 (two stages, jump multipliers 1/2, 1/2) and WENO7 (ghosts four
-    cells deep) on multi-level trees: the strict build against the oracle."""
+    """TVD-RK2 (two stages, jump multipliers 1/2, 1/2), WENO7 (ghosts four
+    cells deep) and GlobalLaxFriedrichs (maxima over the leaves computing in
+    each stage) on multi-level trees: the strict build against the oracle."""
     c = small_trees()[name]
     ref, t_ref, m_ref, _ = reference_run(c, variant, 1)
     eng = api.LevelEngine(c, variant, max_macro=1, strict=True)

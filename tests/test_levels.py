@@ -141,18 +141,18 @@ def test_invalid_trees_are_rejected(what):
     assert msg
 
 
-def test_global_lax_friedrichs_is_rejected_for_levels():
-    """The reference takes the GLF maxima over the levels integrated in each
-    micro step; the multi-level engine does not restate that and says so."""
-    lib = N.lib()
-    sch = N.Scheme.make("fs_glf")
-    mat = N.Material.make(1.4)
-    level = np.zeros(2, dtype=np.int32)
-    coord = np.array([[0, 0, 0], [1, 0, 0]], dtype=np.int32)
-    n0 = np.array([2, 1, 1], dtype=np.int32)
-    u = np.zeros((2, 3) + cases.block_shape(1))
-    h = C.c_void_p()
-    rc = lib.alp_levels_create(1, C.byref(sch), C.byref(mat), n0.ctypes.data_as(N._I), 1 / 32,
-                               2, level.ctypes.data_as(N._I), coord.ctypes.data_as(N._I), 0.6,
-                               0.0, 1.0, 1, u.ctypes.data_as(N._D), C.byref(h))
-    assert rc == N.ALP_ERR_INVALID and b"GlobalLaxFriedrichs" in lib.alp_last_error()
+def test_global_lax_friedrichs_three_level_tree_conserves():
+    """GlobalLaxFriedrichs on a three-level tree: the wave speeds are the maxima
+    over the leaves computing in each stage (as ComputeRightHandSide takes
+    them over the levels it is given); mass and energy stay conserved. No
+    density blobs: their tails reach the zero-gradient domain faces, where the
+    global wave speed's dissipation moves mass through the faces (6e-9 of it
+    in two macro steps on a single level too)."""
+    c = cases.spherical_shock_levels(n0=4, dim=2, lmax=2, nblobs=0)
+    u, t, m, dts = oracle.Restatement(2, "fs_glf").levels_run(
+        c.u, c.level, c.coord, c.n0, c.h0, c.gamma, 0.0, False, 0.6, 1e300, max_macro=2,
+        nthreads=4)
+    I = cases.interior(2)
+    assert m == 2 and np.isfinite(u[I]).all()
+    a, b = totals(c, c.u), totals(c, u)
+    assert abs(b[0] - a[0]) <= 1e-14 * a[0] and abs(b[1] - a[1]) <= 1e-14 * a[1]

@@ -402,7 +402,7 @@ int alp_levels_step(alp_levels *m, int n_macro);
 /* Copies the leaves (interiors valid) and the time / macro steps reached;
  * synchronises. ALP_ERR_NUMERIC once a non-finite state stopped the case. */
 int alp_levels_get(alp_levels *m, double *h_blocks, double *t, int *macro_steps);
-/* Ghost blocks at level jumps, finest level, interior cells x RK3 steps per
+/* Ghost blocks at level jumps, finest level, interior cells x time steps per
  * macro step summed over the leaves, kernel launches per macro step. */
 int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
                     long long *cell_updates_per_macro_step, int *launches_per_macro_step);

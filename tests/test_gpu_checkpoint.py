@@ -74,3 +74,37 @@ def test_resumed_level_case_equals_uninterrupted(cuda):
     assert ma == 3 and ck["macro"] == 1 and mr == 2
     assert ta == tr
     assert np.array_equal(ua[I], ur[I])
+
+
+def test_restore_beside_a_running_case(cuda):
+    """Restored into an engine that already runs another case (so at another
+    place in the block pool): the restored case still ends where the
+    uninterrupted one ends, and the other case is untouched."""
+    sod = cases.sod_1d()
+    other = cases.sod_1d(nblocks=6)
+    ref = api.Engine(1, "fvchar", capacity_blocks=16, max_cases=2)
+    r = ref.add_case(sod)
+    ref.step(30)
+    u_ref, t_ref, s_ref = ref.get(r)
+    ref.close()
+    a = api.Engine(1, "fvchar", capacity_blocks=16, max_cases=2)
+    ca = a.add_case(sod)
+    a.step(12)
+    ck = a.checkpoint(ca)
+    a.close()
+    b = api.Engine(1, "fvchar", capacity_blocks=32, max_cases=3)
+    ob = b.add_case(other)
+    b.step(5)
+    cb = b.restore(ck)
+    b.step(18)
+    u, t, s = b.get(cb)
+    uo, to, so = b.get(ob)
+    b.close()
+    solo = api.Engine(1, "fvchar", capacity_blocks=16, max_cases=1)
+    oo = solo.add_case(other)
+    solo.step(23)
+    u_solo, t_solo, s_solo = solo.get(oo)
+    solo.close()
+    I = cases.interior(1)
+    assert s == s_ref == 30 and t == t_ref and np.array_equal(u[I], u_ref[I])
+    assert so == s_solo == 23 and to == t_solo and np.array_equal(uo[I], u_solo[I])

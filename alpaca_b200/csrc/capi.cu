@@ -1,6 +1,7 @@
 // C ABI (include/alpaca_b200.h): stateless drop-in calls and the engine that
 // keeps cases device-resident and replays its step as a CUDA graph.
 #include <cuda_runtime.h>
+#include <nvtx3/nvtx3.hpp>
 
 #include <algorithm>
 #include <cstdio>
@@ -516,6 +517,8 @@ int alp_engine_remove_case(alp_engine *e, int case_id) {
 int alp_engine_step(alp_engine *e, int n) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");
   if (n <= 0 || e->nwork == 0) return ALP_OK;
+  // profiler ranges (no cost unless a tool is attached): one per call, one per capture
+  nvtx3::scoped_range range{"alp_engine_step"};
   if (!e->use_graph) {
     for (int i = 0; i < n; ++i)
       if (int rc = e->record_step()) return rc;
@@ -527,6 +530,7 @@ int alp_engine_step(alp_engine *e, int n) {
       e->graph = nullptr;
     }
     cudaGraph_t g;
+    nvtx3::scoped_range capture{"alp_engine_step: capture the step graph"};
     ALP_CUDA(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
     int const rc = e->record_step();
     cudaError_t const ce = cudaStreamEndCapture(e->stream, &g);

@@ -44,6 +44,7 @@
 // - CMS(coarse sums) + CMS(fine sums) per unit cell size (JumpFluxAdjustment,
 // modular_algorithm_assembler.cpp:1347-1636).
 #include <cuda_runtime.h>
+#include <nvtx3/nvtx3.hpp>
 
 #include <algorithm>
 #include <cfloat>
@@ -1239,6 +1240,7 @@ int alp_levels_destroy(alp_levels *m) {
 int alp_levels_step(alp_levels *m, int n_macro) {
   if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
   if (n_macro <= 0) return ALP_OK;
+  nvtx3::scoped_range range{"alp_levels_step"};
   if (!m->graph) {
     cudaGraph_t g;
     ALP_CUDA(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));

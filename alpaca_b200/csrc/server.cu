@@ -20,6 +20,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvtx3.hpp>
+
 #include "engine.hpp"
 
 namespace {
@@ -55,6 +57,7 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     if (reqs[i].dim < 1 || reqs[i].dim > 3) return fail(ALP_ERR_INVALID, "request dim");
     need[reqs[i].dim] = true;
   }
+  nvtx3::scoped_range range{"alp_serve"};  // its engine steps show as alp_engine_step
   // size the pools from the budget
   DimPool pool[4];
   auto cleanup = [&]() {

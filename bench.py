@@ -314,6 +314,20 @@ def precision_report(steps: int = 200, emit=None):
     return rows
 
 
+def levels_fp64_compute(args, value):
+    """The face kernel bounds the multi-level step as it bounds the single-level
+    one (FP64 pipe): the counted operations per cell-update against the measured
+    FP64 peak (ghost fills and jump-flux kernels not counted)."""
+    fp64 = fp64_peak()
+    if not fp64:
+        return None
+    flops = FLOPS_PER_CELL_UPDATE_3D[args.variant]
+    return {"flops_per_cell_update": flops, "achieved_tflops": value * flops / 1e12,
+            "peak_tflops": fp64, "frac": value * flops / 1e12 / fp64,
+            "peak_source": "measured FP64 FMA chains (2 flops per FMA)",
+            "count": "the single-level count of the variant; ghost and jump kernels excluded"}
+
+
 def levels_report(args):
     """Multi-level batching form: the 8 / 294 / 1232-leaf three-level
     spherical-shock hierarchy advanced with local time stepping (a macro step
@@ -357,7 +371,8 @@ def levels_report(args):
                    "l2": "state %.2f GB per pool > 126 MB L2 (no flush needed)"
                          % ((case.nleaf + info["ghosts"]) * 5 * 24 ** 3 * 8 / 1e9)},
         "roofline": {"bound": "hbm", "achieved": value * B_ALG_3D / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": value * B_ALG_3D / 1e9 / hbm, "traffic": None, "peak_source": src},
+                     "frac": value * B_ALG_3D / 1e9 / hbm, "traffic": None, "peak_source": src,
+                     "fp64_compute": levels_fp64_compute(args, value)},
         "gpu_launches": info["launches_per_macro_step"] * args.steps,
         "clocks": clocks.summary(),
     }

@@ -335,9 +335,11 @@ class LevelEngine:
 def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: int = N.FP64,
           share_3d: float = 0.9, max_cases: int = 256, steps_per_poll: int = 8,
           one_at_a_time: bool = False, keep_results: bool = False, shortest_first: bool = False,
-          step_set_cells: float = float(1 << 21)):
+          step_set_cells: float = float(1 << 21), abort_file: str | None = None):
     """Runs the C++ request loop (alp_serve) over a list of serving.Request
-    specs. Returns (results as dicts, makespan seconds, final states or None)."""
+    specs. Returns (results as dicts, makespan seconds, final states or None).
+    abort_file: once that path exists (checked after every poll) the loop stops
+    cleanly; every unfinished request then has status ALP_ABORTED."""
     n = len(requests)
     reqs = (N.Request * n)()
     outs = []
@@ -380,9 +382,10 @@ def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: i
     cfg.one_at_a_time = int(one_at_a_time)
     cfg.shortest_first = int(shortest_first)
     cfg.step_set_cells = step_set_cells
+    cfg.abort_file = abort_file.encode() if abort_file else None
     mk = C.c_double()
     rc = N.lib().alp_serve(C.byref(cfg), reqs, n, res, C.byref(mk))
-    if rc not in (N.ALP_OK, N.ALP_ERR_CAPACITY):
+    if rc not in (N.ALP_OK, N.ALP_ERR_CAPACITY, N.ALP_ABORTED):
         N.check(rc)
     results = [dict(arrival_s=x.arrival_s, admitted_s=x.admitted_s, finished_s=x.finished_s, t=x.t,
                     steps=x.steps, status=x.status) for x in res]

@@ -21,6 +21,7 @@
 #include <vector>
 
 #include <nvtx3/nvtx3.hpp>
+#include <unistd.h>
 
 #include "engine.hpp"
 
@@ -91,6 +92,7 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
                    [&](int a, int b) { return reqs[a].arrival_s < reqs[b].arrival_s; });
   std::deque<int> queue;
   int next = 0, done = 0;
+  std::vector<char> ended(n, 0);  // requests with a final result
   Clock::time_point const t0 = Clock::now();
   auto elapsed = [&]() { return std::chrono::duration<double>(Clock::now() - t0).count(); };
   int rc_all = ALP_OK;
@@ -129,6 +131,7 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
         if (total_active == 0 && it == queue.begin()) {
           // does not fit even into an empty pool: fail the request
           results[*it] = alp_result{r.arrival_s, now, now, 0.0, 0, ALP_ERR_CAPACITY};
+          ended[*it] = 1;
           ++done;
           it = queue.erase(it);
           rc_all = ALP_ERR_CAPACITY;
@@ -232,9 +235,39 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
           return rc;
         }
         p.req_of_case[c] = -1;
+        ended[ri] = 1;
         --p.active;
         ++done;
       }
+    }
+    // a clean stop on request: the abort file exists
+    if (done < n && cfg->abort_file && access(cfg->abort_file, F_OK) == 0) {
+      double const t_now = elapsed();
+      for (auto &p : pool) {
+        if (p.active == 0) continue;
+        for (int c = 0; c < cfg->max_cases; ++c) {
+          int const ri = p.req_of_case[c];
+          if (ri < 0) continue;
+          ended[ri] = 1;
+          double t = 0.0;
+          int st = 0;
+          int const grc = alp_engine_get_case(p.eng, c, reqs[ri].h_result, &t, &st);
+          if (grc != ALP_OK && grc != ALP_ERR_NUMERIC) {
+            cleanup();
+            return grc;
+          }
+          alp_result &out = results[ri];
+          out.finished_s = t_now;
+          out.t = t;
+          out.steps = st;
+          out.status = ALP_ABORTED;
+        }
+      }
+      for (int i = 0; i < n; ++i)
+        if (!ended[i]) results[i] = alp_result{reqs[i].arrival_s, -1.0, t_now, 0.0, 0, ALP_ABORTED};
+      if (makespan_s) *makespan_s = t_now;
+      cleanup();
+      return fail(ALP_ABORTED, "stopped: the abort file exists");
     }
   }
   if (makespan_s) *makespan_s = elapsed();

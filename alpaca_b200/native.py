@@ -15,6 +15,7 @@ STRICT_LIB_PATH = os.path.join(HERE, "libalpaca_b200_strict.so")
 HEADER = os.path.join(os.path.dirname(HERE), "include", "alpaca_b200.h")
 
 ALP_OK, ALP_ERR_INVALID, ALP_ERR_CUDA, ALP_ERR_CAPACITY, ALP_ERR_NOT_FOUND, ALP_ERR_NUMERIC = range(6)
+ALP_ABORTED = 6
 FLUX_SPLITTING, FINITE_VOLUME = 0, 1
 RECON_CONSERVATIVE, RECON_PRIMITIVE, RECON_CHARACTERISTIC = 0, 1, 2
 STENCIL_FIRST_ORDER, STENCIL_WENO3, STENCIL_WENO5, STENCIL_WENO5Z, STENCIL_TENO5 = 0, 1, 4, 7, 11
@@ -162,7 +163,8 @@ class Result(C.Structure):
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_size_t), ("share_3d", C.c_double), ("scheme", Scheme),
                 ("max_cases", C.c_int), ("steps_per_poll", C.c_int), ("one_at_a_time", C.c_int),
-                ("shortest_first", C.c_int), ("step_set_cells", C.c_double)]
+                ("shortest_first", C.c_int), ("step_set_cells", C.c_double),
+                ("abort_file", C.c_char_p)]
 
 
 _D = C.POINTER(C.c_double)

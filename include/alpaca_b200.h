@@ -34,7 +34,8 @@ enum {
   ALP_ERR_CUDA = 2,          /* a CUDA call failed (see alp_last_error) */
   ALP_ERR_CAPACITY = 3,      /* engine pool / case table full */
   ALP_ERR_NOT_FOUND = 4,     /* unknown case id */
-  ALP_ERR_NUMERIC = 5        /* non-finite or non-positive state detected */
+  ALP_ERR_NUMERIC = 5,       /* non-finite or non-positive state detected */
+  ALP_ABORTED = 6            /* alp_serve stopped by its abort file */
 };
 
 /* ---- scheme selection ---------------------------------------------------
@@ -443,7 +444,7 @@ typedef struct {
   double finished_s;
   double t;       /* simulated time reached */
   int steps;      /* SSP-RK3 steps taken */
-  int status;     /* ALP_OK, ALP_ERR_NUMERIC or ALP_ERR_CAPACITY */
+  int status;     /* ALP_OK, ALP_ERR_NUMERIC, ALP_ERR_CAPACITY or ALP_ABORTED */
 } alp_result;
 
 typedef struct {
@@ -457,6 +458,13 @@ typedef struct {
                                work (cells x steps left) up to step_set_cells cells, holding
                                the others; 0: every resident case steps */
   double step_set_cells;    /* cells stepped together under shortest_first (>= one case) */
+  const char *abort_file;   /* null, or a path checked after every poll, as the reference
+                               checks its ABORTFILE after each micro step
+                               (modular_algorithm_assembler.cpp:903-907): once the file
+                               exists, every request ends with status ALP_ABORTED (resident
+                               cases with their state, time and steps so far, written to
+                               h_result; the others with none) and alp_serve returns
+                               ALP_ABORTED */
 } alp_server_config;
 
 /* Serves n requests: admits arrived requests whose blocks fit (FIFO with

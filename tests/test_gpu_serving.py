@@ -179,3 +179,26 @@ def test_serving_request_too_large_is_reported(cuda):
     res, _, _ = api.serve([big, small], 8 * per_block, share_3d=1.0)
     assert res[0]["status"] == N.ALP_ERR_CAPACITY
     assert res[1]["status"] == 0 and res[1]["steps"] == 3
+
+
+def test_abort_file_stops_serving_cleanly(cuda, tmp_path):
+    """The reference stops a run when its ABORTFILE appears; alp_serve checks
+    its abort file after every poll. Present from the start, one case (one at
+    a time) has taken one poll of steps when the loop stops: that case comes
+    back with its state and steps, the others with none, all ALP_ABORTED."""
+    stop = tmp_path / "ABORTFILE"
+    stop.write_text("")
+    reqs = small_stream()
+    res, _, states = api.serve(reqs, 2 << 30, one_at_a_time=True, steps_per_poll=4,
+                               keep_results=True, abort_file=str(stop))
+    assert all(x["status"] == N.ALP_ABORTED for x in res)
+    ran = [i for i, x in enumerate(res) if x["steps"] > 0]
+    assert len(ran) == 1 and res[ran[0]]["steps"] == 4 and res[ran[0]]["t"] > 0.0
+    I = cases.interior(reqs[ran[0]].dim)
+    assert np.isfinite(states[ran[0]][I]).all() and (states[ran[0]][I][:, 0] > 0).all()
+    assert all(x["steps"] == 0 and x["t"] == 0.0 for i, x in enumerate(res) if i != ran[0])
+    # without the file the same stream runs to the end
+    stop.unlink()
+    done, _, _ = api.serve(reqs, 2 << 30, one_at_a_time=True, steps_per_poll=4,
+                           abort_file=str(stop))
+    assert all(x["status"] == 0 and x["steps"] == r.max_steps for x, r in zip(done, reqs))

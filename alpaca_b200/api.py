@@ -104,7 +104,8 @@ class Engine:
         self.variant = variant
         self.strict = strict
         self.lib = N.lib(strict)
-        sch = N.Scheme.make(variant, precision)
+        # a variant name, or an alp_scheme selection as it is
+        sch = variant if isinstance(variant, N.Scheme) else N.Scheme.make(variant, precision)
         h = C.c_void_p()
         self._check(self.lib.alp_engine_create(dim, C.byref(sch), capacity_blocks, max_cases,
                                                C.byref(h)))
@@ -236,8 +237,8 @@ class Engine:
     def autotune(self, trial_steps: int = 3):
         """Times the stepping candidates on the resident cases (state unchanged)
         and keeps the fastest; returns (chosen index, ms per step per candidate)."""
-        chosen = C.c_int()  # candidates 0..3
-        ms = (C.c_float * 4)()
+        chosen = C.c_int()
+        ms = (C.c_float * N.STEP_CANDIDATES)()
         self._check(self.lib.alp_engine_autotune(self.h, trial_steps, C.byref(chosen), ms))
         return chosen.value, [float(x) for x in ms]
 
@@ -245,8 +246,17 @@ class Engine:
         self._check(self.lib.alp_engine_set_path(self.h, candidate))
 
     @property
+    def path(self) -> int:
+        """The current stepping candidate (numbered as for autotune)."""
+        return self.lib.alp_engine_path(self.h)
+
+    @property
     def launches_per_step(self) -> int:
         return self.lib.alp_engine_launches_per_step(self.h)
+
+    def launches(self, n: int) -> int:
+        """Kernel launches of one step(n) call."""
+        return self.lib.alp_engine_launches(self.h, n)
 
     @property
     def stream_handle(self) -> int:

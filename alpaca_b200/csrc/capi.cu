@@ -354,7 +354,7 @@ int engine_case_states(alp_engine *e, std::vector<CaseState> &out) {
   ALP_CUDA(cudaMemcpyAsync(out.data(), e->cases, sizeof(CaseState) * e->max_cases,
                            cudaMemcpyDeviceToHost, e->stream));
   ALP_CUDA(cudaStreamSynchronize(e->stream));
-  return ALP_OK;
+  return e->tile_check();
 }
 
 int engine_set_hold(alp_engine *e, int case_id, int hold) {
@@ -375,9 +375,11 @@ size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
   size_t const blk = ne * cells_of(dim) * sizeof(double);
   size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double) +
                       ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
+  // the fused tile path's flags, orders and case sizes (3D)
+  size_t const tiles = dim == 3 ? sizeof(int) * (2 + 4 * (size_t)capacity_blocks + 3 * (size_t)max_cases) : 0;
   return (size_t)capacity_blocks *
              (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
-         (size_t)max_cases * sizeof(CaseState);
+         (size_t)max_cases * sizeof(CaseState) + tiles;
 }
 
 int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
@@ -422,6 +424,14 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
   grab((void **)&e->cases, sizeof(CaseState) * max_cases);
   grab((void **)&e->glf, sizeof(unsigned long long) * 4 * max_cases);
+  // fused tile stages: 3D, the compiled default schemes (WENO5, HLLC/Einfeldt, Roe)
+  bool const tiles = dim == 3 && e->opt.is_default();
+  if (tiles) {
+    grab((void **)&e->tsync, sizeof(int) * (2 + (size_t)capacity_blocks + 2 * (size_t)max_cases));
+    grab((void **)&e->torder, sizeof(int) * 3 * (size_t)capacity_blocks);
+    grab((void **)&e->tcase_nb, sizeof(int) * (size_t)max_cases);
+    if (err == cudaSuccess) err = cudaMemset(e->tsync, 0, sizeof(int) * 2);
+  }
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream, cudaStreamNonBlocking);
   if (err == cudaSuccess) err = cudaStreamCreateWithFlags(&e->stream2, cudaStreamNonBlocking);
   for (cudaEvent_t &ev : e->ev_batch)
@@ -434,6 +444,40 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
     e->release();
     delete e;
     return cuda_fail(err, "alp_engine_create");
+  }
+  if (tiles) {
+    // TMA descriptors of the pools and the launch shapes; engines whose
+    // descriptors or kernels are unavailable keep the face-flux path
+    double *const pools[3] = {e->U, e->UB, e->UC};
+    std::string why;
+    bool ok = alp::tile_encode(e->targs, pools, capacity_blocks, why);
+    int sms = 0, dev = 0;
+    if (ok && (cudaGetDevice(&dev) != cudaSuccess ||
+               cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess))
+      ok = false;
+    for (int v = 0; ok && v < alp::kTileVariants; ++v) {
+      if (alp::tile_info(sid, v, prec, &e->tinfo[v]) != cudaSuccess || e->tinfo[v].ctas_per_sm < 1)
+        ok = false;
+      else
+        e->tgrid[v] = e->tinfo[v].ctas_per_sm * sms;
+    }
+    cudaGetLastError();  // a refused attribute or query leaves the face-flux path
+    if (ok) {
+      alp::TileArgs &a = e->targs;
+      a.order = e->torder;
+      a.nstages = e->rk2 ? 2 : 3;
+      a.stage0 = e->rk2 ? 3 : 0;
+      a.meta = e->meta;
+      a.nbr26 = e->nbr26;
+      a.cases = e->cases;
+      a.ctrl = e->tsync;
+      a.done = e->tsync + 2;
+      a.dtflag = e->tsync + 2 + capacity_blocks;
+      a.cnt = e->tsync + 2 + capacity_blocks + max_cases;
+      a.case_nb = e->tcase_nb;
+      e->tile_ok = true;
+      e->path = 3;
+    }
   }
   e->h_meta.assign(capacity_blocks, BlockMeta{});
   e->h_nbr26.assign((size_t)capacity_blocks * 26, -1);
@@ -519,6 +563,7 @@ int alp_engine_step(alp_engine *e, int n) {
   if (n <= 0 || e->nwork == 0) return ALP_OK;
   // profiler ranges (no cost unless a tool is attached): one per call, one per capture
   nvtx3::scoped_range range{"alp_engine_step"};
+  if (e->path == 3) return e->run_tiles(n);
   if (!e->use_graph) {
     for (int i = 0; i < n; ++i)
       if (int rc = e->record_step()) return rc;
@@ -567,6 +612,7 @@ int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t,
   }
   ALP_CUDA(cudaMemcpyAsync(&cs, e->cases + case_id, sizeof(cs), cudaMemcpyDeviceToHost, e->stream));
   ALP_CUDA(cudaStreamSynchronize(e->stream));
+  if (int rc = e->tile_check()) return rc;
   if (t) *t = cs.t;
   if (steps) *steps = cs.steps;
   if (cs.status) return fail(ALP_ERR_NUMERIC, "non-finite or non-positive state; case stopped");
@@ -625,6 +671,7 @@ int alp_engine_all_done(alp_engine *e, int *done) {
   ALP_CUDA(cudaMemcpyAsync(cs.data(), e->cases, sizeof(CaseState) * e->max_cases,
                            cudaMemcpyDeviceToHost, e->stream));
   ALP_CUDA(cudaStreamSynchronize(e->stream));
+  if (int rc = e->tile_check()) return rc;
   int d = 1;
   for (int c = 0; c < e->max_cases; ++c) {
     if (!e->case_rec[c].live) continue;
@@ -639,43 +686,62 @@ int alp_engine_all_done(alp_engine *e, int *done) {
 
 alp_stream_t alp_engine_stream(alp_engine *e) { return e ? (alp_stream_t)e->stream : nullptr; }
 
+namespace {
+// Stepping candidates of alp_engine_autotune / alp_engine_set_path: path,
+// face-kernel threads (paths 0-2) or tile variant (path 3).
+struct Cand {
+  int path, param;
+};
+Cand const kCands[ALP_STEP_CANDIDATES] = {{1, 128}, {1, 64}, {0, 128}, {2, 128}, {3, 0}, {3, 1}};
+
+// Why candidate i cannot step engine e (null: it can).
+char const *cand_refusal(alp_engine const *e, int i) {
+  if (kCands[i].path == 0) {
+#ifdef ALP_STRICT
+    return "the strict build steps the face-flux path";
+#endif
+    if (!e->opt.is_default() || e->rk2)
+      return "pencil sweeps are compiled for WENO5 + HLLC/Einfeldt and Roe with RK3 only";
+  }
+  if (kCands[i].path == 3 && !e->tile_ok)
+    return "fused tile stages are compiled for 3D blocks with WENO5 + HLLC/Einfeldt and Roe";
+  return nullptr;
+}
+
+void select_cand(alp_engine *e, int i) {
+  e->path = kCands[i].path;
+  if (e->path == 3) e->tile_variant = kCands[i].param;
+  else e->face_threads = kCands[i].param;
+  e->graph_dirty = true;
+}
+}  // namespace
+
 int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");
   if (trial_steps <= 0) return fail(ALP_ERR_INVALID, "trial_steps must be positive");
-  // candidates: face fluxes with 128- or 64-thread blocks, pencil sweeps,
-  // face fluxes and stage updates overlapped in batches
-  struct Cand {
-    int path, threads;
-  };
-  Cand const cands[4] = {{1, 128}, {1, 64}, {0, 128}, {2, 128}};
-  int const ncand = 4;
-  auto allowed = [&](int i) {
-    if (i != 2) return true;
-    if (!e->opt.is_default() || e->rk2) return false;  // pencils: default schemes, RK3
-#ifdef ALP_STRICT
-    return false;  // the pencil path changes the flux summation order
-#else
-    return true;
-#endif
-  };
-  int const saved_path = e->path, saved_threads = e->face_threads;
+  int const saved_path = e->path, saved_threads = e->face_threads, saved_var = e->tile_variant;
   float best = 0.f;
   int best_i = 0;
   cudaEvent_t t0, t1;
   ALP_CUDA(cudaEventCreate(&t0));
   ALP_CUDA(cudaEventCreate(&t1));
-  for (int i = 0; i < ncand; ++i) {
+  for (int i = 0; i < ALP_STEP_CANDIDATES; ++i) {
     float ms = -1.f;
-    if (allowed(i) && e->nwork > 0) {
-      e->path = cands[i].path;
-      e->face_threads = cands[i].threads;
-      if (int rc = e->record_step(true)) return rc;  // warm-up
+    if (!cand_refusal(e, i) && e->nwork > 0) {
+      select_cand(e, i);
+      auto trial = [&](int n) {
+        if (e->path == 3) return e->record_tiles(n, true);
+        for (int k = 0; k < n; ++k)
+          if (int rc = e->record_step(true)) return rc;
+        return (int)ALP_OK;
+      };
+      if (int rc = trial(1)) return rc;  // warm-up
       ALP_CUDA(cudaEventRecord(t0, e->stream));
-      for (int k = 0; k < trial_steps; ++k)
-        if (int rc = e->record_step(true)) return rc;
+      if (int rc = trial(trial_steps)) return rc;
       ALP_CUDA(cudaEventRecord(t1, e->stream));
       ALP_CUDA(cudaEventSynchronize(t1));
       ALP_CUDA(cudaEventElapsedTime(&ms, t0, t1));
+      if (int rc = e->tile_check()) return rc;
       ms /= trial_steps;
       if (best == 0.f || ms < best) {
         best = ms;
@@ -687,11 +753,11 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
   cudaEventDestroy(t0);
   cudaEventDestroy(t1);
   if (e->nwork > 0) {
-    e->path = cands[best_i].path;
-    e->face_threads = cands[best_i].threads;
+    select_cand(e, best_i);
   } else {
     e->path = saved_path;
     e->face_threads = saved_threads;
+    e->tile_variant = saved_var;
   }
   e->graph_dirty = true;
   if (chosen) *chosen = e->nwork > 0 ? best_i : -1;
@@ -700,19 +766,20 @@ int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_p
 
 int alp_engine_set_path(alp_engine *e, int candidate) {
   if (!e) return fail(ALP_ERR_INVALID, "null engine");
-  int const paths[4] = {1, 1, 0, 2}, threads[4] = {128, 64, 128, 128};
-  if (candidate < 0 || candidate > 3)
-    return fail(ALP_ERR_INVALID, "candidate must be 0, 1, 2 or 3");
-#ifdef ALP_STRICT
-  if (candidate == 2) return fail(ALP_ERR_INVALID, "the strict build steps the face-flux path");
-#endif
-  if (candidate == 2 && (!e->opt.is_default() || e->rk2))
-    return fail(ALP_ERR_INVALID,
-                "pencil sweeps are compiled for WENO5 + HLLC/Einfeldt and Roe with RK3 only");
-  e->path = paths[candidate];
-  e->face_threads = threads[candidate];
-  e->graph_dirty = true;
+  if (candidate < 0 || candidate >= ALP_STEP_CANDIDATES)
+    return fail(ALP_ERR_INVALID, "candidate must be 0 .. ALP_STEP_CANDIDATES - 1");
+  if (char const *why = cand_refusal(e, candidate)) return fail(ALP_ERR_INVALID, why);
+  select_cand(e, candidate);
   return ALP_OK;
+}
+
+int alp_engine_path(alp_engine *e) {
+  if (!e) return -1;
+  for (int i = 0; i < ALP_STEP_CANDIDATES; ++i)
+    if (kCands[i].path == e->path &&
+        (e->path == 3 ? kCands[i].param == e->tile_variant : kCands[i].param == e->face_threads))
+      return i;
+  return -1;
 }
 
 int alp_engine_set_graph(alp_engine *e, int enabled) {
@@ -724,9 +791,16 @@ int alp_engine_set_graph(alp_engine *e, int enabled) {
 int alp_engine_launches_per_step(alp_engine *e) {
   if (!e) return 0;
   // signal speed, dt, 3 stages x (one pencil sweep per direction, or face
-  // fluxes + stage update, per batch on the overlapped path), commit
+  // fluxes + stage update, per batch on the overlapped path), commit; the tile
+  // path launches signal speed, dt and one persistent kernel per call
+  if (e->path == 3) return 3;
   int const batches = e->path == 2 ? std::min(alp_engine::kMaxBatches, std::max(1, e->nwork / 64)) : 1;
   return 2 + (e->rk2 ? 2 : 3) * (e->path == 0 ? e->dim : 2 * batches) + 1;
+}
+
+int alp_engine_launches(alp_engine *e, int n) {
+  if (!e || n <= 0 || e->nwork == 0) return 0;
+  return e->path == 3 ? 3 : n * alp_engine_launches_per_step(e);
 }
 
 }  // extern "C"

@@ -10,6 +10,7 @@
 
 #include "../../include/alpaca_b200.h"
 #include "kernels.cuh"
+#include "tile_api.cuh"
 
 namespace alp {
 int fail(int code, std::string const &msg);
@@ -48,7 +49,8 @@ struct alp_engine {
   double *F = nullptr;  // face fluxes [slot][dim][NE][faces] (face-flux path)
   double *R = nullptr;  // per-cell flux differences [slot][NE][interior] (pencil path)
   int path = 1;         // 0: pencil sweeps, 1: face fluxes + stage update, 2: the same in
-                        // overlapped batches
+                        // overlapped batches, 3: fused tile stages (one persistent launch
+                        // for all steps of a call; 3D, default schemes)
   cudaStream_t stream2 = nullptr;  // stage updates of the overlapped path
   static constexpr int kMaxBatches = 16;
   cudaEvent_t ev_batch[kMaxBatches] = {};
@@ -64,6 +66,21 @@ struct alp_engine {
   bool use_graph = true;
   bool graph_dirty = true;
 
+  // fused tile stages (path 3)
+  bool tile_ok = false;       // 3D, default schemes, descriptors encoded
+  int tile_variant = 0;       // index into alp::kTileWarps
+  alp::TileArgs targs{};      // TMA descriptors and device pointers (nsteps set per launch)
+  alp::TileKernelInfo tinfo[alp::kTileVariants] = {};
+  int tgrid[alp::kTileVariants] = {};
+  int *tsync = nullptr;       // [2 + capacity + 2 max_cases]: next item, error, block flags,
+                              // dt flags, last-stage counts
+  int *torder = nullptr;      // [3][capacity] block slots per stage, in readiness order
+  int *tcase_nb = nullptr;    // [max_cases] blocks of each case in the work list
+  cudaGraph_t tile_graph_src = nullptr;  // the graph `graph` was instantiated from (kept:
+                                         // its node handle addresses the launch to update)
+  cudaGraphNode_t tile_node = nullptr;    // the persistent launch in it
+  int tile_graph_n = 0;                   // its step count
+
   // host mirrors
   std::vector<BlockMeta> h_meta;
   std::vector<int> h_nbr26;
@@ -76,6 +93,7 @@ struct alp_engine {
   };
   std::vector<CaseRec> case_rec;
   std::vector<int> h_work;
+  std::vector<int> h_torder, h_case_nb;  // staging of the tile path's orders and case sizes
   std::vector<CaseState> h_case_state;  // staging for case records sent to the device
   int nwork = 0;
 
@@ -115,6 +133,124 @@ struct alp_engine {
     }
     if (!trial) ALP_CUDA(launch_step_commit(cases, max_cases, stream));
     return ALP_OK;
+  }
+
+  // Path 3: the dt of the first step (signal speed, dt_finalize, which marks
+  // it ready), then one persistent launch for n steps (tile_step.cuh); the
+  // flags and counters of the launch start at zero, the error word is kept.
+  int record_tiles(int n, bool trial) {
+    if (nwork == 0 || n <= 0) return ALP_OK;
+    int *dtflag = tsync + 2 + capacity;
+    ALP_CUDA(cudaMemsetAsync(tsync, 0, sizeof(int), stream));
+    ALP_CUDA(cudaMemsetAsync(tsync + 2, 0, sizeof(int) * ((size_t)capacity + 2 * max_cases), stream));
+    Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
+    ALP_CUDA(launch_signal_speed(L, cases, nullptr));
+    ALP_CUDA(launch_dt_finalize(cases, max_cases, stream, dtflag));
+    alp::TileArgs a = targs;
+    a.nwork = nwork;
+    a.nsteps = n;
+    a.trial = trial ? 1 : 0;
+    // one CTA per SM and kernel variant; CTAs that find no item left return
+    ALP_CUDA(alp::tile_launch(a, tinfo[tile_variant], tgrid[tile_variant], stream));
+    return ALP_OK;
+  }
+
+  // Path 3 through a CUDA graph: captured once per work list; a call with a
+  // different step count updates the persistent launch's parameters in place.
+  int run_tiles(int n) {
+    if (!use_graph) return record_tiles(n, false);
+    if (graph_dirty || !graph) {
+      if (graph) {
+        cudaGraphExecDestroy(graph);
+        graph = nullptr;
+      }
+      if (tile_graph_src) {
+        cudaGraphDestroy(tile_graph_src);
+        tile_graph_src = nullptr;
+      }
+      cudaGraph_t g;
+      ALP_CUDA(cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal));
+      int const rc = record_tiles(n, false);
+      cudaError_t const ce = cudaStreamEndCapture(stream, &g);
+      if (rc) {
+        if (ce == cudaSuccess) cudaGraphDestroy(g);
+        return rc;
+      }
+      if (ce != cudaSuccess) return alp::cuda_fail(ce, "cudaStreamEndCapture");
+      tile_node = nullptr;
+      size_t nn = 0;
+      cudaGraphGetNodes(g, nullptr, &nn);
+      std::vector<cudaGraphNode_t> nodes(nn);
+      if (nn) cudaGraphGetNodes(g, nodes.data(), &nn);
+      for (cudaGraphNode_t nd : nodes) {
+        cudaGraphNodeType ty;
+        cudaKernelNodeParams kp;
+        if (cudaGraphNodeGetType(nd, &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel &&
+            cudaGraphKernelNodeGetParams(nd, &kp) == cudaSuccess &&
+            kp.func == tinfo[tile_variant].fn)
+          tile_node = nd;
+      }
+      cudaError_t const ie = cudaGraphInstantiate(&graph, g, 0);
+      if (ie != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return alp::cuda_fail(ie, "cudaGraphInstantiate");
+      }
+      tile_graph_src = g;
+      if (!tile_node) return fail(ALP_ERR_CUDA, "tile launch not found in the step graph");
+      graph_dirty = false;
+      tile_graph_n = n;
+    } else if (n != tile_graph_n) {
+      alp::TileArgs a = targs;
+      a.nwork = nwork;
+      a.nsteps = n;
+      a.trial = 0;
+      void *args[] = {&a};
+      cudaKernelNodeParams kp{};
+      kp.func = const_cast<void *>(tinfo[tile_variant].fn);
+      kp.gridDim = dim3(tgrid[tile_variant]);
+      kp.blockDim = dim3(tinfo[tile_variant].threads);
+      kp.sharedMemBytes = (unsigned)tinfo[tile_variant].smem;
+      kp.kernelParams = args;
+      kp.extra = nullptr;
+      ALP_CUDA(cudaGraphExecKernelNodeSetParams(graph, tile_node, &kp));
+      tile_graph_n = n;
+    }
+    ALP_CUDA(cudaGraphLaunch(graph, stream));
+    return ALP_OK;
+  }
+
+  // Per-stage orders of the work list for the tile path: a block is taken as
+  // soon after the blocks its stage reads (itself and its face neighbours, in
+  // the previous stage's order) as the order allows, so that a CTA seldom waits.
+  // The cycle of stage orders is relaxed a few times so that the first stage of
+  // the next step also follows the last stage of this one.
+  void tile_orders(int nst, std::vector<int> &ord) const {
+    static int const faces6[6] = {4, 21, 10, 15, 12, 13};
+    std::vector<int> pos((size_t)capacity, 0);
+    std::vector<std::vector<int>> o(nst, h_work);
+    auto relax = [&](std::vector<int> const &prev, std::vector<int> &next) {
+      for (size_t i = 0; i < prev.size(); ++i) pos[prev[i]] = (int)i;
+      std::vector<std::pair<int, int>> key;
+      key.reserve(prev.size());
+      for (int b : h_work) {
+        int k = pos[b];
+        for (int f : faces6) {
+          int const n = h_nbr26[(size_t)b * 26 + f];
+          if (n >= 0) k = std::max(k, pos[n]);
+        }
+        key.push_back({k, pos[b]});
+      }
+      std::vector<int> idx(h_work.size());
+      for (size_t i = 0; i < idx.size(); ++i) idx[i] = (int)i;
+      std::stable_sort(idx.begin(), idx.end(),
+                       [&](int x, int y) { return key[x] < key[y]; });
+      next.resize(h_work.size());
+      for (size_t i = 0; i < idx.size(); ++i) next[i] = h_work[idx[i]];
+    };
+    for (int it = 0; it < 3; ++it)
+      for (int s = 0; s < nst; ++s) relax(o[(s + nst - 1) % nst], o[s]);
+    ord.clear();
+    for (int s = 0; s < nst; ++s) ord.insert(ord.end(), o[s].begin(), o[s].end());
   }
 
   // One stage in batches of work items: the faces of batch k+1 run on `stream`
@@ -158,8 +294,33 @@ struct alp_engine {
     if (nwork)
       ALP_CUDA(cudaMemcpyAsync(work, h_work.data(), sizeof(int) * nwork, cudaMemcpyHostToDevice,
                                stream));
+    if (tile_ok && nwork) {
+      tile_orders(rk2 ? 2 : 3, h_torder);
+      h_case_nb.assign(max_cases, 0);
+      for (int c = 0; c < max_cases; ++c)
+        if (case_rec[c].live) h_case_nb[c] = case_rec[c].nb;
+      ALP_CUDA(cudaMemcpyAsync(torder, h_torder.data(), sizeof(int) * h_torder.size(),
+                               cudaMemcpyHostToDevice, stream));
+      ALP_CUDA(cudaMemcpyAsync(tcase_nb, h_case_nb.data(), sizeof(int) * max_cases,
+                               cudaMemcpyHostToDevice, stream));
+      // the staging vectors must outlive the copies
+      ALP_CUDA(cudaStreamSynchronize(stream));
+    }
     graph_dirty = true;
     return ALP_OK;
+  }
+
+  // Reads and clears the tile path's error word: a bounded device wait that
+  // ran out (the results of that launch are not trusted).
+  int tile_check() {
+    if (!tsync) return ALP_OK;
+    int e = 0;
+    ALP_CUDA(cudaMemcpyAsync(&e, tsync + 1, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ALP_CUDA(cudaStreamSynchronize(stream));
+    if (!e) return ALP_OK;
+    ALP_CUDA(cudaMemsetAsync(tsync + 1, 0, sizeof(int), stream));
+    return fail(ALP_ERR_CUDA, "tile path: a bounded device wait ran out (code " +
+                                  std::to_string(e) + "); the step results are not valid");
   }
 
   int alloc_range(int n, int *first) {
@@ -193,6 +354,7 @@ struct alp_engine {
 
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
+    if (tile_graph_src) cudaGraphDestroy(tile_graph_src);
     cudaFree(U);
     cudaFree(UB);
     cudaFree(UC);
@@ -203,6 +365,9 @@ struct alp_engine {
     cudaFree(work);
     cudaFree(cases);
     cudaFree(glf);
+    cudaFree(tsync);
+    cudaFree(torder);
+    cudaFree(tcase_nb);
     for (cudaEvent_t &ev : ev_batch)
       if (ev) cudaEventDestroy(ev);
     if (ev_join) cudaEventDestroy(ev_join);

@@ -10,12 +10,8 @@
 #include <mutex>
 
 #include "kernels.cuh"
-
-// The FP32-flux branches return early, which leaves the shared FP64 tail
-// unreachable in those instantiations.
-#pragma nv_diag_suppress 128
-#include "numerics.cuh"
-#include "schemes_ext.cuh"
+#include "face.cuh"
+#include "step_common.cuh"
 
 namespace alp {
 
@@ -23,27 +19,6 @@ namespace {
 
 __device__ __forceinline__ int slot_of(int const *work, int item) {
   return work ? work[item] : item;
-}
-
-// SSP-RK3 stage coefficients (runge_kutta_3_TVD.h:41-59): Uout = a0 U + a1 U0 +
-// c dt RHS (time_integrator.h:98-113, 434-457)
-// Stage coefficients: indices 0-2 the SSP-RK3 stages (runge_kutta_3_TVD.h:
-// 41-59), 3-4 the TVD-RK2 stages (runge_kutta_2_TVD.h:37-56); per stage the
-// multiplier of dt and the buffer multipliers of the stage input and of the
-// step's initial state (unused in a first stage).
-__constant__ double kRkC[5] = {1.0, 0.25, 2.0 / 3.0, 1.0, 0.5};
-__constant__ double kRkA0[5] = {0.0, 0.25, 2.0 / 3.0, 0.0, 0.5};
-__constant__ double kRkA1[5] = {0.0, 0.75, 1.0 / 3.0, 0.0, 0.5};
-__host__ __device__ constexpr bool rk_first_stage(int stage) { return stage == 0 || stage == 3; }
-
-// Structural nonzeros of the left eigenvector matrix row n, column l
-// (eigendecomposition.h:316-359).
-template <int DIM, int DIR>
-__host__ __device__ constexpr bool left_nonzero(int n, int l) {
-  // the rows of the two acoustic waves and of the principal-momentum wave are full
-  if (n == 0 || n == DIM + 1 || n == DIM) return true;
-  // minor-momentum waves: mass and their own momentum only
-  return l == MASS || l == MOMX + (n == 1 ? Minor<DIR>::m1 : Minor<DIR>::m2);
 }
 
 // ---------------------------------------------------------------------------
@@ -184,264 +159,6 @@ __device__ __forceinline__ void stencil_load(double const *__restrict__ U, doubl
     return;
   }
   load_cell<DIM, DIR>(stencil_cell<DIM, DIR, GATHER>(U, blk, c, cell0, nlo, nhi), dst);
-}
-
-// Flux of one face from its 6-cell stencil (the reference's per-face work:
-// FiniteVolumeScheme::ComputeFluxes<DIR> with the selected reconstruction and
-// HLLC, or FluxSplittingScheme::ComputeFluxes<DIR>). Writes the flux in double
-// to fd and returns false for a face the reference skips (invalid
-// reconstructed state, finite_volume_scheme.cpp:218-225) or whose Roe average
-// has a non-positive density (eigendecomposition.h:244).
-// P selects reconstruction stencil, Riemann solver and splitting eigenvalues
-// (DefaultPolicy: WENO5, HLLC/Einfeldt, Roe; ExtPolicy: run-time choice, FP64).
-template <int DIM, int DIR, int SCHEME, typename T, typename P = DefaultPolicy, int W = 6>
-__device__ __forceinline__ bool face_compute(Eos const &eos, double B,
-                                             double const (&cons)[W][DIM + 2],
-                                             double (&fd)[DIM + 2], P const &pol = P()) {
-  constexpr int NE = DIM + 2;
-  T flux[NE];
-  bool valid = true;
-  constexpr int mP = MOMX + DIR;
-  constexpr int C = W / 2 - 1;  // the face's left cell i in the stencil
-
-  if constexpr (SCHEME == FV_CHAR || SCHEME == FS_ROE) {
-    auto const pt = cell_prims<DIM, DIR>(eos, cons[C]);
-    auto const pn = cell_prims<DIM, DIR>(eos, cons[C + 1]);
-    if (!(pt.rho > 0.0) || !(pn.rho > 0.0)) valid = false;
-    Roe<T> const r = roe_average<DIM, DIR, T>(eos, pt, pn);
-    T ch[2][NE];
-    if constexpr (SCHEME == FV_CHAR && sizeof(T) == 4) {
-      // FP32 form: characteristic projection and WENO5 of the increments
-      // U_m - U_i against the face's left cell i (WENO5 is translation
-      // invariant and R L = I), the left cell's state added back in double.
-#pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T L[NE];
-        left_row<DIM, DIR, T>(n, r, L);
-        T uc[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) {
-          T s = T(0);
-#pragma unroll
-          for (int q = 0; q < NE; ++q) {
-            int const l = sum_seq<DIM, DIR>(q);
-            if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            s = fmaf(L[l], m == C ? 0.0f : float(cons[m][l] - cons[C][l]), s);
-          }
-          uc[m] = s;
-        }
-        weno5_pair(uc, ch[0][n], ch[1][n]);
-      }
-      T dm[NE], dp[NE];
-      to_physical<DIM, DIR, T>(r, ch[0], dm);
-      to_physical<DIM, DIR, T>(r, ch[1], dp);
-      double cm[NE], cp[NE];
-#pragma unroll
-      for (int f = 0; f < NE; ++f) {
-        cm[f] = cons[C][f] + double(dm[f]);
-        cp[f] = cons[C][f] + double(dp[f]);
-      }
-      if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
-      double const one_l = inv(cm[MASS]), one_r = inv(cp[MASS]);
-      double const pm = eos_pressure<DIM>(eos, cm[MASS], cm[MOMX], DIM > 1 ? cm[MOMX + (DIM > 1)] : 0.0,
-                                          DIM > 2 ? cm[MOMX + 2 * (DIM > 2)] : 0.0, cm[ENERGY], one_l);
-      double const pp = eos_pressure<DIM>(eos, cp[MASS], cp[MOMX], DIM > 1 ? cp[MOMX + (DIM > 1)] : 0.0,
-                                          DIM > 2 ? cp[MOMX + 2 * (DIM > 2)] : 0.0, cp[ENERGY], one_r);
-      if (!(pm > -B) || !(pp > -B)) valid = false;
-      hllc_mixed<DIM, DIR>(eos, cm, cp, pm, pp, cm[mP] * one_l, cp[mP] * one_r, one_l, one_r, fd);
-      return valid;
-    } else if constexpr (SCHEME == FV_CHAR) {
-#pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T L[NE];
-        left_row<DIM, DIR, T>(n, r, L);
-        T uc[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) {
-          T s = T(0);
-          bool first = true;
-#pragma unroll
-          for (int q = 0; q < NE; ++q) {
-            int const l = sum_seq<DIM, DIR>(q);
-            if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            T const prod = L[l] * T(cons[m][l]);
-            s = first ? prod : s + prod;
-            first = false;
-          }
-          uc[m] = s;
-        }
-        pol.pair(uc, ch[0][n], ch[1][n]);
-      }
-      T cm[NE], cp[NE];
-      to_physical<DIM, DIR, T>(r, ch[0], cm);
-      to_physical<DIM, DIR, T>(r, ch[1], cp);
-      if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
-      // prime states of the reconstructed states (prime_state_handler.h:277-371),
-      // pressure recovered in double
-      T const one_l = inv(cm[MASS]), one_r = inv(cp[MASS]);
-      double const pm = eos_pressure<DIM>(eos, double(cm[MASS]), double(cm[MOMX]),
-                                          DIM > 1 ? double(cm[MOMX + (DIM > 1)]) : 0.0,
-                                          DIM > 2 ? double(cm[MOMX + 2 * (DIM > 2)]) : 0.0,
-                                          double(cm[ENERGY]), double(one_l));
-      double const pp = eos_pressure<DIM>(eos, double(cp[MASS]), double(cp[MOMX]),
-                                          DIM > 1 ? double(cp[MOMX + (DIM > 1)]) : 0.0,
-                                          DIM > 2 ? double(cp[MOMX + 2 * (DIM > 2)]) : 0.0,
-                                          double(cp[ENERGY]), double(one_r));
-      if (!(pm > -B) || !(pp > -B)) valid = false;
-      T const vl = cm[mP] * one_l;
-      T const vr = cp[mP] * one_r;
-      pol.template riemann<DIM, DIR, T>(eos, cm, cp, T(pm), T(pp), vl, vr, one_l, one_r, flux);
-    } else {
-      // Roe flux-vector splitting (flux_splitting_scheme.cpp:42-76, 185-315)
-      double advd[W][NE];
-#pragma unroll
-      for (int m = 0; m < W; ++m) {
-        double const one_rho = inv(cons[m][MASS]);
-        double const p = eos_pressure<DIM>(
-            eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
-            DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY], one_rho);
-        double const vel = cons[m][mP] * one_rho;
-        double const rho = cons[m][MASS];
-        // the fast build uses rho u = m for the mass and momentum fluxes
-        advd[m][MASS] = ALP_FAST ? cons[m][mP] : rho * vel;
-        advd[m][ENERGY] = (cons[m][ENERGY] + p) * vel;
-#pragma unroll
-        for (int d = 0; d < DIM; ++d) {
-          double const vd = cons[m][MOMX + d] * one_rho;
-          double v = ALP_FAST ? cons[m][mP] * vd : rho * (vel * vd);
-          if (d == DIR) v += p;
-          advd[m][MOMX + d] = v;
-        }
-      }
-      T ev_nl0, ev_lin, ev_nl1;
-      pol.template fs_eigenvalues<DIM, DIR, T>(eos, r, pt, pn, ev_nl0, ev_lin, ev_nl1);
-      // FP32 form: increments against the face's left cell; the characteristic
-      // flux of that cell, L f_i, is restored by R as f_i in double
-      constexpr bool DELTA = sizeof(T) == 4;
-#pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T L[NE];
-        left_row<DIM, DIR, T>(n, r, L);
-        T const alpha = n == 0 ? ev_nl0 : (n == NE - 1 ? ev_nl1 : ev_lin);
-        T pos[W], neg[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) {
-          T sp = T(0), sn = T(0);
-          bool first = true;
-#pragma unroll
-          for (int q = 0; q < NE; ++q) {
-            int const l = sum_seq<DIM, DIR>(q);
-            if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            T const uct = (DELTA ? T(cons[m][l] - cons[C][l]) : T(cons[m][l])) * L[l];
-            T const act = (DELTA ? T(advd[m][l] - advd[C][l]) : T(advd[m][l])) * L[l];
-            if constexpr (ALP_FAST) {
-              // project state (into sp) and flux (into sn), split afterwards:
-              // L (f +/- alpha u) = L f +/- alpha L u
-              sp = first ? uct : sp + uct;
-              sn = first ? act : sn + act;
-            } else {
-              T const tp = act + alpha * uct;
-              T const tn = act - alpha * uct;
-              sp = first ? tp : sp + tp;
-              sn = first ? tn : sn + tn;
-            }
-            first = false;
-          }
-          if constexpr (ALP_FAST) {
-            pos[m] = sn + alpha * sp;
-            neg[m] = sn - alpha * sp;
-          } else {
-            pos[m] = sp;
-            neg[m] = sn;
-          }
-        }
-        T wl, wr;
-        pol.two(pos, neg, wl, wr);
-        ch[0][n] = T(0.5) * (wl + wr);
-      }
-      to_physical<DIM, DIR, T>(r, ch[0], flux);
-      if constexpr (DELTA) {
-#pragma unroll
-        for (int f = 0; f < NE; ++f) fd[f] = advd[C][f] + double(flux[f]);
-        return valid;
-      }
-    }
-  } else {
-    // FV primitive reconstruction (primitive_state_reconstruction.h:56-107)
-    double prim[W][NE];
-#pragma unroll
-    for (int m = 0; m < W; ++m) {
-      prim[m][RHO] = cons[m][MASS];
-      double const one_rho = inv(cons[m][MASS]);
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) prim[m][VELX + d] = cons[m][MOMX + d] * one_rho;
-      prim[m][PRES] = eos_pressure<DIM>(
-          eos, cons[m][MASS], cons[m][MOMX], DIM > 1 ? cons[m][MOMX + (DIM > 1)] : 0.0,
-          DIM > 2 ? cons[m][MOMX + 2 * (DIM > 2)] : 0.0, cons[m][ENERGY], one_rho);
-    }
-    if constexpr (sizeof(T) == 4) {
-      // FP32 form: WENO5 of the increments against the left cell's primes
-      double pmd[NE], ppd[NE];
-#pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T arr[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) arr[m] = T(prim[m][n] - prim[C][n]);
-        T wl, wr;
-        weno5_pair(arr, wl, wr);
-        pmd[n] = prim[C][n] + double(wl);
-        ppd[n] = prim[C][n] + double(wr);
-      }
-      double cm[NE], cp[NE];
-      cm[MASS] = pmd[RHO];
-      cp[MASS] = ppd[RHO];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        cm[MOMX + d] = pmd[VELX + d] * pmd[RHO];
-        cp[MOMX + d] = ppd[VELX + d] * ppd[RHO];
-      }
-      cm[ENERGY] = eos_energy<DIM, double>(eos, pmd[RHO], pmd[VELX], DIM > 1 ? pmd[VELX + (DIM > 1)] : 0.0,
-                                           DIM > 2 ? pmd[VELX + 2 * (DIM > 2)] : 0.0, pmd[PRES]);
-      cp[ENERGY] = eos_energy<DIM, double>(eos, ppd[RHO], ppd[VELX], DIM > 1 ? ppd[VELX + (DIM > 1)] : 0.0,
-                                           DIM > 2 ? ppd[VELX + 2 * (DIM > 2)] : 0.0, ppd[PRES]);
-      if (!(cm[MASS] > DBL_EPSILON) || !(cp[MASS] > DBL_EPSILON)) valid = false;
-      if (!(pmd[PRES] > -B) || !(ppd[PRES] > -B)) valid = false;
-      hllc_mixed<DIM, DIR>(eos, cm, cp, pmd[PRES], ppd[PRES], pmd[VELX + DIR], ppd[VELX + DIR],
-                           inv(cm[MASS]), inv(cp[MASS]), fd);
-      return valid;
-    } else {
-      T pm[NE], pp[NE];
-#pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T arr[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) arr[m] = T(prim[m][n]);
-        pol.pair(arr, pm[n], pp[n]);
-      }
-      // PrimeStatesToConservatives (prime_state_handler.h:195-275)
-      T cm[NE], cp[NE];
-      cm[MASS] = pm[RHO];
-      cp[MASS] = pp[RHO];
-#pragma unroll
-      for (int d = 0; d < DIM; ++d) {
-        cm[MOMX + d] = pm[VELX + d] * pm[RHO];
-        cp[MOMX + d] = pp[VELX + d] * pp[RHO];
-      }
-      cm[ENERGY] = eos_energy<DIM, T>(eos, pm[RHO], pm[VELX], DIM > 1 ? pm[VELX + (DIM > 1)] : T(0),
-                                      DIM > 2 ? pm[VELX + 2 * (DIM > 2)] : T(0), pm[PRES]);
-      cp[ENERGY] = eos_energy<DIM, T>(eos, pp[RHO], pp[VELX], DIM > 1 ? pp[VELX + (DIM > 1)] : T(0),
-                                      DIM > 2 ? pp[VELX + 2 * (DIM > 2)] : T(0), pp[PRES]);
-      if (!(cm[MASS] > eps_of<T>()) || !(cp[MASS] > eps_of<T>())) valid = false;
-      if (!(double(pm[PRES]) > -B) || !(double(pp[PRES]) > -B)) valid = false;
-      // HLLC's own 1/density (hllc_riemann_solver.h:75-78)
-      pol.template riemann<DIM, DIR, T>(eos, cm, cp, pm[PRES], pp[PRES], pm[VELX + DIR], pp[VELX + DIR],
-                        inv(cm[MASS]), inv(cp[MASS]), flux);
-    }
-  }
-
-#pragma unroll
-  for (int f = 0; f < NE; ++f) fd[f] = double(flux[f]);
-  return valid;
 }
 
 // Flux of the face with thread index t of direction DIR of the block in `slot`.
@@ -638,8 +355,7 @@ pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
   for (int m = 0; m < 6; ++m)
     stencil_load<DIM, DIR, true>(Uin, blk, HS - 3 + m, cell0, nlo, nhi, w[m]);
   double const ocs = inv(bm.cell_size);
-  double const cdt = kRkC[stage] * (0.0 + dt);
-  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+  RkStage const rk = rk_stage(stage, dt);
   double fprev[NE];
 #pragma unroll 1
   for (int a = 0; a <= IC; ++a) {
@@ -662,9 +378,7 @@ pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
           double const sum = DIM > 1 ? Rb[n * G::INTERIOR + ix] + d : d;
           double const rhs = 0.0 + sum * ocs;
           size_t const xf = x + (size_t)n * G::CELLS;
-          double u = Uin[xf];
-          if (stage != 0) u = a0 * u + a1 * U0[xf];
-          Uout[xf] = u + cdt * rhs;
+          Uout[xf] = rk_apply(rk, Uin[xf], rk.first ? 0.0 : U0[xf], rhs);
         }
       }
     }
@@ -691,11 +405,11 @@ __device__ __forceinline__ double divergence(double const *Fx, double const *Fy,
                                              double const *Fz, int i, int j, int k,
                                              double one_cell_size) {
   using G = Geo<DIM>;
-  double const dx = Fx[G::face(i, j + 1, k + 1)] - Fx[G::face(i + 1, j + 1, k + 1)];
-  double dy = 0.0, dz = 0.0;
-  if constexpr (DIM > 1) dy = Fy[G::face(i + 1, j, k + 1)] - Fy[G::face(i + 1, j + 1, k + 1)];
-  if constexpr (DIM > 2) dz = Fz[G::face(i + 1, j + 1, k)] - Fz[G::face(i + 1, j + 1, k + 1)];
-  return dacms<DIM>(dx, dy, dz) * one_cell_size;
+  return flux_divergence<DIM>(Fx[G::face(i, j + 1, k + 1)], Fx[G::face(i + 1, j + 1, k + 1)],
+                              DIM > 1 ? Fy[G::face(i + 1, j, k + 1)] : 0.0,
+                              DIM > 1 ? Fy[G::face(i + 1, j + 1, k + 1)] : 0.0,
+                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k)] : 0.0,
+                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k + 1)] : 0.0, one_cell_size);
 }
 
 template <int DIM>
@@ -765,8 +479,7 @@ stage_update_kernel(double const *Uin, double const *U0, double *Uout,
   interior_coords<DIM>(t, i, j, k);
   int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
   double const ocs = inv(bm.cell_size);
-  double const cdt = kRkC[stage] * (0.0 + dt);
-  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+  RkStage const rk = rk_stage(stage, dt);
   double const *Fb = F + (long long)item * stride;
   size_t const base = (size_t)slot * G::BLOCK_DOUBLES + c;
 #pragma unroll
@@ -774,9 +487,7 @@ stage_update_kernel(double const *Uin, double const *U0, double *Uout,
     double const *fx = Fb + f * G::FACES;
     double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
     size_t const x = base + (size_t)f * G::CELLS;
-    double u = Uin[x];
-    if (!rk_first_stage(stage)) u = a0 * u + a1 * U0[x];
-    Uout[x] = u + cdt * rhs;
+    Uout[x] = rk_apply(rk, Uin[x], rk.first ? 0.0 : U0[x], rhs);
   }
 }
 
@@ -792,15 +503,13 @@ rk_stage_rhs_kernel(double *__restrict__ U, double *__restrict__ U0,
   int i, j, k;
   interior_coords<DIM>(t, i, j, k);
   int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
-  double const cdt = kRkC[stage] * (0.0 + dt);
-  double const a0 = kRkA0[stage], a1 = kRkA1[stage];
+  RkStage const rk = rk_stage(stage, dt);
 #pragma unroll
   for (int f = 0; f < G::NE; ++f) {
     size_t const x = (size_t)slot * G::BLOCK_DOUBLES + (size_t)f * G::CELLS + c;
-    double u = U[x];
+    double const u = U[x];
     if (stage == 0) U0[x] = u;
-    else u = a0 * u + a1 * U0[x];
-    U[x] = u + cdt * rhs[x];
+    U[x] = rk_apply(rk, u, rk.first ? 0.0 : U0[x], rhs[x]);
   }
 }
 
@@ -967,19 +676,7 @@ signal_speed_kernel(double const *__restrict__ U, int const *__restrict__ work,
     double c[G::NE];
 #pragma unroll
     for (int f = 0; f < G::NE; ++f) c[f] = ub[f * G::CELLS + x];
-    double const one_density = inv(c[MASS]);
-    double const p = eos_pressure<DIM>(eos, c[MASS], c[MOMX], DIM > 1 ? c[MOMX + (DIM > 1)] : 0.0,
-                                       DIM > 2 ? c[MOMX + 2 * (DIM > 2)] : 0.0, c[ENERGY],
-                                       one_density);
-    double const cs = eos_speed_of_sound<double>(eos, c[MASS], p, one_density);
-    double v[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-    for (int d = 0; d < DIM; ++d) v[d] = fabs(c[MOMX + d] * one_density) + cs;
-    double s;
-    if constexpr (DIM == 1) s = v[0];
-    else if constexpr (DIM == 2) s = v[0] + v[1];
-    else s = cms3(v[0], v[1], v[2]);
-    if (!(s >= 0.0) || !(c[MASS] > 0.0)) bad = 1;  // NaN, negative density or c^2 < 0
+    double const s = cell_signal_speed<DIM>(eos, c, bad);
     smax = dmax(smax, s);
   }
   if (__syncthreads_or(bad) && threadIdx.x == 0 && cases) atomicOr(&cases[bm.case_id].status, 1);
@@ -1003,29 +700,19 @@ signal_speed_kernel(double const *__restrict__ U, int const *__restrict__ work,
 // dt = CFL / (smax / dx_finest), clipped to the end time
 // (modular_algorithm_assembler.cpp:1932, 1961-1982); 0 once t >= t_end or the
 // step budget is spent, which makes every kernel skip the case.
-__global__ void dt_finalize_kernel(CaseState *cases, int n) {
+// dt of every case from its smax (case_dt_finalize); dtflag, when given,
+// marks each case's dt as ready for a tile-stage launch (its step 0).
+__global__ void dt_finalize_kernel(CaseState *cases, int n, int *dtflag) {
   int const c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  CaseState &s = cases[c];
-  double const smax = __longlong_as_double((long long)s.smax_bits);
-  s.smax_bits = 0ull;
-  double dt = smax / s.h_min;
-  double local = dt == 0.0 ? DBL_MAX : s.cfl / dt;
-  if (s.t + local > s.t_end) local = dmax(s.t_end - s.t, 0.0);
-  if (!(s.t < s.t_end)) local = 0.0;
-  if (s.max_steps > 0 && s.steps >= s.max_steps) local = 0.0;
-  if (s.status || s.hold) local = 0.0;
-  s.dt = local;
+  case_dt_finalize(cases[c]);
+  if (dtflag) dtflag[c] = 1;
 }
 
 __global__ void step_commit_kernel(CaseState *cases, int n) {
   int const c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n) return;
-  CaseState &s = cases[c];
-  if (s.dt > 0.0) {
-    s.t = s.t + (0.0 + s.dt);
-    s.steps += 1;
-  }
+  case_commit(cases[c]);
 }
 
 }  // namespace
@@ -1406,9 +1093,9 @@ cudaError_t launch_initial_condition(int dim, double *U, int first, int const nb
   return cudaGetLastError();
 }
 
-cudaError_t launch_dt_finalize(CaseState *cases, int n, cudaStream_t stream) {
+cudaError_t launch_dt_finalize(CaseState *cases, int n, cudaStream_t stream, int *dtflag) {
   if (n <= 0) return cudaSuccess;
-  dt_finalize_kernel<<<(n + 127) / 128, 128, 0, stream>>>(cases, n);
+  dt_finalize_kernel<<<(n + 127) / 128, 128, 0, stream>>>(cases, n, dtflag);
   return cudaGetLastError();
 }
 

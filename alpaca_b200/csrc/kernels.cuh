@@ -135,8 +135,11 @@ cudaError_t launch_initial_condition(int dim, double *U, int first, int const nb
                                      double cell_size, double gamma, double B, int type,
                                      IcParams const &params, cudaStream_t stream);
 
-// dt for every case from its smax (ComputeTimestepSize), then resets smax.
-cudaError_t launch_dt_finalize(CaseState *cases, int ncases, cudaStream_t stream);
+// dt for every case from its smax (ComputeTimestepSize), then resets smax;
+// with dtflag, also sets dtflag[c] = 1 (dt of the first step of a tile-stage
+// launch is ready).
+cudaError_t launch_dt_finalize(CaseState *cases, int ncases, cudaStream_t stream,
+                               int *dtflag = nullptr);
 // t += dt, steps += (dt > 0) for every case.
 cudaError_t launch_step_commit(CaseState *cases, int ncases, cudaStream_t stream);
 

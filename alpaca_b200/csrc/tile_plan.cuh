@@ -1,0 +1,236 @@
+// Index plan of the fused tile-stage kernel (tile_step.cuh), as host and
+// device functions so that tests can replay it on the CPU.
+//
+// One work item is one SSP-RK3 (or TVD-RK2) stage of one 3D block. The block's
+// cells are walked in x-planes. Stencils are read from shared memory:
+//   * a ring of RING x-planes (16 x 16 cells, all five conserved fields) of the
+//     stage input: planes -3 .. 18 in interior numbering, the six outside the
+//     block taken from the x neighbours, none at walls (the readers map those
+//     cells onto the block, stencil_src);
+//   * per plane, the three rows beyond each y face and the (aligned, four wide)
+//     columns beyond each z face, from the y / z neighbours.
+// The item is a stream of warp tasks, taken by the CTA's warps in order:
+//   X0              x face 0 (8 tasks of 32 faces)
+//   for g = 0 .. 15:
+//     FX(g)         x face g + 1 (8 tasks)
+//     FY(g), FZ(g)  the 17 x 16 y faces and 16 x 17 z faces of plane g (9 tasks
+//                   each, the last one half full)
+//     U(g - 1)      flux divergence and stage update of plane g - 1 (8 tasks of
+//                   32 cells), for g >= 1
+//   U(15)
+// Every task waits only for tasks earlier in the stream (shared-memory
+// counters) and for the loads those tasks released, so the warps never wait in
+// a cycle. Faces are numbered as in the reference's flux arrays: face a of a
+// direction lies between cells a - 1 and a (convective_term_solver.h:67-81).
+#pragma once
+
+#include "layout.cuh"
+
+namespace alp {
+namespace tile {
+
+constexpr int NE = 5;           // conserved fields in 3D
+constexpr int PLANE = IC * IC;  // cells of one x-plane
+constexpr int YROW = 3 * IC;    // cells of one y halo (3 rows of 16)
+constexpr int ZCOL = IC * 4;    // cells of one z halo (16 rows, 4 columns loaded)
+constexpr int FACE_ROW = IC + 1;
+constexpr int NPLANES = IC + 6;  // planes -3 .. 18
+
+// shared-memory buffers
+constexpr int RING = 8;  // x-planes of the stage input
+constexpr int RFX = 4;   // x-face flux planes (face a in slot a % RFX)
+constexpr int BYZ = 3;   // y / z face flux buffers (plane g in buffer g % BYZ)
+constexpr int BH = 2;    // y / z halo buffers (plane g in buffer g % BH)
+constexpr int BU = 2;    // U0 planes (plane g in buffer g % BU)
+
+// Neighbour entries of the six faces in the 26-direction table (x slowest):
+// W, E, S, N, B, T = (-1,0,0), (+1,0,0), (0,-1,0), (0,+1,0), (0,0,-1), (0,0,+1).
+__host__ __device__ constexpr int face_slot(int d) {
+  return d == 0 ? 4 : d == 1 ? 21 : d == 2 ? 10 : d == 3 ? 15 : d == 4 ? 12 : 13;
+}
+
+__host__ __device__ constexpr int ring_slot(int q) { return (q + 3) % RING; }
+
+// Source of a stencil cell beyond the block along one direction: the index in
+// the neighbour's buffer, or, at a domain face, the block's own cell (zero
+// gradient: the first / last interior cell; symmetry: the mirror image, whose
+// momentum normal to the wall is negated; symmetry_boundary_condition.h:60-217,
+// boundary_constants.h:35-46, 103-160).
+struct Src {
+  int index;    // -3 .. 18: cell index along the direction
+  bool own;     // true: the block's own cell `index` (0 .. 15)
+  bool negate;  // mirror cell of a symmetry wall
+};
+__host__ __device__ inline Src stencil_src(int c, int nlo, int nhi) {
+  if (c < 0) {
+    if (nlo >= 0) return Src{c, false, false};
+    if (nlo == -1) return Src{0, true, false};
+    return Src{-1 - c, true, true};
+  }
+  if (c >= IC) {
+    if (nhi >= 0) return Src{c, false, false};
+    if (nhi == -1) return Src{IC - 1, true, false};
+    return Src{2 * IC - 1 - c, true, true};
+  }
+  return Src{c, true, false};
+}
+
+// ---- the task stream ------------------------------------------------------
+enum TaskType { T_FX = 0, T_FY = 1, T_FZ = 2, T_U = 3, T_NONE = 4 };
+constexpr int XT = PLANE / 32;                  // warp tasks of one x-face plane (8)
+constexpr int YT = (FACE_ROW * IC + 31) / 32;   // of the y faces of one plane (9)
+constexpr int UT = PLANE / 32;                  // of one plane's stage update (8)
+constexpr int ITER = XT + 2 * YT + UT;          // tasks of one plane g >= 1 (34)
+constexpr int STREAM = XT + (XT + 2 * YT) + (IC - 1) * ITER + UT;  // 552
+
+struct Task {
+  int type;  // TaskType
+  int g;     // FX: face g (0 .. 16); FY, FZ, U: plane g
+  int w;     // task index within its kind (selects the 32 faces or cells)
+};
+__host__ __device__ inline Task decode(int pos) {
+  if (pos < XT) return Task{T_FX, 0, pos};
+  pos -= XT;
+  int g, r;
+  if (pos < XT + 2 * YT) {
+    g = 0;
+    r = pos;
+  } else {
+    pos -= XT + 2 * YT;
+    if (pos >= (IC - 1) * ITER) {
+      pos -= (IC - 1) * ITER;
+      return pos < UT ? Task{T_U, IC - 1, pos} : Task{T_NONE, 0, 0};
+    }
+    g = 1 + pos / ITER;
+    r = pos % ITER;
+  }
+  if (r < XT) return Task{T_FX, g + 1, r};
+  if (r < XT + YT) return Task{T_FY, g, r - XT};
+  if (r < XT + 2 * YT) return Task{T_FZ, g, r - XT - YT};
+  return Task{T_U, g - 1, r - XT - 2 * YT};
+}
+
+// Reads of each x-plane (index q + 3) by the item's warp tasks, given the x
+// neighbours (walls map cells onto the block): 8 tasks per x face per stencil
+// cell, and for the block's own planes 9 + 9 (y, z faces) + 8 (stage update).
+// A plane with no reads is not loaded; when a plane's count drops to zero its
+// ring slot takes the next loaded plane of that slot.
+__host__ __device__ inline void plane_reads(int nlo, int nhi, int (&reads)[NPLANES]) {
+  for (int q = 0; q < NPLANES; ++q) reads[q] = 0;
+  for (int a = 0; a <= IC; ++a)
+    for (int m = 0; m < 6; ++m) reads[stencil_src(a - 3 + m, nlo, nhi).index + 3] += XT;
+  for (int g = 0; g < IC; ++g) reads[g + 3] += 2 * YT + UT;
+}
+// First loaded plane of ring slot s (or 99 when none).
+__host__ __device__ inline int first_plane_of_slot(int s, int const (&reads)[NPLANES]) {
+  for (int q = s - 3; q <= IC + 2; q += RING)
+    if (reads[q + 3] > 0) return q;
+  return 99;
+}
+// The loaded plane after q in q's ring slot (or 99 when none).
+__host__ __device__ inline int next_plane_of_slot(int q, int const (&reads0)[NPLANES]) {
+  for (int n = q + RING; n <= IC + 2; n += RING)
+    if (reads0[n + 3] > 0) return n;
+  return 99;
+}
+
+
+// ---- TMA boxes ------------------------------------------------------------------
+// Start of a box in the reference-layout pool [block][field][24][24][24]
+// (coordinates z, y, x, field 0, block; z fastest). The z start must be a
+// multiple of two doubles (16 bytes), which HS and HS + 12 are.
+struct Box {
+  int k, j, i, blk;
+};
+// Plane q (-3..18) of block `slot`: box 16 (z) x 16 (y) x 1 (x) x 5 fields.
+__host__ __device__ inline Box plane_box(int q, int slot, int const (&nbr)[6]) {
+  if (q < 0) return Box{HS, HS, HS + q + IC, nbr[0]};
+  if (q >= IC) return Box{HS, HS, HS + q - IC, nbr[1]};
+  return Box{HS, HS, HS + q, slot};
+}
+// y halo rows of plane g: rows 13..15 of the low neighbour (side 0), 0..2 of
+// the high one (side 1); box 16 x 3 x 1 x 5.
+__host__ __device__ inline Box yhalo_box(int g, int side, int const (&nbr)[6]) {
+  return Box{HS, side ? HS : HS + IC - 3, HS + g, nbr[2 + side]};
+}
+// z halo columns of plane g: columns 12..15 of the low neighbour, 0..3 of the
+// high one; box 4 x 16 x 1 x 5.
+__host__ __device__ inline Box zhalo_box(int g, int side, int const (&nbr)[6]) {
+  return Box{side ? HS : HS + IC - 4, HS, HS + g, nbr[4 + side]};
+}
+
+// ---- shared memory of one CTA ------------------------------------------------
+struct Smem {
+  double ring[RING][NE][PLANE];
+  double fx[RFX][NE][PLANE];
+  double fy[BYZ][NE][FACE_ROW * IC];  // [a][k]
+  double fz[BYZ][NE][IC * FACE_ROW];  // [j][a]
+  double yh[BH][2][NE][YROW];         // [buffer][low / high side]
+  double zh[BH][2][NE][ZCOL];
+  double u0[BU][NE][PLANE];
+  unsigned long long bar_plane[NPLANES];  // one load per plane and item
+  unsigned long long bar_halo[IC];
+  unsigned long long bar_u0[IC];
+  int reads[NPLANES];   // outstanding reads of each x-plane
+  int reads0[NPLANES];  // reads at the item's start
+  int reads_h[IC];      // outstanding reads of each plane's y / z halos
+  int reads_u[IC];      // outstanding reads of each U0 plane
+  int cnt_x[IC + 1];    // finished tasks of each x face
+  int cnt_yz[IC];       // finished y and z face tasks of each plane
+  int cnt_u[IC];        // finished stage-update tasks of each plane
+  int next_task;
+  int item, skip, bad, dt_ready;
+  int nbr[6];
+  double dt;
+  double red[32];
+};
+
+
+// The 6-cell stencil (cells a - 3 .. a + 2 along x, all fields) of x face a at
+// transverse position jk = j * 16 + k, from the ring.
+__host__ __device__ inline void gather_x(Smem const &S, int a, int jk, double (&cons)[6][NE]) {
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    Src const s = stencil_src(a - 3 + m, S.nbr[0], S.nbr[1]);
+    double const *src = &S.ring[ring_slot(s.index)][0][jk];
+#pragma unroll
+    for (int f = 0; f < NE; ++f) cons[m][f] = src[f * PLANE];
+    if (s.negate) cons[m][MOMX] = -1.0 * cons[m][MOMX];
+  }
+}
+
+// The stencil of face q (0 .. 271) of plane g along y (DIR 1: face a of column
+// k = t) or z (DIR 2: face a of row j = t), from the plane and its halos.
+template <int DIR>
+__host__ __device__ inline void gather_yz(Smem const &S, int g, int q, int &a, int &t,
+                                          double (&cons)[6][NE]) {
+  a = DIR == 1 ? q / IC : q % FACE_ROW;
+  t = DIR == 1 ? q % IC : q / FACE_ROW;
+  double const *plane = &S.ring[ring_slot(g)][0][0];
+  int const hb = g % BH;
+  int const nlo = S.nbr[2 * DIR], nhi = S.nbr[2 * DIR + 1];
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    Src const s = stencil_src(a - 3 + m, nlo, nhi);
+    double const *src;
+    int fs;
+    if (s.own) {
+      src = DIR == 1 ? plane + s.index * IC + t : plane + t * IC + s.index;
+      fs = PLANE;
+    } else if (DIR == 1) {
+      src = s.index < 0 ? &S.yh[hb][0][0][(s.index + 3) * IC + t]
+                        : &S.yh[hb][1][0][(s.index - IC) * IC + t];
+      fs = YROW;
+    } else {
+      src = s.index < 0 ? &S.zh[hb][0][0][t * 4 + s.index + 4]
+                        : &S.zh[hb][1][0][t * 4 + s.index - IC];
+      fs = ZCOL;
+    }
+#pragma unroll
+    for (int f = 0; f < NE; ++f) cons[m][f] = src[f * fs];
+    if (s.negate) cons[m][MOMX + DIR] = -1.0 * cons[m][MOMX + DIR];
+  }
+}
+
+}  // namespace tile
+}  // namespace alp

@@ -213,6 +213,8 @@ _SIGS = {
     "alp_engine_stream": (_S, [_V]),
     "alp_engine_set_graph": (C.c_int, [_V, C.c_int]),
     "alp_engine_launches_per_step": (C.c_int, [_V]),
+    "alp_engine_launches": (C.c_int, [_V, C.c_int]),
+    "alp_engine_path": (C.c_int, [_V]),
     "alp_engine_autotune": (C.c_int, [_V, C.c_int, _I, C.POINTER(C.c_float)]),
     "alp_engine_set_path": (C.c_int, [_V, C.c_int]),
     "alp_levels_create": (C.c_int, [C.c_int, C.POINTER(Scheme), C.POINTER(Material), _I, C.c_double,
@@ -224,6 +226,11 @@ _SIGS = {
     "alp_levels_info": (C.c_int, [_V, _I, _I, C.POINTER(C.c_longlong), _I]),
     "alp_levels_stream": (_S, [_V]),
 }
+
+# stepping candidates of alp_engine_autotune (ALP_STEP_CANDIDATES)
+STEP_CANDIDATES = 6
+# the fused tile-stage candidates (16 and 12 warps per CTA)
+TILE_CANDIDATES = (4, 5)
 
 _libs = {}
 

@@ -39,6 +39,11 @@ FLOPS_PER_CELL_UPDATE_3D = {"fvchar": 15767, "fvprim": 10192, "fsroe": 22478}
 # and dram__bytes_write.sum over the step's kernels, one ncu capture; summary in
 # profiles/step_fvchar_128cubed.md)
 TRAFFIC_PER_STEP = {("fvchar", "fp64"): 4.359e9}
+# stepping candidates of alp_engine_autotune, in its numbering
+CANDIDATES = ["face fluxes, 128-thread blocks", "face fluxes, 64-thread blocks", "pencil sweeps",
+              "face fluxes and stage updates overlapped in batches",
+              "fused tile stages (TMA-staged, one persistent launch), 16 warps",
+              "fused tile stages (TMA-staged, one persistent launch), 12 warps"]
 
 
 def parse():
@@ -410,7 +415,7 @@ def run_ours(args, ws, rank, local):
     ms = max_over_ranks(e0.elapsed_time(e1), ws, dev)
     value = cells * args.steps * ws / (ms * 1e-3)
     _, t_sim, steps_done = eng.get(cid)
-    launches = args.steps * eng.launches_per_step
+    launches = eng.launches(args.steps)
     eng.close()
 
     # end to end through the public C ABI from pinned host buffers: upload the
@@ -489,10 +494,7 @@ def run_ours(args, ws, rank, local):
                    "cfl": 0.6, "l2": "state 283 MB per buffer > 126 MB L2 (no flush needed)",
                    "parallelism": f"replicas x{ws}", "sim_time_reached": t_sim,
                    "steps_done": steps_done,
-                   "autotune": {"chosen": ["face fluxes, 128-thread blocks",
-                                           "face fluxes, 64-thread blocks",
-                                           "pencil sweeps",
-                                           "face fluxes and stage updates overlapped in batches"][chosen],
+                   "autotune": {"chosen": CANDIDATES[chosen], "candidates": CANDIDATES,
                                 "ms_per_step": cand_ms}},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm,

@@ -346,6 +346,9 @@ alp_stream_t alp_engine_stream(alp_engine *e);
 /* Enables (1) or disables (0) CUDA-graph replay of the step (default on). */
 int alp_engine_set_graph(alp_engine *e, int enabled);
 
+/* Number of stepping candidates of alp_engine_autotune / alp_engine_set_path. */
+#define ALP_STEP_CANDIDATES 6
+
 /* Times the stepping candidates on the engine's resident cases and keeps the
  * fastest: 0 = face fluxes (128-thread blocks, all directions in one launch)
  * + divergence/stage update, 1 = the same with 64-thread blocks, 2 = pencil
@@ -354,18 +357,34 @@ int alp_engine_set_graph(alp_engine *e, int enabled);
  * the last direction; not available in the strict build; default schemes
  * only), 3 = candidate 0 in batches of about 64 blocks, the stage update of
  * one batch on a second stream overlapping the face fluxes of the next (same
- * arithmetic). Each candidate runs trial_steps steps
- * whose last stage writes scratch memory and that are not committed, so the
- * cases' state and time are unchanged. *chosen receives the candidate (-1 when
- * no case is resident), ms_per_step[4] (may be null) the measured time per
- * step of each candidate (-1 when not run). Synchronises. */
+ * arithmetic), 4 = fused tile stages with 16 warps per CTA, 5 = the same with
+ * 12 warps. The fused tile stages (3D engines with WENO5 + HLLC/Einfeldt or
+ * Roe splitting, RK3 or RK2) advance all steps of one alp_engine_step call in
+ * one persistent launch: per (step, stage, block) work item, the block's cell
+ * planes and the neighbours' cells beyond its faces are staged into shared
+ * memory by TMA, every face flux is computed once into shared memory and the
+ * divergence and RK stage are applied there, so no face flux reaches HBM. Its
+ * arithmetic is that of candidate 0, so results are bit-identical; it is the
+ * default where it applies. Each candidate runs trial_steps steps whose last
+ * stage writes scratch memory and that are not committed, so the cases' state
+ * and time are unchanged. *chosen receives the candidate (-1 when no case is
+ * resident), ms_per_step[ALP_STEP_CANDIDATES] (may be null) the measured time
+ * per step of each candidate (-1 when not run). Synchronises. */
 int alp_engine_autotune(alp_engine *e, int trial_steps, int *chosen, float *ms_per_step);
 
-/* Selects a stepping candidate (as numbered for alp_engine_autotune). */
+/* Selects a stepping candidate (as numbered for alp_engine_autotune);
+ * ALP_ERR_INVALID for a candidate that cannot step this engine. */
 int alp_engine_set_path(alp_engine *e, int candidate);
 
-/* Number of kernel launches one engine step issues. */
+/* The engine's current stepping candidate (-1 for a null engine). */
+int alp_engine_path(alp_engine *e);
+
+/* Number of kernel launches one engine step issues (the fused tile stages:
+ * per alp_engine_step call, whatever its step count). */
 int alp_engine_launches_per_step(alp_engine *e);
+
+/* Number of kernel launches alp_engine_step(e, n) issues. */
+int alp_engine_launches(alp_engine *e, int n);
 
 /* ---- multi-level cases: leaves of a block tree, local time stepping ----- */
 

@@ -485,8 +485,9 @@ def test_fp32_flux_3d_100_steps(cuda, variant):
 def test_autotune_leaves_state_and_candidates_agree(cuda):
     """Autotuning runs uncommitted trial steps (state and time unchanged); every
     candidate advances the case to the same result within the FP64 tolerance
-    (face paths, one launch or overlapped batches, bit-identical to each other;
-    the pencil path sums the three flux differences in a different order)."""
+    (face paths, one launch or overlapped batches, and the fused tile stages
+    with 16 or 12 warps, bit-identical to each other; the pencil path sums the
+    three flux differences in a different order)."""
     case = cases.fourier_shock(2, dim=3, seed=31, steps=6)
     eng = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
     cid = eng.add_case(case)
@@ -494,21 +495,23 @@ def test_autotune_leaves_state_and_candidates_agree(cuda):
     before = eng.get(cid)
     chosen, ms = eng.autotune(trial_steps=2)
     after = eng.get(cid)
-    assert chosen in (0, 1, 2, 3) and all(m > 0 for m in ms)
+    assert chosen in range(N.STEP_CANDIDATES) and all(m > 0 for m in ms)
+    assert eng.path == chosen
     assert np.array_equal(before[0], after[0]) and before[1:] == after[1:]
     results = []
-    for cand in (0, 1, 2, 3):
+    for cand in range(N.STEP_CANDIDATES):
         e = api.Engine(3, "fvchar", capacity_blocks=8, max_cases=1)
         i = e.add_case(case)
         e.set_path(cand)
         e.run_to_end(chunk=6)
-        results.append(e.get(i)[0])
+        results.append(e.get(i))
         e.close()
     eng.close()
     I = cases.interior(3)
-    assert np.array_equal(results[0], results[1])
-    assert np.array_equal(results[0][I], results[3][I])
-    assert l1_per_field(results[2][I], results[0][I]) <= 1e-13
+    for cand in (1, 3, 4, 5):
+        assert np.array_equal(results[0][0][I], results[cand][0][I]), cand
+        assert results[0][1:] == results[cand][1:], cand
+    assert l1_per_field(results[2][0][I], results[0][0][I]) <= 1e-13
 
 
 @pytest.mark.parametrize("variant", ["fvchar", "fsroe"])

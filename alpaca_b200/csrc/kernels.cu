@@ -11,6 +11,7 @@
 
 #include "kernels.cuh"
 #include "face.cuh"
+#include "rotate.cuh"
 #include "step_common.cuh"
 
 namespace alp {
@@ -186,7 +187,22 @@ __device__ __forceinline__ void face_flux(double const *__restrict__ U,
   for (int m = 0; m < W; ++m)
     stencil_load<DIM, DIR, GATHER>(U, blk, HS + a - W / 2 + m, cell0, nlo, nhi, cons[m]);
   double fd[NE];
-  bool const valid = face_compute<DIM, DIR, SCHEME, T, P, W>(eos, bm.B, cons, fd, pol);
+  bool valid;
+  if constexpr (DIM == 3 && DIR != 0) {
+    // 3D y and z faces: the x-face computation of the rotated stencil
+    // (canon_field), the same code as the fused tile kernel
+    double rc[W][NE];
+#pragma unroll
+    for (int m = 0; m < W; ++m)
+#pragma unroll
+      for (int c = 0; c < NE; ++c) rc[m][c] = cons[m][canon_field(DIR, c)];
+    double rf[NE];
+    valid = face_compute<3, 0, SCHEME, T, P, W>(eos, bm.B, rc, rf, pol);
+#pragma unroll
+    for (int c = 0; c < NE; ++c) fd[canon_field(DIR, c)] = rf[c];
+  } else {
+    valid = face_compute<DIM, DIR, SCHEME, T, P, W>(eos, bm.B, cons, fd, pol);
+  }
   write_flux<DIM, DIR, ACCUM>(F, item, stride, a, p1, p2, valid, fd);
 }
 

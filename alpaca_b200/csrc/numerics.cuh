@@ -89,6 +89,10 @@ __device__ __forceinline__ float tsqrt(float x) {
   }
 }
 
+// A product rounded on its own (never fused into a following addition).
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+
 template <typename T> __device__ __forceinline__ T dmin(T a, T b) { return (b < a) ? b : a; }
 template <typename T> __device__ __forceinline__ T dmax(T a, T b) { return (a < b) ? b : a; }
 template <typename T> __device__ __forceinline__ T eps_of();
@@ -505,8 +509,17 @@ __device__ __forceinline__ void to_physical(Roe<T> const &r, T const (&ch)[DIM +
   // R[ENERGY][*] = (H - u c, -u1 rho, rho u2, gru H - c c, H + u c)
   {
     T s = T(0);
-    if constexpr (DIM > 1) s = ch[1] * (-r.u1 * r.rho);
-    if constexpr (DIM > 2) s = s + ch[2] * (r.rho * r.u2);
+    if constexpr (DIM == 2) s = ch[1] * (-r.u1 * r.rho);
+    if constexpr (DIM > 2) {
+      // The two minor-wave terms are rounded as products before they are
+      // added, so that the sum does not depend on which minor momentum is
+      // numbered first: with the minor momenta exchanged (and their waves'
+      // signs, as the characteristic variables then are) the bits are the
+      // same. The strict build rounds every product anyway.
+      T const t1 = rmul(ch[1], -r.u1 * r.rho);
+      T const t2 = rmul(ch[2], r.rho * r.u2);
+      s = t1 + t2;
+    }
     s = s + ch[EV] * (r.gru * r.H - r.c * r.c);
     out[ENERGY] = s + (ch[0] * (r.H - r.up * r.c) + ch[NE - 1] * (r.H + r.up * r.c));
   }

@@ -97,6 +97,40 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
   auto elapsed = [&]() { return std::chrono::duration<double>(Clock::now() - t0).count(); };
   int rc_all = ALP_OK;
 
+  // A clean stop on request: once the abort file exists, every unfinished
+  // request ends with ALP_ABORTED (resident cases with their state so far).
+  auto abort_requested = [&]() {
+    return done < n && cfg->abort_file && access(cfg->abort_file, F_OK) == 0;
+  };
+  auto abort_now = [&]() -> int {
+    double const t_now = elapsed();
+    for (auto &p : pool) {
+      if (p.active == 0) continue;
+      for (int c = 0; c < cfg->max_cases; ++c) {
+        int const ri = p.req_of_case[c];
+        if (ri < 0) continue;
+        ended[ri] = 1;
+        double t = 0.0;
+        int st = 0;
+        int const grc = alp_engine_get_case(p.eng, c, reqs[ri].h_result, &t, &st);
+        if (grc != ALP_OK && grc != ALP_ERR_NUMERIC) {
+          cleanup();
+          return grc;
+        }
+        alp_result &out = results[ri];
+        out.finished_s = t_now;
+        out.t = t;
+        out.steps = st;
+        out.status = ALP_ABORTED;
+      }
+    }
+    for (int i = 0; i < n; ++i)
+      if (!ended[i]) results[i] = alp_result{reqs[i].arrival_s, -1.0, t_now, 0.0, 0, ALP_ABORTED};
+    if (makespan_s) *makespan_s = t_now;
+    cleanup();
+    return fail(ALP_ABORTED, "stopped: the abort file exists");
+  };
+
   while (done < n) {
     double const now = elapsed();
     while (next < n && reqs[order[next]].arrival_s <= now) queue.push_back(order[next++]);
@@ -145,6 +179,8 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     }
 
     if (total_active == 0) {
+      // nothing resident: the file is checked while the loop waits for arrivals
+      if (abort_requested()) return abort_now();
       if (next < n && queue.empty()) {
         double const wait = reqs[order[next]].arrival_s - elapsed();
         if (wait > 0) std::this_thread::sleep_for(std::chrono::duration<double>(std::min(wait, 1e-3)));
@@ -240,35 +276,8 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
         ++done;
       }
     }
-    // a clean stop on request: the abort file exists
-    if (done < n && cfg->abort_file && access(cfg->abort_file, F_OK) == 0) {
-      double const t_now = elapsed();
-      for (auto &p : pool) {
-        if (p.active == 0) continue;
-        for (int c = 0; c < cfg->max_cases; ++c) {
-          int const ri = p.req_of_case[c];
-          if (ri < 0) continue;
-          ended[ri] = 1;
-          double t = 0.0;
-          int st = 0;
-          int const grc = alp_engine_get_case(p.eng, c, reqs[ri].h_result, &t, &st);
-          if (grc != ALP_OK && grc != ALP_ERR_NUMERIC) {
-            cleanup();
-            return grc;
-          }
-          alp_result &out = results[ri];
-          out.finished_s = t_now;
-          out.t = t;
-          out.steps = st;
-          out.status = ALP_ABORTED;
-        }
-      }
-      for (int i = 0; i < n; ++i)
-        if (!ended[i]) results[i] = alp_result{reqs[i].arrival_s, -1.0, t_now, 0.0, 0, ALP_ABORTED};
-      if (makespan_s) *makespan_s = t_now;
-      cleanup();
-      return fail(ALP_ABORTED, "stopped: the abort file exists");
-    }
+    // after every poll, as the reference checks its ABORTFILE after every step
+    if (abort_requested()) return abort_now();
   }
   if (makespan_s) *makespan_s = elapsed();
   cleanup();

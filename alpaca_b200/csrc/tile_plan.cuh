@@ -25,6 +25,7 @@
 #pragma once
 
 #include "layout.cuh"
+#include "rotate.cuh"
 
 namespace alp {
 namespace tile {
@@ -186,50 +187,71 @@ struct Smem {
 };
 
 
-// The 6-cell stencil (cells a - 3 .. a + 2 along x, all fields) of x face a at
-// transverse position jk = j * 16 + k, from the ring.
-__host__ __device__ inline void gather_x(Smem const &S, int a, int jk, double (&cons)[6][NE]) {
-#pragma unroll
-  for (int m = 0; m < 6; ++m) {
-    Src const s = stencil_src(a - 3 + m, S.nbr[0], S.nbr[1]);
-    double const *src = &S.ring[ring_slot(s.index)][0][jk];
-#pragma unroll
-    for (int f = 0; f < NE; ++f) cons[m][f] = src[f * PLANE];
-    if (s.negate) cons[m][MOMX] = -1.0 * cons[m][MOMX];
-  }
+// One face of a warp task: direction dir; x faces: face a at jk = j * 16 + k
+// (q = jk); y faces of plane g: face a of column k = t (q = a * 16 + t); z
+// faces of plane g: face a of row j = t (q = t * 17 + a).
+struct FaceAt {
+  int a, t;
+};
+__host__ __device__ inline FaceAt face_at(int dir, int q) {
+  if (dir == 0) return FaceAt{0, q};
+  if (dir == 1) return FaceAt{q / IC, q % IC};
+  return FaceAt{q % FACE_ROW, q / FACE_ROW};
 }
 
-// The stencil of face q (0 .. 271) of plane g along y (DIR 1: face a of column
-// k = t) or z (DIR 2: face a of row j = t), from the plane and its halos.
-template <int DIR>
-__host__ __device__ inline void gather_yz(Smem const &S, int g, int q, int &a, int &t,
-                                          double (&cons)[6][NE]) {
-  a = DIR == 1 ? q / IC : q % FACE_ROW;
-  t = DIR == 1 ? q % IC : q / FACE_ROW;
+// The 6-cell stencil (cells a - 3 .. a + 2 along dir, the five fields in
+// canonical order) of face q of x face plane g (dir 0) or of plane g (dir 1,
+// 2), from the ring and the halo buffers; symmetry walls negate the principal
+// momentum of mirrored cells.
+__host__ __device__ inline void gather_face(Smem const &S, int dir, int g, int q,
+                                            double (&cons)[6][NE]) {
+  FaceAt const f = face_at(dir, q);
+  int const a = dir == 0 ? g : f.a;
+  int const nlo = S.nbr[2 * dir], nhi = S.nbr[2 * dir + 1];
+  int const o2 = canon_field(dir, MOMX), o3 = canon_field(dir, MOMX + 1),
+            o4 = canon_field(dir, MOMX + 2);
   double const *plane = &S.ring[ring_slot(g)][0][0];
   int const hb = g % BH;
-  int const nlo = S.nbr[2 * DIR], nhi = S.nbr[2 * DIR + 1];
 #pragma unroll
   for (int m = 0; m < 6; ++m) {
     Src const s = stencil_src(a - 3 + m, nlo, nhi);
     double const *src;
     int fs;
-    if (s.own) {
-      src = DIR == 1 ? plane + s.index * IC + t : plane + t * IC + s.index;
+    if (dir == 0) {
+      src = &S.ring[ring_slot(s.index)][0][f.t];
       fs = PLANE;
-    } else if (DIR == 1) {
-      src = s.index < 0 ? &S.yh[hb][0][0][(s.index + 3) * IC + t]
-                        : &S.yh[hb][1][0][(s.index - IC) * IC + t];
+    } else if (s.own) {
+      src = dir == 1 ? plane + s.index * IC + f.t : plane + f.t * IC + s.index;
+      fs = PLANE;
+    } else if (dir == 1) {
+      src = s.index < 0 ? &S.yh[hb][0][0][(s.index + 3) * IC + f.t]
+                        : &S.yh[hb][1][0][(s.index - IC) * IC + f.t];
       fs = YROW;
     } else {
-      src = s.index < 0 ? &S.zh[hb][0][0][t * 4 + s.index + 4]
-                        : &S.zh[hb][1][0][t * 4 + s.index - IC];
+      src = s.index < 0 ? &S.zh[hb][0][0][f.t * 4 + s.index + 4]
+                        : &S.zh[hb][1][0][f.t * 4 + s.index - IC];
       fs = ZCOL;
     }
-#pragma unroll
-    for (int f = 0; f < NE; ++f) cons[m][f] = src[f * fs];
-    if (s.negate) cons[m][MOMX + DIR] = -1.0 * cons[m][MOMX + DIR];
+    cons[m][MASS] = src[MASS * fs];
+    cons[m][ENERGY] = src[ENERGY * fs];
+    cons[m][MOMX] = src[o2 * fs];
+    cons[m][MOMX + 1] = src[o3 * fs];
+    cons[m][MOMX + 2] = src[o4 * fs];
+    if (s.negate) cons[m][MOMX] = -1.0 * cons[m][MOMX];
   }
+}
+
+// Where the flux of that face goes (field f of the reference's order at
+// base + f * stride).
+struct FluxAt {
+  double *base;
+  int stride;
+};
+__host__ __device__ inline FluxAt flux_at(Smem &S, int dir, int g, int q) {
+  FaceAt const f = face_at(dir, q);
+  if (dir == 0) return FluxAt{&S.fx[g % RFX][0][f.t], PLANE};
+  if (dir == 1) return FluxAt{&S.fy[g % BYZ][0][f.a * IC + f.t], FACE_ROW * IC};
+  return FluxAt{&S.fz[g % BYZ][0][f.t * FACE_ROW + f.a], IC * FACE_ROW};
 }
 
 }  // namespace tile

@@ -185,66 +185,55 @@ struct ItemCtx {
   double const *dt_case;
 };
 
-// x face a (32 faces of task w): stencils from the ring.
+// A face task: 32 faces of x face plane g (FX) or of plane g's y / z faces
+// (FY, FZ). Lane 0 waits until the buffers the task writes are free and the
+// planes it reads have arrived, and afterwards counts the task done and
+// releases its reads. Every direction goes through the one face_compute<3, 0>
+// of the rotated stencil (gather_face), so the SM runs one copy of the face
+// arithmetic.
 template <int SCHEME, typename T>
-__device__ __forceinline__ void task_fx(Smem &S, ItemCtx const &C, int a, int w, bool compute) {
+__device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const &t, bool compute) {
   int const lane = threadIdx.x & 31;
+  int const dir = t.type;  // T_FX, T_FY, T_FZ are 0, 1, 2
+  int const g = t.g;
   if (lane == 0) {
-    // the flux slot of face a held face a - RFX, read by the updates of planes
-    // a - RFX - 1 and a - RFX
-    if (a > RFX) smem_wait_ge(&S.cnt_u[a - RFX - 1], UT, C.err);
-    if (a >= RFX) smem_wait_ge(&S.cnt_u[a - RFX], UT, C.err);
-    for (int m = 0; m < 6; ++m)
-      mbar_wait(&S.bar_plane[stencil_src(a - 3 + m, S.nbr[0], S.nbr[1]).index + 3], C.err);
+    if (dir == 0) {
+      // the flux slot of face g held face g - RFX, read by the updates of
+      // planes g - RFX - 1 and g - RFX
+      if (g > RFX) smem_wait_ge(&S.cnt_u[g - RFX - 1], UT, C.err);
+      if (g >= RFX) smem_wait_ge(&S.cnt_u[g - RFX], UT, C.err);
+      for (int m = 0; m < 6; ++m)
+        mbar_wait(&S.bar_plane[stencil_src(g - 3 + m, S.nbr[0], S.nbr[1]).index + 3], C.err);
+    } else {
+      // the flux buffer held plane g - BYZ, read by its stage update
+      if (g >= BYZ) smem_wait_ge(&S.cnt_u[g - BYZ], UT, C.err);
+      mbar_wait(&S.bar_plane[g + 3], C.err);
+      mbar_wait(&S.bar_halo[g], C.err);
+    }
   }
   __syncwarp();
-  if (compute) {
-    int const jk = w * 32 + lane;
+  int const q = t.w * 32 + lane;
+  if (compute && (dir == 0 || q < FACE_ROW * IC)) {
     double cons[6][NE];
-    gather_x(S, a, jk, cons);
+    gather_face(S, dir, g, q, cons);
     double fd[NE];
     bool const valid = face_compute<3, 0, SCHEME, T>(C.eos, C.B, cons, fd);
-    double *dst = &S.fx[a % RFX][0][jk];
+    FluxAt const o = flux_at(S, dir, g, q);
 #pragma unroll
-    for (int f = 0; f < NE; ++f) dst[f * PLANE] = valid ? fd[f] : 0.0;
+    for (int c = 0; c < NE; ++c) o.base[canon_field(dir, c) * o.stride] = valid ? fd[c] : 0.0;
   }
   __syncwarp();
   if (lane == 0) {
     __threadfence_block();
-    atomicAdd(&S.cnt_x[a], 1);
-    for (int m = 0; m < 6; ++m)
-      release_plane(S, C.pmap, C.slot, stencil_src(a - 3 + m, S.nbr[0], S.nbr[1]).index);
-  }
-}
-
-// y (DIR 1) or z (DIR 2) faces of plane g (32 faces of task w).
-template <int DIR, int SCHEME, typename T>
-__device__ __forceinline__ void task_fyz(Smem &S, ItemCtx const &C, int g, int w, bool compute) {
-  int const lane = threadIdx.x & 31;
-  if (lane == 0) {
-    // the flux buffer held plane g - BYZ, read by its stage update
-    if (g >= BYZ) smem_wait_ge(&S.cnt_u[g - BYZ], UT, C.err);
-    mbar_wait(&S.bar_plane[g + 3], C.err);
-    mbar_wait(&S.bar_halo[g], C.err);
-  }
-  __syncwarp();
-  int const q = w * 32 + lane;
-  if (compute && q < FACE_ROW * IC) {
-    int a, t;
-    double cons[6][NE];
-    gather_yz<DIR>(S, g, q, a, t, cons);
-    double fd[NE];
-    bool const valid = face_compute<3, DIR, SCHEME, T>(C.eos, C.B, cons, fd);
-    double *dst = DIR == 1 ? &S.fy[g % BYZ][0][a * IC + t] : &S.fz[g % BYZ][0][t * FACE_ROW + a];
-#pragma unroll
-    for (int f = 0; f < NE; ++f) dst[f * FACE_ROW * IC] = valid ? fd[f] : 0.0;
-  }
-  __syncwarp();
-  if (lane == 0) {
-    __threadfence_block();
-    atomicAdd(&S.cnt_yz[g], 1);
-    release_plane(S, C.pmap, C.slot, g);
-    if (atomicSub(&S.reads_h[g], 1) == 1 && g + BH < IC) issue_halos(S, C.ymap, C.zmap, g + BH);
+    if (dir == 0) {
+      atomicAdd(&S.cnt_x[g], 1);
+      for (int m = 0; m < 6; ++m)
+        release_plane(S, C.pmap, C.slot, stencil_src(g - 3 + m, S.nbr[0], S.nbr[1]).index);
+    } else {
+      atomicAdd(&S.cnt_yz[g], 1);
+      release_plane(S, C.pmap, C.slot, g);
+      if (atomicSub(&S.reads_h[g], 1) == 1 && g + BH < IC) issue_halos(S, C.ymap, C.zmap, g + BH);
+    }
   }
 }
 
@@ -305,13 +294,19 @@ __device__ __forceinline__ void task_u(Smem &S, ItemCtx const &C, int g, int w, 
 template <int SCHEME, typename T, int NW>
 __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__ const TileArgs A) {
   using namespace tile;
-  extern __shared__ unsigned char smem_raw[];
-  Smem &S = *reinterpret_cast<Smem *>((reinterpret_cast<size_t>(smem_raw) + 127) &
-                                      ~static_cast<size_t>(127));
+  // no static shared memory: the dynamic block starts the CTA's shared window,
+  // so it is aligned as declared (TMA destinations need 128 bytes); the cast
+  // keeps the shared state space, so the stencil reads are shared loads
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  Smem &S = *reinterpret_cast<Smem *>(smem_raw);
   int const tid = threadIdx.x, lane = tid & 31;
   int const per_step = A.nstages * A.nwork;
   int const total = per_step * A.nsteps;
   int *err = A.ctrl + 1;
+  if (smem_addr(smem_raw) & 127) {
+    if (tid == 0) atomicOr(err, 16);  // never issue a TMA to a misaligned buffer
+    return;
+  }
   bool bars_live = false;  // thread 0: the barriers hold an earlier item's phases
 
 #pragma unroll 1
@@ -421,10 +416,8 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
         Task const t = decode(pos);
         // a first stage whose dt turned out 0 keeps the bookkeeping, skips the work
         bool const compute = !*reinterpret_cast<int volatile *>(&S.skip);
-        if (t.type == T_FX) task_fx<SCHEME, T>(S, C, t.g, t.w, compute);
-        else if (t.type == T_FY) task_fyz<1, SCHEME, T>(S, C, t.g, t.w, compute);
-        else if (t.type == T_FZ) task_fyz<2, SCHEME, T>(S, C, t.g, t.w, compute);
-        else task_u(S, C, t.g, t.w, smax, bad);
+        if (t.type == T_U) task_u(S, C, t.g, t.w, smax, bad);
+        else task_face<SCHEME, T>(S, C, t, compute);
       }
       __syncthreads();
       if (C.reduce && !S.skip) {
@@ -483,7 +476,7 @@ namespace tile {
 template <int SCHEME, typename T, int NW>
 cudaError_t info_one(TileKernelInfo *out) {
   void const *fn = reinterpret_cast<void const *>(&tile_step_kernel<SCHEME, T, NW>);
-  size_t const smem = sizeof(Smem) + 128;
+  size_t const smem = sizeof(Smem);
   cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   int per_sm = 0;

@@ -66,6 +66,9 @@ def parse():
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving comparison and print its JSON")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--path", type=int, default=None,
+                   help="stepping candidate to use instead of the autotuner's choice "
+                        "(numbered as alp_engine_autotune; for profiling one path)")
     p.add_argument("--levels", action="store_true",
                    help="multi-level batching: 3-level spherical-shock hierarchy with local "
                         "time stepping (one line; steps are macro steps)")
@@ -174,14 +177,17 @@ def barrier(ws: int, dev=None):
 # ---------------------------------------------------------------------------
 
 def reference_cpu_sample(variant: str, budget_s: float, nthreads: int, steps: int | None = None,
-                         warmup: int = 0):
+                         warmup: int = 0, nblocks: int = 8):
     """Times the reference's compiled code (oracle/_ref; the restatement when the
-    reference was not built) on a 4x4x4-block periodic sample of the workload."""
+    reference was not built) on the bench workload itself: the periodic 8x8x8-
+    block (128^3-cell) Fourier + Mach-2 case, all blocks of every step (the
+    reference parallelises over blocks; here host threads over blocks). With
+    steps None, as many steps as fit in about budget_s seconds."""
     import oracle
     from alpaca_b200 import cases
     kind = "reference" if oracle.Reference.available(3, variant) else "port"
     impl = oracle.Reference(3, variant) if kind == "reference" else oracle.Restatement(3, variant)
-    case = cases.fourier_shock(4, dim=3, seed=1)
+    case = cases.fourier_shock(nblocks, dim=3, seed=1)
     g = case.grid
     u = case.u
     if warmup:
@@ -198,24 +204,27 @@ def reference_cpu_sample(variant: str, budget_s: float, nthreads: int, steps: in
              nthreads=nthreads)
     dt = time.perf_counter() - t0
     cells = g.nb * 4096
+    side = nblocks * 16
     return {"value": cells * steps / dt, "unit": METRIC, "cores": nthreads, "kind": kind,
-            "sample": f"{steps} SSP-RK3 steps of a 4x4x4-block (64^3-cell) periodic sample of the "
-                      f"same Fourier + Mach-2 workload, {variant}, FP64, {nthreads} threads",
-            "seconds": dt, "steps": steps}
+            "sample": f"{steps} SSP-RK3 steps of the {nblocks}x{nblocks}x{nblocks}-block "
+                      f"({side}^3-cell) periodic Fourier + Mach-2 workload, {variant}, FP64, "
+                      f"{nthreads} threads",
+            "seconds": dt, "steps": steps, "blocks": g.nb}
 
 
 def run_reference_arm(args, ws, rank):
     if rank != 0:
         return
     n = os.cpu_count() or 1
-    r = reference_cpu_sample(args.variant, 0.0, n, steps=args.steps, warmup=args.warmup)
+    r = reference_cpu_sample(args.variant, 0.0, n, steps=args.steps, warmup=args.warmup,
+                             nblocks=args.blocks)
     line = {"metric": METRIC, "value": r["value"], "unit": METRIC, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": r["seconds"] * 1e3 / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
-            "config": {"workload": "3d_periodic_fourier_mach2_128cubed_sample64cubed",
-                       "variant": args.variant, "blocks": 64, "cells": 64 ** 3},
+            "config": {"workload": "3d_periodic_fourier_mach2_128cubed", "variant": args.variant,
+                       "blocks": r["blocks"], "cells": r["blocks"] * 4096},
             "cpu_baseline": {k: r[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": r["value"], "unit": METRIC, "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
@@ -399,7 +408,11 @@ def run_ours(args, ws, rank, local):
     eng = api.Engine(3, args.variant, precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
     stream = torch.cuda.ExternalStream(eng.stream_handle)
     cid = eng.add_case(case, max_steps=0)
-    chosen, cand_ms = eng.autotune(trial_steps=3)
+    if args.path is None:
+        chosen, cand_ms = eng.autotune(trial_steps=3)
+    else:
+        eng.set_path(args.path)
+        chosen, cand_ms = args.path, None
     eng.step(args.warmup)
     torch.cuda.synchronize()
     barrier(ws, dev)
@@ -473,7 +486,7 @@ def run_ours(args, ws, rank, local):
                                                    "; the FP32-flux form runs part of them in FP32")}
     cpu = None
     if not args.no_cpu_baseline:
-        cpu = reference_cpu_sample(args.variant, 15.0, os.cpu_count() or 1)
+        cpu = reference_cpu_sample(args.variant, 15.0, os.cpu_count() or 1, nblocks=args.blocks)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     clk = clocks.summary()
     serv = None

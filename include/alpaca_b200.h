@@ -479,7 +479,8 @@ typedef struct {
   double step_set_cells;    /* cells stepped together under shortest_first (>= one case) */
   const char *abort_file;   /* null, or a path checked after every poll, as the reference
                                checks its ABORTFILE after each micro step
-                               (modular_algorithm_assembler.cpp:903-907): once the file
+                               (modular_algorithm_assembler.cpp:903-907), and while no case
+                               is resident (the loop waits for arrivals): once the file
                                exists, every request ends with status ALP_ABORTED (resident
                                cases with their state, time and steps so far, written to
                                h_result; the others with none) and alp_serve returns

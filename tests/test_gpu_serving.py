@@ -202,3 +202,21 @@ def test_abort_file_stops_serving_cleanly(cuda, tmp_path):
     done, _, _ = api.serve(reqs, 2 << 30, one_at_a_time=True, steps_per_poll=4,
                            abort_file=str(stop))
     assert all(x["status"] == 0 and x["steps"] == r.max_steps for x, r in zip(done, reqs))
+
+
+def test_abort_file_while_waiting_for_arrivals(cuda, tmp_path):
+    """With nothing resident the loop still checks its abort file: every
+    request arrives seconds after the start and the file exists from the
+    start, so alp_serve returns ALP_ABORTED at once, nothing admitted and no
+    step taken."""
+    import time
+    stop = tmp_path / "ABORTFILE"
+    stop.write_text("")
+    reqs = small_stream()
+    for r in reqs:
+        r.arrival_s = 5.0
+    t0 = time.perf_counter()
+    res, mk, _ = api.serve(reqs, 2 << 30, steps_per_poll=4, abort_file=str(stop))
+    assert time.perf_counter() - t0 < 3.0 and mk < 3.0
+    assert all(x["status"] == N.ALP_ABORTED and x["steps"] == 0 and x["t"] == 0.0 and
+               x["admitted_s"] < 0.0 for x in res)

@@ -3,9 +3,10 @@ launch per alp_engine_step call, every block's stage staged into shared memory
 by TMA, fluxes and stage update on chip) against the face-flux + stage-update
 path (candidate 0), through the C ABI.
 
-The two paths evaluate every face with the same face_compute and every cell
-with the same divergence and stage arithmetic, so the results must be equal
-bit for bit: state, time and step count. The face-flux path itself is checked
+The two paths evaluate every 3D face with the same face_compute (the x-face
+computation of the rotated stencil, canon_field) and every cell with the same
+divergence and stage arithmetic, so the results must be equal bit for bit:
+state, time and step count. The face-flux path itself is checked
 against the reference in test_gpu_parity.py (and, in the strict build, bit for
 bit), and the default 3D engine there now runs the tile path.
 """

@@ -175,10 +175,13 @@ int main(int argc, char **argv) {
       for (int l = 0; l < 32; ++l) {
         int const jk = t.w * 32 + l;
         double cons[6][NE];
-        gather_x(S, a, jk, cons);
+        gather_face(S, 0, a, jk, cons);
         for (int m = 0; m < 6; ++m)
-          for (int f = 0; f < NE; ++f)
-            check(cons[m][f] == expect(0, a - 3 + m, jk / IC, jk % IC, f), "x stencil", a, jk, m);
+          for (int c = 0; c < NE; ++c)
+            check(cons[m][c] == expect(0, a - 3 + m, jk / IC, jk % IC, canon_field(0, c)),
+                  "x stencil", a, jk, m);
+        FluxAt const o = flux_at(S, 0, a, jk);
+        check(o.base == &S.fx[a % RFX][0][jk] && o.stride == PLANE, "x flux slot", a, jk, 0);
         covered_x[a][jk]++;
         faces++;
       }
@@ -193,16 +196,21 @@ int main(int argc, char **argv) {
       for (int l = 0; l < 32; ++l) {
         int const q = t.w * 32 + l;
         if (q >= FACE_ROW * IC) continue;
-        int a, tt;
+        FaceAt const fa = face_at(dir, q);
+        int const a = fa.a, tt = fa.t;
         double cons[6][NE];
-        if (dir == 1) gather_yz<1>(S, g, q, a, tt, cons);
-        else gather_yz<2>(S, g, q, a, tt, cons);
+        gather_face(S, dir, g, q, cons);
         for (int m = 0; m < 6; ++m)
-          for (int f = 0; f < NE; ++f) {
-            // transverse indices: y faces (x = g, z = tt); z faces (x = g, y = tt)
-            double const e = expect(dir, a - 3 + m, g, tt, f);
-            check(cons[m][f] == e, dir == 1 ? "y stencil" : "z stencil", a, tt, m);
+          for (int c = 0; c < NE; ++c) {
+            // transverse indices: y faces (x = g, z = tt); z faces (x = g, y = tt);
+            // canonical slot c holds the rotated field
+            double const e = expect(dir, a - 3 + m, g, tt, canon_field(dir, c));
+            check(cons[m][c] == e, dir == 1 ? "y stencil" : "z stencil", a, tt, m);
           }
+        FluxAt const o = flux_at(S, dir, g, q);
+        check(dir == 1 ? (o.base == &S.fy[g % BYZ][0][a * IC + tt] && o.stride == FACE_ROW * IC)
+                       : (o.base == &S.fz[g % BYZ][0][tt * FACE_ROW + a] && o.stride == IC * FACE_ROW),
+              "yz flux slot", dir, q, g);
         if (dir == 1) covered_y[g][a * IC + tt]++;
         else covered_z[g][tt * FACE_ROW + a]++;
         faces++;

@@ -12,15 +12,17 @@
 // The item is a stream of warp tasks, taken by the CTA's warps in order:
 //   X0              x face 0 (8 tasks of 32 faces)
 //   for g = 0 .. 15:
+//     U(g - LAG)    flux divergence and stage update of plane g - LAG (8 tasks
+//                   of 32 cells), for g >= LAG
 //     FX(g)         x face g + 1 (8 tasks)
 //     FY(g), FZ(g)  the 17 x 16 y faces and 16 x 17 z faces of plane g (9 tasks
 //                   each, the last one half full)
-//     U(g - 1)      flux divergence and stage update of plane g - 1 (8 tasks of
-//                   32 cells), for g >= 1
-//   U(15)
-// Every task waits only for tasks earlier in the stream (shared-memory
-// counters) and for the loads those tasks released, so the warps never wait in
-// a cycle. Faces are numbered as in the reference's flux arrays: face a of a
+//   U(16 - LAG) .. U(15)
+// A plane's update trails its faces by LAG planes, so that the fluxes it reads
+// were computed a whole plane of tasks earlier, and the flux buffers it frees
+// are next written a plane of tasks later. Every task waits only for tasks
+// earlier in the stream (shared-memory counters) and for the loads those tasks
+// released, so the warps never wait in a cycle. Faces are numbered as in the reference's flux arrays: face a of a
 // direction lies between cells a - 1 and a (convective_term_solver.h:67-81).
 #pragma once
 
@@ -62,18 +64,18 @@ struct Src {
   bool own;     // true: the block's own cell `index` (0 .. 15)
   bool negate;  // mirror cell of a symmetry wall
 };
+// Written with selects only: the lanes of a warp hold faces at different
+// positions, and a branch here would split the warp for the whole face
+// computation that follows.
 __host__ __device__ inline Src stencil_src(int c, int nlo, int nhi) {
-  if (c < 0) {
-    if (nlo >= 0) return Src{c, false, false};
-    if (nlo == -1) return Src{0, true, false};
-    return Src{-1 - c, true, true};
-  }
-  if (c >= IC) {
-    if (nhi >= 0) return Src{c, false, false};
-    if (nhi == -1) return Src{IC - 1, true, false};
-    return Src{2 * IC - 1 - c, true, true};
-  }
-  return Src{c, true, false};
+  bool const lo = c < 0, out = lo || c >= IC;
+  int const n = lo ? nlo : nhi;
+  bool const wall = out && n < 0;
+  bool const sym = wall && n == -2;
+  int const mirror = lo ? -1 - c : 2 * IC - 1 - c;
+  int const clamp = lo ? 0 : IC - 1;
+  int const index = !wall ? c : (sym ? mirror : clamp);
+  return Src{index, !out || wall, sym};
 }
 
 // ---- the task stream ------------------------------------------------------
@@ -81,34 +83,34 @@ enum TaskType { T_FX = 0, T_FY = 1, T_FZ = 2, T_U = 3, T_NONE = 4 };
 constexpr int XT = PLANE / 32;                  // warp tasks of one x-face plane (8)
 constexpr int YT = (FACE_ROW * IC + 31) / 32;   // of the y faces of one plane (9)
 constexpr int UT = PLANE / 32;                  // of one plane's stage update (8)
-constexpr int ITER = XT + 2 * YT + UT;          // tasks of one plane g >= 1 (34)
-constexpr int STREAM = XT + (XT + 2 * YT) + (IC - 1) * ITER + UT;  // 552
+constexpr int FT = XT + 2 * YT;                  // face tasks of one plane (26)
+constexpr int ITER = FT + UT;                     // tasks of one plane g >= LAG (34)
+constexpr int LAG = 2;                            // planes between faces and update
+constexpr int STREAM = XT + LAG * FT + (IC - LAG) * ITER + LAG * UT;  // 552
 
 struct Task {
   int type;  // TaskType
   int g;     // FX: face g (0 .. 16); FY, FZ, U: plane g
   int w;     // task index within its kind (selects the 32 faces or cells)
 };
+// Face task r (0 .. FT - 1) of plane g.
+__host__ __device__ inline Task face_task(int g, int r) {
+  if (r < XT) return Task{T_FX, g + 1, r};
+  if (r < XT + YT) return Task{T_FY, g, r - XT};
+  return Task{T_FZ, g, r - XT - YT};
+}
 __host__ __device__ inline Task decode(int pos) {
   if (pos < XT) return Task{T_FX, 0, pos};
   pos -= XT;
-  int g, r;
-  if (pos < XT + 2 * YT) {
-    g = 0;
-    r = pos;
-  } else {
-    pos -= XT + 2 * YT;
-    if (pos >= (IC - 1) * ITER) {
-      pos -= (IC - 1) * ITER;
-      return pos < UT ? Task{T_U, IC - 1, pos} : Task{T_NONE, 0, 0};
-    }
-    g = 1 + pos / ITER;
-    r = pos % ITER;
+  if (pos < LAG * FT) return face_task(pos / FT, pos % FT);
+  pos -= LAG * FT;
+  if (pos < (IC - LAG) * ITER) {
+    int const g = LAG + pos / ITER, r = pos % ITER;
+    return r < UT ? Task{T_U, g - LAG, r} : face_task(g, r - UT);
   }
-  if (r < XT) return Task{T_FX, g + 1, r};
-  if (r < XT + YT) return Task{T_FY, g, r - XT};
-  if (r < XT + 2 * YT) return Task{T_FZ, g, r - XT - YT};
-  return Task{T_U, g - 1, r - XT - 2 * YT};
+  pos -= (IC - LAG) * ITER;
+  if (pos < LAG * UT) return Task{T_U, IC - LAG + pos / UT, pos % UT};
+  return Task{T_NONE, 0, 0};
 }
 
 // Reads of each x-plane (index q + 3) by the item's warp tasks, given the x
@@ -212,25 +214,26 @@ __host__ __device__ inline void gather_face(Smem const &S, int dir, int g, int q
             o4 = canon_field(dir, MOMX + 2);
   double const *plane = &S.ring[ring_slot(g)][0][0];
   int const hb = g % BH;
+  // base and field stride of the halo buffers of the face's direction; the
+  // cell offsets below are chosen with selects (the lanes' faces differ, a
+  // branch would split the warp)
+  double const *lo_buf = dir == 1 ? &S.yh[hb][0][0][0] : &S.zh[hb][0][0][0];
+  double const *hi_buf = dir == 1 ? &S.yh[hb][1][0][0] : &S.zh[hb][1][0][0];
+  int const hfs = dir == 1 ? YROW : ZCOL;
 #pragma unroll
   for (int m = 0; m < 6; ++m) {
     Src const s = stencil_src(a - 3 + m, nlo, nhi);
     double const *src;
     int fs;
-    if (dir == 0) {
+    if (dir == 0) {  // uniform over the warp
       src = &S.ring[ring_slot(s.index)][0][f.t];
       fs = PLANE;
-    } else if (s.own) {
-      src = dir == 1 ? plane + s.index * IC + f.t : plane + f.t * IC + s.index;
-      fs = PLANE;
-    } else if (dir == 1) {
-      src = s.index < 0 ? &S.yh[hb][0][0][(s.index + 3) * IC + f.t]
-                        : &S.yh[hb][1][0][(s.index - IC) * IC + f.t];
-      fs = YROW;
     } else {
-      src = s.index < 0 ? &S.zh[hb][0][0][f.t * 4 + s.index + 4]
-                        : &S.zh[hb][1][0][f.t * 4 + s.index - IC];
-      fs = ZCOL;
+      int const own_off = dir == 1 ? s.index * IC + f.t : f.t * IC + s.index;
+      int const lo_off = dir == 1 ? (s.index + 3) * IC + f.t : f.t * 4 + s.index + 4;
+      int const hi_off = dir == 1 ? (s.index - IC) * IC + f.t : f.t * 4 + s.index - IC;
+      src = s.own ? plane + own_off : (s.index < 0 ? lo_buf + lo_off : hi_buf + hi_off);
+      fs = s.own ? PLANE : hfs;
     }
     cons[m][MASS] = src[MASS * fs];
     cons[m][ENERGY] = src[ENERGY * fs];

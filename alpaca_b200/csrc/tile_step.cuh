@@ -67,19 +67,15 @@ __device__ __forceinline__ bool mbar_try(unsigned long long *b) {
       : "memory");
   return ok != 0;
 }
+// Every wait below is executed by all lanes of a warp and decided with
+// __all_sync / __any_sync, so that a warp never splits around a wait: a split
+// warp would run the face arithmetic that follows in two partial passes.
+constexpr unsigned kFull = 0xffffffffu;
+
 // Set once any wait of the launch ran out: every other wait then returns at
 // once, so a failed launch ends within about one wait's bound.
 __device__ __forceinline__ bool failed(int const *err) {
-  return *reinterpret_cast<int const volatile *>(err) != 0;
-}
-// Bounded wait for the (single) load phase of a barrier (each try_wait
-// suspends for a while itself); on running out sets err bit 2 and returns.
-__device__ __forceinline__ void mbar_wait(unsigned long long *b, int *err) {
-  for (int i = 0; i < (1 << 21); ++i) {
-    if (mbar_try(b)) return;
-    if ((i & 255) == 255 && failed(err)) return;
-  }
-  atomicOr(err, 2);
+  return __any_sync(kFull, *reinterpret_cast<int const volatile *>(err) != 0);
 }
 // TMA tile load of a 5D box into shared memory, completion on mbarrier b.
 __device__ __forceinline__ void tma_load(void *dst, CUtensorMap const *map, int k, int j, int i,
@@ -99,32 +95,18 @@ __device__ __forceinline__ int ld_acquire(int const *p) {
 __device__ __forceinline__ void st_release(int *p, int v) {
   asm volatile("st.release.gpu.global.b32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
-// Bounded spin until *p >= v (global, another CTA's release); on running out
-// sets err bit `code` and returns.
+// Bounded spin of a warp until *p >= v (global, another CTA's release); on
+// running out sets err bit `code` and returns.
 __device__ __forceinline__ void spin_ge(int const *p, int v, int *err, int code) {
   unsigned ns = 32;
   for (int i = 0; i < (1 << 22); ++i) {
-    if (ld_acquire(p) >= v) return;
+    if (__all_sync(kFull, ld_acquire(p) >= v)) return;
     if (failed(err)) return;
     __nanosleep(ns);
     if (ns < 256) ns <<= 1;
   }
-  atomicOr(err, code);
+  if ((threadIdx.x & 31) == 0) atomicOr(err, code);
 }
-// Bounded spin until the shared-memory counter *p >= v (lane 0 of a warp);
-// the fence orders the caller's following reads after the writers' data.
-__device__ __forceinline__ void smem_wait_ge(int const *p, int v, int *err) {
-  for (int i = 0; i < (1 << 24); ++i) {
-    if (*reinterpret_cast<int const volatile *>(p) >= v) {
-      __threadfence_block();
-      return;
-    }
-    if ((i & 255) == 255 && failed(err)) return;
-    __nanosleep(20);
-  }
-  atomicOr(err, 8);
-}
-
 // ---- loads ---------------------------------------------------------------
 constexpr unsigned kPlaneBytes = NE * PLANE * sizeof(double);
 constexpr unsigned kYBytes = NE * YROW * sizeof(double);
@@ -163,15 +145,6 @@ __device__ __forceinline__ void issue_u0(Smem &S, CUtensorMap const *map, int sl
   tma_load(&S.u0[g % BU][0][0], map, HS, HS, HS + g, 0, slot, &S.bar_u0[g]);
 }
 
-// A read of plane q finished (lane 0): the last one hands the ring slot to the
-// slot's next loaded plane.
-__device__ __forceinline__ void release_plane(Smem &S, CUtensorMap const *map, int slot, int q) {
-  if (atomicSub(&S.reads[q + 3], 1) == 1) {
-    int const n = next_plane_of_slot(q, S.reads0);
-    if (n != 99) issue_plane(S, map, slot, n);
-  }
-}
-
 // ---- tasks -----------------------------------------------------------------
 struct ItemCtx {
   CUtensorMap const *pmap, *ymap, *zmap, *u0map;
@@ -185,10 +158,30 @@ struct ItemCtx {
   double const *dt_case;
 };
 
+// Warp wait until ready() holds on every lane (each lane tests its own
+// condition: a counter, a load barrier, or nothing); on success the lane that
+// saw a condition acquires it (fence) and the warp barrier passes that on to
+// every lane. Bounded: on running out sets err bit `code` and returns.
+template <class Ready>
+__device__ __forceinline__ void wait_until(Ready ready, int *err, int code) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (__all_sync(kFull, ready())) {
+      __threadfence_block();
+      __syncwarp();
+      return;
+    }
+    if ((i & 255) == 255 && failed(err)) return;
+    __nanosleep(20);
+  }
+  if ((threadIdx.x & 31) == 0) atomicOr(err, code);
+}
+__device__ __forceinline__ int vol(int const &x) { return *reinterpret_cast<int const volatile *>(&x); }
+
 // A face task: 32 faces of x face plane g (FX) or of plane g's y / z faces
-// (FY, FZ). Lane 0 waits until the buffers the task writes are free and the
+// (FY, FZ). The warp waits until the buffers the task writes are free and the
 // planes it reads have arrived, and afterwards counts the task done and
-// releases its reads. Every direction goes through the one face_compute<3, 0>
+// releases its reads; the waits and the bookkeeping atomics run on separate
+// lanes side by side. Every direction goes through the one face_compute<3, 0>
 // of the rotated stencil (gather_face), so the SM runs one copy of the face
 // arithmetic.
 template <int SCHEME, typename T>
@@ -196,22 +189,30 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
   int const lane = threadIdx.x & 31;
   int const dir = t.type;  // T_FX, T_FY, T_FZ are 0, 1, 2
   int const g = t.g;
-  if (lane == 0) {
-    if (dir == 0) {
-      // the flux slot of face g held face g - RFX, read by the updates of
-      // planes g - RFX - 1 and g - RFX
-      if (g > RFX) smem_wait_ge(&S.cnt_u[g - RFX - 1], UT, C.err);
-      if (g >= RFX) smem_wait_ge(&S.cnt_u[g - RFX], UT, C.err);
-      for (int m = 0; m < 6; ++m)
-        mbar_wait(&S.bar_plane[stencil_src(g - 3 + m, S.nbr[0], S.nbr[1]).index + 3], C.err);
-    } else {
-      // the flux buffer held plane g - BYZ, read by its stage update
-      if (g >= BYZ) smem_wait_ge(&S.cnt_u[g - BYZ], UT, C.err);
-      mbar_wait(&S.bar_plane[g + 3], C.err);
-      mbar_wait(&S.bar_halo[g], C.err);
-    }
+  if (dir == 0) {
+    // the flux slot of face g held face g - RFX, read by the updates of
+    // planes g - RFX - 1 and g - RFX; lanes 2..7 wait for the six stencil
+    // planes
+    int const nlo = S.nbr[0], nhi = S.nbr[1];
+    wait_until(
+        [&] {
+          if (lane == 0) return g <= RFX || vol(S.cnt_u[g - RFX - 1]) >= UT;
+          if (lane == 1) return g < RFX || vol(S.cnt_u[g - RFX]) >= UT;
+          if (lane < 8) return mbar_try(&S.bar_plane[stencil_src(g - 5 + lane, nlo, nhi).index + 3]);
+          return true;
+        },
+        C.err, 2);
+  } else {
+    // the flux buffer held plane g - BYZ, read by its stage update
+    wait_until(
+        [&] {
+          if (lane == 0) return g < BYZ || vol(S.cnt_u[g - BYZ]) >= UT;
+          if (lane == 1) return mbar_try(&S.bar_plane[g + 3]);
+          if (lane == 2) return mbar_try(&S.bar_halo[g]);
+          return true;
+        },
+        C.err, 2);
   }
-  __syncwarp();
   int const q = t.w * 32 + lane;
   if (compute && (dir == 0 || q < FACE_ROW * IC)) {
     double cons[6][NE];
@@ -223,18 +224,31 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
     for (int c = 0; c < NE; ++c) o.base[canon_field(dir, c) * o.stride] = valid ? fd[c] : 0.0;
   }
   __syncwarp();
-  if (lane == 0) {
-    __threadfence_block();
-    if (dir == 0) {
+  __threadfence_block();
+  if (dir == 0) {
+    // lane 0 counts the task, lanes 1..6 release the six stencil planes
+    if (lane == 0) {
       atomicAdd(&S.cnt_x[g], 1);
-      for (int m = 0; m < 6; ++m)
-        release_plane(S, C.pmap, C.slot, stencil_src(g - 3 + m, S.nbr[0], S.nbr[1]).index);
-    } else {
+    } else if (lane < 7) {
+      int const pq = stencil_src(g - 4 + lane, S.nbr[0], S.nbr[1]).index;
+      if (atomicSub(&S.reads[pq + 3], 1) == 1) {
+        int const n = next_plane_of_slot(pq, S.reads0);
+        if (n != 99) issue_plane(S, C.pmap, C.slot, n);
+      }
+    }
+  } else {
+    if (lane == 0) {
       atomicAdd(&S.cnt_yz[g], 1);
-      release_plane(S, C.pmap, C.slot, g);
+    } else if (lane == 1) {
+      if (atomicSub(&S.reads[g + 3], 1) == 1) {
+        int const n = next_plane_of_slot(g, S.reads0);
+        if (n != 99) issue_plane(S, C.pmap, C.slot, n);
+      }
+    } else if (lane == 2) {
       if (atomicSub(&S.reads_h[g], 1) == 1 && g + BH < IC) issue_halos(S, C.ymap, C.zmap, g + BH);
     }
   }
+  __syncwarp();
 }
 
 // Stage update of 32 cells of plane g: flux divergence and RK stage into the
@@ -242,23 +256,27 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
 __device__ __forceinline__ void task_u(Smem &S, ItemCtx const &C, int g, int w, double &smax,
                                        int &bad) {
   int const lane = threadIdx.x & 31;
-  if (lane == 0) {
-    smem_wait_ge(&S.cnt_x[g], XT, C.err);
-    smem_wait_ge(&S.cnt_x[g + 1], XT, C.err);
-    smem_wait_ge(&S.cnt_yz[g], 2 * YT, C.err);
-    if (!C.first) mbar_wait(&S.bar_u0[g], C.err);
-    if (!*reinterpret_cast<int volatile *>(&S.dt_ready)) {
-      // a first stage computes its fluxes ahead of the step's dt
-      spin_ge(C.dtflag_case, C.step + 1, C.err, 4);
-      double const dt = *reinterpret_cast<double const volatile *>(C.dt_case);
-      *reinterpret_cast<double volatile *>(&S.dt) = dt;
-      *reinterpret_cast<int volatile *>(&S.skip) = dt == 0.0;
-      __threadfence_block();
-      *reinterpret_cast<int volatile *>(&S.dt_ready) = 1;
-    }
+  bool const first = C.first;
+  wait_until(
+      [&] {
+        if (lane == 0) return vol(S.cnt_x[g]) >= XT;
+        if (lane == 1) return vol(S.cnt_x[g + 1]) >= XT;
+        if (lane == 2) return vol(S.cnt_yz[g]) >= 2 * YT;
+        if (lane == 3) return first || mbar_try(&S.bar_u0[g]);
+        return true;
+      },
+      C.err, 8);
+  if (!__all_sync(kFull, vol(S.dt_ready) != 0)) {
+    // a first stage computes its fluxes ahead of the step's dt; every lane
+    // reads and stores the same values
+    spin_ge(C.dtflag_case, C.step + 1, C.err, 4);
+    double const dt = *reinterpret_cast<double const volatile *>(C.dt_case);
+    *reinterpret_cast<double volatile *>(&S.dt) = dt;
+    *reinterpret_cast<int volatile *>(&S.skip) = dt == 0.0;
+    __threadfence_block();
+    *reinterpret_cast<int volatile *>(&S.dt_ready) = 1;
   }
-  __syncwarp();
-  if (!*reinterpret_cast<int volatile *>(&S.skip)) {
+  if (!__any_sync(kFull, vol(S.skip) != 0)) {
     RkStage const rk = rk_stage(C.stage, *reinterpret_cast<double volatile *>(&S.dt));
     int const jk = w * 32 + lane, j = jk / IC, k = jk % IC;
     double const *uin = &S.ring[ring_slot(g)][0][jk];
@@ -272,20 +290,26 @@ __device__ __forceinline__ void task_u(Smem &S, ItemCtx const &C, int g, int w, 
                                    S.fy[by][f][j * IC + k], S.fy[by][f][(j + 1) * IC + k],
                                    S.fz[by][f][j * FACE_ROW + k], S.fz[by][f][j * FACE_ROW + k + 1],
                                    C.ocs);
-      double const v = rk_apply(rk, uin[f * PLANE], C.first ? 0.0 : S.u0[g % BU][f][jk], rhs);
+      double const v = rk_apply(rk, uin[f * PLANE], first ? 0.0 : S.u0[g % BU][f][jk], rhs);
       out[(size_t)f * Geo<3>::CELLS] = v;
       c[f] = v;
     }
     if (C.reduce) smax = dmax(smax, cell_signal_speed<3>(C.eos, c, bad));
   }
   __syncwarp();
+  __threadfence_block();
+  // lane 0 counts the task, lane 1 releases the plane, lane 2 the U0 plane
   if (lane == 0) {
-    __threadfence_block();
     atomicAdd(&S.cnt_u[g], 1);
-    release_plane(S, C.pmap, C.slot, g);
-    if (!C.first && atomicSub(&S.reads_u[g], 1) == 1 && g + BU < IC)
-      issue_u0(S, C.u0map, C.slot, g + BU);
+  } else if (lane == 1) {
+    if (atomicSub(&S.reads[g + 3], 1) == 1) {
+      int const n = next_plane_of_slot(g, S.reads0);
+      if (n != 99) issue_plane(S, C.pmap, C.slot, n);
+    }
+  } else if (lane == 2 && !first) {
+    if (atomicSub(&S.reads_u[g], 1) == 1 && g + BU < IC) issue_u0(S, C.u0map, C.slot, g + BU);
   }
+  __syncwarp();
 }
 
 }  // namespace tile
@@ -311,7 +335,10 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
 
 #pragma unroll 1
   for (;;) {
-    if (tid == 0) S.item = failed(err) ? total : atomicAdd(A.ctrl, 1);
+    if (tid < 32) {
+      bool const f = failed(err);
+      if (tid == 0) S.item = f ? total : atomicAdd(A.ctrl, 1);
+    }
     __syncthreads();
     int const item = S.item;
     if (item >= total) break;
@@ -330,14 +357,20 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
     int const cid = bm.case_id;
     bool const first = rk_first_stage(stage);
 
+    if (tid < 32) {
+      // the inputs of this stage are final once the block and its face
+      // neighbours finished the previous one (warp 0 waits)
+      int const *nb = A.nbr26 + (size_t)slot * 26;
+      spin_ge(A.done + slot, need, err, 1);
+#pragma unroll 1
+      for (int d = 0; d < 6; ++d) {
+        int const n = nb[face_slot(d)];
+        if (n >= 0) spin_ge(A.done + n, need, err, 1);
+      }
+    }
     if (tid == 0) {
       int const *nb = A.nbr26 + (size_t)slot * 26;
       for (int d = 0; d < 6; ++d) S.nbr[d] = nb[face_slot(d)];
-      // the inputs of this stage are final once the block and its face
-      // neighbours finished the previous one
-      spin_ge(A.done + slot, need, err, 1);
-      for (int d = 0; d < 6; ++d)
-        if (S.nbr[d] >= 0) spin_ge(A.done + S.nbr[d], need, err, 1);
       // dt of this step: final for later stages; for a first stage only once
       // the previous step's last blocks of the case committed
       int const ready = s > 0 || ld_acquire(A.dtflag + cid) >= step + 1;
@@ -386,6 +419,7 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
       }
     }
     __syncthreads();
+    __syncwarp();
 
     if (!S.skip) {
       ItemCtx C;
@@ -407,24 +441,29 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
       C.dt_case = &A.cases[cid].dt;
       double smax = 0.0;
       int bad = 0;
+      // a warp claims its next task when it starts one (the claim's latency
+      // hides behind the task); tasks still only wait on earlier positions, and
+      // the earliest unfinished one is always some warp's current task
+      int pos = 0;
+      if (lane == 0) pos = atomicAdd(&S.next_task, 1);
+      pos = __shfl_sync(kFull, pos, 0);
 #pragma unroll 1
-      for (;;) {
-        int pos = 0;
-        if (lane == 0) pos = atomicAdd(&S.next_task, 1);
-        pos = __shfl_sync(0xffffffffu, pos, 0);
-        if (pos >= STREAM) break;
+      while (pos < STREAM) {
+        int claim = 0;
+        if (lane == 0) claim = atomicAdd(&S.next_task, 1);
         Task const t = decode(pos);
         // a first stage whose dt turned out 0 keeps the bookkeeping, skips the work
         bool const compute = !*reinterpret_cast<int volatile *>(&S.skip);
         if (t.type == T_U) task_u(S, C, t.g, t.w, smax, bad);
-        else task_face<SCHEME, T>(S, C, t, compute);
+        else if (t.type != T_NONE) task_face<SCHEME, T>(S, C, t, compute);
+        pos = __shfl_sync(kFull, claim, 0);
       }
       __syncthreads();
       if (C.reduce && !S.skip) {
         // block maximum of the signal speed (non-negative doubles order like
         // their bit patterns) and the bad-cell flag
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) smax = dmax(smax, __shfl_xor_sync(0xffffffffu, smax, o));
+        for (int o = 16; o > 0; o >>= 1) smax = dmax(smax, __shfl_xor_sync(kFull, smax, o));
         if (lane == 0) S.red[tid >> 5] = smax;
         if (__syncthreads_or(bad) && tid == 0) S.bad = 1;
         if (tid == 0) {

@@ -204,7 +204,8 @@ class Engine:
         return {"dim": info.dim, "steps": info.steps, "max_steps": info.max_steps, "t": info.t,
                 "t_end": info.t_end, "cfl": info.cfl, "cell_size": info.cell_size,
                 "gamma": info.material.gamma, "background_pressure": info.material.background_pressure,
-                "safe": info.material.safe, "nbr26": nbr, "blocks": u}
+                "safe": info.material.safe, "scheme": scheme_fields(info.scheme),
+                "nbr26": nbr, "blocks": u}
 
     def restore(self, ck: dict) -> int:
         """Adds the case a checkpoint describes; it continues where it stopped."""
@@ -214,7 +215,8 @@ class Engine:
                                 float(ck["t"]), float(ck["t_end"]), float(ck["cfl"]),
                                 float(ck["cell_size"]),
                                 N.Material.make(float(ck["gamma"]), float(ck["background_pressure"]),
-                                                bool(ck["safe"])))
+                                                bool(ck["safe"])),
+                                N.Scheme(*[int(v) for v in ck["scheme"]]))
         cid = C.c_int()
         self._check(self.lib.alp_engine_restore_case(
             self.h, C.byref(info), nbr.ctypes.data_as(C.POINTER(C.c_int)),
@@ -462,6 +464,11 @@ _CASE_KEYS = ("steps", "max_steps", "t_end", "cfl", "cell_size", "gamma", "backg
               "safe")
 
 
+def scheme_fields(s) -> np.ndarray:
+    """The alp_scheme fields in declaration order (int32[8])."""
+    return np.array([getattr(s, f) for f, _ in N.Scheme._fields_], dtype=np.int32)
+
+
 def save_checkpoint(path: str, ck: dict) -> None:
     """Writes one case checkpoint (Engine.checkpoint) to path (.npz)."""
     out = {"simulation_data/Time": np.float64(ck["t"]),
@@ -470,7 +477,8 @@ def save_checkpoint(path: str, ck: dict) -> None:
            "simulation_data/HaloSize": np.uint32(4),
            "simulation_data/MaximumLevel": np.uint32(0),
            "node_cell_data/Conservatives": np.ascontiguousarray(ck["blocks"], dtype=np.float64),
-           "case/Neighbours": np.ascontiguousarray(ck["nbr26"], dtype=np.int32)}
+           "case/Neighbours": np.ascontiguousarray(ck["nbr26"], dtype=np.int32),
+           "case/Scheme": np.asarray(ck["scheme"], dtype=np.int32)}
     for k in _CASE_KEYS:
         out["case/" + k] = np.asarray(ck[k])
     with open(path, "wb") as f:
@@ -485,6 +493,9 @@ def load_checkpoint(path: str) -> dict:
         ck = {"t": float(z["simulation_data/Time"]), "dim": int(z["simulation_data/Dimensions"]),
               "blocks": z["node_cell_data/Conservatives"].copy(),
               "nbr26": z["case/Neighbours"].copy()}
+        if "case/Scheme" not in z:
+            raise ValueError("checkpoint without its scheme selection")
+        ck["scheme"] = z["case/Scheme"].copy()
         for k in _CASE_KEYS:
             v = z["case/" + k]
             ck[k] = v.item()

@@ -395,6 +395,7 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   e->dim = dim;
   e->scheme = sid;
   e->precision = prec;
+  e->selection = *scheme;
   e->opt = scheme_options(scheme);
   e->rk2 = scheme->time_integrator == ALP_RK2;
   e->capacity = capacity_blocks;
@@ -638,6 +639,7 @@ int alp_engine_checkpoint_case(alp_engine *e, int case_id, alp_case_checkpoint *
   info->cfl = cs.cfl;
   info->cell_size = c.cell_size;
   info->material = c.mat;
+  info->scheme = e->selection;
   if (h_nbr26)
     for (size_t i = 0; i < (size_t)c.nb * 26; ++i) {
       int const n = e->h_nbr26[(size_t)c.first * 26 + i];
@@ -651,6 +653,19 @@ int alp_engine_restore_case(alp_engine *e, const alp_case_checkpoint *info, cons
   if (!e || !info || !case_id) return fail(ALP_ERR_INVALID, "null argument");
   if (info->dim != e->dim) return fail(ALP_ERR_INVALID, "checkpoint of another dimension");
   if (info->steps < 0) return fail(ALP_ERR_INVALID, "negative step count");
+  {
+    alp_scheme const &a = info->scheme, &b = e->selection;
+    if (a.convective_term_solver != b.convective_term_solver ||
+        a.state_reconstruction != b.state_reconstruction ||
+        a.reconstruction_stencil != b.reconstruction_stencil ||
+        a.riemann_solver != b.riemann_solver || a.signal_speed != b.signal_speed ||
+        a.flux_splitting != b.flux_splitting || a.time_integrator != b.time_integrator ||
+        a.precision != b.precision)
+      return fail(ALP_ERR_INVALID,
+                  "checkpoint of another scheme selection (solver, reconstruction, stencil, "
+                  "Riemann solver, signal speed, splitting, time integrator or precision "
+                  "differs from the engine's)");
+  }
   int cid;
   if (int rc = alp_engine_add_case(e, &info->material, info->cell_size, info->cfl, info->t,
                                    info->t_end, info->max_steps, info->nb, h_nbr26, h_blocks,

@@ -41,6 +41,7 @@ using alp::launch_step_commit;
 // a case is exported.
 struct alp_engine {
   int dim = 3, scheme = FV_CHAR, precision = FP64;
+  alp_scheme selection{};  // the selection the engine was created with
   alp::SchemeOptions opt;  // run-time selected schemes (face-flux path only)
   int rk2 = 0;             // 1: TVD-RK2 (2 stages, face-flux paths), 0: SSP-RK3
   int capacity = 0, max_cases = 0;

@@ -15,7 +15,6 @@
 // its own and costs nothing until the first call asks for its address.
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 #include "../../include/alpaca_b200.h"
@@ -23,6 +22,8 @@
 namespace alp {
 int fail(int code, std::string const &msg);
 int cuda_fail(cudaError_t e, char const *where);
+int scheme_id(alp_scheme const *s, int *id, int *precision);
+int check_material(alp_material const *m);
 }  // namespace alp
 
 namespace {
@@ -32,28 +33,16 @@ namespace {
 constexpr size_t kStaticScratchBytes = size_t(16) << 20;
 static __device__ __align__(256) double g_space_rhs_scratch[kStaticScratchBytes / sizeof(double)];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void *g_scratch_ptr[kMaxDevices] = {};
-
-// Address of the array in the current device's context, looked up once per
-// device (cudaGetSymbolAddress may load the module, so it is done before the
-// first use, not per call).
+// Address of the array in the current device's context. It is looked up on
+// every call (a symbol lookup in the loaded module, no allocation once the
+// module is loaded): after cudaDeviceReset the next context loads the module
+// again, possibly at another address, so an address kept from an earlier call
+// could be stale.
 int scratch_of_current_device(void **out) {
-  int dev = 0;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return alp::cuda_fail(e, "cudaGetDevice");
-  if (dev < 0 || dev >= kMaxDevices)
-    return alp::fail(ALP_ERR_INVALID, "alp_space_rhs_static: device ordinal " +
-                                          std::to_string(dev) + " is beyond 63");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_ptr[dev]) {
-    void *p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_space_rhs_scratch);
-    if (e != cudaSuccess) return alp::cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
-    g_scratch_ptr[dev] = p;
-  }
-  *out = g_scratch_ptr[dev];
+  void *p = nullptr;
+  cudaError_t const e = cudaGetSymbolAddress(&p, g_space_rhs_scratch);
+  if (e != cudaSuccess) return alp::cuda_fail(e, "cudaGetSymbolAddress(static scratch)");
+  *out = p;
   return ALP_OK;
 }
 
@@ -64,7 +53,12 @@ extern "C" {
 int alp_space_rhs_static(int dim, const alp_scheme *scheme, const alp_material *mat,
                          const double *d_blocks, int nb, double cell_size, double *d_rhs,
                          alp_stream_t stream) {
+  // the argument checks of alp_space_rhs come first, in its order, so a bad
+  // call returns the same code from both entry points
   if (dim < 1 || dim > 3) return alp::fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
+  int sid, prec;
+  if (int rc = alp::scheme_id(scheme, &sid, &prec)) return rc;
+  if (int rc = alp::check_material(mat)) return rc;
   size_t const need = alp_space_rhs_workspace_size(dim, nb);
   if (nb > 0 && need > kStaticScratchBytes) {
     size_t const per_block = alp_space_rhs_workspace_size(dim, 1);

@@ -21,9 +21,10 @@
 // A plane's update trails its faces by LAG planes, so that the fluxes it reads
 // were computed a whole plane of tasks earlier, and the flux buffers it frees
 // are next written a plane of tasks later. Every task waits only for tasks
-// earlier in the stream (shared-memory counters) and for the loads those tasks
-// released, so the warps never wait in a cycle. Faces are numbered as in the reference's flux arrays: face a of a
-// direction lies between cells a - 1 and a (convective_term_solver.h:67-81).
+// earlier in the stream (arrivals on shared-memory mbarriers) and for the
+// loads those tasks released, so the warps never wait in a cycle. Faces are
+// numbered as in the reference's flux arrays: face a of a direction lies
+// between cells a - 1 and a (convective_term_solver.h:67-81).
 #pragma once
 
 #include "layout.cuh"
@@ -171,16 +172,19 @@ struct Smem {
   double yh[BH][2][NE][YROW];         // [buffer][low / high side]
   double zh[BH][2][NE][ZCOL];
   double u0[BU][NE][PLANE];
-  unsigned long long bar_plane[NPLANES];  // one load per plane and item
+  // mbarriers, one phase per item: the loads (TMA transaction bytes) and the
+  // finished tasks of each x face (XT arrivals), of each plane's y and z faces
+  // (2 YT) and of each plane's stage update (UT)
+  unsigned long long bar_plane[NPLANES];
   unsigned long long bar_halo[IC];
   unsigned long long bar_u0[IC];
+  unsigned long long bar_x[IC + 1];
+  unsigned long long bar_yz[IC];
+  unsigned long long bar_u[IC];
   int reads[NPLANES];   // outstanding reads of each x-plane
   int reads0[NPLANES];  // reads at the item's start
   int reads_h[IC];      // outstanding reads of each plane's y / z halos
   int reads_u[IC];      // outstanding reads of each U0 plane
-  int cnt_x[IC + 1];    // finished tasks of each x face
-  int cnt_yz[IC];       // finished y and z face tasks of each plane
-  int cnt_u[IC];        // finished stage-update tasks of each plane
   int next_task;
   int item, skip, bad, dt_ready;
   int nbr[6];

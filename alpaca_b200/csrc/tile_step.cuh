@@ -14,7 +14,7 @@
 //      (32 faces through face_compute, the per-face arithmetic of the face-flux
 //      kernels, into shared-memory flux planes) and stage-update tasks (32 cells:
 //      flux_divergence and rk_apply, the arithmetic of stage_update_kernel,
-//      written to the stage output) in order; shared-memory counters order a
+//      written to the stage output) in order; shared-memory mbarriers order a
 //      task after the tasks it reads from, and a plane's last reader issues the
 //      load that reuses its buffer. The last stage also reduces the cells' signal
 //      speed for the next step's dt;
@@ -46,8 +46,13 @@ namespace tile {
 __device__ __forceinline__ unsigned smem_addr(void const *p) {
   return (unsigned)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ void mbar_init(unsigned long long *b) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(1) : "memory");
+__device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count = 1) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(b)), "r"(count) : "memory");
+}
+// One arrival (release at CTA scope: the arriving thread's earlier writes, and
+// those its warp barrier ordered before them, are visible to the waiters).
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(b)) : "memory");
 }
 __device__ __forceinline__ void mbar_inval(unsigned long long *b) {
   asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(b)) : "memory");
@@ -196,8 +201,8 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
     int const nlo = S.nbr[0], nhi = S.nbr[1];
     wait_until(
         [&] {
-          if (lane == 0) return g <= RFX || vol(S.cnt_u[g - RFX - 1]) >= UT;
-          if (lane == 1) return g < RFX || vol(S.cnt_u[g - RFX]) >= UT;
+          if (lane == 0) return g <= RFX || mbar_try(&S.bar_u[g - RFX - 1]);
+          if (lane == 1) return g < RFX || mbar_try(&S.bar_u[g - RFX]);
           if (lane < 8) return mbar_try(&S.bar_plane[stencil_src(g - 5 + lane, nlo, nhi).index + 3]);
           return true;
         },
@@ -206,7 +211,7 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
     // the flux buffer held plane g - BYZ, read by its stage update
     wait_until(
         [&] {
-          if (lane == 0) return g < BYZ || vol(S.cnt_u[g - BYZ]) >= UT;
+          if (lane == 0) return g < BYZ || mbar_try(&S.bar_u[g - BYZ]);
           if (lane == 1) return mbar_try(&S.bar_plane[g + 3]);
           if (lane == 2) return mbar_try(&S.bar_halo[g]);
           return true;
@@ -228,7 +233,7 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
   if (dir == 0) {
     // lane 0 counts the task, lanes 1..6 release the six stencil planes
     if (lane == 0) {
-      atomicAdd(&S.cnt_x[g], 1);
+      mbar_arrive(&S.bar_x[g]);
     } else if (lane < 7) {
       int const pq = stencil_src(g - 4 + lane, S.nbr[0], S.nbr[1]).index;
       if (atomicSub(&S.reads[pq + 3], 1) == 1) {
@@ -238,7 +243,7 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
     }
   } else {
     if (lane == 0) {
-      atomicAdd(&S.cnt_yz[g], 1);
+      mbar_arrive(&S.bar_yz[g]);
     } else if (lane == 1) {
       if (atomicSub(&S.reads[g + 3], 1) == 1) {
         int const n = next_plane_of_slot(g, S.reads0);
@@ -259,9 +264,9 @@ __device__ __forceinline__ void task_u(Smem &S, ItemCtx const &C, int g, int w, 
   bool const first = C.first;
   wait_until(
       [&] {
-        if (lane == 0) return vol(S.cnt_x[g]) >= XT;
-        if (lane == 1) return vol(S.cnt_x[g + 1]) >= XT;
-        if (lane == 2) return vol(S.cnt_yz[g]) >= 2 * YT;
+        if (lane == 0) return mbar_try(&S.bar_x[g]);
+        if (lane == 1) return mbar_try(&S.bar_x[g + 1]);
+        if (lane == 2) return mbar_try(&S.bar_yz[g]);
         if (lane == 3) return first || mbar_try(&S.bar_u0[g]);
         return true;
       },
@@ -300,7 +305,7 @@ __device__ __forceinline__ void task_u(Smem &S, ItemCtx const &C, int g, int w, 
   __threadfence_block();
   // lane 0 counts the task, lane 1 releases the plane, lane 2 the U0 plane
   if (lane == 0) {
-    atomicAdd(&S.cnt_u[g], 1);
+    mbar_arrive(&S.bar_u[g]);
   } else if (lane == 1) {
     if (atomicSub(&S.reads[g + 3], 1) == 1) {
       int const n = next_plane_of_slot(g, S.reads0);
@@ -386,22 +391,29 @@ __global__ void __launch_bounds__(NW * 32, 1) tile_step_kernel(__grid_constant__
       for (int g = 0; g < IC; ++g) {
         S.reads_h[g] = 2 * YT;
         S.reads_u[g] = UT;
-        S.cnt_x[g] = S.cnt_yz[g] = S.cnt_u[g] = 0;
       }
-      S.cnt_x[IC] = 0;
-      // every barrier phase of the previous item completed and was waited
-      // for, so the barriers restart at phase 0 for this item
+      // every barrier of the previous item has no operation pending (its
+      // phase completed and was waited for, or, in a skipped item, nothing was
+      // issued), so the barriers restart at phase 0 for this item
       for (int q = 0; q < NPLANES; ++q) {
         if (bars_live) mbar_inval(&S.bar_plane[q]);
         mbar_init(&S.bar_plane[q]);
+      }
+      for (int g = 0; g <= IC; ++g) {
+        if (bars_live) mbar_inval(&S.bar_x[g]);
+        mbar_init(&S.bar_x[g], XT);
       }
       for (int g = 0; g < IC; ++g) {
         if (bars_live) {
           mbar_inval(&S.bar_halo[g]);
           mbar_inval(&S.bar_u0[g]);
+          mbar_inval(&S.bar_yz[g]);
+          mbar_inval(&S.bar_u[g]);
         }
         mbar_init(&S.bar_halo[g]);
         mbar_init(&S.bar_u0[g]);
+        mbar_init(&S.bar_yz[g], 2 * YT);
+        mbar_init(&S.bar_u[g], UT);
       }
       asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
       bars_live = true;

@@ -134,7 +134,7 @@ class CaseCheckpoint(C.Structure):
     neighbour table and blocks."""
     _fields_ = [("dim", C.c_int), ("nb", C.c_int), ("steps", C.c_int), ("max_steps", C.c_int),
                 ("t", C.c_double), ("t_end", C.c_double), ("cfl", C.c_double),
-                ("cell_size", C.c_double), ("material", Material)]
+                ("cell_size", C.c_double), ("material", Material), ("scheme", Scheme)]
 
 
 IC_QUADRANTS, IC_BLAST, IC_PROGRAM = 1, 2, 3

@@ -151,10 +151,12 @@ int alp_space_rhs(int dim, const alp_scheme *scheme, const alp_material *mat,
  * counterpart in the reference. The face-flux scratch is a 16 MiB array of
  * this library in device memory instead of a caller workspace, so at most 28
  * blocks in 3D, 453 in 2D and 10,280 in 1D per call; a larger nb returns
- * ALP_ERR_CAPACITY and launches nothing. Nothing is allocated by the call. The
- * first call on each device (with that device current) looks up the array's
- * address, which may load the library's module: make that first call before
- * any stream capture. All calls on a device share the one array and it keeps
+ * ALP_ERR_CAPACITY and launches nothing (after the dim, scheme and material
+ * checks of alp_space_rhs, which come first). Nothing is allocated by the
+ * call. Every call looks up the array's address in the current context; the
+ * first call in a context (the first on a device, or the first after
+ * cudaDeviceReset) may load the library's module: make that call before any
+ * stream capture. All calls on a device share the one array and it keeps
  * the last call's contents (no call relies on them): calls that may overlap
  * (different streams or threads without ordering) race on it, so order them.
  * Results are those of alp_space_rhs on the same inputs. */
@@ -319,12 +321,16 @@ int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t,
  * conservatives in the block layout), plus the case's own settings. A case
  * restored from its checkpoint continues exactly as the uninterrupted case:
  * state, time and step count are the same, and nothing else carries over
- * between steps. */
+ * between steps. The checkpoint records the engine's scheme selection
+ * (precision and time integrator included); restoring into an engine with
+ * another selection returns ALP_ERR_INVALID, since the case would continue
+ * with other numerics. */
 typedef struct {
   int dim, nb;
   int steps, max_steps;  /* steps taken; the step budget (<= 0: none) */
   double t, t_end, cfl, cell_size;
   alp_material material;
+  alp_scheme scheme;     /* the selection the case was stepped with */
 } alp_case_checkpoint;
 
 /* Fills *info, and (when not null) h_nbr26 [nb][26] with the case-local

@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from alpaca_b200 import api, cases
+from alpaca_b200 import native as N
 
 pytestmark = pytest.mark.gpu
 
@@ -48,10 +49,32 @@ def test_restore_rejects_another_dimension(cuda):
     ck = e.checkpoint(e.add_case(case))
     e.close()
     e2 = api.Engine(2, "fvchar", capacity_blocks=64, max_cases=1)
-    from alpaca_b200 import native as N
     with pytest.raises(N.AlpacaError):
         e2.restore(ck)
     e2.close()
+
+
+@pytest.mark.parametrize("other", [("fsroe", N.FP64, None), ("fvchar", N.FP32_FLUX, None),
+                                   ("fvchar", N.FP64, N.RK2)])
+def test_restore_rejects_another_scheme(cuda, other):
+    """A case checkpointed under FV char / FP64 / RK3 is refused by an engine
+    with another scheme, precision or time integrator, and accepted by one
+    with the same selection."""
+    case = cases.fourier_shock(1, dim=3, seed=6)
+    e = api.Engine(3, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    ck = e.checkpoint(e.add_case(case))
+    e.close()
+    variant, precision, integrator = other
+    sch = N.Scheme.make(variant, precision)
+    if integrator is not None:
+        sch.time_integrator = integrator
+    e2 = api.Engine(3, sch, precision=precision, capacity_blocks=case.grid.nb, max_cases=1)
+    with pytest.raises(N.AlpacaError, match="scheme selection"):
+        e2.restore(ck)
+    e2.close()
+    e3 = api.Engine(3, "fvchar", capacity_blocks=case.grid.nb, max_cases=1)
+    e3.restore(ck)
+    e3.close()
 
 
 def test_resumed_level_case_equals_uninterrupted(cuda):

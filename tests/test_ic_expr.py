@@ -18,7 +18,9 @@ from alpaca_b200 import api
 from alpaca_b200 import native as N
 from oracle import ic_expr as X
 
-REF = os.environ.get("ALPACA_REFERENCE_DIR", "/root/reference")
+# the reference checkout: $ALPACA_REFERENCE_DIR, else `reference` beside the repository
+REF = os.environ.get("ALPACA_REFERENCE_DIR",
+                     os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "reference"))
 
 SOD = """if (x < 0.5)
 {

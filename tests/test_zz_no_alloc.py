@@ -61,7 +61,7 @@ def assert_same_rhs(dim, a, b):
 
 
 def test_static_scratch_matches_workspace_on_consecutive_calls(cuda):
-    # 1st call: the largest 3D batch that fits (27 blocks), 2nd call: a
+    # 1st call: a 27-block 3D batch, 2nd call: a
     # different single block, so the 2nd call finds the 1st call's contents in
     # the shared array; 3rd and 4th: 2D and flux splitting on other inputs.
     big = cases.fourier_shock(3, dim=3, seed=7)
@@ -84,6 +84,49 @@ def test_static_scratch_matches_workspace_on_consecutive_calls(cuda):
     assert_same_rhs(3, a, b)
 
 
+def test_static_scratch_at_its_exact_3d_limit(cuda):
+    """28 blocks in 3D (a 7 x 2 x 2 periodic grid) fill the static array."""
+    g = cases.BlockGrid(3, (7, 2, 2), (1, 1, 1), 1.0 / 32)  # 3.5 x 1 x 1
+    assert g.nb == MAX_BLOCKS[3]
+    x, y, z = g.cell_centres()
+    rho = 1.0 + 0.2 * np.sin(2 * np.pi * x / 3.5) + 0.1 * np.cos(2 * np.pi * y)
+    p = 1.0 + 0.1 * np.cos(2 * np.pi * z)
+    vel = [0.3 * np.sin(2 * np.pi * y), 0.2 * np.cos(2 * np.pi * z), -0.1 + 0 * x]
+    glob = cases.primes_to_conservatives(3, rho, p, vel, 1.4)
+    case = cases.Case("limit28", g, g.scatter(glob), 1.4)
+    ud = _dev(filled(case), cuda)
+    mat = N.Material.make(1.4)
+    got = rhs_static(3, "fvchar", mat, ud, g.cell_size)
+    assert_same_rhs(3, got, rhs_workspace(3, "fvchar", mat, ud, g.cell_size))
+
+
+def test_static_scratch_glf_and_no_allocation(cuda):
+    """Global Lax-Friedrichs splitting (its stateless per-call maximum takes
+    a second device slot of the library) matches alp_space_rhs; after a warm-up
+    call, repeated static calls leave the device's free memory unchanged."""
+    import torch
+    case = cases.fourier_shock(3, dim=3, seed=11)
+    ud = _dev(filled(case), cuda)
+    mat = N.Material.make(case.gamma)
+    h = case.grid.cell_size
+    got = rhs_static(3, "fs_glf", mat, ud, h)
+    assert_same_rhs(3, got, rhs_workspace(3, "fs_glf", mat, ud, h))
+    lib = N.lib()
+    rhs = torch.empty_like(ud)
+    calls = [(v, N.Scheme.make(v)) for v in ("fvchar", "fs_glf", "fsroe")]
+    for _, sch in calls:  # warm-up: every path loaded once
+        N.check(lib.alp_space_rhs_static(3, C.byref(sch), C.byref(mat), ud.data_ptr(),
+                                         ud.shape[0], h, rhs.data_ptr(), None))
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    for _ in range(5):
+        for _, sch in calls:
+            N.check(lib.alp_space_rhs_static(3, C.byref(sch), C.byref(mat), ud.data_ptr(),
+                                             ud.shape[0], h, rhs.data_ptr(), None))
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+
+
 def test_static_scratch_rejects_batches_beyond_its_size(cuda):
     lib = N.lib()
     sch = N.Scheme.make("fvchar")
@@ -96,3 +139,9 @@ def test_static_scratch_rejects_batches_beyond_its_size(cuda):
         assert f"at most {cap} blocks" in lib.alp_last_error().decode()
     assert lib.alp_space_rhs_static(3, C.byref(sch), C.byref(mat), None, 0, 0.1, None,
                                     None) == N.ALP_OK
+    # the argument checks of alp_space_rhs come before the capacity check
+    bad = N.Material.make(-1.0)
+    assert lib.alp_space_rhs_static(3, C.byref(sch), C.byref(bad), None, 1000, 0.1, None,
+                                    None) == N.ALP_ERR_INVALID
+    assert lib.alp_space_rhs_static(3, None, C.byref(mat), None, 1000, 0.1, None,
+                                    None) == N.ALP_ERR_INVALID

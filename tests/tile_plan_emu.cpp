@@ -94,6 +94,8 @@ int main(int argc, char **argv) {
   };
 
   static Smem S;
+  // finished tasks of each x face / plane (the kernel counts them on mbarriers)
+  int cnt_x[IC + 1] = {}, cnt_yz[IC] = {}, cnt_u[IC] = {};
   std::memset(&S, 0, sizeof(S));
   for (int d = 0; d < 6; ++d) S.nbr[d] = nbr[d];
   // buffer tags: which plane / face each buffer holds (-100: none)
@@ -164,8 +166,8 @@ int main(int argc, char **argv) {
     if (t.type == T_FX) {
       int const a = t.g;
       // waits: flux slot free, source planes loaded
-      if (a > RFX) check(S.cnt_u[a - RFX - 1] >= UT, "fx wait (a-5) unsatisfied", a, pos, 0);
-      if (a >= RFX) check(S.cnt_u[a - RFX] >= UT, "fx wait (a-4) unsatisfied", a, pos, 0);
+      if (a > RFX) check(cnt_u[a - RFX - 1] >= UT, "fx wait (a-5) unsatisfied", a, pos, 0);
+      if (a >= RFX) check(cnt_u[a - RFX] >= UT, "fx wait (a-4) unsatisfied", a, pos, 0);
       for (int m = 0; m < 6; ++m) {
         int const q = stencil_src(a - 3 + m, nbr[0], nbr[1]).index;
         check(plane_loaded[q + 3], "fx source plane not loaded", a, q, pos);
@@ -186,11 +188,11 @@ int main(int argc, char **argv) {
         faces++;
       }
       fx_tag[a % RFX] = a;
-      S.cnt_x[a]++;
+      cnt_x[a]++;
       for (int m = 0; m < 6; ++m) release_plane(stencil_src(a - 3 + m, nbr[0], nbr[1]).index);
     } else if (t.type == T_FY || t.type == T_FZ) {
       int const g = t.g, dir = t.type == T_FY ? 1 : 2;
-      if (g >= BYZ) check(S.cnt_u[g - BYZ] >= UT, "yz buffer wait unsatisfied", g, pos, 0);
+      if (g >= BYZ) check(cnt_u[g - BYZ] >= UT, "yz buffer wait unsatisfied", g, pos, 0);
       check(plane_loaded[g + 3] && ring_tag[ring_slot(g)] == g, "yz plane", g, pos, 0);
       check(halo_loaded[g] && h_tag[g % BH] == g, "yz halos", g, pos, 0);
       for (int l = 0; l < 32; ++l) {
@@ -216,12 +218,12 @@ int main(int argc, char **argv) {
         faces++;
       }
       fyz_tag[g % BYZ] = g;
-      S.cnt_yz[g]++;
+      cnt_yz[g]++;
       release_plane(g);
       if (--S.reads_h[g] == 0 && g + BH < IC) issue_halos(g + BH);
     } else if (t.type == T_U) {
       int const g = t.g;
-      check(S.cnt_x[g] >= XT && S.cnt_x[g + 1] >= XT && S.cnt_yz[g] >= 2 * YT,
+      check(cnt_x[g] >= XT && cnt_x[g + 1] >= XT && cnt_yz[g] >= 2 * YT,
             "update wait unsatisfied", g, pos, 0);
       check(u0_loaded[g] && u_tag[g % BU] == g, "U0 plane", g, pos, 0);
       check(fx_tag[g % RFX] == g && fx_tag[(g + 1) % RFX] == g + 1, "update reads fx", g,
@@ -239,7 +241,7 @@ int main(int argc, char **argv) {
         covered_u[g][jk]++;
         cells++;
       }
-      S.cnt_u[g]++;
+      cnt_u[g]++;
       release_plane(g);
       if (--S.reads_u[g] == 0 && g + BU < IC) issue_u0(g + BU);
     } else {

@@ -82,7 +82,16 @@ __host__ __device__ inline Src stencil_src(int c, int nlo, int nhi) {
 // ---- the task stream ------------------------------------------------------
 enum TaskType { T_FX = 0, T_FY = 1, T_FZ = 2, T_U = 3, T_NONE = 4 };
 constexpr int XT = PLANE / 32;                  // warp tasks of one x-face plane (8)
-constexpr int YT = (FACE_ROW * IC + 31) / 32;   // of the y faces of one plane (9)
+// The 17 x 16 y (or z) faces of a plane split into interior faces (a = 3 ..
+// 13, whose six stencil cells all lie in the block's own plane: one warp
+// reads them with constant offsets) and edge faces (a = 0, 1, 2, 14, 15, 16,
+// whose stencils reach the halo rows / columns or a wall).
+constexpr int NIF = (IC - 5) * IC;             // interior faces (176)
+constexpr int NEF = 6 * IC;                    // edge faces (96)
+constexpr int IFT = (NIF + 31) / 32;           // tasks of interior faces (6)
+constexpr int EFT = NEF / 32;                  // tasks of edge faces (3)
+constexpr int YT = IFT + EFT;                  // of the y faces of one plane (9)
+static_assert(NEF % 32 == 0, "edge-face tasks are full");
 constexpr int UT = PLANE / 32;                  // of one plane's stage update (8)
 constexpr int FT = XT + 2 * YT;                  // face tasks of one plane (26)
 constexpr int ITER = FT + UT;                     // tasks of one plane g >= LAG (34)
@@ -194,29 +203,63 @@ struct Smem {
 
 
 // One face of a warp task: direction dir; x faces: face a at jk = j * 16 + k
-// (q = jk); y faces of plane g: face a of column k = t (q = a * 16 + t); z
-// faces of plane g: face a of row j = t (q = t * 17 + a).
+// (q = jk); y faces of plane g: face a of column k = t; z faces of plane g:
+// face a of row j = t. Lanes q < 32 IFT take the interior faces (y: t fastest,
+// z: a fastest, so that a warp's stencil reads are consecutive cells), the
+// others the edge faces; `valid` is false for the idle lanes of the last
+// interior task (their a, t name a real face, which they neither compute nor
+// store).
 struct FaceAt {
   int a, t;
+  bool valid;
 };
 __host__ __device__ inline FaceAt face_at(int dir, int q) {
-  if (dir == 0) return FaceAt{0, q};
-  if (dir == 1) return FaceAt{q / IC, q % IC};
-  return FaceAt{q % FACE_ROW, q / FACE_ROW};
+  if (dir == 0) return FaceAt{0, q, true};
+  if (q < 32 * IFT) {
+    bool const valid = q < NIF;
+    int const i = valid ? q : NIF - 1;
+    return dir == 1 ? FaceAt{3 + i / IC, i % IC, valid} : FaceAt{3 + i % (IC - 5), i / (IC - 5), valid};
+  }
+  int const r = q - 32 * IFT;
+  int const e = dir == 1 ? r / IC : r % 6;  // which edge face: a = 0, 1, 2, 14, 15, 16
+  return FaceAt{e < 3 ? e : e + IC - 5, dir == 1 ? r % IC : r / 6, true};
+}
+// True for the tasks of interior y / z faces (uniform over the warp).
+__host__ __device__ inline bool interior_task(int dir, int w) { return dir != 0 && w < IFT; }
+
+// Stencil of an interior face from consecutive cells of the block's own plane
+// with constant offsets: cell m at p[m * STEP], field f at f * PLANE; the
+// momenta in canonical order for direction DIR.
+template <int DIR, int STEP>
+__host__ __device__ inline void gather_interior(double const *p, double (&cons)[6][NE]) {
+#pragma unroll
+  for (int m = 0; m < 6; ++m) {
+    double const *c = p + m * STEP;
+    cons[m][MASS] = c[MASS * PLANE];
+    cons[m][ENERGY] = c[ENERGY * PLANE];
+    cons[m][MOMX] = c[canon_field(DIR, MOMX) * PLANE];
+    cons[m][MOMX + 1] = c[canon_field(DIR, MOMX + 1) * PLANE];
+    cons[m][MOMX + 2] = c[canon_field(DIR, MOMX + 2) * PLANE];
+  }
 }
 
 // The 6-cell stencil (cells a - 3 .. a + 2 along dir, the five fields in
 // canonical order) of face q of x face plane g (dir 0) or of plane g (dir 1,
 // 2), from the ring and the halo buffers; symmetry walls negate the principal
 // momentum of mirrored cells.
-__host__ __device__ inline void gather_face(Smem const &S, int dir, int g, int q,
+__host__ __device__ inline void gather_face(Smem const &S, int dir, int g, int w, int q,
                                             double (&cons)[6][NE]) {
   FaceAt const f = face_at(dir, q);
+  double const *plane = &S.ring[ring_slot(g)][0][0];
+  if (interior_task(dir, w)) {
+    if (dir == 1) gather_interior<1, IC>(plane + (f.a - 3) * IC + f.t, cons);
+    else gather_interior<2, 1>(plane + f.t * IC + f.a - 3, cons);
+    return;
+  }
   int const a = dir == 0 ? g : f.a;
   int const nlo = S.nbr[2 * dir], nhi = S.nbr[2 * dir + 1];
   int const o2 = canon_field(dir, MOMX), o3 = canon_field(dir, MOMX + 1),
             o4 = canon_field(dir, MOMX + 2);
-  double const *plane = &S.ring[ring_slot(g)][0][0];
   int const hb = g % BH;
   // base and field stride of the halo buffers of the face's direction; the
   // cell offsets below are chosen with selects (the lanes' faces differ, a

@@ -208,20 +208,22 @@ __device__ __forceinline__ void task_face(Smem &S, ItemCtx const &C, Task const 
         },
         C.err, 2);
   } else {
-    // the flux buffer held plane g - BYZ, read by its stage update
+    // the flux buffer held plane g - BYZ, read by its stage update; interior
+    // faces read no halo
+    bool const edge = !interior_task(dir, t.w);
     wait_until(
         [&] {
           if (lane == 0) return g < BYZ || mbar_try(&S.bar_u[g - BYZ]);
           if (lane == 1) return mbar_try(&S.bar_plane[g + 3]);
-          if (lane == 2) return mbar_try(&S.bar_halo[g]);
+          if (lane == 2) return !edge || mbar_try(&S.bar_halo[g]);
           return true;
         },
         C.err, 2);
   }
   int const q = t.w * 32 + lane;
-  if (compute && (dir == 0 || q < FACE_ROW * IC)) {
+  if (compute && face_at(dir, q).valid) {
     double cons[6][NE];
-    gather_face(S, dir, g, q, cons);
+    gather_face(S, dir, g, t.w, q, cons);
     double fd[NE];
     bool const valid = face_compute<3, 0, SCHEME, T>(C.eos, C.B, cons, fd);
     FluxAt const o = flux_at(S, dir, g, q);

@@ -177,7 +177,7 @@ int main(int argc, char **argv) {
       for (int l = 0; l < 32; ++l) {
         int const jk = t.w * 32 + l;
         double cons[6][NE];
-        gather_face(S, 0, a, jk, cons);
+        gather_face(S, 0, a, t.w, jk, cons);
         for (int m = 0; m < 6; ++m)
           for (int c = 0; c < NE; ++c)
             check(cons[m][c] == expect(0, a - 3 + m, jk / IC, jk % IC, canon_field(0, c)),
@@ -197,11 +197,11 @@ int main(int argc, char **argv) {
       check(halo_loaded[g] && h_tag[g % BH] == g, "yz halos", g, pos, 0);
       for (int l = 0; l < 32; ++l) {
         int const q = t.w * 32 + l;
-        if (q >= FACE_ROW * IC) continue;
         FaceAt const fa = face_at(dir, q);
+        if (!fa.valid) continue;
         int const a = fa.a, tt = fa.t;
         double cons[6][NE];
-        gather_face(S, dir, g, q, cons);
+        gather_face(S, dir, g, t.w, q, cons);
         for (int m = 0; m < 6; ++m)
           for (int c = 0; c < NE; ++c) {
             // transverse indices: y faces (x = g, z = tt); z faces (x = g, y = tt);

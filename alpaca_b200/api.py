@@ -128,13 +128,25 @@ class Engine:
         except Exception:
             pass
 
-    def add_case(self, case: Case, t0: float = 0.0, max_steps: int | None = None) -> int:
+    def add_case(self, case: Case, t0: float = 0.0, max_steps: int | None = None,
+                 interior: np.ndarray | None = None) -> int:
+        """Adds the case; with `interior` ([nb][NE][16..] interiors, e.g.
+        pinned host memory) only those cells are transferred
+        (alp_engine_add_case_interior) instead of case.u's full blocks."""
         g = case.grid
-        u = np.ascontiguousarray(case.u, dtype=np.float64)
         nbr = np.ascontiguousarray(g.nbr26, dtype=np.int32)
         mat = N.Material.make(case.gamma, case.B, False)
         cid = C.c_int()
         steps = case.steps if max_steps is None else max_steps
+        if interior is not None:
+            assert interior.flags.c_contiguous and interior.dtype == np.float64
+            self._check(self.lib.alp_engine_add_case_interior(
+                self.h, C.byref(mat), g.cell_size, case.cfl, t0, case.t_end, steps, g.nb,
+                nbr.ctypes.data_as(C.POINTER(C.c_int)),
+                interior.ctypes.data_as(C.POINTER(C.c_double)), C.byref(cid)))
+            self.nb[cid.value] = (g.nb, (g.nb, self.ne) + block_shape(self.dim))
+            return cid.value
+        u = np.ascontiguousarray(case.u, dtype=np.float64)
         self._check(self.lib.alp_engine_add_case(
             self.h, C.byref(mat), g.cell_size, case.cfl, t0, case.t_end, steps, g.nb,
             nbr.ctypes.data_as(C.POINTER(C.c_int)), u.ctypes.data_as(C.POINTER(C.c_double)),
@@ -189,6 +201,21 @@ class Engine:
         self._check(self.lib.alp_engine_get_case(self.h, cid,
                                                  out.ctypes.data_as(C.POINTER(C.c_double)),
                                                  C.byref(t), C.byref(steps)))
+        return out, t.value, steps.value
+
+    def get_interior(self, cid: int, out: np.ndarray | None = None):
+        """(interiors [nb][NE][16..], t, steps) of case cid
+        (alp_engine_get_case_interior); `out` may be a preallocated
+        (e.g. pinned) C-contiguous array."""
+        nb, _ = self.nb[cid]
+        shp = (nb, self.ne) + tuple(16 if d < self.dim else 1 for d in range(3))
+        if out is None:
+            out = np.empty(shp, dtype=np.float64)
+        assert out.shape == shp and out.flags.c_contiguous and out.dtype == np.float64
+        t = C.c_double()
+        steps = C.c_int()
+        self._check(self.lib.alp_engine_get_case_interior(
+            self.h, cid, out.ctypes.data_as(C.POINTER(C.c_double)), C.byref(t), C.byref(steps)))
         return out, t.value, steps.value
 
     def checkpoint(self, cid: int) -> dict:

@@ -37,6 +37,7 @@ int faces_of(int dim) {
   return 17 * (dim > 1 ? 17 : 2) * (dim > 2 ? 17 : 2);
 }
 int cells_of(int dim) { return 24 * (dim > 1 ? 24 : 1) * (dim > 2 ? 24 : 1); }
+int interior_of(int dim) { return 16 * (dim > 1 ? 16 : 1) * (dim > 2 ? 16 : 1); }
 
 }  // namespace
 
@@ -418,8 +419,8 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   // flux sum matches the reference bit for bit.
   e->path = 1;
   grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
-  grab((void **)&e->R, (size_t)e->ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) *
-                           capacity_blocks * sizeof(double));
+  // R also stages interior-only case transfers (alp_engine_*_case_interior)
+  grab((void **)&e->R, (size_t)e->ne * interior_of(dim) * capacity_blocks * sizeof(double));
   grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
@@ -515,6 +516,24 @@ int alp_engine_add_case(alp_engine *e, const alp_material *mat, double cell_size
   return ALP_OK;
 }
 
+int alp_engine_add_case_interior(alp_engine *e, const alp_material *mat, double cell_size,
+                                 double cfl, double t0, double t_end, int max_steps, int nb,
+                                 const int *h_nbr26, const double *h_interior, int *case_id) {
+  if (!e || !case_id) return fail(ALP_ERR_INVALID, "null argument");
+  if (nb <= 0 || !h_nbr26 || !h_interior) return fail(ALP_ERR_INVALID, "bad case blocks");
+  int cid, first;
+  if (int rc = engine_add_case_core(e, mat, cell_size, cfl, t0, t_end, max_steps, nb, h_nbr26,
+                                    &cid, &first))
+    return rc;
+  // staged in the pencil path's per-cell scratch R, sized [capacity][NE][interior]
+  size_t const bytes = (size_t)nb * e->ne * interior_of(e->dim) * sizeof(double);
+  ALP_CUDA(cudaMemcpyAsync(e->R, h_interior, bytes, cudaMemcpyHostToDevice, e->stream));
+  ALP_CUDA(launch_interior_copy(e->dim, e->U, first, nb, e->R, true, e->stream));
+  ALP_CUDA(cudaStreamSynchronize(e->stream));
+  *case_id = cid;
+  return ALP_OK;
+}
+
 int alp_engine_add_case_ic(alp_engine *e, const alp_material *mat, double cell_size, double cfl,
                            double t0, double t_end, int max_steps, const int *nblocks,
                            const int *periodic, int ic_type, const double *ic_params,
@@ -592,6 +611,20 @@ int alp_engine_step(alp_engine *e, int n) {
   }
   for (int i = 0; i < n; ++i) ALP_CUDA(cudaGraphLaunch(e->graph, e->stream));
   return ALP_OK;
+}
+
+int alp_engine_get_case_interior(alp_engine *e, int case_id, double *h_interior, double *t,
+                                 int *steps) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (case_id < 0 || case_id >= e->max_cases || !e->case_rec[case_id].live)
+    return fail(ALP_ERR_NOT_FOUND, "unknown case");
+  auto const &c = e->case_rec[case_id];
+  if (h_interior) {
+    size_t const bytes = (size_t)c.nb * e->ne * interior_of(e->dim) * sizeof(double);
+    ALP_CUDA(launch_interior_copy(e->dim, e->U, c.first, c.nb, e->R, false, e->stream));
+    ALP_CUDA(cudaMemcpyAsync(h_interior, e->R, bytes, cudaMemcpyDeviceToHost, e->stream));
+  }
+  return alp_engine_get_case(e, case_id, nullptr, t, steps);
 }
 
 int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t, int *steps) {

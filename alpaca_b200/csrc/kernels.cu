@@ -7,7 +7,6 @@
 #include <cfloat>
 #include <cstdio>
 
-#include <mutex>
 
 #include "kernels.cuh"
 #include "face.cuh"
@@ -1183,16 +1182,45 @@ cudaError_t launch_glf_maxima(Launch const &L, unsigned long long *glf, int ncas
   return cudaGetLastError();
 }
 
-// The address is looked up once per device (the lookup may load the module).
+// The address is looked up on every call (a symbol lookup in the loaded
+// module): after cudaDeviceReset the module loads again, possibly at another
+// address, so an address kept from an earlier call could be stale.
 unsigned long long *glf_stateless_slot() {
-  static std::mutex mu;
-  static void *addr[64] = {};
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return nullptr;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev] && cudaGetSymbolAddress(&addr[dev], g_glf_stateless) != cudaSuccess)
-    addr[dev] = nullptr;
-  return static_cast<unsigned long long *>(addr[dev]);
+  void *addr = nullptr;
+  if (cudaGetSymbolAddress(&addr, g_glf_stateless) != cudaSuccess) return nullptr;
+  return static_cast<unsigned long long *>(addr);
+}
+
+namespace {
+// packed [b][field][ICX][ICY][ICZ] <-> the interiors of pool blocks first + b
+// (one thread per cell; consecutive threads take consecutive z cells).
+template <int DIM>
+__global__ void interior_copy_kernel(double *U, int first, int nb, double *P, bool to_pool) {
+  using G = Geo<DIM>;
+  long long const n = (long long)nb * G::NE * G::INTERIOR;
+  for (long long x = blockIdx.x * (long long)blockDim.x + threadIdx.x; x < n;
+       x += (long long)gridDim.x * blockDim.x) {
+    int const c = int(x % G::INTERIOR);
+    long long const bf = x / G::INTERIOR;  // b * NE + field
+    int const k = c % G::ICZ, j = (c / G::ICZ) % G::ICY, i = c / (G::ICZ * G::ICY);
+    long long const u = ((long long)first * G::NE + bf) * G::CELLS +
+                        G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+    if (to_pool) U[u] = P[x];
+    else P[x] = U[u];
+  }
+}
+}  // namespace
+
+cudaError_t launch_interior_copy(int dim, double *U, int first, int nb, double *packed,
+                                 bool to_pool, cudaStream_t stream) {
+  if (nb <= 0) return cudaSuccess;
+  int const grid = 148 * 8, threads = 256;
+  switch (dim) {
+    case 1: interior_copy_kernel<1><<<grid, threads, 0, stream>>>(U, first, nb, packed, to_pool); break;
+    case 2: interior_copy_kernel<2><<<grid, threads, 0, stream>>>(U, first, nb, packed, to_pool); break;
+    default: interior_copy_kernel<3><<<grid, threads, 0, stream>>>(U, first, nb, packed, to_pool); break;
+  }
+  return cudaGetLastError();
 }
 
 }  // namespace alp

@@ -140,6 +140,10 @@ cudaError_t launch_initial_condition(int dim, double *U, int first, int const nb
 // launch is ready).
 cudaError_t launch_dt_finalize(CaseState *cases, int ncases, cudaStream_t stream,
                                int *dtflag = nullptr);
+// Interiors of the nb pool blocks from slot `first` to (to_pool false) or from
+// (to_pool true) packed [nb][NE][ICX][ICY][ICZ]; halos untouched.
+cudaError_t launch_interior_copy(int dim, double *U, int first, int nb, double *packed,
+                                 bool to_pool, cudaStream_t stream);
 // t += dt, steps += (dt > 0) for every case.
 cudaError_t launch_step_commit(CaseState *cases, int ncases, cudaStream_t stream);
 

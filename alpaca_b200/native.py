@@ -192,6 +192,9 @@ _SIGS = {
     "alp_engine_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
     "alp_engine_add_case": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _I, _D, _I]),
+    "alp_engine_add_case_interior": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double,
+                                               C.c_double, C.c_double, C.c_int, C.c_int, _I, _D,
+                                               _I]),
     "alp_engine_add_case_ic": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_int, _I, _I, C.c_int, _D, C.c_int, _I]),
     "alp_ic_program_create": (C.c_int, [C.c_char_p, C.POINTER(C.c_void_p)]),
@@ -206,6 +209,7 @@ _SIGS = {
                             _D]),
     "alp_engine_remove_case": (C.c_int, [_V, C.c_int]),
     "alp_engine_step": (C.c_int, [_V, C.c_int]),
+    "alp_engine_get_case_interior": (C.c_int, [_V, C.c_int, _D, _D, _I]),
     "alp_engine_get_case": (C.c_int, [_V, C.c_int, _D, _D, _I]),
     "alp_engine_all_done": (C.c_int, [_V, _I]),
     "alp_engine_checkpoint_case": (C.c_int, [_V, C.c_int, C.POINTER(CaseCheckpoint), _I, _D]),

@@ -39,6 +39,11 @@ FLOPS_PER_CELL_UPDATE_3D = {"fvchar": 15767, "fvprim": 10192, "fsroe": 22478}
 # and dram__bytes_write.sum over the step's kernels, one ncu capture; summary in
 # profiles/step_fvchar_128cubed.md)
 TRAFFIC_PER_STEP = {("fvchar", "fp64"): 4.359e9}
+# DRAM bytes per cell-update of the multi-level step (fvchar, FP64): one ncu
+# capture of a macro step of the same hierarchy at n0 = 2 (31 / 264 leaves, 176
+# ghosts, 4.58 M cell-updates, 9.43 GB), scaled by cell-updates (summary in
+# profiles/levels_3d_spherical_shock.md)
+LEVELS_DRAM_PER_CELL_UPDATE = {("fvchar", "fp64"): 2059.0}
 # stepping candidates of alp_engine_autotune, in its numbering
 CANDIDATES = ["face fluxes, 128-thread blocks", "face fluxes, 64-thread blocks", "pencil sweeps",
               "face fluxes and stage updates overlapped in batches",
@@ -385,8 +390,14 @@ def levels_report(args):
                    "l2": "state %.2f GB per pool > 126 MB L2 (no flush needed)"
                          % ((case.nleaf + info["ghosts"]) * 5 * 24 ** 3 * 8 / 1e9)},
         "roofline": {"bound": "hbm", "achieved": value * B_ALG_3D / 1e9, "peak": hbm, "unit": "GB/s",
-                     "frac": value * B_ALG_3D / 1e9 / hbm, "traffic": None, "peak_source": src,
-                     "fp64_compute": levels_fp64_compute(args, value)},
+                     "frac": value * B_ALG_3D / 1e9 / hbm,
+                     "traffic": (LEVELS_DRAM_PER_CELL_UPDATE[(args.variant, args.precision)] *
+                                 info["cell_updates_per_macro_step"]
+                                 if (args.variant, args.precision) in LEVELS_DRAM_PER_CELL_UPDATE
+                                 else None),
+                     "traffic_note": "DRAM bytes per macro step, scaled by cell-updates from an "
+                                     "ncu capture of the same hierarchy at n0 = 2",
+                     "peak_source": src, "fp64_compute": levels_fp64_compute(args, value)},
         "gpu_launches": info["launches_per_macro_step"] * args.steps,
         "clocks": clocks.summary(),
     }
@@ -432,17 +443,17 @@ def run_ours(args, ws, rank, local):
     eng.close()
 
     # end to end through the public C ABI from pinned host buffers: upload the
-    # case, run the steps, read the state back (copies inside the timed region)
+    # case's interiors, run the steps, read the interiors back (copies inside
+    # the timed region; the engine keeps nothing else of a case)
     e2e = None
     if not args.no_e2e:
-        host = torch.from_numpy(np.ascontiguousarray(case.u)).pin_memory()
-        case_p = cases.Case(case.name, case.grid, host.numpy(), case.gamma, case.B, case.cfl,
-                            case.t_end, 0)
+        inner = np.ascontiguousarray(case.u[cases.interior(3)])
+        host = torch.from_numpy(inner).pin_memory()
         out = torch.empty_like(host).pin_memory()
         eng = api.Engine(3, args.variant, precision=prec, capacity_blocks=case.grid.nb,
                          max_cases=1)
         stream = torch.cuda.ExternalStream(eng.stream_handle)
-        cid = eng.add_case(case_p, max_steps=0)
+        cid = eng.add_case(case, max_steps=0, interior=host.numpy())
         eng.set_path(chosen)
         eng.step(args.warmup)
         eng.remove_case(cid)
@@ -450,12 +461,9 @@ def run_ours(args, ws, rank, local):
         barrier(ws, dev)
         f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         f0.record(stream)
-        cid = eng.add_case(case_p, max_steps=0)
+        cid = eng.add_case(case, max_steps=0, interior=host.numpy())
         eng.step(args.steps)
-        t_ = C.c_double()
-        s_ = C.c_int()
-        N.check(N.lib().alp_engine_get_case(eng.h, cid, C.cast(out.data_ptr(), C.POINTER(C.c_double)),
-                                            C.byref(t_), C.byref(s_)))
+        eng.get_interior(cid, out.numpy())
         f1.record(stream)
         f1.synchronize()
         barrier(ws, dev)
@@ -464,9 +472,37 @@ def run_ours(args, ws, rank, local):
         nbytes = host.numel() * 8
         e2e = {"value": cells * args.steps * ws / (ems * 1e-3), "unit": METRIC,
                "h2d_bytes_per_step": nbytes / args.steps, "d2h_bytes_per_step": nbytes / args.steps,
-               "ms": ems, "note": "one case per timed region: pinned H2D of the 512 blocks, "
-                                  f"{args.steps} steps, D2H of the final state; bytes amortised per step"}
+               "ms": ems, "note": "one case per timed region: pinned H2D of the 512 blocks' "
+                                  f"interiors (alp_engine_add_case_interior), {args.steps} steps, "
+                                  "D2H of the final interiors (alp_engine_get_case_interior); "
+                                  "bytes amortised per step"}
 
+    # single GPU: the FP32-flux form and the multi-level batching form timed
+    # beside the headline (their own lines come from --precision fp32 / --levels)
+    fp32 = levels = None
+    if ws == 1 and args.precision == "fp64":
+        eng = api.Engine(3, args.variant, precision=N.FP32_FLUX, capacity_blocks=case.grid.nb,
+                         max_cases=1)
+        stream = torch.cuda.ExternalStream(eng.stream_handle)
+        eng.add_case(case, max_steps=0)
+        f_chosen, _ = eng.autotune(trial_steps=3)
+        eng.step(args.warmup)
+        torch.cuda.synchronize()
+        g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        eng.step(args.steps)
+        g1.record(stream)
+        g1.synchronize()
+        fms = g0.elapsed_time(g1)
+        eng.close()
+        fp32 = {"value": cells * args.steps / (fms * 1e-3), "unit": METRIC,
+                "ms_per_step": fms / args.steps, "steps": args.steps, "warmup": args.warmup,
+                "dtype": "f32-flux/f64-state", "path": CANDIDATES[f_chosen],
+                "vs_fp64": ms / fms}
+        lv = argparse.Namespace(**vars(args))
+        lv.steps = min(args.steps, 20)
+        lv.warmup = min(max(args.warmup, 3), 5)
+        levels = levels_report(lv)
     if rank != 0:
         return
     hbm, src = peaks()
@@ -520,6 +556,8 @@ def run_ours(args, ws, rank, local):
         "e2e": e2e,
         "gpu_launches": launches,
         "clocks": clk,
+        "fp32_flux": fp32,
+        "levels": levels,
         "serving": serv,
     }
     print(json.dumps(line), flush=True)

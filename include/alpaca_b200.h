@@ -315,6 +315,19 @@ int alp_engine_step(alp_engine *e, int n);
  * may be null. */
 int alp_engine_get_case(alp_engine *e, int case_id, double *h_blocks, double *t, int *steps);
 
+/* alp_engine_add_case / alp_engine_get_case with the blocks' interiors only:
+ * h_interior [nb][NE][16][16][16] (16^dim cells per field, C order), which is
+ * all the engine keeps of a case (its pools' halos are never read while
+ * stepping), so a transfer moves 16^3 instead of 24^3 cells per field in 3D.
+ * The copy is staged in the engine's own device scratch and placed into (or
+ * taken from) the pool by a kernel on the engine stream; both calls
+ * synchronise that stream. */
+int alp_engine_add_case_interior(alp_engine *e, const alp_material *mat, double cell_size,
+                                 double cfl, double t0, double t_end, int max_steps, int nb,
+                                 const int *h_nbr26, const double *h_interior, int *case_id);
+int alp_engine_get_case_interior(alp_engine *e, int case_id, double *h_interior, double *t,
+                                 int *steps);
+
 /* Checkpoint and resume of one case: what the reference's restart file keeps
  * of a simulation (RestartManager::WriteRestartFile / RestoreSimulation,
  * input_output/restart_manager.h:66-68: the time, and every node's

@@ -97,6 +97,7 @@ struct alp_engine {
   std::vector<int> h_torder, h_case_nb;  // staging of the tile path's orders and case sizes
   std::vector<CaseState> h_case_state;  // staging for case records sent to the device
   int nwork = 0;
+  int compactions = 0;  // times the live cases were moved together (compact)
 
   long long dstride() const { return (long long)ne * faces; }
   long long stride() const { return dstride() * dim; }
@@ -324,17 +325,74 @@ struct alp_engine {
                                   std::to_string(e) + "); the step results are not valid");
   }
 
+  // A range of n slots: the first free range that holds it; when the free
+  // slots suffice only in total, the live cases are compacted first.
   int alloc_range(int n, int *first) {
-    for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
-      if (it->second >= n) {
-        *first = it->first;
-        int const rest = it->second - n, start = it->first + n;
-        free_ranges.erase(it);
-        if (rest > 0) free_ranges[start] = rest;
-        return ALP_OK;
+    for (int pass = 0; pass < 2; ++pass) {
+      for (auto it = free_ranges.begin(); it != free_ranges.end(); ++it) {
+        if (it->second >= n) {
+          *first = it->first;
+          int const rest = it->second - n, start = it->first + n;
+          free_ranges.erase(it);
+          if (rest > 0) free_ranges[start] = rest;
+          return ALP_OK;
+        }
       }
+      int total = 0;
+      for (auto const &r : free_ranges) total += r.second;
+      if (pass > 0 || total < n) break;
+      if (int rc = compact()) return rc;
     }
-    return fail(ALP_ERR_CAPACITY, "no contiguous free block range of the requested size");
+    return fail(ALP_ERR_CAPACITY, "not enough free block slots for the case");
+  }
+
+  // Moves the live cases down, in slot order, so that they occupy slots
+  // [0, used) and the free slots form one range at the end. Between steps a
+  // case's state lives in U alone (B and C hold stage values within a step),
+  // so U moves on the stream (in pieces no longer than the shift, so that no
+  // copy overlaps itself); the block metadata and the neighbour rows move on
+  // the host mirrors (neighbours are blocks of the same case, so their slots
+  // shift by the same amount) and are uploaded again.
+  int compact() {
+    std::vector<int> order;
+    for (int c = 0; c < max_cases; ++c)
+      if (case_rec[c].live) order.push_back(c);
+    std::sort(order.begin(), order.end(),
+              [&](int a, int b) { return case_rec[a].first < case_rec[b].first; });
+    size_t const blk = (size_t)ne * cells;
+    int next = 0;
+    for (int c : order) {
+      CaseRec &r = case_rec[c];
+      int const shift = r.first - next;
+      if (shift > 0) {
+        for (int b = 0; b < r.nb; b += shift) {
+          int const n = std::min(shift, r.nb - b);
+          ALP_CUDA(cudaMemcpyAsync(U + blk * (next + b), U + blk * (r.first + b),
+                                   blk * n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+        }
+        for (int b = 0; b < r.nb; ++b) {
+          h_meta[next + b] = h_meta[r.first + b];
+          for (int s = 0; s < 26; ++s) {
+            int const nb = h_nbr26[(size_t)(r.first + b) * 26 + s];
+            h_nbr26[(size_t)(next + b) * 26 + s] = nb < 0 ? nb : nb - shift;
+          }
+        }
+        r.first = next;
+      }
+      next += r.nb;
+    }
+    if (next > 0) {
+      ALP_CUDA(cudaMemcpyAsync(meta, h_meta.data(), sizeof(BlockMeta) * next,
+                               cudaMemcpyHostToDevice, stream));
+      ALP_CUDA(cudaMemcpyAsync(nbr26, h_nbr26.data(), sizeof(int) * 26 * (size_t)next,
+                               cudaMemcpyHostToDevice, stream));
+      // the host mirrors are changed again by later calls: the copies finish first
+      ALP_CUDA(cudaStreamSynchronize(stream));
+    }
+    free_ranges.clear();
+    if (next < capacity) free_ranges[next] = capacity - next;
+    ++compactions;
+    return rebuild_work();
   }
 
   void free_range(int first, int n) {

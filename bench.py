@@ -35,6 +35,7 @@ B_ALG_3D = 320.0  # algorithmic HBM bytes per 3D cell-update (64 * N_eq, FP64 st
 # by the operation-counting build of the oracle on a seeded one-block case;
 # tests/test_oracle.py::test_op_counts_match_bench_constants re-counts them.
 FLOPS_PER_CELL_UPDATE_3D = {"fvchar": 15767, "fvprim": 10192, "fsroe": 22478}
+FLOPS_PER_CELL_UPDATE_2D = {"fvchar": 8004, "fvprim": 5448, "fsroe": 10605}
 # DRAM bytes per SSP-RK3 step of the 128^3 workload (sum of dram__bytes_read.sum
 # and dram__bytes_write.sum over the step's kernels, one ncu capture; summary in
 # profiles/step_fvchar_128cubed.md)
@@ -77,6 +78,9 @@ def parse():
     p.add_argument("--levels", action="store_true",
                    help="multi-level batching: 3-level spherical-shock hierarchy with local "
                         "time stepping (one line; steps are macro steps)")
+    p.add_argument("--levels-n0", type=int, default=4,
+                   help="level-0 nodes per dimension of that hierarchy (4: 8 / 294 / 1232 "
+                        "leaves; 2, a small case for profiling: 0 / 31 / 264)")
     return p.parse_args()
 
 
@@ -249,42 +253,117 @@ def fp64_peak():
     return v.value
 
 
+def serving_bound(reqs, one_at_a_time_makespan_s, fp64_tflops):
+    """Lower bound on the makespan of a request stream: the FP64 operations of
+    all its cell-updates (the reference algorithm's count per 2D / 3D
+    cell-update, FV characteristic) at the measured FP64 peak, and the last
+    arrival. Against the one-at-a-time makespan it bounds the cases/s gain any
+    batching can reach, and gives the throughput a 3x gain would need."""
+    flops = sum(r.blocks * 16 ** r.dim * r.max_steps *
+                (FLOPS_PER_CELL_UPDATE_3D if r.dim == 3 else FLOPS_PER_CELL_UPDATE_2D)["fvchar"]
+                for r in reqs)
+    cu = sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs)
+    work_floor = flops / (fp64_tflops * 1e12) if fp64_tflops else None
+    last = max(r.arrival_s for r in reqs)
+    floor = max(work_floor or 0.0, last)
+    return {"cell_updates": int(cu), "fp64_operations": float(flops),
+            "fp64_peak_tflops": fp64_tflops, "work_floor_makespan_s": work_floor,
+            "last_arrival_s": last, "floor_makespan_s": floor,
+            "one_at_a_time_makespan_s": one_at_a_time_makespan_s,
+            "max_cases_per_s_vs_one_at_a_time": one_at_a_time_makespan_s / floor,
+            "three_x_reachable_in_fp64": one_at_a_time_makespan_s / floor >= 3.0,
+            "cell_updates_per_s_needed_for_3x": 3.0 * cu / one_at_a_time_makespan_s}
+
+
 def serving_report(args):
-    """Serving form: one seeded request stream (2D four-quadrant problems and 3D
+    """Serving form: seeded request streams (2D four-quadrant problems and 3D
     gas / water blasts, log-uniform 4-2048 blocks, 200-2000 steps, Poisson
-    arrivals at 50/s) served one case at a time in FP64, and with continuous
-    batching in FP64 and in the FP32-flux form, every resident case stepping or
-    shortest remaining work first (--step-set-cells stepping together); time-
-    to-solution percentiles and cases/s per mode."""
+    arrivals at 10, 50 and 200 requests/s) served one case at a time in FP64,
+    and with continuous batching in FP64 and in the FP32-flux form (at 50/s also
+    shortest remaining work first, --step-set-cells stepping together); time-
+    to-solution percentiles and cases/s per mode, and the work bound of each
+    stream (serving_bound)."""
     import numpy as np
 
     from alpaca_b200 import api, serving
     from alpaca_b200 import native as N
-    reqs = serving.request_stream(args.serving_requests, seed=11, rate_hz=50.0)
     budget = 160 << 30
-    out = {"requests": len(reqs), "arrival_rate_hz": 50.0, "hbm_budget_gb": 160,
-           "mix": {k: sum(1 for r in reqs if r.kind == k) for k in
-                   ("quadrants2d", "blast3d_gas", "blast3d_water")},
-           "cell_updates": int(sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs))}
-    out["step_set_cells"] = float(args.step_set_cells)
-    modes = (("one_at_a_time_fp64", N.FP64, True, False), ("batched_fp64", N.FP64, False, False),
-             ("batched_fp32_flux", N.FP32_FLUX, False, False),
-             ("batched_shortest_first_fp64", N.FP64, False, True),
-             ("batched_shortest_first_fp32_flux", N.FP32_FLUX, False, True))
-    for name, prec, one, srpt in modes:
-        res, mk, _ = api.serve(reqs, budget, precision=prec, one_at_a_time=one,
-                               shortest_first=srpt, step_set_cells=out["step_set_cells"])
-        tts = np.array([r["finished_s"] - r["arrival_s"] for r in res])
-        ok = sum(1 for r in res if r["status"] == 0)
-        out[name] = {"cases_per_s": ok / mk, "makespan_s": mk, "p50_tts_s": float(np.percentile(tts, 50)),
-                     "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok,
-                     "cell_updates_per_s": out["cell_updates"] / mk}
-    base = out["one_at_a_time_fp64"]
-    for k, _, one, _ in modes:
-        if not one:
-            out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base["cases_per_s"]
-            out[k]["p50_tts_vs_one_at_a_time"] = out[k]["p50_tts_s"] / base["p50_tts_s"]
+    fp64 = fp64_peak()
+    base_modes = (("one_at_a_time_fp64", N.FP64, True, False), ("batched_fp64", N.FP64, False, False),
+                  ("batched_fp32_flux", N.FP32_FLUX, False, False))
+    srpt_modes = (("batched_shortest_first_fp64", N.FP64, False, True),
+                  ("batched_shortest_first_fp32_flux", N.FP32_FLUX, False, True))
+
+    def serve_stream(rate, modes):
+        reqs = serving.request_stream(args.serving_requests, seed=11, rate_hz=rate)
+        out = {"requests": len(reqs), "arrival_rate_hz": rate, "hbm_budget_gb": 160,
+               "mix": {k: sum(1 for r in reqs if r.kind == k) for k in
+                       ("quadrants2d", "blast3d_gas", "blast3d_water")},
+               "cell_updates": int(sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs)),
+               "step_set_cells": float(args.step_set_cells)}
+        for name, prec, one, srpt in modes:
+            res, mk, _ = api.serve(reqs, budget, precision=prec, one_at_a_time=one,
+                                   shortest_first=srpt, step_set_cells=out["step_set_cells"])
+            tts = np.array([r["finished_s"] - r["arrival_s"] for r in res])
+            ok = sum(1 for r in res if r["status"] == 0)
+            out[name] = {"cases_per_s": ok / mk, "makespan_s": mk,
+                         "p50_tts_s": float(np.percentile(tts, 50)),
+                         "p99_tts_s": float(np.percentile(tts, 99)), "completed": ok,
+                         "cell_updates_per_s": out["cell_updates"] / mk}
+        base = out["one_at_a_time_fp64"]
+        for k, _, one, _ in modes:
+            if not one:
+                out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base["cases_per_s"]
+                out[k]["p50_tts_vs_one_at_a_time"] = out[k]["p50_tts_s"] / base["p50_tts_s"]
+        out["bound"] = serving_bound(reqs, base["makespan_s"], fp64)
+        return out
+
+    out = serve_stream(50.0, base_modes + srpt_modes)
+    out["rates"] = {"10": serve_stream(10.0, base_modes), "200": serve_stream(200.0, base_modes)}
     return out
+
+
+def water_failure_outcome(steps: int = 200):
+    """The stated water configuration (spheres up to 1e9 Pa) run for `steps`
+    SSP-RK3 steps in FP64 and in the FP32-flux form: where the case stops
+    (ALP_ERR_NUMERIC: a cell whose stiffened-gas sound speed is not real, or a
+    non-positive density) and what fails there, read from the state at the
+    stop: cells with p + B <= 0 (tension beyond the stiffened-gas limit -B),
+    with rho <= 0, with non-finite values."""
+    import numpy as np
+
+    from alpaca_b200 import api, cases
+    from alpaca_b200 import native as N
+    case = cases.water_spheres(8, seed=3, p_max=1e9, steps=steps)
+    I = cases.interior(3)
+    rows = []
+    for prec in (N.FP64, N.FP32_FLUX):
+        eng = api.Engine(3, "fvchar", precision=prec, capacity_blocks=case.grid.nb, max_cases=1)
+        cid = eng.add_case(case, max_steps=steps)
+        eng.run_to_end(chunk=50)
+        out = np.empty_like(case.u)
+        t = C.c_double()
+        st = C.c_int()
+        rc = N.lib().alp_engine_get_case(eng.h, cid, out.ctypes.data_as(C.POINTER(C.c_double)),
+                                         C.byref(t), C.byref(st))
+        eng.close()
+        u = out[I]
+        rho, E, m = u[:, 0], u[:, 1], u[:, 2:5]
+        with np.errstate(all="ignore"):
+            ke = 0.5 * (m ** 2).sum(axis=1) / rho
+            p = (case.gamma - 1.0) * (E - ke) - case.gamma * case.B
+        finite = np.isfinite(u).all(axis=1)
+        row = {"case": "stiffened-gas water 128^3, spheres up to 1e9 Pa", "variant": "fvchar",
+               "precision": "fp64" if prec == N.FP64 else "fp32-flux", "steps_asked": steps,
+               "status": "ALP_ERR_NUMERIC" if rc == N.ALP_ERR_NUMERIC else
+                         ("ok" if rc == N.ALP_OK else f"rc {rc}"),
+               "steps_done": st.value, "t": t.value,
+               "cells_p_plus_B_nonpositive": int(((p + case.B <= 0) & finite).sum()),
+               "cells_rho_nonpositive": int((rho <= 0).sum()),
+               "cells_nonfinite": int((~finite).sum()),
+               "min_p_over_B": float(np.nanmin(np.where(finite, p, np.nan)) / case.B)}
+        rows.append(row)
+    return rows
 
 
 def precision_report(steps: int = 200, emit=None):
@@ -356,7 +435,7 @@ def levels_report(args):
     import torch
 
     from alpaca_b200 import api, cases
-    case = cases.spherical_shock_levels()
+    case = cases.spherical_shock_levels(n0=getattr(args, "levels_n0", 4))
     prec = 1 if args.precision == "fp32" else 0
     eng = api.LevelEngine(case, args.variant, precision=prec)
     info = eng.info()
@@ -573,6 +652,8 @@ def main():
             import torch
             torch.cuda.set_device(local)
             precision_report(emit=lambda row: print(json.dumps(row), flush=True))
+            for row in water_failure_outcome():
+                print(json.dumps(row), flush=True)
         elif args.levels:
             import torch
             torch.cuda.set_device(local)

@@ -219,23 +219,26 @@ def test_sod_physics_sanity():
 
 # ---- 4. operation counts (the FP64 compute ceiling of the path) --------------
 
-def test_op_counts_match_bench_constants():
+@pytest.mark.parametrize("dim", [2, 3])
+def test_op_counts_match_bench_constants(dim):
     """The operation-counting build computes the restatement's results bit for
-    bit, and its flops per 3D cell-update are the constants bench.py reports."""
+    bit, and its flops per 2D / 3D cell-update are the constants bench.py
+    reports (the 2D ones bound the serving streams' makespan)."""
     import bench
-    case = cases.fourier_shock(1, dim=3, seed=5)
+    case = cases.fourier_shock(1, dim=dim, seed=5)
     u = filled(case)
-    for variant, expected in bench.FLOPS_PER_CELL_UPDATE_3D.items():
-        O = oracle.OpCounting(3, variant)
-        a = oracle.Restatement(3, variant).space_rhs(u, case.gamma, 0.0, False,
-                                                     case.grid.cell_size)[3]
+    table = bench.FLOPS_PER_CELL_UPDATE_3D if dim == 3 else bench.FLOPS_PER_CELL_UPDATE_2D
+    for variant, expected in table.items():
+        O = oracle.OpCounting(dim, variant)
+        a = oracle.Restatement(dim, variant).space_rhs(u, case.gamma, 0.0, False,
+                                                       case.grid.cell_size)[3]
         b = O.space_rhs(u, case.gamma, 0.0, False, case.grid.cell_size)[3]
         assert np.array_equal(a, b)
         O.reset()
         O.run(case.u, case.grid.nbr, case.gamma, 0.0, False, case.grid.cell_size, case.cfl,
               1e300, max_steps=1)
         c = O.counts()
-        flops = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / 4096
+        flops = (c["add"] + c["mul"] + c["div"] + c["sqrt"]) / 16 ** dim
         assert abs(flops - expected) <= 0.01 * expected, (variant, flops)
 
 

@@ -98,7 +98,9 @@ class Engine:
 
     def __init__(self, dim: int, variant: str = "fvchar", precision: int = N.FP64,
                  capacity_blocks: int = 1024, max_cases: int = 64, graph: bool = True,
-                 strict: bool = False):
+                 strict: bool = False, elastic: bool = False):
+        """elastic: pools reserved for capacity_blocks but backed only by
+        reserve() (alp_engine_create_elastic)."""
         self.dim = dim
         self.ne = dim + 2
         self.variant = variant
@@ -107,8 +109,8 @@ class Engine:
         # a variant name, or an alp_scheme selection as it is
         sch = variant if isinstance(variant, N.Scheme) else N.Scheme.make(variant, precision)
         h = C.c_void_p()
-        self._check(self.lib.alp_engine_create(dim, C.byref(sch), capacity_blocks, max_cases,
-                                               C.byref(h)))
+        create = self.lib.alp_engine_create_elastic if elastic else self.lib.alp_engine_create
+        self._check(create(dim, C.byref(sch), capacity_blocks, max_cases, C.byref(h)))
         self.h = h
         self.nb = {}
         if not graph:
@@ -116,6 +118,17 @@ class Engine:
 
     def _check(self, rc):
         N.check(rc, self.strict)
+
+    def reserve(self, capacity_blocks: int):
+        """Backs exactly that many block slots of an elastic engine."""
+        self._check(self.lib.alp_engine_reserve(self.h, capacity_blocks))
+
+    def capacity(self) -> dict:
+        cap, used = C.c_int(), C.c_int()
+        nbytes = C.c_size_t()
+        self._check(self.lib.alp_engine_capacity(self.h, C.byref(cap), C.byref(used),
+                                                 C.byref(nbytes)))
+        return {"blocks": cap.value, "used": used.value, "bytes": nbytes.value}
 
     def close(self):
         if getattr(self, "h", None):
@@ -372,7 +385,7 @@ class LevelEngine:
 
 
 def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: int = N.FP64,
-          share_3d: float = 0.9, max_cases: int = 256, steps_per_poll: int = 8,
+          max_cases: int = 256, steps_per_poll: int = 8,
           one_at_a_time: bool = False, keep_results: bool = False, shortest_first: bool = False,
           step_set_cells: float = float(1 << 21), abort_file: str | None = None):
     """Runs the C++ request loop (alp_serve) over a list of serving.Request
@@ -414,7 +427,6 @@ def serve(requests, hbm_budget_bytes: int, variant: str = "fvchar", precision: i
     res = (N.Result * n)()
     cfg = N.ServerConfig()
     cfg.hbm_budget_bytes = int(hbm_budget_bytes)
-    cfg.share_3d = share_3d
     cfg.scheme = N.Scheme.make(variant, precision)
     cfg.max_cases = max_cases
     cfg.steps_per_poll = steps_per_poll

@@ -22,6 +22,7 @@ PROBE_LIB = os.path.join(HERE, "libalpaca_b200_probe.so")
 # CUDA arithmetic follows the reference's operation order bit for bit.
 STRICT_LIB = os.path.join(HERE, "libalpaca_b200_strict.so")
 SOURCES = ["kernels.cu", "capi.cu", "server.cu", "levels.cu", "static_scratch.cu", "ic_expr.cu",
+           "elastic.cu",
            "tile_step.cu", "tile_step_fvchar.cu", "tile_step_fvprim.cu", "tile_step_fsroe.cu"]
 PROBE_SOURCES = ["probe.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

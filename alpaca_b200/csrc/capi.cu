@@ -368,23 +368,13 @@ int engine_set_hold(alp_engine *e, int case_id, int hold) {
 
 }  // namespace alp
 
-extern "C" {
+namespace {
 
-size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
-  if (dim < 1 || dim > 3) return 0;
-  size_t const ne = dim + 2;
-  size_t const blk = ne * cells_of(dim) * sizeof(double);
-  size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double) +
-                      ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
-  // the fused tile path's flags, orders and case sizes (3D)
-  size_t const tiles = dim == 3 ? sizeof(int) * (2 + 4 * (size_t)capacity_blocks + 3 * (size_t)max_cases) : 0;
-  return (size_t)capacity_blocks *
-             (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
-         (size_t)max_cases * sizeof(CaseState) + tiles;
-}
-
-int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
-                      alp_engine **out) {
+// Engine with block tables for capacity_blocks slots. Fixed: the pools and
+// scratch are allocated for all of them. Elastic: they are reserved for all of
+// them and backed by nothing until alp_engine_reserve (no fused tile path).
+int engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
+                  bool elastic, alp_engine **out) {
   if (!out) return fail(ALP_ERR_INVALID, "out is null");
   *out = nullptr;
   if (dim < 1 || dim > 3) return fail(ALP_ERR_INVALID, "dim must be 1, 2 or 3");
@@ -399,35 +389,47 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   e->selection = *scheme;
   e->opt = scheme_options(scheme);
   e->rk2 = scheme->time_integrator == ALP_RK2;
-  e->capacity = capacity_blocks;
+  e->elastic = elastic;
+  e->slots_max = capacity_blocks;
+  e->capacity = elastic ? 0 : capacity_blocks;
   e->max_cases = max_cases;
   e->ne = dim + 2;
   e->cells = cells_of(dim);
   e->faces = faces_of(dim);
-  size_t const blk = (size_t)e->ne * e->cells;
   cudaError_t err = cudaSuccess;
+  int erc = ALP_OK;
   auto grab = [&](void **p, size_t bytes) {
     if (err == cudaSuccess) err = cudaMalloc(p, bytes);
   };
-  grab((void **)&e->U, blk * capacity_blocks * sizeof(double));
-  grab((void **)&e->UB, blk * capacity_blocks * sizeof(double));
-  grab((void **)&e->UC, blk * capacity_blocks * sizeof(double));
   // The strict build reproduces the reference's three-order symmetric flux
   // sum, so it keeps the face-flux arrays; the fast build sweeps pencils.
   // Both stepping paths keep their scratch so the autotuner can switch; the
   // strict build always uses the face-flux path, whose three-order symmetric
   // flux sum matches the reference bit for bit.
+  // R also stages interior-only case transfers (alp_engine_*_case_interior).
   e->path = 1;
-  grab((void **)&e->F, (size_t)e->stride() * capacity_blocks * sizeof(double));
-  // R also stages interior-only case transfers (alp_engine_*_case_interior)
-  grab((void **)&e->R, (size_t)e->ne * interior_of(dim) * capacity_blocks * sizeof(double));
+  double **big[5] = {&e->U, &e->UB, &e->UC, &e->F, &e->R};
+  for (int k = 0; k < 5; ++k) {
+    size_t const bytes = e->slot_bytes(k) * (size_t)capacity_blocks;
+    if (!elastic) {
+      grab((void **)big[k], bytes);
+    } else if (erc == ALP_OK && err == cudaSuccess) {
+      erc = alp::elastic_reserve(e->ea[k], bytes);
+      *big[k] = reinterpret_cast<double *>(e->ea[k].base);
+    }
+  }
+  if (erc != ALP_OK) {
+    e->release();
+    delete e;
+    return erc;
+  }
   grab((void **)&e->meta, sizeof(BlockMeta) * capacity_blocks);
   grab((void **)&e->nbr26, sizeof(int) * 26 * capacity_blocks);
   grab((void **)&e->work, sizeof(int) * capacity_blocks);
   grab((void **)&e->cases, sizeof(CaseState) * max_cases);
   grab((void **)&e->glf, sizeof(unsigned long long) * 4 * max_cases);
   // fused tile stages: 3D, the compiled default schemes (WENO5, HLLC/Einfeldt, Roe)
-  bool const tiles = dim == 3 && e->opt.is_default();
+  bool const tiles = dim == 3 && e->opt.is_default() && !elastic;
   if (tiles) {
     grab((void **)&e->tsync, sizeof(int) * (2 + (size_t)capacity_blocks + 2 * (size_t)max_cases));
     grab((void **)&e->torder, sizeof(int) * 3 * (size_t)capacity_blocks);
@@ -483,10 +485,60 @@ int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, in
   }
   e->h_meta.assign(capacity_blocks, BlockMeta{});
   e->h_nbr26.assign((size_t)capacity_blocks * 26, -1);
-  e->free_ranges[0] = capacity_blocks;
+  if (e->capacity > 0) e->free_ranges[0] = e->capacity;
   e->case_rec.assign(max_cases, {});
   e->h_case_state.assign(max_cases, CaseState{});
   *out = e;
+  return ALP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t alp_engine_bytes(int dim, int capacity_blocks, int max_cases) {
+  if (dim < 1 || dim > 3) return 0;
+  size_t const ne = dim + 2;
+  size_t const blk = ne * cells_of(dim) * sizeof(double);
+  size_t const flux = (size_t)dim * ne * faces_of(dim) * sizeof(double) +
+                      ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
+  // the fused tile path's flags, orders and case sizes (3D)
+  size_t const tiles = dim == 3 ? sizeof(int) * (2 + 4 * (size_t)capacity_blocks + 3 * (size_t)max_cases) : 0;
+  return (size_t)capacity_blocks *
+             (3 * blk + flux + sizeof(BlockMeta) + 26 * sizeof(int) + sizeof(int)) +
+         (size_t)max_cases * sizeof(CaseState) + tiles;
+}
+
+int alp_engine_create(int dim, const alp_scheme *scheme, int capacity_blocks, int max_cases,
+                      alp_engine **out) {
+  return engine_create(dim, scheme, capacity_blocks, max_cases, false, out);
+}
+
+int alp_engine_create_elastic(int dim, const alp_scheme *scheme, int max_blocks, int max_cases,
+                              alp_engine **out) {
+  return engine_create(dim, scheme, max_blocks, max_cases, true, out);
+}
+
+int alp_engine_reserve(alp_engine *e, int capacity_blocks) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  return e->set_capacity(capacity_blocks);
+}
+
+int alp_engine_capacity(alp_engine *e, int *capacity_blocks, int *used_blocks,
+                        size_t *pool_bytes) {
+  if (!e) return fail(ALP_ERR_INVALID, "null engine");
+  if (capacity_blocks) *capacity_blocks = e->capacity;
+  if (used_blocks) {
+    int u = 0;
+    for (auto const &c : e->case_rec)
+      if (c.live) u += c.nb;
+    *used_blocks = u;
+  }
+  if (pool_bytes) {
+    size_t b = 0;
+    for (int k = 0; k < 5; ++k) b += e->slot_bytes(k) * (size_t)e->capacity;
+    *pool_bytes = e->elastic ? e->mapped_bytes() : b;
+  }
   return ALP_OK;
 }
 

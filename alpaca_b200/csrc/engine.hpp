@@ -15,6 +15,24 @@
 namespace alp {
 int fail(int code, std::string const &msg);
 int cuda_fail(cudaError_t e, char const *where);
+
+// A device array that grows and shrinks in place (elastic.cu): its virtual
+// range is reserved for the largest size, physical memory is mapped into it
+// in chunks of elastic_chunk_bytes() from the start.
+struct ElasticArray {
+  unsigned long long base = 0;  // reserved virtual address
+  size_t reserved = 0;          // bytes of virtual range
+  size_t mapped = 0;            // bytes backed from base
+  int device = 0;
+  std::vector<unsigned long long> chunks;  // physical allocation handles, in order
+};
+size_t elastic_chunk_bytes();
+int elastic_reserve(ElasticArray &a, size_t bytes);
+// Maps or unmaps whole chunks at the end so that the array holds at least
+// `bytes` with the fewest chunks; the caller makes sure nothing in flight
+// touches a range it unmaps.
+int elastic_resize(ElasticArray &a, size_t bytes);
+void elastic_release(ElasticArray &a);
 }  // namespace alp
 
 #define ALP_CUDA(call)                                        \
@@ -45,6 +63,7 @@ struct alp_engine {
   alp::SchemeOptions opt;  // run-time selected schemes (face-flux path only)
   int rk2 = 0;             // 1: TVD-RK2 (2 stages, face-flux paths), 0: SSP-RK3
   int capacity = 0, max_cases = 0;
+  int slots_max = 0;  // slots of the per-block tables (= capacity unless elastic)
   int ne = 5, cells = 0, faces = 0;
   double *U = nullptr, *UB = nullptr, *UC = nullptr;
   double *F = nullptr;  // face fluxes [slot][dim][NE][faces] (face-flux path)
@@ -142,9 +161,9 @@ struct alp_engine {
   // flags and counters of the launch start at zero, the error word is kept.
   int record_tiles(int n, bool trial) {
     if (nwork == 0 || n <= 0) return ALP_OK;
-    int *dtflag = tsync + 2 + capacity;
+    int *dtflag = tsync + 2 + slots_max;
     ALP_CUDA(cudaMemsetAsync(tsync, 0, sizeof(int), stream));
-    ALP_CUDA(cudaMemsetAsync(tsync + 2, 0, sizeof(int) * ((size_t)capacity + 2 * max_cases), stream));
+    ALP_CUDA(cudaMemsetAsync(tsync + 2, 0, sizeof(int) * ((size_t)slots_max + 2 * max_cases), stream));
     Launch L{dim, scheme, precision, U, work, nwork, meta, BlockMeta{}, stream};
     ALP_CUDA(launch_signal_speed(L, cases, nullptr));
     ALP_CUDA(launch_dt_finalize(cases, max_cases, stream, dtflag));
@@ -411,14 +430,95 @@ struct alp_engine {
     }
   }
 
+  // ---- elastic engines (alp_engine_create_elastic): the block pools U, UB,
+  // UC and the scratch F, R are elastic arrays; `capacity` is the number of
+  // slots backed by memory, slots_max the reservation.
+  bool elastic = false;
+  alp::ElasticArray ea[5];  // U, UB, UC, F, R
+
+  size_t slot_bytes(int k) const {
+    size_t const blk = (size_t)ne * cells * sizeof(double);
+    if (k < 3) return blk;
+    if (k == 3) return (size_t)stride() * sizeof(double);
+    return (size_t)ne * (dim == 3 ? 4096 : (dim == 2 ? 256 : 16)) * sizeof(double);
+  }
+  // device bytes the elastic arrays take when n slots are backed
+  size_t elastic_bytes(int n) const {
+    size_t const q = alp::elastic_chunk_bytes();
+    size_t b = 0;
+    for (int k = 0; k < 5; ++k) b += ((size_t)n * slot_bytes(k) + q - 1) / q * q;
+    return b;
+  }
+  size_t mapped_bytes() const {
+    size_t b = 0;
+    for (auto const &a : ea) b += a.mapped;
+    return b;
+  }
+  // one past the highest slot a live case holds
+  int used_slots() const {
+    int top = 0;
+    for (auto const &c : case_rec)
+      if (c.live) top = std::max(top, c.first + c.nb);
+    return top;
+  }
+  // Backs exactly n slots (compacting the cases first when they reach beyond
+  // n); refused when the cases need more than n slots.
+  int set_capacity(int n) {
+    if (!elastic) return fail(ALP_ERR_INVALID, "the engine's pools are not elastic");
+    if (n < 0 || n > slots_max) return fail(ALP_ERR_CAPACITY, "beyond the engine's reservation");
+    if (used_slots() > n) {
+      if (int rc = compact()) return rc;
+      if (used_slots() > n) return fail(ALP_ERR_CAPACITY, "the resident cases need more slots");
+    }
+    // nothing in flight may touch a range that is unmapped
+    ALP_CUDA(cudaStreamSynchronize(stream));
+    ALP_CUDA(cudaStreamSynchronize(stream2));
+    int const old = capacity;
+    for (int k = 0; k < 5; ++k) {
+      if (int rc = alp::elastic_resize(ea[k], (size_t)n * slot_bytes(k))) {
+        // keep every array at the smaller of the two sizes, as `capacity` says
+        int const keep = std::min(old, n);
+        for (int j = 0; j < 5; ++j) alp::elastic_resize(ea[j], (size_t)keep * slot_bytes(j));
+        set_free_tail(keep);
+        return rc;
+      }
+    }
+    set_free_tail(n);
+    return ALP_OK;
+  }
+  // capacity becomes n: free ranges end at n, slots from the old capacity up
+  // to n are free
+  void set_free_tail(int n) {
+    if (n < capacity) {
+      for (auto it = free_ranges.begin(); it != free_ranges.end();) {
+        if (it->first >= n) {
+          it = free_ranges.erase(it);
+        } else {
+          if (it->first + it->second > n) it->second = n - it->first;
+          ++it;
+        }
+      }
+      capacity = n;
+    } else if (n > capacity) {
+      int const old = capacity;
+      capacity = n;
+      free_range(old, n - old);
+    }
+  }
+
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
     if (tile_graph_src) cudaGraphDestroy(tile_graph_src);
-    cudaFree(U);
-    cudaFree(UB);
-    cudaFree(UC);
-    cudaFree(F);
-    cudaFree(R);
+    if (elastic) {
+      if (stream) cudaStreamSynchronize(stream);
+      for (auto &a : ea) alp::elastic_release(a);
+    } else {
+      cudaFree(U);
+      cudaFree(UB);
+      cudaFree(UC);
+      cudaFree(F);
+      cudaFree(R);
+    }
     cudaFree(meta);
     cudaFree(nbr26);
     cudaFree(work);

@@ -7,8 +7,13 @@
 // engine's batched step (one launch per kernel for all resident blocks of all
 // cases, each case with its own dt), and leave the pool when their end time or
 // step budget is reached. The 2D and 3D engines step on their own streams, so
-// their work overlaps on the device. Device memory is sized once from the HBM
-// budget; nothing is allocated while serving. With shortest_first, only the
+// their work overlaps on the device. Their pools share one HBM budget: each
+// engine is elastic (alp_engine_create_elastic), its address range reserved
+// for the whole budget, and a request that does not fit grows its engine's
+// backed slots while the budget allows, after the other engines have given
+// back the slots their cases no longer hold (moving their cases together).
+// Memory is mapped and unmapped only then, never between the polls of a
+// steady batch. With shortest_first, only the
 // resident cases with the least remaining work (cells x steps left) step, up to
 // step_set_cells cells together, and the others are held (they keep their
 // state and take no steps): the GPU stays busy while short cases finish first.
@@ -49,8 +54,6 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
   if (!cfg || (n > 0 && (!reqs || !results))) return fail(ALP_ERR_INVALID, "null argument");
   if (cfg->steps_per_poll <= 0 || cfg->max_cases <= 0)
     return fail(ALP_ERR_INVALID, "steps_per_poll and max_cases must be positive");
-  if (!(cfg->share_3d >= 0.0 && cfg->share_3d <= 1.0))
-    return fail(ALP_ERR_INVALID, "share_3d must lie in [0, 1]");
   if (cfg->shortest_first && !(cfg->step_set_cells > 0.0))
     return fail(ALP_ERR_INVALID, "step_set_cells must be positive");
   bool need[4] = {false, false, false, false};
@@ -59,24 +62,24 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     need[reqs[i].dim] = true;
   }
   nvtx3::scoped_range range{"alp_serve"};  // its engine steps show as alp_engine_step
-  // size the pools from the budget
+  // one budget for the pools of every dimension: each engine may grow to all
+  // of it, and holds memory only for the block slots it backs
   DimPool pool[4];
+  size_t per_block[4] = {0, 0, 0, 0};
   auto cleanup = [&]() {
     for (auto &p : pool)
       if (p.eng) alp_engine_destroy(p.eng);
   };
-  double const share[4] = {0.0, 0.0, 1.0 - cfg->share_3d, cfg->share_3d};
   for (int d = 1; d <= 3; ++d) {
     if (!need[d]) continue;
-    double const s = d == 1 ? 1.0 : (need[2] && need[3] ? share[d] : 1.0);
-    size_t const per_block = alp_engine_bytes(d, 1, 0);
-    size_t const cap = (size_t)(s * (double)cfg->hbm_budget_bytes) / per_block;
+    per_block[d] = alp_engine_bytes(d, 1, 0);
+    size_t const cap = cfg->hbm_budget_bytes / per_block[d];
     if (cap < 1) {
       cleanup();
       return fail(ALP_ERR_CAPACITY, "HBM budget below one block");
     }
-    if (int rc = alp_engine_create(d, &cfg->scheme, (int)std::min<size_t>(cap, 1 << 30),
-                                   cfg->max_cases, &pool[d].eng)) {
+    if (int rc = alp_engine_create_elastic(d, &cfg->scheme, (int)std::min<size_t>(cap, 1 << 30),
+                                           cfg->max_cases, &pool[d].eng)) {
       cleanup();
       return rc;
     }
@@ -84,6 +87,33 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
     pool[d].held.assign(cfg->max_cases, 0);
     pool[d].states.assign(cfg->max_cases, CaseState{});
   }
+  auto blocks_used = [&](int d) {
+    int u = 0;
+    alp_engine_capacity(pool[d].eng, nullptr, &u, nullptr);
+    return u;
+  };
+  auto budget_used = [&]() {
+    size_t b = 0;
+    for (int d = 1; d <= 3; ++d)
+      if (pool[d].eng) b += (size_t)pool[d].eng->capacity * per_block[d];
+    return b;
+  };
+  // Backs enough slots in dimension d's engine for nb more blocks, within the
+  // budget; first the other engines give back what their cases do not hold.
+  // ALP_ERR_CAPACITY when the budget cannot hold it now.
+  auto make_room = [&](int d, int nb) -> int {
+    alp_engine *e = pool[d].eng;
+    int const want = blocks_used(d) + nb;
+    if (want <= e->capacity) return e->set_capacity(e->capacity);  // compacts if needed
+    size_t const extra = (size_t)(want - e->capacity) * per_block[d];
+    if (budget_used() + extra > cfg->hbm_budget_bytes)
+      for (int o = 1; o <= 3; ++o)
+        if (o != d && pool[o].eng && pool[o].eng->capacity > blocks_used(o))
+          if (int rc = pool[o].eng->set_capacity(blocks_used(o))) return rc;
+    if (budget_used() + extra > cfg->hbm_budget_bytes)
+      return fail(ALP_ERR_CAPACITY, "the HBM budget is held by resident cases");
+    return e->set_capacity(want);
+  };
 
 
   std::vector<int> order(n);
@@ -144,14 +174,27 @@ extern "C" int alp_serve(const alp_server_config *cfg, const alp_request *reqs, 
       DimPool &p = pool[r.dim];
       int cid = -1;
       bool const unit = r.units.density == 0.0 && r.units.velocity == 0.0 && r.units.length == 0.0;
-      int const rc =
-          r.ic_type == ALP_IC_PROGRAM
-              ? alp_engine_add_case_expr(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
-                                         r.max_steps, r.nblocks, r.periodic, r.origin,
-                                         unit ? nullptr : &r.units, r.program, &cid)
-              : alp_engine_add_case_ic(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
-                                       r.max_steps, r.nblocks, r.periodic, r.ic_type,
-                                       r.ic_params, r.n_params, &cid);
+      auto add = [&]() {
+        return r.ic_type == ALP_IC_PROGRAM
+                   ? alp_engine_add_case_expr(p.eng, &r.material, r.cell_size, r.cfl, 0.0,
+                                              r.t_end, r.max_steps, r.nblocks, r.periodic,
+                                              r.origin, unit ? nullptr : &r.units, r.program,
+                                              &cid)
+                   : alp_engine_add_case_ic(p.eng, &r.material, r.cell_size, r.cfl, 0.0, r.t_end,
+                                            r.max_steps, r.nblocks, r.periodic, r.ic_type,
+                                            r.ic_params, r.n_params, &cid);
+      };
+      int rc = add();
+      if (rc == ALP_ERR_CAPACITY && p.active < cfg->max_cases) {
+        // the blocks of the request against the budget shared by all engines
+        long long const nb = (long long)r.nblocks[0] * (r.dim > 1 ? r.nblocks[1] : 1) *
+                             (r.dim > 2 ? r.nblocks[2] : 1);
+        int const room = nb * (long long)per_block[r.dim] <= (long long)cfg->hbm_budget_bytes
+                             ? make_room(r.dim, (int)nb)
+                             : ALP_ERR_CAPACITY;
+        if (room == ALP_OK) rc = add();
+        else if (room != ALP_ERR_CAPACITY) rc = room;
+      }
       if (rc == ALP_OK) {
         p.req_of_case[cid] = *it;
         p.held[cid] = 0;

@@ -161,7 +161,7 @@ class Result(C.Structure):
 
 
 class ServerConfig(C.Structure):
-    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("share_3d", C.c_double), ("scheme", Scheme),
+    _fields_ = [("hbm_budget_bytes", C.c_size_t), ("scheme", Scheme),
                 ("max_cases", C.c_int), ("steps_per_poll", C.c_int), ("one_at_a_time", C.c_int),
                 ("shortest_first", C.c_int), ("step_set_cells", C.c_double),
                 ("abort_file", C.c_char_p)]
@@ -188,6 +188,10 @@ _SIGS = {
                                     C.c_double, C.c_double, C.c_double, _D, _V, _S]),
     "alp_rk3_stage": (C.c_int, [C.c_int, _V, _V, _V, C.c_int, C.c_int, C.c_double, _S]),
     "alp_engine_create": (C.c_int, [C.c_int, C.POINTER(Scheme), C.c_int, C.c_int, C.POINTER(_V)]),
+    "alp_engine_create_elastic": (C.c_int, [C.c_int, C.POINTER(Scheme), C.c_int, C.c_int,
+                                            C.POINTER(_V)]),
+    "alp_engine_reserve": (C.c_int, [_V, C.c_int]),
+    "alp_engine_capacity": (C.c_int, [_V, _I, _I, C.POINTER(C.c_size_t)]),
     "alp_engine_destroy": (C.c_int, [_V]),
     "alp_engine_bytes": (C.c_size_t, [C.c_int, C.c_int, C.c_int]),
     "alp_engine_add_case": (C.c_int, [_V, C.POINTER(Material), C.c_double, C.c_double, C.c_double,

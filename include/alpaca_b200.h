@@ -310,6 +310,28 @@ int alp_engine_remove_case(alp_engine *e, int case_id);
  * t_end or whose step budget is spent do no work. Asynchronous. */
 int alp_engine_step(alp_engine *e, int n);
 
+/* An engine whose block pools grow and shrink in place: the pools and their
+ * scratch are reserved (virtual address range) for max_blocks blocks, and
+ * device memory is mapped into them only by alp_engine_reserve, in chunks of
+ * 32 MiB per array. Pointers into the pools stay valid as they change, so
+ * the step's CUDA graph and a caller's stream order need no update. Such an
+ * engine steps on the face-flux path (no fused tile path). Cases are added
+ * as to any engine, within the slots reserved. */
+int alp_engine_create_elastic(int dim, const alp_scheme *scheme, int max_blocks, int max_cases,
+                              alp_engine **out);
+/* Backs exactly capacity_blocks block slots of an elastic engine with device
+ * memory (mapping or unmapping chunks at the pools' end); when the resident
+ * cases reach beyond that, they are moved together first (their order and
+ * results are unchanged). Synchronises the engine's streams. ALP_ERR_CAPACITY
+ * when the cases need more slots, or the device has no memory left (the
+ * engine then keeps the smaller of the two capacities). */
+int alp_engine_reserve(alp_engine *e, int capacity_blocks);
+/* Block slots backed by memory, blocks in use by cases, and the device bytes
+ * of the pools and scratch (what alp_engine_reserve maps, for an elastic
+ * engine); any output may be null. */
+int alp_engine_capacity(alp_engine *e, int *capacity_blocks, int *used_blocks,
+                        size_t *pool_bytes);
+
 /* Copies a case's state (reference layout, halos included) to h_blocks and
  * its time / step count. Synchronises the engine stream. Any of the outputs
  * may be null. */
@@ -486,8 +508,10 @@ typedef struct {
 } alp_result;
 
 typedef struct {
-  size_t hbm_budget_bytes;  /* device memory for case state (all engines) */
-  double share_3d;          /* fraction of the budget given to 3D blocks when both occur */
+  size_t hbm_budget_bytes;  /* device memory for case state, shared by the 2D and 3D
+                               pools: alp_engine_bytes(dim, 1, 0) per backed block slot
+                               (the pools map it in 32 MiB chunks, so the device bytes
+                               exceed it by less than 5 chunks per dimension) */
   alp_scheme scheme;
   int max_cases;            /* resident cases per dimension */
   int steps_per_poll;       /* steps between completion checks */

@@ -151,7 +151,7 @@ def test_serving_budget_bounds_admission(cuda):
     rng = np.random.default_rng(9)
     reqs = [serving.blast_request(rng, 8, 6, water=False) for _ in range(3)]
     per_block = N.lib().alp_engine_bytes(3, 1, 0)
-    res, makespan, _ = api.serve(reqs, 9 * per_block, share_3d=1.0)
+    res, makespan, _ = api.serve(reqs, 9 * per_block)
     assert all(r["status"] == 0 and r["steps"] == 6 for r in res)
     spans = sorted((x["admitted_s"], x["finished_s"]) for x in res)
     for (a0, f0), (a1, _) in zip(spans, spans[1:]):
@@ -176,7 +176,7 @@ def test_serving_request_too_large_is_reported(cuda):
     big = serving.blast_request(rng, 64, 3, water=False)
     small = serving.blast_request(rng, 1, 3, water=False)
     per_block = N.lib().alp_engine_bytes(3, 1, 0)
-    res, _, _ = api.serve([big, small], 8 * per_block, share_3d=1.0)
+    res, _, _ = api.serve([big, small], 8 * per_block)
     assert res[0]["status"] == N.ALP_ERR_CAPACITY
     assert res[1]["status"] == 0 and res[1]["steps"] == 3
 

@@ -163,6 +163,7 @@ def _load(path: str):
     lib.oracle_set_options.argtypes = [C.c_int] * 4
     lib.oracle_prediction.argtypes = [C.c_int, _D, C.c_int, _I, _I, _D]
     lib.oracle_set_time_integrator.argtypes = [C.c_int]
+    lib.oracle_level_halos.argtypes = [C.c_int, _D, C.c_int, _I, _I, _I]
     lib.oracle_levels_run.argtypes = [C.c_int, C.c_int, C.c_int, _D, C.c_int, _I, _I, _I,
                                       C.c_double, C.c_double, C.c_double, C.c_int, C.c_double,
                                       C.c_double, C.c_int, C.c_int, _D, _I, _D]
@@ -275,6 +276,19 @@ class Restatement(_Common):
         if rc:
             raise RuntimeError(f"oracle_run rc={rc}")
         return u, t.value, steps.value, dts[: steps.value].copy()
+
+    def level_halos(self, u, level, coord, n0):
+        """The leaves' face halos of one multi-level snapshot, as a stage of
+        the level step fills them (oracle_level_halos); returns a copy of u."""
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        level = np.ascontiguousarray(level, dtype=np.int32)
+        coord = np.ascontiguousarray(coord, dtype=np.int32).reshape(-1, 3)
+        n0 = np.ascontiguousarray(list(n0) + [1] * (3 - len(n0)), dtype=np.int32)
+        rc = self.lib.oracle_level_halos(self.dim, _dp(u), u.shape[0], _ip(level), _ip(coord),
+                                         _ip(n0))
+        if rc:
+            raise RuntimeError(f"oracle_level_halos rc={rc}")
+        return u
 
     def levels_run(self, u, level, coord, n0, h0, gamma, B, safe, cfl, t_end, max_macro=0,
                    t0=0.0, nthreads=1):
@@ -398,3 +412,36 @@ class Reference(_Common):
         self.lib.ref_run(_dp(u), u.shape[0], _ip(nbr), gamma, B, int(safe), cell_size, cfl, t_end,
                          max_steps, nthreads, C.byref(t), C.byref(steps), _dp(dts))
         return u, t.value, steps.value, dts[: steps.value].copy()
+
+
+class Glue:
+    """ALPACA's own multi-level glue (TopologyManager, Tree, Averager,
+    InternalHaloManager) on one rank, 3D: oracle/_ref/libalpglue_d3.so."""
+
+    _lib = None
+    path = os.path.join(REF_DIR, "libalpglue_d3.so")
+
+    @classmethod
+    def available(cls) -> bool:
+        return os.path.exists(cls.path)
+
+    def __init__(self):
+        cls = type(self)
+        if cls._lib is None:
+            lib = C.CDLL(cls.path)
+            lib.glue_level_halos.restype = C.c_int
+            lib.glue_level_halos.argtypes = [_D, C.c_int, _I, _I, _I]
+            lib.glue_last_error.restype = C.c_char_p
+            cls._lib = lib
+        self.lib = cls._lib
+
+    def level_halos(self, u, level, coord, n0):
+        """Every leaf's buffer after the reference's averaging and level-by-
+        level halo update of one snapshot (levels_glue_harness.cpp)."""
+        u = np.array(u, dtype=np.float64, order="C", copy=True)
+        level = np.ascontiguousarray(level, dtype=np.int32)
+        coord = np.ascontiguousarray(coord, dtype=np.int32).reshape(-1, 3)
+        n0 = np.ascontiguousarray(list(n0) + [1] * (3 - len(n0)), dtype=np.int32)
+        if self.lib.glue_level_halos(_dp(u), u.shape[0], _ip(level), _ip(coord), _ip(n0)):
+            raise RuntimeError(self.lib.glue_last_error().decode())
+        return u

@@ -1820,6 +1820,31 @@ static void level_halos(const Geom *g, const Tree *t, int b, double *dst, double
   }
 }
 
+/* The face halos of every leaf of one snapshot u [nleaf][ne][cells] (interiors
+ * read), as a stage of the level step fills them (level_halos with every
+ * level's values in u): same-level neighbours copied, finer neighbours
+ * averaged, coarser neighbours predicted. Returns tree_build's status. */
+int oracle_level_halos(int dim, double *u, int nleaf, const int *level, const int *coord,
+                       const int *n0) {
+  if (dim < 1 || dim > 3 || nleaf <= 0) return 1;
+  Geom g = make_geom(dim);
+  Tree tr;
+  int const rc = tree_build(&tr, dim, nleaf, level, coord, n0);
+  if (rc) {
+    tree_free(&tr);
+    return rc;
+  }
+  double *src[MAXLEV];
+  for (int l = 0; l < MAXLEV; ++l) src[l] = u;
+  LevelField field;
+  lf_init(&field, &g, &tr, src);
+  /* halos are written, interiors only read: u serves as source and target */
+  for (int b = 0; b < nleaf; ++b) level_halos(&g, &tr, b, u, src, &field);
+  lf_free(&field);
+  tree_free(&tr);
+  return 0;
+}
+
 /* Face neighbour kind of leaf b across face loc (East 0, West 1, North 2,
  * South 3, Top 4, Bottom 5; boundary_specifications.h:56-63): 0 domain face,
  * 1 same-level leaf, 2 refined node (finer leaves), 3 inside a coarser leaf.

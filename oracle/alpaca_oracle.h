@@ -79,6 +79,10 @@ int oracle_run(int dim, int solver, int recon, double *u, int nb,
  * buffer [tc] into a child's cells start .. start + count (even numbers). */
 int oracle_prediction(int dim, const double *parent, int octant, const int *start,
                       const int *count, double *child);
+/* Face halos of every leaf of a multi-level snapshot (same-level copy, finer
+ * neighbours averaged, coarser ones predicted), in place in u. */
+int oracle_level_halos(int dim, double *u, int nleaf, const int *level, const int *coord,
+                       const int *n0);
 int oracle_levels_run(int dim, int solver, int recon, double *u, int nleaf,
                       const int *level, const int *coord, const int *n0, double h0,
                       double gamma, double B, int safe, double cfl, double t_end,

@@ -54,6 +54,13 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       // FP32 form: characteristic projection and WENO5 of the increments
       // U_m - U_i against the face's left cell i (WENO5 is translation
       // invariant and R L = I), the left cell's state added back in double.
+      // The increments are formed in double and converted once each, for all
+      // five characteristic fields.
+      float du[W][NE];
+#pragma unroll
+      for (int m = 0; m < W; ++m)
+#pragma unroll
+        for (int l = 0; l < NE; ++l) du[m][l] = m == C ? 0.0f : float(cons[m][l] - cons[C][l]);
 #pragma unroll
       for (int n = 0; n < NE; ++n) {
         T L[NE];
@@ -66,7 +73,7 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            s = fmaf(L[l], m == C ? 0.0f : float(cons[m][l] - cons[C][l]), s);
+            s = fmaf(L[l], du[m][l], s);
           }
           uc[m] = s;
         }

@@ -72,6 +72,8 @@ def parse():
     p.add_argument("--serving-only", action="store_true",
                    help="run only the serving comparison and print its JSON")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the FP32-flux and multi-level entries of the default line")
     p.add_argument("--path", type=int, default=None,
                    help="stepping candidate to use instead of the autotuner's choice "
                         "(numbered as alp_engine_autotune; for profiling one path)")
@@ -559,7 +561,7 @@ def run_ours(args, ws, rank, local):
     # single GPU: the FP32-flux form and the multi-level batching form timed
     # beside the headline (their own lines come from --precision fp32 / --levels)
     fp32 = levels = None
-    if ws == 1 and args.precision == "fp64":
+    if ws == 1 and args.precision == "fp64" and not args.no_extras and args.path is None:
         eng = api.Engine(3, args.variant, precision=N.FP32_FLUX, capacity_blocks=case.grid.nb,
                          max_cases=1)
         stream = torch.cuda.ExternalStream(eng.stream_handle)

@@ -55,15 +55,21 @@ __device__ __forceinline__ double rsqrt_nr(double x) {
   return y;
 }
 
-// 1/x: IEEE division in the strict build, rcp_nr (double) or the hardware
-// approximate quotient (float) in the fast build.
+// 1/x: IEEE division in the strict build, rcp_nr (double) or the PTX
+// approximate reciprocal (float, one instruction, about 1 ulp) in the fast
+// build.
 __device__ __forceinline__ double inv(double x) {
   if constexpr (ALP_FAST) return rcp_nr(x);
   else return 1.0 / x;
 }
 __device__ __forceinline__ float inv(float x) {
-  if constexpr (ALP_FAST) return __fdividef(1.0f, x);
-  else return 1.0f / x;
+  if constexpr (ALP_FAST) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+  } else {
+    return 1.0f / x;
+  }
 }
 // a / b, where ib is 1/b as returned by inv(b): the strict build divides.
 template <typename T> __device__ __forceinline__ T quot(T a, T b, T ib) {
@@ -251,8 +257,11 @@ template <typename T> __device__ __forceinline__ T weno5_right(T const (&a)[6]) 
 // The ideal weights 0.1, 0.6, 0.3 enter as 1, 6, 3. The result is
 // v3 + num / (6 den); passing the differences of the mirrored stencil without
 // their sign change (g_k' = -g) negates num and leaves den unchanged.
-// Double: alpha_k scaled by t1 t2 t3 (no reciprocal here); float keeps one
-// reciprocal per weight, as products of the t_k leave the float range.
+// alpha_k scaled by t1 t2 t3 (no reciprocal here). In float the t_k are first
+// multiplied by the power of two that brings the largest into [1, 2) (exact:
+// the scale is built from the exponent bits), so the products stay inside the
+// float range; a product that underflows belongs to a weight below 2^-126 of
+// the largest.
 template <typename T> struct Weno5Frac { T num, den; };
 
 template <typename T>
@@ -269,22 +278,25 @@ __device__ __forceinline__ Weno5Frac<T> weno5_frac(T g1, T g2, T g3, T g4, T d1,
   T const r1 = T(5.0) * g2 + T(-2.0) * g1;
   T const r2 = g2 + T(2.0) * g3;
   T const r3 = T(4.0) * g3 - g4;
-  T b1, b2, b3;
-  if constexpr (sizeof(T) == 8) {
-    b1 = t2 * t3;
-    b2 = T(6.0) * (t1 * t3);
-    b3 = T(3.0) * (t1 * t2);
-  } else {
-    b1 = inv(t1);
-    b2 = T(6.0) * inv(t2);
-    b3 = T(3.0) * inv(t3);
+  T u1 = t1, u2 = t2, u3 = t3;
+  if constexpr (sizeof(T) == 4) {
+    unsigned const e = min((__float_as_uint(fmaxf(t1, fmaxf(t2, t3))) >> 23) & 0xffu, 253u);
+    float const sc = __uint_as_float((254u - e) << 23);
+    u1 = t1 * sc;
+    u2 = t2 * sc;
+    u3 = t3 * sc;
   }
+  T const b1 = u2 * u3;
+  T const b2 = T(6.0) * (u1 * u3);
+  T const b3 = T(3.0) * (u1 * u2);
   return {b1 * r1 + b2 * r2 + b3 * r3, b1 + b2 + b3};
 }
 
 // v_l + num_l / (6 den_l) and v_r - num_r / (6 den_r). Double: one reciprocal
 // of the product of the two denominators (each between ~1e-22 and ~1e7 |g|^8,
-// so the product stays in range for differences up to ~1e17).
+// so the product stays in range for differences up to ~1e17). Float: one
+// reciprocal per side (a scaled denominator can be as small as the ratio of two
+// smoothness terms, so the product of two could underflow).
 template <typename T>
 __device__ __forceinline__ void weno5_finish(T v_l, Weno5Frac<T> const &l, T v_r,
                                              Weno5Frac<T> const &r, T &left, T &right) {

@@ -255,12 +255,14 @@ def fp64_peak():
     return v.value
 
 
-def serving_bound(reqs, one_at_a_time_makespan_s, fp64_tflops):
+def serving_bound(reqs, one_at_a_time_makespan_s, fp64_tflops, engine_3d_rate=None):
     """Lower bound on the makespan of a request stream: the FP64 operations of
     all its cell-updates (the reference algorithm's count per 2D / 3D
     cell-update, FV characteristic) at the measured FP64 peak, and the last
     arrival. Against the one-at-a-time makespan it bounds the cases/s gain any
-    batching can reach, and gives the throughput a 3x gain would need."""
+    batching can reach, and gives the throughput a 3x gain would need. With
+    the engine's measured 3D FP64 rate, also the time its 3D work alone takes
+    at that rate (a floor for this engine, 2D work not counted)."""
     flops = sum(r.blocks * 16 ** r.dim * r.max_steps *
                 (FLOPS_PER_CELL_UPDATE_3D if r.dim == 3 else FLOPS_PER_CELL_UPDATE_2D)["fvchar"]
                 for r in reqs)
@@ -268,16 +270,24 @@ def serving_bound(reqs, one_at_a_time_makespan_s, fp64_tflops):
     work_floor = flops / (fp64_tflops * 1e12) if fp64_tflops else None
     last = max(r.arrival_s for r in reqs)
     floor = max(work_floor or 0.0, last)
+    cu3 = sum(r.blocks * 16 ** r.dim * r.max_steps for r in reqs if r.dim == 3)
+    engine = None
+    if engine_3d_rate:
+        floor_e = max(cu3 / engine_3d_rate, last)
+        engine = {"cell_updates_3d": int(cu3), "rate_3d_fp64": engine_3d_rate,
+                  "floor_makespan_s": floor_e,
+                  "max_cases_per_s_vs_one_at_a_time": one_at_a_time_makespan_s / floor_e}
     return {"cell_updates": int(cu), "fp64_operations": float(flops),
             "fp64_peak_tflops": fp64_tflops, "work_floor_makespan_s": work_floor,
             "last_arrival_s": last, "floor_makespan_s": floor,
             "one_at_a_time_makespan_s": one_at_a_time_makespan_s,
             "max_cases_per_s_vs_one_at_a_time": one_at_a_time_makespan_s / floor,
             "three_x_reachable_in_fp64": one_at_a_time_makespan_s / floor >= 3.0,
-            "cell_updates_per_s_needed_for_3x": 3.0 * cu / one_at_a_time_makespan_s}
+            "cell_updates_per_s_needed_for_3x": 3.0 * cu / one_at_a_time_makespan_s,
+            "engine": engine}
 
 
-def serving_report(args):
+def serving_report(args, engine_3d_rate=None):
     """Serving form: seeded request streams (2D four-quadrant problems and 3D
     gas / water blasts, log-uniform 4-2048 blocks, 200-2000 steps, Poisson
     arrivals at 10, 50 and 200 requests/s) served one case at a time in FP64,
@@ -317,7 +327,7 @@ def serving_report(args):
             if not one:
                 out[k]["cases_per_s_vs_one_at_a_time"] = out[k]["cases_per_s"] / base["cases_per_s"]
                 out[k]["p50_tts_vs_one_at_a_time"] = out[k]["p50_tts_s"] / base["p50_tts_s"]
-        out["bound"] = serving_bound(reqs, base["makespan_s"], fp64)
+        out["bound"] = serving_bound(reqs, base["makespan_s"], fp64, engine_3d_rate)
         return out
 
     out = serve_stream(50.0, base_modes + srpt_modes)
@@ -608,7 +618,7 @@ def run_ours(args, ws, rank, local):
     clk = clocks.summary()
     serv = None
     if not args.no_serving and ws == 1:
-        serv = serving_report(args)
+        serv = serving_report(args, value if args.precision == "fp64" else None)
     line = {
         "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,

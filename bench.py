@@ -529,7 +529,7 @@ def run_ours(args, ws, rank, local):
     barrier(ws, dev)
     ms = max_over_ranks(e0.elapsed_time(e1), ws, dev)
     value = cells * args.steps * ws / (ms * 1e-3)
-    _, t_sim, steps_done = eng.get(cid)
+    u_fp64, t_sim, steps_done = eng.get(cid)
     launches = eng.launches(args.steps)
     eng.close()
 
@@ -575,7 +575,7 @@ def run_ours(args, ws, rank, local):
         eng = api.Engine(3, args.variant, precision=N.FP32_FLUX, capacity_blocks=case.grid.nb,
                          max_cases=1)
         stream = torch.cuda.ExternalStream(eng.stream_handle)
-        eng.add_case(case, max_steps=0)
+        fcid = eng.add_case(case, max_steps=0)
         f_chosen, _ = eng.autotune(trial_steps=3)
         eng.step(args.warmup)
         torch.cuda.synchronize()
@@ -585,11 +585,23 @@ def run_ours(args, ws, rank, local):
         g1.record(stream)
         g1.synchronize()
         fms = g0.elapsed_time(g1)
+        # the same case after the same W + K steps in both forms: per-field
+        # relative L1 / Linf of the FP32-flux state against the FP64 one
+        u_fp32, t32, s32 = eng.get(fcid)
         eng.close()
+        I = cases.interior(3)
+        a, b = u_fp32[I], u_fp64[I]
+        errs = {}
+        for f, nm in enumerate(("density", "energy", "momentum_x", "momentum_y", "momentum_z")):
+            d = np.abs(a[:, f] - b[:, f])
+            errs[nm] = {"l1": float(d.sum() / max(np.abs(b[:, f]).sum(), 1e-300)),
+                        "linf": float(d.max() / max(np.abs(b[:, f]).max(), 1e-300))}
         fp32 = {"value": cells * args.steps / (fms * 1e-3), "unit": METRIC,
                 "ms_per_step": fms / args.steps, "steps": args.steps, "warmup": args.warmup,
                 "dtype": "f32-flux/f64-state", "path": CANDIDATES[f_chosen],
-                "vs_fp64": ms / fms}
+                "vs_fp64": ms / fms,
+                "errors_vs_fp64": {"steps": s32, "same_steps": s32 == steps_done,
+                                   "t_fp32": t32, "t_fp64": t_sim, "fields": errs}}
         lv = argparse.Namespace(**vars(args))
         lv.steps = min(args.steps, 20)
         lv.warmup = min(max(args.warmup, 3), 5)

@@ -413,37 +413,6 @@ pencil_kernel(double const *Uin, double const *U0, double *Uout, double *R,
 // divergence, stage update
 // ---------------------------------------------------------------------------
 
-// Flux divergence of interior cell (i, j, k) for field f (space_solver.cpp:131-153):
-// DimensionAwareConsistencyManagedSum(dFx, dFy, dFz) * (1 / cell_size).
-template <int DIM>
-__device__ __forceinline__ double divergence(double const *Fx, double const *Fy,
-                                             double const *Fz, int i, int j, int k,
-                                             double one_cell_size) {
-  using G = Geo<DIM>;
-  return flux_divergence<DIM>(Fx[G::face(i, j + 1, k + 1)], Fx[G::face(i + 1, j + 1, k + 1)],
-                              DIM > 1 ? Fy[G::face(i + 1, j, k + 1)] : 0.0,
-                              DIM > 1 ? Fy[G::face(i + 1, j + 1, k + 1)] : 0.0,
-                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k)] : 0.0,
-                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k + 1)] : 0.0, one_cell_size);
-}
-
-template <int DIM>
-__device__ __forceinline__ void interior_coords(int t, int &i, int &j, int &k) {
-  if constexpr (DIM == 3) {
-    i = t >> 8;
-    j = (t >> 4) & 15;
-    k = t & 15;
-  } else if constexpr (DIM == 2) {
-    i = t >> 4;
-    j = t & 15;
-    k = 0;
-  } else {
-    i = t;
-    j = 0;
-    k = 0;
-  }
-}
-
 template <int DIM>
 __global__ void __launch_bounds__(256)
 divergence_kernel(int const *__restrict__ work, BlockMeta const *__restrict__ meta, BlockMeta def,
@@ -490,20 +459,8 @@ stage_update_kernel(double const *Uin, double const *U0, double *Uout,
   if (!(dt > 0.0)) return;
   int const t = blockIdx.y * blockDim.x + threadIdx.x;
   if (t >= G::INTERIOR) return;
-  int i, j, k;
-  interior_coords<DIM>(t, i, j, k);
-  int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
-  double const ocs = inv(bm.cell_size);
-  RkStage const rk = rk_stage(stage, dt);
-  double const *Fb = F + (long long)item * stride;
-  size_t const base = (size_t)slot * G::BLOCK_DOUBLES + c;
-#pragma unroll
-  for (int f = 0; f < G::NE; ++f) {
-    double const *fx = Fb + f * G::FACES;
-    double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k, ocs);
-    size_t const x = base + (size_t)f * G::CELLS;
-    Uout[x] = rk_apply(rk, Uin[x], rk.first ? 0.0 : U0[x], rhs);
-  }
+  stage_update_cell<DIM>(Uin, U0, Uout, F + (long long)item * stride, dstride, slot, t,
+                         inv(bm.cell_size), rk_stage(stage, dt));
 }
 
 // Stage update from a reference-layout right-hand-side buffer.

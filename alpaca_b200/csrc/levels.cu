@@ -57,6 +57,7 @@
 #include "../../include/alpaca_b200.h"
 #include "engine.hpp"
 #include "numerics.cuh"
+#include "step_common.cuh"
 
 namespace {
 
@@ -64,6 +65,10 @@ using alp::cms3;
 using alp::Geo;
 using alp::HS;
 using alp::IC;
+using alp::interior_coords;
+using alp::inv;
+using alp::rk_stage;
+using alp::stage_update_cell;
 
 constexpr int kMaxLevels = 7;            // lmax <= 6: 64 micro steps per macro step
 constexpr int kMaxMicro = 1 << (kMaxLevels - 1);
@@ -144,16 +149,19 @@ __device__ __forceinline__ bool ghost_part(GhostRec const &g, int part, int lo[3
   return true;
 }
 
-// Type 1 ghosts of one level: averages of the children.
+// Fields whose children one thread holds at once in the averages (two fit the
+// ghost kernel's 64 registers; one was 1 % slower on the three-level step).
+constexpr int kAverageFields = 2;
+
+// Part `part` of a type 1 ghost, by one CTA: averages of the children.
 template <int DIM>
-__global__ void __launch_bounds__(256)
-ghost_average_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
-                     int nleaf, CaseState const *__restrict__ gate,
-                     CaseState const *__restrict__ cu, int stage) {
+__device__ __forceinline__ void ghost_average_unit(GhostRec const &g, int part, double *Ug,
+                                                   double const *UA, int nleaf,
+                                                   CaseState const *__restrict__ gate,
+                                                   CaseState const *__restrict__ cu, int stage) {
   using G = Geo<DIM>;
-  GhostRec const &g = ghosts[blockIdx.x];
   int lo[3], hi[3];
-  if (!ghost_part<DIM>(g, blockIdx.y, lo, hi)) return;
+  if (!ghost_part<DIM>(g, part, lo, hi)) return;
   if (!(gate[g.gate].dt > 0.0)) return;  // no block reading this ghost computes now
   int const n1 = hi[1] - lo[1], n2 = hi[2] - lo[2];
   int const count = (hi[0] - lo[0]) * n1 * n2;
@@ -170,23 +178,37 @@ ghost_average_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double con
     if (child < 0) continue;  // never read: the host checks face children are leaves
     double const *sb =
         ghost_source(child, nleaf, g.level + 1, Ug, UA, cu, stage) + (size_t)child * G::BLOCK_DOUBLES;
+    // kAverageFields fields' children are loaded before any of their averages
+    // is stored: the stores may alias the sources, so the compiler would not
+    // move later loads above them, and these loads in flight are what keeps
+    // the averages near the memory rate
 #pragma unroll
-    for (int e = 0; e < G::NE; ++e) {
-      double const *s = sb + e * G::CELLS;
-      double v;
-      if constexpr (DIM == 1) {
-        v = (s[G::cell(c[0], 0, 0)] + s[G::cell(c[0] + 1, 0, 0)]) * 0.5;
-      } else if constexpr (DIM == 2) {
-        v = ((s[G::cell(c[0], c[1], 0)] + s[G::cell(c[0] + 1, c[1] + 1, 0)]) +
-             (s[G::cell(c[0] + 1, c[1], 0)] + s[G::cell(c[0], c[1] + 1, 0)])) * 0.25;
-      } else {
-        double w[8];
+    for (int e0 = 0; e0 < G::NE; e0 += kAverageFields) {
+      constexpr int K = 1 << DIM;
+      double w[kAverageFields][K];
 #pragma unroll
-        for (int k = 0; k < 8; ++k)
-          w[k] = s[G::cell(c[0] + (k & 1), c[1] + ((k >> 1) & 1), c[2] + ((k >> 2) & 1))];
-        v = ghost_average3(w[0], w[1], w[2], w[3], w[4], w[5], w[6], w[7]);
-      }
-      dst[e * G::CELLS + x] = v;
+      for (int f = 0; f < kAverageFields; ++f)
+        if (e0 + f < G::NE) {
+          double const *s = sb + (e0 + f) * G::CELLS;
+#pragma unroll
+          for (int k = 0; k < K; ++k)
+            w[f][k] = s[G::cell(c[0] + (k & 1), c[1] + (DIM > 1 ? (k >> 1) & 1 : 0),
+                                c[2] + (DIM > 2 ? (k >> 2) & 1 : 0))];
+        }
+#pragma unroll
+      for (int f = 0; f < kAverageFields; ++f)
+        if (e0 + f < G::NE) {
+          double v;
+          if constexpr (DIM == 1) {
+            v = (w[f][0] + w[f][1]) * 0.5;
+          } else if constexpr (DIM == 2) {
+            v = ((w[f][0] + w[f][3]) + (w[f][1] + w[f][2])) * 0.25;
+          } else {
+            v = ghost_average3(w[f][0], w[f][1], w[f][2], w[f][3], w[f][4], w[f][5], w[f][6],
+                               w[f][7]);
+          }
+          dst[(e0 + f) * G::CELLS + x] = v;
+        }
     }
   }
 }
@@ -267,11 +289,16 @@ __device__ __forceinline__ void predict_children(V const &val, double (&out)[1 <
   }
 }
 
-// Type 0 ghosts of one level: predicted from the parent level. The parent
-// cells under the filled part plus two on every side are staged in shared
-// memory for all fields at once; then one thread per (field, parent cell)
-// writes the children.
+// Part `part` of a type 0 ghost, by one CTA: predicted from the parent level.
+// The parent cells under the part plus two on every side are staged in the
+// shared memory `box`, kFieldsPerPass fields at a time; then one thread per
+// (field, parent cell) writes the children. The CTA's threads take the same
+// early returns.
 constexpr int kBox = IC / 2 + 4;  // parent cells of a whole octant plus the stencil reach
+// Two fields per pass keep the box at 28 KB in 3D, within the 56 KB a CTA
+// has at the ghost kernel's 4 CTAs per SM (64 registers a thread). On the
+// three-level step one field per pass was 1.3 % slower and three 1.4 %.
+constexpr int kFieldsPerPass = 2;
 
 template <int DIM>
 __host__ __device__ constexpr int predict_box_doubles() {
@@ -279,21 +306,20 @@ __host__ __device__ constexpr int predict_box_doubles() {
 }
 template <int DIM>
 constexpr size_t predict_smem_bytes() {
-  return sizeof(double) * Geo<DIM>::NE * predict_box_doubles<DIM>();
+  return sizeof(double) * kFieldsPerPass * predict_box_doubles<DIM>();
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256)
-ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double const *UA,
-                     int nleaf, CaseState const *__restrict__ gate,
-                     CaseState const *__restrict__ cu, int stage) {
+__device__ __forceinline__ void ghost_predict_unit(GhostRec const &g, int part, double *Ug,
+                                                   double const *UA, int nleaf,
+                                                   CaseState const *__restrict__ gate,
+                                                   CaseState const *__restrict__ cu, int stage,
+                                                   double *box) {
   using G = Geo<DIM>;
   constexpr int B1 = DIM > 1 ? kBox : 1, B2 = DIM > 2 ? kBox : 1;
   constexpr int BOX = predict_box_doubles<DIM>();
-  extern __shared__ double box[];  // [NE][kBox][B1][B2]
-  GhostRec const &g = ghosts[blockIdx.x];
   int lo[3], hi[3];
-  if (!ghost_part<DIM>(g, blockIdx.y, lo, hi)) return;
+  if (!ghost_part<DIM>(g, part, lo, hi)) return;
   if (!(gate[g.gate].dt > 0.0)) return;
   // parent cells (relative to the parent node's origin) under the part
   int plo[3] = {0, 0, 0}, pn[3] = {1, 1, 1}, bn[3] = {1, 1, 1};
@@ -304,48 +330,147 @@ ghost_predict_kernel(GhostRec const *__restrict__ ghosts, double *Ug, double con
     bn[e] = pn[e] + 4;
   }
   int const nbox = bn[0] * bn[1] * bn[2], npar = pn[0] * pn[1] * pn[2];
-  for (int t = threadIdx.x; t < nbox; t += blockDim.x) {
-    int const r[3] = {t / (bn[1] * bn[2]), (t / bn[2]) % bn[1], t % bn[2]};
-    int y[3] = {0, 0, 0}, k = 0;
-    for (int d = 0; d < 3; ++d) {
-      int dn = 0;
-      if (d < DIM) {
-        int gc = g.q[d] * IC + plo[d] - 2 + r[d];  // parent-level cell
-        gc = gc < 0 ? 0 : (gc >= g.ext[d] ? g.ext[d] - 1 : gc);
-        dn = gc / IC - g.q[d];
-        y[d] = gc - (g.q[d] + dn) * IC + G::fic(d);
-      }
-      k = 3 * k + dn + 1;
-    }
-    int const slot = g.nb[k];
-    double const *sb =
-        ghost_source(slot, nleaf, g.level - 1, Ug, UA, cu, stage) + (size_t)slot * G::BLOCK_DOUBLES;
-    int const c = G::cell(y[0], y[1], y[2]);
-    int const b = (r[0] * B1 + r[1]) * B2 + r[2];
-#pragma unroll
-    for (int e = 0; e < G::NE; ++e) box[e * BOX + b] = sb[e * G::CELLS + c];
-  }
-  __syncthreads();
   double *dst = Ug + (size_t)g.slot * G::BLOCK_DOUBLES;
-  for (int t = threadIdx.x; t < npar * G::NE; t += blockDim.x) {
-    int const e = t / npar, tp = t - e * npar;
-    int const r[3] = {tp / (pn[1] * pn[2]) + 2, (tp / pn[2]) % pn[1] + (DIM > 1 ? 2 : 0),
-                      tp % pn[2] + (DIM > 2 ? 2 : 0)};
-    double const *bx = box + e * BOX;
-    auto val = [&](int a, int b, int c) {
-      return bx[((r[0] + a) * B1 + (DIM > 1 ? r[1] + b : 0)) * B2 + (DIM > 2 ? r[2] + c : 0)];
-    };
-    double out[1 << DIM];
-    predict_children<DIM>(val, out);
+  for (int e0 = 0; e0 < G::NE; e0 += kFieldsPerPass) {
+    int const ne = G::NE - e0 < kFieldsPerPass ? G::NE - e0 : kFieldsPerPass;
+    if (e0 > 0) __syncthreads();  // the previous pass has read the box
+    for (int t = threadIdx.x; t < nbox; t += blockDim.x) {
+      int const r[3] = {t / (bn[1] * bn[2]), (t / bn[2]) % bn[1], t % bn[2]};
+      int y[3] = {0, 0, 0}, k = 0;
+      for (int d = 0; d < 3; ++d) {
+        int dn = 0;
+        if (d < DIM) {
+          int gc = g.q[d] * IC + plo[d] - 2 + r[d];  // parent-level cell
+          gc = gc < 0 ? 0 : (gc >= g.ext[d] ? g.ext[d] - 1 : gc);
+          dn = gc / IC - g.q[d];
+          y[d] = gc - (g.q[d] + dn) * IC + G::fic(d);
+        }
+        k = 3 * k + dn + 1;
+      }
+      int const slot = g.nb[k];
+      double const *sb = ghost_source(slot, nleaf, g.level - 1, Ug, UA, cu, stage) +
+                         (size_t)slot * G::BLOCK_DOUBLES;
+      int const c = G::cell(y[0], y[1], y[2]);
+      int const b = (r[0] * B1 + r[1]) * B2 + r[2];
 #pragma unroll
-    for (int o = 0; o < (1 << DIM); ++o) {
-      int a[3] = {0, 0, 0};
-      for (int d = 0; d < DIM; ++d)
-        a[d] = 2 * (plo[d] + r[d] - 2 - (IC / 2) * ((g.oct >> d) & 1)) + ((o >> d) & 1);
-      dst[e * G::CELLS + G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2))] = out[o];
+      for (int e = 0; e < kFieldsPerPass; ++e)
+        if (e < ne) box[e * BOX + b] = sb[(e0 + e) * G::CELLS + c];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < npar * ne; t += blockDim.x) {
+      int const e = t / npar, tp = t - e * npar;
+      int const r[3] = {tp / (pn[1] * pn[2]) + 2, (tp / pn[2]) % pn[1] + (DIM > 1 ? 2 : 0),
+                        tp % pn[2] + (DIM > 2 ? 2 : 0)};
+      double const *bx = box + e * BOX;
+      auto val = [&](int a, int b, int c) {
+        return bx[((r[0] + a) * B1 + (DIM > 1 ? r[1] + b : 0)) * B2 + (DIM > 2 ? r[2] + c : 0)];
+      };
+      double out[1 << DIM];
+      predict_children<DIM>(val, out);
+#pragma unroll
+      for (int o = 0; o < (1 << DIM); ++o) {
+        int a[3] = {0, 0, 0};
+        for (int d = 0; d < DIM; ++d)
+          a[d] = 2 * (plo[d] + r[d] - 2 - (IC / 2) * ((g.oct >> d) & 1)) + ((o >> d) & 1);
+        dst[(e0 + e) * G::CELLS + G::cell(a[0] + G::fic(0), a[1] + G::fic(1), a[2] + G::fic(2))] =
+            out[o];
+      }
     }
   }
 }
+
+// The ghost groups of a stage in launch order (averages finest level first,
+// then predictions coarsest first): a group's records read only records of
+// earlier groups.
+constexpr int kMaxGhostGroups = 16;
+struct GhostPlan {
+  int n;
+  int type[kMaxGhostGroups], first[kMaxGhostGroups];
+  int start[kMaxGhostGroups + 1];  // the groups' first (record, part) units, then the total
+};
+
+__device__ __forceinline__ unsigned ld_acquire_u32(unsigned const *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits (thread 0 of a CTA) until *c reaches `target`, bounded: 2^22 polls
+// (a second or two of L2 round trips).
+// On running out it sets *err and returns false; a wait that finds *err set
+// gives up at once.
+__device__ bool wait_count(unsigned const *c, unsigned target, int *err) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (ld_acquire_u32(c) >= target) return true;
+    if ((i & 1023) == 1023 && *reinterpret_cast<int volatile *>(err)) return false;
+  }
+  if (ld_acquire_u32(c) >= target) return true;
+  atomicOr(err, 1);
+  return false;
+}
+
+// The ghost groups of one stage in one launch. The CTAs pull the (record,
+// part) units of all groups in order from one counter, so that cheap units
+// (parts a record does not serve, ghosts whose readers are idle) and
+// expensive ones (prediction boxes) even out. A unit of group k reads what
+// group k-1 wrote: its CTA first waits for group k-1's count of finished units
+// (which implies all earlier groups). Units are handed out in order, so every
+// unit of an earlier group belongs to a CTA that is already running and waits
+// only on groups before its own: the waits end whatever the number of
+// resident CTAs. words: [0] the next unit, [1 + k] group k's finished units,
+// [1 + kMaxGhostGroups] the CTAs done; the last CTA done zeroes them for the
+// next launch.
+template <int DIM>
+__global__ void __launch_bounds__(256, 4)
+ghost_kernel(GhostRec const *__restrict__ ghosts, GhostPlan plan, double *Ug, double const *UA,
+             int nleaf, CaseState const *__restrict__ gate, CaseState const *__restrict__ cu,
+             int stage, unsigned *words, int *err) {
+  extern __shared__ double box[];
+  __shared__ unsigned unit;
+  __shared__ int ok;
+  constexpr int PARTS = 2 * DIM + 1;
+  unsigned *const next = words, *const done = words + 1, *const finished = words + 1 + kMaxGhostGroups;
+  unsigned const total = (unsigned)plan.start[plan.n];
+  int ready = 0;  // the groups below `ready` are known finished
+  for (;;) {
+    if (threadIdx.x == 0) unit = atomicAdd(next, 1u);
+    __syncthreads();
+    unsigned const u = unit;
+    if (u >= total) break;
+    int k = 0;
+    while (u >= (unsigned)plan.start[k + 1]) ++k;
+    if (k > ready) {
+      if (threadIdx.x == 0)
+        ok = wait_count(done + k - 1, (unsigned)(plan.start[k] - plan.start[k - 1]), err);
+      __syncthreads();
+      if (!ok) return;
+      ready = k;
+    }
+    unsigned const v = u - (unsigned)plan.start[k];
+    GhostRec const &g = ghosts[plan.first[k] + v / PARTS];
+    if (plan.type[k] == 1)
+      ghost_average_unit<DIM>(g, v % PARTS, Ug, UA, nleaf, gate, cu, stage);
+    else
+      ghost_predict_unit<DIM>(g, v % PARTS, Ug, UA, nleaf, gate, cu, stage, box);
+    __syncthreads();  // the unit's stores are done; the box and `unit` are free again
+    if (threadIdx.x == 0) {
+      __threadfence();
+      atomicAdd(done + k, 1u);
+    }
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(finished, 1u) == gridDim.x - 1) {
+      *next = 0u;
+      for (int k = 0; k < plan.n; ++k) done[k] = 0u;
+      *finished = 0u;
+    }
+  }
+}
+
+// The ghost kernel's device words: the next unit, the groups' finished
+// units, the CTAs done.
+constexpr int kGhostWords = 1 + kMaxGhostGroups + 1;
 
 // The GlobalLaxFriedrichs maxima of all levels into every level's words (bit
 // patterns of non-negative doubles order as the values).
@@ -370,24 +495,6 @@ struct CorrectRec {
   int slot, level, rec[6];
 };
 
-template <int DIM>
-__device__ __forceinline__ void interior_coords_of(int t, int &i, int &j, int &k) {
-  if constexpr (DIM == 3) {
-    i = t >> 8;
-    j = (t >> 4) & 15;
-    k = t & 15;
-  } else if constexpr (DIM == 2) {
-    i = t >> 4;
-    j = t & 15;
-    k = 0;
-  } else {
-    i = t;
-    j = 0;
-    k = 0;
-  }
-}
-
-// RK3 jump multipliers (runge_kutta_3_TVD.h:42-46)
 // jump multipliers per stage: SSP-RK3 (runge_kutta_3_TVD.h:42-46), then
 // TVD-RK2 (runge_kutta_2_TVD.h:40-44), as the stage tables of the update kernel
 __constant__ double kRkJump[5] = {1.0 / 6.0, 1.0 / 6.0, 2.0 / 3.0, 0.5, 0.5};
@@ -398,25 +505,45 @@ template <int DIM> struct FaceCells {
   __host__ __device__ static int n(int t) { return t < DIM ? IC : 1; }
 };
 
-// IntegrateJumpConservatives: J += (w_stage * dt_level) * F for the jump faces
-// of the leaves that integrated in this stage.
+// A stage's update and jump sums in one launch: CTAs (x < nupd, y) run the
+// stage update of work item x (stage_update_cell, the arithmetic of every
+// stage update); CTAs (nupd + r, 0) add jump record r's face fluxes to its
+// sums, J += (w_stage * dt_level) * F (IntegrateJumpConservatives,
+// time_integrator.h:64-80). The sums read the stage's fluxes, not its output,
+// so the two parts are independent.
 template <int DIM>
 __global__ void __launch_bounds__(256)
-jump_accumulate_kernel(JumpRec const *__restrict__ recs, double const *__restrict__ F,
-                       long long stride, long long dstride, double *__restrict__ jbuf,
-                       CaseState const *__restrict__ cu, int stage) {
+level_update_kernel(double const *Uin, double const *U0, double *Uout, int const *__restrict__ work,
+                    BlockMeta const *__restrict__ meta, double const *__restrict__ F,
+                    long long stride, long long dstride, int stage,
+                    CaseState const *__restrict__ cu, int nupd, JumpRec const *__restrict__ recs,
+                    double *__restrict__ jbuf) {
   using G = Geo<DIM>;
+  int const x = blockIdx.x;
+  if (x < nupd) {
+    int const slot = work[x];
+    BlockMeta const bm = meta[slot];
+    double const dt = cu[bm.case_id].dt;
+    if (!(dt > 0.0)) return;
+    int const t = blockIdx.y * blockDim.x + threadIdx.x;
+    if (t >= G::INTERIOR) return;
+    stage_update_cell<DIM>(Uin, U0, Uout, F + (long long)x * stride, dstride, slot, t,
+                           inv(bm.cell_size), rk_stage(stage, dt));
+    return;
+  }
+  if (blockIdx.y != 0) return;
   using FC = FaceCells<DIM>;
-  JumpRec const r = recs[blockIdx.x];
+  int const ri = x - nupd;
+  JumpRec const r = recs[ri];
   double const dtl = cu[r.level].dt;
   if (!(dtl > 0.0)) return;
   double const jstep = kRkJump[stage] * dtl;
   int const d = r.loc / 2, a = (r.loc % 2) ? 0 : IC;
   int const t1 = FC::t1(d), t2 = FC::t2(d), n1 = FC::n(t1), n2 = FC::n(t2);
   double const *Fd = F + (long long)r.item * stride + d * dstride;
-  double *J = jbuf + (size_t)blockIdx.x * G::NE * IC * IC;
-  for (int x = threadIdx.x; x < G::NE * n1 * n2; x += blockDim.x) {
-    int const e = x / (n1 * n2), q = x % (n1 * n2), p1 = q / n2, p2 = q % n2;
+  double *J = jbuf + (size_t)ri * G::NE * IC * IC;
+  for (int y = threadIdx.x; y < G::NE * n1 * n2; y += blockDim.x) {
+    int const e = y / (n1 * n2), q = y % (n1 * n2), p1 = q / n2, p2 = q % n2;
     int fi[3];
     fi[d] = a;
     fi[t1] = p1 + 1;
@@ -473,7 +600,7 @@ jump_correct_kernel(CorrectRec const *__restrict__ corr, JumpRec const *__restri
   double *ub = U + (size_t)cr.slot * G::BLOCK_DOUBLES;
   for (int t = threadIdx.x; t < G::INTERIOR; t += blockDim.x) {
     int a[3];
-    interior_coords_of<DIM>(t, a[0], a[1], a[2]);
+    interior_coords<DIM>(t, a[0], a[1], a[2]);
     bool touched = false;
 #pragma unroll
     for (int loc = 0; loc < 2 * DIM; ++loc) {
@@ -585,6 +712,7 @@ struct JumpFace {
 // A run of ghost records of one type and level, filled by one launch.
 struct GhostGroup {
   int type, level, first, count;
+  int max_gate;  // the finest level that reads a ghost of the group
 };
 
 struct alp_levels {
@@ -598,6 +726,10 @@ struct alp_levels {
   int *nbr26 = nullptr, *work = nullptr;
   GhostRec *ghosts = nullptr;
   std::vector<GhostGroup> ghost_groups;  // launch order of the ghost records
+  int ghost_grid = 0;                     // CTAs of the ghost kernel: those resident at once
+  unsigned *gwords = nullptr;  // its unit counters (kGhostWords)
+  int *gerr = nullptr;                    // set when a wait for a ghost group ran out
+  unsigned stall_next = 0;                // the second group's first unit in the macro step's first ghost launch
   // jump-flux conservation: records, per-record sums, parent-face sums,
   // fine-side record list, coarse leaves to correct
   int nrec = 0, nfine = 0, ncorr = 0, nacc = 0;
@@ -616,6 +748,38 @@ struct alp_levels {
 
   long long dstride() const { return (long long)ne * faces; }
   long long stride() const { return dstride() * dim; }
+  int cells_interior() const { return dim == 3 ? 4096 : (dim == 2 ? 256 : 16); }
+
+  cudaError_t launch_ghosts(GhostPlan const &plan, double *Ug, CaseState const *gate, int s) {
+    dim3 const grid((unsigned)ghost_grid);
+    switch (dim) {
+      case 1:
+        ghost_kernel<1><<<grid, 256, predict_smem_bytes<1>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        break;
+      case 2:
+        ghost_kernel<2><<<grid, 256, predict_smem_bytes<2>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        break;
+      default:
+        ghost_kernel<3><<<grid, 256, predict_smem_bytes<3>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        break;
+    }
+    return cudaGetLastError();
+  }
+
+  // Reads and clears the ghost kernel's error word (a wait for a group that
+  // ran out: the results of those steps are not valid).
+  int ghost_check() {
+    if (!gerr) return ALP_OK;
+    int e = 0;
+    ALP_CUDA(cudaMemcpyAsync(&e, gerr, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    ALP_CUDA(cudaStreamSynchronize(stream));
+    if (!e) return ALP_OK;
+    ALP_CUDA(cudaMemsetAsync(gwords, 0, kGhostWords * sizeof(unsigned), stream));
+    ALP_CUDA(cudaMemsetAsync(gerr, 0, sizeof(int), stream));
+    ALP_CUDA(cudaStreamSynchronize(stream));
+    return alp::fail(ALP_ERR_CUDA, "level ghosts: a wait for a ghost group ran out; the step "
+                                   "results are not valid");
+  }
 
   int record_macro() {
     Launch L{dim, scheme, precision, U, work, nleaf, meta, BlockMeta{}, stream};
@@ -625,6 +789,8 @@ struct alp_levels {
     double *out[3] = {UB, UC, U};
     int const nst = rk2 ? 2 : 3, s0 = rk2 ? 3 : 0;
     if (rk2) out[1] = U;
+    bool first_ghost = true;
+    stall_next = 0;
     for (int tm = 0; tm < nmicro; ++tm) {
       Launch La = L;
       ALP_CUDA(launch_signal_speed(La, cu, nullptr));
@@ -635,24 +801,24 @@ struct alp_levels {
       int const lf = tm == 0 ? 0 : lmax - height(tm - 1) + 1;
       for (int s = 0; s < nst; ++s) {
         CaseState const *gate = s == 0 ? cf : cu;
-        // averaged ghosts finest level first, then predicted ones coarsest first
-        for (GhostGroup const &gg : ghost_groups) {
-          dim3 grid(gg.count, 2 * dim + 1);
-          GhostRec const *g0 = ghosts + gg.first;
-          if (gg.type == 1) {
-            switch (dim) {
-              case 1: ghost_average_kernel<1><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              case 2: ghost_average_kernel<2><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              default: ghost_average_kernel<3><<<grid, 256, 0, stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-            }
-          } else {
-            switch (dim) {
-              case 1: ghost_predict_kernel<1><<<grid, 256, predict_smem_bytes<1>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              case 2: ghost_predict_kernel<2><<<grid, 256, predict_smem_bytes<2>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-              default: ghost_predict_kernel<3><<<grid, 256, predict_smem_bytes<3>(), stream>>>(g0, in[s], U, nleaf, gate, cu, s); break;
-            }
+        // the stage's ghosts in one launch: averaged ghosts finest level
+        // first, then predicted ones coarsest first, each group after the one
+        // before. A group fires only when a level reading it computes in this
+        // stage (level >= lf for the first stage's fluxes, >= lu after), so
+        // the others are left out of the plan.
+        GhostPlan plan{};
+        int const thr = s == 0 ? lf : lu;
+        for (GhostGroup const &gg : ghost_groups)
+          if (gg.max_gate >= thr) {
+            plan.type[plan.n] = gg.type;
+            plan.first[plan.n] = gg.first;
+            plan.start[plan.n + 1] = plan.start[plan.n] + gg.count * (2 * dim + 1);
+            ++plan.n;
           }
-          ALP_CUDA(cudaGetLastError());
+        if (plan.n > 0) {
+          if (first_ghost) stall_next = plan.n >= 2 ? (unsigned)plan.start[1] : 0u;
+          first_ghost = false;
+          ALP_CUDA(launch_ghosts(plan, in[s], gate, s));
         }
         Launch Ls = L;
         Ls.U = in[s];
@@ -667,14 +833,14 @@ struct alp_levels {
         }
         if (Ls.nwork > 0)
           ALP_CUDA(launch_face_flux_all(Ls, nbr26, gate, F, stride(), dstride(), 128));
-        Ls.nwork = nwork_ge[lu];
-        if (Ls.nwork > 0)
-          ALP_CUDA(launch_stage_update(Ls, U, out[s], F, stride(), dstride(), s0 + s, cu, 0.0));
-        if (nrec > 0) {
+        // stage update of the integrating leaves and their jump sums, one launch
+        int const nupd = nwork_ge[lu];
+        if (nupd + nrec > 0) {
+          dim3 const grid((unsigned)(nupd + nrec), (unsigned)((cells_interior() + 255) / 256));
           switch (dim) {
-            case 1: jump_accumulate_kernel<1><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
-            case 2: jump_accumulate_kernel<2><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
-            default: jump_accumulate_kernel<3><<<nrec, 256, 0, stream>>>(jrecs, F, stride(), dstride(), jbuf, cu, s0 + s); break;
+            case 1: level_update_kernel<1><<<grid, 256, 0, stream>>>(in[s], U, out[s], work, meta, F, stride(), dstride(), s0 + s, cu, nupd, jrecs, jbuf); break;
+            case 2: level_update_kernel<2><<<grid, 256, 0, stream>>>(in[s], U, out[s], work, meta, F, stride(), dstride(), s0 + s, cu, nupd, jrecs, jbuf); break;
+            default: level_update_kernel<3><<<grid, 256, 0, stream>>>(in[s], U, out[s], work, meta, F, stride(), dstride(), s0 + s, cu, nupd, jrecs, jbuf); break;
           }
           ALP_CUDA(cudaGetLastError());
         }
@@ -705,6 +871,8 @@ struct alp_levels {
 
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
+    cudaFree(gwords);
+    cudaFree(gerr);
     cudaFree(U);
     cudaFree(UB);
     cudaFree(UC);
@@ -1129,12 +1297,25 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   };
   cudaError_t e = cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
   if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaStreamCreate"));
-  // the 3D prediction kernel stages 69 KB of parent cells: above the default
-  // 48 KB of dynamic shared memory, so it is allowed here, before any capture
-  if (dim == 3) {
-    e = cudaFuncSetAttribute(ghost_predict_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)predict_smem_bytes<3>());
-    if (e != cudaSuccess) return cleanup(cuda_fail(e, "cudaFuncSetAttribute(ghost_predict_kernel)"));
+  // the ghost kernel's grid: the CTAs the device holds at once (one wave,
+  // each pulling units until none is left), and its counters
+  {
+    void const *fn = dim == 1 ? (void const *)ghost_kernel<1>
+                     : dim == 2 ? (void const *)ghost_kernel<2> : (void const *)ghost_kernel<3>;
+    size_t const smem = dim == 1 ? predict_smem_bytes<1>()
+                        : dim == 2 ? predict_smem_bytes<2>() : predict_smem_bytes<3>();
+    int per_sm = 0, sms = 0, dev = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, 256, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return cleanup(cuda_fail(e, "ghost kernel setup"));
+    if (per_sm < 1) return cleanup(alp::fail(ALP_ERR_CUDA, "the ghost kernel does not fit an SM"));
+    m->ghost_grid = per_sm * sms;
+    if ((e = cudaMalloc(&m->gwords, kGhostWords * sizeof(unsigned))) != cudaSuccess ||
+        (e = cudaMalloc(&m->gerr, sizeof(int))) != cudaSuccess ||
+        (e = cudaMemsetAsync(m->gwords, 0, kGhostWords * sizeof(unsigned), m->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(m->gerr, 0, sizeof(int), m->stream)) != cudaSuccess)
+      return cleanup(cuda_fail(e, "ghost counters"));
   }
   void **bufs[] = {(void **)&m->U, (void **)&m->UB, (void **)&m->UC};
   for (void **b : bufs) {
@@ -1205,13 +1386,19 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   std::vector<GhostRec> order;
   auto group = [&](int type, int lev) {
     int const first = (int)order.size();
+    int max_gate = -1;
     for (GhostRec const &g : gh)
-      if (g.type == type && g.level == lev) order.push_back(g);
+      if (g.type == type && g.level == lev) {
+        order.push_back(g);
+        max_gate = std::max(max_gate, g.gate);
+      }
     if ((int)order.size() > first)
-      m->ghost_groups.push_back({type, lev, first, (int)order.size() - first});
+      m->ghost_groups.push_back({type, lev, first, (int)order.size() - first, max_gate});
   };
   for (int l = lmax; l >= 0; --l) group(1, l);
   for (int l = 0; l <= lmax; ++l) group(0, l);
+  if ((int)m->ghost_groups.size() > kMaxGhostGroups)
+    return cleanup(alp::fail(ALP_ERR_INVALID, "too many ghost groups for the ghost kernel"));
   if (e == cudaSuccess && m->nghost)
     e = cudaMemcpyAsync(m->ghosts, order.data(), sizeof(GhostRec) * m->nghost,
                         cudaMemcpyHostToDevice, m->stream);
@@ -1267,6 +1454,7 @@ int alp_levels_get(alp_levels *m, double *h_blocks, double *t, int *macro_steps)
   LevelState st;
   ALP_CUDA(cudaMemcpyAsync(&st, m->ls, sizeof(st), cudaMemcpyDeviceToHost, m->stream));
   ALP_CUDA(cudaStreamSynchronize(m->stream));
+  if (int rc = m->ghost_check()) return rc;
   if (t) *t = st.t;
   if (macro_steps) *macro_steps = st.macro;
   if (st.status) return alp::fail(ALP_ERR_NUMERIC, "non-finite or non-positive state; case stopped");
@@ -1288,10 +1476,12 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
       int const lf = tm == 0 ? 0 : m->lmax - height(tm - 1) + 1;
       n += per_micro;
       for (int s = 0; s < (m->rk2 ? 2 : 3); ++s) {
-        n += (int)m->ghost_groups.size();
+        int const thr = s == 0 ? lf : lu;
+        bool any = false;
+        for (auto const &gg : m->ghost_groups) any |= gg.max_gate >= thr;
+        n += any ? 1 : 0;  // the ghost kernel
         n += m->nwork_ge[s == 0 ? lf : lu] > 0 ? (m->glf ? 3 : 1) : 0;  // GLF: maxima, fold
-        n += m->nwork_ge[lu] > 0 ? 1 : 0;
-        n += m->nrec > 0 ? 1 : 0;
+        n += m->nwork_ge[lu] + m->nrec > 0 ? 1 : 0;  // stage update with the jump sums
       }
       n += (m->nfine > 0 ? 1 : 0) + (m->ncorr > 0 ? 1 : 0);
     }
@@ -1301,5 +1491,16 @@ int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
 }
 
 alp_stream_t alp_levels_stream(alp_levels *m) { return m ? (alp_stream_t)m->stream : nullptr; }
+
+// The next ghost launch starts handing out units at its second group, so the
+// first group never finishes and the waits for it run out.
+int alp_levels_test_stall_ghosts(alp_levels *m) {
+  if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  if (m->stall_next == 0)
+    return alp::fail(ALP_ERR_INVALID, "the macro step's first ghost launch has one group");
+  ALP_CUDA(cudaStreamSynchronize(m->stream));
+  ALP_CUDA(cudaMemcpy(m->gwords, &m->stall_next, sizeof(unsigned), cudaMemcpyHostToDevice));
+  return ALP_OK;
+}
 
 }  // extern "C"

@@ -52,6 +52,60 @@ __device__ __forceinline__ double flux_divergence(double fx_lo, double fx_hi, do
   return dacms<DIM>(dx, dy, dz) * one_cell_size;
 }
 
+// Flux divergence of interior cell (i, j, k) of one field from the reference
+// flux arrays of the three directions (Fx, Fy, Fz at the field's offset).
+template <int DIM>
+__device__ __forceinline__ double divergence(double const *Fx, double const *Fy,
+                                             double const *Fz, int i, int j, int k,
+                                             double one_cell_size) {
+  using G = Geo<DIM>;
+  return flux_divergence<DIM>(Fx[G::face(i, j + 1, k + 1)], Fx[G::face(i + 1, j + 1, k + 1)],
+                              DIM > 1 ? Fy[G::face(i + 1, j, k + 1)] : 0.0,
+                              DIM > 1 ? Fy[G::face(i + 1, j + 1, k + 1)] : 0.0,
+                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k)] : 0.0,
+                              DIM > 2 ? Fz[G::face(i + 1, j + 1, k + 1)] : 0.0, one_cell_size);
+}
+
+// Interior cell (i, j, k) of thread t of a block's 16^DIM cells (z fastest).
+template <int DIM>
+__host__ __device__ __forceinline__ void interior_coords(int t, int &i, int &j, int &k) {
+  if constexpr (DIM == 3) {
+    i = t >> 8;
+    j = (t >> 4) & 15;
+    k = t & 15;
+  } else if constexpr (DIM == 2) {
+    i = t >> 4;
+    j = t & 15;
+    k = 0;
+  } else {
+    i = t;
+    j = 0;
+    k = 0;
+  }
+}
+
+// Stage update of interior cell t of the block in `slot`, every field: the flux
+// divergence from the block's face-flux arrays Fb (directions dstride apart)
+// and the RK stage into Uout. Every stage update computes it this way.
+template <int DIM>
+__device__ __forceinline__ void stage_update_cell(double const *Uin, double const *U0, double *Uout,
+                                                  double const *Fb, long long dstride, int slot,
+                                                  int t, double one_cell_size, RkStage const &rk) {
+  using G = Geo<DIM>;
+  int i, j, k;
+  interior_coords<DIM>(t, i, j, k);
+  int const c = G::cell(i + G::fic(0), j + G::fic(1), k + G::fic(2));
+  size_t const base = (size_t)slot * G::BLOCK_DOUBLES + c;
+#pragma unroll
+  for (int f = 0; f < G::NE; ++f) {
+    double const *fx = Fb + f * G::FACES;
+    double const rhs = 0.0 + divergence<DIM>(fx, fx + dstride, fx + 2 * dstride, i, j, k,
+                                             one_cell_size);
+    size_t const x = base + (size_t)f * G::CELLS;
+    Uout[x] = rk_apply(rk, Uin[x], rk.first ? 0.0 : U0[x], rhs);
+  }
+}
+
 // Signal speed of one cell for ComputeTimestepSize
 // (modular_algorithm_assembler.cpp:1840-1870): ConsistencyManagedSum(|u_d| + c).
 // Sets bad for a NaN, a non-positive density or an imaginary sound speed.

@@ -233,6 +233,7 @@ _SIGS = {
     "alp_levels_get": (C.c_int, [_V, _D, _D, _I]),
     "alp_levels_info": (C.c_int, [_V, _I, _I, C.POINTER(C.c_longlong), _I]),
     "alp_levels_stream": (_S, [_V]),
+    "alp_levels_test_stall_ghosts": (C.c_int, [_V]),
 }
 
 # stepping candidates of alp_engine_autotune (ALP_STEP_CANDIDATES)

@@ -468,6 +468,12 @@ int alp_levels_get(alp_levels *m, double *h_blocks, double *t, int *macro_steps)
 int alp_levels_info(alp_levels *m, int *n_ghosts, int *max_level,
                     long long *cell_updates_per_macro_step, int *launches_per_macro_step);
 alp_stream_t alp_levels_stream(alp_levels *m);
+/* Test of the ghost kernel's bounded waits (no ALPACA counterpart): the next
+ * macro step's first ghost launch skips its first group, so the launch's waits
+ * for that group run out (about a second) and set the engine's error word;
+ * the next alp_levels_get returns ALP_ERR_CUDA and clears it. The leaves are
+ * not valid after that step. ALP_ERR_INVALID when that launch has one group. */
+int alp_levels_test_stall_ghosts(alp_levels *m);
 
 /* ---- serving: continuous batching of independent cases ------------------ */
 

@@ -168,3 +168,27 @@ def test_levels_rk2_conserve_mass_and_energy(cuda):
         a = (c.u[I][:, f].reshape(c.nleaf, -1).sum(1) * vol).sum()
         b = (got[I][:, f].reshape(c.nleaf, -1).sum(1) * vol).sum()
         assert abs(b - a) <= 1e-14 * a, f
+
+
+def test_ghost_wait_runs_out_with_an_error(cuda):
+    """The ghost kernel's waits for an earlier group are bounded: when that
+    group never finishes (its units are skipped), the waits run out, the step
+    ends, and alp_levels_get reports it. The engine's stream and the context
+    stay usable, and the next steps run without error again."""
+    import torch
+
+    c = cases.spherical_shock_levels(n0=2, dim=3, lmax=2)
+    eng = api.LevelEngine(c, "fvchar")
+    eng.step(1)
+    eng.get()
+    assert eng.lib.alp_levels_test_stall_ghosts(eng.h) == N.ALP_OK
+    eng.step(1)
+    with pytest.raises(N.AlpacaError, match="ran out"):
+        eng.get()
+    # the error word and counters were cleared: the next step is clean
+    eng.step(1)
+    _, _, m = eng.get()
+    assert m == 3
+    x = torch.ones(1 << 20, device="cuda")
+    assert float(x.sum()) == float(1 << 20)
+    eng.close()

@@ -69,6 +69,7 @@ using alp::interior_coords;
 using alp::inv;
 using alp::rk_stage;
 using alp::stage_update_cell;
+using alp::wait_count;
 
 constexpr int kMaxLevels = 7;            // lmax <= 6: 64 micro steps per macro step
 constexpr int kMaxMicro = 1 << (kMaxLevels - 1);
@@ -388,26 +389,6 @@ struct GhostPlan {
   int type[kMaxGhostGroups], first[kMaxGhostGroups];
   int start[kMaxGhostGroups + 1];  // the groups' first (record, part) units, then the total
 };
-
-__device__ __forceinline__ unsigned ld_acquire_u32(unsigned const *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-// Waits (thread 0 of a CTA) until *c reaches `target`, bounded: 2^22 polls
-// (a second or two of L2 round trips).
-// On running out it sets *err and returns false; a wait that finds *err set
-// gives up at once.
-__device__ bool wait_count(unsigned const *c, unsigned target, int *err) {
-  for (int i = 0; i < (1 << 22); ++i) {
-    if (ld_acquire_u32(c) >= target) return true;
-    if ((i & 1023) == 1023 && *reinterpret_cast<int volatile *>(err)) return false;
-  }
-  if (ld_acquire_u32(c) >= target) return true;
-  atomicOr(err, 1);
-  return false;
-}
 
 // The ghost groups of one stage in one launch. The CTAs pull the (record,
 // part) units of all groups in order from one counter, so that cheap units

@@ -106,6 +106,25 @@ __device__ __forceinline__ void stage_update_cell(double const *Uin, double cons
   }
 }
 
+__device__ __forceinline__ unsigned ld_acquire_u32(unsigned const *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+// Waits (one thread of a CTA) until *c reaches `target`, bounded: 2^22 polls
+// (a second or two of L2 round trips). On running out it sets *err and
+// returns false; a wait that finds *err set gives up within 1024 polls.
+__device__ __forceinline__ bool wait_count(unsigned const *c, unsigned target, int *err) {
+  for (int i = 0; i < (1 << 22); ++i) {
+    if (ld_acquire_u32(c) >= target) return true;
+    if ((i & 1023) == 1023 && *reinterpret_cast<int volatile *>(err)) return false;
+  }
+  if (ld_acquire_u32(c) >= target) return true;
+  atomicOr(err, 1);
+  return false;
+}
+
 // Signal speed of one cell for ComputeTimestepSize
 // (modular_algorithm_assembler.cpp:1840-1870): ConsistencyManagedSum(|u_d| + c).
 // Sets bad for a NaN, a non-positive density or an imaginary sound speed.

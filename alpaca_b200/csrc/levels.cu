@@ -393,26 +393,29 @@ struct GhostPlan {
 // The ghost groups of one stage in one launch. The CTAs pull the (record,
 // part) units of all groups in order from one counter, so that cheap units
 // (parts a record does not serve, ghosts whose readers are idle) and
-// expensive ones (prediction boxes) even out. A unit of group k reads what
-// group k-1 wrote: its CTA first waits for group k-1's count of finished units
-// (which implies all earlier groups). Units are handed out in order, so every
-// unit of an earlier group belongs to a CTA that is already running and waits
-// only on groups before its own: the waits end whatever the number of
-// resident CTAs. words: [0] the next unit, [1 + k] group k's finished units,
-// [1 + kMaxGhostGroups] the CTAs done; the last CTA done zeroes them for the
-// next launch.
+// expensive ones (prediction boxes) even out. A unit that fills cells first
+// waits until every ghost record it reads (children of an average, the
+// parent's neighbourhood of a prediction; rank: ghost slot - nleaf -> record)
+// has all its parts done. Those records belong to earlier groups (checked on
+// the host), so they were handed out earlier and are held by running CTAs:
+// every wait ends. Each is bounded all the same (wait_count) and sets *err on
+// running out. A record whose reader does not compute reads nothing new and
+// waits for nothing; a record whose reader computes reads only records whose
+// readers compute as well (the host gives a ghost the finest gate of its
+// readers), which are in the plan.
+// words: [0] the next unit, [1] the CTAs done, [2 + r] the parts of record r
+// done; the last CTA done zeroes them for the next launch.
 template <int DIM>
 __global__ void __launch_bounds__(256, 4)
 ghost_kernel(GhostRec const *__restrict__ ghosts, GhostPlan plan, double *Ug, double const *UA,
              int nleaf, CaseState const *__restrict__ gate, CaseState const *__restrict__ cu,
-             int stage, unsigned *words, int *err) {
+             int stage, unsigned *words, int const *__restrict__ rank, int *err) {
   extern __shared__ double box[];
   __shared__ unsigned unit;
   __shared__ int ok;
   constexpr int PARTS = 2 * DIM + 1;
-  unsigned *const next = words, *const done = words + 1, *const finished = words + 1 + kMaxGhostGroups;
+  unsigned *const next = words, *const finished = words + 1, *const done = words + 2;
   unsigned const total = (unsigned)plan.start[plan.n];
-  int ready = 0;  // the groups below `ready` are known finished
   for (;;) {
     if (threadIdx.x == 0) unit = atomicAdd(next, 1u);
     __syncthreads();
@@ -420,38 +423,50 @@ ghost_kernel(GhostRec const *__restrict__ ghosts, GhostPlan plan, double *Ug, do
     if (u >= total) break;
     int k = 0;
     while (u >= (unsigned)plan.start[k + 1]) ++k;
-    if (k > ready) {
-      if (threadIdx.x == 0)
-        ok = wait_count(done + k - 1, (unsigned)(plan.start[k] - plan.start[k - 1]), err);
+    unsigned const v = u - (unsigned)plan.start[k];
+    int const rec = plan.first[k] + (int)(v / PARTS), part = (int)(v % PARTS);
+    GhostRec const &g = ghosts[rec];
+    int lo[3], hi[3];
+    if (gate[g.gate].dt > 0.0 && ghost_part<DIM>(g, part, lo, hi)) {
+      if (threadIdx.x == 0) {
+        ok = 1;
+        int const *src = plan.type[k] == 1 ? g.src : g.nb;
+        int const n = plan.type[k] == 1 ? (1 << DIM) : 27;
+        for (int o = 0; o < n && ok; ++o)
+          if (src[o] >= nleaf) ok = wait_count(done + rank[src[o] - nleaf], PARTS, err);
+      }
       __syncthreads();
       if (!ok) return;
-      ready = k;
+      if (plan.type[k] == 1)
+        ghost_average_unit<DIM>(g, part, Ug, UA, nleaf, gate, cu, stage);
+      else
+        ghost_predict_unit<DIM>(g, part, Ug, UA, nleaf, gate, cu, stage, box);
     }
-    unsigned const v = u - (unsigned)plan.start[k];
-    GhostRec const &g = ghosts[plan.first[k] + v / PARTS];
-    if (plan.type[k] == 1)
-      ghost_average_unit<DIM>(g, v % PARTS, Ug, UA, nleaf, gate, cu, stage);
-    else
-      ghost_predict_unit<DIM>(g, v % PARTS, Ug, UA, nleaf, gate, cu, stage, box);
-    __syncthreads();  // the unit's stores are done; the box and `unit` are free again
+    __syncthreads();  // the unit's stores are issued; the box and `unit` are free again
     if (threadIdx.x == 0) {
       __threadfence();
-      atomicAdd(done + k, 1u);
+      atomicAdd(done + rec, 1u);
     }
   }
   if (threadIdx.x == 0) {
     __threadfence();
-    if (atomicAdd(finished, 1u) == gridDim.x - 1) {
+    ok = atomicAdd(finished, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (ok) {
+    for (int k = 0; k < plan.n; ++k)
+      for (int r = threadIdx.x; r < (plan.start[k + 1] - plan.start[k]) / PARTS; r += blockDim.x)
+        done[plan.first[k] + r] = 0u;
+    if (threadIdx.x == 0) {
       *next = 0u;
-      for (int k = 0; k < plan.n; ++k) done[k] = 0u;
       *finished = 0u;
     }
   }
 }
 
-// The ghost kernel's device words: the next unit, the groups' finished
-// units, the CTAs done.
-constexpr int kGhostWords = 1 + kMaxGhostGroups + 1;
+// The ghost kernel's device words: the next unit, the CTAs done, the parts
+// done of each ghost record.
+inline size_t ghost_words(int nghost) { return 2 + (size_t)nghost; }
 
 // The GlobalLaxFriedrichs maxima of all levels into every level's words (bit
 // patterns of non-negative doubles order as the values).
@@ -708,7 +723,8 @@ struct alp_levels {
   GhostRec *ghosts = nullptr;
   std::vector<GhostGroup> ghost_groups;  // launch order of the ghost records
   int ghost_grid = 0;                     // CTAs of the ghost kernel: those resident at once
-  unsigned *gwords = nullptr;  // its unit counters (kGhostWords)
+  unsigned *gwords = nullptr;  // its unit counters (ghost_words)
+  int *grank = nullptr;        // [nghost] launch-order record of each ghost slot
   int *gerr = nullptr;                    // set when a wait for a ghost group ran out
   unsigned stall_next = 0;                // the second group's first unit in the macro step's first ghost launch
   // jump-flux conservation: records, per-record sums, parent-face sums,
@@ -735,13 +751,13 @@ struct alp_levels {
     dim3 const grid((unsigned)ghost_grid);
     switch (dim) {
       case 1:
-        ghost_kernel<1><<<grid, 256, predict_smem_bytes<1>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        ghost_kernel<1><<<grid, 256, predict_smem_bytes<1>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, grank, gerr);
         break;
       case 2:
-        ghost_kernel<2><<<grid, 256, predict_smem_bytes<2>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        ghost_kernel<2><<<grid, 256, predict_smem_bytes<2>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, grank, gerr);
         break;
       default:
-        ghost_kernel<3><<<grid, 256, predict_smem_bytes<3>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, gerr);
+        ghost_kernel<3><<<grid, 256, predict_smem_bytes<3>(), stream>>>(ghosts, plan, Ug, U, nleaf, gate, cu, s, gwords, grank, gerr);
         break;
     }
     return cudaGetLastError();
@@ -755,7 +771,7 @@ struct alp_levels {
     ALP_CUDA(cudaMemcpyAsync(&e, gerr, sizeof(int), cudaMemcpyDeviceToHost, stream));
     ALP_CUDA(cudaStreamSynchronize(stream));
     if (!e) return ALP_OK;
-    ALP_CUDA(cudaMemsetAsync(gwords, 0, kGhostWords * sizeof(unsigned), stream));
+    ALP_CUDA(cudaMemsetAsync(gwords, 0, ghost_words(nghost) * sizeof(unsigned), stream));
     ALP_CUDA(cudaMemsetAsync(gerr, 0, sizeof(int), stream));
     ALP_CUDA(cudaStreamSynchronize(stream));
     return alp::fail(ALP_ERR_CUDA, "level ghosts: a wait for a ghost group ran out; the step "
@@ -853,6 +869,7 @@ struct alp_levels {
   void release() {
     if (graph) cudaGraphExecDestroy(graph);
     cudaFree(gwords);
+    cudaFree(grank);
     cudaFree(gerr);
     cudaFree(U);
     cudaFree(UB);
@@ -1292,9 +1309,11 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
     if (e != cudaSuccess) return cleanup(cuda_fail(e, "ghost kernel setup"));
     if (per_sm < 1) return cleanup(alp::fail(ALP_ERR_CUDA, "the ghost kernel does not fit an SM"));
     m->ghost_grid = per_sm * sms;
-    if ((e = cudaMalloc(&m->gwords, kGhostWords * sizeof(unsigned))) != cudaSuccess ||
+    size_t const gw = ghost_words(m->nghost) * sizeof(unsigned);
+    if ((e = cudaMalloc(&m->gwords, gw)) != cudaSuccess ||
+        (e = cudaMalloc(&m->grank, sizeof(int) * std::max(m->nghost, 1))) != cudaSuccess ||
         (e = cudaMalloc(&m->gerr, sizeof(int))) != cudaSuccess ||
-        (e = cudaMemsetAsync(m->gwords, 0, kGhostWords * sizeof(unsigned), m->stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(m->gwords, 0, gw, m->stream)) != cudaSuccess ||
         (e = cudaMemsetAsync(m->gerr, 0, sizeof(int), m->stream)) != cudaSuccess)
       return cleanup(cuda_fail(e, "ghost counters"));
   }
@@ -1380,6 +1399,23 @@ int alp_levels_create(int dim, const alp_scheme *scheme, const alp_material *mat
   for (int l = 0; l <= lmax; ++l) group(0, l);
   if ((int)m->ghost_groups.size() > kMaxGhostGroups)
     return cleanup(alp::fail(ALP_ERR_INVALID, "too many ghost groups for the ghost kernel"));
+  // the launch-order record of each ghost slot; every ghost a record reads
+  // must come from an earlier group (the ghost kernel's waits rely on it)
+  std::vector<int> rank(m->nghost);
+  for (int r = 0; r < m->nghost; ++r) rank[order[r].slot - nleaf] = r;
+  for (GhostGroup const &gg : m->ghost_groups)
+    for (int r = gg.first; r < gg.first + gg.count; ++r) {
+      GhostRec const &g = order[r];
+      int const *src = g.type == 1 ? g.src : g.nb;
+      int const n = g.type == 1 ? (1 << dim) : 27;
+      for (int o = 0; o < n; ++o)
+        if (src[o] >= nleaf && rank[src[o] - nleaf] >= gg.first)
+          return cleanup(alp::fail(ALP_ERR_INVALID,
+                                   "a ghost block reads a ghost of its own or a later group"));
+    }
+  if (e == cudaSuccess && m->nghost)
+    e = cudaMemcpyAsync(m->grank, rank.data(), sizeof(int) * m->nghost, cudaMemcpyHostToDevice,
+                        m->stream);
   if (e == cudaSuccess && m->nghost)
     e = cudaMemcpyAsync(m->ghosts, order.data(), sizeof(GhostRec) * m->nghost,
                         cudaMemcpyHostToDevice, m->stream);

@@ -42,9 +42,9 @@ FLOPS_PER_CELL_UPDATE_2D = {"fvchar": 8004, "fvprim": 5448, "fsroe": 10605}
 TRAFFIC_PER_STEP = {("fvchar", "fp64"): 4.359e9}
 # DRAM bytes per cell-update of the multi-level step (fvchar, FP64): one ncu
 # capture of a macro step of the same hierarchy at n0 = 2 (31 / 264 leaves, 176
-# ghosts, 4.58 M cell-updates, 9.43 GB), scaled by cell-updates (summary in
+# ghosts, 4.58 M cell-updates, 9.38 GB), scaled by cell-updates (summary in
 # profiles/levels_3d_spherical_shock.md)
-LEVELS_DRAM_PER_CELL_UPDATE = {("fvchar", "fp64"): 2059.0}
+LEVELS_DRAM_PER_CELL_UPDATE = {("fvchar", "fp64"): 2048.0}
 # stepping candidates of alp_engine_autotune, in its numbering
 CANDIDATES = ["face fluxes, 128-thread blocks", "face fluxes, 64-thread blocks", "pencil sweeps",
               "face fluxes and stage updates overlapped in batches",

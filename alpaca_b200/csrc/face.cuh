@@ -61,27 +61,62 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
       for (int m = 0; m < W; ++m)
 #pragma unroll
         for (int l = 0; l < NE; ++l) du[m][l] = m == C ? 0.0f : float(cons[m][l] - cons[C][l]);
+      T dm[NE], dp[NE];
+      if constexpr (ALP_FAST && W == 6 && C == 2) {
+        // both sides of every characteristic field in packed f32x2 arithmetic
+        // the projection of cells (0, 5) and (1, 4) packed as well; cell 2 is
+        // the face's left cell, whose increment is zero
+        float2 chp[NE], out[NE];
 #pragma unroll
-      for (int n = 0; n < NE; ++n) {
-        T L[NE];
-        left_row<DIM, DIR, T>(n, r, L);
-        T uc[W];
-#pragma unroll
-        for (int m = 0; m < W; ++m) {
-          T s = T(0);
+        for (int n = 0; n < NE; ++n) {
+          T L[NE];
+          left_row<DIM, DIR, T>(n, r, L);
+          float2 P0 = make_float2(0.0f, 0.0f), P1 = P0;
+          float u3 = 0.0f;
+          bool first = true;
 #pragma unroll
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);
             if (!left_nonzero<DIM, DIR>(n, l)) continue;
-            s = fmaf(L[l], du[m][l], s);
+            float2 const Ld = dup2(L[l]);
+            float2 const a0 = make_float2(du[0][l], du[5][l]);
+            float2 const a1 = make_float2(du[1][l], du[4][l]);
+            P0 = first ? mul2(Ld, a0) : fma2(Ld, a0, P0);
+            P1 = first ? mul2(Ld, a1) : fma2(Ld, a1, P1);
+            u3 = fmaf(L[l], du[3][l], u3);
+            first = false;
           }
-          uc[m] = s;
+          chp[n] = weno5_packed(P0, P1, make_float2(0.0f, u3), make_float2(u3, 0.0f),
+                                make_float2(P1.y, P1.x));
         }
-        weno5_pair(uc, ch[0][n], ch[1][n]);
+        to_physical_packed<DIM, DIR>(r, chp, out);
+#pragma unroll
+        for (int f = 0; f < NE; ++f) {
+          dm[f] = out[f].x;
+          dp[f] = out[f].y;
+        }
+      } else {
+#pragma unroll
+        for (int n = 0; n < NE; ++n) {
+          T L[NE];
+          left_row<DIM, DIR, T>(n, r, L);
+          T uc[W];
+#pragma unroll
+          for (int m = 0; m < W; ++m) {
+            T s = T(0);
+#pragma unroll
+            for (int q = 0; q < NE; ++q) {
+              int const l = sum_seq<DIM, DIR>(q);
+              if (!left_nonzero<DIM, DIR>(n, l)) continue;
+              s = fmaf(L[l], du[m][l], s);
+            }
+            uc[m] = s;
+          }
+          weno5_pair(uc, ch[0][n], ch[1][n]);
+        }
+        to_physical<DIM, DIR, T>(r, ch[0], dm);
+        to_physical<DIM, DIR, T>(r, ch[1], dp);
       }
-      T dm[NE], dp[NE];
-      to_physical<DIM, DIR, T>(r, ch[0], dm);
-      to_physical<DIM, DIR, T>(r, ch[1], dp);
       double cm[NE], cp[NE];
 #pragma unroll
       for (int f = 0; f < NE; ++f) {

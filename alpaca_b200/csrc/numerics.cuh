@@ -310,14 +310,64 @@ __device__ __forceinline__ void weno5_finish(T v_l, Weno5Frac<T> const &l, T v_r
   }
 }
 
+// ---- packed FP32 pairs (Blackwell f32x2: one instruction for two lanes) ----
+// Used by the fast build's FP32-flux form, where both sides of a face run the
+// same arithmetic: lane x the left (UpwindLeft) side, lane y the right one.
+__device__ __forceinline__ float2 dup2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+// a - b, rounded once (a + (-1) b)
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, dup2(-1.0f), a); }
+
+// UpwindLeft and UpwindRight of one face, packed: P_k = (a[k], a[5-k]) for
+// k = 0 .. 4 of the six cells a[0..5] (i-2 .. i+3). Lane y runs the mirrored
+// stencil, whose first differences are the negated ones weno5_frac takes for
+// the right side, so both lanes end as P_2 + num / (6 den) (weno5_frac; the
+// second differences and the e_k enter squared, so their signs do not matter).
+__device__ __forceinline__ float2 weno5_packed(float2 P0, float2 P1, float2 P2, float2 P3,
+                                               float2 P4) {
+  float2 const ng1 = sub2(P0, P1), g2 = sub2(P2, P1), g3 = sub2(P3, P2), ng4 = sub2(P3, P4);
+  float2 const d1 = add2(g2, ng1), d2 = sub2(g3, g2), d3 = add2(ng4, g3);
+  float2 const e1 = fma2(dup2(3.0f), g2, ng1);
+  float2 const e2 = add2(g2, g3);
+  float2 const e3 = fma2(dup2(3.0f), g3, ng4);
+  float2 const c = dup2(13.0f / 3.0f), eps = dup2(4.0e-6f);
+  float2 const s1 = fma2(mul2(c, d1), d1, fma2(e1, e1, eps));
+  float2 const s2 = fma2(mul2(c, d2), d2, fma2(e2, e2, eps));
+  float2 const s3 = fma2(mul2(c, d3), d3, fma2(e3, e3, eps));
+  float2 const t1 = mul2(s1, s1), t2 = mul2(s2, s2), t3 = mul2(s3, s3);
+  float2 const r1 = fma2(dup2(2.0f), ng1, mul2(dup2(5.0f), g2));
+  float2 const r2 = fma2(dup2(2.0f), g3, g2);
+  float2 const r3 = fma2(dup2(4.0f), g3, ng4);
+  // per lane: the power of two that brings the largest t_k into [1, 2)
+  unsigned const ex = min((__float_as_uint(fmaxf(t1.x, fmaxf(t2.x, t3.x))) >> 23) & 0xffu, 253u);
+  unsigned const ey = min((__float_as_uint(fmaxf(t1.y, fmaxf(t2.y, t3.y))) >> 23) & 0xffu, 253u);
+  float2 const sc = make_float2(__uint_as_float((254u - ex) << 23), __uint_as_float((254u - ey) << 23));
+  float2 const u1 = mul2(t1, sc), u2 = mul2(t2, sc), u3 = mul2(t3, sc);
+  float2 const b1 = mul2(u2, u3);
+  float2 const b2 = mul2(dup2(6.0f), mul2(u1, u3));
+  float2 const b3 = mul2(dup2(3.0f), mul2(u1, u2));
+  float2 const num = fma2(b3, r3, fma2(b2, r2, mul2(b1, r1)));
+  float2 const q = mul2(dup2(6.0f), add2(add2(b1, b2), b3));
+  return fma2(num, make_float2(inv(q.x), inv(q.y)), P2);
+}
+
 // UpwindLeft and UpwindRight of one face from the same six cells a[0..5]
 // (i-2..i+3). The fast build shares the first differences and the second
-// differences centred on a[2] and a[3] between the two.
+// differences centred on a[2] and a[3] between the two (double), or runs the
+// two sides as the lanes of packed f32x2 arithmetic (float).
 template <typename T>
 __device__ __forceinline__ void weno5_pair(T const (&a)[6], T &left, T &right) {
   if constexpr (!ALP_FAST) {
     left = weno5_left(a);
     right = weno5_right(a);
+  } else if constexpr (sizeof(T) == 4) {
+    float2 const r = weno5_packed(make_float2(a[0], a[5]), make_float2(a[1], a[4]),
+                                  make_float2(a[2], a[3]), make_float2(a[3], a[2]),
+                                  make_float2(a[4], a[1]));
+    left = r.x;
+    right = r.y;
   } else {
     T const G0 = a[1] - a[0], G1 = a[2] - a[1], G2 = a[3] - a[2], G3 = a[4] - a[3];
     T const G4 = a[5] - a[4];
@@ -334,6 +384,13 @@ __device__ __forceinline__ void weno5_two(T const (&a)[6], T const (&b)[6], T &l
   if constexpr (!ALP_FAST) {
     left = weno5_left(a);
     right = weno5_right(b);
+  } else if constexpr (sizeof(T) == 4) {
+    // lane y: b mirrored
+    float2 const r = weno5_packed(make_float2(a[0], b[5]), make_float2(a[1], b[4]),
+                                  make_float2(a[2], b[3]), make_float2(a[3], b[2]),
+                                  make_float2(a[4], b[1]));
+    left = r.x;
+    right = r.y;
   } else {
     T const A0 = a[1] - a[0], A1 = a[2] - a[1], A2 = a[3] - a[2], A3 = a[4] - a[3];
     T const B1 = b[2] - b[1], B2 = b[3] - b[2], B3 = b[4] - b[3], B4 = b[5] - b[4];
@@ -535,6 +592,36 @@ __device__ __forceinline__ void to_physical(Roe<T> const &r, T const (&ch)[DIM +
     s = s + ch[EV] * (r.gru * r.H - r.c * r.c);
     out[ENERGY] = s + (ch[0] * (r.H - r.up * r.c) + ch[NE - 1] * (r.H + r.up * r.c));
   }
+}
+
+// to_physical of both sides at once: ch[n] = (left, right) characteristic
+// values; the same right-eigenvector entries, packed.
+template <int DIM, int DIR>
+__device__ __forceinline__ void to_physical_packed(Roe<float> const &r, float2 const (&ch)[DIM + 2],
+                                                   float2 (&out)[DIM + 2]) {
+  constexpr int NE = DIM + 2;
+  constexpr int EV = DIM;
+  constexpr int mP = MOMX + DIR;
+  constexpr int m1 = MOMX + (DIM > 1 ? Minor<DIR>::m1 : 0);
+  constexpr int m2 = MOMX + (DIM > 2 ? Minor<DIR>::m2 : 0);
+  float2 const a = ch[0], z = ch[NE - 1], w = ch[EV];
+  out[MASS] = fma2(w, dup2(r.gru), add2(a, z));
+  out[mP] = fma2(w, dup2(r.gru * r.up), fma2(a, dup2(r.up - r.c), mul2(z, dup2(r.up + r.c))));
+  if constexpr (DIM > 1)
+    out[m1] = fma2(ch[1], dup2(-r.rho),
+                   fma2(w, dup2(r.gru * r.u1), mul2(add2(a, z), dup2(r.u1))));
+  if constexpr (DIM > 2)
+    out[m2] = fma2(ch[2], dup2(r.rho),
+                   fma2(w, dup2(r.gru * r.u2), mul2(add2(a, z), dup2(r.u2))));
+  float2 s = fma2(w, dup2(r.gru * r.H - r.c * r.c),
+                  fma2(a, dup2(r.H - r.up * r.c), mul2(z, dup2(r.H + r.up * r.c))));
+  if constexpr (DIM == 2) s = fma2(ch[1], dup2(-r.u1 * r.rho), s);
+  if constexpr (DIM > 2) {
+    // the two minor-wave products rounded before they are added, as in
+    // to_physical (the same bits with the minor momenta exchanged)
+    s = add2(add2(mul2(ch[1], dup2(-r.u1 * r.rho)), mul2(ch[2], dup2(r.rho * r.u2))), s);
+  }
+  out[ENERGY] = s;
 }
 
 // ---- HLLC with Einfeldt signal speeds -------------------------------------

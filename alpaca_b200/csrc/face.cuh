@@ -210,6 +210,23 @@ __device__ __forceinline__ bool face_compute(Eos const &eos, double B,
         for (int m = 0; m < W; ++m) {
           T sp = T(0), sn = T(0);
           bool first = true;
+          if constexpr (DELTA && ALP_FAST) {
+            // state and flux projections as the two lanes of packed f32x2
+            // arithmetic: (L u, L f) += L[l] (du, df)
+            float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+            for (int q = 0; q < NE; ++q) {
+              int const l = sum_seq<DIM, DIR>(q);
+              if (!left_nonzero<DIM, DIR>(n, l)) continue;
+              float2 const d = make_float2(float(cons[m][l] - cons[C][l]),
+                                           float(advd[m][l] - advd[C][l]));
+              acc = first ? mul2(d, dup2(L[l])) : fma2(d, dup2(L[l]), acc);
+              first = false;
+            }
+            pos[m] = fmaf(alpha, acc.x, acc.y);
+            neg[m] = fmaf(-alpha, acc.x, acc.y);
+            continue;
+          }
 #pragma unroll
           for (int q = 0; q < NE; ++q) {
             int const l = sum_seq<DIM, DIR>(q);

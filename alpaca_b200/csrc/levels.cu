@@ -1513,6 +1513,8 @@ alp_stream_t alp_levels_stream(alp_levels *m) { return m ? (alp_stream_t)m->stre
 // first group never finishes and the waits for it run out.
 int alp_levels_test_stall_ghosts(alp_levels *m) {
   if (!m) return alp::fail(ALP_ERR_INVALID, "null level case");
+  if (!m->graph)
+    return alp::fail(ALP_ERR_INVALID, "no macro step recorded yet: step the case first");
   if (m->stall_next == 0)
     return alp::fail(ALP_ERR_INVALID, "the macro step's first ghost launch has one group");
   ALP_CUDA(cudaStreamSynchronize(m->stream));

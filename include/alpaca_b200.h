@@ -472,7 +472,8 @@ alp_stream_t alp_levels_stream(alp_levels *m);
  * macro step's first ghost launch skips its first group, so the launch's waits
  * for that group run out (about a second) and set the engine's error word;
  * the next alp_levels_get returns ALP_ERR_CUDA and clears it. The leaves are
- * not valid after that step. ALP_ERR_INVALID when that launch has one group. */
+ * not valid after that step. ALP_ERR_INVALID before the first alp_levels_step
+ * (nothing recorded yet) and when that launch has one group. */
 int alp_levels_test_stall_ghosts(alp_levels *m);
 
 /* ---- serving: continuous batching of independent cases ------------------ */

@@ -227,12 +227,15 @@ __global__ void __launch_bounds__(128, FaceOccupancy<SCHEME, T>::min_ctas)
 face_flux_all_kernel(double const *__restrict__ U, int const *__restrict__ work,
                      BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
                      CaseState const *__restrict__ cases, double *__restrict__ F,
-                     long long stride, long long dstride, int chunks) {
+                     long long stride, long long dstride, int chunks,
+                     int const *__restrict__ items) {
   // grid (items x chunks, 1, dir): an item's chunks are consecutive, so the
   // CTAs resident at any time share few blocks' stencils (a few MB of L2
-  // instead of one stencil plane of every item in the launch)
+  // instead of one stencil plane of every item in the launch). items (when
+  // given): the work-list position of each launch position
   int const chunk = (int)(blockIdx.x % chunks);
-  int const item = (int)(blockIdx.x / chunks);
+  int const pos = (int)(blockIdx.x / chunks);
+  int const item = items ? items[pos] : pos;
   int const t = chunk * blockDim.x + threadIdx.x;
   int const slot = work[item];
   BlockMeta const bm = meta[slot];
@@ -287,9 +290,10 @@ face_flux_all_ext_kernel(double const *__restrict__ U, int const *__restrict__ w
                          BlockMeta const *__restrict__ meta, int const *__restrict__ nbr26,
                          CaseState const *__restrict__ cases, double *__restrict__ F,
                          long long stride, long long dstride, ExtPolicy pol0,
-                         unsigned long long const *__restrict__ glf) {
+                         unsigned long long const *__restrict__ glf,
+                         int const *__restrict__ items) {
   int const t = blockIdx.y * blockDim.x + threadIdx.x;
-  int const item = blockIdx.x;
+  int const item = items ? items[blockIdx.x] : (int)blockIdx.x;
   int const slot = work[item];
   BlockMeta const bm = meta[slot];
   if (!(cases[bm.case_id].dt > 0.0)) return;
@@ -868,13 +872,13 @@ cudaError_t face_flux_all_ext(Launch const &L, dim3 grid, int const *nbr26, Case
   ExtPolicy const pol{L.opt};
   switch (L.scheme) {
     case FV_CHAR:
-      face_flux_all_ext_kernel<DIM, FV_CHAR, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      face_flux_all_ext_kernel<DIM, FV_CHAR, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf, L.items);
       break;
     case FV_PRIM:
-      face_flux_all_ext_kernel<DIM, FV_PRIM, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      face_flux_all_ext_kernel<DIM, FV_PRIM, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf, L.items);
       break;
     case FS_ROE:
-      face_flux_all_ext_kernel<DIM, FS_ROE, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf);
+      face_flux_all_ext_kernel<DIM, FS_ROE, W><<<grid, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, pol, L.glf, L.items);
       break;
     default:
       return cudaErrorInvalidValue;
@@ -897,13 +901,13 @@ cudaError_t face_flux_all_t(Launch const &L, int const *nbr26, CaseState const *
   dim3 const g2((unsigned)(L.nwork * chunks), 1, DIM);
   switch (L.scheme) {
     case FV_CHAR:
-      face_flux_all_kernel<DIM, FV_CHAR, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
+      face_flux_all_kernel<DIM, FV_CHAR, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks, L.items);
       break;
     case FV_PRIM:
-      face_flux_all_kernel<DIM, FV_PRIM, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
+      face_flux_all_kernel<DIM, FV_PRIM, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks, L.items);
       break;
     case FS_ROE:
-      face_flux_all_kernel<DIM, FS_ROE, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks);
+      face_flux_all_kernel<DIM, FS_ROE, T><<<g2, threads, 0, L.stream>>>(L.U, L.work, L.meta, nbr26, cases, F, stride, dstride, chunks, L.items);
       break;
     default:
       return cudaErrorInvalidValue;

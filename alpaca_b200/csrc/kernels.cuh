@@ -56,6 +56,10 @@ struct Launch {
   // GlobalLaxFriedrichs wave speeds |u-c|, |u|, |u+c| per case, as the bit
   // patterns of non-negative doubles, 4 words per case (launch_glf_maxima)
   unsigned long long const *glf = nullptr;
+  // launch_face_flux_all only: the work-list positions the launch covers, in
+  // order (nwork of them; null: positions 0 .. nwork-1). Fluxes still go to
+  // the F slot of the work-list position.
+  int const *items = nullptr;
 };
 
 // GlobalLaxFriedrichs: zeroes glf[0 .. 4 ncases) and sets, per case, the

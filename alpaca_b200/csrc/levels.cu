@@ -515,21 +515,23 @@ level_update_kernel(double const *Uin, double const *U0, double *Uout, int const
                     CaseState const *__restrict__ cu, int nupd, JumpRec const *__restrict__ recs,
                     double *__restrict__ jbuf) {
   using G = Geo<DIM>;
-  int const x = blockIdx.x;
+  // 1D grid: the update CTAs of each leaf consecutively (parts of its cells),
+  // then one CTA per jump record
+  constexpr int PARTS = (G::INTERIOR + 255) / 256;
+  int const x = blockIdx.x / PARTS;
   if (x < nupd) {
     int const slot = work[x];
     BlockMeta const bm = meta[slot];
     double const dt = cu[bm.case_id].dt;
     if (!(dt > 0.0)) return;
-    int const t = blockIdx.y * blockDim.x + threadIdx.x;
+    int const t = (blockIdx.x - x * PARTS) * blockDim.x + threadIdx.x;
     if (t >= G::INTERIOR) return;
     stage_update_cell<DIM>(Uin, U0, Uout, F + (long long)x * stride, dstride, slot, t,
                            inv(bm.cell_size), rk_stage(stage, dt));
     return;
   }
-  if (blockIdx.y != 0) return;
   using FC = FaceCells<DIM>;
-  int const ri = x - nupd;
+  int const ri = (int)blockIdx.x - nupd * PARTS;
   JumpRec const r = recs[ri];
   double const dtl = cu[r.level].dt;
   if (!(dtl > 0.0)) return;
@@ -879,7 +881,7 @@ struct alp_levels {
         // stage update of the integrating leaves and their jump sums, one launch
         int const nupd = nwork_ge[lu];
         if (nupd + nrec > 0) {
-          dim3 const grid((unsigned)(nupd + nrec), (unsigned)((cells_interior() + 255) / 256));
+          dim3 const grid((unsigned)(nupd * ((cells_interior() + 255) / 256) + nrec));
           switch (dim) {
             case 1: level_update_kernel<1><<<grid, 256, 0, stream>>>(in[s], U, out[s], work, meta, F, stride(), dstride(), s0 + s, cu, nupd, jrecs, jbuf); break;
             case 2: level_update_kernel<2><<<grid, 256, 0, stream>>>(in[s], U, out[s], work, meta, F, stride(), dstride(), s0 + s, cu, nupd, jrecs, jbuf); break;

@@ -96,7 +96,10 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: through
+    NVML every 5 ms (the GPU found by its PCI bus id, so a restricted device
+    list maps correctly), one sample taken before the region starts and one as
+    it ends; nvidia-smi every 100 ms when NVML is unavailable."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -106,8 +109,46 @@ class ClockSampler:
         self.index = index
         self.rows = []
         self.proc = None
+        self.nvml = None
+        self.stop = threading.Event()
+
+    def _nvml_sample(self):
+        n = self.nvml
+        sm = n.nvmlDeviceGetClockInfo(self.h, n.NVML_CLOCK_SM)
+        mx = n.nvmlDeviceGetMaxClockInfo(self.h, n.NVML_CLOCK_SM)
+        r = n.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+        flag = lambda bit: "Active" if r & bit else "Not Active"
+        self.rows.append([str(self.index), str(sm), str(mx), "", hex(r),
+                          flag(n.nvmlClocksEventReasonHwSlowdown),
+                          flag(n.nvmlClocksEventReasonHwThermalSlowdown),
+                          flag(n.nvmlClocksEventReasonSwThermalSlowdown),
+                          flag(n.nvmlClocksEventReasonSwPowerCap)])
+
+    def _nvml_loop(self):
+        while not self.stop.wait(0.005):
+            try:
+                self._nvml_sample()
+            except Exception:
+                return
 
     def __enter__(self):
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            try:
+                import torch
+                pr = torch.cuda.get_device_properties(self.index)
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                self.h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.nvml = pynvml
+            self._nvml_sample()
+            self.thread = threading.Thread(target=self._nvml_loop, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
@@ -123,6 +164,18 @@ class ClockSampler:
             self.rows.append([x.strip() for x in line.split(",")])
 
     def __exit__(self, *a):
+        if self.nvml:
+            try:
+                self._nvml_sample()
+            except Exception:
+                pass
+            self.stop.set()
+            self.thread.join(timeout=1)
+            try:
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return
         if self.proc:
             time.sleep(0.25)
             self.proc.terminate()
